@@ -1,0 +1,160 @@
+// M2L on CUDA cores over the dense class-major grid of one level.
+//
+//   L(F) = sum_{S in IL(F)} E_{k(F,S)} M(S)     (m2l_kern_basic.cu:82-130 semantics,
+//                                                k from m2l_aux.c:1135-1191)
+//
+// For a target of sibling class b = (bx,by,bz) the interaction list is the set of
+// offsets v with v_a in [-2-b_a, 3-b_a] and max|v_a| > 1: 189 offsets per class
+// (anotherInteractionList.c:46-110 on a full tree). Out-of-grid sources contribute
+// zero, which reproduces the shorter lists of boundary cells.
+//
+// CTA tile: a box of up to 4x4x4 targets of one class x all r outputs. The kernel loops
+// over the class's offsets and over chunks of 16 contraction indices j in [j0, j1),
+// staging the shifted source box and the operator chunk in shared memory, and keeps a
+// register-blocked accumulator. With [j0, j1) = [0, r) this is the plain FP64 (or FP32)
+// M2L; with [0, 16) it is the FP64 leading-component part of the mixed-precision M2L.
+//
+// Operators: Ert[k][i][j] = E_k(i, j) (row-major), i.e. the transpose of the
+// reference's column-major K file blocks.
+#include "common.cuh"
+
+namespace bbfmm {
+
+struct OffsetTable {
+  // per class c: 189 entries (k, vx, vy, vz) packed as int4
+  const int4 *offs;
+};
+
+template <typename T, int R, int TM, int TN>
+__global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, const T *__restrict__ Ert,
+                                                       T *__restrict__ Lout, int level, int j0, int j1,
+                                                       const int4 *__restrict__ offs, int accumulate) {
+  constexpr int BK = 16;
+  constexpr int NT = 64;  // targets per tile (4x4x4 box)
+  static_assert((NT / TM) * (R / TN) == 256, "thread tile must cover the CTA tile");
+  constexpr int TGX = NT / TM;  // thread groups along targets
+  __shared__ T sa[BK][NT];
+  __shared__ T sb[BK][R + (sizeof(T) == 8 ? 1 : 0)];
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;  // box width per dimension
+  const int nbox = P / bw;
+  const int tiles_per_class = nbox * nbox * nbox;
+  const int c = blockIdx.x / tiles_per_class;
+  const int tb = blockIdx.x % tiles_per_class;
+  const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
+  const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
+  const int nt = bw * bw * bw;
+  const int tid = threadIdx.x;
+  const int tg = tid % TGX, og = tid / TGX;
+  T acc[TM][TN];
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TN; ++b) acc[a][b] = 0;
+  const int64_t P3 = (int64_t)P * P * P;
+  for (int o = 0; o < 189; ++o) {
+    const int4 ov = offs[c * 189 + o];
+    const int k = ov.x;
+    // source class and parent-grid shift for this class/offset
+    const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
+    const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
+    const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
+    const int sc = (scx << 2) | (scy << 1) | scz;
+    for (int jc = j0; jc < j1; jc += BK) {
+      __syncthreads();
+      for (int e = tid; e < NT * BK; e += 256) {
+        const int t = e / BK, jj = e % BK;
+        T v = 0;
+        if (t < nt && jc + jj < j1) {
+          const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
+          if (px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P)
+            v = M[(((int64_t)sc * P3 + ((int64_t)pz * P + py) * P + px)) * R + jc + jj];
+        }
+        sa[jj][t] = v;
+      }
+      const T *Ek = Ert + (int64_t)k * R * R;
+      for (int e = tid; e < R * BK; e += 256) {
+        const int i = e / BK, jj = e % BK;
+        sb[jj][i] = (jc + jj < j1) ? Ek[(int64_t)i * R + jc + jj] : (T)0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int jj = 0; jj < BK; ++jj) {
+        T a[TM], b[TN];
+#pragma unroll
+        for (int x = 0; x < TM; ++x) a[x] = sa[jj][tg + TGX * x];
+#pragma unroll
+        for (int y = 0; y < TN; ++y) b[y] = sb[jj][og + (R / TN) * y];
+#pragma unroll
+        for (int x = 0; x < TM; ++x)
+#pragma unroll
+          for (int y = 0; y < TN; ++y) acc[x][y] += a[x] * b[y];
+      }
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < TM; ++x) {
+    const int t = tg + TGX * x;
+    if (t >= nt) continue;
+    const int px = bxo + (t % bw), py = byo + ((t / bw) % bw), pz = bzo + (t / (bw * bw));
+    T *dst = Lout + (((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px)) * R;
+#pragma unroll
+    for (int y = 0; y < TN; ++y) {
+      const int i = og + (R / TN) * y;
+      if (accumulate) dst[i] += acc[x][y];
+      else dst[i] = acc[x][y];
+    }
+  }
+}
+
+int m2l_simt_tiles(int level) {
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;
+  const int nbox = P / bw;
+  return 8 * nbox * nbox * nbox;
+}
+
+template <typename T>
+int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs,
+                    int accumulate, cudaStream_t s) {
+  const int grid = m2l_simt_tiles(level);
+  if (r == 256) {
+    m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, Lout, level, j0, j1, offs, accumulate);
+  } else if (r == 32) {
+    m2l_simt_kernel<T, 32, 2, 4><<<grid, 256, 0, s>>>(M, Ert, Lout, level, j0, j1, offs, accumulate);
+  } else {
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L rank must be 32 or 256 (n = 4 or 8)");
+  }
+  return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_simt", __FILE__, __LINE__);
+}
+
+template int launch_m2l_simt<double>(int, const double *, const double *, double *, int, int, int, const int4 *, int,
+                                     cudaStream_t);
+template int launch_m2l_simt<float>(int, const float *, const float *, float *, int, int, int, const int4 *, int,
+                                    cudaStream_t);
+
+// Host table of the 189 offsets of each sibling class, as (k, vx, vy, vz).
+void build_offset_table(int *out /* 8*189*4 */) {
+  for (int c = 0; c < 8; ++c) {
+    const int b[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
+    int cnt = 0;
+    int k = 0;
+    for (int vx = -3; vx <= 3; ++vx)
+      for (int vy = -3; vy <= 3; ++vy)
+        for (int vz = -3; vz <= 3; ++vz) {
+          const bool far = vx < -1 || vx > 1 || vy < -1 || vy > 1 || vz < -1 || vz > 1;
+          if (!far) continue;
+          const int v[3] = {vx, vy, vz};
+          bool ok = true;
+          for (int a = 0; a < 3; ++a) ok = ok && v[a] >= -2 - b[a] && v[a] <= 3 - b[a];
+          if (ok) {
+            int *e = out + 4 * (c * 189 + cnt);
+            e[0] = k; e[1] = vx; e[2] = vy; e[3] = vz;
+            ++cnt;
+          }
+          ++k;
+        }
+  }
+}
+
+}  // namespace bbfmm

@@ -1,0 +1,152 @@
+// Near-field P2P: phi_i += q_i * sum_{B in N(A)} sum_{j in B, r_ij != 0} q_j / r_ij over
+// the <= 27 neighbour leaves of each leaf (reference: anotherNearField.c:141-206 on the
+// CPU, direct.cu:69-209 on the GPU).
+//
+// One thread per target particle; particles are leaf-sorted, so a warp covers a run of
+// neighbouring leaves and the source particles it streams are shared through L1.
+//  * p2p_kernel<T>: positions and arithmetic in T (the reference's d and s builds),
+//    1/sqrt as in the reference's CPU code.
+//  * p2p_local_kernel: FP32 arithmetic on leaf-local coordinates. Each particle carries
+//    its offset from its own leaf centre in FP32; a pair's separation is
+//    (xl_j - xl_i) + (c_B - c_A), where the centre difference is a multiple of the leaf
+//    length and exact in FP32, so the separation keeps FP32 relative accuracy instead of
+//    losing the bits of the absolute coordinate. Per-target sums are Neumaier-compensated
+//    and the result is added to an FP64 potential.
+#include "common.cuh"
+
+namespace bbfmm {
+
+template <typename T>
+__global__ void __launch_bounds__(256) p2p_kernel(int N, const T *__restrict__ pos4, const int *__restrict__ leaf_start,
+                                                  const int *__restrict__ leafm, int maxlev, T *__restrict__ phi) {
+  const int ncpd = 1 << maxlev;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const T fx = pos4[4 * (int64_t)i], fy = pos4[4 * (int64_t)i + 1], fz = pos4[4 * (int64_t)i + 2];
+    const T qi = pos4[4 * (int64_t)i + 3];
+    int ix, iy, iz;
+    morton_to_grid(leafm[i], maxlev, ix, iy, iz);
+    T v = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int jx = ix + dx;
+      if (jx < 0 || jx >= ncpd) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jy = iy + dy;
+        if (jy < 0 || jy >= ncpd) continue;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int jz = iz + dz;
+          if (jz < 0 || jz >= ncpd) continue;
+          const int64_t B = grid_to_morton(jx, jy, jz, maxlev);
+          const int s0 = leaf_start[B], s1 = leaf_start[B + 1];
+          for (int s = s0; s < s1; ++s) {
+            const T ex = pos4[4 * (int64_t)s] - fx, ey = pos4[4 * (int64_t)s + 1] - fy,
+                    ez = pos4[4 * (int64_t)s + 2] - fz;
+            const T rr = ex * ex + ey * ey + ez * ez;
+            if (rr != (T)0) v += pos4[4 * (int64_t)s + 3] * ((T)1 / sqrt(rr));
+          }
+        }
+      }
+    }
+    phi[i] += qi * v;
+  }
+}
+
+// loc4 = (x - c_leaf, y - c_leaf, z - c_leaf, q) in FP32; h = leaf length.
+__global__ void __launch_bounds__(256) p2p_local_kernel(int N, const float4 *__restrict__ loc4,
+                                                        const int *__restrict__ leaf_start,
+                                                        const int *__restrict__ leafm, int maxlev, float h,
+                                                        double *__restrict__ phi) {
+  const int ncpd = 1 << maxlev;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const float4 f = loc4[i];
+    int ix, iy, iz;
+    morton_to_grid(leafm[i], maxlev, ix, iy, iz);
+    float sum = 0.f, comp = 0.f;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int jx = ix + dx;
+      if (jx < 0 || jx >= ncpd) continue;
+      const float ox = (float)dx * h;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jy = iy + dy;
+        if (jy < 0 || jy >= ncpd) continue;
+        const float oy = (float)dy * h;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int jz = iz + dz;
+          if (jz < 0 || jz >= ncpd) continue;
+          const float oz = (float)dz * h;
+          const int64_t B = grid_to_morton(jx, jy, jz, maxlev);
+          const int s0 = leaf_start[B], s1 = leaf_start[B + 1];
+          for (int s = s0; s < s1; ++s) {
+            const float4 g = loc4[s];
+            const float ex = (g.x - f.x) + ox, ey = (g.y - f.y) + oy, ez = (g.z - f.z) + oz;
+            const float rr = ex * ex + ey * ey + ez * ez;
+            if (rr != 0.f) {
+              const float t = g.w * rsqrtf(rr);
+              const float y = sum + t;
+              comp += (fabsf(sum) >= fabsf(t)) ? ((sum - y) + t) : ((t - y) + sum);
+              sum = y;
+            }
+          }
+        }
+      }
+    }
+    phi[i] += (double)f.w * ((double)sum + (double)comp);
+  }
+}
+
+// Leaf-local FP32 coordinates from FP64 sorted positions.
+__global__ void make_local_kernel(int N, const double *__restrict__ pos4, const int *__restrict__ leafm, int maxlev,
+                                  double L, float4 *__restrict__ loc4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    morton_to_grid(leafm[i], maxlev, ix, iy, iz);
+    loc4[i] = make_float4((float)(pos4[4 * (int64_t)i] - cell_center_1d<double>(ix, maxlev, L)),
+                          (float)(pos4[4 * (int64_t)i + 1] - cell_center_1d<double>(iy, maxlev, L)),
+                          (float)(pos4[4 * (int64_t)i + 2] - cell_center_1d<double>(iz, maxlev, L)),
+                          (float)pos4[4 * (int64_t)i + 3]);
+  }
+}
+
+// Per-particle leaf (Morton) index from the leaf ranges.
+__global__ void leaf_of_kernel(int64_t nleaf, const int *__restrict__ leaf_start, int *__restrict__ leafm) {
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nleaf; m += (int64_t)gridDim.x * blockDim.x)
+    for (int p = leaf_start[m]; p < leaf_start[m + 1]; ++p) leafm[p] = (int)m;
+}
+
+static int p2p_grid(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 148 * 64) g = 148 * 64;
+  return (int)g;
+}
+
+template <typename T>
+int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  p2p_kernel<T><<<p2p_grid(N), 256, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "p2p", __FILE__, __LINE__);
+}
+template int launch_p2p<double>(int, const double *, const int *, const int *, int, double *, cudaStream_t);
+template int launch_p2p<float>(int, const float *, const int *, const int *, int, float *, cudaStream_t);
+
+int launch_p2p_local(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L,
+                     double *phi, cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  const float h = (float)cell_length<double>(maxlev, L);
+  p2p_local_kernel<<<p2p_grid(N), 256, 0, s>>>(N, loc4, leaf_start, leafm, maxlev, h, phi);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "p2p_local", __FILE__, __LINE__);
+}
+
+int launch_make_local(int N, const double *pos4, const int *leafm, int maxlev, double L, float4 *loc4,
+                      cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  make_local_kernel<<<p2p_grid(N), 256, 0, s>>>(N, pos4, leafm, maxlev, L, loc4);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "make_local", __FILE__, __LINE__);
+}
+
+int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s) {
+  const int64_t nleaf = pow8i(maxlev);
+  leaf_of_kernel<<<p2p_grid(nleaf), 256, 0, s>>>(nleaf, leaf_start, leafm);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "leaf_of", __FILE__, __LINE__);
+}
+
+}  // namespace bbfmm

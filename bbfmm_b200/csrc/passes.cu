@@ -1,0 +1,492 @@
+// Upward and downward passes on the device (P2M, M2M, L2L, L2P), the U-projections
+// around M2L, and the particle permutations. Expansions stay resident in HBM.
+//
+// Reference semantics (all CPU in the reference):
+//   P2M  anotherUpwardPass.c:61-330   S = (2/n)^3 sum_p q_p Sx(x_p) Sy(y_p) Sz(z_p)
+//   M2M  anotherUpwardPass.c:345-539  z, then y, then x contraction with Cweights
+//   proj anotherUpwardPass.c:311-324  P = U^T (S o Kweights)       (atransx.c:48-86)
+//   post auxAnotherFMMInteraction.c:398-416  F = (1/L_l) Kweights o (U PF)
+//   L2L  anotherDownwardPassX.c:40-211  x, then y, then z interpolation, accumulated
+//   L2P  anotherDownwardPassX.c:226-331  phi_p = q_p (2/n)^3 sum F Sx Sy Sz
+// The summation order of each output follows the reference loops.
+#include "common.cuh"
+
+namespace bbfmm {
+
+// Clenshaw evaluation of S(x_m, x) for all nodes m (bbfmm.c:1682-1690).
+template <typename T, int NN>
+__device__ __forceinline__ void sn_nodes(const T *__restrict__ tkz, T x, T *out) {
+#pragma unroll
+  for (int m = 0; m < NN; ++m) {
+    T d1 = 0, d2 = 0;
+#pragma unroll
+    for (int j = NN - 1; j > 0; --j) {
+      const T d0 = 2 * x * d1 - d2 + tkz[m * NN + j];
+      d2 = d1;
+      d1 = d0;
+    }
+    out[m] = x * d1 - d2 + (T)0.5 * tkz[m * NN];
+  }
+}
+
+template <typename T> __device__ __forceinline__ const T *tab_tkz(const Tables &t);
+template <> __device__ __forceinline__ const double *tab_tkz<double>(const Tables &t) { return t.tkz_d; }
+template <> __device__ __forceinline__ const float *tab_tkz<float>(const Tables &t) { return t.tkz_f; }
+template <typename T> __device__ __forceinline__ const T *tab_cw(const Tables &t);
+template <> __device__ __forceinline__ const double *tab_cw<double>(const Tables &t) { return t.cw_d; }
+template <> __device__ __forceinline__ const float *tab_cw<float>(const Tables &t) { return t.cw_f; }
+
+// ----------------------------------------------------------------------------- P2M
+// One warp per leaf (grid-stride). pos4 = (x, y, z, q) in leaf-sorted order.
+// S_leaf[m * n3 + l], Morton order at maxlev.
+template <typename T, int NN>
+__global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
+                                                  int maxlev, T L, Tables tabs, T *__restrict__ S) {
+  constexpr int N3 = NN * NN * NN;
+  constexpr int PER = (N3 + 31) / 32;
+  __shared__ T s_tkz[NN * NN];
+  const T *tkz = tab_tkz<T>(tabs);
+  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nleaf = pow8i(maxlev);
+  const T len = cell_length<T>(maxlev, L);
+  const T ihalf = (T)1 / (len / (T)2);
+  const T prefac = (T)2 / (T)NN;
+  const T pre3 = prefac * prefac * prefac;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t m = warp; m < nleaf; m += nwarps) {
+    int ix, iy, iz;
+    morton_to_grid(m, maxlev, ix, iy, iz);
+    const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
+            cz = cell_center_1d<T>(iz, maxlev, L);
+    T acc[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) acc[k] = 0;
+    const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
+    for (int p = p0; p < p1; ++p) {
+      const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
+      const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
+      const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
+      const T q = pos4[4 * (int64_t)p + 3];
+      T sx[NN], sy[NN], sz[NN];
+      sn_nodes<T, NN>(s_tkz, x, sx);
+      sn_nodes<T, NN>(s_tkz, y, sy);
+      sn_nodes<T, NN>(s_tkz, z, sz);
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int l = lane + 32 * k;
+        if (l < N3) {
+          const int l1 = l / (NN * NN), l2 = (l / NN) % NN, l3 = l % NN;
+          const T w = q * sx[l1] * sy[l2];
+          acc[k] += w * sz[l3];
+        }
+      }
+    }
+    T *out = S + m * N3;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int l = lane + 32 * k;
+      if (l < N3) out[l] = pre3 * acc[k];
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- M2M
+// One CTA per parent (grid-stride): children S (level l+1, Morton, contiguous block of
+// 8 n^3) -> parent S (level l). All eight children are visited.
+template <typename T, int NN>
+__global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *__restrict__ Sp, int level,
+                                                  Tables tabs) {
+  constexpr int N2 = NN * NN, N3 = N2 * NN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sc = reinterpret_cast<T *>(smem_raw);  // 8 * N3
+  T *sz = sc + 8 * N3;                       // 4 * N3
+  T *sy = sz + 4 * N3;                       // 2 * N3
+  __shared__ T cw[2 * N2];
+  const T *cwg = tab_cw<T>(tabs);
+  for (int i = threadIdx.x; i < 2 * N2; i += blockDim.x) cw[i] = cwg[i];
+  const T prefac = (T)2 / (T)NN;
+  const T pre3 = prefac * prefac * prefac;
+  const int64_t ncell = pow8i(level);
+  for (int64_t A = blockIdx.x; A < ncell; A += gridDim.x) {
+    __syncthreads();
+    const T *src = Sc + A * 8 * N3;
+    for (int i = threadIdx.x; i < 8 * N3; i += blockDim.x) sc[i] = src[i];
+    __syncthreads();
+    // z: sz[(j/2) n3 + l1 n + l3] = sum over zbit of sum_m child_j[l1 n + m] C[zbit][l3][m]
+    for (int o = threadIdx.x; o < 4 * N3; o += blockDim.x) {
+      const int jj = o / N3, rem = o % N3, l1 = rem / NN, l3 = rem % NN;
+      T v = 0;
+#pragma unroll
+      for (int zb = 0; zb < 2; ++zb) {
+        const T *ch = sc + (2 * jj + zb) * N3 + l1 * NN;
+        const T *c = cw + zb * N2 + l3 * NN;
+        T s = 0;
+#pragma unroll
+        for (int m = 0; m < NN; ++m) s += ch[m] * c[m];
+        v += s;
+      }
+      sz[o] = v;
+    }
+    __syncthreads();
+    // y: sy[(j/2) n3 + l1 n2 + l2 n + l3] = sum over ybit of sum_m sz[j n3 + l1 n2 + m n + l3] C[ybit][l2][m]
+    for (int o = threadIdx.x; o < 2 * N3; o += blockDim.x) {
+      const int xb = o / N3, rem = o % N3, l1 = rem / N2, l2 = (rem / NN) % NN, l3 = rem % NN;
+      T v = 0;
+#pragma unroll
+      for (int yb = 0; yb < 2; ++yb) {
+        const int j = 2 * xb + yb;
+        const T *c = cw + yb * N2 + l2 * NN;
+        T s = 0;
+#pragma unroll
+        for (int m = 0; m < NN; ++m) s += sz[j * N3 + l1 * N2 + m * NN + l3] * c[m];
+        v += s;
+      }
+      sy[o] = v;
+    }
+    __syncthreads();
+    // x: S[l1 n2 + l2 n + l3] = sum over xbit of sum_m sy[j n3 + m n2 + l2 n + l3] C[xbit][l1][m]
+    T *dst = Sp + A * N3;
+    for (int o = threadIdx.x; o < N3; o += blockDim.x) {
+      const int l1 = o / N2, l2 = (o / NN) % NN, l3 = o % NN;
+      T v = 0;
+#pragma unroll
+      for (int xb = 0; xb < 2; ++xb) {
+        const T *c = cw + xb * N2 + l1 * NN;
+        T s = 0;
+#pragma unroll
+        for (int m = 0; m < NN; ++m) s += sy[xb * N3 + m * N2 + l2 * NN + l3] * c[m];
+        v += s;
+      }
+      dst[o] = v * pre3;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- L2L
+// One CTA per parent: F_child[j] += (2/n)^3 * interp_j(F_parent), children contiguous.
+template <typename T, int NN>
+__global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *__restrict__ Fc, int level,
+                                                  Tables tabs) {
+  constexpr int N2 = NN * NN, N3 = N2 * NN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *fp = reinterpret_cast<T *>(smem_raw);  // N3
+  T *fx = fp + N3;                           // 2 * N3
+  T *fy = fx + 2 * N3;                       // 4 * N3
+  __shared__ T cw[2 * N2];
+  const T *cwg = tab_cw<T>(tabs);
+  for (int i = threadIdx.x; i < 2 * N2; i += blockDim.x) cw[i] = cwg[i];
+  const T prefac = (T)2 / (T)NN;
+  const T pre3 = prefac * prefac * prefac;
+  const int64_t ncell = pow8i(level);
+  for (int64_t A = blockIdx.x; A < ncell; A += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) fp[i] = Fp[A * N3 + i];
+    __syncthreads();
+    // Fx[j n3 + l1 n2 + l2 n + l3] = sum_m F[m n2 + l2 n + l3] C[j][m][l1]
+    for (int o = threadIdx.x; o < 2 * N3; o += blockDim.x) {
+      const int j = o / N3, rem = o % N3, l1 = rem / N2, l2 = (rem / NN) % NN, l3 = rem % NN;
+      T s = 0;
+#pragma unroll
+      for (int m = 0; m < NN; ++m) s += fp[m * N2 + l2 * NN + l3] * cw[j * N2 + m * NN + l1];
+      fx[o] = s;
+    }
+    __syncthreads();
+    // Fy[j n3 + l1 n2 + l2 n + l3] = sum_m Fx[(j/2) n3 + l1 n2 + m n + l3] C[j%2][m][l2]
+    for (int o = threadIdx.x; o < 4 * N3; o += blockDim.x) {
+      const int j = o / N3, rem = o % N3, l1 = rem / N2, l2 = (rem / NN) % NN, l3 = rem % NN;
+      T s = 0;
+#pragma unroll
+      for (int m = 0; m < NN; ++m) s += fx[(j / 2) * N3 + l1 * N2 + m * NN + l3] * cw[(j % 2) * N2 + m * NN + l2];
+      fy[o] = s;
+    }
+    __syncthreads();
+    // Fchild_j[l1l2 n + l3] += pre3 * sum_m Fy[(j/2) n3 + l1l2 n + m] C[j%2][m][l3]
+    for (int o = threadIdx.x; o < 8 * N3; o += blockDim.x) {
+      const int j = o / N3, rem = o % N3, l12 = rem / NN, l3 = rem % NN;
+      T s = 0;
+#pragma unroll
+      for (int m = 0; m < NN; ++m) s += fy[(j / 2) * N3 + l12 * NN + m] * cw[(j % 2) * N2 + m * NN + l3];
+      Fc[(A * 8 + j) * N3 + rem] += pre3 * s;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- L2P
+// One warp per leaf; phi_sorted[p] = q_p (2/n)^3 sum_l F[l] Sx Sy Sz (assign).
+template <typename T, int NN>
+__global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
+                                                  int maxlev, T L, Tables tabs, const T *__restrict__ F,
+                                                  T *__restrict__ phi) {
+  constexpr int N2 = NN * NN, N3 = N2 * NN;
+  __shared__ T s_tkz[NN * NN];
+  const T *tkz = tab_tkz<T>(tabs);
+  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nleaf = pow8i(maxlev);
+  const T len = cell_length<T>(maxlev, L);
+  const T ihalf = (T)1 / (len / (T)2);
+  const T prefac = (T)2 / (T)NN;
+  const T pre3 = prefac * prefac * prefac;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t m = warp; m < nleaf; m += nwarps) {
+    const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
+    if (p1 == p0) continue;
+    int ix, iy, iz;
+    morton_to_grid(m, maxlev, ix, iy, iz);
+    const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
+            cz = cell_center_1d<T>(iz, maxlev, L);
+    const T *Fm = F + m * N3;
+    for (int p = p0; p < p1; ++p) {
+      const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
+      const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
+      const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
+      const T q = pos4[4 * (int64_t)p + 3];
+      T sx[NN], sy[NN], sz[NN];
+      sn_nodes<T, NN>(s_tkz, x, sx);
+      sn_nodes<T, NN>(s_tkz, y, sy);
+      sn_nodes<T, NN>(s_tkz, z, sz);
+      // lanes split the (l1, l2) pairs; each sums its l3 row
+      T part = 0;
+      for (int l12 = lane; l12 < N2; l12 += 32) {
+        const int l1 = l12 / NN, l2 = l12 % NN;
+        const T *f = Fm + l12 * NN;
+        T inner = 0;
+#pragma unroll
+        for (int l3 = 0; l3 < NN; ++l3) inner += sz[l3] * f[l3];
+        part += sx[l1] * sy[l2] * inner;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+      if (lane == 0) phi[p] = q * pre3 * part;
+    }
+  }
+}
+
+// --------------------------------------------------------------- projections (GEMM)
+// C[out_row(m)][0:N] = scale * cs[0:N] o sum_k A[in_row(m)][k] B[k][0:N] for m < M,
+// where rows are mapped between Morton and cpg order at the given level.
+// A may be the sum of two sources (T and float) for the split M2L output.
+// Register-blocked SIMT GEMM: CTA tile 128 x BN, K-chunks of 16, 256 threads.
+__device__ __forceinline__ int64_t map_row(int64_t m, int level, int which, int mode) {
+  if (mode == which) {
+    int ix, iy, iz;
+    morton_to_grid(m, level, ix, iy, iz);
+    return grid_to_cpg(ix, iy, iz, level);
+  }
+  return m;
+}
+
+template <typename T, int BN>
+__global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N, const T *__restrict__ A,
+                                                        const float *__restrict__ A2, const T *__restrict__ B,
+                                                        const T *__restrict__ cs, T scale, T *__restrict__ C,
+                                                        int level, int mapmode) {
+  constexpr int BM = 128, BK = 16, TN = BN / 16;
+  __shared__ T sa[BK][BM + 1];
+  __shared__ T sb[BK][BN];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int64_t m0 = (int64_t)blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  T acc[8][TN];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0;
+  // each thread loads 8 A elements (rows) per chunk
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    for (int e = threadIdx.x; e < BM * BK; e += 256) {
+      const int r = e / BK, c = e % BK;
+      const int64_t m = m0 + r;
+      T v = 0;
+      if (m < M && k0 + c < K) {
+        const int64_t ar = map_row(m, level, MAP_IN_CPG, mapmode);
+        v = A[ar * K + k0 + c];
+        if (A2) v += (T)A2[ar * K + k0 + c];
+      }
+      sa[c][r] = v;
+    }
+    for (int e = threadIdx.x; e < BK * BN; e += 256) {
+      const int r = e / BN, c = e % BN;
+      sb[r][c] = (k0 + r < K && n0 + c < N) ? B[(int64_t)(k0 + r) * N + n0 + c] : (T)0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      T a[8], b[TN];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = sa[k][ty * 8 + i];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) b[j] = sb[k][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t m = m0 + ty * 8 + i;
+    if (m >= M) continue;
+    const int64_t cr = map_row(m, level, MAP_OUT_CPG, mapmode);
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int n = n0 + tx + 16 * j;
+      if (n < N) C[cr * N + n] = scale * (cs ? cs[n] : (T)1) * acc[i][j];
+    }
+  }
+}
+
+// ----------------------------------------------------------------- permutations
+template <typename T, typename TI>
+__global__ void gather_pos4_kernel(int N, const int *__restrict__ perm, const TI *__restrict__ xyz,
+                                   const TI *__restrict__ q, T *__restrict__ pos4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const int k = perm[i];
+    if (xyz) {
+      pos4[4 * (int64_t)i] = (T)xyz[3 * (int64_t)k];
+      pos4[4 * (int64_t)i + 1] = (T)xyz[3 * (int64_t)k + 1];
+      pos4[4 * (int64_t)i + 2] = (T)xyz[3 * (int64_t)k + 2];
+    }
+    if (q) pos4[4 * (int64_t)i + 3] = (T)q[k];
+  }
+}
+
+template <typename T, typename TO>
+__global__ void scatter_phi_kernel(int N, const int *__restrict__ perm, const T *__restrict__ phis,
+                                   TO *__restrict__ phi) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    phi[perm[i]] = (TO)phis[i];
+}
+
+// Morton-ordered r-vectors (reference layout, one level) <-> cpg layout.
+template <typename T>
+__global__ void morton_to_cpg_kernel(int level, int r, const T *__restrict__ src, T *__restrict__ dst, int inverse) {
+  const int64_t total = pow8i(level) * r;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = e / r;
+    const int j = (int)(e % r);
+    int ix, iy, iz;
+    morton_to_grid(m, level, ix, iy, iz);
+    const int64_t c = grid_to_cpg(ix, iy, iz, level);
+    if (inverse) dst[m * r + j] = src[c * r + j];
+    else dst[c * r + j] = src[m * r + j];
+  }
+}
+
+// ------------------------------------------------------------------ launchers
+static int grid_for(int64_t work, int per_block, int cap) {
+  int64_t g = (work + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+template <typename T>
+int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s) {
+  const int64_t nleaf = pow8i(maxlev);
+  const int grid = grid_for(nleaf, 4, 148 * 64);
+  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S);
+  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S);
+  else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
+  return bbfmm_set_cuda_error(cudaGetLastError(), "p2m", __FILE__, __LINE__);
+}
+
+template <typename T>
+int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s) {
+  const int n3 = n * n * n;
+  const size_t smem = sizeof(T) * 14 * n3;
+  const int grid = grid_for(pow8i(level), 1, 148 * 8);
+  if (n == 4) {
+    m2m_kernel<T, 4><<<grid, 256, smem, s>>>(Sc, Sp, level, t);
+  } else if (n == 8) {
+    cudaFuncSetAttribute(m2m_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    m2m_kernel<T, 8><<<grid, 256, smem, s>>>(Sc, Sp, level, t);
+  } else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
+  return bbfmm_set_cuda_error(cudaGetLastError(), "m2m", __FILE__, __LINE__);
+}
+
+template <typename T>
+int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s) {
+  const int n3 = n * n * n;
+  const size_t smem = sizeof(T) * 7 * n3;
+  const int grid = grid_for(pow8i(level), 1, 148 * 8);
+  if (n == 4) {
+    l2l_kernel<T, 4><<<grid, 256, smem, s>>>(Fp, Fc, level, t);
+  } else if (n == 8) {
+    cudaFuncSetAttribute(l2l_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    l2l_kernel<T, 8><<<grid, 256, smem, s>>>(Fp, Fc, level, t);
+  } else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
+  return bbfmm_set_cuda_error(cudaGetLastError(), "l2l", __FILE__, __LINE__);
+}
+
+template <typename T>
+int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi,
+               cudaStream_t s) {
+  const int grid = grid_for(pow8i(maxlev), 4, 148 * 64);
+  if (n == 4) l2p_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi);
+  else if (n == 8) l2p_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi);
+  else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
+  return bbfmm_set_cuda_error(cudaGetLastError(), "l2p", __FILE__, __LINE__);
+}
+
+template <typename T>
+int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C,
+                int level, int mapmode, cudaStream_t s) {
+  if (M <= 0) return BBFMM_OK;
+  if (N >= 64) {
+    dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 63) / 64));
+    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode);
+  } else {
+    dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 31) / 32));
+    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode);
+  }
+  return bbfmm_set_cuda_error(cudaGetLastError(), "proj", __FILE__, __LINE__);
+}
+
+template <typename T, typename TI>
+int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  gather_pos4_kernel<T, TI><<<grid_for(N, 256, 148 * 32), 256, 0, s>>>(N, perm, xyz, q, pos4);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "gather", __FILE__, __LINE__);
+}
+
+template <typename T, typename TO>
+int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  scatter_phi_kernel<T, TO><<<grid_for(N, 256, 148 * 32), 256, 0, s>>>(N, perm, phis, phi);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "scatter", __FILE__, __LINE__);
+}
+
+template <typename T>
+int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s) {
+  morton_to_cpg_kernel<T><<<grid_for(pow8i(level) * r, 256, 148 * 32), 256, 0, s>>>(level, r, src, dst, inverse);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "morton_cpg", __FILE__, __LINE__);
+}
+
+#define INST(T)                                                                                           \
+  template int launch_p2m<T>(int, const T *, const int *, int, T, const Tables &, T *, cudaStream_t);      \
+  template int launch_m2m<T>(int, const T *, T *, int, const Tables &, cudaStream_t);                      \
+  template int launch_l2l<T>(int, const T *, T *, int, const Tables &, cudaStream_t);                      \
+  template int launch_l2p<T>(int, const T *, const int *, int, T, const Tables &, const T *, T *,          \
+                             cudaStream_t);                                                                \
+  template int launch_proj<T>(int64_t, int, int, const T *, const float *, const T *, const T *, T, T *,   \
+                              int, int, cudaStream_t);                                                     \
+  template int launch_morton_cpg<T>(int, int, const T *, T *, int, cudaStream_t);
+INST(float)
+INST(double)
+template int launch_gather<double, double>(int, const int *, const double *, const double *, double *, cudaStream_t);
+template int launch_gather<float, double>(int, const int *, const double *, const double *, float *, cudaStream_t);
+template int launch_gather<float, float>(int, const int *, const float *, const float *, float *, cudaStream_t);
+template int launch_gather<double, float>(int, const int *, const float *, const float *, double *, cudaStream_t);
+template int launch_scatter<double, double>(int, const int *, const double *, double *, cudaStream_t);
+template int launch_scatter<float, float>(int, const int *, const float *, float *, cudaStream_t);
+template int launch_scatter<float, double>(int, const int *, const float *, double *, cudaStream_t);
+template int launch_scatter<double, float>(int, const int *, const double *, float *, cudaStream_t);
+
+}  // namespace bbfmm

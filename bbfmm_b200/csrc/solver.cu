@@ -1,0 +1,498 @@
+// Device-resident FMM solve: orchestration of the pass kernels, the M2L kernels and the
+// near field, plus the handle-based C-ABI (include/bbfmm_b200.h).
+//
+// One solve (anotherFMMCompute.c:3-40 order):
+//   gather q -> P2M (maxlev) -> [U-projection, M2M] up to level 2      (upward)
+//   per level 2..maxlev: M2L -> post projection (assign) -> L2L from the parent level
+//   L2P (assign) -> P2P (add) -> scatter phi to the caller's particle order
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bbfmm_b200.h"
+#include "solver.cuh"
+
+template <typename T>
+int bbfmm_weights(int n, T *Tkz, int *Ktable, T *Kweights, T *Cweights);
+template <typename T>
+int bbfmm_sort_particles(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf_start);
+
+static thread_local std::string g_last_error;
+
+int bbfmm_set_error(int code, const char *msg) {
+  if (code != BBFMM_OK) g_last_error = msg ? msg : "error";
+  return code;
+}
+
+int bbfmm_set_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+  if (e == cudaSuccess) return BBFMM_OK;
+  char buf[512];
+  snprintf(buf, sizeof(buf), "CUDA error '%s' in %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+  g_last_error = buf;
+  return BBFMM_ERR_CUDA;
+}
+
+namespace bbfmm {
+
+template <typename T>
+static int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return BBFMM_OK;
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    char buf[160];
+    snprintf(buf, sizeof(buf), "device allocation of %zu bytes failed (%s)", sizeof(T) * count,
+             cudaGetErrorString(e));
+    return bbfmm_set_error(BBFMM_ERR_NOMEM, buf);
+  }
+  return BBFMM_OK;
+}
+
+#define TRY(x)                       \
+  do {                               \
+    int rc__ = (x);                  \
+    if (rc__ != BBFMM_OK) return rc__; \
+  } while (0)
+
+template <typename T>
+Tables Solver<T>::tables() const {
+  Tables t{};
+  if (sizeof(T) == 8) {
+    t.tkz_d = (const double *)tkz; t.cw_d = (const double *)cw; t.kw_d = (const double *)kw;
+  } else {
+    t.tkz_f = (const float *)tkz; t.cw_f = (const float *)cw; t.kw_f = (const float *)kw;
+  }
+  return t;
+}
+
+template <typename T>
+int Solver<T>::init(int n_, int maxlev_, double L_, int mode_, int lead_, int device_, cudaStream_t s) {
+  if (n_ != 4 && n_ != 8) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
+  if (maxlev_ < BBFMM_MINLEV || maxlev_ > 10) return bbfmm_set_error(BBFMM_ERR_ARG, "maxlev must be in [2, 10]");
+  if (!(L_ > 0)) return bbfmm_set_error(BBFMM_ERR_ARG, "root length L must be positive");
+  if (mode_ < MODE_D || mode_ > MODE_MIXED) return bbfmm_set_error(BBFMM_ERR_ARG, "unknown precision mode");
+  if ((mode_ == MODE_S) != (sizeof(T) == 4)) return bbfmm_set_error(BBFMM_ERR_ARG, "precision mode / type mismatch");
+  n = n_; n3 = n * n * n; r = n3 / 2; maxlev = maxlev_; L = L_; mode = mode_; device = device_;
+  lead = (mode == MODE_MIXED) ? lead_ : 0;
+  if (mode == MODE_MIXED && (lead < 0 || lead > r || lead % 16 != 0))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "lead must be a multiple of 16 in [0, r]");
+  BBFMM_CUDA_OK(cudaSetDevice(device));
+  if (s) {
+    stream = s;
+  } else {
+    BBFMM_CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  std::vector<int> ot(8 * 189 * 4);
+  build_offset_table(ot.data());
+  TRY(dalloc(&offs, 8 * 189));
+  BBFMM_CUDA_OK(cudaMemcpy(offs, ot.data(), sizeof(int) * ot.size(), cudaMemcpyHostToDevice));
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::set_tables(const T *Tkz_h, const T *Cw_h, const T *Kw_h) {
+  if (!tkz) {
+    TRY(dalloc(&tkz, n * n));
+    TRY(dalloc(&cw, 2 * n * n));
+    TRY(dalloc(&kw, n3));
+  }
+  BBFMM_CUDA_OK(cudaMemcpy(tkz, Tkz_h, sizeof(T) * n * n, cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaMemcpy(cw, Cw_h, sizeof(T) * 2 * n * n, cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaMemcpy(kw, Kw_h, sizeof(T) * n3, cudaMemcpyHostToDevice));
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::set_operators(const T *U, const T *E) {
+  if (!kw) return bbfmm_set_error(BBFMM_ERR_STATE, "tables must be set before operators");
+  std::vector<T> kwh(n3);
+  BBFMM_CUDA_OK(cudaMemcpy(kwh.data(), kw, sizeof(T) * n3, cudaMemcpyDeviceToHost));
+  std::vector<T> ert((size_t)BBFMM_NUM_OFFSETS * r * r), bup((size_t)n3 * r), bdn((size_t)r * n3);
+  for (int k = 0; k < BBFMM_NUM_OFFSETS; ++k)
+    for (int i = 0; i < r; ++i)
+      for (int j = 0; j < r; ++j)
+        ert[((size_t)k * r + i) * r + j] = E[((size_t)k * r + j) * r + i];
+  for (int l = 0; l < n3; ++l)
+    for (int i = 0; i < r; ++i) {
+      bup[(size_t)l * r + i] = kwh[l] * U[(size_t)i * n3 + l];
+      bdn[(size_t)i * n3 + l] = U[(size_t)i * n3 + l];
+    }
+  if (!Ert) {
+    TRY(dalloc(&Ert, ert.size()));
+    TRY(dalloc(&Bup, bup.size()));
+    TRY(dalloc(&Bdn, bdn.size()));
+  }
+  BBFMM_CUDA_OK(cudaMemcpy(Ert, ert.data(), sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaMemcpy(Bup, bup.data(), sizeof(T) * bup.size(), cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaMemcpy(Bdn, bdn.data(), sizeof(T) * bdn.size(), cudaMemcpyHostToDevice));
+  if (mode == MODE_MIXED) {
+    if (!tc_supported()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "mixed mode needs an sm_100 GPU");
+    if (tcops) tc_free_operators(tcops);
+    tcops = nullptr;
+    TRY(tc_prepare_operators(r, (const double *)Ert, lead, &tcops, stream));
+    BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
+  }
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::alloc_work() {
+  const int64_t nl = pow8i(maxlev);
+  int64_t smax[2] = {0, 0};
+  for (int l = BBFMM_MINLEV; l <= maxlev; ++l)
+    if (pow8i(l) > smax[l & 1]) smax[l & 1] = pow8i(l);
+  for (int b = 0; b < 2; ++b) {
+    if (S[b]) cudaFree(S[b]);
+    if (F[b]) cudaFree(F[b]);
+    TRY(dalloc(&S[b], (size_t)smax[b] * n3));
+    TRY(dalloc(&F[b], (size_t)smax[b] * n3));
+  }
+  Moff.assign(maxlev + 2, 0);
+  int64_t tot = 0;
+  for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
+    Moff[l] = tot;
+    tot += pow8i(l) * r;
+  }
+  if (Mall) cudaFree(Mall);
+  TRY(dalloc(&Mall, (size_t)tot));
+  if (Lbuf) cudaFree(Lbuf);
+  TRY(dalloc(&Lbuf, (size_t)nl * r));
+  if (mode == MODE_MIXED) {
+    if (L32) cudaFree(L32);
+    TRY(dalloc(&L32, (size_t)nl * r));
+    if (Msplit) cudaFree(Msplit);
+    unsigned char *p = nullptr;
+    TRY(dalloc(&p, tc_split_bytes(r, tot / r)));
+    Msplit = p;
+  }
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::set_particles_sorted(int N_, const int *perm_h, const int *leaf_start_h, const T *xyz_h) {
+  const int64_t nl = pow8i(maxlev);
+  if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(leafm); cudaFree(pos4); cudaFree(phis); }
+  if (loc4) cudaFree(loc4);
+  perm = leaf_start = leafm = nullptr; pos4 = phis = nullptr; loc4 = nullptr;
+  N = N_;
+  TRY(dalloc(&perm, N > 0 ? N : 1));
+  TRY(dalloc(&leaf_start, nl + 1));
+  TRY(dalloc(&leafm, N > 0 ? N : 1));
+  TRY(dalloc(&pos4, 4 * (size_t)(N > 0 ? N : 1)));
+  TRY(dalloc(&phis, N > 0 ? N : 1));
+  if (mode == MODE_MIXED) TRY(dalloc(&loc4, N > 0 ? N : 1));
+  if (N > 0) BBFMM_CUDA_OK(cudaMemcpy(perm, perm_h, sizeof(int) * N, cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaMemcpy(leaf_start, leaf_start_h, sizeof(int) * (nl + 1), cudaMemcpyHostToDevice));
+  TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream));
+  if (N > 0) {
+    T *xyz_d = nullptr;
+    TRY(dalloc(&xyz_d, 3 * (size_t)N));
+    BBFMM_CUDA_OK(cudaMemcpyAsync(xyz_d, xyz_h, sizeof(T) * 3 * N, cudaMemcpyHostToDevice, stream));
+    int rc = launch_gather<T, T>(N, perm, xyz_d, nullptr, pos4, stream);
+    cudaStreamSynchronize(stream);
+    cudaFree(xyz_d);
+    TRY(rc);
+  }
+  TRY(alloc_work());
+  BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
+  return BBFMM_OK;
+}
+
+template <typename T>
+void Solver<T>::mark(int stage) {
+  ++kernel_launches;
+  if (!timing) return;
+  if (stage < 0) {
+    cudaEventRecord(ev[ST_COUNT], stream);
+    return;
+  }
+  // attribute the time since the previous mark to this stage
+  static_assert(ST_COUNT + 1 <= (int)(sizeof(ev) / sizeof(ev[0])), "event table");
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, stream);
+  cudaEventSynchronize(e);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev[ST_COUNT], e);
+  stage_ms[stage] += ms;
+  cudaEventDestroy(ev[ST_COUNT]);
+  ev[ST_COUNT] = e;
+}
+
+template <typename T>
+int Solver<T>::upward(const void *q_dev, int q_is_double) {
+  const Tables tb = tables();
+  if (q_dev) {
+    if (q_is_double) TRY((launch_gather<T, double>(N, perm, nullptr, (const double *)q_dev, pos4, stream)));
+    else TRY((launch_gather<T, float>(N, perm, nullptr, (const float *)q_dev, pos4, stream)));
+    mark(ST_GATHER);
+  }
+  T *Sl = S[maxlev & 1];
+  TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream));
+  mark(ST_P2M);
+  TRY(launch_proj<T>(pow8i(maxlev), n3, r, Sl, nullptr, Bup, nullptr, (T)1, Mall + Moff[maxlev], maxlev,
+                     MAP_OUT_CPG, stream));
+  mark(ST_PROJ_UP);
+  for (int l = maxlev - 1; l >= BBFMM_MINLEV; --l) {
+    TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream));
+    mark(ST_M2M);
+    TRY(launch_proj<T>(pow8i(l), n3, r, S[l & 1], nullptr, Bup, nullptr, (T)1, Mall + Moff[l], l, MAP_OUT_CPG,
+                       stream));
+    mark(ST_PROJ_UP);
+  }
+  if (mode == MODE_MIXED) {
+    const int64_t tot = (Moff[maxlev] + pow8i(maxlev) * r) / r;
+    TRY(tc_split_multipoles(r, tot, (const double *)Mall, lead, Msplit, stream));
+    mark(ST_PROJ_UP);
+  }
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::interaction(int lo, int hi) {
+  const Tables tb = tables();
+  for (int l = lo; l <= hi; ++l) {
+    const T *Ml = Mall + Moff[l];
+    if (mode == MODE_MIXED) {
+      // leading components in FP64 on CUDA cores, the rest as split bf16 on tensor cores
+      if (lead > 0) TRY(launch_m2l_simt<T>(r, Ml, Ert, Lbuf, l, 0, lead, offs, 0, stream));
+      else BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * pow8i(l) * r, stream));
+      TRY(launch_m2l_tc(r, (const unsigned char *)Msplit + tc_split_bytes(r, Moff[l] / r), tcops, L32, l, offs,
+                        lead, stream));
+    } else {
+      TRY(launch_m2l_simt<T>(r, Ml, Ert, Lbuf, l, 0, r, offs, 0, stream));
+    }
+    mark(ST_M2L);
+    const T scale = (T)1 / cell_length<T>(l, (T)L);
+    TRY(launch_proj<T>(pow8i(l), r, n3, Lbuf, mode == MODE_MIXED ? L32 : nullptr, Bdn, kw, scale, F[l & 1], l,
+                       MAP_IN_CPG, stream));
+    mark(ST_PROJ_DOWN);
+    if (l > BBFMM_MINLEV) {
+      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream));
+      mark(ST_L2L);
+    }
+  }
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::downward_finish(void *phi_dev, int phi_is_double, bool near) {
+  const Tables tb = tables();
+  TRY(launch_l2p<T>(n, pos4, leaf_start, maxlev, (T)L, tb, F[maxlev & 1], phis, stream));
+  mark(ST_L2P);
+  if (near) {
+    if (mode == MODE_MIXED) {
+      TRY(launch_make_local(N, (const double *)pos4, leafm, maxlev, L, loc4, stream));
+      TRY(launch_p2p_local(N, loc4, leaf_start, leafm, maxlev, L, (double *)phis, stream));
+    } else {
+      TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, phis, stream));
+    }
+    mark(ST_P2P);
+  }
+  if (phi_dev) {
+    if (phi_is_double) TRY((launch_scatter<T, double>(N, perm, phis, (double *)phi_dev, stream)));
+    else TRY((launch_scatter<T, float>(N, perm, phis, (float *)phi_dev, stream)));
+    mark(ST_SCATTER);
+  }
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::solve(const void *q_dev, void *phi_dev, int io_double) {
+  if (!pos4) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
+  if (!Ert) return bbfmm_set_error(BBFMM_ERR_STATE, "operators not set");
+  kernel_launches = 0;
+  if (timing) {
+    for (int i = 0; i < ST_COUNT; ++i) stage_ms[i] = 0.f;
+    if (!ev[ST_COUNT]) cudaEventCreate(&ev[ST_COUNT]);
+    mark(-1);
+    --kernel_launches;
+  }
+  TRY(upward(q_dev, io_double));
+  TRY(interaction(BBFMM_MINLEV, maxlev));
+  TRY(downward_finish(phi_dev, io_double, true));
+  return BBFMM_OK;
+}
+
+template <typename T>
+int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
+  if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "level out of range");
+  T *tmp = nullptr;
+  TRY(dalloc(&tmp, (size_t)pow8i(level) * r));
+  int rc = launch_morton_cpg<T>(level, r, Mall + Moff[level], tmp, 1, stream);
+  if (rc == BBFMM_OK) {
+    cudaError_t e = cudaMemcpyAsync(host_out, tmp, sizeof(T) * pow8i(level) * r, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    rc = bbfmm_set_cuda_error(e, "copy multipoles", __FILE__, __LINE__);
+  }
+  cudaFree(tmp);
+  return rc;
+}
+
+template <typename T>
+void Solver<T>::release() {
+  void *ptrs[] = {tkz, cw, kw, Ert, Bup, Bdn, kwcol, offs, perm, leaf_start, leafm, pos4, loc4,
+                  S[0], S[1], F[0], F[1], Mall, Lbuf, L32, Msplit, phis};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (tcops) tc_free_operators(tcops);
+  if (ev[ST_COUNT]) cudaEventDestroy(ev[ST_COUNT]);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+  *this = Solver<T>();
+}
+
+template struct Solver<double>;
+template struct Solver<float>;
+
+}  // namespace bbfmm
+
+// ============================================================== handle C-ABI
+using bbfmm::Solver;
+
+struct bbfmm_b200_solver {
+  int mode;
+  Solver<double> *d;
+  Solver<float> *f;
+};
+
+extern "C" {
+
+const char *bbfmm_b200_last_error(void) { return g_last_error.c_str(); }
+
+int bbfmm_b200_version(void) { return BBFMM_B200_VERSION; }
+
+int bbfmm_b200_create(const bbfmm_b200_config *cfg, const void *U, const void *E, int operators_fp32,
+                      bbfmm_b200_solver **out) {
+  if (!cfg || !U || !E || !out) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  *out = nullptr;
+  const int n = cfg->n, n3 = n * n * n, r = n3 / 2;
+  bbfmm_b200_solver *h = new bbfmm_b200_solver();
+  h->mode = cfg->mode;
+  int rc = BBFMM_OK;
+  if (cfg->mode == BBFMM_B200_MODE_S) {
+    h->f = new Solver<float>();
+    rc = h->f->init(n, cfg->maxlev, cfg->L, cfg->mode, cfg->lead, cfg->device, (cudaStream_t)cfg->stream);
+    if (rc == BBFMM_OK) {
+      std::vector<float> tkz(n * n), kw(n3), cw(2 * n * n);
+      std::vector<int> kt(343);
+      rc = bbfmm_weights<float>(n, tkz.data(), kt.data(), kw.data(), cw.data());
+      if (rc == BBFMM_OK) rc = h->f->set_tables(tkz.data(), cw.data(), kw.data());
+      std::vector<float> Uf((size_t)n3 * r), Ef((size_t)316 * r * r);
+      for (size_t i = 0; i < Uf.size(); ++i) Uf[i] = operators_fp32 ? ((const float *)U)[i] : (float)((const double *)U)[i];
+      for (size_t i = 0; i < Ef.size(); ++i) Ef[i] = operators_fp32 ? ((const float *)E)[i] : (float)((const double *)E)[i];
+      if (rc == BBFMM_OK) rc = h->f->set_operators(Uf.data(), Ef.data());
+    }
+  } else {
+    h->d = new Solver<double>();
+    rc = h->d->init(n, cfg->maxlev, cfg->L, cfg->mode, cfg->lead, cfg->device, (cudaStream_t)cfg->stream);
+    if (rc == BBFMM_OK) {
+      std::vector<double> tkz(n * n), kw(n3), cw(2 * n * n);
+      std::vector<int> kt(343);
+      rc = bbfmm_weights<double>(n, tkz.data(), kt.data(), kw.data(), cw.data());
+      if (rc == BBFMM_OK) rc = h->d->set_tables(tkz.data(), cw.data(), kw.data());
+      std::vector<double> Ud((size_t)n3 * r), Ed((size_t)316 * r * r);
+      for (size_t i = 0; i < Ud.size(); ++i) Ud[i] = operators_fp32 ? ((const float *)U)[i] : ((const double *)U)[i];
+      for (size_t i = 0; i < Ed.size(); ++i) Ed[i] = operators_fp32 ? ((const float *)E)[i] : ((const double *)E)[i];
+      if (rc == BBFMM_OK) rc = h->d->set_operators(Ud.data(), Ed.data());
+    }
+  }
+  if (rc != BBFMM_OK) {
+    bbfmm_b200_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return BBFMM_OK;
+}
+
+int bbfmm_b200_set_particles(bbfmm_b200_solver *h, int N, const void *xyz) {
+  if (!h || (N > 0 && !xyz) || N < 0) return bbfmm_set_error(BBFMM_ERR_ARG, "bad particle arguments");
+  if (h->f) {
+    Solver<float> &s = *h->f;
+    std::vector<int> perm(N > 0 ? N : 1), ls(::pow8i(s.maxlev) + 1);
+    int rc = bbfmm_sort_particles<float>(N, (const float *)xyz, (float)s.L, s.maxlev, perm.data(), ls.data());
+    if (rc != BBFMM_OK) return rc;
+    return s.set_particles_sorted(N, perm.data(), ls.data(), (const float *)xyz);
+  }
+  Solver<double> &s = *h->d;
+  std::vector<int> perm(N > 0 ? N : 1), ls(::pow8i(s.maxlev) + 1);
+  int rc = bbfmm_sort_particles<double>(N, (const double *)xyz, s.L, s.maxlev, perm.data(), ls.data());
+  if (rc != BBFMM_OK) return rc;
+  return s.set_particles_sorted(N, perm.data(), ls.data(), (const double *)xyz);
+}
+
+int bbfmm_b200_solve(bbfmm_b200_solver *h, const void *q_dev, void *phi_dev) {
+  if (!h || !q_dev || !phi_dev) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  if (h->f) return h->f->solve(q_dev, phi_dev, 0);
+  return h->d->solve(q_dev, phi_dev, 1);
+}
+
+int bbfmm_b200_solve_host(bbfmm_b200_solver *h, const void *q_host, void *phi_host) {
+  if (!h || !q_host || !phi_host) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  const int N = h->f ? h->f->N : h->d->N;
+  const size_t es = h->f ? sizeof(float) : sizeof(double);
+  cudaStream_t st = h->f ? h->f->stream : h->d->stream;
+  if (N == 0) return BBFMM_OK;
+  void *qd = nullptr, *pd = nullptr;
+  if (cudaMalloc(&qd, es * N) != cudaSuccess || cudaMalloc(&pd, es * N) != cudaSuccess) {
+    if (qd) cudaFree(qd);
+    return bbfmm_set_error(BBFMM_ERR_NOMEM, "device allocation for host solve failed");
+  }
+  int rc = bbfmm_set_cuda_error(cudaMemcpyAsync(qd, q_host, es * N, cudaMemcpyHostToDevice, st), "h2d q", __FILE__,
+                                __LINE__);
+  if (rc == BBFMM_OK) rc = bbfmm_b200_solve(h, qd, pd);
+  if (rc == BBFMM_OK)
+    rc = bbfmm_set_cuda_error(cudaMemcpyAsync(phi_host, pd, es * N, cudaMemcpyDeviceToHost, st), "d2h phi",
+                              __FILE__, __LINE__);
+  if (rc == BBFMM_OK) rc = bbfmm_set_cuda_error(cudaStreamSynchronize(st), "sync", __FILE__, __LINE__);
+  cudaFree(qd);
+  cudaFree(pd);
+  return rc;
+}
+
+int bbfmm_b200_set_timing(bbfmm_b200_solver *h, int on) {
+  if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
+  if (h->f) h->f->timing = on != 0;
+  else h->d->timing = on != 0;
+  return BBFMM_OK;
+}
+
+int bbfmm_b200_stage_times(const bbfmm_b200_solver *h, float *ms, int count) {
+  if (!h || !ms) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  const float *src = h->f ? h->f->stage_ms : h->d->stage_ms;
+  for (int i = 0; i < count && i < bbfmm::ST_COUNT; ++i) ms[i] = src[i];
+  return h->f ? h->f->kernel_launches : h->d->kernel_launches;
+}
+
+int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *h, int level, void *host_out) {
+  if (!h || !host_out) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  if (h->f) return h->f->copy_multipoles_morton(level, (float *)host_out);
+  return h->d->copy_multipoles_morton(level, (double *)host_out);
+}
+
+void *bbfmm_b200_stream(bbfmm_b200_solver *h) {
+  if (!h) return nullptr;
+  return h->f ? (void *)h->f->stream : (void *)h->d->stream;
+}
+
+void bbfmm_b200_destroy(bbfmm_b200_solver *h) {
+  if (!h) return;
+  if (h->f) { h->f->release(); delete h->f; }
+  if (h->d) { h->d->release(); delete h->d; }
+  delete h;
+}
+
+int bbfmm_b200_weights(int n, int fp32, void *Tkz, int *Ktable, void *Kweights, void *Cweights) {
+  if (fp32) return bbfmm_weights<float>(n, (float *)Tkz, Ktable, (float *)Kweights, (float *)Cweights);
+  return bbfmm_weights<double>(n, (double *)Tkz, Ktable, (double *)Kweights, (double *)Cweights);
+}
+
+int bbfmm_b200_sort_particles(int N, int fp32, const void *xyz, double L, int maxlev, int *perm, int *leaf_start) {
+  if (fp32) return bbfmm_sort_particles<float>(N, (const float *)xyz, (float)L, maxlev, perm, leaf_start);
+  return bbfmm_sort_particles<double>(N, (const double *)xyz, L, maxlev, perm, leaf_start);
+}
+
+}  // extern "C"

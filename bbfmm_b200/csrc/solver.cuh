@@ -1,0 +1,99 @@
+// Device-resident FMM solver (internal C++ interface shared by the handle C-ABI and by
+// the reference-compatible drop-in entry points).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+struct __nv_bfloat16;
+
+namespace bbfmm {
+
+enum Mode { MODE_D = 0, MODE_S = 1, MODE_MIXED = 2 };
+
+enum Stage {
+  ST_GATHER = 0, ST_P2M, ST_M2M, ST_PROJ_UP, ST_M2L, ST_PROJ_DOWN, ST_L2L, ST_L2P, ST_P2P, ST_SCATTER,
+  ST_COUNT
+};
+
+// Launchers (passes.cu, p2p.cu, m2l_simt.cu, m2l_tc.cu)
+template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s);
+template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s);
+template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s);
+template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s);
+template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s);
+template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
+template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
+template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
+template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s);
+int launch_p2p_local(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L, double *phi, cudaStream_t s);
+int launch_make_local(int N, const double *pos4, const int *leafm, int maxlev, double L, float4 *loc4, cudaStream_t s);
+int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s);
+template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s);
+void build_offset_table(int *out);
+
+template <typename T> int bbfmm_weights_t(int n, T *Tkz, int *Ktable, T *Kweights, T *Cweights);
+
+// Mixed-precision tensor-core M2L (m2l_tc.cu).
+struct TcOperators;
+int tc_supported();
+int tc_prepare_operators(int r, const double *Ert, int lead, void **out, cudaStream_t s);
+void tc_free_operators(void *ops);
+int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s);
+size_t tc_split_bytes(int r, int64_t ncell);
+int launch_m2l_tc(int r, const void *Msplit, const void *ops, float *L32, int level, const int4 *offs, int lead,
+                  cudaStream_t s);
+
+template <typename T>
+struct Solver {
+  int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, device = 0;
+  double L = 1.0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // tables and operators (device)
+  T *tkz = nullptr, *cw = nullptr, *kw = nullptr;
+  T *Ert = nullptr;  // [316][r][r] row-major
+  T *Bup = nullptr;  // [n3][r]  Kweights[l] U(l, i)
+  T *Bdn = nullptr;  // [r][n3]  U(l, j)
+  T *kwcol = nullptr;
+  int4 *offs = nullptr;
+  void *tcops = nullptr;  // mixed mode: split operators for the tensor-core kernel
+  // particles (sorted by leaf, Morton leaf order)
+  int N = 0;
+  int *perm = nullptr, *leaf_start = nullptr, *leafm = nullptr;
+  T *pos4 = nullptr;
+  float4 *loc4 = nullptr;
+  // expansions
+  T *S[2] = {nullptr, nullptr};
+  T *F[2] = {nullptr, nullptr};
+  T *Mall = nullptr;
+  std::vector<int64_t> Moff;  // offset (elements) of level l in Mall, cpg layout
+  T *Lbuf = nullptr;
+  float *L32 = nullptr;
+  void *Msplit = nullptr;
+  T *phis = nullptr;
+  // timing
+  bool timing = false;
+  cudaEvent_t ev[ST_COUNT + 1] = {};
+  float stage_ms[ST_COUNT] = {};
+  int kernel_launches = 0;
+
+  Tables tables() const;
+  int init(int n_, int maxlev_, double L_, int mode_, int lead_, int device_, cudaStream_t s);
+  int set_tables(const T *Tkz, const T *Cweights, const T *Kweights);  // host arrays
+  int set_operators(const T *U, const T *E);                              // host, reference layout
+  int set_particles_sorted(int N_, const int *perm_host, const int *leaf_start_host, const T *xyz_host);
+  int alloc_work();
+  int upward(const void *q_dev, int q_is_double);   // gather q, P2M, M2M, projections -> Mall
+  int interaction(int level_lo, int level_hi);       // M2L + post projection + L2L into F
+  int downward_finish(void *phi_dev, int phi_is_double, bool near);  // L2P, P2P, scatter
+  int solve(const void *q_dev, void *phi_dev, int io_double);
+  int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order
+  void mark(int stage);
+  void release();
+};
+
+}  // namespace bbfmm

@@ -1,0 +1,141 @@
+"""Host-side Python interface of the B200 bbFMM solver.
+
+Mirrors the reference's user-facing call ``bbfmm(field, source, q, Nf, Ns, L, n, phi, l)``
+(bbfmm.h:97, bbfmm.c:15-87) with field = source, and exposes a handle (``Solver``) that
+keeps the tree, the operators and every expansion on the GPU between solves.
+
+Conventions follow the reference: the root cell is [-L/2, L/2]^3, the output is
+q_i * phi_i (bbfmm.c:501), the rank is r = n^3/2 and the depth formula of FMMSetup
+(bbfmm.c:151-160) is available as ``reference_depth``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from . import operators as ops
+
+
+def reference_depth(N: int, level_modifier: int = 0) -> int:
+    """maxlev as the reference's FMMSetup computes it: the integer cast binds to log(N)
+    only, then one level is subtracted, with a floor of MINLEV = 2 (bbfmm.c:151-160)."""
+    l = level_modifier + int(math.log(N)) / math.log(8.0) if N > 0 else float(level_modifier)
+    l = int(l)
+    if l > 0:
+        l -= 1
+    return max(l, 2)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else C.c_void_p(a.data_ptr())
+
+
+class Solver:
+    """Device-resident FMM for one particle set.
+
+    mode: "d" (FP64 everywhere), "s" (FP32 everywhere), "mixed" (FP64 passes,
+    split-precision tensor-core M2L with ``lead`` FP64 leading components, FP32
+    compensated P2P)."""
+
+    def __init__(self, n: int, maxlev: int, L: float = 1.0, mode: str = "d", lead: int = 16,
+                 device: int = 0, operators=None, stream=None):
+        import torch
+        self.torch = torch
+        self.n, self.maxlev, self.L, self.mode = n, maxlev, float(L), mode
+        self.r = n ** 3 // 2
+        self.lead = lead if mode == "mixed" else 0
+        self.device = device
+        self.dtype = torch.float32 if mode == "s" else torch.float64
+        self.np_dtype = np.float32 if mode == "s" else np.float64
+        if operators is None:
+            _, U, E = ops.load_operators(n, single=(mode == "s"))
+        else:
+            U, E = operators
+        U = np.ascontiguousarray(U)
+        E = np.ascontiguousarray(E)
+        fp32 = int(U.dtype == np.float32)
+        assert E.dtype == U.dtype
+        cfg = _lib.Config(n=n, maxlev=maxlev, L=self.L, mode=_lib.MODES[mode], lead=self.lead,
+                          device=device, stream=C.c_void_p(stream) if stream else None)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().bbfmm_b200_create(C.byref(cfg), _ptr(U), _ptr(E), fp32, C.byref(h)))
+        self.h = h
+        self.N = 0
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            _lib.lib().bbfmm_b200_destroy(h)
+            self.h = None
+
+    def close(self):
+        self.__del__()
+
+    @property
+    def stream(self):
+        return _lib.lib().bbfmm_b200_stream(self.h)
+
+    def set_particles(self, xyz):
+        """Particle positions, N x 3 inside [-L/2, L/2]^3 (host array)."""
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=self.np_dtype).reshape(-1, 3))
+        self.N = xyz.shape[0]
+        _lib.check(_lib.lib().bbfmm_b200_set_particles(self.h, self.N, _ptr(xyz)))
+
+    def solve(self, q, out=None):
+        """q: CUDA tensor (N,) -> q_i * phi_i as a CUDA tensor, on the solver's stream."""
+        torch = self.torch
+        q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        if out is None:
+            out = torch.empty_like(q)
+        # order the solver's stream after the caller's work on q, and the caller's stream
+        # after the solve; keep both buffers alive for the solver's stream
+        caller = torch.cuda.current_stream(q.device)
+        mine = torch.cuda.ExternalStream(self.stream, device=q.device)
+        ready = torch.cuda.Event()
+        ready.record(caller)
+        mine.wait_event(ready)
+        _lib.check(_lib.lib().bbfmm_b200_solve(self.h, C.c_void_p(q.data_ptr()), C.c_void_p(out.data_ptr())))
+        done = torch.cuda.Event()
+        done.record(mine)
+        caller.wait_event(done)
+        q.record_stream(mine)
+        out.record_stream(mine)
+        return out
+
+    def solve_host(self, q):
+        q = np.ascontiguousarray(np.asarray(q, dtype=self.np_dtype))
+        phi = np.empty_like(q)
+        _lib.check(_lib.lib().bbfmm_b200_solve_host(self.h, _ptr(q), _ptr(phi)))
+        return phi
+
+    def set_timing(self, on: bool):
+        _lib.check(_lib.lib().bbfmm_b200_set_timing(self.h, int(on)))
+
+    def stage_times(self):
+        ms = (C.c_float * len(_lib.STAGES))()
+        nl = _lib.lib().bbfmm_b200_stage_times(self.h, ms, len(_lib.STAGES))
+        return dict(zip(_lib.STAGES, list(ms))), nl
+
+    def multipoles(self, level: int):
+        out = np.empty(8 ** level * self.r, dtype=self.np_dtype)
+        _lib.check(_lib.lib().bbfmm_b200_copy_multipoles(self.h, level, _ptr(out)))
+        return out
+
+
+def bbfmm(xyz, q, L: float = 1.0, n: int = 4, level_modifier: int = 0, mode: str = "d", maxlev=None,
+          operators=None):
+    """One solve from host arrays, like the reference's ``bbfmm()`` with field = source.
+
+    Returns q_i * phi_i in the input order."""
+    xyz = np.asarray(xyz)
+    N = xyz.shape[0]
+    lev = maxlev if maxlev is not None else reference_depth(N, level_modifier)
+    s = Solver(n, lev, L, mode=mode, operators=operators)
+    try:
+        s.set_particles(xyz)
+        return s.solve_host(q)
+    finally:
+        s.close()

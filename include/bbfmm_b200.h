@@ -1,0 +1,133 @@
+/*
+ * bbfmm_b200 -- B200 (sm_100a) implementation of the bbFMM hot path: the SVD-compressed
+ * Chebyshev M2L, the near-field P2P and the P2M/M2M/L2L/L2P passes, with expansions
+ * resident in device memory.
+ *
+ * Two C-ABI surfaces are exported:
+ *
+ *  1. The reference's own entry points (m2l_drv, m2l_host_*, anotherFMMCompute,
+ *     anotherUpwardPass, anotherFMMInteraction, anotherDownwardPass, anotherNearField,
+ *     kernel_exec_time), declared in bbfmm_b200_reference.h with the reference's
+ *     signatures so that its host objects link against this library unchanged.
+ *
+ *  2. The handle API below: tree, operators and expansions stay on the device and one
+ *     call runs one whole solve. This surface has no counterpart in the reference, whose
+ *     GPU path copies every array to and from the host around each kernel.
+ *
+ * Conventions shared with the reference: the root cell is the cube [-L/2, L/2]^3 centred
+ * at the origin (anotherFMMDistribute.c:321-324); the result is q_i * phi_i, the target
+ * charge times the potential (bbfmm.c:501, anotherDownwardPassX.c:330); leaves sit at
+ * level maxlev of a full uniform octree; the rank of the compressed operators is the
+ * reference's fixed cutoff r = n^3 / 2 (bbfmm.c:1340-1343); operator arrays use the
+ * layouts of the reference's [s]laplacian{K,U}{n}.bin files: U is n^3 x r column-major,
+ * E ("K") holds 316 r x r column-major blocks (bbfmm.c:1361-1405).
+ *
+ * Every function returns 0 on success or a positive BBFMM_B200_ERR_* code; the message of
+ * the last failure on the calling thread is available from bbfmm_b200_last_error().
+ */
+#ifndef BBFMM_B200_H
+#define BBFMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BBFMM_B200_API __attribute__((visibility("default")))
+#else
+#define BBFMM_B200_API
+#endif
+
+#define BBFMM_B200_VERSION 1
+
+#define BBFMM_B200_OK 0
+#define BBFMM_B200_ERR_ARG 1
+#define BBFMM_B200_ERR_CUDA 2
+#define BBFMM_B200_ERR_NOMEM 3
+#define BBFMM_B200_ERR_UNSUPPORTED 4
+#define BBFMM_B200_ERR_STATE 5
+
+/* Precision modes.
+ *  D      FP64 storage and arithmetic in every stage (the reference's double build).
+ *  S      FP32 storage and arithmetic in every stage (the reference's SINGLE build).
+ *  MIXED  FP64 passes; M2L with the first `lead` contraction components in FP64 and the
+ *         rest as three-term split BF16 products on tcgen05 tensor cores accumulated in
+ *         FP32; P2P in FP32 on leaf-local coordinates with compensated sums. */
+#define BBFMM_B200_MODE_D 0
+#define BBFMM_B200_MODE_S 1
+#define BBFMM_B200_MODE_MIXED 2
+
+typedef struct {
+  int n;        /* Chebyshev nodes per dimension: 4 (r = 32) or 8 (r = 256) */
+  int maxlev;   /* level of the leaves, >= 2 (the reference's maxlev) */
+  double L;     /* edge of the root cube */
+  int mode;     /* BBFMM_B200_MODE_* */
+  int lead;     /* MIXED: leading contraction components kept in FP64 (multiple of 16) */
+  int device;   /* CUDA device ordinal */
+  void *stream; /* cudaStream_t to run on, or NULL for a private stream */
+} bbfmm_b200_config;
+
+typedef struct bbfmm_b200_solver bbfmm_b200_solver;
+
+/* Stage indices of bbfmm_b200_stage_times(). */
+enum {
+  BBFMM_B200_STAGE_GATHER = 0,
+  BBFMM_B200_STAGE_P2M,
+  BBFMM_B200_STAGE_M2M,
+  BBFMM_B200_STAGE_PROJ_UP,
+  BBFMM_B200_STAGE_M2L,
+  BBFMM_B200_STAGE_PROJ_DOWN,
+  BBFMM_B200_STAGE_L2L,
+  BBFMM_B200_STAGE_L2P,
+  BBFMM_B200_STAGE_P2P,
+  BBFMM_B200_STAGE_SCATTER,
+  BBFMM_B200_NUM_STAGES
+};
+
+BBFMM_B200_API const char *bbfmm_b200_last_error(void);
+BBFMM_B200_API int bbfmm_b200_version(void);
+
+/* Chebyshev tables of ComputeWeights (bbfmm.c:922-1028) in FP64 (fp32 = 0) or FP32:
+ * Tkz[n*n], Ktable[343], Kweights[n^3], Cweights[2*n*n]. */
+BBFMM_B200_API int bbfmm_b200_weights(int n, int fp32, void *Tkz, int *Ktable, void *Kweights, void *Cweights);
+
+/* Leaf assignment and stable counting sort (anotherFMMDistribute.c:258-473):
+ * perm[k] = index of the k-th particle in leaf-sorted order, leaf_start[8^maxlev + 1] =
+ * CSR offsets of the leaves in Morton (reference) order. xyz is N x 3, FP64 or FP32. */
+BBFMM_B200_API int bbfmm_b200_sort_particles(int N, int fp32, const void *xyz, double L, int maxlev, int *perm,
+                              int *leaf_start);
+
+/* Create a solver: uploads tables and operators (U, E in the reference file layouts,
+ * FP64 unless operators_fp32). */
+BBFMM_B200_API int bbfmm_b200_create(const bbfmm_b200_config *cfg, const void *U, const void *E, int operators_fp32,
+                      bbfmm_b200_solver **out);
+
+/* Positions (host, N x 3; FP32 in mode S, FP64 otherwise), inside [-L/2, L/2]^3. Builds
+ * the leaf order on the host and keeps the sorted particles on the device. */
+BBFMM_B200_API int bbfmm_b200_set_particles(bbfmm_b200_solver *s, int N, const void *xyz);
+
+/* One solve with device-resident charges and result (original particle order; FP32 in
+ * mode S, FP64 otherwise): phi[i] = q_i * sum_{j != i} q_j / |x_i - x_j| (FMM-approximated).
+ * Runs on the solver's stream and returns without synchronising. */
+BBFMM_B200_API int bbfmm_b200_solve(bbfmm_b200_solver *s, const void *q_dev, void *phi_dev);
+
+/* The same with host buffers: copies q in, solves, copies phi out and synchronises. */
+BBFMM_B200_API int bbfmm_b200_solve_host(bbfmm_b200_solver *s, const void *q_host, void *phi_host);
+
+/* Per-stage device times (ms) of the last solve run with timing on; returns the number of
+ * kernel launches of that solve. Timing inserts a synchronisation after every stage. */
+BBFMM_B200_API int bbfmm_b200_set_timing(bbfmm_b200_solver *s, int on);
+BBFMM_B200_API int bbfmm_b200_stage_times(const bbfmm_b200_solver *s, float *ms, int count);
+
+/* The multipole (proxy source) coefficients of one level after a solve, r per cell in
+ * the reference's Morton cell order (the level's slice of proxysval). */
+BBFMM_B200_API int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *s, int level, void *host_out);
+
+BBFMM_B200_API void *bbfmm_b200_stream(bbfmm_b200_solver *s);
+BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBFMM_B200_H */

@@ -1,0 +1,49 @@
+#!/bin/bash
+# Builds the REFERENCE implementation's CPU code, from its own sources where they lie,
+# into oracle/_ref/ as shared libraries driven by oracle/ref_harness.c. Test
+# infrastructure only (pins the CPU oracle; CPU baseline of the benchmark).
+#
+#   libref_cpu8a_{d,s}.so  default CPU path: sibling-blocking M2L (CPU8A)
+#   libref_cpu9a_{d,s}.so  ij-blocking CPU M2L (CPU9A, the aux_CPU9* family)
+#
+# Flags follow the reference's own recipes (www.sh:23-36, zzz.sh:209-212) with gcc,
+# -fcommon (bbfmm.h defines globals in a header) and gettimeofday timers. BLAS/LAPACK
+# (?gesvd, ?gemm, ?dot) come from the OpenBLAS that ships inside the opencv wheel of
+# this image. Usage: oracle/build_ref.sh [reference-dir]
+set -euo pipefail
+REF=${1:-${BBFMM_REFERENCE_DIR:-/root/reference}}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+[ -f "$REF/bbfmm.c" ] || { echo "reference sources not found in $REF" >&2; exit 2; }
+PY=${PYTHON:-python}
+SITE=$($PY -c 'import sysconfig; print(sysconfig.get_paths()["purelib"])')
+BL="$SITE/opencv_python_headless.libs"
+BLAS=$(cd "$BL" && ls libopenblas*.so 2>/dev/null | head -1)
+[ -n "$BLAS" ] || { echo "no OpenBLAS found under $BL" >&2; exit 3; }
+mkdir -p "$OUT"
+SRCS="bbfmm.c options.c checks.c opts.c envs.c output.c timer.c elapsed.c anotherFMMCompute.c
+      anotherFMMInteraction.c anotherDownwardPassX.c anotherDownwardPass.c anotherUpwardPass.c
+      anotherFMMDistribute.c anotherInteractionList.c anotherNearField.c m2l_aux.c
+      auxAnotherFMMInteraction.c anotherBuildFMMHierachy.c xdot.c atransx.c m2l_aux_cpu.c"
+build() {  # $1 = output name, rest = extra defines
+  local name=$1; shift
+  local objdir="$OUT/obj_$name"
+  mkdir -p "$objdir"
+  local objs=""
+  for s in $SRCS; do
+    gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE \
+        -DENABLE_GETTIMEOFDAY "$@" -I"$REF" -c "$REF/$s" -o "$objdir/${s%.c}.o" &
+    objs="$objs $objdir/${s%.c}.o"
+  done
+  gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE "$@" -I"$REF" \
+      -c "$HERE/ref_harness.c" -o "$objdir/ref_harness.o" &
+  wait
+  gcc -shared -fopenmp -o "$OUT/$name.so" $objs "$objdir/ref_harness.o" \
+      -L"$BL" -l:"$BLAS" -Wl,--disable-new-dtags,-rpath,"$BL" -lm
+  rm -rf "$objdir"
+}
+build libref_cpu8a_d -DCPU8 -DCPU8A
+build libref_cpu8a_s -DCPU8 -DCPU8A -DSINGLE
+build libref_cpu9a_d -DCPU9 -DCPU9A
+build libref_cpu9a_s -DCPU9 -DCPU9A -DSINGLE
+echo "built reference CPU libraries in $OUT"

@@ -1,0 +1,109 @@
+"""CUDA path vs the CPU oracle on identical seeded inputs and operators (-m gpu).
+
+Tolerances (relative L2 over all particles):
+  mode d (FP64): 1e-12 against the FP64 oracle (summation order only).
+  mode s (FP32): 2e-5 against the FP32 oracle (FP32 order/FMA differences; the FP32
+                 oracle itself differs from the reference SINGLE build by ~2e-7).
+"""
+import numpy as np
+import pytest
+
+from conftest import uniform_inputs
+from oracle.oracle import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(mode, n, maxlev, x, q, U, E):
+    import torch
+    from bbfmm_b200 import Solver
+    s = Solver(n, maxlev, 1.0, mode=mode, operators=(U, E))
+    s.set_particles(x)
+    dt = torch.float32 if mode == "s" else torch.float64
+    phi = s.solve(torch.as_tensor(q, dtype=dt, device="cuda"))
+    torch.cuda.synchronize()
+    out = phi.cpu().numpy()
+    return s, out
+
+
+@pytest.mark.parametrize("n,maxlev,N", [(4, 2, 4096), (4, 3, 32768), (4, 4, 32768), (8, 3, 32768)])
+def test_fp64_matches_oracle(oracle_d, n, maxlev, N):
+    from bbfmm_b200 import operators as ops
+    _, U, E = ops.load_operators(n, single=False)
+    x, q = uniform_inputs(N, seed=n * 10 + maxlev)
+    ref = oracle_d.fmm(x, q, n, maxlev, U, E)
+    s, got = _solve("d", n, maxlev, x, q, U, E)
+    assert rel_l2(got, ref) < 1e-12
+    # multipoles of every level in the reference's cell order
+    tree = oracle_d.build_tree(x, maxlev)
+    _, P = oracle_d.upward(tree, x, q, n, U)
+    r = n ** 3 // 2
+    for lev in range(2, maxlev + 1):
+        lo = (8 ** lev - 1) // 7
+        want = P[lo * r:(lo + 8 ** lev) * r]
+        assert rel_l2(s.multipoles(lev), want) < 1e-13
+    s.close()
+
+
+@pytest.mark.parametrize("n,maxlev,N", [(4, 3, 32768), (8, 3, 32768)])
+def test_fp32_matches_oracle(oracle_s, n, maxlev, N):
+    from bbfmm_b200 import operators as ops
+    _, U, E = ops.load_operators(n, single=True)
+    x, q = uniform_inputs(N, seed=7, dtype="float32")
+    ref = oracle_s.fmm(x, q, n, maxlev, U, E)
+    s, got = _solve("s", n, maxlev, x, q, U, E)
+    assert rel_l2(got, ref) < 2e-5
+    s.close()
+
+
+def test_fp64_against_direct(oracle_d):
+    """Absolute accuracy: FP64 FMM vs the FP64 direct sum on sampled targets matches the
+    oracle FMM's own error (n=8 truncation error ~1e-7)."""
+    from bbfmm_b200 import operators as ops
+    _, U, E = ops.load_operators(8, single=False)
+    x, q = uniform_inputs(32768, seed=3)
+    targets = np.random.default_rng(0).choice(32768, 1024, replace=False).astype(np.int32)
+    dref = oracle_d.direct_fp64(x, q, targets)
+    s, got = _solve("d", 8, 3, x, q, U, E)
+    err = rel_l2(got[targets], dref)
+    assert err < 5e-7
+    s.close()
+
+
+@pytest.mark.parametrize("case", ["one_leaf", "boundary", "sparse", "single"])
+def test_edge_cases_fp64(oracle_d, case):
+    from bbfmm_b200 import operators as ops
+    _, U, E = ops.load_operators(4, single=False)
+    rng = np.random.default_rng(5)
+    if case == "one_leaf":          # every particle in one leaf, all others empty
+        x = rng.random((500, 3)) * 0.1 - 0.45
+    elif case == "boundary":        # particles exactly on the faces and corners of the root
+        x = rng.random((600, 3)) - 0.5
+        x[:100, 0] = 0.5; x[100:200, 1] = -0.5; x[200:220] = 0.5; x[220:240] = -0.5
+    elif case == "sparse":          # far fewer particles than leaves
+        x = rng.random((37, 3)) - 0.5
+    else:
+        x = np.array([[0.1, -0.2, 0.3]])
+    q = rng.uniform(-1, 1, x.shape[0])
+    ref = oracle_d.fmm(x, q, 4, 3, U, E)
+    s, got = _solve("d", 4, 3, x, q, U, E)
+    assert np.all(np.isfinite(got))
+    if np.linalg.norm(ref) == 0:
+        assert np.linalg.norm(got) == 0
+    else:
+        assert rel_l2(got, ref) < 1e-12
+    s.close()
+
+
+def test_host_entry_matches_device_entry():
+    from bbfmm_b200 import operators as ops
+    import torch
+    from bbfmm_b200 import Solver
+    _, U, E = ops.load_operators(4, single=False)
+    x, q = uniform_inputs(20000, seed=11)
+    s = Solver(4, 3, 1.0, mode="d", operators=(U, E))
+    s.set_particles(x)
+    a = s.solve(torch.as_tensor(q, device="cuda")).cpu().numpy()
+    b = s.solve_host(q)
+    assert np.array_equal(a, b)
+    s.close()
