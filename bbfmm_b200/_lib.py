@@ -47,6 +47,9 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_set_timing.argtypes = [vp, i]
         L.bbfmm_b200_stage_times.argtypes = [vp, C.POINTER(C.c_float), i]
         L.bbfmm_b200_copy_multipoles.argtypes = [vp, i, vp]
+        L.bbfmm_b200_time_m2l.argtypes = [vp, i, i, C.POINTER(C.c_float)]
+        L.bbfmm_b200_direct.argtypes = [i, vp, vp, i, vp, vp, vp]
+        L.bbfmm_b200_device_status.argtypes = [i]
         L.bbfmm_b200_stream.argtypes = [vp]
         L.bbfmm_b200_stream.restype = vp
         L.bbfmm_b200_destroy.argtypes = [vp]

@@ -29,6 +29,7 @@ UNITS = [
     ("p2p.cu", [], "p2p"),
     ("m2l_simt.cu", [], "m2l_simt"),
     ("m2l_tc.cu", [], "m2l_tc"),
+    ("direct.cu", [], "direct"),
     ("solver.cu", [], "solver"),
 ]
 

@@ -1,18 +1,411 @@
-// Mixed-precision M2L on tcgen05 tensor cores (placeholder until the kernel lands).
+// Mixed-precision M2L on tcgen05 tensor cores (sm_100a).
+//
+// For one level, the contraction components j >= lead of
+//   L_i(F) = sum_{v in IL(F)} sum_j E_v(i, j) M_j(F + v)
+// are computed as three-term split products: with x = x_hi + x_lo (bf16 each),
+//   E M ~= E_hi M_hi + E_hi M_lo + E_lo M_hi,
+// accumulated in FP32 in tensor memory over all 189 offsets. The components j < lead
+// (default 16), whose FP32 accumulation would dominate the error, are computed in FP64
+// by the CUDA-core kernel (m2l_simt.cu); the projection after M2L sums both parts.
+//
+// Tile: 128 targets of one sibling class forming an 8x4x4 box of its parent grid
+// (GEMM M = 128) x all 256 outputs i (N = 256) in a 128 x 256 FP32 TMEM accumulator.
+// For an offset v the 128 sources form the same box in one class grid, shifted by a
+// whole number of parent cells, so each K-chunk of the A operand (64 bf16 of j per row)
+// is ONE 5-D TMA box load from the class-major multipole grid; out-of-grid sources are
+// zero-filled by TMA. The B operand chunk is rows i of E_v for the same 64 j.
+//
+// Warp roles (192 threads): warp 0 = TMA producer (and TMEM allocator), warp 1 = MMA
+// issuer, warps 2-5 = epilogue (tcgen05.ld of the accumulator, FP32 store of L).
+// Two pipeline stages of 96 KB (A_hi, A_lo 16 KB each; B_hi, B_lo 32 KB each).
+// Every mbarrier wait is bounded; on timeout the kernel records an error code in a
+// device status word, skips the remaining work, frees its tensor memory and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cstdio>
+#include <vector>
+
 #include "solver.cuh"
 
 namespace bbfmm {
-int tc_supported() { return 0; }
-int tc_prepare_operators(int, const double *, int, void **out, cudaStream_t) {
+
+namespace tc {
+
+constexpr int BM = 128, BN = 256, BK = 64;  // targets, outputs, bf16 per K-chunk (128 B)
+constexpr int STAGES = 2;
+constexpr int A_BYTES = BM * BK * 2;        // 16 KB
+constexpr int B_BYTES = BN * BK * 2;        // 32 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int BOX_X = 8, BOX_Y = 4, BOX_Z = 4;
+constexpr uint32_t WAIT_LIMIT = 1u << 26;
+
+__device__ int g_tc_status = 0;  // 0 = ok; else code of the first failed wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false (and the status word set) if the phase did not complete in time.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int code) {
+  for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try(bar, parity)) return true;
+  atomicCAS(&g_tc_status, 0, code);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1,
+                                            int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+// K-major, 128-byte swizzled operand tile: rows of 128 B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
+  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for SW128 K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;               // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1 << 46;                         // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                         // 128-byte swizzle
+  return d;
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = 256.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Grid: one CTA per tile (class c, 8x4x4 box). L32: the level's output, cpg layout [cell][256].
+__global__ void __launch_bounds__(192, 1)
+    m2l_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
+                  const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
+                  float *__restrict__ L32, int level, const int4 *__restrict__ offs, int lead) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *gbase = smem_raw + (base - raw);
+  const uint32_t bar_base = base + STAGES * STAGE_BYTES;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * STAGE_BYTES);
+  // bars[0..S-1] = full, bars[S..2S-1] = empty, bars[2S] = accumulator ready; tmem slot after
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 1);
+  auto full_bar = [&](int s) { return bar_base + 8u * s; };
+  auto empty_bar = [&](int s) { return bar_base + 8u * (STAGES + s); };
+  const uint32_t acc_bar = bar_base + 8u * (2 * STAGES);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int P = 1 << (level - 1);
+  const int nbx = P / BOX_X, nby = P / BOX_Y, nbz = P / BOX_Z;
+  const int tiles_per_class = nbx * nby * nbz;
+  const int c = blockIdx.x / tiles_per_class;
+  const int tb = blockIdx.x % tiles_per_class;
+  const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
+  const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
+  const int kfirst = lead / 16;  // K-steps of 16 skipped in chunk 0 (computed in FP64)
+  const int nchunk = BN / BK;    // 4 K-chunks per offset (r = 256)
+  const int chunk0 = kfirst / 4;  // whole chunks skipped
+  const int kstep0 = kfirst % 4;  // K-steps skipped in the first used chunk
+  const int used_chunks = nchunk - chunk0;
+  const int niter = 189 * used_chunks;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(acc_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(empty_bar(s), ph ^ 1u, 1)) break;
+      const int o = it / used_chunks, kc = chunk0 + it % used_chunks;
+      const int4 ov = offs[c * 189 + o];
+      const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
+      const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
+      const int sc = (scx << 2) | (scy << 1) | scz;
+      const int sx = bx0 + (gx - scx) / 2, sy = by0 + (gy - scy) / 2, sz = bz0 + (gz - scz) / 2;
+      const uint32_t st = base + s * STAGE_BYTES;
+      mbar_expect_tx(full_bar(s), STAGE_BYTES);
+      tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, sc);
+      tma_load_5d(st + A_BYTES, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, sc);
+      tma_load_3d(st + 2 * A_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
+      tma_load_3d(st + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    uint32_t acc = 0;
+    bool ok = true;
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(full_bar(s), ph, 2)) { ok = false; break; }
+      tc_fence_after();
+      const uint32_t st = base + s * STAGE_BYTES;
+      const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
+      for (int ks = k0; ks < BK / 16; ++ks) {
+        const uint64_t ahi = sw128_desc(st + ks * 32), alo = sw128_desc(st + A_BYTES + ks * 32);
+        const uint64_t bhi = sw128_desc(st + 2 * A_BYTES + ks * 32);
+        const uint64_t blo = sw128_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
+        mma_bf16(tmem, ahi, bhi, acc);
+        mma_bf16(tmem, ahi, blo, 1u);
+        mma_bf16(tmem, alo, bhi, 1u);
+        acc = 1u;
+      }
+      mma_commit(empty_bar(s));
+    }
+    (void)ok;
+    mma_commit(acc_bar);
+  } else if (warp >= 2) {
+    // ---------------- epilogue: TMEM -> registers -> L32
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = q * 32 + lane;
+    const bool ok = mbar_wait(acc_bar, 0, 3);
+    tc_fence_after();
+    if (ok) {
+      const int tx = row % BOX_X, ty = (row / BOX_X) % BOX_Y, tz = row / (BOX_X * BOX_Y);
+      const int64_t P3 = (int64_t)P * P * P;
+      const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
+      float *dst = L32 + cell * BN;
+      for (int col = 0; col < BN; col += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
+#pragma unroll
+        for (int i = 0; i < 32; i += 4)
+          *reinterpret_cast<float4 *>(dst + col + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------- splitting
+__global__ void split_kernel(int64_t count, const double *__restrict__ src, __nv_bfloat16 *__restrict__ hi,
+                             __nv_bfloat16 *__restrict__ lo) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+    const double x = src[e];
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[e] = h;
+    lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+  }
+}
+
+}  // namespace tc
+
+// --------------------------------------------------------------------- host side
+using PFN_encodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                     const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled encode_fn() {
+  static PFN_encodeTiled fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_encodeTiled)p;
+  }
+  return fn;
+}
+
+struct TcOps {
+  int r = 0;
+  __nv_bfloat16 *Ehi = nullptr, *Elo = nullptr;
+  CUtensorMap mapBhi, mapBlo;
+};
+
+int tc_supported() {
+  int dev = 0, major = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) return 0;
+  return major == 10 && encode_fn() != nullptr;
+}
+
+static int make_map(CUtensorMap *m, void *ptr, int rank, const cuuint64_t *dims, const cuuint64_t *strides_bytes,
+                    const cuuint32_t *box) {
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult rc = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, ptr, dims, strides_bytes, box, es,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) {
+    char buf[96];
+    snprintf(buf, sizeof(buf), "cuTensorMapEncodeTiled failed (%d)", (int)rc);
+    return bbfmm_set_error(BBFMM_ERR_CUDA, buf);
+  }
+  return BBFMM_OK;
+}
+
+int tc_prepare_operators(int r, const double *Ert, int lead, void **out, cudaStream_t s) {
   *out = nullptr;
-  return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L not built");
+  if (r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L is built for r = 256 (n = 8)");
+  if (lead < 0 || lead > 64 || lead % 16) return bbfmm_set_error(BBFMM_ERR_ARG, "lead must be 0, 16, 32, 48 or 64");
+  if (!encode_fn()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  TcOps *ops = new TcOps();
+  ops->r = r;
+  const size_t cnt = (size_t)BBFMM_NUM_OFFSETS * r * r;
+  if (cudaMalloc(&ops->Ehi, cnt * 2) != cudaSuccess || cudaMalloc(&ops->Elo, cnt * 2) != cudaSuccess) {
+    tc_free_operators(ops);
+    return bbfmm_set_error(BBFMM_ERR_NOMEM, "operator split allocation failed");
+  }
+  tc::split_kernel<<<148 * 8, 256, 0, s>>>((int64_t)cnt, Ert, ops->Ehi, ops->Elo);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    tc_free_operators(ops);
+    return bbfmm_set_cuda_error(e, "split operators", __FILE__, __LINE__);
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)r, (cuuint64_t)r, (cuuint64_t)BBFMM_NUM_OFFSETS};
+  const cuuint64_t strides[2] = {(cuuint64_t)r * 2, (cuuint64_t)r * r * 2};
+  const cuuint32_t box[3] = {tc::BK, (cuuint32_t)tc::BN, 1};
+  int rc = make_map(&ops->mapBhi, ops->Ehi, 3, dims, strides, box);
+  if (rc == BBFMM_OK) rc = make_map(&ops->mapBlo, ops->Elo, 3, dims, strides, box);
+  if (rc != BBFMM_OK) {
+    tc_free_operators(ops);
+    return rc;
+  }
+  *out = ops;
+  return BBFMM_OK;
 }
-void tc_free_operators(void *) {}
-size_t tc_split_bytes(int r, int64_t ncell) { return (size_t)ncell * r * 4; }
-int tc_split_multipoles(int, int64_t, const double *, int, void *, cudaStream_t) {
-  return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L not built");
+
+void tc_free_operators(void *p) {
+  TcOps *ops = (TcOps *)p;
+  if (!ops) return;
+  if (ops->Ehi) cudaFree(ops->Ehi);
+  if (ops->Elo) cudaFree(ops->Elo);
+  delete ops;
 }
-int launch_m2l_tc(int, const void *, const void *, float *, int, const int4 *, int, cudaStream_t) {
-  return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L not built");
+
+size_t tc_split_bytes(int r, int64_t ncell) { return (size_t)ncell * r * 2 * 2; }
+
+// Msplit = [hi plane | lo plane], each ncell_total * r bf16, same cell order as M.
+int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s) {
+  (void)lead;
+  __nv_bfloat16 *hi = (__nv_bfloat16 *)Msplit;
+  __nv_bfloat16 *lo = hi + (size_t)ncell * r;
+  tc::split_kernel<<<148 * 8, 256, 0, s>>>(ncell * r, M, hi, lo);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "split multipoles", __FILE__, __LINE__);
 }
+
+int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, float *L32,
+                  int level, const int4 *offs, int lead, cudaStream_t s) {
+  const TcOps *ops = (const TcOps *)opsv;
+  if (!ops || r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L needs r = 256 operators");
+  const int P = 1 << (level - 1);
+  if (P < tc::BOX_X) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs level >= 4");
+  const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Msplit + (size_t)cell_offset * r;
+  const __nv_bfloat16 *lo = (const __nv_bfloat16 *)Msplit + (size_t)(ncell_total + cell_offset) * r;
+  CUtensorMap mapAhi, mapAlo;
+  const cuuint64_t dims[5] = {(cuuint64_t)r, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)P, 8};
+  const cuuint64_t strides[4] = {(cuuint64_t)r * 2, (cuuint64_t)r * 2 * P, (cuuint64_t)r * 2 * P * P,
+                                 (cuuint64_t)r * 2 * P * P * P};
+  const cuuint32_t box[5] = {tc::BK, tc::BOX_X, tc::BOX_Y, tc::BOX_Z, 1};
+  int rc = make_map(&mapAhi, (void *)hi, 5, dims, strides, box);
+  if (rc == BBFMM_OK) rc = make_map(&mapAlo, (void *)lo, 5, dims, strides, box);
+  if (rc != BBFMM_OK) return rc;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc::m2l_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc smem attribute", __FILE__, __LINE__);
+    attr = true;
+  }
+  const int tiles = 8 * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
+  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo, L32, level, offs,
+                                                       lead);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc", __FILE__, __LINE__);
+}
+
+// Reads and clears the kernel status word (0 = every bounded wait completed).
+int tc_status(int clear) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, tc::g_tc_status, sizeof(int)) != cudaSuccess) return -1;
+  if (clear && v) {
+    int z = 0;
+    cudaMemcpyToSymbol(tc::g_tc_status, &z, sizeof(int));
+  }
+  return v;
+}
+
 }  // namespace bbfmm

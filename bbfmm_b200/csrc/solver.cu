@@ -203,8 +203,8 @@ int Solver<T>::set_particles_sorted(int N_, const int *perm_h, const int *leaf_s
 }
 
 template <typename T>
-void Solver<T>::mark(int stage) {
-  ++kernel_launches;
+void Solver<T>::mark(int stage, int launches) {
+  kernel_launches += launches;
   if (!timing) return;
   if (stage < 0) {
     cudaEventRecord(ev[ST_COUNT], stream);
@@ -245,8 +245,7 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
     mark(ST_PROJ_UP);
   }
   if (mode == MODE_MIXED) {
-    const int64_t tot = (Moff[maxlev] + pow8i(maxlev) * r) / r;
-    TRY(tc_split_multipoles(r, tot, (const double *)Mall, lead, Msplit, stream));
+    TRY(tc_split_multipoles(r, Mcells(), (const double *)Mall, lead, Msplit, stream));
     mark(ST_PROJ_UP);
   }
   return BBFMM_OK;
@@ -257,19 +256,20 @@ int Solver<T>::interaction(int lo, int hi) {
   const Tables tb = tables();
   for (int l = lo; l <= hi; ++l) {
     const T *Ml = Mall + Moff[l];
-    if (mode == MODE_MIXED) {
+    const bool split = mode == MODE_MIXED && l >= TC_MIN_LEVEL;
+    if (split) {
       // leading components in FP64 on CUDA cores, the rest as split bf16 on tensor cores
       if (lead > 0) TRY(launch_m2l_simt<T>(r, Ml, Ert, Lbuf, l, 0, lead, offs, 0, stream));
       else BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * pow8i(l) * r, stream));
-      TRY(launch_m2l_tc(r, (const unsigned char *)Msplit + tc_split_bytes(r, Moff[l] / r), tcops, L32, l, offs,
-                        lead, stream));
+      TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, L32, l, offs, lead, stream));
+      mark(ST_M2L, 2);
     } else {
       TRY(launch_m2l_simt<T>(r, Ml, Ert, Lbuf, l, 0, r, offs, 0, stream));
+      mark(ST_M2L);
     }
-    mark(ST_M2L);
     const T scale = (T)1 / cell_length<T>(l, (T)L);
-    TRY(launch_proj<T>(pow8i(l), r, n3, Lbuf, mode == MODE_MIXED ? L32 : nullptr, Bdn, kw, scale, F[l & 1], l,
-                       MAP_IN_CPG, stream));
+    TRY(launch_proj<T>(pow8i(l), r, n3, Lbuf, split ? L32 : nullptr, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG,
+                       stream));
     mark(ST_PROJ_DOWN);
     if (l > BBFMM_MINLEV) {
       TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream));
@@ -288,10 +288,11 @@ int Solver<T>::downward_finish(void *phi_dev, int phi_is_double, bool near) {
     if (mode == MODE_MIXED) {
       TRY(launch_make_local(N, (const double *)pos4, leafm, maxlev, L, loc4, stream));
       TRY(launch_p2p_local(N, loc4, leaf_start, leafm, maxlev, L, (double *)phis, stream));
+      mark(ST_P2P, 2);
     } else {
       TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, phis, stream));
+      mark(ST_P2P);
     }
-    mark(ST_P2P);
   }
   if (phi_dev) {
     if (phi_is_double) TRY((launch_scatter<T, double>(N, perm, phis, (double *)phi_dev, stream)));
@@ -309,13 +310,44 @@ int Solver<T>::solve(const void *q_dev, void *phi_dev, int io_double) {
   if (timing) {
     for (int i = 0; i < ST_COUNT; ++i) stage_ms[i] = 0.f;
     if (!ev[ST_COUNT]) cudaEventCreate(&ev[ST_COUNT]);
-    mark(-1);
-    --kernel_launches;
+    mark(-1, 0);
   }
   TRY(upward(q_dev, io_double));
   TRY(interaction(BBFMM_MINLEV, maxlev));
   TRY(downward_finish(phi_dev, io_double, true));
   return BBFMM_OK;
+}
+
+// Re-runs the M2L of one level `reps` times between two events on the solver's stream
+// (multipoles of the last solve as input) and reports the mean time per launch group.
+template <typename T>
+int Solver<T>::time_m2l(int level, int reps, float *ms) {
+  if (level < BBFMM_MINLEV || level > maxlev || reps < 1) return bbfmm_set_error(BBFMM_ERR_ARG, "bad level/reps");
+  cudaEvent_t a, b;
+  BBFMM_CUDA_OK(cudaEventCreate(&a));
+  BBFMM_CUDA_OK(cudaEventCreate(&b));
+  const T *Ml = Mall + Moff[level];
+  int rc = BBFMM_OK;
+  float tot[2] = {0.f, 0.f};
+  for (int part = 0; part < (mode == MODE_MIXED ? 2 : 1) && rc == BBFMM_OK; ++part) {
+    cudaEventRecord(a, stream);
+    for (int i = 0; i < reps && rc == BBFMM_OK; ++i) {
+      if (mode != MODE_MIXED) rc = launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, 0, r, offs, 0, stream);
+      else if (part == 0) rc = level >= TC_MIN_LEVEL
+                                   ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, L32, level, offs,
+                                                   lead, stream)
+                                   : launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, 0, r, offs, 0, stream);
+      else rc = lead > 0 ? launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, 0, lead, offs, 0, stream) : BBFMM_OK;
+    }
+    cudaEventRecord(b, stream);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&tot[part], a, b);
+  }
+  ms[0] = tot[0] / reps;
+  ms[1] = tot[1] / reps;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
 }
 
 template <typename T>
@@ -471,6 +503,20 @@ int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *h, int level, void *host_out) 
   if (!h || !host_out) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   if (h->f) return h->f->copy_multipoles_morton(level, (float *)host_out);
   return h->d->copy_multipoles_morton(level, (double *)host_out);
+}
+
+int bbfmm_b200_time_m2l(bbfmm_b200_solver *h, int level, int reps, float *ms) {
+  if (!h || !ms) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  return h->f ? h->f->time_m2l(level, reps, ms) : h->d->time_m2l(level, reps, ms);
+}
+
+int bbfmm_b200_device_status(int clear) { return bbfmm::tc_status(clear); }
+
+int bbfmm_b200_direct(int N, const double *xyz_dev, const double *q_dev, int ntarget, const int *targets_dev,
+                      double *out_dev, void *stream) {
+  if (N < 0 || ntarget < 0 || (ntarget > 0 && (!xyz_dev || !q_dev || !targets_dev || !out_dev)))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "bad direct-sum arguments");
+  return bbfmm::launch_direct_fp64(N, xyz_dev, q_dev, ntarget, targets_dev, out_dev, (cudaStream_t)stream);
 }
 
 void *bbfmm_b200_stream(bbfmm_b200_solver *h) {

@@ -34,6 +34,7 @@ int launch_make_local(int N, const double *pos4, const int *leafm, int maxlev, d
 int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s);
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s);
 void build_offset_table(int *out);
+int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
 
 template <typename T> int bbfmm_weights_t(int n, T *Tkz, int *Ktable, T *Kweights, T *Cweights);
 
@@ -44,8 +45,10 @@ int tc_prepare_operators(int r, const double *Ert, int lead, void **out, cudaStr
 void tc_free_operators(void *ops);
 int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s);
 size_t tc_split_bytes(int r, int64_t ncell);
-int launch_m2l_tc(int r, const void *Msplit, const void *ops, float *L32, int level, const int4 *offs, int lead,
-                  cudaStream_t s);
+int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, float *L32,
+                  int level, const int4 *offs, int lead, cudaStream_t s);
+int tc_status(int clear);
+constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
 
 template <typename T>
 struct Solver {
@@ -82,6 +85,7 @@ struct Solver {
   int kernel_launches = 0;
 
   Tables tables() const;
+  int64_t Mcells() const { return (Moff[maxlev] + pow8i(maxlev) * r) / r; }
   int init(int n_, int maxlev_, double L_, int mode_, int lead_, int device_, cudaStream_t s);
   int set_tables(const T *Tkz, const T *Cweights, const T *Kweights);  // host arrays
   int set_operators(const T *U, const T *E);                              // host, reference layout
@@ -92,7 +96,8 @@ struct Solver {
   int downward_finish(void *phi_dev, int phi_is_double, bool near);  // L2P, P2P, scatter
   int solve(const void *q_dev, void *phi_dev, int io_double);
   int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order
-  void mark(int stage);
+  void mark(int stage, int launches = 1);
+  int time_m2l(int level, int reps, float *ms);
   void release();
 };
 

@@ -91,7 +91,8 @@ class Solver:
         if out is None:
             out = torch.empty_like(q)
         # order the solver's stream after the caller's work on q, and the caller's stream
-        # after the solve; keep both buffers alive for the solver's stream
+        # after the solve: both buffers belong to the caller's stream, which cannot reuse
+        # them before the solve has finished with them
         caller = torch.cuda.current_stream(q.device)
         mine = torch.cuda.ExternalStream(self.stream, device=q.device)
         ready = torch.cuda.Event()
@@ -101,8 +102,6 @@ class Solver:
         done = torch.cuda.Event()
         done.record(mine)
         caller.wait_event(done)
-        q.record_stream(mine)
-        out.record_stream(mine)
         return out
 
     def solve_host(self, q):
@@ -119,10 +118,30 @@ class Solver:
         nl = _lib.lib().bbfmm_b200_stage_times(self.h, ms, len(_lib.STAGES))
         return dict(zip(_lib.STAGES, list(ms))), nl
 
+    def time_m2l(self, level: int, reps: int = 3):
+        ms = (C.c_float * 2)()
+        _lib.check(_lib.lib().bbfmm_b200_time_m2l(self.h, level, reps, ms))
+        return float(ms[0]), float(ms[1])
+
     def multipoles(self, level: int):
         out = np.empty(8 ** level * self.r, dtype=self.np_dtype)
         _lib.check(_lib.lib().bbfmm_b200_copy_multipoles(self.h, level, _ptr(out)))
         return out
+
+
+def direct(xyz, q, targets, stream=None):
+    """FP64 direct sum q_i sum_{j != i} q_j / r_ij on the GPU for the given targets
+    (torch CUDA tensors: xyz (N,3) float64, q (N,) float64, targets (T,) int32)."""
+    import torch
+    xyz = xyz.to(torch.float64).contiguous()
+    q = q.to(torch.float64).contiguous()
+    targets = targets.to(torch.int32).contiguous()
+    out = torch.empty(targets.numel(), dtype=torch.float64, device=q.device)
+    st = torch.cuda.current_stream(q.device).cuda_stream if stream is None else stream
+    _lib.check(_lib.lib().bbfmm_b200_direct(q.numel(), C.c_void_p(xyz.data_ptr()), C.c_void_p(q.data_ptr()),
+                                             targets.numel(), C.c_void_p(targets.data_ptr()),
+                                             C.c_void_p(out.data_ptr()), C.c_void_p(st)))
+    return out
 
 
 def bbfmm(xyz, q, L: float = 1.0, n: int = 4, level_modifier: int = 0, mode: str = "d", maxlev=None,

@@ -1,0 +1,375 @@
+"""Benchmark: one FMM solve (upward, M2L, downward, near field) of N = 4,194,304 uniform
+particles, n = 8 (r = 256), leaves at level 7 (2 particles per leaf on average), q ~ U[-1,1].
+
+A "step" is one solve with charges resident in HBM (value) or from pinned host memory with
+the result copied back (e2e). The headline mode is the mixed-precision solver; the plain
+FP64 solver of the same FMM is timed beside it for the speed-up and error ratio, both
+against an FP64 direct sum on 4,096 seeded targets.
+
+N > 1 GPUs: independent replicas (one solve per rank and step; the path does not shard),
+timed on the device with the max over ranks.
+
+--impl reference: the reference's own CPU code (oracle/_ref, built from its sources; else
+the CPU oracle port) on the host cores, each step a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_FULL = 4_194_304
+N_ORDER = 8
+MAXLEV = 7
+N_TARGETS = 4096
+METRIC = "FMM solves/s at N=4,194,304, n=8, depth 7 (1 GPU; err <= 1.2x FP64 required)"
+
+
+def interactions_per_level(level: int) -> int:
+    """Exact number of M2L (target, source) pairs at a level of the full uniform tree."""
+    m = 2 ** level
+    tot = 0
+    for c in range(8):
+        b = ((c >> 2) & 1, (c >> 1) & 1, c & 1)
+        for vx in range(-3, 4):
+            for vy in range(-3, 4):
+                for vz in range(-3, 4):
+                    if max(abs(vx), abs(vy), abs(vz)) <= 1:
+                        continue
+                    v = (vx, vy, vz)
+                    if any(v[a] < -2 - b[a] or v[a] > 3 - b[a] for a in range(3)):
+                        continue
+                    cnt = 1
+                    for a in range(3):
+                        t = np.arange(b[a], m, 2)
+                        cnt *= int(((t + v[a] >= 0) & (t + v[a] < m)).sum())
+                    tot += cnt
+    return tot
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (SM clock, max clock, throttle reasons)."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_inputs(N, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.random((N, 3)) - 0.5      # [0,1)^3 shifted onto the origin-centred root cell
+    q = rng.uniform(-1.0, 1.0, N)
+    return x, q
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_sample(N_sample, maxlev_sample, reps=1):
+    """Time the reference's CPU FMM (oracle/_ref) on a sample with the same particles per
+    leaf as the full workload; returns (seconds per sample solve, cores, kind)."""
+    from oracle.oracle import Oracle, Reference, reference_available
+    from bbfmm_b200 import operators as ops
+    x, q = make_inputs(N_sample, 99)
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if reference_available("d"):
+        ref = Reference("d")
+        d = os.path.join(ops.default_cache_dir(), "ref")
+        kp, up = ops.operator_file_names(N_ORDER, False)
+        kp, up = os.path.join(d, kp), os.path.join(d, up)
+        if not (os.path.exists(kp) and os.path.exists(up)):
+            _, U, E = ops.load_operators(N_ORDER, False)
+            ops.write_operator_files(d, N_ORDER, U, E, False)
+        ref.fmm(x, q, N_ORDER, maxlev_sample, kp, up)  # warm (file cache, page faults)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ref.fmm(x, q, N_ORDER, maxlev_sample, kp, up)
+        return (time.perf_counter() - t0) / reps, cores, "reference"
+    _, U, E = ops.load_operators(N_ORDER, False)
+    orc = Oracle("d")
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.fmm(x, q, N_ORDER, maxlev_sample, U, E)
+    return (time.perf_counter() - t0) / reps, 1, "port"
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    # bounded sample: same leaf density (2 per leaf) at level 4 -> 8,192 particles
+    Ns, ls = 8192, 4
+    times = []
+    for i in range(args.warmup + args.steps):
+        t, cores, kind = reference_sample(Ns, ls)
+        if i >= args.warmup:
+            times.append(t)
+    t = float(np.mean(times))
+    value = (1.0 / t) * (Ns / N_FULL)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solve/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "bbFMM Laplace 1/r, N=4,194,304 uniform, n=8, maxlev 7", "sample_N": Ns,
+                       "sample_maxlev": ls},
+            "cpu_baseline": {"value": value, "unit": "solve/s", "cores": cores, "kind": kind,
+                             "sample": f"one reference CPU solve of N={Ns}, n=8, maxlev {ls} (2 particles/leaf) "
+                                       f"per step, scaled by {Ns}/{N_FULL}"},
+            "e2e": {"value": value, "unit": "solve/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "d", "s"])
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--N", type=int, default=N_FULL)
+    ap.add_argument("--maxlev", type=int, default=MAXLEV)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.fmm import direct
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    N, n, lev = args.N, N_ORDER, args.maxlev
+    x, q = make_inputs(N, 2 + rank)
+    dt = torch.float32 if args.mode == "s" else torch.float64
+    sol = Solver(n, lev, 1.0, mode=args.mode, device=local)
+    sol.set_particles(x)
+    q_dev = torch.as_tensor(q, dtype=dt, device="cuda")
+    phi_dev = torch.empty_like(q_dev)
+    stream = torch.cuda.ExternalStream(sol.stream)
+
+    def step():
+        sol.solve(q_dev, out=phi_dev)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3) / args.steps
+    value = world / t_dev
+
+    # end to end through the public host-buffer entry point (pinned host memory)
+    q_host = torch.as_tensor(q, dtype=dt).pin_memory().numpy()
+    for _ in range(2):
+        sol.solve_host(q_host)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ee0.record(stream)
+    for _ in range(args.steps):
+        phi_host = sol.solve_host(q_host)
+    ee1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(max(ee0.elapsed_time(ee1) / 1e3, 0.0) / args.steps)
+    t_e2e_wall = (time.perf_counter() - t0) / args.steps
+    t_e2e = max(t_e2e, max_over_ranks(t_e2e_wall))
+    esz = 4 if args.mode == "s" else 8
+
+    # accuracy against the FP64 direct sum on seeded targets
+    targets = np.random.default_rng(1234).choice(N, N_TARGETS, replace=False).astype(np.int32)
+    xd = torch.as_tensor(x, device="cuda")
+    qd64 = torch.as_tensor(q, device="cuda")
+    td = torch.as_tensor(targets, device="cuda")
+    dref = direct(xd, qd64, td).cpu().numpy()
+    phi_mode = phi_dev.double().cpu().numpy()
+    def rel(a):
+        return float(np.sqrt(((a[targets] - dref) ** 2).sum() / (dref ** 2).sum()))
+    err_mode = rel(phi_mode)
+
+    # stage breakdown and the dominant kernel's launch time (CUDA events on the solver stream)
+    sol.set_timing(True)
+    sol.solve(q_dev, out=phi_dev)
+    torch.cuda.synchronize()
+    stages, launches = sol.stage_times()
+    sol.set_timing(False)
+    m2l_ms, lead_ms = sol.time_m2l(lev, reps=3)
+    I_leaf = interactions_per_level(lev)
+    r = n ** 3 // 2
+    hbm, bf16, bf16_sus, peak_src = measured_peaks()
+    if args.mode == "mixed":
+        tc_flop = 2.0 * r * (r - sol.lead) * I_leaf           # algorithmic flops of the split-bf16 part
+        achieved = tc_flop / (m2l_ms / 1e3) / 1e12
+        peak = bf16 / 3.0                                      # three bf16 products per term
+        roof = {"kernel": "m2l_tc (split-bf16 tcgen05 M2L, leaf level)", "bound": "tensor",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": f"{peak_src} bf16 dense burst / 3 products", "traffic": None,
+                "flop_per_launch": tc_flop, "launch_ms": m2l_ms}
+    else:
+        flop = 2.0 * r * r * I_leaf
+        achieved = flop / (m2l_ms / 1e3) / 1e12
+        peak = 40.0 if args.mode == "d" else 80.0
+        roof = {"kernel": "m2l_simt (leaf level)", "bound": "fp64" if args.mode == "d" else "fp32",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "nominal B200 FP64/FP32 vector rate (no measured figure)", "traffic": None,
+                "flop_per_launch": flop, "launch_ms": m2l_ms}
+
+    # plain FP64 GPU form of the same FMM (the speed-up denominator)
+    plain = None
+    if args.mode != "d" and args.plain_steps > 0:
+        sol.close()
+        del phi_dev
+        torch.cuda.empty_cache()
+        pd = Solver(n, lev, 1.0, mode="d", device=local)
+        pd.set_particles(x)
+        q64 = torch.as_tensor(q, device="cuda")
+        ph64 = torch.empty_like(q64)
+        pd.solve(q64, out=ph64)
+        torch.cuda.synchronize()
+        pstream = torch.cuda.ExternalStream(pd.stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(pstream)
+        for _ in range(args.plain_steps):
+            pd.solve(q64, out=ph64)
+        b.record(pstream)
+        torch.cuda.synchronize()
+        t_plain = max_over_ranks(a.elapsed_time(b) / 1e3 / args.plain_steps)
+        err_plain = rel(ph64.cpu().numpy())
+        plain = {"s_per_solve": t_plain, "err_vs_direct": err_plain, "speedup": t_plain / t_dev,
+                 "err_ratio": err_mode / err_plain}
+        pd.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            Ns, ls = 65536, 5
+            t_ref, cores, kind = reference_sample(Ns, ls)
+            cpu = {"value": (1.0 / t_ref) * (Ns / N_FULL), "unit": "solve/s", "cores": cores, "kind": kind,
+                   "sample": f"one CPU solve of N={Ns}, n=8, maxlev {ls} (2 particles/leaf, same density), "
+                             f"{t_ref:.2f} s, scaled by {Ns}/{N_FULL}"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "solve/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solve/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_dev * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"mixed": "bf16x3+f64", "d": "f64", "s": "f32"}[args.mode],
+            "data": "synthetic (seeded uniform [0,1)^3, q~U[-1,1])",
+            "config": {"workload": "bbFMM Laplace 1/r, N=4,194,304 uniform, n=8 (r=256), maxlev 7",
+                       "N": N, "n": n, "maxlev": lev, "mode": args.mode,
+                       "lead_fp64_components": sol.lead if args.mode == "mixed" else None,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs and working set larger than L2 (operators 166 MB, expansions > 20 GB)"},
+            "err_vs_fp64_direct": err_mode, "n_targets": N_TARGETS,
+            "plain_fp64": plain,
+            "stages_ms": stages,
+            "e2e": {"value": world / t_e2e, "unit": "solve/s", "h2d_bytes_per_step": N * esz,
+                    "d2h_bytes_per_step": N * esz},
+            "gpu_launches": launches * args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

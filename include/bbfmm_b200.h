@@ -123,6 +123,22 @@ BBFMM_B200_API int bbfmm_b200_stage_times(const bbfmm_b200_solver *s, float *ms,
  * the reference's Morton cell order (the level's slice of proxysval). */
 BBFMM_B200_API int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *s, int level, void *host_out);
 
+/* Re-run the M2L of one level `reps` times (inputs of the last solve) between CUDA events
+ * on the solver's stream: ms[0] = mean time of the main M2L kernel per launch, ms[1] =
+ * mean time of the FP64 leading-component kernel (MIXED only, else 0). */
+BBFMM_B200_API int bbfmm_b200_time_m2l(bbfmm_b200_solver *s, int level, int reps, float *ms);
+
+/* FP64 direct sum on the device (DirectCalc3D, bbfmm.c:471-504): out[t] =
+ * q_i sum_{x_j != x_i} q_j / |x_j - x_i| for i = targets[t]; xyz (N x 3), q, targets, out are
+ * device pointers; runs on `stream` (cudaStream_t, may be NULL). */
+BBFMM_B200_API int bbfmm_b200_direct(int N, const double *xyz_dev, const double *q_dev, int ntarget,
+                                     const int *targets_dev, double *out_dev, void *stream);
+
+/* Status word of the tensor-core kernels: 0 when every bounded wait of every launch so far
+ * completed, else the code of the first wait that gave up (the launch then skipped its
+ * remaining work and returned). Synchronises the device; clear != 0 resets the word. */
+BBFMM_B200_API int bbfmm_b200_device_status(int clear);
+
 BBFMM_B200_API void *bbfmm_b200_stream(bbfmm_b200_solver *s);
 BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
 
