@@ -26,7 +26,7 @@ class BBFMMError(RuntimeError):
 
 class Config(C.Structure):
     _fields_ = [("n", C.c_int), ("maxlev", C.c_int), ("L", C.c_double), ("mode", C.c_int),
-                ("lead", C.c_int), ("device", C.c_int), ("stream", C.c_void_p)]
+                ("lead", C.c_int), ("lead_rows", C.c_int), ("device", C.c_int), ("stream", C.c_void_p)]
 
 
 _lib = None

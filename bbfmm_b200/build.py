@@ -29,6 +29,8 @@ UNITS = [
     ("p2p.cu", [], "p2p"),
     ("m2l_simt.cu", [], "m2l_simt"),
     ("m2l_tc.cu", [], "m2l_tc"),
+    ("m2l_dmma.cu", [], "m2l_dmma"),
+    ("proj_dmma.cu", [], "proj_dmma"),
     ("direct.cu", [], "direct"),
     ("solver.cu", [], "solver"),
 ]

@@ -1,0 +1,165 @@
+// FP64 M2L on the FP64 tensor path (mma.sync m8n8k4 f64) over the dense class-major grid.
+//
+// Same contraction and tiling as m2l_simt.cu (one CTA per 4x4x4 box of targets of one
+// sibling class), restricted to contraction components j in [j0, j1) and outputs
+// i in [0, ni):
+//   j in [0, 256), i in [0, 256)   the plain FP64 M2L,
+//   j in [0, lead), i in [0, ilead) the FP64 leading block of the mixed-precision M2L.
+// The A tile (sources x 16 j) is gathered from the cpg multipole grid and the B tile
+// (16 j x 256 i) is read from the operators in the reference's own column-major layout
+// E[k][j][i] (K file, bbfmm.c:1384-1405), so both global reads are contiguous. Tiles are
+// double-buffered with cp.async; 8 warps in a 2 x 4 grid each own a 32-target x 64-output
+// accumulator (4 x 8 fragments of 8x8); warps whose outputs lie beyond ni skip the math.
+#include "common.cuh"
+
+namespace bbfmm {
+
+namespace dm {
+
+constexpr int NT = 64, R = 256, BK = 16;
+constexpr int AST = NT + 4;   // padded row strides (doubles): conflict-free fragment reads
+constexpr int BST = R + 4;
+constexpr int STAGE_DOUBLES = BK * AST + BK * BST;
+constexpr int SMEM_BYTES = 2 * STAGE_DOUBLES * 8;
+
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void *src, bool valid) {
+  const int n = valid ? 8 : 0;  // zero-fill when the source lies outside the grid
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restrict__ M,
+                                                          const double *__restrict__ Ecol,
+                                                          double *__restrict__ Lout, int level, int j0, int j1,
+                                                          int ni, const int4 *__restrict__ offs) {
+  extern __shared__ __align__(16) double smem[];
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;
+  const int nbox = P / bw;
+  const int tiles_per_class = nbox * nbox * nbox;
+  const int c = blockIdx.x / tiles_per_class;
+  const int tb = blockIdx.x % tiles_per_class;
+  const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
+  const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
+  const int nt = bw * bw * bw;
+  const int64_t P3 = (int64_t)P * P * P;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warp grid
+  const bool active = wn * 64 < ni;         // this warp has outputs to compute
+  const int nb = ni < R ? ((ni + 63) / 64) * 64 : R;  // B columns staged
+  const int nchunk = (j1 - j0 + BK - 1) / BK;
+  const int niter = 189 * nchunk;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+
+  auto issue = [&](int it, int buf) {
+    const int o = it / nchunk, jc = j0 + (it % nchunk) * BK;
+    const int4 ov = offs[c * 189 + o];
+    const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
+    const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
+    const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
+    const int sc = (scx << 2) | (scy << 1) | scz;
+    const uint32_t sa = sbase + (uint32_t)(buf * STAGE_DOUBLES) * 8u;
+    const uint32_t sb = sa + (uint32_t)(BK * AST) * 8u;
+    // A: 64 targets x 16 j, 8-byte copies, zero outside the grid / j range
+    for (int e = tid; e < NT * BK; e += 256) {
+      const int t = e / BK, jj = e % BK;
+      const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
+      const bool ok = t < nt && jc + jj < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
+      const double *src = ok ? M + ((int64_t)sc * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + jj : M;
+      cp_async8(sa + (uint32_t)(jj * AST + t) * 8u, src, ok);
+    }
+    // B: 16 rows j of E_k (the first nb outputs i), 16-byte copies
+    const double *Ek = Ecol + (int64_t)ov.x * R * R;
+    for (int e = tid; e < BK * (nb / 2); e += 256) {
+      const int jj = e / (nb / 2), i2 = (e % (nb / 2)) * 2;
+      const int j = jc + jj < j1 ? jc + jj : j1 - 1;  // rows past j1 meet zero A columns
+      cp_async16(sb + (uint32_t)(jj * BST + i2) * 8u, Ek + (int64_t)j * R + i2);
+    }
+    cp_commit();
+  };
+
+  double acc[4][8][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+
+  issue(0, 0);
+  for (int it = 0; it < niter; ++it) {
+    const int buf = it & 1;
+    if (it + 1 < niter) {
+      issue(it + 1, buf ^ 1);
+      cp_wait_one();
+    } else {
+      cp_wait_all();
+    }
+    __syncthreads();
+    if (active) {
+      const double *A = smem + buf * STAGE_DOUBLES;
+      const double *B = A + BK * AST;
+#pragma unroll
+      for (int ks = 0; ks < BK / 4; ++ks) {
+        const int k = ks * 4 + (lane & 3);
+        double af[4], bf[8];
+#pragma unroll
+        for (int mf = 0; mf < 4; ++mf) af[mf] = A[k * AST + wm * 32 + mf * 8 + (lane >> 2)];
+#pragma unroll
+        for (int nf = 0; nf < 8; ++nf) bf[nf] = B[k * BST + wn * 64 + nf * 8 + (lane >> 2)];
+#pragma unroll
+        for (int mf = 0; mf < 4; ++mf)
+#pragma unroll
+          for (int nf = 0; nf < 8; ++nf) dmma(acc[mf][nf][0], acc[mf][nf][1], af[mf], bf[nf]);
+      }
+    }
+    __syncthreads();
+  }
+  if (!active) return;
+  // D fragment: row = lane >> 2, columns 2 (lane & 3) + {0, 1}
+#pragma unroll
+  for (int mf = 0; mf < 4; ++mf) {
+    const int t = wm * 32 + mf * 8 + (lane >> 2);
+    if (t >= nt) continue;
+    const int px = bxo + (t % bw), py = byo + ((t / bw) % bw), pz = bzo + (t / (bw * bw));
+    double *dst = Lout + ((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px) * R;
+#pragma unroll
+    for (int nf = 0; nf < 8; ++nf) {
+      const int i = wn * 64 + nf * 8 + 2 * (lane & 3);
+      if (i < ni) *reinterpret_cast<double2 *>(dst + i) = make_double2(acc[mf][nf][0], acc[mf][nf][1]);
+    }
+  }
+}
+
+}  // namespace dm
+
+// Writes Lout[cell][0:ni) for every cell of the level (assign); entries i >= ni untouched.
+int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
+                    const int4 *offs, cudaStream_t s) {
+  if (r != dm::R) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "FP64 tensor M2L is built for r = 256");
+  if (j0 < 0 || j1 > r || j0 >= j1 || ni < 2 || ni > r || ni % 2)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "bad contraction / output range");
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e =
+        cudaFuncSetAttribute(dm::m2l_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dm::SMEM_BYTES);
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma smem attribute", __FILE__, __LINE__);
+    attr = true;
+  }
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;
+  const int nbox = P / bw;
+  dm::m2l_dmma_kernel<<<8 * nbox * nbox * nbox, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma", __FILE__, __LINE__);
+}
+
+}  // namespace bbfmm

@@ -1,12 +1,15 @@
 // Mixed-precision M2L on tcgen05 tensor cores (sm_100a).
 //
-// For one level, the contraction components j >= lead of
+// For one level, everything outside the leading block (i < lead_rows, j < lead) of
 //   L_i(F) = sum_{v in IL(F)} sum_j E_v(i, j) M_j(F + v)
-// are computed as three-term split products: with x = x_hi + x_lo (bf16 each),
+// is computed as three-term split products: with x = x_hi + x_lo (bf16 each),
 //   E M ~= E_hi M_hi + E_hi M_lo + E_lo M_hi,
-// accumulated in FP32 in tensor memory over all 189 offsets. The components j < lead
-// (default 16), whose FP32 accumulation would dominate the error, are computed in FP64
-// by the CUDA-core kernel (m2l_simt.cu); the projection after M2L sums both parts.
+// accumulated in FP32 in tensor memory over all 189 offsets. The leading block (default
+// 32 outputs x 16 components), whose FP32 accumulation would dominate the error, is
+// computed in FP64 beforehand (m2l_dmma.cu) and this kernel adds its result to it: the
+// split operator copy holds zeros in that block, so the tensor cores skip nothing but
+// contribute nothing there. With lead_rows = r the whole j < lead strip is left out and
+// its K-steps are skipped.
 //
 // Tile: 128 targets of one sibling class forming an 8x4x4 box of its parent grid
 // (GEMM M = 128) x all 256 outputs i (N = 256) in a 128 x 256 FP32 TMEM accumulator.
@@ -16,7 +19,7 @@
 // zero-filled by TMA. The B operand chunk is rows i of E_v for the same 64 j.
 //
 // Warp roles (192 threads): warp 0 = TMA producer (and TMEM allocator), warp 1 = MMA
-// issuer, warps 2-5 = epilogue (tcgen05.ld of the accumulator, FP32 store of L).
+// issuer, warps 2-5 = epilogue (tcgen05.ld of the accumulator, FP64 update of L).
 // Two pipeline stages of 96 KB (A_hi, A_lo 16 KB each; B_hi, B_lo 32 KB each).
 // Every mbarrier wait is bounded; on timeout the kernel records an error code in a
 // device status word, skips the remaining work, frees its tensor memory and returns.
@@ -139,11 +142,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Grid: one CTA per tile (class c, 8x4x4 box). L32: the level's output, cpg layout [cell][256].
+// Grid: one CTA per tile (class c, 8x4x4 box). Lacc: the level's FP64 output, cpg layout
+// [cell][256]; entries i < ilead hold the FP64 leading block and are added to, the others
+// are overwritten.
 __global__ void __launch_bounds__(192, 1)
     m2l_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
-                  float *__restrict__ L32, int level, const int4 *__restrict__ offs, int lead) {
+                  double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -164,7 +169,6 @@ __global__ void __launch_bounds__(192, 1)
   const int tb = blockIdx.x % tiles_per_class;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int kfirst = lead / 16;  // K-steps of 16 skipped in chunk 0 (computed in FP64)
   const int nchunk = BN / BK;    // 4 K-chunks per offset (r = 256)
   const int chunk0 = kfirst / 4;  // whole chunks skipped
   const int kstep0 = kfirst % 4;  // K-steps skipped in the first used chunk
@@ -213,11 +217,10 @@ __global__ void __launch_bounds__(192, 1)
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
     uint32_t acc = 0;
-    bool ok = true;
     for (int it = 0; it < niter; ++it) {
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
-      if (!mbar_wait(full_bar(s), ph, 2)) { ok = false; break; }
+      if (!mbar_wait(full_bar(s), ph, 2)) break;
       tc_fence_after();
       const uint32_t st = base + s * STAGE_BYTES;
       const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
@@ -232,10 +235,9 @@ __global__ void __launch_bounds__(192, 1)
       }
       mma_commit(empty_bar(s));
     }
-    (void)ok;
-    mma_commit(acc_bar);
+    mma_commit(acc_bar);  // also after an early exit: the epilogue must not wait forever
   } else if (warp >= 2) {
-    // ---------------- epilogue: TMEM -> registers -> L32
+    // ---------------- epilogue: TMEM -> registers -> Lacc
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;
     const bool ok = mbar_wait(acc_bar, 0, 3);
@@ -244,13 +246,18 @@ __global__ void __launch_bounds__(192, 1)
       const int tx = row % BOX_X, ty = (row / BOX_X) % BOX_Y, tz = row / (BOX_X * BOX_Y);
       const int64_t P3 = (int64_t)P * P * P;
       const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
-      float *dst = L32 + cell * BN;
+      double *dst = Lacc + cell * BN;
       for (int col = 0; col < BN; col += 32) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
+        const bool add = col < ilead;  // ilead is a multiple of 32
 #pragma unroll
-        for (int i = 0; i < 32; i += 4)
-          *reinterpret_cast<float4 *>(dst + col + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        for (int i = 0; i < 32; i += 2) {
+          double2 o = add ? *reinterpret_cast<const double2 *>(dst + col + i) : make_double2(0.0, 0.0);
+          o.x += (double)v[i];
+          o.y += (double)v[i + 1];
+          *reinterpret_cast<double2 *>(dst + col + i) = o;
+        }
       }
     }
   }
@@ -263,10 +270,16 @@ __global__ void __launch_bounds__(192, 1)
 }
 
 // ---------------------------------------------------------------- splitting
+// hi/lo bf16 split of src; for operators (r > 0) entries with i < zrows and j < zcols of
+// each row-major r x r block are zeroed (the FP64 leading block).
 __global__ void split_kernel(int64_t count, const double *__restrict__ src, __nv_bfloat16 *__restrict__ hi,
-                             __nv_bfloat16 *__restrict__ lo) {
+                             __nv_bfloat16 *__restrict__ lo, int r, int zrows, int zcols) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
-    const double x = src[e];
+    double x = src[e];
+    if (r > 0) {
+      const int j = (int)(e % r), i = (int)((e / r) % r);
+      if (i < zrows && j < zcols) x = 0.0;
+    }
     const __nv_bfloat16 h = __double2bfloat16(x);
     hi[e] = h;
     lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
@@ -293,7 +306,7 @@ static PFN_encodeTiled encode_fn() {
 }
 
 struct TcOps {
-  int r = 0;
+  int r = 0, lead = 0, lead_rows = 0;
   __nv_bfloat16 *Ehi = nullptr, *Elo = nullptr;
   CUtensorMap mapBhi, mapBlo;
 };
@@ -319,19 +332,24 @@ static int make_map(CUtensorMap *m, void *ptr, int rank, const cuuint64_t *dims,
   return BBFMM_OK;
 }
 
-int tc_prepare_operators(int r, const double *Ert, int lead, void **out, cudaStream_t s) {
+int tc_prepare_operators(int r, const double *Ert, int lead, int lead_rows, void **out, cudaStream_t s) {
   *out = nullptr;
   if (r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L is built for r = 256 (n = 8)");
   if (lead < 0 || lead > 64 || lead % 16) return bbfmm_set_error(BBFMM_ERR_ARG, "lead must be 0, 16, 32, 48 or 64");
+  if (lead_rows < 32 || lead_rows > r || lead_rows % 32)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "lead_rows must be a multiple of 32 in [32, 256]");
   if (!encode_fn()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   TcOps *ops = new TcOps();
   ops->r = r;
+  ops->lead = lead;
+  ops->lead_rows = lead_rows;
   const size_t cnt = (size_t)BBFMM_NUM_OFFSETS * r * r;
   if (cudaMalloc(&ops->Ehi, cnt * 2) != cudaSuccess || cudaMalloc(&ops->Elo, cnt * 2) != cudaSuccess) {
     tc_free_operators(ops);
     return bbfmm_set_error(BBFMM_ERR_NOMEM, "operator split allocation failed");
   }
-  tc::split_kernel<<<148 * 8, 256, 0, s>>>((int64_t)cnt, Ert, ops->Ehi, ops->Elo);
+  tc::split_kernel<<<148 * 8, 256, 0, s>>>((int64_t)cnt, Ert, ops->Ehi, ops->Elo, r, lead_rows < r ? lead_rows : 0,
+                                           lead);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     tc_free_operators(ops);
@@ -365,12 +383,12 @@ int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *M
   (void)lead;
   __nv_bfloat16 *hi = (__nv_bfloat16 *)Msplit;
   __nv_bfloat16 *lo = hi + (size_t)ncell * r;
-  tc::split_kernel<<<148 * 8, 256, 0, s>>>(ncell * r, M, hi, lo);
+  tc::split_kernel<<<148 * 8, 256, 0, s>>>(ncell * r, M, hi, lo, 0, 0, 0);
   return bbfmm_set_cuda_error(cudaGetLastError(), "split multipoles", __FILE__, __LINE__);
 }
 
-int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, float *L32,
-                  int level, const int4 *offs, int lead, cudaStream_t s) {
+int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
+                  int level, const int4 *offs, cudaStream_t s) {
   const TcOps *ops = (const TcOps *)opsv;
   if (!ops || r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L needs r = 256 operators");
   const int P = 1 << (level - 1);
@@ -392,8 +410,11 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     attr = true;
   }
   const int tiles = 8 * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
-  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo, L32, level, offs,
-                                                       lead);
+  // with a full-width leading strip its K-steps are skipped; otherwise every K-step runs
+  const int kfirst = ops->lead_rows >= r ? ops->lead / 16 : 0;
+  const int ilead = ops->lead > 0 ? ops->lead_rows : 0;
+  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo, Lacc, level, offs,
+                                                       kfirst, ilead);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc", __FILE__, __LINE__);
 }
 

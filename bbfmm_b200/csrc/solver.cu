@@ -69,7 +69,7 @@ Tables Solver<T>::tables() const {
 }
 
 template <typename T>
-int Solver<T>::init(int n_, int maxlev_, double L_, int mode_, int lead_, int device_, cudaStream_t s) {
+int Solver<T>::init(int n_, int maxlev_, double L_, int mode_, int lead_, int lead_rows_, int device_, cudaStream_t s) {
   if (n_ != 4 && n_ != 8) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   if (maxlev_ < BBFMM_MINLEV || maxlev_ > 10) return bbfmm_set_error(BBFMM_ERR_ARG, "maxlev must be in [2, 10]");
   if (!(L_ > 0)) return bbfmm_set_error(BBFMM_ERR_ARG, "root length L must be positive");
@@ -77,8 +77,11 @@ int Solver<T>::init(int n_, int maxlev_, double L_, int mode_, int lead_, int de
   if ((mode_ == MODE_S) != (sizeof(T) == 4)) return bbfmm_set_error(BBFMM_ERR_ARG, "precision mode / type mismatch");
   n = n_; n3 = n * n * n; r = n3 / 2; maxlev = maxlev_; L = L_; mode = mode_; device = device_;
   lead = (mode == MODE_MIXED) ? lead_ : 0;
-  if (mode == MODE_MIXED && (lead < 0 || lead > r || lead % 16 != 0))
-    return bbfmm_set_error(BBFMM_ERR_ARG, "lead must be a multiple of 16 in [0, r]");
+  lead_rows = lead_rows_ > 0 ? lead_rows_ : r;
+  if (mode == MODE_MIXED && (lead < 0 || lead > 64 || lead % 16 != 0))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "lead must be 0, 16, 32, 48 or 64");
+  if (mode == MODE_MIXED && (lead_rows < 32 || lead_rows > r || lead_rows % 32 != 0))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "lead_rows must be a multiple of 32 in [32, r]");
   BBFMM_CUDA_OK(cudaSetDevice(device));
   if (s) {
     stream = s;
@@ -123,17 +126,19 @@ int Solver<T>::set_operators(const T *U, const T *E) {
     }
   if (!Ert) {
     TRY(dalloc(&Ert, ert.size()));
+    TRY(dalloc(&Ecol, ert.size()));
     TRY(dalloc(&Bup, bup.size()));
     TRY(dalloc(&Bdn, bdn.size()));
   }
   BBFMM_CUDA_OK(cudaMemcpy(Ert, ert.data(), sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaMemcpy(Ecol, E, sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(Bup, bup.data(), sizeof(T) * bup.size(), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(Bdn, bdn.data(), sizeof(T) * bdn.size(), cudaMemcpyHostToDevice));
   if (mode == MODE_MIXED) {
     if (!tc_supported()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "mixed mode needs an sm_100 GPU");
     if (tcops) tc_free_operators(tcops);
     tcops = nullptr;
-    TRY(tc_prepare_operators(r, (const double *)Ert, lead, &tcops, stream));
+    TRY(tc_prepare_operators(r, (const double *)Ert, lead, lead_rows, &tcops, stream));
     BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
   }
   return BBFMM_OK;
@@ -162,8 +167,6 @@ int Solver<T>::alloc_work() {
   if (Lbuf) cudaFree(Lbuf);
   TRY(dalloc(&Lbuf, (size_t)nl * r));
   if (mode == MODE_MIXED) {
-    if (L32) cudaFree(L32);
-    TRY(dalloc(&L32, (size_t)nl * r));
     if (Msplit) cudaFree(Msplit);
     unsigned char *p = nullptr;
     TRY(dalloc(&p, tc_split_bytes(r, tot / r)));
@@ -234,14 +237,12 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
   T *Sl = S[maxlev & 1];
   TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream));
   mark(ST_P2M);
-  TRY(launch_proj<T>(pow8i(maxlev), n3, r, Sl, nullptr, Bup, nullptr, (T)1, Mall + Moff[maxlev], maxlev,
-                     MAP_OUT_CPG, stream));
+  TRY(proj(pow8i(maxlev), n3, r, Sl, Bup, nullptr, (T)1, Mall + Moff[maxlev], maxlev, MAP_OUT_CPG));
   mark(ST_PROJ_UP);
   for (int l = maxlev - 1; l >= BBFMM_MINLEV; --l) {
     TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream));
     mark(ST_M2M);
-    TRY(launch_proj<T>(pow8i(l), n3, r, S[l & 1], nullptr, Bup, nullptr, (T)1, Mall + Moff[l], l, MAP_OUT_CPG,
-                       stream));
+    TRY(proj(pow8i(l), n3, r, S[l & 1], Bup, nullptr, (T)1, Mall + Moff[l], l, MAP_OUT_CPG));
     mark(ST_PROJ_UP);
   }
   if (mode == MODE_MIXED) {
@@ -251,6 +252,27 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
   return BBFMM_OK;
 }
 
+// FP64 with r = 256 runs on the FP64 tensor path (DMMA); FP32 and r = 32 on CUDA cores.
+template <typename T>
+int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
+  if (sizeof(T) == 8 && r == 256)
+    return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
+                           stream);
+  if (ni != r) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
+  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream);
+}
+
+template <typename T>
+int Solver<T>::proj(int64_t Mrows, int K, int Ncols, const T *A, const T *B, const T *cs, T scale, T *C, int level,
+                    int mapmode) {
+  if (sizeof(T) == 8) {
+    int rc = launch_proj_dmma(Mrows, K, Ncols, (const double *)A, (const double *)B, (const double *)cs,
+                              (double)scale, (double *)C, level, mapmode, stream);
+    if (rc != BBFMM_ERR_UNSUPPORTED) return rc;
+  }
+  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream);
+}
+
 template <typename T>
 int Solver<T>::interaction(int lo, int hi) {
   const Tables tb = tables();
@@ -258,18 +280,22 @@ int Solver<T>::interaction(int lo, int hi) {
     const T *Ml = Mall + Moff[l];
     const bool split = mode == MODE_MIXED && l >= TC_MIN_LEVEL;
     if (split) {
-      // leading components in FP64 on CUDA cores, the rest as split bf16 on tensor cores
-      if (lead > 0) TRY(launch_m2l_simt<T>(r, Ml, Ert, Lbuf, l, 0, lead, offs, 0, stream));
-      else BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * pow8i(l) * r, stream));
-      TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, L32, l, offs, lead, stream));
-      mark(ST_M2L, 2);
+      // FP64 leading block (i < lead_rows, j < lead) on the FP64 tensor path, then the
+      // split-bf16 tensor-core kernel adds everything else into the same FP64 output
+      if (lead > 0) {
+        TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
+        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream));
+        mark(ST_M2L, 2);
+      } else {
+        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream));
+        mark(ST_M2L, 1);
+      }
     } else {
-      TRY(launch_m2l_simt<T>(r, Ml, Ert, Lbuf, l, 0, r, offs, 0, stream));
+      TRY(m2l_fp(Ml, l, 0, r, r));
       mark(ST_M2L);
     }
     const T scale = (T)1 / cell_length<T>(l, (T)L);
-    TRY(launch_proj<T>(pow8i(l), r, n3, Lbuf, split ? L32 : nullptr, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG,
-                       stream));
+    TRY(proj(pow8i(l), r, n3, Lbuf, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG));
     mark(ST_PROJ_DOWN);
     if (l > BBFMM_MINLEV) {
       TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream));
@@ -332,12 +358,12 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   for (int part = 0; part < (mode == MODE_MIXED ? 2 : 1) && rc == BBFMM_OK; ++part) {
     cudaEventRecord(a, stream);
     for (int i = 0; i < reps && rc == BBFMM_OK; ++i) {
-      if (mode != MODE_MIXED) rc = launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, 0, r, offs, 0, stream);
+      if (mode != MODE_MIXED) rc = m2l_fp(Ml, level, 0, r, r);
       else if (part == 0) rc = level >= TC_MIN_LEVEL
-                                   ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, L32, level, offs,
-                                                   lead, stream)
-                                   : launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, 0, r, offs, 0, stream);
-      else rc = lead > 0 ? launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, 0, lead, offs, 0, stream) : BBFMM_OK;
+                                   ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf,
+                                                   level, offs, stream)
+                                   : m2l_fp(Ml, level, 0, r, r);
+      else rc = lead > 0 ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
     }
     cudaEventRecord(b, stream);
     cudaEventSynchronize(b);
@@ -367,8 +393,8 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 
 template <typename T>
 void Solver<T>::release() {
-  void *ptrs[] = {tkz, cw, kw, Ert, Bup, Bdn, kwcol, offs, perm, leaf_start, leafm, pos4, loc4,
-                  S[0], S[1], F[0], F[1], Mall, Lbuf, L32, Msplit, phis};
+  void *ptrs[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, offs, perm, leaf_start, leafm, pos4, loc4,
+                  S[0], S[1], F[0], F[1], Mall, Lbuf, Msplit, phis};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (tcops) tc_free_operators(tcops);
@@ -407,7 +433,7 @@ int bbfmm_b200_create(const bbfmm_b200_config *cfg, const void *U, const void *E
   int rc = BBFMM_OK;
   if (cfg->mode == BBFMM_B200_MODE_S) {
     h->f = new Solver<float>();
-    rc = h->f->init(n, cfg->maxlev, cfg->L, cfg->mode, cfg->lead, cfg->device, (cudaStream_t)cfg->stream);
+    rc = h->f->init(n, cfg->maxlev, cfg->L, cfg->mode, cfg->lead, cfg->lead_rows, cfg->device, (cudaStream_t)cfg->stream);
     if (rc == BBFMM_OK) {
       std::vector<float> tkz(n * n), kw(n3), cw(2 * n * n);
       std::vector<int> kt(343);
@@ -420,7 +446,7 @@ int bbfmm_b200_create(const bbfmm_b200_config *cfg, const void *U, const void *E
     }
   } else {
     h->d = new Solver<double>();
-    rc = h->d->init(n, cfg->maxlev, cfg->L, cfg->mode, cfg->lead, cfg->device, (cudaStream_t)cfg->stream);
+    rc = h->d->init(n, cfg->maxlev, cfg->L, cfg->mode, cfg->lead, cfg->lead_rows, cfg->device, (cudaStream_t)cfg->stream);
     if (rc == BBFMM_OK) {
       std::vector<double> tkz(n * n), kw(n3), cw(2 * n * n);
       std::vector<int> kt(343);

@@ -34,6 +34,10 @@ int launch_make_local(int N, const double *pos4, const int *leafm, int maxlev, d
 int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s);
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s);
 void build_offset_table(int *out);
+int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
+                    const int4 *offs, cudaStream_t s);
+int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
+                     double *C, int level, int mapmode, cudaStream_t s);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
 
 template <typename T> int bbfmm_weights_t(int n, T *Tkz, int *Ktable, T *Kweights, T *Cweights);
@@ -41,24 +45,25 @@ template <typename T> int bbfmm_weights_t(int n, T *Tkz, int *Ktable, T *Kweight
 // Mixed-precision tensor-core M2L (m2l_tc.cu).
 struct TcOperators;
 int tc_supported();
-int tc_prepare_operators(int r, const double *Ert, int lead, void **out, cudaStream_t s);
+int tc_prepare_operators(int r, const double *Ert, int lead, int lead_rows, void **out, cudaStream_t s);
 void tc_free_operators(void *ops);
 int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s);
 size_t tc_split_bytes(int r, int64_t ncell);
-int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, float *L32,
-                  int level, const int4 *offs, int lead, cudaStream_t s);
+int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
+                  int level, const int4 *offs, cudaStream_t s);
 int tc_status(int clear);
 constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
 
 template <typename T>
 struct Solver {
-  int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, device = 0;
+  int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, lead_rows = 32, device = 0;
   double L = 1.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   // tables and operators (device)
   T *tkz = nullptr, *cw = nullptr, *kw = nullptr;
   T *Ert = nullptr;  // [316][r][r] row-major
+  T *Ecol = nullptr; // [316][r][r] column-major (the reference's K-file layout)
   T *Bup = nullptr;  // [n3][r]  Kweights[l] U(l, i)
   T *Bdn = nullptr;  // [r][n3]  U(l, j)
   T *kwcol = nullptr;
@@ -75,7 +80,6 @@ struct Solver {
   T *Mall = nullptr;
   std::vector<int64_t> Moff;  // offset (elements) of level l in Mall, cpg layout
   T *Lbuf = nullptr;
-  float *L32 = nullptr;
   void *Msplit = nullptr;
   T *phis = nullptr;
   // timing
@@ -86,7 +90,7 @@ struct Solver {
 
   Tables tables() const;
   int64_t Mcells() const { return (Moff[maxlev] + pow8i(maxlev) * r) / r; }
-  int init(int n_, int maxlev_, double L_, int mode_, int lead_, int device_, cudaStream_t s);
+  int init(int n_, int maxlev_, double L_, int mode_, int lead_, int lead_rows_, int device_, cudaStream_t s);
   int set_tables(const T *Tkz, const T *Cweights, const T *Kweights);  // host arrays
   int set_operators(const T *U, const T *E);                              // host, reference layout
   int set_particles_sorted(int N_, const int *perm_host, const int *leaf_start_host, const T *xyz_host);
@@ -98,6 +102,8 @@ struct Solver {
   int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order
   void mark(int stage, int launches = 1);
   int time_m2l(int level, int reps, float *ms);
+  int m2l_fp(const T *Ml, int level, int j0, int j1, int ni);  // FP64 (DMMA) / FP32 (SIMT) M2L part
+  int proj(int64_t M, int K, int N, const T *A, const T *B, const T *cs, T scale, T *C, int level, int mapmode);
   void release();
 };
 

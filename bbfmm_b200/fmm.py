@@ -37,16 +37,17 @@ class Solver:
     """Device-resident FMM for one particle set.
 
     mode: "d" (FP64 everywhere), "s" (FP32 everywhere), "mixed" (FP64 passes,
-    split-precision tensor-core M2L with ``lead`` FP64 leading components, FP32
-    compensated P2P)."""
+    split-precision tensor-core M2L whose leading operator block -- outputs i < ``lead_rows``,
+    components j < ``lead`` -- runs in FP64, FP32 compensated P2P)."""
 
     def __init__(self, n: int, maxlev: int, L: float = 1.0, mode: str = "d", lead: int = 16,
-                 device: int = 0, operators=None, stream=None):
+                 lead_rows: int = 32, device: int = 0, operators=None, stream=None):
         import torch
         self.torch = torch
         self.n, self.maxlev, self.L, self.mode = n, maxlev, float(L), mode
         self.r = n ** 3 // 2
         self.lead = lead if mode == "mixed" else 0
+        self.lead_rows = lead_rows if mode == "mixed" else 0
         self.device = device
         self.dtype = torch.float32 if mode == "s" else torch.float64
         self.np_dtype = np.float32 if mode == "s" else np.float64
@@ -58,7 +59,7 @@ class Solver:
         E = np.ascontiguousarray(E)
         fp32 = int(U.dtype == np.float32)
         assert E.dtype == U.dtype
-        cfg = _lib.Config(n=n, maxlev=maxlev, L=self.L, mode=_lib.MODES[mode], lead=self.lead,
+        cfg = _lib.Config(n=n, maxlev=maxlev, L=self.L, mode=_lib.MODES[mode], lead=self.lead, lead_rows=self.lead_rows,
                           device=device, stream=C.c_void_p(stream) if stream else None)
         h = C.c_void_p()
         _lib.check(_lib.lib().bbfmm_b200_create(C.byref(cfg), _ptr(U), _ptr(E), fp32, C.byref(h)))

@@ -50,9 +50,10 @@ extern "C" {
 /* Precision modes.
  *  D      FP64 storage and arithmetic in every stage (the reference's double build).
  *  S      FP32 storage and arithmetic in every stage (the reference's SINGLE build).
- *  MIXED  FP64 passes; M2L with the first `lead` contraction components in FP64 and the
- *         rest as three-term split BF16 products on tcgen05 tensor cores accumulated in
- *         FP32; P2P in FP32 on leaf-local coordinates with compensated sums. */
+ *  MIXED  FP64 passes; M2L with the leading block of every operator (outputs i < lead_rows,
+ *         contraction components j < lead) in FP64 and everything else as three-term split
+ *         BF16 products on tcgen05 tensor cores accumulated in FP32; P2P in FP32 on
+ *         leaf-local coordinates with compensated sums. */
 #define BBFMM_B200_MODE_D 0
 #define BBFMM_B200_MODE_S 1
 #define BBFMM_B200_MODE_MIXED 2
@@ -62,7 +63,8 @@ typedef struct {
   int maxlev;   /* level of the leaves, >= 2 (the reference's maxlev) */
   double L;     /* edge of the root cube */
   int mode;     /* BBFMM_B200_MODE_* */
-  int lead;     /* MIXED: leading contraction components kept in FP64 (multiple of 16) */
+  int lead;     /* MIXED: leading contraction components j kept in FP64 (0, 16, 32, 48, 64) */
+  int lead_rows;/* MIXED: ... for the outputs i < lead_rows only (multiple of 32; 0 = all r) */
   int device;   /* CUDA device ordinal */
   void *stream; /* cudaStream_t to run on, or NULL for a private stream */
 } bbfmm_b200_config;
