@@ -150,3 +150,60 @@ int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s
 }
 
 }  // namespace bbfmm
+
+// ====================================================== near-field C-ABI entry points
+#include "../../include/bbfmm_b200.h"
+
+namespace {
+
+// Shared body of the two entry points: given device scratch for the per-particle leaf
+// index (N ints) and, in the FP32 mode, the leaf-local coordinates (N float4), runs the
+// near field on `stream`.
+int near_field_run(int N, int maxlev, double L, const double *xyzq, const int *leaf_start, double *phi, int mode,
+                   cudaStream_t st, int *leafm, float4 *loc4) {
+  int rc = bbfmm::launch_leaf_of(maxlev, leaf_start, leafm, st);
+  if (rc != BBFMM_OK) return rc;
+  if (mode == BBFMM_B200_MODE_MIXED) {
+    rc = bbfmm::launch_make_local(N, xyzq, leafm, maxlev, L, loc4, st);
+    if (rc == BBFMM_OK) rc = bbfmm::launch_p2p_local(N, loc4, leaf_start, leafm, maxlev, L, phi, st);
+    return rc;
+  }
+  return bbfmm::launch_p2p<double>(N, xyzq, leaf_start, leafm, maxlev, phi, st);
+}
+
+int near_field_check(int N, int maxlev, double L, const void *xyzq, const void *leaf_start, const void *phi,
+                     int mode) {
+  if (N < 0 || maxlev < BBFMM_MINLEV || maxlev > 10 || !(L > 0))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "near field: need N >= 0, 2 <= maxlev <= 10, L > 0");
+  if (N > 0 && (!xyzq || !leaf_start || !phi)) return bbfmm_set_error(BBFMM_ERR_ARG, "near field: null pointer");
+  if (mode != BBFMM_B200_MODE_D && mode != BBFMM_B200_MODE_MIXED)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "near field: mode must be BBFMM_B200_MODE_D or BBFMM_B200_MODE_MIXED");
+  return BBFMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bbfmm_b200_near_field(int N, int maxlev, double L, const double *xyzq, const int *leaf_start, double *phi,
+                          int mode, void *stream) {
+  int rc = near_field_check(N, maxlev, L, xyzq, leaf_start, phi, mode);
+  if (rc != BBFMM_OK || N == 0) return rc;
+  const cudaStream_t st = (cudaStream_t)stream;
+  int *leafm = nullptr;
+  float4 *loc4 = nullptr;
+  cudaError_t e = cudaMalloc((void **)&leafm, sizeof(int) * (size_t)N);
+  if (e == cudaSuccess && mode == BBFMM_B200_MODE_MIXED) e = cudaMalloc((void **)&loc4, sizeof(float4) * (size_t)N);
+  if (e != cudaSuccess) {
+    if (leafm) cudaFree(leafm);
+    return bbfmm_set_error(BBFMM_ERR_NOMEM, "near field: scratch allocation failed");
+  }
+  rc = near_field_run(N, maxlev, L, xyzq, leaf_start, phi, mode, st, leafm, loc4);
+  e = cudaStreamSynchronize(st);  // the scratch is freed below
+  if (rc == BBFMM_OK) rc = bbfmm_set_cuda_error(e, "near field", __FILE__, __LINE__);
+  cudaFree(leafm);
+  if (loc4) cudaFree(loc4);
+  return rc;
+}
+
+}  // extern "C"

@@ -141,6 +141,18 @@ BBFMM_B200_API int bbfmm_b200_direct(int N, const double *xyz_dev, const double 
  * remaining work and returned). Synchronises the device; clear != 0 resets the word. */
 BBFMM_B200_API int bbfmm_b200_device_status(int clear);
 
+/* Near-field (P2P) part of the solve on caller-owned device arrays, the work of
+ * anotherNearField (anotherNearField.c:219-346) and of the reference GPU kernel `direct`
+ * (direct.cu:69-209): phi[k] += q_k sum_{B in N(A)} sum_{j in B, r != 0} q_j / r_kj over the
+ * <= 27 neighbour leaves. xyzq is N x 4 (x, y, z, q) FP64 sorted by leaf in Morton order
+ * (as bbfmm_b200_sort_particles orders them), leaf_start holds the 8^maxlev + 1 leaf
+ * offsets, phi is added to; all three are device pointers. mode BBFMM_B200_MODE_D computes
+ * in FP64 like the reference; BBFMM_B200_MODE_MIXED in FP32 on leaf-local coordinates with
+ * compensated sums. Allocates N * (4 + 16) bytes of device scratch for the call, runs on
+ * `stream` (cudaStream_t, may be NULL) and synchronises it before freeing the scratch. */
+BBFMM_B200_API int bbfmm_b200_near_field(int N, int maxlev, double L, const double *xyzq, const int *leaf_start,
+                                         double *phi, int mode, void *stream);
+
 BBFMM_B200_API void *bbfmm_b200_stream(bbfmm_b200_solver *s);
 BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
 

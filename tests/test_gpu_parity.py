@@ -107,3 +107,33 @@ def test_host_entry_matches_device_entry():
     b = s.solve_host(q)
     assert np.array_equal(a, b)
     s.close()
+
+
+@pytest.mark.parametrize("mode,tol", [(0, 1e-13), (2, 1e-6)])
+def test_near_field_entry_matches_oracle(oracle_d, mode, tol):
+    """bbfmm_b200_near_field on caller-owned device arrays vs the oracle's P2P
+    (anotherNearField semantics). FP64 mode: 1e-13; FP32 leaf-local mode: 1e-6."""
+    import ctypes as C
+    import torch
+    from bbfmm_b200 import _lib
+    N, lev = 50000, 4
+    x, q = uniform_inputs(N, seed=31)
+    tree = oracle_d.build_tree(x, lev)
+    want = oracle_d.nearfield(tree, x, q, np.zeros(N))
+    perm = np.zeros(N, dtype=np.int32)
+    ls = np.zeros(8 ** lev + 1, dtype=np.int32)
+    xc = np.ascontiguousarray(x)
+    _lib.check(_lib.lib().bbfmm_b200_sort_particles(N, 0, C.c_void_p(xc.ctypes.data), 1.0, lev,
+                                                    perm.ctypes.data_as(C.POINTER(C.c_int)),
+                                                    ls.ctypes.data_as(C.POINTER(C.c_int))))
+    assert np.array_equal(perm, tree.fieldlist)          # same leaf order as the reference
+    xyzq = np.concatenate([x[perm], q[perm, None]], axis=1)
+    dx = torch.as_tensor(xyzq, device="cuda")
+    dl = torch.as_tensor(ls, device="cuda")
+    phi = torch.zeros(N, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().bbfmm_b200_near_field(N, lev, 1.0, C.c_void_p(dx.data_ptr()), C.c_void_p(dl.data_ptr()),
+                                                C.c_void_p(phi.data_ptr()), mode, None))
+    got = np.empty(N)
+    got[perm] = phi.cpu().numpy()
+    assert rel_l2(got, want) < tol
