@@ -51,6 +51,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_direct.argtypes = [i, vp, vp, i, vp, vp, vp]
         L.bbfmm_b200_device_status.argtypes = [i]
         L.bbfmm_b200_near_field.argtypes = [i, i, d, vp, vp, vp, i, vp]
+        L.bbfmm_b200_near_field_noalloc.argtypes = [i, i, d, vp, vp, vp, i, vp]
         L.bbfmm_b200_stream.argtypes = [vp]
         L.bbfmm_b200_stream.restype = vp
         L.bbfmm_b200_destroy.argtypes = [vp]

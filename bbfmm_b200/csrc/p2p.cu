@@ -152,6 +152,8 @@ int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s
 }  // namespace bbfmm
 
 // ====================================================== near-field C-ABI entry points
+#include <mutex>
+
 #include "../../include/bbfmm_b200.h"
 
 namespace {
@@ -181,6 +183,37 @@ int near_field_check(int N, int maxlev, double L, const void *xyzq, const void *
   return BBFMM_OK;
 }
 
+// Scratch of the allocation-free entry point: room for BBFMM_B200_NOALLOC_MAX_PARTICLES
+// particles (one float4 of leaf-local coordinates and one int leaf index each). Every GPU
+// that loads the library holds this array until the process exits.
+constexpr size_t kNoallocLoc4Bytes = (size_t)BBFMM_B200_NOALLOC_MAX_PARTICLES * sizeof(float4);
+constexpr size_t kNoallocBytes = kNoallocLoc4Bytes + (size_t)BBFMM_B200_NOALLOC_MAX_PARTICLES * sizeof(int);
+static __device__ __align__(256) unsigned char g_near_field_scratch[kNoallocBytes];
+
+// Device addresses of the array, one per device, looked up once with that device current
+// (the array's name in host code is only a stand-in and must never reach a kernel).
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void *g_scratch_ptr[kMaxDevices] = {};
+
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "cudaGetDevice", __FILE__, __LINE__);
+  if (dev < 0 || dev >= kMaxDevices) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "device ordinal above 63");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_near_field_scratch);
+    if (e != cudaSuccess || !p)
+      return bbfmm_set_cuda_error(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(scratch)",
+                                  __FILE__, __LINE__);
+    g_scratch_ptr[dev] = p;
+  }
+  *out = g_scratch_ptr[dev];
+  return BBFMM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -204,6 +237,23 @@ int bbfmm_b200_near_field(int N, int maxlev, double L, const double *xyzq, const
   cudaFree(leafm);
   if (loc4) cudaFree(loc4);
   return rc;
+}
+
+int bbfmm_b200_near_field_noalloc(int N, int maxlev, double L, const double *xyzq, const int *leaf_start,
+                                  double *phi, int mode, void *stream) {
+  int rc = near_field_check(N, maxlev, L, xyzq, leaf_start, phi, mode);
+  if (rc != BBFMM_OK || N == 0) return rc;
+  if (N > BBFMM_B200_NOALLOC_MAX_PARTICLES)
+    return bbfmm_set_error(BBFMM_ERR_ARG,
+                           "near field (no allocation): N exceeds BBFMM_B200_NOALLOC_MAX_PARTICLES = 262144");
+  void *base = nullptr;
+  rc = noalloc_scratch(&base);
+  if (rc != BBFMM_OK) return rc;
+  // Both scratch arrays are written in full by this call before they are read, so the
+  // previous call's contents need no clearing.
+  float4 *loc4 = reinterpret_cast<float4 *>(base);
+  int *leafm = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(base) + kNoallocLoc4Bytes);
+  return near_field_run(N, maxlev, L, xyzq, leaf_start, phi, mode, (cudaStream_t)stream, leafm, loc4);
 }
 
 }  // extern "C"

@@ -153,6 +153,23 @@ BBFMM_B200_API int bbfmm_b200_device_status(int clear);
 BBFMM_B200_API int bbfmm_b200_near_field(int N, int maxlev, double L, const double *xyzq, const int *leaf_start,
                                          double *phi, int mode, void *stream);
 
+/* The same near field without any device allocation. This entry point has no counterpart
+ * in the reference. It is for callers that must not call cudaMalloc: code whose device
+ * memory is handed out by another framework's allocator (which may hold all of it), and
+ * time-critical loops that cannot afford the device-wide synchronisation cudaMalloc and
+ * cudaFree imply. Inputs and output are the caller's, as above; the per-particle scratch
+ * lives in one fixed array of device memory inside the library, sized for
+ * BBFMM_B200_NOALLOC_MAX_PARTICLES particles (5 MiB), which every GPU that loads the library
+ * keeps until the process exits. Larger N is rejected with BBFMM_B200_ERR_ARG.
+ * The first call on a device looks up that array's device address (with the device
+ * current), so make the first call on each device before any stream capture. All calls
+ * share the array: calls that overlap on the GPU (other streams, other host threads) race
+ * on it, so order them. Each call rewrites the scratch before reading it. Runs on `stream`
+ * and returns without synchronising. */
+#define BBFMM_B200_NOALLOC_MAX_PARTICLES 262144
+BBFMM_B200_API int bbfmm_b200_near_field_noalloc(int N, int maxlev, double L, const double *xyzq,
+                                                 const int *leaf_start, double *phi, int mode, void *stream);
+
 BBFMM_B200_API void *bbfmm_b200_stream(bbfmm_b200_solver *s);
 BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
 
