@@ -13,6 +13,12 @@ os.environ.setdefault("BBFMM_B200_OPERATOR_DIR", os.path.join(ROOT, "tests", ".o
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200 / sm_100a)")
     config.addinivalue_line("markers", "slow: long CPU test")
+    # build outputs are not versioned: build what a fresh checkout lacks
+    import subprocess
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_build", "liboracle_d.so")):
+        subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_oracle.sh")], check=True)
+    if not os.path.exists(os.path.join(ROOT, "bbfmm_b200", "lib", "libbbfmm_b200.so")):
+        subprocess.run([sys.executable, "-m", "bbfmm_b200.build"], check=True, cwd=ROOT)
 
 
 @pytest.fixture(scope="session")

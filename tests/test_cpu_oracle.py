@@ -1,0 +1,90 @@
+"""CPU oracle against the reference's golden fixtures (tests/golden, made by
+tests/golden/make_golden.py from the reference's own code).
+
+Bitwise: Chebyshev tables, the reference's particle generator, tree and lists.
+Known answers: relL2 of the FMM against the direct sum with the reference's own U files
+(operators E = U^T K U rebuilt here in FP64, so agreement is to ~1e-10 relative in d).
+"""
+import hashlib
+import json
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from oracle.oracle import rel_l2
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+G = json.load(open(os.path.join(GOLD, "golden.json")))
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _hexarr(v, dt):
+    return np.array([float.fromhex(x) for x in v]).astype(dt)
+
+
+def ref_operators(n, prec):
+    """U from the reference's own SVD file; E = U^T K_k U in FP64 (bbfmm.c:1384-1405)."""
+    from bbfmm_b200 import operators as ops
+    dt = np.float64 if prec == "d" else np.float32
+    raw = open(os.path.join(GOLD, f"refU{n}_{prec}.bin"), "rb").read()
+    r = struct.unpack("i", raw[:4])[0]
+    Ucol = np.frombuffer(raw[4:], dtype=dt).astype(np.float64)
+    n3 = n ** 3
+    U = Ucol.reshape(r, n3).T
+    K0 = ops.kernel_matrix(n)
+    E = np.stack([U.T @ K0[:, k * n3:(k + 1) * n3] @ U for k in range(316)])
+    Ecol = np.ascontiguousarray(E.transpose(0, 2, 1)).reshape(-1)
+    return Ucol.astype(dt), Ecol.astype(dt)
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+@pytest.mark.parametrize("n", [4, 8])
+def test_weights_bitwise(prec, n, oracle_d, oracle_s):
+    o = oracle_d if prec == "d" else oracle_s
+    Tkz, Kt, Kw, Cw = o.weights(n)
+    g = G[f"weights_{prec}_n{n}"]
+    assert np.array_equal(Tkz, _hexarr(g["Tkz"], o.dt))
+    assert np.array_equal(Kt, np.array(g["Ktable"]))
+    assert np.array_equal(Kw, _hexarr(g["Kweights"], o.dt))
+    assert np.array_equal(Cw, _hexarr(g["Cweights"], o.dt))
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+def test_reference_generator_and_tree_bitwise(prec, oracle_d, oracle_s):
+    o = oracle_d if prec == "d" else oracle_s
+    xyz, q = o.ref_sources(32768)
+    g = G[f"sources_{prec}_N32768"]
+    assert _digest(xyz) == g["xyz"] and _digest(q) == g["q"]
+    for lev in (3, 4):
+        t = o.build_tree(xyz, lev)
+        want = G[f"tree_{prec}_N32768_l{lev}"]
+        for k, v in want.items():
+            assert _digest(getattr(t, k)) == v, (lev, k)
+
+
+def test_direct_fp64_matches_reference_direct(oracle_d):
+    xyz, q = oracle_d.ref_sources(32768)
+    got = oracle_d.direct_fp64(xyz, q, np.arange(64))
+    want = _hexarr(G["direct_d_N32768_first64"], np.float64)
+    assert rel_l2(got, want) < 1e-13
+
+
+@pytest.mark.parametrize("n,lev,prec,rtol", [(4, 3, "d", 1e-9), (4, 4, "d", 1e-9), (4, 3, "s", 2e-3),
+                                            (8, 3, "d", 1e-7)])
+def test_known_answers(n, lev, prec, rtol, oracle_d, oracle_s):
+    o = oracle_d if prec == "d" else oracle_s
+    U, E = ref_operators(n, prec)
+    xyz, q = o.ref_sources(32768)
+    phi = o.fmm(xyz, q, n, lev, U, E)
+    dref = oracle_d.direct_fp64(xyz.astype(np.float64), q.astype(np.float64), np.arange(32768))
+    err = rel_l2(phi, dref)
+    want = G[f"kat_{prec}_n{n}_l{lev}"]
+    assert abs(err - want) <= rtol * want, (err, want)
+    if (n, lev, prec) == (4, 3, "d"):
+        first = _hexarr(G["fmm_d_n4_l3_first32"], np.float64)
+        assert rel_l2(phi[:32], first) < 1e-10
