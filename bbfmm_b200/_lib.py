@@ -68,12 +68,13 @@ def check(rc: int):
     return rc
 
 
-def exported_symbols() -> list[str]:
-    """Function names declared in include/*.h (for the export check)."""
+def exported_symbols(macro: str = "BBFMM_B200_API") -> list[str]:
+    """Function names declared in include/*.h with the given export macro
+    (BBFMM_B200_API: libbbfmm_b200.so; BBFMM_B200_REF_API: the reference-name shims)."""
     import glob
     import re
     names = []
     for h in sorted(glob.glob(os.path.join(os.path.dirname(HERE), "include", "*.h"))):
         txt = open(h).read()
-        names += re.findall(r"^BBFMM_B200_API\s+[^;(]*?\b(\w+)\s*\(", txt, flags=re.M)
+        names += re.findall(r"^" + macro + r"\s+[^;(]*?\b(\w+)\s*\(", txt, flags=re.M)
     return names

@@ -33,6 +33,7 @@ UNITS = [
     ("proj_dmma.cu", [], "proj_dmma"),
     ("direct.cu", [], "direct"),
     ("solver.cu", [], "solver"),
+    ("reference_abi.cu", [], "reference_abi"),
 ]
 
 
@@ -72,7 +73,25 @@ def build(verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, lib)
+    build_shims()
     return lib
+
+
+SHIMS = {"libbbfmm_b200_ref_d.so": [], "libbbfmm_b200_ref_s.so": ["-DBBFMM_B200_SINGLE"]}
+
+
+def build_shims() -> None:
+    """The reference's own entry-point names, one library per precision, forwarding to
+    libbbfmm_b200.so (found next to them through the $ORIGIN run path)."""
+    for name, defs in SHIMS.items():
+        out = os.path.join(LIBDIR, name)
+        cmd = ["gcc", "-std=gnu99", "-O2", "-fPIC", "-shared", *defs, "-I" + os.path.join(ROOT, "include"),
+               os.path.join(CSRC, "reference_shim.c"), "-o", out + ".tmp", "-L" + LIBDIR, "-l:" + LIBNAME,
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"shim build failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        os.replace(out + ".tmp", out)
 
 
 if __name__ == "__main__":

@@ -106,34 +106,46 @@ int Solver<T>::set_tables(const T *Tkz_h, const T *Cw_h, const T *Kw_h) {
   BBFMM_CUDA_OK(cudaMemcpy(tkz, Tkz_h, sizeof(T) * n * n, cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(cw, Cw_h, sizeof(T) * 2 * n * n, cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(kw, Kw_h, sizeof(T) * n3, cudaMemcpyHostToDevice));
+  // pageable copies may still be in flight when cudaMemcpy returns; the solver's stream does
+  // not order after the legacy stream
+  BBFMM_CUDA_OK(cudaDeviceSynchronize());
   return BBFMM_OK;
 }
 
 template <typename T>
 int Solver<T>::set_operators(const T *U, const T *E) {
+  // either half may be omitted: U feeds the projections, E the M2L
   if (!kw) return bbfmm_set_error(BBFMM_ERR_STATE, "tables must be set before operators");
-  std::vector<T> kwh(n3);
-  BBFMM_CUDA_OK(cudaMemcpy(kwh.data(), kw, sizeof(T) * n3, cudaMemcpyDeviceToHost));
-  std::vector<T> ert((size_t)BBFMM_NUM_OFFSETS * r * r), bup((size_t)n3 * r), bdn((size_t)r * n3);
+  if (U) {
+    std::vector<T> kwh(n3);
+    BBFMM_CUDA_OK(cudaMemcpy(kwh.data(), kw, sizeof(T) * n3, cudaMemcpyDeviceToHost));
+    std::vector<T> bup((size_t)n3 * r), bdn((size_t)r * n3);
+    for (int l = 0; l < n3; ++l)
+      for (int i = 0; i < r; ++i) {
+        bup[(size_t)l * r + i] = kwh[l] * U[(size_t)i * n3 + l];
+        bdn[(size_t)i * n3 + l] = U[(size_t)i * n3 + l];
+      }
+    if (!Bup) {
+      TRY(dalloc(&Bup, bup.size()));
+      TRY(dalloc(&Bdn, bdn.size()));
+    }
+    BBFMM_CUDA_OK(cudaMemcpy(Bup, bup.data(), sizeof(T) * bup.size(), cudaMemcpyHostToDevice));
+    BBFMM_CUDA_OK(cudaMemcpy(Bdn, bdn.data(), sizeof(T) * bdn.size(), cudaMemcpyHostToDevice));
+    BBFMM_CUDA_OK(cudaDeviceSynchronize());
+  }
+  if (!E) return BBFMM_OK;
+  std::vector<T> ert((size_t)BBFMM_NUM_OFFSETS * r * r);
   for (int k = 0; k < BBFMM_NUM_OFFSETS; ++k)
     for (int i = 0; i < r; ++i)
       for (int j = 0; j < r; ++j)
         ert[((size_t)k * r + i) * r + j] = E[((size_t)k * r + j) * r + i];
-  for (int l = 0; l < n3; ++l)
-    for (int i = 0; i < r; ++i) {
-      bup[(size_t)l * r + i] = kwh[l] * U[(size_t)i * n3 + l];
-      bdn[(size_t)i * n3 + l] = U[(size_t)i * n3 + l];
-    }
   if (!Ert) {
     TRY(dalloc(&Ert, ert.size()));
     TRY(dalloc(&Ecol, ert.size()));
-    TRY(dalloc(&Bup, bup.size()));
-    TRY(dalloc(&Bdn, bdn.size()));
   }
   BBFMM_CUDA_OK(cudaMemcpy(Ert, ert.data(), sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(Ecol, E, sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
-  BBFMM_CUDA_OK(cudaMemcpy(Bup, bup.data(), sizeof(T) * bup.size(), cudaMemcpyHostToDevice));
-  BBFMM_CUDA_OK(cudaMemcpy(Bdn, bdn.data(), sizeof(T) * bdn.size(), cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaDeviceSynchronize());
   if (mode == MODE_MIXED) {
     if (!tc_supported()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "mixed mode needs an sm_100 GPU");
     if (tcops) tc_free_operators(tcops);
@@ -190,6 +202,7 @@ int Solver<T>::set_particles_sorted(int N_, const int *perm_h, const int *leaf_s
   if (mode == MODE_MIXED) TRY(dalloc(&loc4, N > 0 ? N : 1));
   if (N > 0) BBFMM_CUDA_OK(cudaMemcpy(perm, perm_h, sizeof(int) * N, cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(leaf_start, leaf_start_h, sizeof(int) * (nl + 1), cudaMemcpyHostToDevice));
+  BBFMM_CUDA_OK(cudaDeviceSynchronize());
   TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream));
   if (N > 0) {
     T *xyz_d = nullptr;
@@ -277,6 +290,19 @@ template <typename T>
 int Solver<T>::interaction(int lo, int hi) {
   const Tables tb = tables();
   for (int l = lo; l <= hi; ++l) {
+    TRY(m2l_post(l));
+    if (l > BBFMM_MINLEV) {
+      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream));
+      mark(ST_L2L);
+    }
+  }
+  return BBFMM_OK;
+}
+
+// M2L of one level into Lbuf, then the post-M2L projection into F[l & 1] (assign).
+template <typename T>
+int Solver<T>::m2l_post(int l) {
+  {
     const T *Ml = Mall + Moff[l];
     const bool split = mode == MODE_MIXED && l >= TC_MIN_LEVEL;
     if (split) {
@@ -297,10 +323,6 @@ int Solver<T>::interaction(int lo, int hi) {
     const T scale = (T)1 / cell_length<T>(l, (T)L);
     TRY(proj(pow8i(l), r, n3, Lbuf, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG));
     mark(ST_PROJ_DOWN);
-    if (l > BBFMM_MINLEV) {
-      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream));
-      mark(ST_L2L);
-    }
   }
   return BBFMM_OK;
 }

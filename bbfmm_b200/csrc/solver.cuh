@@ -97,6 +97,7 @@ struct Solver {
   int alloc_work();
   int upward(const void *q_dev, int q_is_double);   // gather q, P2M, M2M, projections -> Mall
   int interaction(int level_lo, int level_hi);       // M2L + post projection + L2L into F
+  int m2l_post(int level);                           // M2L + post projection of one level
   int downward_finish(void *phi_dev, int phi_is_double, bool near);  // L2P, P2P, scatter
   int solve(const void *q_dev, void *phi_dev, int io_double);
   int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order

@@ -46,4 +46,29 @@ build libref_cpu8a_d -DCPU8 -DCPU8A
 build libref_cpu8a_s -DCPU8 -DCPU8A -DSINGLE
 build libref_cpu9a_d -DCPU9 -DCPU9A
 build libref_cpu9a_s -DCPU9 -DCPU9A -DSINGLE
+# Drop-in build: the reference's own code with its pass objects (anotherFMMCompute,
+# anotherUpwardPass, anotherFMMInteraction, anotherDownwardPass[X], anotherNearField) left
+# out and resolved from the B200 library's reference-name shims instead.
+LIBDIR="$HERE/../bbfmm_b200/lib"
+if [ -f "$LIBDIR/libbbfmm_b200_ref_d.so" ]; then
+  DROP="anotherFMMCompute.c anotherFMMInteraction.c anotherDownwardPassX.c anotherDownwardPass.c
+        anotherUpwardPass.c anotherNearField.c"
+  for prec in d s; do
+    def=""; [ $prec = s ] && def="-DSINGLE"
+    objdir="$OUT/obj_dropin_$prec"; mkdir -p "$objdir"; objs=""
+    for src in $SRCS; do
+      case " $(echo $DROP) " in *" $src "*) continue;; esac
+      gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE -DENABLE_GETTIMEOFDAY \
+          -DCPU8 -DCPU8A $def -I"$REF" -c "$REF/$src" -o "$objdir/${src%.c}.o" &
+      objs="$objs $objdir/${src%.c}.o"
+    done
+    gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE -DCPU8 -DCPU8A $def -I"$REF" \
+        -c "$HERE/ref_harness.c" -o "$objdir/ref_harness.o" &
+    wait
+    gcc -shared -fopenmp -o "$OUT/libref_dropin_$prec.so" $objs "$objdir/ref_harness.o" \
+        -L"$LIBDIR" -l:libbbfmm_b200_ref_$prec.so -Wl,--disable-new-dtags,-rpath,'$ORIGIN/../../bbfmm_b200/lib' \
+        -L"$BL" -l:"$BLAS" -Wl,-rpath,"$BL" -lm
+    rm -rf "$objdir"
+  done
+fi
 echo "built reference CPU libraries in $OUT"

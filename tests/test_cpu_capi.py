@@ -22,6 +22,19 @@ def test_library_exports_every_declared_symbol():
         getattr(L, n)
 
 
+@pytest.mark.parametrize("shim", ["libbbfmm_b200_ref_d.so", "libbbfmm_b200_ref_s.so"])
+def test_reference_name_shims_export_the_reference_symbols(shim):
+    import os
+    names = _lib.exported_symbols("BBFMM_B200_REF_API")
+    assert {"m2l_drv", "anotherFMMCompute", "anotherUpwardPass", "anotherFMMInteraction", "anotherDownwardPass",
+            "anotherNearField", "m2l_host_basic", "m2l_host_ij_blocking"} <= set(names)
+    path = os.path.join(os.path.dirname(_lib.LIB_PATH), shim)
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines()}
+    assert not [n for n in names + ["kernel_exec_time"] if n not in exported]
+    C.CDLL(path)  # loads, resolving libbbfmm_b200.so through its run path
+
+
 @pytest.mark.parametrize("fp32", [0, 1])
 @pytest.mark.parametrize("n", [4, 8])
 def test_weights_equal_oracle(fp32, n, oracle_d, oracle_s):
