@@ -140,6 +140,99 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   }
 }
 
+// Leading block only (outputs i < NI <= 64, components j < j1 <= 64): every warp owns one
+// 8-target fragment row and all NI/8 output fragments; a 4-stage cp.async pipeline over
+// the (offset, 16-component chunk) sequence keeps the small per-offset tiles in flight.
+// A is stored [target][j] (stride 20 doubles, conflict-free fragment reads, 16-byte copies).
+namespace lead {
+constexpr int NT = 64, BK = 16, STAGES = 4, AST = BK + 4;
+template <int NI>
+struct Cfg {
+  static constexpr int BST = NI + 4;
+  static constexpr int STAGE = NT * AST + BK * BST;
+  static constexpr int SMEM = STAGES * STAGE * 8;
+};
+}  // namespace lead
+
+template <int NI>
+__global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict__ M, const double *__restrict__ Ecol,
+                                                       double *__restrict__ Lout, int level, int j1,
+                                                       const int4 *__restrict__ offs) {
+  constexpr int BST = lead::Cfg<NI>::BST, STAGE = lead::Cfg<NI>::STAGE, NF = NI / 8;
+  extern __shared__ __align__(16) double smem[];
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;
+  const int nbox = P / bw;
+  const int tiles_per_class = nbox * nbox * nbox;
+  const int c = blockIdx.x / tiles_per_class;
+  const int tb = blockIdx.x % tiles_per_class;
+  const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
+  const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
+  const int nt = bw * bw * bw;
+  const int64_t P3 = (int64_t)P * P * P;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nchunk = (j1 + lead::BK - 1) / lead::BK;
+  const int niter = 189 * nchunk;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+
+  auto issue = [&](int it) {
+    if (it < niter) {
+      const int o = it / nchunk, jc = (it % nchunk) * lead::BK;
+      const int4 ov = offs[c * 189 + o];
+      const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
+      const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
+      const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
+      const int sc = (scx << 2) | (scy << 1) | scz;
+      const uint32_t sa = sbase + (uint32_t)((it % lead::STAGES) * STAGE) * 8u;
+      const uint32_t sb = sa + (uint32_t)(lead::NT * lead::AST) * 8u;
+      for (int e = tid; e < lead::NT * (lead::BK / 2); e += 256) {  // 64 targets x 8 pairs of j
+        const int t = e / (lead::BK / 2), j2 = (e % (lead::BK / 2)) * 2;
+        const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
+        const bool ok = t < nt && jc + j2 < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
+        const double *src = ok ? M + ((int64_t)sc * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + j2 : M;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa + (uint32_t)(t * lead::AST + j2) * 8u),
+                     "l"(src), "r"(ok ? 16 : 0)
+                     : "memory");
+      }
+      const double *Ek = Ecol + (int64_t)ov.x * R * R;
+      for (int e = tid; e < lead::BK * (NI / 2); e += 256) {  // 16 rows j x NI/2 pairs of i
+        const int jj = e / (NI / 2), i2 = (e % (NI / 2)) * 2;
+        const int j = jc + jj < j1 ? jc + jj : j1 - 1;
+        cp_async16(sb + (uint32_t)(jj * BST + i2) * 8u, Ek + (int64_t)j * R + i2);
+      }
+    }
+    cp_commit();  // (possibly empty) group keeps the wait counts uniform
+  };
+
+  double acc[NF][2];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) acc[f][0] = acc[f][1] = 0.0;
+#pragma unroll
+  for (int s = 0; s < lead::STAGES - 1; ++s) issue(s);
+  for (int it = 0; it < niter; ++it) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(lead::STAGES - 2) : "memory");
+    __syncthreads();
+    issue(it + lead::STAGES - 1);  // refills the stage consumed in iteration it - 1
+    const double *A = smem + (it % lead::STAGES) * STAGE;
+    const double *B = A + lead::NT * lead::AST;
+#pragma unroll
+    for (int ks = 0; ks < lead::BK / 4; ++ks) {
+      const int k = ks * 4 + (lane & 3);
+      const double af = A[(warp * 8 + (lane >> 2)) * lead::AST + k];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) dmma(acc[f][0], acc[f][1], af, B[k * BST + f * 8 + (lane >> 2)]);
+    }
+  }
+  cp_wait_all();
+  const int t = warp * 8 + (lane >> 2);
+  if (t >= nt) return;
+  const int px = bxo + (t % bw), py = byo + ((t / bw) % bw), pz = bzo + (t / (bw * bw));
+  double *dst = Lout + ((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px) * R;
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+    *reinterpret_cast<double2 *>(dst + f * 8 + 2 * (lane & 3)) = make_double2(acc[f][0], acc[f][1]);
+}
+
 }  // namespace dm
 
 // Writes Lout[cell][0:ni) for every cell of the level (assign); entries i >= ni untouched.
@@ -148,6 +241,23 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
   if (r != dm::R) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "FP64 tensor M2L is built for r = 256");
   if (j0 < 0 || j1 > r || j0 >= j1 || ni < 2 || ni > r || ni % 2)
     return bbfmm_set_error(BBFMM_ERR_ARG, "bad contraction / output range");
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;
+  const int nbox = P / bw;
+  const int grid = 8 * nbox * nbox * nbox;
+  if (j0 == 0 && j1 <= 64 && (ni == 32 || ni == 64)) {  // the FP64 leading block
+    static bool lattr = false;
+    if (!lattr) {
+      cudaFuncSetAttribute(dm::m2l_lead_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           dm::lead::Cfg<32>::SMEM);
+      cudaFuncSetAttribute(dm::m2l_lead_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           dm::lead::Cfg<64>::SMEM);
+      lattr = true;
+    }
+    if (ni == 32) dm::m2l_lead_kernel<32><<<grid, 256, dm::lead::Cfg<32>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
+    else dm::m2l_lead_kernel<64><<<grid, 256, dm::lead::Cfg<64>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
+    return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_lead", __FILE__, __LINE__);
+  }
   static bool attr = false;
   if (!attr) {
     cudaError_t e =
@@ -155,10 +265,7 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma smem attribute", __FILE__, __LINE__);
     attr = true;
   }
-  const int P = 1 << (level - 1);
-  const int bw = P < 4 ? P : 4;
-  const int nbox = P / bw;
-  dm::m2l_dmma_kernel<<<8 * nbox * nbox * nbox, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs);
+  dm::m2l_dmma_kernel<<<grid, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma", __FILE__, __LINE__);
 }
 

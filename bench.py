@@ -32,6 +32,10 @@ N_ORDER = 8
 MAXLEV = 7
 N_TARGETS = 4096
 METRIC = "FMM solves/s at N=4,194,304, n=8, depth 7 (1 GPU; err <= 1.2x FP64 required)"
+# DRAM bytes of one m2l_tc_kernel launch per cell of its level, from an ncu capture of the
+# level-5 launch (32,768 cells: 207.8 MB read + 42.5 MB written); the traffic scales with
+# the number of cells (multipole split in, FP64 M2L output read-modify-written).
+TC_DRAM_BYTES_PER_CELL = (207.783168e6 + 42.53184e6) / 32768
 
 
 def interactions_per_level(level: int) -> int:
@@ -296,7 +300,9 @@ def main():
         peak = bf16 / 3.0                                      # three bf16 products per term
         roof = {"kernel": "m2l_tc (split-bf16 tcgen05 M2L, leaf level)", "bound": "tensor",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": f"{peak_src} bf16 dense burst / 3 products", "traffic": None,
+                "peak_source": f"{peak_src} bf16 dense burst / 3 products",
+                "traffic": TC_DRAM_BYTES_PER_CELL * 8 ** lev,
+                "traffic_note": "ncu dram bytes of the level-5 launch scaled by cells",
                 "flop_per_launch": tc_flop, "launch_ms": m2l_ms}
     else:
         flop = 2.0 * r * r * I_leaf
