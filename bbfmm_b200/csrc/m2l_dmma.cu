@@ -43,6 +43,8 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
                                                           const double *__restrict__ Ecol,
                                                           double *__restrict__ Lout, int level, int j0, int j1,
                                                           int ni, const int4 *__restrict__ offs) {
+  // blockIdx.y selects one of gridDim.y groups of the 189 offsets; with several groups each
+  // writes its partial sums to its own slice of Lout (level cells x R apart)
   extern __shared__ __align__(16) double smem[];
   const int P = 1 << (level - 1);
   const int bw = P < 4 ? P : 4;
@@ -59,11 +61,14 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   const bool active = wn * 64 < ni;         // this warp has outputs to compute
   const int nb = ni < R ? ((ni + 63) / 64) * 64 : R;  // B columns staged
   const int nchunk = (j1 - j0 + BK - 1) / BK;
-  const int niter = 189 * nchunk;
+  const int og = blockIdx.y, ng = gridDim.y;
+  const int o0 = (189 * og) / ng, o1 = (189 * (og + 1)) / ng;
+  const int niter = (o1 - o0) * nchunk;
+  Lout += (int64_t)og * 8 * P3 * R;
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
 
   auto issue = [&](int it, int buf) {
-    const int o = it / nchunk, jc = j0 + (it % nchunk) * BK;
+    const int o = o0 + it / nchunk, jc = j0 + (it % nchunk) * BK;
     const int4 ov = offs[c * 189 + o];
     const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
     const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
@@ -233,11 +238,21 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
     *reinterpret_cast<double2 *>(dst + f * 8 + 2 * (lane & 3)) = make_double2(acc[f][0], acc[f][1]);
 }
 
+// Lout[e] = sum_g part[g][e], in a fixed order.
+__global__ void sum_parts_kernel(int64_t count, int ng, const double *__restrict__ part, double *__restrict__ Lout) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int g = 0; g < ng; ++g) v += part[(int64_t)g * count + e];
+    Lout[e] = v;
+  }
+}
+
 }  // namespace dm
 
 // Writes Lout[cell][0:ni) for every cell of the level (assign); entries i >= ni untouched.
+// part: scratch of 21 x 8^level x r doubles for levels <= 3 (or null: single pass).
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
-                    const int4 *offs, cudaStream_t s) {
+                    const int4 *offs, double *part, cudaStream_t s) {
   if (r != dm::R) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "FP64 tensor M2L is built for r = 256");
   if (j0 < 0 || j1 > r || j0 >= j1 || ni < 2 || ni > r || ni % 2)
     return bbfmm_set_error(BBFMM_ERR_ARG, "bad contraction / output range");
@@ -264,6 +279,16 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
         cudaFuncSetAttribute(dm::m2l_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dm::SMEM_BYTES);
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma smem attribute", __FILE__, __LINE__);
     attr = true;
+  }
+  if (level <= 3 && part) {
+    // few target tiles: spread the offsets over 21 CTAs per tile, then sum the partials
+    const int ng = 21;
+    const int64_t count = 8 * (int64_t)P * P * P * r;
+    dm::m2l_dmma_kernel<<<dim3(grid, ng), 256, dm::SMEM_BYTES, s>>>(M, Ecol, part, level, j0, j1, ni, offs);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma", __FILE__, __LINE__);
+    dm::sum_parts_kernel<<<(int)((count + 255) / 256), 256, 0, s>>>(count, ng, part, Lout);
+    return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma parts", __FILE__, __LINE__);
   }
   dm::m2l_dmma_kernel<<<grid, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma", __FILE__, __LINE__);

@@ -178,6 +178,9 @@ int Solver<T>::alloc_work() {
   TRY(dalloc(&Mall, (size_t)tot));
   if (Lbuf) cudaFree(Lbuf);
   TRY(dalloc(&Lbuf, (size_t)nl * r));
+  if (Lpart) cudaFree(Lpart);
+  Lpart = nullptr;
+  if (sizeof(T) == 8 && r == 256) TRY(dalloc(&Lpart, (size_t)DMMA_PARTS * pow8i(maxlev < 3 ? maxlev : 3) * r));
   if (mode == MODE_MIXED) {
     if (Msplit) cudaFree(Msplit);
     unsigned char *p = nullptr;
@@ -270,7 +273,7 @@ template <typename T>
 int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
   if (sizeof(T) == 8 && r == 256)
     return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
-                           stream);
+                           (double *)Lpart, stream);
   if (ni != r) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
   return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream);
 }
@@ -416,7 +419,7 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 template <typename T>
 void Solver<T>::release() {
   void *ptrs[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, offs, perm, leaf_start, leafm, pos4, loc4,
-                  S[0], S[1], F[0], F[1], Mall, Lbuf, Msplit, phis};
+                  S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit, phis};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (tcops) tc_free_operators(tcops);

@@ -35,7 +35,8 @@ int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s);
 void build_offset_table(int *out);
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
-                    const int4 *offs, cudaStream_t s);
+                    const int4 *offs, double *part, cudaStream_t s);
+constexpr int DMMA_PARTS = 21;  // offset groups of the small-level FP64 M2L
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
                      double *C, int level, int mapmode, cudaStream_t s);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
@@ -80,6 +81,7 @@ struct Solver {
   T *Mall = nullptr;
   std::vector<int64_t> Moff;  // offset (elements) of level l in Mall, cpg layout
   T *Lbuf = nullptr;
+  T *Lpart = nullptr;  // partial sums of the small-level FP64 M2L (levels <= 3)
   void *Msplit = nullptr;
   T *phis = nullptr;
   // timing
