@@ -151,6 +151,122 @@ int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s
 
 }  // namespace bbfmm
 
+namespace bbfmm {
+// ------------------------------------------------------------- near field with gradient
+// pot[i] += sum_j q_j / r_ij and fld[3i + a] += sum_j q_j (x_j - x_i)_a / r_ij^3 (the
+// gradient of the potential at x_i), no target factor; sorted order.
+template <typename T>
+__global__ void __launch_bounds__(256) p2p_field_kernel(int N, const T *__restrict__ pos4,
+                                                        const int *__restrict__ leaf_start,
+                                                        const int *__restrict__ leafm, int maxlev, T *__restrict__ pot,
+                                                        T *__restrict__ fld) {
+  const int ncpd = 1 << maxlev;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const T fx = pos4[4 * (int64_t)i], fy = pos4[4 * (int64_t)i + 1], fz = pos4[4 * (int64_t)i + 2];
+    int ix, iy, iz;
+    morton_to_grid(leafm[i], maxlev, ix, iy, iz);
+    T v = 0, gx = 0, gy = 0, gz = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int jx = ix + dx;
+      if (jx < 0 || jx >= ncpd) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jy = iy + dy;
+        if (jy < 0 || jy >= ncpd) continue;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int jz = iz + dz;
+          if (jz < 0 || jz >= ncpd) continue;
+          const int64_t B = grid_to_morton(jx, jy, jz, maxlev);
+          for (int s = leaf_start[B]; s < leaf_start[B + 1]; ++s) {
+            const T ex = pos4[4 * (int64_t)s] - fx, ey = pos4[4 * (int64_t)s + 1] - fy,
+                    ez = pos4[4 * (int64_t)s + 2] - fz;
+            const T rr = ex * ex + ey * ey + ez * ez;
+            if (rr != (T)0) {
+              const T rinv = (T)1 / sqrt(rr), qr = pos4[4 * (int64_t)s + 3] * rinv;
+              const T qr3 = qr * rinv * rinv;
+              v += qr;
+              gx += qr3 * ex;
+              gy += qr3 * ey;
+              gz += qr3 * ez;
+            }
+          }
+        }
+      }
+    }
+    pot[i] += v;
+    fld[3 * (int64_t)i] += gx;
+    fld[3 * (int64_t)i + 1] += gy;
+    fld[3 * (int64_t)i + 2] += gz;
+  }
+}
+
+// The same on FP32 leaf-local coordinates (see p2p_local_kernel); FP64 outputs.
+__global__ void __launch_bounds__(256) p2p_local_field_kernel(int N, const float4 *__restrict__ loc4,
+                                                              const int *__restrict__ leaf_start,
+                                                              const int *__restrict__ leafm, int maxlev, float h,
+                                                              double *__restrict__ pot, double *__restrict__ fld) {
+  const int ncpd = 1 << maxlev;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const float4 f = loc4[i];
+    int ix, iy, iz;
+    morton_to_grid(leafm[i], maxlev, ix, iy, iz);
+    float sum = 0.f, comp = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int jx = ix + dx;
+      if (jx < 0 || jx >= ncpd) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jy = iy + dy;
+        if (jy < 0 || jy >= ncpd) continue;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int jz = iz + dz;
+          if (jz < 0 || jz >= ncpd) continue;
+          const int64_t B = grid_to_morton(jx, jy, jz, maxlev);
+          for (int s = leaf_start[B]; s < leaf_start[B + 1]; ++s) {
+            const float4 g = loc4[s];
+            const float ex = (g.x - f.x) + (float)dx * h, ey = (g.y - f.y) + (float)dy * h,
+                        ez = (g.z - f.z) + (float)dz * h;
+            const float rr = ex * ex + ey * ey + ez * ez;
+            if (rr != 0.f) {
+              const float rinv = rsqrtf(rr), t = g.w * rinv, t3 = t * rinv * rinv;
+              const float y = sum + t;
+              comp += (fabsf(sum) >= fabsf(t)) ? ((sum - y) + t) : ((t - y) + sum);
+              sum = y;
+              gx += t3 * ex;
+              gy += t3 * ey;
+              gz += t3 * ez;
+            }
+          }
+        }
+      }
+    }
+    pot[i] += (double)sum + (double)comp;
+    fld[3 * (int64_t)i] += gx;
+    fld[3 * (int64_t)i + 1] += gy;
+    fld[3 * (int64_t)i + 2] += gz;
+  }
+}
+
+template <typename T>
+int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld,
+                     cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  p2p_field_kernel<T><<<p2p_grid(N), 256, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, pot, fld);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "p2p_field", __FILE__, __LINE__);
+}
+template int launch_p2p_field<double>(int, const double *, const int *, const int *, int, double *, double *,
+                                      cudaStream_t);
+template int launch_p2p_field<float>(int, const float *, const int *, const int *, int, float *, float *,
+                                     cudaStream_t);
+
+int launch_p2p_local_field(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L,
+                           double *pot, double *fld, cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  const float h = (float)cell_length<double>(maxlev, L);
+  p2p_local_field_kernel<<<p2p_grid(N), 256, 0, s>>>(N, loc4, leaf_start, leafm, maxlev, h, pot, fld);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "p2p_local_field", __FILE__, __LINE__);
+}
+
+}  // namespace bbfmm
+
 // ====================================================== near-field C-ABI entry points
 #include <mutex>
 

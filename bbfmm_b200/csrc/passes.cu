@@ -490,3 +490,135 @@ template int launch_scatter<float, double>(int, const int *, const float *, doub
 template int launch_scatter<double, float>(int, const int *, const double *, float *, cudaStream_t);
 
 }  // namespace bbfmm
+
+// ------------------------------------------------------------ L2P with gradient
+namespace bbfmm {
+
+// S(x_m, x) and dS/dx for all nodes m: Clenshaw recurrence and its derivative.
+template <typename T, int NN>
+__device__ __forceinline__ void sn_nodes_d(const T *__restrict__ tkz, T x, T *out, T *dout) {
+#pragma unroll
+  for (int m = 0; m < NN; ++m) {
+    T d1 = 0, d2 = 0, e1 = 0, e2 = 0;  // d_j and d_j' at j+1, j+2
+#pragma unroll
+    for (int j = NN - 1; j > 0; --j) {
+      const T d0 = 2 * x * d1 - d2 + tkz[m * NN + j];
+      const T e0 = 2 * d1 + 2 * x * e1 - e2;
+      d2 = d1; d1 = d0;
+      e2 = e1; e1 = e0;
+    }
+    out[m] = x * d1 - d2 + (T)0.5 * tkz[m * NN];
+    dout[m] = d1 + x * e1 - e2;
+  }
+}
+
+// One warp per leaf: pot[p] = (2/n)^3 sum_l F[l] Sx Sy Sz (no target factor) and
+// fld[3p + a] = d pot / d x_a, with the chain factor 2 / leaf length of the leaf map.
+template <typename T, int NN>
+__global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
+                                                        int maxlev, T L, Tables tabs, const T *__restrict__ F,
+                                                        T *__restrict__ pot, T *__restrict__ fld) {
+  constexpr int N2 = NN * NN, N3 = N2 * NN;
+  __shared__ T s_tkz[NN * NN];
+  const T *tkz = tab_tkz<T>(tabs);
+  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nleaf = pow8i(maxlev);
+  const T len = cell_length<T>(maxlev, L);
+  const T ihalf = (T)1 / (len / (T)2);
+  const T prefac = (T)2 / (T)NN;
+  const T pre3 = prefac * prefac * prefac;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t m = warp; m < nleaf; m += nwarps) {
+    const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
+    if (p1 == p0) continue;
+    int ix, iy, iz;
+    morton_to_grid(m, maxlev, ix, iy, iz);
+    const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
+            cz = cell_center_1d<T>(iz, maxlev, L);
+    const T *Fm = F + m * N3;
+    for (int p = p0; p < p1; ++p) {
+      const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
+      const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
+      const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
+      T sx[NN], sy[NN], sz[NN], dx[NN], dy[NN], dz[NN];
+      sn_nodes_d<T, NN>(s_tkz, x, sx, dx);
+      sn_nodes_d<T, NN>(s_tkz, y, sy, dy);
+      sn_nodes_d<T, NN>(s_tkz, z, sz, dz);
+      T v = 0, gx = 0, gy = 0, gz = 0;
+      for (int l12 = lane; l12 < N2; l12 += 32) {
+        const int l1 = l12 / NN, l2 = l12 % NN;
+        const T *f = Fm + l12 * NN;
+        T in0 = 0, in1 = 0;
+#pragma unroll
+        for (int l3 = 0; l3 < NN; ++l3) {
+          in0 += sz[l3] * f[l3];
+          in1 += dz[l3] * f[l3];
+        }
+        v += sx[l1] * sy[l2] * in0;
+        gx += dx[l1] * sy[l2] * in0;
+        gy += sx[l1] * dy[l2] * in0;
+        gz += sx[l1] * sy[l2] * in1;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+        gx += __shfl_xor_sync(0xffffffffu, gx, off);
+        gy += __shfl_xor_sync(0xffffffffu, gy, off);
+        gz += __shfl_xor_sync(0xffffffffu, gz, off);
+      }
+      if (lane == 0) {
+        pot[p] = pre3 * v;
+        fld[3 * (int64_t)p] = pre3 * ihalf * gx;
+        fld[3 * (int64_t)p + 1] = pre3 * ihalf * gy;
+        fld[3 * (int64_t)p + 2] = pre3 * ihalf * gz;
+      }
+    }
+  }
+}
+
+// Sorted (potential, field) -> caller's order.
+template <typename T, typename TO>
+__global__ void scatter_field_kernel(int N, const int *__restrict__ perm, const T *__restrict__ pot,
+                                     const T *__restrict__ fld, TO *__restrict__ pot_out, TO *__restrict__ fld_out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const int k = perm[i];
+    if (pot_out) pot_out[k] = (TO)pot[i];
+    if (fld_out) {
+      fld_out[3 * (int64_t)k] = (TO)fld[3 * (int64_t)i];
+      fld_out[3 * (int64_t)k + 1] = (TO)fld[3 * (int64_t)i + 1];
+      fld_out[3 * (int64_t)k + 2] = (TO)fld[3 * (int64_t)i + 2];
+    }
+  }
+}
+
+template <typename T>
+int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F,
+                     T *pot, T *fld, cudaStream_t s) {
+  const int grid = grid_for(pow8i(maxlev), 4, 148 * 64);
+  if (n == 4) l2p_field_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld);
+  else if (n == 8) l2p_field_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld);
+  else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
+  return bbfmm_set_cuda_error(cudaGetLastError(), "l2p_field", __FILE__, __LINE__);
+}
+
+template <typename T, typename TO>
+int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out,
+                         cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  scatter_field_kernel<T, TO><<<grid_for(N, 256, 148 * 32), 256, 0, s>>>(N, perm, pot, fld, pot_out, fld_out);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "scatter_field", __FILE__, __LINE__);
+}
+
+template int launch_l2p_field<double>(int, const double *, const int *, int, double, const Tables &, const double *,
+                                      double *, double *, cudaStream_t);
+template int launch_l2p_field<float>(int, const float *, const int *, int, float, const Tables &, const float *,
+                                     float *, float *, cudaStream_t);
+template int launch_scatter_field<double, double>(int, const int *, const double *, const double *, double *,
+                                                  double *, cudaStream_t);
+template int launch_scatter_field<float, float>(int, const int *, const float *, const float *, float *, float *,
+                                                cudaStream_t);
+
+}  // namespace bbfmm

@@ -401,6 +401,32 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   return rc;
 }
 
+// pot[i] = sum_j q_j / r_ij and fld[i] = grad pot at x_i (FMM), caller's order, no target
+// factor: the quantities a backward pass needs.
+template <typename T>
+int Solver<T>::solve_fields(const void *q_dev, void *pot_dev, void *fld_dev) {
+  if (!pos4) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
+  if (!Ert) return bbfmm_set_error(BBFMM_ERR_STATE, "operators not set");
+  if (!flds) TRY(dalloc(&flds, 3 * (size_t)(N > 0 ? N : 1)));
+  kernel_launches = 0;
+  TRY(upward(q_dev, sizeof(T) == 8));
+  TRY(interaction(BBFMM_MINLEV, maxlev));
+  const Tables tb = tables();
+  TRY(launch_l2p_field<T>(n, pos4, leaf_start, maxlev, (T)L, tb, F[maxlev & 1], phis, flds, stream));
+  mark(ST_L2P);
+  if (mode == MODE_MIXED) {
+    TRY(launch_make_local(N, (const double *)pos4, leafm, maxlev, L, loc4, stream));
+    TRY(launch_p2p_local_field(N, loc4, leaf_start, leafm, maxlev, L, (double *)phis, (double *)flds, stream));
+    mark(ST_P2P, 2);
+  } else {
+    TRY(launch_p2p_field<T>(N, pos4, leaf_start, leafm, maxlev, phis, flds, stream));
+    mark(ST_P2P);
+  }
+  TRY((launch_scatter_field<T, T>(N, perm, phis, flds, (T *)pot_dev, (T *)fld_dev, stream)));
+  mark(ST_SCATTER);
+  return BBFMM_OK;
+}
+
 template <typename T>
 int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
   if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "level out of range");
@@ -419,7 +445,7 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 template <typename T>
 void Solver<T>::release() {
   void *ptrs[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, offs, perm, leaf_start, leafm, pos4, loc4,
-                  S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit, phis};
+                  S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit, phis, flds};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (tcops) tc_free_operators(tcops);
@@ -511,6 +537,12 @@ int bbfmm_b200_solve(bbfmm_b200_solver *h, const void *q_dev, void *phi_dev) {
   if (!h || !q_dev || !phi_dev) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   if (h->f) return h->f->solve(q_dev, phi_dev, 0);
   return h->d->solve(q_dev, phi_dev, 1);
+}
+
+int bbfmm_b200_solve_fields(bbfmm_b200_solver *h, const void *q_dev, void *pot_dev, void *field_dev) {
+  if (!h || !q_dev || (!pot_dev && !field_dev)) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  if (h->f) return h->f->solve_fields(q_dev, pot_dev, field_dev);
+  return h->d->solve_fields(q_dev, pot_dev, field_dev);
 }
 
 int bbfmm_b200_solve_host(bbfmm_b200_solver *h, const void *q_host, void *phi_host) {

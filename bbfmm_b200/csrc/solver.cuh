@@ -32,6 +32,10 @@ template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start
 int launch_p2p_local(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L, double *phi, cudaStream_t s);
 int launch_make_local(int N, const double *pos4, const int *leafm, int maxlev, double L, float4 *loc4, cudaStream_t s);
 int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s);
+template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s);
+template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
+template <typename T> int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld, cudaStream_t s);
+int launch_p2p_local_field(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L, double *pot, double *fld, cudaStream_t s);
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s);
 void build_offset_table(int *out);
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
@@ -84,6 +88,7 @@ struct Solver {
   T *Lpart = nullptr;  // partial sums of the small-level FP64 M2L (levels <= 3)
   void *Msplit = nullptr;
   T *phis = nullptr;
+  T *flds = nullptr;  // 3 N, sorted field of the last solve_fields
   // timing
   bool timing = false;
   cudaEvent_t ev[ST_COUNT + 1] = {};
@@ -102,6 +107,7 @@ struct Solver {
   int m2l_post(int level);                           // M2L + post projection of one level
   int downward_finish(void *phi_dev, int phi_is_double, bool near);  // L2P, P2P, scatter
   int solve(const void *q_dev, void *phi_dev, int io_double);
+  int solve_fields(const void *q_dev, void *pot_dev, void *fld_dev);  // potential and its gradient
   int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order
   void mark(int stage, int launches = 1);
   int time_m2l(int level, int reps, float *ms);

@@ -105,6 +105,25 @@ class Solver:
         caller.wait_event(done)
         return out
 
+    def solve_fields(self, q, want_field=True):
+        """q: CUDA tensor (N,) -> (pot, field): pot_i = sum_j q_j / r_ij and field = grad pot
+        at every particle, (N,) and (N, 3) CUDA tensors (field None unless want_field)."""
+        torch = self.torch
+        q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        pot = torch.empty_like(q)
+        fld = torch.empty((q.numel(), 3), dtype=self.dtype, device=q.device) if want_field else None
+        caller = torch.cuda.current_stream(q.device)
+        mine = torch.cuda.ExternalStream(self.stream, device=q.device)
+        ready = torch.cuda.Event()
+        ready.record(caller)
+        mine.wait_event(ready)
+        _lib.check(_lib.lib().bbfmm_b200_solve_fields(self.h, C.c_void_p(q.data_ptr()), C.c_void_p(pot.data_ptr()),
+                                                       C.c_void_p(fld.data_ptr()) if fld is not None else None))
+        done = torch.cuda.Event()
+        done.record(mine)
+        caller.wait_event(done)
+        return pot, fld
+
     def solve_host(self, q):
         q = np.ascontiguousarray(np.asarray(q, dtype=self.np_dtype))
         phi = np.empty_like(q)

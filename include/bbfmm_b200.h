@@ -113,6 +113,15 @@ BBFMM_B200_API int bbfmm_b200_set_particles(bbfmm_b200_solver *s, int N, const v
  * Runs on the solver's stream and returns without synchronising. */
 BBFMM_B200_API int bbfmm_b200_solve(bbfmm_b200_solver *s, const void *q_dev, void *phi_dev);
 
+/* Potential and its gradient at every particle, without the target-charge factor:
+ * pot[i] = sum_{j != i} q_j / r_ij, field[3i + a] = d pot / d x_{i,a} (FMM-approximated, both
+ * device arrays in the caller's order; either may be NULL). With phi = q o pot this gives a
+ * backward pass in one extra solve: dL/dq = g o pot(q) + pot(g o q),
+ * dL/dx = q o (g o field(q) + field(g o q)) for L with dL/dphi = g. The reference has no
+ * derivative code; the gradient of the Chebyshev interpolant (S_n of bbfmm.c:1682-1690) is
+ * new. Runs on the solver's stream without synchronising. */
+BBFMM_B200_API int bbfmm_b200_solve_fields(bbfmm_b200_solver *s, const void *q_dev, void *pot_dev, void *field_dev);
+
 /* The same with host buffers: copies q in, solves, copies phi out and synchronises. */
 BBFMM_B200_API int bbfmm_b200_solve_host(bbfmm_b200_solver *s, const void *q_host, void *phi_host);
 

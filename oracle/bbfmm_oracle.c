@@ -588,3 +588,34 @@ void SFX(orc_ref_sources)(int N, real L, real *xyz, real *q)
     xyz[3 * i + 2] = halfm + (halfp - halfm) * rand() * inv_rand_max;
   }
 }
+
+/* FP64 potential and its gradient on sampled targets, without the target-charge factor:
+   pot[t] = sum_{x_j != x_i} q_j / r_ij, fld[3t + a] = sum_j q_j (x_j - x_i)_a / r_ij^3,
+   i = targets[t] (the derivative of the direct sum of bbfmm.c:880-913; the reference has
+   no gradient code). Neumaier-compensated sums. */
+void SFX(orc_direct_field_fp64)(int N, const double *xyz, const double *q, int ntarget, const int *targets,
+                                double *pot, double *fld)
+{
+  for (int t = 0; t < ntarget; t++) {
+    int i = targets[t];
+    double fx = xyz[3 * i], fy = xyz[3 * i + 1], fz = xyz[3 * i + 2];
+    double s[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};
+    for (int j = 0; j < N; j++) {
+      double dx = xyz[3 * j] - fx, dy = xyz[3 * j + 1] - fy, dz = xyz[3 * j + 2] - fz;
+      double rr = dx * dx + dy * dy + dz * dz;
+      if (rr == 0.0) continue;
+      double rinv = 1.0 / sqrt(rr), v[4];
+      v[0] = q[j] * rinv;
+      v[1] = v[0] * rinv * rinv * dx;
+      v[2] = v[0] * rinv * rinv * dy;
+      v[3] = v[0] * rinv * rinv * dz;
+      for (int a = 0; a < 4; a++) {
+        double y = s[a] + v[a];
+        c[a] += (fabs(s[a]) >= fabs(v[a])) ? ((s[a] - y) + v[a]) : ((v[a] - y) + s[a]);
+        s[a] = y;
+      }
+    }
+    pot[t] = s[0] + c[0];
+    for (int a = 0; a < 3; a++) fld[3 * t + a] = s[a + 1] + c[a + 1];
+  }
+}

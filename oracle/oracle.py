@@ -146,6 +146,16 @@ class Oracle:
         self._f("orc_ref_sources")(N, self.R(L), _p(xyz), _p(q))
         return xyz.reshape(N, 3), q
 
+    def direct_field_fp64(self, xyz, q, targets):
+        """FP64 potential (no target factor) and its gradient at the targets."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        targets = np.ascontiguousarray(targets, dtype=np.int32)
+        pot = np.zeros(targets.size)
+        fld = np.zeros(3 * targets.size)
+        self._f("orc_direct_field_fp64")(q.size, _p(xyz), _p(q), targets.size, _p(targets), _p(pot), _p(fld))
+        return pot, fld.reshape(-1, 3)
+
     def direct_fp64(self, xyz, q, targets):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
         q = np.ascontiguousarray(q, dtype=np.float64)
