@@ -8,46 +8,62 @@ side), so for a loss with g = dL/dphi:
     dL/dq_k = g_k pot_k(q) + pot_k(g o q)                       (the transposed FMM)
     dL/dx_k = q_k (g_k field_k(q) + field_k(g o q))             (field = grad pot)
 
-pot(q) and field(q) come out of the forward solve (bbfmm_b200_solve_fields), so the
-backward is ONE more solve with charges g o q. Neither pass keeps per-level expansions:
-each solve recomputes them on the device, and the saved state is O(N) (pot, field).
+Two ways to get pot(q) and field(q) to the backward (``save``):
+
+  "fields"     checkpoint: the forward runs bbfmm_b200_solve_fields and keeps pot and
+               field (4 values per particle); the backward is ONE more solve, with charges
+               g o q.
+  "recompute"  the forward runs the plain solve and keeps nothing but q; the backward
+               solves twice (charges q and g o q).
+
+Neither keeps per-level expansions between the passes (each solve rebuilds them on the
+device in its own work buffers), so the saved state is O(N) either way.
 The reference has no derivative code; the interpolant derivative (Clenshaw recurrence
 differentiated) and the P2P gradient kernel are new.
 """
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 
 class _FMMPhi(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, q, x, solver, need_field):
-        pot, fld = solver.solve_fields(q, want_field=need_field)
+    def forward(ctx, q, x, solver, need_field, recompute):
         ctx.solver = solver
-        ctx.save_for_backward(q, pot, fld if fld is not None else torch.empty(0, device=q.device))
         ctx.need_field = need_field
+        ctx.recompute = recompute
+        empty = torch.empty(0, device=q.device)
+        if recompute:
+            ctx.save_for_backward(q, empty, empty)
+            return solver.solve(q)
+        pot, fld = solver.solve_fields(q, want_field=need_field)
+        ctx.save_for_backward(q, pot, fld if fld is not None else empty)
         return q.to(pot.dtype) * pot
 
     @staticmethod
     def backward(ctx, g):
         q, pot, fld = ctx.saved_tensors
         solver = ctx.solver
+        if ctx.recompute:
+            pot, fld = solver.solve_fields(q, want_field=ctx.need_field)
         g = g.to(pot.dtype).contiguous()
+        q = q.to(pot.dtype)
         pot2, fld2 = solver.solve_fields(g * q, want_field=ctx.need_field)
         dq = g * pot + pot2 if ctx.needs_input_grad[0] else None
         dx = None
         if ctx.needs_input_grad[1] and ctx.need_field:
             dx = q[:, None] * (g[:, None] * fld + fld2)
-        return dq, dx, None, None
+        return dq, dx, None, None, None
 
 
-def fmm_phi(solver, q: torch.Tensor, x: torch.Tensor | None = None) -> torch.Tensor:
+def fmm_phi(solver, q: torch.Tensor, x: torch.Tensor | None = None, save: str = "fields") -> torch.Tensor:
     """q_i * phi_i on the solver's particles, differentiable in q and (if given and
     requiring grad) in the positions x, an (N, 3) tensor equal to the solver's particles.
-    Positions define the tree: pass the same x that was given to solver.set_particles."""
+    Positions define the tree: pass the same x that was given to solver.set_particles.
+    save: "fields" (keep pot and field from the forward) or "recompute" (keep only q)."""
+    if save not in ("fields", "recompute"):
+        raise ValueError(f"save must be 'fields' or 'recompute', not {save!r}")
     need_field = x is not None and x.requires_grad
     if x is None:
         x = torch.empty(0, device=q.device)
-    return _FMMPhi.apply(q, x, solver, need_field)
-
+    return _FMMPhi.apply(q, x, solver, need_field, save == "recompute")

@@ -602,6 +602,15 @@ int bbfmm_b200_direct(int N, const double *xyz_dev, const double *q_dev, int nta
   return bbfmm::launch_direct_fp64(N, xyz_dev, q_dev, ntarget, targets_dev, out_dev, (cudaStream_t)stream);
 }
 
+int bbfmm_b200_direct_field(int N, const double *xyz_dev, const double *q_dev, int ntarget, const int *targets_dev,
+                            double *pot_dev, double *field_dev, void *stream) {
+  if (N < 0 || ntarget < 0 ||
+      (ntarget > 0 && (!xyz_dev || !q_dev || !targets_dev || (!pot_dev && !field_dev))))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "bad direct-sum arguments");
+  return bbfmm::launch_direct_field_fp64(N, xyz_dev, q_dev, ntarget, targets_dev, pot_dev, field_dev,
+                                         (cudaStream_t)stream);
+}
+
 void *bbfmm_b200_stream(bbfmm_b200_solver *h) {
   if (!h) return nullptr;
   return h->f ? (void *)h->f->stream : (void *)h->d->stream;

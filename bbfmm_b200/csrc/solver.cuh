@@ -44,6 +44,8 @@ constexpr int DMMA_PARTS = 21;  // offset groups of the small-level FP64 M2L
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
                      double *C, int level, int mapmode, cudaStream_t s);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
+int launch_direct_field_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *pot,
+                             double *fld, cudaStream_t s);
 
 template <typename T> int bbfmm_weights_t(int n, T *Tkz, int *Ktable, T *Kweights, T *Cweights);
 

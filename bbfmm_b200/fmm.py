@@ -164,6 +164,23 @@ def direct(xyz, q, targets, stream=None):
     return out
 
 
+def direct_field(xyz, q, targets, stream=None):
+    """FP64 direct potential sum_{j != i} q_j / r_ij and its gradient at the given targets
+    (torch CUDA tensors as in ``direct``) -> (pot (T,), field (T, 3))."""
+    import torch
+    xyz = xyz.to(torch.float64).contiguous()
+    q = q.to(torch.float64).contiguous()
+    targets = targets.to(torch.int32).contiguous()
+    pot = torch.empty(targets.numel(), dtype=torch.float64, device=q.device)
+    fld = torch.empty((targets.numel(), 3), dtype=torch.float64, device=q.device)
+    st = torch.cuda.current_stream(q.device).cuda_stream if stream is None else stream
+    _lib.check(_lib.lib().bbfmm_b200_direct_field(q.numel(), C.c_void_p(xyz.data_ptr()), C.c_void_p(q.data_ptr()),
+                                                   targets.numel(), C.c_void_p(targets.data_ptr()),
+                                                   C.c_void_p(pot.data_ptr()), C.c_void_p(fld.data_ptr()),
+                                                   C.c_void_p(st)))
+    return pot, fld
+
+
 def bbfmm(xyz, q, L: float = 1.0, n: int = 4, level_modifier: int = 0, mode: str = "d", maxlev=None,
           operators=None):
     """One solve from host arrays, like the reference's ``bbfmm()`` with field = source.

@@ -131,7 +131,7 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------ reference arm
-def reference_sample(N_sample, maxlev_sample, reps=1):
+def reference_sample(N_sample, maxlev_sample, reps=1, n=N_ORDER):
     """Time the reference's CPU FMM (oracle/_ref) on a sample with the same particles per
     leaf as the full workload; returns (seconds per sample solve, cores, kind)."""
     from oracle.oracle import Oracle, Reference, reference_available
@@ -142,21 +142,21 @@ def reference_sample(N_sample, maxlev_sample, reps=1):
     if reference_available("d"):
         ref = Reference("d")
         d = os.path.join(ops.default_cache_dir(), "ref")
-        kp, up = ops.operator_file_names(N_ORDER, False)
+        kp, up = ops.operator_file_names(n, False)
         kp, up = os.path.join(d, kp), os.path.join(d, up)
         if not (os.path.exists(kp) and os.path.exists(up)):
-            _, U, E = ops.load_operators(N_ORDER, False)
-            ops.write_operator_files(d, N_ORDER, U, E, False)
-        ref.fmm(x, q, N_ORDER, maxlev_sample, kp, up)  # warm (file cache, page faults)
+            _, U, E = ops.load_operators(n, False)
+            ops.write_operator_files(d, n, U, E, False)
+        ref.fmm(x, q, n, maxlev_sample, kp, up)  # warm (file cache, page faults)
         t0 = time.perf_counter()
         for _ in range(reps):
-            ref.fmm(x, q, N_ORDER, maxlev_sample, kp, up)
+            ref.fmm(x, q, n, maxlev_sample, kp, up)
         return (time.perf_counter() - t0) / reps, cores, "reference"
-    _, U, E = ops.load_operators(N_ORDER, False)
+    _, U, E = ops.load_operators(n, False)
     orc = Oracle("d")
     t0 = time.perf_counter()
     for _ in range(reps):
-        orc.fmm(x, q, N_ORDER, maxlev_sample, U, E)
+        orc.fmm(x, q, n, maxlev_sample, U, E)
     return (time.perf_counter() - t0) / reps, 1, "port"
 
 
@@ -186,6 +186,155 @@ def run_reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ other workloads
+def _device_time(fn, steps, stream=None):
+    """Mean device time (s) of fn() over `steps` calls, CUDA events on `stream` (default:
+    torch's current stream), synchronised on both sides."""
+    import torch
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3 / steps
+
+
+def clustered_inputs(N, seed, clusters=8, sigma=0.05, lo=0.15, hi=0.85):
+    """Positions from isotropic Gaussian clusters (centres U[lo, hi]^3) clipped to [0,1)^3 and
+    shifted onto the origin-centred root cell; charges U[-1, 1]; loss weights N(0, 1)."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(lo, hi, (clusters, 3))
+    x = c[rng.integers(0, clusters, N)] + sigma * rng.standard_normal((N, 3))
+    x = np.clip(x, 0.0, np.nextafter(1.0, 0.0)) - 0.5
+    return x, rng.uniform(-1.0, 1.0, N), rng.standard_normal(N)
+
+
+def run_uniform_32k(args):
+    """N = 32,768 uniform, n = 4, maxlev 4, FP64: every potential against the FP64 direct sum,
+    the reference CPU code on the same input beside it."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.fmm import direct
+    N, n, lev = 32768, 4, 4
+    x, q = make_inputs(N, 1)
+    sol = Solver(n, lev, 1.0, mode="d")
+    sol.set_particles(x)
+    qd = torch.as_tensor(q, device="cuda")
+    out = torch.empty_like(qd)
+    stream = torch.cuda.ExternalStream(sol.stream)
+    for _ in range(args.warmup):
+        sol.solve(qd, out=out)
+    t = _device_time(lambda: sol.solve(qd, out=out), args.steps, stream)
+    qh = torch.as_tensor(q).pin_memory().numpy()
+    for _ in range(2):
+        sol.solve_host(qh)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ph = sol.solve_host(qh)
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    sol.set_timing(True)
+    sol.solve(qd, out=out)
+    torch.cuda.synchronize()
+    stages, launches = sol.stage_times()
+    ex = direct(torch.as_tensor(x, device="cuda"), qd, torch.arange(N, dtype=torch.int32, device="cuda")).cpu().numpy()
+    err = float(np.linalg.norm(ph - ex) / np.linalg.norm(ex))
+    t_ref, cores, kind = reference_sample(N, lev, reps=3, n=n) if not args.no_cpu_baseline else (None, 0, None)
+    line = {"metric": "FMM solves/s at N=32,768 uniform, n=4, depth 4, FP64", "value": 1.0 / t, "unit": "solve/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded uniform [0,1)^3, q~U[-1,1])",
+            "config": {"workload": "bbFMM Laplace 1/r, N=32,768 uniform, n=4 (r=32), maxlev 4", "N": N, "n": n,
+                       "maxlev": lev, "mode": "d", "l2": "working set fits in L2 (small configuration)"},
+            "err_vs_fp64_direct_all_targets": err, "stages_ms": stages, "gpu_launches": launches * args.steps,
+            "e2e": {"value": 1.0 / t_e2e, "unit": "solve/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
+            "cpu_baseline": None if t_ref is None else {
+                "value": 1.0 / t_ref, "unit": "solve/s", "cores": cores, "kind": kind,
+                "sample": f"the whole workload (N={N}, n={n}, maxlev {lev}), mean of 3 solves"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gradient_1m(args):
+    """N = 1,048,576 from 8 Gaussian clusters, n = 8, maxlev 6, FP32 forward: forward, and
+    forward + backward of L = sum_i w_i phi_i through fmm_phi with both ways of keeping the
+    backward's inputs (fields checkpointed, or recomputed), their saved bytes, and the
+    gradients against the FP64 direct-sum analytic gradient on 4,096 targets."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.autograd import fmm_phi
+    from bbfmm_b200.fmm import direct_field
+    N, n, lev, mode = 1_048_576, 8, 6, args.mode if args.mode != "mixed" else "s"
+    x, q, w = clustered_inputs(N, 11)
+    free0 = torch.cuda.mem_get_info()[0]
+    sol = Solver(n, lev, 1.0, mode=mode)
+    sol.set_particles(x)
+    dt = sol.dtype
+    qd = torch.as_tensor(q, dtype=dt, device="cuda")
+    xd = torch.as_tensor(x, dtype=dt, device="cuda")
+    wd = torch.as_tensor(w, dtype=dt, device="cuda")
+    out = torch.empty_like(qd)
+    stream = torch.cuda.ExternalStream(sol.stream)
+    for _ in range(args.warmup):
+        sol.solve(qd, out=out)
+    torch.cuda.synchronize()
+    solver_bytes = free0 - torch.cuda.mem_get_info()[0]
+    t_fwd = _device_time(lambda: sol.solve(qd, out=out), args.steps, stream)
+
+    res = {}
+    for save in ("fields", "recompute"):
+        def fwd_bwd():
+            qt = qd.clone().requires_grad_(True)
+            xt = xd.clone().requires_grad_(True)
+            L = (wd * fmm_phi(sol, qt, xt, save=save)).sum()
+            L.backward()
+            return qt.grad, xt.grad
+        for _ in range(args.warmup):
+            fwd_bwd()
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        base = torch.cuda.memory_allocated()
+        gq, gx = fwd_bwd()
+        torch.cuda.synchronize()
+        peak = torch.cuda.max_memory_allocated() - base
+        t = _device_time(fwd_bwd, args.steps)
+        # bytes the forward keeps for the backward
+        qt = qd.clone().requires_grad_(True)
+        xt = xd.clone().requires_grad_(True)
+        m0 = torch.cuda.memory_allocated()
+        y = fmm_phi(sol, qt, xt, save=save)
+        torch.cuda.synchronize()
+        kept = torch.cuda.memory_allocated() - m0 - y.numel() * y.element_size()
+        del y
+        res[save] = {"fwd_bwd_ms": t * 1e3, "fwd_bwd_over_fwd": t / t_fwd, "saved_bytes": int(kept),
+                     "peak_torch_bytes_fwd_bwd": int(peak)}
+        grads = (gq.double(), gx.double())
+
+    targets = np.random.default_rng(1234).choice(N, N_TARGETS, replace=False).astype(np.int32)
+    td = torch.as_tensor(targets, device="cuda")
+    x64, q64, w64 = (torch.as_tensor(a, device="cuda") for a in (x, q, w))
+    p1, f1 = direct_field(x64, q64, td)
+    p2, f2 = direct_field(x64, w64 * q64, td)
+    wt, qt_ = w64[td.long()], q64[td.long()]
+    dq = wt * p1 + p2
+    dx = qt_[:, None] * (wt[:, None] * f1 + f2)
+    gq, gx = grads
+    err_q = float(torch.linalg.norm(gq[td.long()] - dq) / torch.linalg.norm(dq))
+    err_x = float(torch.linalg.norm(gx[td.long()] - dx) / torch.linalg.norm(dx))
+    line = {"metric": "forward+backward of sum(w*phi) at N=1,048,576 clustered, n=8, depth 6",
+            "value": 1.0 / (res["fields"]["fwd_bwd_ms"] / 1e3), "unit": "fwd+bwd/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["fields"]["fwd_bwd_ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"d": "f64", "s": "f32"}[mode], "data": "synthetic (seeded 8-Gaussian mixture, sigma 0.05)",
+            "config": {"workload": "bbFMM Laplace 1/r gradients, N=1,048,576 clustered, n=8, maxlev 6", "N": N,
+                       "n": n, "maxlev": lev, "mode": mode},
+            "forward_ms": t_fwd * 1e3, "save_modes": res, "solver_device_bytes": int(solver_bytes),
+            "grad_err_vs_fp64_direct": {"dq": err_q, "dx": err_x, "n_targets": N_TARGETS}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -198,9 +347,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--N", type=int, default=N_FULL)
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
+    ap.add_argument("--workload", default="uniform-4m", choices=["uniform-4m", "uniform-32k", "gradient-1m"],
+                    help="uniform-4m: the headline line; the others measure further configurations")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "uniform-32k":
+        return run_uniform_32k(args)
+    if args.workload == "gradient-1m":
+        return run_gradient_1m(args)
 
     import torch
     import torch.distributed as dist

@@ -145,6 +145,14 @@ BBFMM_B200_API int bbfmm_b200_time_m2l(bbfmm_b200_solver *s, int level, int reps
 BBFMM_B200_API int bbfmm_b200_direct(int N, const double *xyz_dev, const double *q_dev, int ntarget,
                                      const int *targets_dev, double *out_dev, void *stream);
 
+/* FP64 direct potential and gradient at the targets, without the target-charge factor (the
+ * exact counterpart of bbfmm_b200_solve_fields): pot[t] = sum_{x_j != x_i} q_j / r_ij,
+ * field[3t + a] = sum q_j (x_j - x_i)_a / r_ij^3 for i = targets[t]; either output may be
+ * NULL. The reference has no gradient code; this is the analytic derivative of its kernel. */
+BBFMM_B200_API int bbfmm_b200_direct_field(int N, const double *xyz_dev, const double *q_dev, int ntarget,
+                                           const int *targets_dev, double *pot_dev, double *field_dev,
+                                           void *stream);
+
 /* Status word of the tensor-core kernels: 0 when every bounded wait of every launch so far
  * completed, else the code of the first wait that gave up (the launch then skipped its
  * remaining work and returned). Synchronises the device; clear != 0 resets the word. */

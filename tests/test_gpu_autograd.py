@@ -25,13 +25,13 @@ def _clustered(N, seed):
     return x, rng.uniform(-1, 1, N), rng.standard_normal(N)
 
 
-def _loss(solver, x, q, w):
+def _loss(solver, x, q, w, save="fields"):
     import torch
     from bbfmm_b200.autograd import fmm_phi
     solver.set_particles(x)
     xt = torch.as_tensor(x, device="cuda").requires_grad_(True)
     qt = torch.as_tensor(q, device="cuda").requires_grad_(True)
-    L = (torch.as_tensor(w, device="cuda") * fmm_phi(solver, qt, xt)).sum()
+    L = (torch.as_tensor(w, device="cuda") * fmm_phi(solver, qt, xt, save=save)).sum()
     return L, qt, xt
 
 
@@ -75,13 +75,13 @@ def test_gradients_match_finite_differences():
     s.close()
 
 
-@pytest.mark.parametrize("mode", ["d", "mixed"])
-def test_gradients_match_direct_sum(oracle_d, mode):
+@pytest.mark.parametrize("mode,save", [("d", "fields"), ("mixed", "fields"), ("mixed", "recompute")])
+def test_gradients_match_direct_sum(oracle_d, mode, save):
     from bbfmm_b200 import Solver
     N = 16384
     x, q, w = _clustered(N, 3)
     s = Solver(8, 3 if mode == "d" else 4, 1.0, mode=mode)
-    L, qt, xt = _loss(s, x, q, w)
+    L, qt, xt = _loss(s, x, q, w, save)
     L.backward()
     gq, gx = qt.grad.cpu().numpy(), xt.grad.cpu().numpy()
     t = np.arange(N)
@@ -94,8 +94,10 @@ def test_gradients_match_direct_sum(oracle_d, mode):
     s.close()
 
 
-def test_backward_costs_one_solve():
-    """Forward + backward = two solves of fields (the backward is one solve)."""
+@pytest.mark.parametrize("save,n_fields,n_plain", [("fields", 2, 0), ("recompute", 2, 1)])
+def test_solves_per_forward_backward(save, n_fields, n_plain):
+    """fields: forward + backward = two solves of fields (the backward is one solve);
+    recompute: one plain solve forward, two solves of fields backward."""
     import torch
     from bbfmm_b200 import Solver
     from bbfmm_b200.autograd import fmm_phi
@@ -106,9 +108,44 @@ def test_backward_costs_one_solve():
     qt = torch.as_tensor(q, device="cuda").requires_grad_(True)
     xt = torch.as_tensor(x, device="cuda").requires_grad_(True)
     wt = torch.as_tensor(w, device="cuda")
-    calls = []
-    orig = s.solve_fields
-    s.solve_fields = lambda *a, **k: (calls.append(1), orig(*a, **k))[1]
-    (wt * fmm_phi(s, qt, xt)).sum().backward()
-    assert len(calls) == 2 and qt.grad is not None and xt.grad is not None
+    calls = {"fields": 0, "plain": 0}
+    of, op = s.solve_fields, s.solve
+
+    def count(kind, f):
+        def g(*a, **k):
+            calls[kind] += 1
+            return f(*a, **k)
+        return g
+    s.solve_fields, s.solve = count("fields", of), count("plain", op)
+    (wt * fmm_phi(s, qt, xt, save=save)).sum().backward()
+    assert calls == {"fields": n_fields, "plain": n_plain}
+    assert qt.grad is not None and xt.grad is not None
     s.close()
+
+
+def test_save_modes_agree():
+    import torch
+    from bbfmm_b200 import Solver
+    x, q, w = _clustered(20000, 5)
+    s = Solver(8, 4, 1.0, mode="s")
+    grads = []
+    for save in ("fields", "recompute"):
+        L, qt, xt = _loss(s, x, q, w, save)
+        L.backward()
+        grads.append((qt.grad.cpu().numpy(), xt.grad.cpu().numpy()))
+    assert np.array_equal(grads[0][0], grads[1][0]) and np.array_equal(grads[0][1], grads[1][1])
+    s.close()
+
+
+def test_direct_field_matches_oracle(oracle_d):
+    """The GPU FP64 direct potential/gradient used for the gradient error of the N = 1M
+    benchmark agrees with the oracle's (relative L2 1e-14: summation order only)."""
+    import torch
+    from bbfmm_b200.fmm import direct_field
+    x, q, _ = _clustered(6000, 6)
+    t = np.random.default_rng(7).choice(6000, 500, replace=False).astype(np.int32)
+    pot, fld = direct_field(torch.as_tensor(x, device="cuda"), torch.as_tensor(q, device="cuda"),
+                            torch.as_tensor(t, device="cuda"))
+    p0, f0 = oracle_d.direct_field_fp64(x, q, t)
+    assert rel_l2(pot.cpu().numpy(), p0) < 1e-14
+    assert rel_l2(fld.cpu().numpy().reshape(-1), f0.reshape(-1)) < 1e-14
