@@ -51,6 +51,21 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_time_m2l.argtypes = [vp, i, i, C.POINTER(C.c_float)]
         L.bbfmm_b200_direct.argtypes = [i, vp, vp, i, vp, vp, vp]
         L.bbfmm_b200_direct_field.argtypes = [i, vp, vp, i, vp, vp, vp, vp]
+        L.bbfmm_b200_autotune.argtypes = [vp, vp]
+        L.bbfmm_b200_set_tc_products.argtypes = [vp, i]
+        L.bbfmm_b200_set_leaf_slab.argtypes = [vp, C.c_longlong]
+        L.bbfmm_b200_tuning.argtypes = [vp, ip]
+        L.bbfmm_b200_batch_create.argtypes = [C.POINTER(Config), i, ip, ip, ip, vp, vp, vp, vp, vp, i, C.POINTER(vp)]
+        L.bbfmm_b200_batch_solve.argtypes = [vp, vp, vp, i]
+        L.bbfmm_b200_batch_autotune.argtypes = [vp, vp]
+        L.bbfmm_b200_batch_groups.argtypes = [vp]
+        L.bbfmm_b200_batch_graph_nodes.argtypes = [vp]
+        L.bbfmm_b200_batch_graph_nodes.restype = C.c_longlong
+        L.bbfmm_b200_batch_group_info.argtypes = [vp, i, ip]
+        L.bbfmm_b200_batch_stream.argtypes = [vp]
+        L.bbfmm_b200_batch_stream.restype = vp
+        L.bbfmm_b200_batch_destroy.argtypes = [vp]
+        L.bbfmm_b200_batch_destroy.restype = None
         L.bbfmm_b200_device_status.argtypes = [i]
         L.bbfmm_b200_near_field.argtypes = [i, i, d, vp, vp, vp, i, vp]
         L.bbfmm_b200_near_field_noalloc.argtypes = [i, i, d, vp, vp, vp, i, vp]

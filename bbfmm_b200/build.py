@@ -34,6 +34,7 @@ UNITS = [
     ("direct.cu", [], "direct"),
     ("solver.cu", [], "solver"),
     ("reference_abi.cu", [], "reference_abi"),
+    ("batch.cu", [], "batch"),
 ]
 
 

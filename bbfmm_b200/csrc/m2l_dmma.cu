@@ -10,7 +10,7 @@
 // E[k][j][i] (K file, bbfmm.c:1384-1405), so both global reads are contiguous. Tiles are
 // double-buffered with cp.async; 8 warps in a 2 x 4 grid each own a 32-target x 64-output
 // accumulator (4 x 8 fragments of 8x8); warps whose outputs lie beyond ni skip the math.
-#include "common.cuh"
+#include "solver.cuh"
 
 namespace bbfmm {
 
@@ -64,12 +64,12 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   const int og = blockIdx.y, ng = gridDim.y;
   const int o0 = (189 * og) / ng, o1 = (189 * (og + 1)) / ng;
   const int niter = (o1 - o0) * nchunk;
-  Lout += (int64_t)og * 8 * P3 * R;
+  Lout += (int64_t)og * (gridDim.x / tiles_per_class) * P3 * R;  // all classes of all sets
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
 
   auto issue = [&](int it, int buf) {
     const int o = o0 + it / nchunk, jc = j0 + (it % nchunk) * BK;
-    const int4 ov = offs[c * 189 + o];
+    const int4 ov = offs[(c & 7) * 189 + o];
     const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
     const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
     const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
       const int t = e / BK, jj = e % BK;
       const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
       const bool ok = t < nt && jc + jj < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
-      const double *src = ok ? M + ((int64_t)sc * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + jj : M;
+      const double *src = ok ? M + ((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + jj : M;
       cp_async8(sa + (uint32_t)(jj * AST + t) * 8u, src, ok);
     }
     // B: 16 rows j of E_k (the first nb outputs i), 16-byte copies
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
   auto issue = [&](int it) {
     if (it < niter) {
       const int o = it / nchunk, jc = (it % nchunk) * lead::BK;
-      const int4 ov = offs[c * 189 + o];
+      const int4 ov = offs[(c & 7) * 189 + o];
       const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
       const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
       const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
         const int t = e / (lead::BK / 2), j2 = (e % (lead::BK / 2)) * 2;
         const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
         const bool ok = t < nt && jc + j2 < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
-        const double *src = ok ? M + ((int64_t)sc * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + j2 : M;
+        const double *src = ok ? M + ((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + j2 : M;
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa + (uint32_t)(t * lead::AST + j2) * 8u),
                      "l"(src), "r"(ok ? 16 : 0)
                      : "memory");
@@ -249,17 +249,39 @@ __global__ void sum_parts_kernel(int64_t count, int ng, const double *__restrict
 
 }  // namespace dm
 
+// Target tiles (CTAs) of the full FP64 M2L of one level.
+static int64_t dmma_tiles(int level, int nsets) {
+  const int P = 1 << (level - 1);
+  const int bw = P < 4 ? P : 4;
+  const int nbox = P / bw;
+  return 8 * (int64_t)nsets * nbox * nbox * nbox;
+}
+
+// Offset groups (CTAs per target tile) that fill about two waves of the 148 SMs.
+int dmma_default_groups(int level, int nsets) {
+  const int64_t tiles = dmma_tiles(level, nsets);
+  int64_t g = (2 * 148 + tiles - 1) / tiles;
+  return (int)(g < 1 ? 1 : (g > DMMA_PARTS ? DMMA_PARTS : g));
+}
+
+// Doubles of partial-sum scratch a level needs with `groups` offset groups (0 when 1).
+int64_t dmma_part_elems(int level, int nsets, int groups, int r) {
+  return groups > 1 ? (int64_t)groups * nsets * pow8i(level) * r : 0;
+}
+
 // Writes Lout[cell][0:ni) for every cell of the level (assign); entries i >= ni untouched.
-// part: scratch of 21 x 8^level x r doubles for levels <= 3 (or null: single pass).
+// The full M2L (ni = r) may split the 189 offsets into `ngroups` CTAs per target tile
+// (0: dmma_default_groups) whose partials go to `part` (part_elems doubles) and are then
+// summed in a fixed order; with too little scratch the groups are reduced to fit.
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
-                    const int4 *offs, double *part, cudaStream_t s) {
+                    const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets, int ngroups) {
   if (r != dm::R) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "FP64 tensor M2L is built for r = 256");
   if (j0 < 0 || j1 > r || j0 >= j1 || ni < 2 || ni > r || ni % 2)
     return bbfmm_set_error(BBFMM_ERR_ARG, "bad contraction / output range");
   const int P = 1 << (level - 1);
   const int bw = P < 4 ? P : 4;
   const int nbox = P / bw;
-  const int grid = 8 * nbox * nbox * nbox;
+  const int grid = 8 * nsets * nbox * nbox * nbox;
   if (j0 == 0 && j1 <= 64 && (ni == 32 || ni == 64)) {  // the FP64 leading block
     static bool lattr = false;
     if (!lattr) {
@@ -280,10 +302,13 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma smem attribute", __FILE__, __LINE__);
     attr = true;
   }
-  if (level <= 3 && part) {
-    // few target tiles: spread the offsets over 21 CTAs per tile, then sum the partials
-    const int ng = 21;
-    const int64_t count = 8 * (int64_t)P * P * P * r;
+  int ng = ngroups > 0 ? ngroups : dmma_default_groups(level, nsets);
+  if (ng > DMMA_PARTS) ng = DMMA_PARTS;
+  const int64_t count = 8 * (int64_t)nsets * P * P * P * r;
+  if (!part) ng = 1;
+  else if ((int64_t)ng * count > part_elems) ng = (int)(part_elems / count);
+  if (ng > 1) {
+    // few target tiles: spread the offsets over ng CTAs per tile, then sum the partials
     dm::m2l_dmma_kernel<<<dim3(grid, ng), 256, dm::SMEM_BYTES, s>>>(M, Ecol, part, level, j0, j1, ni, offs);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma", __FILE__, __LINE__);

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, 
     for (int b = 0; b < TN; ++b) acc[a][b] = 0;
   const int64_t P3 = (int64_t)P * P * P;
   for (int o = 0; o < 189; ++o) {
-    const int4 ov = offs[c * 189 + o];
+    const int4 ov = offs[(c & 7) * 189 + o];
     const int k = ov.x;
     // source class and parent-grid shift for this class/offset
     const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, 
         if (t < nt && jc + jj < j1) {
           const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
           if (px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P)
-            v = M[(((int64_t)sc * P3 + ((int64_t)pz * P + py) * P + px)) * R + jc + jj];
+            v = M[(((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px)) * R + jc + jj];
         }
         sa[jj][t] = v;
       }
@@ -116,8 +116,8 @@ int m2l_simt_tiles(int level) {
 
 template <typename T>
 int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs,
-                    int accumulate, cudaStream_t s) {
-  const int grid = m2l_simt_tiles(level);
+                    int accumulate, cudaStream_t s, int nsets) {
+  const int grid = nsets * m2l_simt_tiles(level);  // the class index runs over all sets' 8 classes
   if (r == 256) {
     m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, Lout, level, j0, j1, offs, accumulate);
   } else if (r == 32) {
@@ -129,9 +129,9 @@ int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0,
 }
 
 template int launch_m2l_simt<double>(int, const double *, const double *, double *, int, int, int, const int4 *, int,
-                                     cudaStream_t);
+                                     cudaStream_t, int);
 template int launch_m2l_simt<float>(int, const float *, const float *, float *, int, int, int, const int4 *, int,
-                                    cudaStream_t);
+                                    cudaStream_t, int);
 
 // Host table of the 189 offsets of each sibling class, as (k, vx, vy, vz).
 void build_offset_table(int *out /* 8*189*4 */) {

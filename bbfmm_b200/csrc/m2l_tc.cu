@@ -148,7 +148,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 __global__ void __launch_bounds__(192, 1)
     m2l_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
-                  double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead) {
+                  double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
+                  int nprod) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -202,17 +203,20 @@ __global__ void __launch_bounds__(192, 1)
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
       if (!mbar_wait(empty_bar(s), ph ^ 1u, 1)) break;
       const int o = it / used_chunks, kc = chunk0 + it % used_chunks;
-      const int4 ov = offs[c * 189 + o];
+      const int4 ov = offs[(c & 7) * 189 + o];
       const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
       const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
       const int sc = (scx << 2) | (scy << 1) | scz;
       const int sx = bx0 + (gx - scx) / 2, sy = by0 + (gy - scy) / 2, sz = bz0 + (gz - scz) / 2;
       const uint32_t st = base + s * STAGE_BYTES;
-      mbar_expect_tx(full_bar(s), STAGE_BYTES);
-      tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, sc);
-      tma_load_5d(st + A_BYTES, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, sc);
+      // one product (hi x hi) needs only the hi halves of A and B
+      mbar_expect_tx(full_bar(s), nprod == 1 ? A_BYTES + B_BYTES : STAGE_BYTES);
+      tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
       tma_load_3d(st + 2 * A_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
-      tma_load_3d(st + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
+      if (nprod != 1) {
+        tma_load_5d(st + A_BYTES, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
+        tma_load_3d(st + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
@@ -229,8 +233,10 @@ __global__ void __launch_bounds__(192, 1)
         const uint64_t bhi = sw128_desc(st + 2 * A_BYTES + ks * 32);
         const uint64_t blo = sw128_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
         mma_bf16(tmem, ahi, bhi, acc);
-        mma_bf16(tmem, ahi, blo, 1u);
-        mma_bf16(tmem, alo, bhi, 1u);
+        if (nprod != 1) {
+          mma_bf16(tmem, ahi, blo, 1u);
+          mma_bf16(tmem, alo, bhi, 1u);
+        }
         acc = 1u;
       }
       mma_commit(empty_bar(s));
@@ -388,15 +394,17 @@ int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *M
 }
 
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
-                  int level, const int4 *offs, cudaStream_t s) {
+                  int level, const int4 *offs, cudaStream_t s, int nsets, int nprod) {
   const TcOps *ops = (const TcOps *)opsv;
+  if (nprod != 1 && nprod != 3) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 1 or 3");
   if (!ops || r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L needs r = 256 operators");
   const int P = 1 << (level - 1);
   if (P < tc::BOX_X) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs level >= 4");
   const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Msplit + (size_t)cell_offset * r;
   const __nv_bfloat16 *lo = (const __nv_bfloat16 *)Msplit + (size_t)(ncell_total + cell_offset) * r;
   CUtensorMap mapAhi, mapAlo;
-  const cuuint64_t dims[5] = {(cuuint64_t)r, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)P, 8};
+  // the class dimension runs over the 8 sibling classes of every stacked set
+  const cuuint64_t dims[5] = {(cuuint64_t)r, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)8 * nsets};
   const cuuint64_t strides[4] = {(cuuint64_t)r * 2, (cuuint64_t)r * 2 * P, (cuuint64_t)r * 2 * P * P,
                                  (cuuint64_t)r * 2 * P * P * P};
   const cuuint32_t box[5] = {tc::BK, tc::BOX_X, tc::BOX_Y, tc::BOX_Z, 1};
@@ -409,12 +417,12 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc smem attribute", __FILE__, __LINE__);
     attr = true;
   }
-  const int tiles = 8 * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
+  const int tiles = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
   // with a full-width leading strip its K-steps are skipped; otherwise every K-step runs
   const int kfirst = ops->lead_rows >= r ? ops->lead / 16 : 0;
   const int ilead = ops->lead > 0 ? ops->lead_rows : 0;
   tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo, Lacc, level, offs,
-                                                       kfirst, ilead);
+                                                       kfirst, ilead, nprod);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc", __FILE__, __LINE__);
 }
 

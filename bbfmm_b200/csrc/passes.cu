@@ -41,7 +41,8 @@ template <> __device__ __forceinline__ const float *tab_cw<float>(const Tables &
 // S_leaf[m * n3 + l], Morton order at maxlev.
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
-                                                  int maxlev, T L, Tables tabs, T *__restrict__ S) {
+                                                  int maxlev, T L, Tables tabs, T *__restrict__ S, int64_t m0,
+                                                  int64_t count) {
   constexpr int N3 = NN * NN * NN;
   constexpr int PER = (N3 + 31) / 32;
   __shared__ T s_tkz[NN * NN];
@@ -49,16 +50,16 @@ __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, co
   for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int64_t nleaf = pow8i(maxlev);
   const T len = cell_length<T>(maxlev, L);
   const T ihalf = (T)1 / (len / (T)2);
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t m = warp; m < nleaf; m += nwarps) {
+  for (int64_t mm = warp; mm < count; mm += nwarps) {
+    const int64_t m = m0 + mm;  // leaf; S holds leaves m0 .. m0 + count - 1
     int ix, iy, iz;
-    morton_to_grid(m, maxlev, ix, iy, iz);
+    morton_to_grid(m, maxlev, ix, iy, iz);  // the set index above bit 3 maxlev is ignored
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
     T acc[PER];
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, co
         }
       }
     }
-    T *out = S + m * N3;
+    T *out = S + mm * N3;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
       const int l = lane + 32 * k;
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, co
 // 8 n^3) -> parent S (level l). All eight children are visited.
 template <typename T, int NN>
 __global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *__restrict__ Sp, int level,
-                                                  Tables tabs) {
+                                                  Tables tabs, int64_t A0, int64_t count) {
   constexpr int N2 = NN * NN, N3 = N2 * NN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sc = reinterpret_cast<T *>(smem_raw);  // 8 * N3
@@ -109,10 +110,10 @@ __global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *_
   for (int i = threadIdx.x; i < 2 * N2; i += blockDim.x) cw[i] = cwg[i];
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
-  const int64_t ncell = pow8i(level);
-  for (int64_t A = blockIdx.x; A < ncell; A += gridDim.x) {
+  for (int64_t a = blockIdx.x; a < count; a += gridDim.x) {
+    const int64_t A = A0 + a;  // parent; Sc holds the children of parents A0 .. A0 + count - 1
     __syncthreads();
-    const T *src = Sc + A * 8 * N3;
+    const T *src = Sc + a * 8 * N3;
     for (int i = threadIdx.x; i < 8 * N3; i += blockDim.x) sc[i] = src[i];
     __syncthreads();
     // z: sz[(j/2) n3 + l1 n + l3] = sum over zbit of sum_m child_j[l1 n + m] C[zbit][l3][m]
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *_
 // One CTA per parent: F_child[j] += (2/n)^3 * interp_j(F_parent), children contiguous.
 template <typename T, int NN>
 __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *__restrict__ Fc, int level,
-                                                  Tables tabs) {
+                                                  Tables tabs, int64_t A0, int64_t count) {
   constexpr int N2 = NN * NN, N3 = N2 * NN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *fp = reinterpret_cast<T *>(smem_raw);  // N3
@@ -180,8 +181,8 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
   for (int i = threadIdx.x; i < 2 * N2; i += blockDim.x) cw[i] = cwg[i];
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
-  const int64_t ncell = pow8i(level);
-  for (int64_t A = blockIdx.x; A < ncell; A += gridDim.x) {
+  for (int64_t a = blockIdx.x; a < count; a += gridDim.x) {
+    const int64_t A = A0 + a;  // parent; Fc holds the children of parents A0 .. A0 + count - 1
     __syncthreads();
     for (int i = threadIdx.x; i < N3; i += blockDim.x) fp[i] = Fp[A * N3 + i];
     __syncthreads();
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
       T s = 0;
 #pragma unroll
       for (int m = 0; m < NN; ++m) s += fy[(j / 2) * N3 + l12 * NN + m] * cw[(j % 2) * N2 + m * NN + l3];
-      Fc[(A * 8 + j) * N3 + rem] += pre3 * s;
+      Fc[(a * 8 + j) * N3 + rem] += pre3 * s;
     }
   }
 }
@@ -219,28 +220,28 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   int maxlev, T L, Tables tabs, const T *__restrict__ F,
-                                                  T *__restrict__ phi) {
+                                                  T *__restrict__ phi, int64_t m0, int64_t count) {
   constexpr int N2 = NN * NN, N3 = N2 * NN;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
   for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int64_t nleaf = pow8i(maxlev);
   const T len = cell_length<T>(maxlev, L);
   const T ihalf = (T)1 / (len / (T)2);
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t m = warp; m < nleaf; m += nwarps) {
+  for (int64_t mm = warp; mm < count; mm += nwarps) {
+    const int64_t m = m0 + mm;  // leaf; F holds leaves m0 .. m0 + count - 1
     const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
     if (p1 == p0) continue;
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
-    const T *Fm = F + m * N3;
+    const T *Fm = F + mm * N3;
     for (int p = p0; p < p1; ++p) {
       const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
       const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
@@ -272,11 +273,14 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
 // where rows are mapped between Morton and cpg order at the given level.
 // A may be the sum of two sources (T and float) for the split M2L output.
 // Register-blocked SIMT GEMM: CTA tile 128 x BN, K-chunks of 16, 256 threads.
-__device__ __forceinline__ int64_t map_row(int64_t m, int level, int which, int mode) {
+// Local row m of a slab starting at cell row0: its cpg index when `which` is the mapped
+// side, else m itself.
+__device__ __forceinline__ int64_t map_row(int64_t m, int64_t row0, int level, int which, int mode) {
   if (mode == which) {
+    m += row0;
     int ix, iy, iz;
     morton_to_grid(m, level, ix, iy, iz);
-    return grid_to_cpg(ix, iy, iz, level);
+    return (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);  // set base + in-set index
   }
   return m;
 }
@@ -285,7 +289,7 @@ template <typename T, int BN>
 __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N, const T *__restrict__ A,
                                                         const float *__restrict__ A2, const T *__restrict__ B,
                                                         const T *__restrict__ cs, T scale, T *__restrict__ C,
-                                                        int level, int mapmode) {
+                                                        int level, int mapmode, int64_t row0) {
   constexpr int BM = 128, BK = 16, TN = BN / 16;
   __shared__ T sa[BK][BM + 1];
   __shared__ T sb[BK][BN];
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N,
       const int64_t m = m0 + r;
       T v = 0;
       if (m < M && k0 + c < K) {
-        const int64_t ar = map_row(m, level, MAP_IN_CPG, mapmode);
+        const int64_t ar = map_row(m, row0, level, MAP_IN_CPG, mapmode);
         v = A[ar * K + k0 + c];
         if (A2) v += (T)A2[ar * K + k0 + c];
       }
@@ -333,7 +337,7 @@ __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N,
   for (int i = 0; i < 8; ++i) {
     const int64_t m = m0 + ty * 8 + i;
     if (m >= M) continue;
-    const int64_t cr = map_row(m, level, MAP_OUT_CPG, mapmode);
+    const int64_t cr = map_row(m, row0, level, MAP_OUT_CPG, mapmode);
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
       const int n = n0 + tx + 16 * j;
@@ -388,63 +392,73 @@ static int grid_for(int64_t work, int per_block, int cap) {
 }
 
 template <typename T>
-int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s) {
-  const int64_t nleaf = pow8i(maxlev);
-  const int grid = grid_for(nleaf, 4, 148 * 64);
-  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S);
-  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S);
+int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s,
+               int nsets, int64_t first, int64_t count) {
+  if (count < 0) count = nsets * pow8i(maxlev) - first;
+  if (count <= 0) return BBFMM_OK;
+  const int grid = grid_for(count, 4, 148 * 64);
+  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count);
+  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2m", __FILE__, __LINE__);
 }
 
 template <typename T>
-int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s) {
+int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s, int nsets, int64_t first,
+               int64_t count) {
   const int n3 = n * n * n;
   const size_t smem = sizeof(T) * 14 * n3;
-  const int grid = grid_for(pow8i(level), 1, 148 * 8);
+  if (count < 0) count = nsets * pow8i(level) - first;
+  if (count <= 0) return BBFMM_OK;
+  const int grid = grid_for(count, 1, 148 * 8);
   if (n == 4) {
-    m2m_kernel<T, 4><<<grid, 256, smem, s>>>(Sc, Sp, level, t);
+    m2m_kernel<T, 4><<<grid, 256, smem, s>>>(Sc, Sp, level, t, first, count);
   } else if (n == 8) {
     cudaFuncSetAttribute(m2m_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    m2m_kernel<T, 8><<<grid, 256, smem, s>>>(Sc, Sp, level, t);
+    m2m_kernel<T, 8><<<grid, 256, smem, s>>>(Sc, Sp, level, t, first, count);
   } else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2m", __FILE__, __LINE__);
 }
 
 template <typename T>
-int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s) {
+int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets, int64_t first,
+               int64_t count) {
   const int n3 = n * n * n;
   const size_t smem = sizeof(T) * 7 * n3;
-  const int grid = grid_for(pow8i(level), 1, 148 * 8);
+  if (count < 0) count = nsets * pow8i(level) - first;
+  if (count <= 0) return BBFMM_OK;
+  const int grid = grid_for(count, 1, 148 * 8);
   if (n == 4) {
-    l2l_kernel<T, 4><<<grid, 256, smem, s>>>(Fp, Fc, level, t);
+    l2l_kernel<T, 4><<<grid, 256, smem, s>>>(Fp, Fc, level, t, first, count);
   } else if (n == 8) {
     cudaFuncSetAttribute(l2l_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    l2l_kernel<T, 8><<<grid, 256, smem, s>>>(Fp, Fc, level, t);
+    l2l_kernel<T, 8><<<grid, 256, smem, s>>>(Fp, Fc, level, t, first, count);
   } else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2l", __FILE__, __LINE__);
 }
 
 template <typename T>
 int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi,
-               cudaStream_t s) {
-  const int grid = grid_for(pow8i(maxlev), 4, 148 * 64);
-  if (n == 4) l2p_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi);
-  else if (n == 8) l2p_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi);
+               cudaStream_t s, int nsets, int64_t first, int64_t count) {
+  if (count < 0) count = nsets * pow8i(maxlev) - first;
+  if (count <= 0) return BBFMM_OK;
+  const int grid = grid_for(count, 4, 148 * 64);
+  if (n == 4) l2p_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi, first, count);
+  else if (n == 8) l2p_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi, first, count);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p", __FILE__, __LINE__);
 }
 
 template <typename T>
 int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C,
-                int level, int mapmode, cudaStream_t s) {
+                int level, int mapmode, cudaStream_t s, int64_t row0) {
   if (M <= 0) return BBFMM_OK;
   if (N >= 64) {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 63) / 64));
-    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode);
+    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0);
   } else {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 31) / 32));
-    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode);
+    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0);
   }
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj", __FILE__, __LINE__);
 }
@@ -470,13 +484,14 @@ int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaS
 }
 
 #define INST(T)                                                                                           \
-  template int launch_p2m<T>(int, const T *, const int *, int, T, const Tables &, T *, cudaStream_t);      \
-  template int launch_m2m<T>(int, const T *, T *, int, const Tables &, cudaStream_t);                      \
-  template int launch_l2l<T>(int, const T *, T *, int, const Tables &, cudaStream_t);                      \
+  template int launch_p2m<T>(int, const T *, const int *, int, T, const Tables &, T *, cudaStream_t, int,   \
+                             int64_t, int64_t);                                                            \
+  template int launch_m2m<T>(int, const T *, T *, int, const Tables &, cudaStream_t, int, int64_t, int64_t); \
+  template int launch_l2l<T>(int, const T *, T *, int, const Tables &, cudaStream_t, int, int64_t, int64_t); \
   template int launch_l2p<T>(int, const T *, const int *, int, T, const Tables &, const T *, T *,          \
-                             cudaStream_t);                                                                \
+                             cudaStream_t, int, int64_t, int64_t);                                         \
   template int launch_proj<T>(int64_t, int, int, const T *, const float *, const T *, const T *, T, T *,   \
-                              int, int, cudaStream_t);                                                     \
+                              int, int, cudaStream_t, int64_t);                                            \
   template int launch_morton_cpg<T>(int, int, const T *, T *, int, cudaStream_t);
 INST(float)
 INST(double)
@@ -517,28 +532,29 @@ __device__ __forceinline__ void sn_nodes_d(const T *__restrict__ tkz, T x, T *ou
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                         int maxlev, T L, Tables tabs, const T *__restrict__ F,
-                                                        T *__restrict__ pot, T *__restrict__ fld) {
+                                                        T *__restrict__ pot, T *__restrict__ fld, int64_t m0,
+                                                        int64_t count) {
   constexpr int N2 = NN * NN, N3 = N2 * NN;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
   for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int64_t nleaf = pow8i(maxlev);
   const T len = cell_length<T>(maxlev, L);
   const T ihalf = (T)1 / (len / (T)2);
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t m = warp; m < nleaf; m += nwarps) {
+  for (int64_t mm = warp; mm < count; mm += nwarps) {
+    const int64_t m = m0 + mm;  // leaf; F holds leaves m0 .. m0 + count - 1
     const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
     if (p1 == p0) continue;
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
-    const T *Fm = F + m * N3;
+    const T *Fm = F + mm * N3;
     for (int p = p0; p < p1; ++p) {
       const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
       const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
@@ -596,10 +612,13 @@ __global__ void scatter_field_kernel(int N, const int *__restrict__ perm, const 
 
 template <typename T>
 int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F,
-                     T *pot, T *fld, cudaStream_t s) {
-  const int grid = grid_for(pow8i(maxlev), 4, 148 * 64);
-  if (n == 4) l2p_field_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld);
-  else if (n == 8) l2p_field_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld);
+                     T *pot, T *fld, cudaStream_t s, int nsets, int64_t first, int64_t count) {
+  if (count < 0) count = nsets * pow8i(maxlev) - first;
+  if (count <= 0) return BBFMM_OK;
+  const int grid = grid_for(count, 4, 148 * 64);
+  if (n == 4) l2p_field_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
+  else if (n == 8)
+    l2p_field_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p_field", __FILE__, __LINE__);
 }
@@ -613,9 +632,9 @@ int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO 
 }
 
 template int launch_l2p_field<double>(int, const double *, const int *, int, double, const Tables &, const double *,
-                                      double *, double *, cudaStream_t);
+                                      double *, double *, cudaStream_t, int, int64_t, int64_t);
 template int launch_l2p_field<float>(int, const float *, const int *, int, float, const Tables &, const float *,
-                                     float *, float *, cudaStream_t);
+                                     float *, float *, cudaStream_t, int, int64_t, int64_t);
 template int launch_scatter_field<double, double>(int, const int *, const double *, const double *, double *,
                                                   double *, cudaStream_t);
 template int launch_scatter_field<float, float>(int, const int *, const float *, const float *, float *, float *,

@@ -30,17 +30,20 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ int64_t remap(int64_t m, int level, bool to_cpg) {
+// Local row m of a slab starting at cell row0: its cpg index (to_cpg) or m itself.
+__device__ __forceinline__ int64_t remap(int64_t m, int64_t row0, int level, bool to_cpg) {
   if (!to_cpg) return m;
+  m += row0;
   int ix, iy, iz;
   morton_to_grid(m, level, ix, iy, iz);
-  return grid_to_cpg(ix, iy, iz, level);
+  return (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);  // set base + in-set index
 }
 
 __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int N, const double *__restrict__ A,
                                                            const double *__restrict__ B,
                                                            const double *__restrict__ cs, double scale,
-                                                           double *__restrict__ C, int level, int mapmode) {
+                                                           double *__restrict__ C, int level, int mapmode,
+                                                           int64_t row0) {
   extern __shared__ __align__(16) double smem[];
   __shared__ int64_t arow[BM];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -51,7 +54,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
   const int nk = K / BK;
   if (tid < BM) {
     const int64_t m = m0 + tid;
-    arow[tid] = m < M ? remap(m, level, mapmode == MAP_IN_CPG) : -1;
+    arow[tid] = m < M ? remap(m, row0, level, mapmode == MAP_IN_CPG) : -1;
   }
   __syncthreads();
 
@@ -108,7 +111,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
   for (int mf = 0; mf < 4; ++mf) {
     const int64_t m = m0 + wm * 32 + mf * 8 + (lane >> 2);
     if (m >= M) continue;
-    double *dst = C + remap(m, level, mapmode == MAP_OUT_CPG) * N;
+    double *dst = C + remap(m, row0, level, mapmode == MAP_OUT_CPG) * N;
 #pragma unroll
     for (int nf = 0; nf < 8; ++nf) {
       const int n = n0 + wn * 64 + nf * 8 + 2 * (lane & 3);
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
 // Returns BBFMM_ERR_UNSUPPORTED (without recording an error) when the shape does not fit
 // the tile (K % 16, N % 256); the caller then uses the CUDA-core GEMM.
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
-                     double *C, int level, int mapmode, cudaStream_t s) {
+                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0) {
   if (K % pj::BK || N % pj::BN) return BBFMM_ERR_UNSUPPORTED;
   if (M <= 0) return BBFMM_OK;
   static bool attr = false;
@@ -134,7 +137,7 @@ int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, 
     attr = true;
   }
   dim3 grid((unsigned)((M + pj::BM - 1) / pj::BM), (unsigned)(N / pj::BN));
-  pj::proj_dmma_kernel<<<grid, 256, pj::SMEM_BYTES, s>>>(M, K, N, A, B, cs, scale, C, level, mapmode);
+  pj::proj_dmma_kernel<<<grid, 256, pj::SMEM_BYTES, s>>>(M, K, N, A, B, cs, scale, C, level, mapmode, row0);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_dmma", __FILE__, __LINE__);
 }
 

@@ -74,6 +74,8 @@ int make_solver(Solver<T> &s, int n, int maxlev, double L0, const T *Tkz, const 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
   TRY(s.init(n, maxlev, L0, mode_of<T>(), 0, 0, dev, nullptr));
+  // the reference's arrays hold whole levels (fieldval, proxysval): no leaf slabs
+  s.slab_request = (int64_t)1 << 62;
   // the caller's tables where given (the reference passes ComputeWeights' output), else ours
   std::vector<T> tkz(n * n), kw(n * n * n), cw(2 * n * n);
   std::vector<int> kt(343);

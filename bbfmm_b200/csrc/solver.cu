@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -146,7 +148,7 @@ int Solver<T>::set_operators(const T *U, const T *E) {
   BBFMM_CUDA_OK(cudaMemcpy(Ert, ert.data(), sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(Ecol, E, sizeof(T) * ert.size(), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaDeviceSynchronize());
-  if (mode == MODE_MIXED) {
+  if (mode == MODE_MIXED && r == 256) {  // r = 32 (n = 4): the M2L stays in FP64 on CUDA cores
     if (!tc_supported()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "mixed mode needs an sm_100 GPU");
     if (tcops) tc_free_operators(tcops);
     tcops = nullptr;
@@ -157,11 +159,56 @@ int Solver<T>::set_operators(const T *U, const T *E) {
 }
 
 template <typename T>
+int Solver<T>::share_operators(const Solver<T> &o) {
+  if (o.n != n || o.mode != mode || o.lead != lead || o.lead_rows != lead_rows || o.device != device)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "operators can only be shared between solvers of the same n and mode");
+  if (!o.Ert || !o.kw) return bbfmm_set_error(BBFMM_ERR_STATE, "the sharing solver has no operators");
+  if (own_ops) {
+    void *mine[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol};
+    for (void *p : mine)
+      if (p) cudaFree(p);
+    if (tcops) tc_free_operators(tcops);
+  }
+  tkz = o.tkz; cw = o.cw; kw = o.kw; Ert = o.Ert; Ecol = o.Ecol; Bup = o.Bup; Bdn = o.Bdn; kwcol = o.kwcol;
+  tcops = o.tcops;
+  own_ops = false;
+  return BBFMM_OK;
+}
+
+// Partial-sum scratch of the offset-group FP64 M2L for the current tuning.
+template <typename T>
+int Solver<T>::alloc_partials() {
+  int64_t need = 0;
+  if (sizeof(T) == 8 && r == 256)
+    for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
+      const bool tc = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
+      if (tc) continue;
+      const int g = tune.m2l_groups[l] > 0 ? tune.m2l_groups[l] : dmma_default_groups(l, nsets);
+      const int64_t e = dmma_part_elems(l, nsets, g, r);
+      if (e > need) need = e;
+    }
+  if (need <= Lpart_elems && (need == 0 || Lpart)) return BBFMM_OK;
+  if (Lpart) cudaFree(Lpart);
+  Lpart = nullptr;
+  Lpart_elems = 0;
+  if (need > 0) {
+    TRY(dalloc(&Lpart, (size_t)need));
+    Lpart_elems = need;
+  }
+  return BBFMM_OK;
+}
+
+template <typename T>
 int Solver<T>::alloc_work() {
-  const int64_t nl = pow8i(maxlev);
+  const int64_t nl = cells(maxlev);
+  const int64_t cell_bytes = (int64_t)n3 * sizeof(T);
+  if (slab_request > 0) slab = slab_request;
+  else slab = nl * cell_bytes > ((int64_t)16 << 30) ? ((((int64_t)16 << 30) / cell_bytes) & ~(int64_t)63) : 0;
   int64_t smax[2] = {0, 0};
-  for (int l = BBFMM_MINLEV; l <= maxlev; ++l)
-    if (pow8i(l) > smax[l & 1]) smax[l & 1] = pow8i(l);
+  for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
+    const int64_t c = l == maxlev ? leaf_slab() : cells(l);
+    if (c > smax[l & 1]) smax[l & 1] = c;
+  }
   for (int b = 0; b < 2; ++b) {
     if (S[b]) cudaFree(S[b]);
     if (F[b]) cudaFree(F[b]);
@@ -172,16 +219,14 @@ int Solver<T>::alloc_work() {
   int64_t tot = 0;
   for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
     Moff[l] = tot;
-    tot += pow8i(l) * r;
+    tot += cells(l) * r;
   }
   if (Mall) cudaFree(Mall);
   TRY(dalloc(&Mall, (size_t)tot));
   if (Lbuf) cudaFree(Lbuf);
   TRY(dalloc(&Lbuf, (size_t)nl * r));
-  if (Lpart) cudaFree(Lpart);
-  Lpart = nullptr;
-  if (sizeof(T) == 8 && r == 256) TRY(dalloc(&Lpart, (size_t)DMMA_PARTS * pow8i(maxlev < 3 ? maxlev : 3) * r));
-  if (mode == MODE_MIXED) {
+  TRY(alloc_partials());
+  if (mode == MODE_MIXED && r == 256) {
     if (Msplit) cudaFree(Msplit);
     unsigned char *p = nullptr;
     TRY(dalloc(&p, tc_split_bytes(r, tot / r)));
@@ -192,25 +237,33 @@ int Solver<T>::alloc_work() {
 
 template <typename T>
 int Solver<T>::set_particles_sorted(int N_, const int *perm_h, const int *leaf_start_h, const T *xyz_h) {
-  const int64_t nl = pow8i(maxlev);
+  return set_particles_global(1, N_, perm_h, leaf_start_h, N_, xyz_h);
+}
+
+template <typename T>
+int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const int *leaf_start_h, int Nxyz,
+                                    const T *xyz_h) {
+  if (nsets_ < 1 || nsets_ * pow8i(maxlev) > (int64_t)1 << 30)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "number of stacked sets out of range");
+  nsets = nsets_;
+  const int64_t nl = cells(maxlev);
   if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(leafm); cudaFree(pos4); cudaFree(phis); }
-  if (loc4) cudaFree(loc4);
-  perm = leaf_start = leafm = nullptr; pos4 = phis = nullptr; loc4 = nullptr;
+  if (flds) cudaFree(flds);  // sized 3 N: reallocated by the next solve_fields
+  perm = leaf_start = leafm = nullptr; pos4 = phis = flds = nullptr;
   N = N_;
   TRY(dalloc(&perm, N > 0 ? N : 1));
   TRY(dalloc(&leaf_start, nl + 1));
   TRY(dalloc(&leafm, N > 0 ? N : 1));
   TRY(dalloc(&pos4, 4 * (size_t)(N > 0 ? N : 1)));
   TRY(dalloc(&phis, N > 0 ? N : 1));
-  if (mode == MODE_MIXED) TRY(dalloc(&loc4, N > 0 ? N : 1));
   if (N > 0) BBFMM_CUDA_OK(cudaMemcpy(perm, perm_h, sizeof(int) * N, cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(leaf_start, leaf_start_h, sizeof(int) * (nl + 1), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaDeviceSynchronize());
-  TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream));
+  TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream, nsets));
   if (N > 0) {
     T *xyz_d = nullptr;
-    TRY(dalloc(&xyz_d, 3 * (size_t)N));
-    BBFMM_CUDA_OK(cudaMemcpyAsync(xyz_d, xyz_h, sizeof(T) * 3 * N, cudaMemcpyHostToDevice, stream));
+    TRY(dalloc(&xyz_d, 3 * (size_t)Nxyz));
+    BBFMM_CUDA_OK(cudaMemcpyAsync(xyz_d, xyz_h, sizeof(T) * 3 * Nxyz, cudaMemcpyHostToDevice, stream));
     int rc = launch_gather<T, T>(N, perm, xyz_d, nullptr, pos4, stream);
     cudaStreamSynchronize(stream);
     cudaFree(xyz_d);
@@ -250,18 +303,29 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
     else TRY((launch_gather<T, float>(N, perm, nullptr, (const float *)q_dev, pos4, stream)));
     mark(ST_GATHER);
   }
+  // leaf level, slab by slab: P2M, up projection, M2M into the parents
   T *Sl = S[maxlev & 1];
-  TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream));
-  mark(ST_P2M);
-  TRY(proj(pow8i(maxlev), n3, r, Sl, Bup, nullptr, (T)1, Mall + Moff[maxlev], maxlev, MAP_OUT_CPG));
-  mark(ST_PROJ_UP);
+  const int64_t nl = cells(maxlev), sl = leaf_slab();
+  for (int64_t a = 0; a < nl; a += sl) {
+    const int64_t c = nl - a < sl ? nl - a : sl;
+    TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream, nsets, a, c));
+    mark(ST_P2M);
+    TRY(proj(c, n3, r, Sl, Bup, nullptr, (T)1, Mall + Moff[maxlev], maxlev, MAP_OUT_CPG, a));
+    mark(ST_PROJ_UP);
+    if (maxlev - 1 >= BBFMM_MINLEV) {
+      TRY(launch_m2m<T>(n, Sl, S[(maxlev - 1) & 1], maxlev - 1, tb, stream, nsets, a / 8, c / 8));
+      mark(ST_M2M);
+    }
+  }
   for (int l = maxlev - 1; l >= BBFMM_MINLEV; --l) {
-    TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream));
-    mark(ST_M2M);
-    TRY(proj(pow8i(l), n3, r, S[l & 1], Bup, nullptr, (T)1, Mall + Moff[l], l, MAP_OUT_CPG));
+    if (l < maxlev - 1) {
+      TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream, nsets));
+      mark(ST_M2M);
+    }
+    TRY(proj(cells(l), n3, r, S[l & 1], Bup, nullptr, (T)1, Mall + Moff[l], l, MAP_OUT_CPG));
     mark(ST_PROJ_UP);
   }
-  if (mode == MODE_MIXED) {
+  if (mode == MODE_MIXED && tcops) {
     TRY(tc_split_multipoles(r, Mcells(), (const double *)Mall, lead, Msplit, stream));
     mark(ST_PROJ_UP);
   }
@@ -273,20 +337,45 @@ template <typename T>
 int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
   if (sizeof(T) == 8 && r == 256)
     return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
-                           (double *)Lpart, stream);
+                           (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level]);
   if (ni != r) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
-  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream);
+  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets);
 }
 
 template <typename T>
 int Solver<T>::proj(int64_t Mrows, int K, int Ncols, const T *A, const T *B, const T *cs, T scale, T *C, int level,
-                    int mapmode) {
+                    int mapmode, int64_t row0) {
   if (sizeof(T) == 8) {
     int rc = launch_proj_dmma(Mrows, K, Ncols, (const double *)A, (const double *)B, (const double *)cs,
-                              (double)scale, (double *)C, level, mapmode, stream);
+                              (double)scale, (double *)C, level, mapmode, stream, row0);
     if (rc != BBFMM_ERR_UNSUPPORTED) return rc;
   }
-  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream);
+  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream, row0);
+}
+
+// Leaf level after the M2L: per slab, the down projection of the M2L output (assign), L2L
+// from the parents (add), then L2P (assign) -- the order of the whole-level path.
+template <typename T>
+int Solver<T>::leaf_down(bool field) {
+  const Tables tb = tables();
+  T *Fl = F[maxlev & 1];
+  const int64_t nl = cells(maxlev), sl = leaf_slab();
+  const T scale = (T)1 / cell_length<T>(maxlev, (T)L);
+  for (int64_t a = 0; a < nl; a += sl) {
+    const int64_t c = nl - a < sl ? nl - a : sl;
+    if (slabbed()) {
+      TRY(proj(c, r, n3, Lbuf, Bdn, kw, scale, Fl, maxlev, MAP_IN_CPG, a));
+      mark(ST_PROJ_DOWN);
+      if (maxlev > BBFMM_MINLEV) {
+        TRY(launch_l2l<T>(n, F[(maxlev - 1) & 1], Fl, maxlev - 1, tb, stream, nsets, a / 8, c / 8));
+        mark(ST_L2L);
+      }
+    }
+    if (field) TRY(launch_l2p_field<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Fl, phis, flds, stream, nsets, a, c));
+    else TRY(launch_l2p<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Fl, phis, stream, nsets, a, c));
+    mark(ST_L2P);
+  }
+  return BBFMM_OK;
 }
 
 template <typename T>
@@ -294,8 +383,8 @@ int Solver<T>::interaction(int lo, int hi) {
   const Tables tb = tables();
   for (int l = lo; l <= hi; ++l) {
     TRY(m2l_post(l));
-    if (l > BBFMM_MINLEV) {
-      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream));
+    if (l > BBFMM_MINLEV && !(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
+      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream, nsets));
       mark(ST_L2L);
     }
   }
@@ -307,25 +396,31 @@ template <typename T>
 int Solver<T>::m2l_post(int l) {
   {
     const T *Ml = Mall + Moff[l];
-    const bool split = mode == MODE_MIXED && l >= TC_MIN_LEVEL;
+    const bool split = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
     if (split) {
       // FP64 leading block (i < lead_rows, j < lead) on the FP64 tensor path, then the
       // split-bf16 tensor-core kernel adds everything else into the same FP64 output
       if (lead > 0) {
         TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
-        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream));
+        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
+                          tc_products));
         mark(ST_M2L, 2);
       } else {
-        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream));
+        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
+                          tc_products));
         mark(ST_M2L, 1);
       }
     } else {
       TRY(m2l_fp(Ml, l, 0, r, r));
-      mark(ST_M2L);
+      int g = tune.m2l_groups[l] > 0 ? tune.m2l_groups[l] : dmma_default_groups(l, nsets);
+      if ((int64_t)g * cells(l) * r > Lpart_elems) g = 1;
+      mark(ST_M2L, sizeof(T) == 8 && r == 256 && g > 1 ? 2 : 1);  // groups add the partial sum
     }
-    const T scale = (T)1 / cell_length<T>(l, (T)L);
-    TRY(proj(pow8i(l), r, n3, Lbuf, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG));
-    mark(ST_PROJ_DOWN);
+    if (!(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
+      const T scale = (T)1 / cell_length<T>(l, (T)L);
+      TRY(proj(cells(l), r, n3, Lbuf, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG));
+      mark(ST_PROJ_DOWN);
+    }
   }
   return BBFMM_OK;
 }
@@ -333,18 +428,8 @@ int Solver<T>::m2l_post(int l) {
 template <typename T>
 int Solver<T>::downward_finish(void *phi_dev, int phi_is_double, bool near) {
   const Tables tb = tables();
-  TRY(launch_l2p<T>(n, pos4, leaf_start, maxlev, (T)L, tb, F[maxlev & 1], phis, stream));
-  mark(ST_L2P);
-  if (near) {
-    if (mode == MODE_MIXED) {
-      TRY(launch_make_local(N, (const double *)pos4, leafm, maxlev, L, loc4, stream));
-      TRY(launch_p2p_local(N, loc4, leaf_start, leafm, maxlev, L, (double *)phis, stream));
-      mark(ST_P2P, 2);
-    } else {
-      TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, phis, stream));
-      mark(ST_P2P);
-    }
-  }
+  TRY(leaf_down(false));
+  if (near) TRY(this->near(phis, nullptr));
   if (phi_dev) {
     if (phi_is_double) TRY((launch_scatter<T, double>(N, perm, phis, (double *)phi_dev, stream)));
     else TRY((launch_scatter<T, float>(N, perm, phis, (float *)phi_dev, stream)));
@@ -378,17 +463,17 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   BBFMM_CUDA_OK(cudaEventCreate(&a));
   BBFMM_CUDA_OK(cudaEventCreate(&b));
   const T *Ml = Mall + Moff[level];
+  const bool split = mode == MODE_MIXED && tcops && level >= TC_MIN_LEVEL && tune.m2l_kind[level] == 0;
   int rc = BBFMM_OK;
   float tot[2] = {0.f, 0.f};
-  for (int part = 0; part < (mode == MODE_MIXED ? 2 : 1) && rc == BBFMM_OK; ++part) {
+  for (int part = 0; part < (split ? 2 : 1) && rc == BBFMM_OK; ++part) {
     cudaEventRecord(a, stream);
     for (int i = 0; i < reps && rc == BBFMM_OK; ++i) {
-      if (mode != MODE_MIXED) rc = m2l_fp(Ml, level, 0, r, r);
-      else if (part == 0) rc = level >= TC_MIN_LEVEL
-                                   ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf,
-                                                   level, offs, stream)
-                                   : m2l_fp(Ml, level, 0, r, r);
-      else rc = lead > 0 ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
+      if (!split) rc = m2l_fp(Ml, level, 0, r, r);
+      else if (part == 0) rc = split ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf,
+                                                     level, offs, stream, nsets, tc_products)
+                                     : m2l_fp(Ml, level, 0, r, r);
+      else rc = split && lead > 0 ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
     }
     cudaEventRecord(b, stream);
     cudaEventSynchronize(b);
@@ -399,6 +484,23 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   return rc;
+}
+
+// Near field into the sorted potential (and field when fld != null), added.
+template <typename T>
+int Solver<T>::near(T *pot, T *fld) {
+  const int th = tune.p2p_threads;
+  if (mode == MODE_MIXED) {
+    if (fld) TRY(launch_p2p_mixed_field(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot,
+                                        (double *)fld, stream, th));
+    else TRY(launch_p2p_mixed(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot, stream, th));
+    mark(ST_P2P);
+  } else {
+    if (fld) TRY(launch_p2p_field<T>(N, pos4, leaf_start, leafm, maxlev, pot, fld, stream, th));
+    else TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, pot, stream, th));
+    mark(ST_P2P);
+  }
+  return BBFMM_OK;
 }
 
 // pot[i] = sum_j q_j / r_ij and fld[i] = grad pot at x_i (FMM), caller's order, no target
@@ -412,24 +514,126 @@ int Solver<T>::solve_fields(const void *q_dev, void *pot_dev, void *fld_dev) {
   TRY(upward(q_dev, sizeof(T) == 8));
   TRY(interaction(BBFMM_MINLEV, maxlev));
   const Tables tb = tables();
-  TRY(launch_l2p_field<T>(n, pos4, leaf_start, maxlev, (T)L, tb, F[maxlev & 1], phis, flds, stream));
-  mark(ST_L2P);
-  if (mode == MODE_MIXED) {
-    TRY(launch_make_local(N, (const double *)pos4, leafm, maxlev, L, loc4, stream));
-    TRY(launch_p2p_local_field(N, loc4, leaf_start, leafm, maxlev, L, (double *)phis, (double *)flds, stream));
-    mark(ST_P2P, 2);
-  } else {
-    TRY(launch_p2p_field<T>(N, pos4, leaf_start, leafm, maxlev, phis, flds, stream));
-    mark(ST_P2P);
-  }
+  TRY(leaf_down(true));
+  TRY(near(phis, flds));
   TRY((launch_scatter_field<T, T>(N, perm, phis, flds, (T *)pot_dev, (T *)fld_dev, stream)));
   mark(ST_SCATTER);
+  return BBFMM_OK;
+}
+
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::string, std::pair<int, int>> g_tune_cache;  // key -> (kind, groups) or (threads, 0)
+
+int bucket(int64_t v) {  // power-of-two bucket
+  int b = 0;
+  while (v > 1) { v >>= 1; ++b; }
+  return b;
+}
+}  // namespace
+
+template <typename T>
+int Solver<T>::autotune(const void *q_dev, int io_double) {
+  if (!pos4) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
+  const bool was_timing = timing;
+  timing = false;
+  TRY(upward(q_dev, io_double));
+  BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
+  for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
+    char key[96];
+    snprintf(key, sizeof(key), "m2l/%d/%d/%d/%d", mode, n, l, bucket(cells(l)));
+    {
+      std::lock_guard<std::mutex> g(g_tune_mutex);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        tune.m2l_kind[l] = it->second.first;
+        tune.m2l_groups[l] = it->second.second;
+        continue;
+      }
+    }
+    // candidates: (kind, offset groups); only the FP64 DMMA M2L (r = 256) has groups, only
+    // the mixed mode has the tensor-core kind
+    std::vector<std::pair<int, int>> cand;
+    const bool fp64_tc_path = sizeof(T) == 8 && r == 256;
+    if (mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL) cand.push_back({0, 0});
+    if (fp64_tc_path) {
+      for (int g : {1, 3, 7, 21})
+        if (dmma_part_elems(l, nsets, g, r) <= ((int64_t)1 << 27)) cand.push_back({1, g});
+    } else {
+      cand.push_back({1, 0});
+    }
+    float best = 3.4e38f;
+    std::pair<int, int> pick = cand[0];
+    if (cand.size() > 1) {
+      for (auto c : cand) {
+        tune.m2l_kind[l] = c.first;
+        tune.m2l_groups[l] = c.second;
+        TRY(alloc_partials());
+        float ms[2] = {0.f, 0.f};
+        TRY(time_m2l(l, 1, ms));  // warm
+        TRY(time_m2l(l, 3, ms));
+        if (ms[0] + ms[1] < best) {
+          best = ms[0] + ms[1];
+          pick = c;
+        }
+      }
+    }
+    tune.m2l_kind[l] = pick.first;
+    tune.m2l_groups[l] = pick.second;
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    g_tune_cache[key] = pick;
+  }
+  TRY(alloc_partials());
+  // near field: threads per block
+  char key[96];
+  snprintf(key, sizeof(key), "p2p/%d/%d/%d", mode, bucket(N), bucket(cells(maxlev)));
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      tune.p2p_threads = it->second.first;
+      cached = true;
+    }
+  }
+  if (!cached && N > 0) {
+    cudaEvent_t a, b;
+    BBFMM_CUDA_OK(cudaEventCreate(&a));
+    BBFMM_CUDA_OK(cudaEventCreate(&b));
+    float best = 3.4e38f;
+    int pick = 256;
+    int rc = BBFMM_OK;
+    for (int th : {64, 128, 256}) {
+      tune.p2p_threads = th;
+      rc = near(phis, nullptr);  // warm; phis is scratch that the next solve assigns
+      if (rc != BBFMM_OK) break;
+      cudaEventRecord(a, stream);
+      for (int i = 0; i < 3 && rc == BBFMM_OK; ++i) rc = near(phis, nullptr);
+      cudaEventRecord(b, stream);
+      cudaEventSynchronize(b);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rc == BBFMM_OK && ms < best) {
+        best = ms;
+        pick = th;
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    TRY(rc);
+    tune.p2p_threads = pick;
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    g_tune_cache[key] = {pick, 0};
+  }
+  timing = was_timing;
+  BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
   return BBFMM_OK;
 }
 
 template <typename T>
 int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
   if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "level out of range");
+  if (nsets != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "multipole copies are per single-set solver");
   T *tmp = nullptr;
   TRY(dalloc(&tmp, (size_t)pow8i(level) * r));
   int rc = launch_morton_cpg<T>(level, r, Mall + Moff[level], tmp, 1, stream);
@@ -444,11 +648,16 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 
 template <typename T>
 void Solver<T>::release() {
-  void *ptrs[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, offs, perm, leaf_start, leafm, pos4, loc4,
-                  S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit, phis, flds};
+  void *ptrs[] = {offs, perm, leaf_start, leafm, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
+                  phis, flds};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (tcops) tc_free_operators(tcops);
+  if (own_ops) {
+    void *ops[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol};
+    for (void *p : ops)
+      if (p) cudaFree(p);
+    if (tcops) tc_free_operators(tcops);
+  }
   if (ev[ST_COUNT]) cudaEventDestroy(ev[ST_COUNT]);
   if (own_stream && stream) cudaStreamDestroy(stream);
   *this = Solver<T>();
@@ -609,6 +818,39 @@ int bbfmm_b200_direct_field(int N, const double *xyz_dev, const double *q_dev, i
     return bbfmm_set_error(BBFMM_ERR_ARG, "bad direct-sum arguments");
   return bbfmm::launch_direct_field_fp64(N, xyz_dev, q_dev, ntarget, targets_dev, pot_dev, field_dev,
                                          (cudaStream_t)stream);
+}
+
+int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *h, long long cells) {
+  if (!h || cells < 0 || (cells > 0 && cells % 64)) return bbfmm_set_error(BBFMM_ERR_ARG, "slab must be a multiple of 64");
+  if (h->f) {
+    h->f->slab_request = cells;
+    return h->f->pos4 ? h->f->alloc_work() : BBFMM_OK;
+  }
+  h->d->slab_request = cells;
+  return h->d->pos4 ? h->d->alloc_work() : BBFMM_OK;
+}
+
+int bbfmm_b200_set_tc_products(bbfmm_b200_solver *h, int nprod) {
+  if (!h || (nprod != 1 && nprod != 3)) return bbfmm_set_error(BBFMM_ERR_ARG, "products must be 1 or 3");
+  if (h->f) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core products apply to the mixed mode");
+  h->d->tc_products = nprod;
+  return BBFMM_OK;
+}
+
+int bbfmm_b200_autotune(bbfmm_b200_solver *h, const void *q_dev) {
+  if (!h || !q_dev) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  return h->f ? h->f->autotune(q_dev, 0) : h->d->autotune(q_dev, 1);
+}
+
+int bbfmm_b200_tuning(const bbfmm_b200_solver *h, int *info) {
+  if (!h || !info) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  const bbfmm::Tuning &t = h->f ? h->f->tune : h->d->tune;
+  info[0] = t.p2p_threads;
+  for (int l = 0; l <= 10; ++l) {
+    info[1 + l] = t.m2l_kind[l];
+    info[12 + l] = t.m2l_groups[l];
+  }
+  return BBFMM_OK;
 }
 
 void *bbfmm_b200_stream(bbfmm_b200_solver *h) {

@@ -20,29 +20,37 @@ enum Stage {
 };
 
 // Launchers (passes.cu, p2p.cu, m2l_simt.cu, m2l_tc.cu)
-template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s);
-template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s);
-template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s);
-template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s);
-template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s);
+// nsets: number of particle sets of the same depth stacked in one launch (cells of set k
+// are the Morton indices [k 8^l, (k+1) 8^l) of each level; see common.cuh).
+// first, count: a range of cells (P2M, L2P: leaves; M2M, L2L: parents) whose per-cell n^3
+// arrays (S of P2M, F of L2P; the children in M2M and L2L) start at the pointer given, so a
+// level can be processed in slabs; count < 0 means every cell from `first` on.
+template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+// rows are a slab of the level starting at cell row0 (the cpg side is indexed by level cell)
+template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0);
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
-template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s);
-int launch_p2p_local(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L, double *phi, cudaStream_t s);
-int launch_make_local(int N, const double *pos4, const int *leafm, int maxlev, double L, float4 *loc4, cudaStream_t s);
-int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s);
-template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s);
+template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s, int threads = 256);
+int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi, cudaStream_t s, int threads = 256);
+int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s, int nsets = 1);
+template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
-template <typename T> int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld, cudaStream_t s);
-int launch_p2p_local_field(int N, const float4 *loc4, const int *leaf_start, const int *leafm, int maxlev, double L, double *pot, double *fld, cudaStream_t s);
-template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s);
+template <typename T> int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld, cudaStream_t s, int threads = 256);
+int launch_p2p_mixed_field(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *pot, double *fld, cudaStream_t s, int threads = 256);
+template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1);
 void build_offset_table(int *out);
+constexpr int DMMA_PARTS = 21;  // most offset groups of the FP64 M2L (189 = 9 x 21)
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
-                    const int4 *offs, double *part, cudaStream_t s);
-constexpr int DMMA_PARTS = 21;  // offset groups of the small-level FP64 M2L
+                    const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets = 1,
+                    int ngroups = 0);
+int dmma_default_groups(int level, int nsets);
+int64_t dmma_part_elems(int level, int nsets, int groups, int r);
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
-                     double *C, int level, int mapmode, cudaStream_t s);
+                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
 int launch_direct_field_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *pot,
                              double *fld, cudaStream_t s);
@@ -56,17 +64,34 @@ int tc_prepare_operators(int r, const double *Ert, int lead, int lead_rows, void
 void tc_free_operators(void *ops);
 int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s);
 size_t tc_split_bytes(int r, int64_t ncell);
+// nprod: 3 = hi*hi + hi*lo + lo*hi (split BF16), 1 = hi*hi only (plain BF16 products).
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
-                  int level, const int4 *offs, cudaStream_t s);
+                  int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3);
 int tc_status(int clear);
 constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
+
+// Launch choices of one solver, per level (index = level): what the autotuner sets.
+struct Tuning {
+  int m2l_kind[11] = {};    // 0: default (tensor-core split M2L where the mode has it), 1: FP64/SIMT M2L
+  int m2l_groups[11] = {};  // offset groups of the FP64 DMMA M2L (0: dmma_default_groups)
+  int p2p_threads = 256;    // threads per block of the near-field kernels
+};
 
 template <typename T>
 struct Solver {
   int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, lead_rows = 32, device = 0;
+  int nsets = 1;  // particle sets of this depth stacked in every launch (set k = cells [k 8^l, (k+1) 8^l))
+  // Leaf cells per slab of the leaf level (multiple of 64): P2M -> up projection -> M2M and
+  // down projection -> L2L -> L2P run slab by slab through one slab-sized S / F buffer, so
+  // the leaf level's n^3 arrays never exist in full. 0: automatic (slabs only when a full
+  // leaf-level array would exceed 16 GiB); slab_request > 0 forces that size.
+  int64_t slab = 0, slab_request = 0;
   double L = 1.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  bool own_ops = true;  // false: tables and operators borrowed from another solver (share_operators)
+  Tuning tune;
+  int tc_products = 3;  // mixed mode: products per term of the tensor-core M2L (3 split, 1 plain BF16)
   // tables and operators (device)
   T *tkz = nullptr, *cw = nullptr, *kw = nullptr;
   T *Ert = nullptr;  // [316][r][r] row-major
@@ -80,14 +105,14 @@ struct Solver {
   int N = 0;
   int *perm = nullptr, *leaf_start = nullptr, *leafm = nullptr;
   T *pos4 = nullptr;
-  float4 *loc4 = nullptr;
   // expansions
   T *S[2] = {nullptr, nullptr};
   T *F[2] = {nullptr, nullptr};
   T *Mall = nullptr;
   std::vector<int64_t> Moff;  // offset (elements) of level l in Mall, cpg layout
   T *Lbuf = nullptr;
-  T *Lpart = nullptr;  // partial sums of the small-level FP64 M2L (levels <= 3)
+  T *Lpart = nullptr;  // partial sums of the offset-group FP64 M2L
+  int64_t Lpart_elems = 0;
   void *Msplit = nullptr;
   T *phis = nullptr;
   T *flds = nullptr;  // 3 N, sorted field of the last solve_fields
@@ -98,11 +123,27 @@ struct Solver {
   int kernel_launches = 0;
 
   Tables tables() const;
-  int64_t Mcells() const { return (Moff[maxlev] + pow8i(maxlev) * r) / r; }
+  int64_t cells(int l) const { return nsets * pow8i(l); }
+  int64_t leaf_slab() const { return slab > 0 && slab < cells(maxlev) ? slab : cells(maxlev); }
+  bool slabbed() const { return leaf_slab() < cells(maxlev); }
+  int leaf_down(bool field);  // down projection, L2L and L2P (or L2P with field) of the leaf level
+  int64_t Mcells() const { return (Moff[maxlev] + cells(maxlev) * r) / r; }
   int init(int n_, int maxlev_, double L_, int mode_, int lead_, int lead_rows_, int device_, cudaStream_t s);
   int set_tables(const T *Tkz, const T *Cweights, const T *Kweights);  // host arrays
   int set_operators(const T *U, const T *E);                              // host, reference layout
   int set_particles_sorted(int N_, const int *perm_host, const int *leaf_start_host, const T *xyz_host);
+  // N_ particles of nsets_ stacked sets: perm_host[k] indexes the caller's arrays of Nxyz
+  // particles (positions xyz_host, and later q and phi); leaf_start_host has nsets_ 8^maxlev + 1
+  // entries over the sorted order.
+  int set_particles_global(int nsets_, int N_, const int *perm_host, const int *leaf_start_host, int Nxyz,
+                           const T *xyz_host);
+  int share_operators(const Solver<T> &from);  // borrow tables and operators (same n, mode, lead)
+  int alloc_partials();                          // Lpart for the current tuning
+  int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
+  // Times the launch choices of every level's M2L and of the near field on this solver's
+  // own tree (after an upward pass with q_dev) and keeps the fastest; results are cached per
+  // (mode, n, level, target tiles) and (mode, particles, leaves) for later solvers.
+  int autotune(const void *q_dev, int io_double);
   int alloc_work();
   int upward(const void *q_dev, int q_is_double);   // gather q, P2M, M2M, projections -> Mall
   int interaction(int level_lo, int level_hi);       // M2L + post projection + L2L into F
@@ -114,7 +155,8 @@ struct Solver {
   void mark(int stage, int launches = 1);
   int time_m2l(int level, int reps, float *ms);
   int m2l_fp(const T *Ml, int level, int j0, int j1, int ni);  // FP64 (DMMA) / FP32 (SIMT) M2L part
-  int proj(int64_t M, int K, int N, const T *A, const T *B, const T *cs, T scale, T *C, int level, int mapmode);
+  int proj(int64_t M, int K, int N, const T *A, const T *B, const T *cs, T scale, T *C, int level, int mapmode,
+           int64_t row0 = 0);
   void release();
 };
 

@@ -130,6 +130,28 @@ class Solver:
         _lib.check(_lib.lib().bbfmm_b200_solve_host(self.h, _ptr(q), _ptr(phi)))
         return phi
 
+    def set_tc_products(self, nprod: int):
+        """Mixed mode: 3 (split BF16, default) or 1 (plain BF16) products per M2L term."""
+        _lib.check(_lib.lib().bbfmm_b200_set_tc_products(self.h, int(nprod)))
+
+    def set_leaf_slab(self, cells: int):
+        """Leaf cells per slab of the leaf level (multiple of 64; 0 = automatic)."""
+        _lib.check(_lib.lib().bbfmm_b200_set_leaf_slab(self.h, int(cells)))
+
+    def autotune(self, q):
+        """Time the per-level M2L and near-field launch choices on this tree (an upward pass
+        with charges q, a CUDA tensor) and keep the fastest; returns the choices."""
+        q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        self.torch.cuda.synchronize(q.device)
+        _lib.check(_lib.lib().bbfmm_b200_autotune(self.h, C.c_void_p(q.data_ptr())))
+        return self.tuning()
+
+    def tuning(self):
+        info = (C.c_int * 23)()
+        _lib.check(_lib.lib().bbfmm_b200_tuning(self.h, info))
+        v = list(info)
+        return {"p2p_threads": v[0], "m2l_kind": v[1:12], "m2l_groups": v[12:23]}
+
     def set_timing(self, on: bool):
         _lib.check(_lib.lib().bbfmm_b200_set_timing(self.h, int(on)))
 
@@ -147,6 +169,112 @@ class Solver:
         out = np.empty(8 ** level * self.r, dtype=self.np_dtype)
         _lib.check(_lib.lib().bbfmm_b200_copy_multipoles(self.h, level, _ptr(out)))
         return out
+
+
+def batch_depth(N: int, per_leaf: float = 32.0) -> int:
+    """Leaf depth for about `per_leaf` particles per leaf: round(log8(N / per_leaf)), >= 2."""
+    return max(2, int(round(math.log(max(N, 1) / per_leaf, 8)))) if N > 0 else 2
+
+
+class Batch:
+    """Many independent particle sets solved together (bbfmm_b200_batch_*).
+
+    sets: a list of (xyz, n, maxlev) with xyz an (N_s, 3) host array inside [-L/2, L/2]^3.
+    Charges and results are CUDA tensors holding the sets back to back in list order
+    (``offsets[s]:offsets[s + 1]``)."""
+
+    def __init__(self, sets, mode: str = "mixed", L: float = 1.0, lead: int = 16, lead_rows: int = 32,
+                 device: int = 0):
+        import torch
+        self.torch = torch
+        self.mode, self.L, self.device = mode, float(L), device
+        self.dtype = torch.float32 if mode == "s" else torch.float64
+        np_dtype = np.float32 if mode == "s" else np.float64
+        counts = np.array([len(x) for x, _, _ in sets], dtype=np.int32)
+        ns = np.array([n for _, n, _ in sets], dtype=np.int32)
+        levs = np.array([lv for _, _, lv in sets], dtype=np.int32)
+        self.offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        self.N = int(self.offsets[-1])
+        xyz = np.ascontiguousarray(np.concatenate([np.asarray(x, np_dtype).reshape(-1, 3) for x, _, _ in sets])
+                                   if len(sets) else np.zeros((0, 3), np_dtype))
+        ops_ = {}
+        for n in sorted(set(ns.tolist())):
+            _, U, E = ops.load_operators(n, single=(mode == "s"))
+            ops_[n] = (np.ascontiguousarray(U), np.ascontiguousarray(E))
+        fp32 = int(mode == "s")
+        p = lambda n, k: _ptr(ops_[n][k]) if n in ops_ else None
+        cfg = _lib.Config(n=0, maxlev=0, L=self.L, mode=_lib.MODES[mode], lead=lead if mode == "mixed" else 0,
+                          lead_rows=lead_rows if mode == "mixed" else 0, device=device, stream=None)
+        h = C.c_void_p()
+        ip = C.POINTER(C.c_int)
+        _lib.check(_lib.lib().bbfmm_b200_batch_create(C.byref(cfg), len(sets), ns.ctypes.data_as(ip),
+                                                       levs.ctypes.data_as(ip), counts.ctypes.data_as(ip), _ptr(xyz),
+                                                       p(4, 0), p(4, 1), p(8, 0), p(8, 1), fp32, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            _lib.lib().bbfmm_b200_batch_destroy(h)
+            self.h = None
+
+    def close(self):
+        self.__del__()
+
+    @property
+    def stream(self):
+        return _lib.lib().bbfmm_b200_batch_stream(self.h)
+
+    def _order(self, q):
+        torch = self.torch
+        caller = torch.cuda.current_stream(q.device)
+        mine = torch.cuda.ExternalStream(self.stream, device=q.device)
+        ev = torch.cuda.Event()
+        ev.record(caller)
+        mine.wait_event(ev)
+        return caller, mine
+
+    def solve(self, q, out=None, graph: bool = True):
+        """q: CUDA tensor (N_total,) -> q_i * phi_i of every set (same layout)."""
+        torch = self.torch
+        q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        if out is None:
+            out = torch.empty_like(q)
+        caller, mine = self._order(q)
+        _lib.check(_lib.lib().bbfmm_b200_batch_solve(self.h, C.c_void_p(q.data_ptr()), C.c_void_p(out.data_ptr()),
+                                                      int(graph)))
+        done = torch.cuda.Event()
+        done.record(mine)
+        caller.wait_event(done)
+        return out
+
+    def set_tc_products(self, nprod: int):
+        """Mixed mode: 3 (split BF16, default) or 1 (plain BF16) products per M2L term."""
+        _lib.check(_lib.lib().bbfmm_b200_set_tc_products(self.h, int(nprod)))
+
+    def set_leaf_slab(self, cells: int):
+        """Leaf cells per slab of the leaf level (multiple of 64; 0 = automatic)."""
+        _lib.check(_lib.lib().bbfmm_b200_set_leaf_slab(self.h, int(cells)))
+
+    def autotune(self, q):
+        q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        self.torch.cuda.synchronize(q.device)
+        _lib.check(_lib.lib().bbfmm_b200_batch_autotune(self.h, C.c_void_p(q.data_ptr())))
+        return self.groups()
+
+    def groups(self):
+        out = []
+        for g in range(_lib.lib().bbfmm_b200_batch_groups(self.h)):
+            info = (C.c_int * 27)()
+            _lib.check(_lib.lib().bbfmm_b200_batch_group_info(self.h, g, info))
+            v = list(info)
+            out.append({"n": v[0], "maxlev": v[1], "sets": v[2], "particles": v[3], "p2p_threads": v[4],
+                        "m2l_kind": v[5:5 + v[1] + 1], "m2l_groups": v[16:16 + v[1] + 1]})
+        return out
+
+    @property
+    def graph_nodes(self) -> int:
+        return int(_lib.lib().bbfmm_b200_batch_graph_nodes(self.h))
 
 
 def direct(xyz, q, targets, stream=None):

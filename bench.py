@@ -335,6 +335,204 @@ def run_gradient_1m(args):
     return 0
 
 
+def clustered_16m_inputs(seed=3, N=16_777_216):
+    """Half uniform in the unit cube, half from 16 isotropic Gaussian clusters (centres
+    U[0.1, 0.9]^3, sigma 0.03, clipped to the cube), shifted onto the origin-centred root
+    cell; charges N(0, 1)."""
+    rng = np.random.default_rng(seed)
+    nu = N // 2
+    c = rng.uniform(0.1, 0.9, (16, 3))
+    xc = c[rng.integers(0, 16, N - nu)] + 0.03 * rng.standard_normal((N - nu, 3))
+    x = np.concatenate([rng.random((nu, 3)), np.clip(xc, 0.0, np.nextafter(1.0, 0.0))]) - 0.5
+    return x, rng.standard_normal(N)
+
+
+def run_clustered_16m(args):
+    """N = 16,777,216 clustered (50% uniform + 50% in 16 Gaussians), n = 8, depth 8: the M2L
+    precisions side by side -- FP64 leading block + 3xBF16 (the mixed mode), 3xBF16 alone,
+    plain BF16 (one product), FP32 and FP64 -- each timed and compared with the FP64 direct
+    sum on 8,192 sampled targets (relative L2 and max error / max |phi|). The leaf level runs
+    in slabs (its n^3 node arrays would take 69 GB each in FP64)."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.fmm import direct
+    N, n, lev = 16_777_216, 8, 8
+    x, q = clustered_16m_inputs()
+    targets = np.random.default_rng(4321).choice(N, 8192, replace=False).astype(np.int32)
+    ref = direct(torch.as_tensor(x, device="cuda"), torch.as_tensor(q, device="cuda"),
+                 torch.as_tensor(targets, device="cuda")).cpu().numpy()
+    variants = [("fp64 lead + 3xbf16", "mixed", 16, 3), ("3xbf16", "mixed", 0, 3), ("1xbf16", "mixed", 0, 1),
+                ("fp32", "s", 0, 3), ("fp64", "d", 0, 3)]
+    res = {}
+    for name, mode, lead, nprod in variants:
+        free0 = torch.cuda.mem_get_info()[0]
+        sol = Solver(n, lev, 1.0, mode=mode, lead=lead if lead else 0)
+        if mode == "mixed" and nprod != 3:
+            sol.set_tc_products(nprod)
+        sol.set_particles(x)
+        dt = sol.dtype
+        qd = torch.as_tensor(q, dtype=dt, device="cuda")
+        out = torch.empty_like(qd)
+        stream = torch.cuda.ExternalStream(sol.stream)
+        sol.solve(qd, out=out)
+        torch.cuda.synchronize()
+        used = free0 - torch.cuda.mem_get_info()[0]
+        steps = args.steps if mode == "mixed" else 1
+        with ClockSampler(0) as clk:
+            t = _device_time(lambda: sol.solve(qd, out=out), steps, stream)
+        sol.set_timing(True)
+        sol.solve(qd, out=out)
+        torch.cuda.synchronize()
+        stages, _ = sol.stage_times()
+        sol.set_timing(False)
+        phi = out.double().cpu().numpy()[targets]
+        res[name] = {"mode": mode, "lead": lead, "products": nprod, "s_per_solve": t,
+                     "err_rel_l2": float(np.linalg.norm(phi - ref) / np.linalg.norm(ref)),
+                     "err_max_over_max_abs": float(np.abs(phi - ref).max() / np.abs(ref).max()),
+                     "device_bytes": int(used), "stages_ms": stages, "clocks": clk.summary()}
+        sol.close()
+        del qd, out
+        torch.cuda.empty_cache()
+    head = res["fp64 lead + 3xbf16"]
+    line = {"metric": "FMM solves/s at N=16,777,216 clustered, n=8, depth 8", "value": 1.0 / head["s_per_solve"],
+            "unit": "solve/s", "n_gpus": 1, "steps": args.steps, "warmup": 1,
+            "ms_per_step": head["s_per_solve"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3+f64",
+            "data": "synthetic (seeded; 50% uniform, 50% in 16 Gaussians sigma 0.03; q ~ N(0,1))",
+            "config": {"workload": "bbFMM Laplace 1/r, N=16,777,216 clustered, n=8 (r=256), maxlev 8", "N": N,
+                       "n": n, "maxlev": lev, "n_targets": 8192},
+            "variants": res,
+            "err_ratio_vs_fp64": head["err_rel_l2"] / res["fp64"]["err_rel_l2"],
+            "speedup_vs_fp64": res["fp64"]["s_per_solve"] / head["s_per_solve"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def batch_sets(seed=5, nsets=256):
+    """256 independent sets: N log-uniform in [4096, 262144], half uniform in the unit cube and
+    half from 4 Gaussian clusters (sigma 0.04, centres U[0.1, 0.9]^3, clipped), n = 4 or 8 at
+    random, depth round(log8(N / 32)) (about 32 particles per leaf); charges U[-1, 1]."""
+    from bbfmm_b200 import batch_depth
+    rng = np.random.default_rng(seed)
+    sets = []
+    for k in range(nsets):
+        N = int(round(np.exp(rng.uniform(np.log(4096), np.log(262144)))))
+        if k % 2 == 0:
+            x = rng.random((N, 3))
+        else:
+            c = rng.uniform(0.1, 0.9, (4, 3))
+            x = np.clip(c[rng.integers(0, 4, N)] + 0.04 * rng.standard_normal((N, 3)), 0.0, np.nextafter(1.0, 0.0))
+        n = int(rng.choice([4, 8]))
+        sets.append((x - 0.5, n, batch_depth(N)))
+    q = rng.uniform(-1.0, 1.0, sum(len(x) for x, _, _ in sets))
+    return sets, q
+
+
+def run_batch_256(args):
+    """256 uneven sets in one batch (stacked per (n, depth), one launch per pass per group,
+    the groups as parallel branches of one CUDA graph), after the autotuner; per-set error
+    against the FP64 direct sum on 512 sampled targets per set."""
+    import torch
+    from bbfmm_b200 import Batch
+    from bbfmm_b200.fmm import direct
+    mode = args.mode
+    sets, q = batch_sets()
+    t0 = time.perf_counter()
+    b = Batch(sets, mode=mode)
+    t_setup = time.perf_counter() - t0
+    dt = torch.float32 if mode == "s" else torch.float64
+    qd = torch.as_tensor(q, dtype=dt, device="cuda")
+    out = torch.empty_like(qd)
+    t0 = time.perf_counter()
+    groups = b.autotune(qd)
+    t_tune = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(b.stream)
+    for _ in range(args.warmup):
+        b.solve(qd, out=out, graph=True)
+    with ClockSampler(0) as clk:
+        t_graph = _device_time(lambda: b.solve(qd, out=out, graph=True), args.steps, stream)
+    t_eager = _device_time(lambda: b.solve(qd, out=out, graph=False), args.steps, stream)
+    phi = out.double().cpu().numpy()
+    # per-set error on 512 sampled targets
+    rng = np.random.default_rng(77)
+    errs = []
+    for k, (x, n, lev) in enumerate(sets):
+        a, e = int(b.offsets[k]), int(b.offsets[k + 1])
+        t = rng.choice(e - a, min(512, e - a), replace=False).astype(np.int32)
+        ref = direct(torch.as_tensor(x, device="cuda"), torch.as_tensor(q[a:e], device="cuda"),
+                     torch.as_tensor(t, device="cuda")).cpu().numpy()
+        errs.append(float(np.linalg.norm(phi[a:e][t] - ref) / np.linalg.norm(ref)))
+    errs = np.array(errs)
+    ns = np.array([n for _, n, _ in sets])
+    Ntot = int(b.offsets[-1])
+    qh = torch.as_tensor(q, dtype=dt).pin_memory()
+    ph = torch.empty_like(qh).pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        qd.copy_(qh, non_blocking=True)
+        b.solve(qd, out=out, graph=True)
+        ph.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    cpu = None
+    if not args.no_cpu_baseline:
+        # the reference CPU code on 4 of the sets (one per (n, depth) seen first), scaled by particles
+        t_ref, n_ref, kinds = 0.0, 0, set()
+        for (x, n, lev) in sets:
+            if (n, lev) in kinds or len(kinds) >= 4:
+                continue
+            kinds.add((n, lev))
+            from oracle.oracle import Reference, reference_available
+            if not reference_available("d"):
+                break
+            tt, cores, kind = reference_sample_xq(x, q[:len(x)], n, lev)
+            t_ref += tt
+            n_ref += len(x)
+        if n_ref:
+            cpu = {"value": (n_ref / t_ref) / Ntot, "unit": "batch/s", "cores": cores, "kind": kind,
+                   "sample": f"the reference CPU code on {len(kinds)} of the sets ({n_ref} particles, {t_ref:.2f} s), "
+                             f"scaled to the batch's {Ntot} particles"}
+    line = {"metric": "batched solves of 256 uneven sets (N log-uniform 4,096..262,144, n in {4,8})",
+            "value": 1.0 / t_graph, "unit": "batch/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_graph * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"mixed": "bf16x3+f64", "d": "f64", "s": "f32"}[mode],
+            "data": "synthetic (seeded; half uniform, half 4-Gaussian sigma 0.04)",
+            "config": {"workload": "256 uneven bbFMM Laplace sets, n in {4,8}, depth round(log8(N/32))",
+                       "particles": Ntot, "mode": mode,
+                       "groups": [{k: g[k] for k in ("n", "maxlev", "sets", "particles", "p2p_threads",
+                                                      "m2l_kind", "m2l_groups")} for g in groups]},
+            "particles_per_s": Ntot / t_graph, "eager_ms": t_eager * 1e3, "graph_nodes": b.graph_nodes,
+            "setup_s": t_setup, "autotune_s": t_tune,
+            "err_vs_fp64_direct": {"median": float(np.median(errs)), "max": float(errs.max()),
+                                   "max_n4": float(errs[ns == 4].max()), "max_n8": float(errs[ns == 8].max()),
+                                   "targets_per_set": 512},
+            "e2e": {"value": 1.0 / t_e2e, "unit": "batch/s", "h2d_bytes_per_step": Ntot * qd.element_size(),
+                    "d2h_bytes_per_step": Ntot * qd.element_size()},
+            "cpu_baseline": cpu, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    b.close()
+    return 0
+
+
+def reference_sample_xq(x, q, n, lev):
+    """Seconds of one reference CPU solve of the given particles (n, depth lev)."""
+    from oracle.oracle import Reference
+    from bbfmm_b200 import operators as ops
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    ref = Reference("d")
+    d = os.path.join(ops.default_cache_dir(), "ref")
+    kp, up = ops.operator_file_names(n, False)
+    kp, up = os.path.join(d, kp), os.path.join(d, up)
+    if not (os.path.exists(kp) and os.path.exists(up)):
+        _, U, E = ops.load_operators(n, False)
+        ops.write_operator_files(d, n, U, E, False)
+    ref.fmm(x, q, n, lev, kp, up)
+    t0 = time.perf_counter()
+    ref.fmm(x, q, n, lev, kp, up)
+    return time.perf_counter() - t0, cores, "reference"
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -347,7 +545,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--N", type=int, default=N_FULL)
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
-    ap.add_argument("--workload", default="uniform-4m", choices=["uniform-4m", "uniform-32k", "gradient-1m"],
+    ap.add_argument("--workload", default="uniform-4m",
+                    choices=["uniform-4m", "uniform-32k", "gradient-1m", "batch-256", "clustered-16m"],
                     help="uniform-4m: the headline line; the others measure further configurations")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -356,6 +555,10 @@ def main():
         return run_uniform_32k(args)
     if args.workload == "gradient-1m":
         return run_gradient_1m(args)
+    if args.workload == "batch-256":
+        return run_batch_256(args)
+    if args.workload == "clustered-16m":
+        return run_clustered_16m(args)
 
     import torch
     import torch.distributed as dist

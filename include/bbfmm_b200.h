@@ -164,9 +164,10 @@ BBFMM_B200_API int bbfmm_b200_device_status(int clear);
  * <= 27 neighbour leaves. xyzq is N x 4 (x, y, z, q) FP64 sorted by leaf in Morton order
  * (as bbfmm_b200_sort_particles orders them), leaf_start holds the 8^maxlev + 1 leaf
  * offsets, phi is added to; all three are device pointers. mode BBFMM_B200_MODE_D computes
- * in FP64 like the reference; BBFMM_B200_MODE_MIXED in FP32 on leaf-local coordinates with
- * compensated sums. Allocates N * (4 + 16) bytes of device scratch for the call, runs on
- * `stream` (cudaStream_t, may be NULL) and synchronises it before freeing the scratch. */
+ * in FP64 like the reference; BBFMM_B200_MODE_MIXED takes each pair's separation in FP64 and
+ * the reciprocal distance, product and compensated sum in FP32. L is checked (> 0) but the
+ * leaf geometry needs only maxlev. Allocates N * 4 bytes of device scratch for the call, runs
+ * on `stream` (cudaStream_t, may be NULL) and synchronises it before freeing the scratch. */
 BBFMM_B200_API int bbfmm_b200_near_field(int N, int maxlev, double L, const double *xyzq, const int *leaf_start,
                                          double *phi, int mode, void *stream);
 
@@ -176,7 +177,7 @@ BBFMM_B200_API int bbfmm_b200_near_field(int N, int maxlev, double L, const doub
  * time-critical loops that cannot afford the device-wide synchronisation cudaMalloc and
  * cudaFree imply. Inputs and output are the caller's, as above; the per-particle scratch
  * lives in one fixed array of device memory inside the library, sized for
- * BBFMM_B200_NOALLOC_MAX_PARTICLES particles (5 MiB), which every GPU that loads the library
+ * BBFMM_B200_NOALLOC_MAX_PARTICLES particles (1 MiB), which every GPU that loads the library
  * keeps until the process exits. Larger N is rejected with BBFMM_B200_ERR_ARG.
  * The first call on a device looks up that array's device address (with the device
  * current), so make the first call on each device before any stream capture. All calls
@@ -189,6 +190,59 @@ BBFMM_B200_API int bbfmm_b200_near_field_noalloc(int N, int maxlev, double L, co
 
 BBFMM_B200_API void *bbfmm_b200_stream(bbfmm_b200_solver *s);
 BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
+
+/* Leaf cells per slab of the leaf level (a multiple of 64; 0 = automatic). The leaf level's
+ * P2M -> up projection -> M2M and down projection -> L2L -> L2P run slab by slab through one
+ * slab-sized buffer of Chebyshev node values, so those per-leaf arrays (n^3 values per leaf)
+ * never exist for the whole level; results are bitwise the same for every slab size.
+ * Automatic: slabs of 16 GiB when a whole-level array would be larger (n = 8, FP64: depth 8
+ * and deeper). Reallocates the work buffers when particles are already set. */
+BBFMM_B200_API int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *s, long long cells);
+
+/* MIXED mode: products per term of the tensor-core M2L: 3 (default; hi*hi + hi*lo + lo*hi of
+ * the split BF16 operands) or 1 (hi*hi: plain BF16 products, for precision comparisons). */
+BBFMM_B200_API int bbfmm_b200_set_tc_products(bbfmm_b200_solver *s, int nprod);
+
+/* Autotuner (no counterpart in the reference): runs an upward pass with q_dev, then times the
+ * launch choices of every level's M2L (mixed mode: tensor-core split vs FP64; FP64 DMMA: the
+ * 189 offsets split over 1, 3, 7 or 21 CTAs per target tile) and of the near field (64, 128
+ * or 256 threads per block) on this solver's tree, and keeps the fastest. Choices are cached
+ * in the process per (mode, n, level, cell count) and (mode, particles, leaves), so solvers
+ * of similar shape reuse them without timing. Synchronises the device. */
+BBFMM_B200_API int bbfmm_b200_autotune(bbfmm_b200_solver *s, const void *q_dev);
+/* Current choices: info[0] = P2P threads per block, info[1 + l] = M2L kind of level l
+ * (0 default, 1 FP64/SIMT), info[12 + l] = offset groups of level l (0 = default); 23 ints. */
+BBFMM_B200_API int bbfmm_b200_tuning(const bbfmm_b200_solver *s, int *info);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent particle sets of uneven size, each with its own order n (4 or 8) and leaf
+ * depth, solved together (no counterpart in the reference, which solves one set per call).
+ * Sets of equal (n, depth) are stacked into one group whose every pass is one launch over all
+ * its sets; groups of the same n share one copy of the operators; the groups run on streams
+ * forked from the batch stream, and the batch solve is captured into a CUDA graph on first use
+ * (and again whenever q_dev or phi_dev changes). cfg supplies mode, L, lead, lead_rows and
+ * device (cfg->n, cfg->maxlev and cfg->stream are not used). Positions, charges and results
+ * hold the sets back to back in set order: set s starts at counts[0] + ... + counts[s-1].
+ * U4/E4 and U8/E8 are the operators of n = 4 and n = 8 (reference file layouts, FP64 unless
+ * operators_fp32); the pair of an order no set uses may be NULL. */
+typedef struct bbfmm_b200_batch bbfmm_b200_batch;
+BBFMM_B200_API int bbfmm_b200_batch_create(const bbfmm_b200_config *cfg, int nsets, const int *n, const int *maxlev,
+                                           const int *counts, const void *xyz, const void *U4, const void *E4,
+                                           const void *U8, const void *E8, int operators_fp32,
+                                           bbfmm_b200_batch **out);
+/* One solve of every set (phi as in bbfmm_b200_solve), on the batch stream, without
+ * synchronising; use_graph != 0 replays the captured graph. */
+BBFMM_B200_API int bbfmm_b200_batch_solve(bbfmm_b200_batch *b, const void *q_dev, void *phi_dev, int use_graph);
+/* bbfmm_b200_autotune for every group (drops the captured graph). */
+BBFMM_B200_API int bbfmm_b200_batch_autotune(bbfmm_b200_batch *b, const void *q_dev);
+BBFMM_B200_API int bbfmm_b200_batch_groups(const bbfmm_b200_batch *b);
+/* Nodes of the captured graph (0 before the first graph solve). */
+BBFMM_B200_API long long bbfmm_b200_batch_graph_nodes(const bbfmm_b200_batch *b);
+/* Group g: info[0] = n, info[1] = depth, info[2] = sets, info[3] = particles, info[4] = P2P
+ * threads, info[5 + l] = M2L kind of level l, info[16 + l] = offset groups; 27 ints. */
+BBFMM_B200_API int bbfmm_b200_batch_group_info(const bbfmm_b200_batch *b, int g, int *info);
+BBFMM_B200_API void *bbfmm_b200_batch_stream(bbfmm_b200_batch *b);
+BBFMM_B200_API void bbfmm_b200_batch_destroy(bbfmm_b200_batch *b);
 
 #ifdef __cplusplus
 }

@@ -149,3 +149,22 @@ def test_direct_field_matches_oracle(oracle_d):
     p0, f0 = oracle_d.direct_field_fp64(x, q, t)
     assert rel_l2(pot.cpu().numpy(), p0) < 1e-14
     assert rel_l2(fld.cpu().numpy().reshape(-1), f0.reshape(-1)) < 1e-14
+
+
+def test_fields_after_growing_particle_set():
+    """solve_fields after set_particles with more particles (the field scratch is resized)."""
+    import torch
+    from bbfmm_b200 import Solver
+    x1, q1, _ = _clustered(5000, 8)
+    x2, q2, _ = _clustered(40000, 9)
+    s = Solver(4, 3, 1.0, mode="d")
+    s.set_particles(x1)
+    s.solve_fields(torch.as_tensor(q1, device="cuda"))
+    s.set_particles(x2)
+    p, f = s.solve_fields(torch.as_tensor(q2, device="cuda"))
+    t = Solver(4, 3, 1.0, mode="d")
+    t.set_particles(x2)
+    p0, f0 = t.solve_fields(torch.as_tensor(q2, device="cuda"))
+    assert torch.equal(p, p0) and torch.equal(f, f0)
+    s.close()
+    t.close()

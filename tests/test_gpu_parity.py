@@ -112,7 +112,7 @@ def test_host_entry_matches_device_entry():
 @pytest.mark.parametrize("mode,tol", [(0, 1e-13), (2, 1e-6)])
 def test_near_field_entry_matches_oracle(oracle_d, mode, tol):
     """bbfmm_b200_near_field on caller-owned device arrays vs the oracle's P2P
-    (anotherNearField semantics). FP64 mode: 1e-13; FP32 leaf-local mode: 1e-6."""
+    (anotherNearField semantics). FP64 mode: 1e-13; mixed mode (FP32 reciprocal distances): 1e-6."""
     import ctypes as C
     import torch
     from bbfmm_b200 import _lib
@@ -137,3 +137,23 @@ def test_near_field_entry_matches_oracle(oracle_d, mode, tol):
     got = np.empty(N)
     got[perm] = phi.cpu().numpy()
     assert rel_l2(got, want) < tol
+
+
+@pytest.mark.parametrize("mode,n", [("d", 8), ("mixed", 8), ("s", 4)])
+def test_leaf_slabs_are_bitwise_identical(mode, n):
+    """The leaf level processed in slabs of 64 / 512 leaves (P2M -> projection -> M2M and
+    projection -> L2L -> L2P per slab) gives exactly the whole-level result."""
+    import torch
+    from bbfmm_b200 import Solver
+    x, q = uniform_inputs(40000, seed=12)
+    s = Solver(n, 4, 1.0, mode=mode)
+    s.set_particles(x)
+    qd = torch.as_tensor(q, device="cuda")
+    whole = s.solve(qd).cpu().numpy()
+    p0, f0 = s.solve_fields(qd)
+    for cells in (64, 512):
+        s.set_leaf_slab(cells)
+        assert np.array_equal(s.solve(qd).cpu().numpy(), whole), cells
+        p, f = s.solve_fields(qd)
+        assert torch.equal(p, p0) and torch.equal(f, f0), cells
+    s.close()
