@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_batch_graph_nodes.argtypes = [vp]
         L.bbfmm_b200_batch_graph_nodes.restype = C.c_longlong
         L.bbfmm_b200_batch_group_info.argtypes = [vp, i, ip]
+        L.bbfmm_b200_batch_group_stage_times.argtypes = [vp, i, vp, vp, C.POINTER(C.c_float), i]
         L.bbfmm_b200_batch_stream.argtypes = [vp]
         L.bbfmm_b200_batch_stream.restype = vp
         L.bbfmm_b200_batch_destroy.argtypes = [vp]

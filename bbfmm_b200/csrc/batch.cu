@@ -281,6 +281,25 @@ int bbfmm_b200_batch_group_info(const bbfmm_b200_batch *b, int g, int *info) {
   return BBFMM_OK;
 }
 
+int bbfmm_b200_batch_group_stage_times(bbfmm_b200_batch *b, int g, const void *q_dev, void *phi_dev, float *ms,
+                                       int count) {
+  if (!b || !ms || !q_dev || !phi_dev) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  const int ng = bbfmm_b200_batch_groups(b);
+  if (g < 0 || g >= ng) return bbfmm_set_error(BBFMM_ERR_ARG, "group index out of range");
+  auto run = [&](auto &batch) -> int {
+    auto &sv = *batch.groups[g].solver;
+    BBFMM_CUDA_OK(cudaDeviceSynchronize());
+    sv.timing = true;
+    int rc = sv.solve(q_dev, phi_dev, sizeof(sv.pos4[0]) == 8);
+    sv.timing = false;
+    if (rc != BBFMM_OK) return rc;
+    BBFMM_CUDA_OK(cudaStreamSynchronize(sv.stream));
+    for (int i = 0; i < count && i < bbfmm::ST_COUNT; ++i) ms[i] = sv.stage_ms[i];
+    return BBFMM_OK;
+  };
+  return b->d ? run(*b->d) : run(*b->f);
+}
+
 void *bbfmm_b200_batch_stream(bbfmm_b200_batch *b) {
   if (!b) return nullptr;
   return b->d ? (void *)b->d->stream : (void *)b->f->stream;

@@ -52,7 +52,12 @@ __global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, 
 #pragma unroll
     for (int b = 0; b < TN; ++b) acc[a][b] = 0;
   const int64_t P3 = (int64_t)P * P * P;
-  for (int o = 0; o < 189; ++o) {
+  // blockIdx.y selects one of gridDim.y groups of the 189 offsets; with several groups each
+  // writes its partial sums to its own slice of Lout (all classes of all sets apart)
+  const int grp = blockIdx.y, ngrp = gridDim.y;
+  const int o0 = (189 * grp) / ngrp, o1 = (189 * (grp + 1)) / ngrp;
+  Lout += (int64_t)grp * (gridDim.x / tiles_per_class) * P3 * R;
+  for (int o = o0; o < o1; ++o) {
     const int4 ov = offs[(c & 7) * 189 + o];
     const int k = ov.x;
     // source class and parent-grid shift for this class/offset
@@ -114,24 +119,51 @@ int m2l_simt_tiles(int level) {
   return 8 * nbox * nbox * nbox;
 }
 
+// Lout[e] = sum_g part[g][e], in a fixed order.
+template <typename T>
+__global__ void simt_sum_parts_kernel(int64_t count, int ng, const T *__restrict__ part, T *__restrict__ Lout) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+    T v = 0;
+    for (int g = 0; g < ng; ++g) v += part[(int64_t)g * count + e];
+    Lout[e] = v;
+  }
+}
+
+// ngroups > 1 splits the 189 offsets over that many CTAs per target tile; their partials go
+// to `part` (part_elems elements) and are summed in a fixed order (groups are reduced to
+// fit the scratch; accumulate then does not apply).
 template <typename T>
 int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs,
-                    int accumulate, cudaStream_t s, int nsets) {
-  const int grid = nsets * m2l_simt_tiles(level);  // the class index runs over all sets' 8 classes
+                    int accumulate, cudaStream_t s, int nsets, int ngroups, T *part, int64_t part_elems) {
+  const int tiles = nsets * m2l_simt_tiles(level);  // the class index runs over all sets' 8 classes
+  const int64_t P = (int64_t)1 << (level - 1);
+  const int64_t count = 8 * nsets * P * P * P * r;
+  int ng = ngroups > 0 ? ngroups : 1;
+  if (ng > 21) ng = 21;
+  if (!part) ng = 1;
+  else if ((int64_t)ng * count > part_elems) ng = (int)(part_elems / count);
+  if (ng < 1) ng = 1;
+  T *dst = ng > 1 ? part : Lout;
+  const dim3 grid(tiles, ng);
   if (r == 256) {
-    m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, Lout, level, j0, j1, offs, accumulate);
+    m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
   } else if (r == 32) {
-    m2l_simt_kernel<T, 32, 2, 4><<<grid, 256, 0, s>>>(M, Ert, Lout, level, j0, j1, offs, accumulate);
+    m2l_simt_kernel<T, 32, 2, 4><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
   } else {
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L rank must be 32 or 256 (n = 4 or 8)");
   }
-  return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_simt", __FILE__, __LINE__);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || ng == 1) return bbfmm_set_cuda_error(e, "m2l_simt", __FILE__, __LINE__);
+  int sg = (int)((count + 255) / 256);
+  if (sg > 148 * 32) sg = 148 * 32;
+  simt_sum_parts_kernel<T><<<sg, 256, 0, s>>>(count, ng, part, Lout);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_simt parts", __FILE__, __LINE__);
 }
 
 template int launch_m2l_simt<double>(int, const double *, const double *, double *, int, int, int, const int4 *, int,
-                                     cudaStream_t, int);
+                                     cudaStream_t, int, int, double *, int64_t);
 template int launch_m2l_simt<float>(int, const float *, const float *, float *, int, int, int, const int4 *, int,
-                                    cudaStream_t, int);
+                                    cudaStream_t, int, int, float *, int64_t);
 
 // Host table of the 189 offsets of each sibling class, as (k, vx, vy, vz).
 void build_offset_table(int *out /* 8*189*4 */) {

@@ -13,21 +13,27 @@
 
 namespace bbfmm {
 
-// Clenshaw evaluation of S(x_m, x) for all nodes m (bbfmm.c:1682-1690).
+// Lane t < 3 NN of a warp: S(x_m, c) for axis t / NN (c = x, y, z) and node m = t % NN by
+// the Clenshaw recurrence of ComputeSn2 (bbfmm.c:1682-1690), S = 1/2 T_0(x_m) + sum_k
+// T_k(x_m) T_k(c) with Tkz[m n + k] = T_k(x_m); other lanes return 0. The warp shares the
+// 3 NN values by shuffles instead of every lane evaluating all of them.
 template <typename T, int NN>
-__device__ __forceinline__ void sn_nodes(const T *__restrict__ tkz, T x, T *out) {
+__device__ __forceinline__ T sn_lane(const T *__restrict__ tkz, int lane, T x, T y, T z) {
+  if (lane >= 3 * NN) return (T)0;
+  const int a = lane / NN, m = lane % NN;
+  const T c = a == 0 ? x : (a == 1 ? y : z);
+  T d1 = 0, d2 = 0;
 #pragma unroll
-  for (int m = 0; m < NN; ++m) {
-    T d1 = 0, d2 = 0;
-#pragma unroll
-    for (int j = NN - 1; j > 0; --j) {
-      const T d0 = 2 * x * d1 - d2 + tkz[m * NN + j];
-      d2 = d1;
-      d1 = d0;
-    }
-    out[m] = x * d1 - d2 + (T)0.5 * tkz[m * NN];
+  for (int j = NN - 1; j > 0; --j) {
+    const T d0 = 2 * c * d1 - d2 + tkz[m * NN + j];
+    d2 = d1;
+    d1 = d0;
   }
+  return c * d1 - d2 + (T)0.5 * tkz[m * NN];
 }
+
+template <typename T>
+__device__ __forceinline__ T wshfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 
 template <typename T> __device__ __forceinline__ const T *tab_tkz(const Tables &t);
 template <> __device__ __forceinline__ const double *tab_tkz<double>(const Tables &t) { return t.tkz_d; }
@@ -71,32 +77,28 @@ __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, co
       const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
       const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
       const T q = pos4[4 * (int64_t)p + 3];
-      T sx[NN], sy[NN], sz[NN];
-      sn_nodes<T, NN>(s_tkz, x, sx);
-      sn_nodes<T, NN>(s_tkz, y, sy);
-      sn_nodes<T, NN>(s_tkz, z, sz);
+      const T val = sn_lane<T, NN>(s_tkz, lane, x, y, z);
+      const T szl = wshfl(val, 2 * NN + lane % NN);  // l3 = lane % NN for every k (32 % NN == 0)
 #pragma unroll
-      for (int k = 0; k < PER; ++k) {
+      for (int k = 0; k < PER; ++k) {  // N3 is a multiple of 32: every lane has PER outputs
         const int l = lane + 32 * k;
-        if (l < N3) {
-          const int l1 = l / (NN * NN), l2 = (l / NN) % NN, l3 = l % NN;
-          const T w = q * sx[l1] * sy[l2];
-          acc[k] += w * sz[l3];
-        }
+        const int l1 = l / (NN * NN), l2 = (l / NN) % NN;
+        const T w = q * wshfl(val, l1) * wshfl(val, NN + l2);
+        acc[k] += w * szl;
       }
     }
     T *out = S + mm * N3;
 #pragma unroll
-    for (int k = 0; k < PER; ++k) {
-      const int l = lane + 32 * k;
-      if (l < N3) out[l] = pre3 * acc[k];
-    }
+    for (int k = 0; k < PER; ++k) out[lane + 32 * k] = pre3 * acc[k];
   }
 }
 
 // ----------------------------------------------------------------------------- M2M
-// One CTA per parent (grid-stride): children S (level l+1, Morton, contiguous block of
-// 8 n^3) -> parent S (level l). All eight children are visited.
+// One CTA of 256 threads per parent (grid-stride): children S (level l+1, Morton,
+// contiguous block of 8 n^3) -> parent S (level l). All eight children are visited. Each
+// thread holds its share of the NEXT parent's children in registers, loaded while the
+// current parent is contracted, so the loads of a parent are all in flight at once and
+// overlap the arithmetic instead of following it.
 template <typename T, int NN>
 __global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *__restrict__ Sp, int level,
                                                   Tables tabs, int64_t A0, int64_t count) {
@@ -110,11 +112,20 @@ __global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *_
   for (int i = threadIdx.x; i < 2 * N2; i += blockDim.x) cw[i] = cwg[i];
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
+  constexpr int PER = 8 * N3 / 256;  // children values per thread (blockDim = 256)
+  T nxt[PER];
+  auto fetch = [&](int64_t a) {
+    const T *src = Sc + a * 8 * N3 + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) nxt[k] = src[256 * k];
+  };
+  if ((int64_t)blockIdx.x < count) fetch(blockIdx.x);
   for (int64_t a = blockIdx.x; a < count; a += gridDim.x) {
     const int64_t A = A0 + a;  // parent; Sc holds the children of parents A0 .. A0 + count - 1
     __syncthreads();
-    const T *src = Sc + a * 8 * N3;
-    for (int i = threadIdx.x; i < 8 * N3; i += blockDim.x) sc[i] = src[i];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) sc[threadIdx.x + 256 * k] = nxt[k];
+    if (a + gridDim.x < count) fetch(a + gridDim.x);
     __syncthreads();
     // z: sz[(j/2) n3 + l1 n + l3] = sum over zbit of sum_m child_j[l1 n + m] C[zbit][l3][m]
     for (int o = threadIdx.x; o < 4 * N3; o += blockDim.x) {
@@ -167,7 +178,9 @@ __global__ void __launch_bounds__(256) m2m_kernel(const T *__restrict__ Sc, T *_
 }
 
 // ----------------------------------------------------------------------------- L2L
-// One CTA per parent: F_child[j] += (2/n)^3 * interp_j(F_parent), children contiguous.
+// One CTA of 256 threads per parent: F_child[j] += (2/n)^3 * interp_j(F_parent), children
+// contiguous. The next parent's F and its children's current values are loaded into
+// registers while the current parent is interpolated (as in M2M).
 template <typename T, int NN>
 __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *__restrict__ Fc, int level,
                                                   Tables tabs, int64_t A0, int64_t count) {
@@ -181,10 +194,27 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
   for (int i = threadIdx.x; i < 2 * N2; i += blockDim.x) cw[i] = cwg[i];
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
+  constexpr int PERC = 8 * N3 / 256;         // children values per thread (blockDim = 256)
+  constexpr int PERP = (N3 + 255) / 256;     // parent values per thread
+  T nc[PERC], np[PERP], old[PERC];
+  auto fetch = [&](int64_t a) {
+    const T *pp = Fp + (A0 + a) * N3;
+#pragma unroll
+    for (int k = 0; k < PERP; ++k)
+      if (threadIdx.x + 256 * k < N3) np[k] = pp[threadIdx.x + 256 * k];
+    const T *cc = Fc + a * 8 * N3 + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) nc[k] = cc[256 * k];
+  };
+  if ((int64_t)blockIdx.x < count) fetch(blockIdx.x);
   for (int64_t a = blockIdx.x; a < count; a += gridDim.x) {
-    const int64_t A = A0 + a;  // parent; Fc holds the children of parents A0 .. A0 + count - 1
     __syncthreads();
-    for (int i = threadIdx.x; i < N3; i += blockDim.x) fp[i] = Fp[A * N3 + i];
+#pragma unroll
+    for (int k = 0; k < PERP; ++k)
+      if (threadIdx.x + 256 * k < N3) fp[threadIdx.x + 256 * k] = np[k];
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) old[k] = nc[k];
+    if (a + gridDim.x < count) fetch(a + gridDim.x);
     __syncthreads();
     // Fx[j n3 + l1 n2 + l2 n + l3] = sum_m F[m n2 + l2 n + l3] C[j][m][l1]
     for (int o = threadIdx.x; o < 2 * N3; o += blockDim.x) {
@@ -205,12 +235,14 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
     }
     __syncthreads();
     // Fchild_j[l1l2 n + l3] += pre3 * sum_m Fy[(j/2) n3 + l1l2 n + m] C[j%2][m][l3]
-    for (int o = threadIdx.x; o < 8 * N3; o += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) {
+      const int o = threadIdx.x + 256 * k;
       const int j = o / N3, rem = o % N3, l12 = rem / NN, l3 = rem % NN;
       T s = 0;
 #pragma unroll
       for (int m = 0; m < NN; ++m) s += fy[(j / 2) * N3 + l12 * NN + m] * cw[(j % 2) * N2 + m * NN + l3];
-      Fc[(a * 8 + j) * N3 + rem] += pre3 * s;
+      Fc[a * 8 * N3 + o] = old[k] + pre3 * s;
     }
   }
 }
@@ -247,19 +279,23 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
       const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
       const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
       const T q = pos4[4 * (int64_t)p + 3];
-      T sx[NN], sy[NN], sz[NN];
-      sn_nodes<T, NN>(s_tkz, x, sx);
-      sn_nodes<T, NN>(s_tkz, y, sy);
-      sn_nodes<T, NN>(s_tkz, z, sz);
-      // lanes split the (l1, l2) pairs; each sums its l3 row
-      T part = 0;
-      for (int l12 = lane; l12 < N2; l12 += 32) {
-        const int l1 = l12 / NN, l2 = l12 % NN;
-        const T *f = Fm + l12 * NN;
-        T inner = 0;
+      const T val = sn_lane<T, NN>(s_tkz, lane, x, y, z);
+      T sz[NN];
 #pragma unroll
-        for (int l3 = 0; l3 < NN; ++l3) inner += sz[l3] * f[l3];
-        part += sx[l1] * sy[l2] * inner;
+      for (int l3 = 0; l3 < NN; ++l3) sz[l3] = wshfl(val, 2 * NN + l3);
+      // lanes split the (l1, l2) pairs; each sums its l3 row (shuffles by every lane)
+      T part = 0;
+#pragma unroll
+      for (int it = 0; it < (N2 + 31) / 32; ++it) {
+        const int l12 = lane + 32 * it, l12c = l12 < N2 ? l12 : 0;
+        const T a = wshfl(val, l12c / NN), b = wshfl(val, NN + l12c % NN);
+        if (l12 < N2) {
+          const T *f = Fm + l12 * NN;
+          T inner = 0;
+#pragma unroll
+          for (int l3 = 0; l3 < NN; ++l3) inner += sz[l3] * f[l3];
+          part += a * b * inner;
+        }
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
@@ -509,22 +545,23 @@ template int launch_scatter<double, float>(int, const int *, const double *, flo
 // ------------------------------------------------------------ L2P with gradient
 namespace bbfmm {
 
-// S(x_m, x) and dS/dx for all nodes m: Clenshaw recurrence and its derivative.
+// sn_lane and dS/dc: the Clenshaw recurrence differentiated term by term (e_j = d'_j).
 template <typename T, int NN>
-__device__ __forceinline__ void sn_nodes_d(const T *__restrict__ tkz, T x, T *out, T *dout) {
+__device__ __forceinline__ void sn_lane_d(const T *__restrict__ tkz, int lane, T x, T y, T z, T &sv, T &dv) {
+  sv = dv = (T)0;
+  if (lane >= 3 * NN) return;
+  const int a = lane / NN, m = lane % NN;
+  const T c = a == 0 ? x : (a == 1 ? y : z);
+  T d1 = 0, d2 = 0, e1 = 0, e2 = 0;
 #pragma unroll
-  for (int m = 0; m < NN; ++m) {
-    T d1 = 0, d2 = 0, e1 = 0, e2 = 0;  // d_j and d_j' at j+1, j+2
-#pragma unroll
-    for (int j = NN - 1; j > 0; --j) {
-      const T d0 = 2 * x * d1 - d2 + tkz[m * NN + j];
-      const T e0 = 2 * d1 + 2 * x * e1 - e2;
-      d2 = d1; d1 = d0;
-      e2 = e1; e1 = e0;
-    }
-    out[m] = x * d1 - d2 + (T)0.5 * tkz[m * NN];
-    dout[m] = d1 + x * e1 - e2;
+  for (int j = NN - 1; j > 0; --j) {
+    const T d0 = 2 * c * d1 - d2 + tkz[m * NN + j];
+    const T e0 = 2 * d1 + 2 * c * e1 - e2;
+    d2 = d1; d1 = d0;
+    e2 = e1; e1 = e0;
   }
+  sv = c * d1 - d2 + (T)0.5 * tkz[m * NN];
+  dv = d1 + c * e1 - e2;
 }
 
 // One warp per leaf: pot[p] = (2/n)^3 sum_l F[l] Sx Sy Sz (no target factor) and
@@ -559,24 +596,33 @@ __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ po
       const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
       const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
       const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
-      T sx[NN], sy[NN], sz[NN], dx[NN], dy[NN], dz[NN];
-      sn_nodes_d<T, NN>(s_tkz, x, sx, dx);
-      sn_nodes_d<T, NN>(s_tkz, y, sy, dy);
-      sn_nodes_d<T, NN>(s_tkz, z, sz, dz);
-      T v = 0, gx = 0, gy = 0, gz = 0;
-      for (int l12 = lane; l12 < N2; l12 += 32) {
-        const int l1 = l12 / NN, l2 = l12 % NN;
-        const T *f = Fm + l12 * NN;
-        T in0 = 0, in1 = 0;
+      T vs, vd;
+      sn_lane_d<T, NN>(s_tkz, lane, x, y, z, vs, vd);
+      T sz[NN], dz[NN];
 #pragma unroll
-        for (int l3 = 0; l3 < NN; ++l3) {
-          in0 += sz[l3] * f[l3];
-          in1 += dz[l3] * f[l3];
+      for (int l3 = 0; l3 < NN; ++l3) {
+        sz[l3] = wshfl(vs, 2 * NN + l3);
+        dz[l3] = wshfl(vd, 2 * NN + l3);
+      }
+      T v = 0, gx = 0, gy = 0, gz = 0;
+#pragma unroll
+      for (int it = 0; it < (N2 + 31) / 32; ++it) {
+        const int l12 = lane + 32 * it, l12c = l12 < N2 ? l12 : 0;
+        const int l1 = l12c / NN, l2 = l12c % NN;
+        const T sx = wshfl(vs, l1), dx = wshfl(vd, l1), sy = wshfl(vs, NN + l2), dy = wshfl(vd, NN + l2);
+        if (l12 < N2) {
+          const T *f = Fm + l12 * NN;
+          T in0 = 0, in1 = 0;
+#pragma unroll
+          for (int l3 = 0; l3 < NN; ++l3) {
+            in0 += sz[l3] * f[l3];
+            in1 += dz[l3] * f[l3];
+          }
+          v += sx * sy * in0;
+          gx += dx * sy * in0;
+          gy += sx * dy * in0;
+          gz += sx * sy * in1;
         }
-        v += sx[l1] * sy[l2] * in0;
-        gx += dx[l1] * sy[l2] * in0;
-        gy += sx[l1] * dy[l2] * in0;
-        gz += sx[l1] * sy[l2] * in1;
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {

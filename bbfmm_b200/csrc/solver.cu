@@ -179,7 +179,7 @@ int Solver<T>::share_operators(const Solver<T> &o) {
 template <typename T>
 int Solver<T>::alloc_partials() {
   int64_t need = 0;
-  if (sizeof(T) == 8 && r == 256)
+  {  // every full M2L (FP64 DMMA or SIMT) may split its offsets
     for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
       const bool tc = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
       if (tc) continue;
@@ -187,6 +187,7 @@ int Solver<T>::alloc_partials() {
       const int64_t e = dmma_part_elems(l, nsets, g, r);
       if (e > need) need = e;
     }
+  }
   if (need <= Lpart_elems && (need == 0 || Lpart)) return BBFMM_OK;
   if (Lpart) cudaFree(Lpart);
   Lpart = nullptr;
@@ -339,7 +340,8 @@ int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
     return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
                            (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level]);
   if (ni != r) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
-  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets);
+  const int g = tune.m2l_groups[level] > 0 ? tune.m2l_groups[level] : dmma_default_groups(level, nsets);
+  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets, g, Lpart, Lpart_elems);
 }
 
 template <typename T>
@@ -414,7 +416,7 @@ int Solver<T>::m2l_post(int l) {
       TRY(m2l_fp(Ml, l, 0, r, r));
       int g = tune.m2l_groups[l] > 0 ? tune.m2l_groups[l] : dmma_default_groups(l, nsets);
       if ((int64_t)g * cells(l) * r > Lpart_elems) g = 1;
-      mark(ST_M2L, sizeof(T) == 8 && r == 256 && g > 1 ? 2 : 1);  // groups add the partial sum
+      mark(ST_M2L, g > 1 ? 2 : 1);  // groups add the partial sum
     }
     if (!(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
       const T scale = (T)1 / cell_length<T>(l, (T)L);
@@ -551,17 +553,12 @@ int Solver<T>::autotune(const void *q_dev, int io_double) {
         continue;
       }
     }
-    // candidates: (kind, offset groups); only the FP64 DMMA M2L (r = 256) has groups, only
-    // the mixed mode has the tensor-core kind
+    // candidates: (kind, offset groups); only the mixed mode has the tensor-core kind
     std::vector<std::pair<int, int>> cand;
-    const bool fp64_tc_path = sizeof(T) == 8 && r == 256;
     if (mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL) cand.push_back({0, 0});
-    if (fp64_tc_path) {
-      for (int g : {1, 3, 7, 21})
-        if (dmma_part_elems(l, nsets, g, r) <= ((int64_t)1 << 27)) cand.push_back({1, g});
-    } else {
-      cand.push_back({1, 0});
-    }
+    // the DMMA and the SIMT M2L both split their offsets over groups
+    for (int g : {1, 3, 7, 21})
+      if (dmma_part_elems(l, nsets, g, r) * (int64_t)sizeof(T) <= ((int64_t)1 << 30)) cand.push_back({1, g});
     float best = 3.4e38f;
     std::pair<int, int> pick = cand[0];
     if (cand.size() > 1) {

@@ -41,7 +41,7 @@ template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
 template <typename T> int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld, cudaStream_t s, int threads = 256);
 int launch_p2p_mixed_field(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *pot, double *fld, cudaStream_t s, int threads = 256);
-template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1);
+template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0);
 void build_offset_table(int *out);
 constexpr int DMMA_PARTS = 21;  // most offset groups of the FP64 M2L (189 = 9 x 21)
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,

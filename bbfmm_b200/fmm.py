@@ -176,6 +176,28 @@ def batch_depth(N: int, per_leaf: float = 32.0) -> int:
     return max(2, int(round(math.log(max(N, 1) / per_leaf, 8)))) if N > 0 else 2
 
 
+def set_cost(N: int, n: int, maxlev: int) -> float:
+    """Model of one set's device work: M2L flops 2 r^2 x (about 189 8^l pairs per level) plus
+    near-field pairs (27 neighbour leaves of N / 8^maxlev particles each, uniform estimate)."""
+    r = n ** 3 // 2
+    m2l = 2.0 * r * r * sum(189.0 * 8 ** l for l in range(2, maxlev + 1))
+    p2p = 27.0 * N * N / 8 ** maxlev
+    return m2l + 20.0 * p2p  # a pair costs about 20 flops
+
+
+def shard_sets(costs, world: int):
+    """Split set indices over `world` ranks, longest job first onto the least loaded rank
+    (greedy LPT: the largest load is within 4/3 of the optimum). Deterministic; returns one
+    sorted index list per rank."""
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(o) for o in out]
+
+
 class Batch:
     """Many independent particle sets solved together (bbfmm_b200_batch_*).
 
@@ -271,6 +293,15 @@ class Batch:
             out.append({"n": v[0], "maxlev": v[1], "sets": v[2], "particles": v[3], "p2p_threads": v[4],
                         "m2l_kind": v[5:5 + v[1] + 1], "m2l_groups": v[16:16 + v[1] + 1]})
         return out
+
+    def group_stage_times(self, q, g: int):
+        """Stage times (ms) of group g solved alone (q: CUDA tensor of all sets)."""
+        q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        out = self.torch.empty_like(q)
+        ms = (C.c_float * len(_lib.STAGES))()
+        _lib.check(_lib.lib().bbfmm_b200_batch_group_stage_times(self.h, g, C.c_void_p(q.data_ptr()),
+                                                                  C.c_void_p(out.data_ptr()), ms, len(_lib.STAGES)))
+        return dict(zip(_lib.STAGES, [round(v, 3) for v in ms]))
 
     @property
     def graph_nodes(self) -> int:

@@ -433,12 +433,26 @@ def run_batch_256(args):
     the groups as parallel branches of one CUDA graph), after the autotuner; per-set error
     against the FP64 direct sum on 512 sampled targets per set."""
     import torch
-    from bbfmm_b200 import Batch
+    import torch.distributed as dist
+    from bbfmm_b200 import Batch, set_cost, shard_sets
     from bbfmm_b200.fmm import direct
     mode = args.mode
-    sets, q = batch_sets()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    all_sets, all_q = batch_sets()
+    # N GPUs: the sets are split by a cost model (no collective on the data path)
+    offs_all = np.concatenate([[0], np.cumsum([len(x) for x, _, _ in all_sets])])
+    mine = shard_sets([set_cost(len(x), n, lev) for x, n, lev in all_sets], world)[rank]
+    sets = [all_sets[i] for i in mine]
+    q = np.concatenate([all_q[offs_all[i]:offs_all[i + 1]] for i in mine]) if mine else np.zeros(0)
     t0 = time.perf_counter()
-    b = Batch(sets, mode=mode)
+    b = Batch(sets, mode=mode, device=local)
     t_setup = time.perf_counter() - t0
     dt = torch.float32 if mode == "s" else torch.float64
     qd = torch.as_tensor(q, dtype=dt, device="cuda")
@@ -449,9 +463,23 @@ def run_batch_256(args):
     stream = torch.cuda.ExternalStream(b.stream)
     for _ in range(args.warmup):
         b.solve(qd, out=out, graph=True)
-    with ClockSampler(0) as clk:
-        t_graph = _device_time(lambda: b.solve(qd, out=out, graph=True), args.steps, stream)
-    t_eager = _device_time(lambda: b.solve(qd, out=out, graph=False), args.steps, stream)
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    barrier()
+    with ClockSampler(local) as clk:
+        t_graph = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=True), args.steps, stream))
+    barrier()
+    t_eager = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=False), args.steps, stream))
+    group_ms = [b.group_stage_times(qd, g) for g in range(len(groups))]
     phi = out.double().cpu().numpy()
     # per-set error on 512 sampled targets
     rng = np.random.default_rng(77)
@@ -462,20 +490,27 @@ def run_batch_256(args):
         ref = direct(torch.as_tensor(x, device="cuda"), torch.as_tensor(q[a:e], device="cuda"),
                      torch.as_tensor(t, device="cuda")).cpu().numpy()
         errs.append(float(np.linalg.norm(phi[a:e][t] - ref) / np.linalg.norm(ref)))
+    if world > 1:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (errs, [n for _, n, _ in sets]))
+        errs = [e for g in gathered for e in g[0]]
+        ns = np.array([n for g in gathered for n in g[1]])
+    else:
+        ns = np.array([n for _, n, _ in sets])
     errs = np.array(errs)
-    ns = np.array([n for _, n, _ in sets])
-    Ntot = int(b.offsets[-1])
+    Ntot = int(offs_all[-1])
     qh = torch.as_tensor(q, dtype=dt).pin_memory()
     ph = torch.empty_like(qh).pin_memory()
+    barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         qd.copy_(qh, non_blocking=True)
         b.solve(qd, out=out, graph=True)
         ph.copy_(out, non_blocking=True)
     torch.cuda.synchronize()
-    t_e2e = (time.perf_counter() - t0) / args.steps
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and rank == 0:
         # the reference CPU code on 4 of the sets (one per (n, depth) seen first), scaled by particles
         t_ref, n_ref, kinds = 0.0, 0, set()
         for (x, n, lev) in sets:
@@ -493,15 +528,16 @@ def run_batch_256(args):
                    "sample": f"the reference CPU code on {len(kinds)} of the sets ({n_ref} particles, {t_ref:.2f} s), "
                              f"scaled to the batch's {Ntot} particles"}
     line = {"metric": "batched solves of 256 uneven sets (N log-uniform 4,096..262,144, n in {4,8})",
-            "value": 1.0 / t_graph, "unit": "batch/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_graph * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "value": 1.0 / t_graph, "unit": "batch/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_graph * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": {"mixed": "bf16x3+f64", "d": "f64", "s": "f32"}[mode],
             "data": "synthetic (seeded; half uniform, half 4-Gaussian sigma 0.04)",
             "config": {"workload": "256 uneven bbFMM Laplace sets, n in {4,8}, depth round(log8(N/32))",
-                       "particles": Ntot, "mode": mode,
+                       "particles": Ntot, "mode": mode, "parallelism": f"sets sharded over {world} GPU(s)",
                        "groups": [{k: g[k] for k in ("n", "maxlev", "sets", "particles", "p2p_threads",
                                                       "m2l_kind", "m2l_groups")} for g in groups]},
             "particles_per_s": Ntot / t_graph, "eager_ms": t_eager * 1e3, "graph_nodes": b.graph_nodes,
+            "group_stage_ms": group_ms,
             "setup_s": t_setup, "autotune_s": t_tune,
             "err_vs_fp64_direct": {"median": float(np.median(errs)), "max": float(errs.max()),
                                    "max_n4": float(errs[ns == 4].max()), "max_n8": float(errs[ns == 8].max()),
@@ -509,8 +545,11 @@ def run_batch_256(args):
             "e2e": {"value": 1.0 / t_e2e, "unit": "batch/s", "h2d_bytes_per_step": Ntot * qd.element_size(),
                     "d2h_bytes_per_step": Ntot * qd.element_size()},
             "cpu_baseline": cpu, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     b.close()
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 

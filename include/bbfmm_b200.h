@@ -241,6 +241,9 @@ BBFMM_B200_API long long bbfmm_b200_batch_graph_nodes(const bbfmm_b200_batch *b)
 /* Group g: info[0] = n, info[1] = depth, info[2] = sets, info[3] = particles, info[4] = P2P
  * threads, info[5 + l] = M2L kind of level l, info[16 + l] = offset groups; 27 ints. */
 BBFMM_B200_API int bbfmm_b200_batch_group_info(const bbfmm_b200_batch *b, int g, int *info);
+/* Group g solved alone with per-stage timing (see bbfmm_b200_stage_times); synchronises. */
+BBFMM_B200_API int bbfmm_b200_batch_group_stage_times(bbfmm_b200_batch *b, int g, const void *q_dev, void *phi_dev,
+                                                      float *ms, int count);
 BBFMM_B200_API void *bbfmm_b200_batch_stream(bbfmm_b200_batch *b);
 BBFMM_B200_API void bbfmm_b200_batch_destroy(bbfmm_b200_batch *b);
 
