@@ -14,13 +14,16 @@
 // Tile: 128 targets of one sibling class forming an 8x4x4 box of its parent grid
 // (GEMM M = 128) x all 256 outputs i (N = 256) in a 128 x 256 FP32 TMEM accumulator.
 // For an offset v the 128 sources form the same box in one class grid, shifted by a
-// whole number of parent cells, so each K-chunk of the A operand (64 bf16 of j per row)
+// whole number of parent cells, so each K-chunk of the A operand (32 bf16 of j per row)
 // is ONE 5-D TMA box load from the class-major multipole grid; out-of-grid sources are
-// zero-filled by TMA. The B operand chunk is rows i of E_v for the same 64 j.
+// zero-filled by TMA. The B operand chunk is rows i of E_v for the same 32 j. Operand
+// tiles are K-major with 64-byte rows in the 64-byte swizzle.
 //
 // Warp roles (192 threads): warp 0 = TMA producer (and TMEM allocator), warp 1 = MMA
 // issuer, warps 2-5 = epilogue (tcgen05.ld of the accumulator, FP64 update of L).
-// Two pipeline stages of 96 KB (A_hi, A_lo 16 KB each; B_hi, B_lo 32 KB each).
+// Four pipeline stages of 48 KB (A_hi, A_lo 8 KB each; B_hi, B_lo 16 KB each): three
+// chunks are in flight while the MMA warp consumes the fourth, which hides the TMA latency
+// that two stages of 96 KB left exposed (tensor pipe idle ~20% of active cycles).
 // Every mbarrier wait is bounded; on timeout the kernel records an error code in a
 // device status word, skips the remaining work, frees its tensor memory and returns.
 #include <cuda.h>
@@ -35,10 +38,11 @@ namespace bbfmm {
 
 namespace tc {
 
-constexpr int BM = 128, BN = 256, BK = 64;  // targets, outputs, bf16 per K-chunk (128 B)
-constexpr int STAGES = 2;
-constexpr int A_BYTES = BM * BK * 2;        // 16 KB
-constexpr int B_BYTES = BN * BK * 2;        // 32 KB
+constexpr int BM = 128, BN = 256, BK = 32;  // targets, outputs, bf16 per K-chunk (64 B rows)
+constexpr int KS = BK / 16;                 // MMA K-steps per chunk
+constexpr int STAGES = 4;                   // three chunks in flight while one is consumed
+constexpr int A_BYTES = BM * BK * 2;        // 8 KB
+constexpr int B_BYTES = BN * BK * 2;        // 16 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int BOX_X = 8, BOX_Y = 4, BOX_Z = 4;
@@ -96,14 +100,14 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
       : "memory");
 }
 
-// K-major, 128-byte swizzled operand tile: rows of 128 B, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// K-major, 64-byte swizzled operand tile: rows of 64 B (32 bf16), 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
-  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for SW128 K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;               // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;                // stride byte offset: 8 rows x 64 B
   d |= (uint64_t)1 << 46;                         // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;                         // 128-byte swizzle
+  d |= (uint64_t)4 << 61;                         // 64-byte swizzle
   return d;
 }
 
@@ -170,9 +174,9 @@ __global__ void __launch_bounds__(192, 1)
   const int tb = blockIdx.x % tiles_per_class;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int nchunk = BN / BK;    // 4 K-chunks per offset (r = 256)
-  const int chunk0 = kfirst / 4;  // whole chunks skipped
-  const int kstep0 = kfirst % 4;  // K-steps skipped in the first used chunk
+  const int nchunk = BN / BK;     // 8 K-chunks per offset (r = 256)
+  const int chunk0 = kfirst / KS;  // whole chunks skipped
+  const int kstep0 = kfirst % KS;  // K-steps skipped in the first used chunk
   const int used_chunks = nchunk - chunk0;
   const int niter = 189 * used_chunks;
 
@@ -228,10 +232,10 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_after();
       const uint32_t st = base + s * STAGE_BYTES;
       const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
-      for (int ks = k0; ks < BK / 16; ++ks) {
-        const uint64_t ahi = sw128_desc(st + ks * 32), alo = sw128_desc(st + A_BYTES + ks * 32);
-        const uint64_t bhi = sw128_desc(st + 2 * A_BYTES + ks * 32);
-        const uint64_t blo = sw128_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
+      for (int ks = k0; ks < KS; ++ks) {
+        const uint64_t ahi = sw64_desc(st + ks * 32), alo = sw64_desc(st + A_BYTES + ks * 32);
+        const uint64_t bhi = sw64_desc(st + 2 * A_BYTES + ks * 32);
+        const uint64_t blo = sw64_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
         mma_bf16(tmem, ahi, bhi, acc);
         if (nprod != 1) {
           mma_bf16(tmem, ahi, blo, 1u);
@@ -328,7 +332,7 @@ static int make_map(CUtensorMap *m, void *ptr, int rank, const cuuint64_t *dims,
                     const cuuint32_t *box) {
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult rc = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, ptr, dims, strides_bytes, box, es,
-                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (rc != CUDA_SUCCESS) {
     char buf[96];
