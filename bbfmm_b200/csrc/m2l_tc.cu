@@ -100,6 +100,14 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
       : "memory");
 }
 
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1)
+      : "memory");
+}
+
 // K-major, 64-byte swizzled operand tile: rows of 64 B (32 bf16), 8-row groups 512 B apart.
 __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   uint64_t d = 0;
@@ -296,6 +304,159 @@ __global__ void split_kernel(int64_t count, const double *__restrict__ src, __nv
   }
 }
 
+// ---------------------------------------------------------------- projections
+// The U-projections around the M2L with the same split-BF16 tensor-core machinery:
+//   C[out(t)][col0 + n] (=, or += when `add`) scale * cs[col0 + n] * sum_k A[t][k] B[col0 + n][k]
+// for one tile of 128 consecutive rows t of A (its storage order) and 256 columns (blockIdx.y
+// selects the 256-column block), K-chunks kc0 .. kc1-1 of 32. Columns below col_skip are not
+// written (the FP64 leading part owns them). outmap: 1 = A rows are Morton cells row0 + t
+// of `level` and C rows their cpg index (up projection); 0 = same row (down projection, whose
+// A rows were gathered into Morton order). Rows t >= rows are zero-filled by TMA and skipped.
+__global__ void __launch_bounds__(192, 1)
+    proj_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
+                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
+                   double *__restrict__ C, int ldc, int64_t rows, int level, int outmap, int64_t row0, int kc0,
+                   int kc1, int col_skip, int add, const double *__restrict__ cs, double scale) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *gbase = smem_raw + (base - raw);
+  const uint32_t bar_base = base + STAGES * STAGE_BYTES;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * STAGE_BYTES);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 1);
+  auto full_bar = [&](int s) { return bar_base + 8u * s; };
+  auto empty_bar = [&](int s) { return bar_base + 8u * (STAGES + s); };
+  const uint32_t acc_bar = bar_base + 8u * (2 * STAGES);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t0 = (int64_t)blockIdx.x * BM;
+  const int col0 = blockIdx.y * BN;
+  const int niter = kc1 - kc0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(acc_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(empty_bar(s), ph ^ 1u, 11)) break;
+      const int k = (kc0 + it) * BK;
+      const uint32_t st = base + s * STAGE_BYTES;
+      mbar_expect_tx(full_bar(s), STAGE_BYTES);
+      tma_load_2d(st, &mapAhi, full_bar(s), k, (int)t0);
+      tma_load_2d(st + A_BYTES, &mapAlo, full_bar(s), k, (int)t0);
+      tma_load_2d(st + 2 * A_BYTES, &mapBhi, full_bar(s), k, col0);
+      tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(s), k, col0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    uint32_t acc = 0;
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(full_bar(s), ph, 12)) break;
+      tc_fence_after();
+      const uint32_t st = base + s * STAGE_BYTES;
+      for (int ks = 0; ks < KS; ++ks) {
+        const uint64_t ahi = sw64_desc(st + ks * 32), alo = sw64_desc(st + A_BYTES + ks * 32);
+        const uint64_t bhi = sw64_desc(st + 2 * A_BYTES + ks * 32);
+        const uint64_t blo = sw64_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
+        mma_bf16(tmem, ahi, bhi, acc);
+        mma_bf16(tmem, ahi, blo, 1u);
+        mma_bf16(tmem, alo, bhi, 1u);
+        acc = 1u;
+      }
+      mma_commit(empty_bar(s));
+    }
+    mma_commit(acc_bar);  // also after an early exit: the epilogue must not wait forever
+  } else if (warp >= 2) {
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = q * 32 + lane;
+    const bool ok = mbar_wait(acc_bar, 0, 13);
+    tc_fence_after();
+    const int64_t t = t0 + row;
+    if (ok) {
+      int64_t orow = t;
+      if (outmap == 1) {
+        const int64_t m = row0 + t;
+        int ix, iy, iz;
+        morton_to_grid(m, level, ix, iy, iz);
+        orow = (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
+      }
+      double *dst = C + orow * ldc + col0;
+      for (int col = 0; col < BN; col += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);  // every lane takes part
+        if (t >= rows || col0 + col < col_skip) continue;
+#pragma unroll
+        for (int i = 0; i < 32; i += 2) {
+          const double c0 = cs ? scale * cs[col0 + col + i] : scale, c1 = cs ? scale * cs[col0 + col + i + 1] : scale;
+          double2 o = add ? *reinterpret_cast<const double2 *>(dst + col + i) : make_double2(0.0, 0.0);
+          o.x += c0 * (double)v[i];
+          o.y += c1 * (double)v[i + 1];
+          *reinterpret_cast<double2 *>(dst + col + i) = o;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
+// dst = [hi | lo] split of rows x K values; row t comes from src row cpg(row0 + t) of
+// `level` when gather != 0 (Morton order from the class-major grid), else from row t.
+__global__ void split_rows_kernel(int64_t rows, int K, const double *__restrict__ src, int gather, int level,
+                                  int64_t row0, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+  const int64_t count = rows * K;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = e / K;
+    int64_t sr = t;
+    if (gather) {
+      const int64_t m = row0 + t;
+      int ix, iy, iz;
+      morton_to_grid(m, level, ix, iy, iz);
+      sr = (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
+    }
+    const double x = src[sr * K + (e - t * K)];
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[e] = h;
+    lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+  }
+}
+
+// out[c][r] = split(src[r][c]) for an R x Cn row-major FP64 matrix (hi, lo: Cn x R bf16);
+// rows c < zero_rows of the output are zero.
+__global__ void transpose_split_kernel(int R, int Cn, const double *__restrict__ src, __nv_bfloat16 *__restrict__ hi,
+                                       __nv_bfloat16 *__restrict__ lo, int zero_rows) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < R * Cn; e += gridDim.x * blockDim.x) {
+    const int c = e / R, r = e % R;
+    const double x = c < zero_rows ? 0.0 : src[(int64_t)r * Cn + c];
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[e] = h;
+    lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+  }
+}
+
 }  // namespace tc
 
 // --------------------------------------------------------------------- host side
@@ -387,6 +548,101 @@ void tc_free_operators(void *p) {
 }
 
 size_t tc_split_bytes(int r, int64_t ncell) { return (size_t)ncell * r * 2 * 2; }
+
+// Split, transposed copies of the projection operators for proj_tc_kernel.
+struct TcProj {
+  int n3 = 0, r = 0, lead = 0;
+  __nv_bfloat16 *up = nullptr;  // [hi | lo] of Bup^T: r x n3, rows j < lead zero
+  __nv_bfloat16 *dn = nullptr;  // [hi | lo] of Bdn^T: n3 x r
+  CUtensorMap up_hi, up_lo, dn_hi, dn_lo;
+};
+
+static int map2d(CUtensorMap *m, const void *ptr, int64_t rows, int K, int box_rows) {
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+  const cuuint32_t box[2] = {tc::BK, (cuuint32_t)box_rows};
+  return make_map(m, (void *)ptr, 2, dims, strides, box);
+}
+
+int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out,
+                           cudaStream_t s) {
+  *out = nullptr;
+  if (r != tc::BN || n3 % tc::BN || lead % 32 || lead <= 0 || lead >= r)
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core projections need n = 8 (r = 256)");
+  if (!encode_fn()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  TcProj *p = new TcProj();
+  p->n3 = n3; p->r = r; p->lead = lead;
+  const size_t cnt = (size_t)n3 * r;
+  if (cudaMalloc(&p->up, cnt * 4) != cudaSuccess || cudaMalloc(&p->dn, cnt * 4) != cudaSuccess) {
+    tc_free_projections(p);
+    return bbfmm_set_error(BBFMM_ERR_NOMEM, "projection operator split allocation failed");
+  }
+  tc::transpose_split_kernel<<<148, 256, 0, s>>>(n3, r, Bup, p->up, p->up + cnt, lead);  // Bup: n3 x r
+  tc::transpose_split_kernel<<<148, 256, 0, s>>>(r, n3, Bdn, p->dn, p->dn + cnt, 0);     // Bdn: r x n3
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    tc_free_projections(p);
+    return bbfmm_set_cuda_error(e, "split projection operators", __FILE__, __LINE__);
+  }
+  int rc = map2d(&p->up_hi, p->up, r, n3, tc::BN);
+  if (rc == BBFMM_OK) rc = map2d(&p->up_lo, p->up + cnt, r, n3, tc::BN);
+  if (rc == BBFMM_OK) rc = map2d(&p->dn_hi, p->dn, n3, r, tc::BN);
+  if (rc == BBFMM_OK) rc = map2d(&p->dn_lo, p->dn + cnt, n3, r, tc::BN);
+  if (rc != BBFMM_OK) {
+    tc_free_projections(p);
+    return rc;
+  }
+  *out = p;
+  return BBFMM_OK;
+}
+
+void tc_free_projections(void *v) {
+  TcProj *p = (TcProj *)v;
+  if (!p) return;
+  if (p->up) cudaFree(p->up);
+  if (p->dn) cudaFree(p->dn);
+  delete p;
+}
+
+// Up (dir 0): M[cpg(row0 + t)][j] = sum_l S[t][l] Bup[l][j] for j >= lead, t < rows (S split in
+// Asplit = [hi | lo], rows x n3). Down (dir 1): F[t][l] += scale Kw[l] sum_{j >= lead} L'[t][j]
+// Bdn[j][l], t < rows, L' the split L rows in the order of F (Asplit, rows x r).
+int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
+                   const double *cs, double scale, cudaStream_t s) {
+  const TcProj *p = (const TcProj *)pv;
+  if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
+  if (rows <= 0) return BBFMM_OK;
+  const int K = dir == 0 ? p->n3 : p->r;
+  const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Asplit;
+  const __nv_bfloat16 *lo = hi + (size_t)rows * K;
+  CUtensorMap ahi, alo;
+  int rc = map2d(&ahi, hi, rows, K, tc::BM);
+  if (rc == BBFMM_OK) rc = map2d(&alo, lo, rows, K, tc::BM);
+  if (rc != BBFMM_OK) return rc;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc::proj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "proj_tc smem attribute", __FILE__, __LINE__);
+    attr = true;
+  }
+  const dim3 grid((unsigned)((rows + tc::BM - 1) / tc::BM), dir == 0 ? 1 : p->n3 / tc::BN);
+  if (dir == 0)
+    tc::proj_tc_kernel<<<grid, 192, tc::SMEM_BYTES, s>>>(ahi, alo, p->up_hi, p->up_lo, C, p->r, rows, level, 1, row0,
+                                                         0, p->n3 / tc::BK, p->lead, 0, nullptr, 1.0);
+  else
+    tc::proj_tc_kernel<<<grid, 192, tc::SMEM_BYTES, s>>>(ahi, alo, p->dn_hi, p->dn_lo, C, p->n3, rows, level, 0, 0,
+                                                         p->lead / tc::BK, p->r / tc::BK, 0, 1, cs, scale);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "proj_tc", __FILE__, __LINE__);
+}
+
+// [hi | lo] split of rows x K FP64 values; gather != 0 reads row t from the cpg row of Morton
+// cell row0 + t of `level`.
+int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
+                  cudaStream_t s) {
+  __nv_bfloat16 *hi = (__nv_bfloat16 *)dst;
+  tc::split_rows_kernel<<<148 * 8, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "split", __FILE__, __LINE__);
+}
 
 // Msplit = [hi plane | lo plane], each ncell_total * r bf16, same cell order as M.
 int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s) {

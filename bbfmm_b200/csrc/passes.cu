@@ -273,7 +273,16 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
+    // lanes split the (l1, l2) rows of the leaf's F; each lane keeps its rows in registers
+    constexpr int NIT = (N2 + 31) / 32;
     const T *Fm = F + mm * N3;
+    T fr[NIT][NN];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int l12 = lane + 32 * it;
+#pragma unroll
+      for (int l3 = 0; l3 < NN; ++l3) fr[it][l3] = l12 < N2 ? Fm[l12 * NN + l3] : (T)0;
+    }
     for (int p = p0; p < p1; ++p) {
       const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
       const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
@@ -283,17 +292,16 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
       T sz[NN];
 #pragma unroll
       for (int l3 = 0; l3 < NN; ++l3) sz[l3] = wshfl(val, 2 * NN + l3);
-      // lanes split the (l1, l2) pairs; each sums its l3 row (shuffles by every lane)
+      // each lane sums its l3 rows (shuffles by every lane)
       T part = 0;
 #pragma unroll
-      for (int it = 0; it < (N2 + 31) / 32; ++it) {
+      for (int it = 0; it < NIT; ++it) {
         const int l12 = lane + 32 * it, l12c = l12 < N2 ? l12 : 0;
         const T a = wshfl(val, l12c / NN), b = wshfl(val, NN + l12c % NN);
         if (l12 < N2) {
-          const T *f = Fm + l12 * NN;
           T inner = 0;
 #pragma unroll
-          for (int l3 = 0; l3 < NN; ++l3) inner += sz[l3] * f[l3];
+          for (int l3 = 0; l3 < NN; ++l3) inner += sz[l3] * fr[it][l3];
           part += a * b * inner;
         }
       }
@@ -325,7 +333,7 @@ template <typename T, int BN>
 __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N, const T *__restrict__ A,
                                                         const float *__restrict__ A2, const T *__restrict__ B,
                                                         const T *__restrict__ cs, T scale, T *__restrict__ C,
-                                                        int level, int mapmode, int64_t row0) {
+                                                        int level, int mapmode, int64_t row0, int ldc) {
   constexpr int BM = 128, BK = 16, TN = BN / 16;
   __shared__ T sa[BK][BM + 1];
   __shared__ T sb[BK][BN];
@@ -377,7 +385,7 @@ __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N,
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
       const int n = n0 + tx + 16 * j;
-      if (n < N) C[cr * N + n] = scale * (cs ? cs[n] : (T)1) * acc[i][j];
+      if (n < N) C[cr * ldc + n] = scale * (cs ? cs[n] : (T)1) * acc[i][j];
     }
   }
 }
@@ -487,14 +495,15 @@ int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, con
 
 template <typename T>
 int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C,
-                int level, int mapmode, cudaStream_t s, int64_t row0) {
+                int level, int mapmode, cudaStream_t s, int64_t row0, int ldc) {
   if (M <= 0) return BBFMM_OK;
+  if (ldc <= 0) ldc = N;
   if (N >= 64) {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 63) / 64));
-    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0);
+    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc);
   } else {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 31) / 32));
-    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0);
+    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc);
   }
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj", __FILE__, __LINE__);
 }
@@ -527,7 +536,7 @@ int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaS
   template int launch_l2p<T>(int, const T *, const int *, int, T, const Tables &, const T *, T *,          \
                              cudaStream_t, int, int64_t, int64_t);                                         \
   template int launch_proj<T>(int64_t, int, int, const T *, const float *, const T *, const T *, T, T *,   \
-                              int, int, cudaStream_t, int64_t);                                            \
+                              int, int, cudaStream_t, int64_t, int);                                       \
   template int launch_morton_cpg<T>(int, int, const T *, T *, int, cudaStream_t);
 INST(float)
 INST(double)

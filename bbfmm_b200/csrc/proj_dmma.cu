@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
                                                            const double *__restrict__ B,
                                                            const double *__restrict__ cs, double scale,
                                                            double *__restrict__ C, int level, int mapmode,
-                                                           int64_t row0) {
+                                                           int64_t row0, int lda) {
   extern __shared__ __align__(16) double smem[];
   __shared__ int64_t arow[BM];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
     for (int e = tid; e < BM * (BK / 2); e += 256) {  // 64 rows x 8 pairs
       const int row = e / (BK / 2), k2 = (e % (BK / 2)) * 2;
       const int64_t ar = arow[row];
-      const double *src = ar >= 0 ? A + ar * K + k0 + k2 : A;
+      const double *src = ar >= 0 ? A + ar * lda + k0 + k2 : A;
       cp_async16(sa + (uint32_t)(row * AST + k2) * 8u, src, ar >= 0);
     }
     for (int e = tid; e < BK * (BN / 2); e += 256) {  // 16 rows x 128 pairs
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
 // Returns BBFMM_ERR_UNSUPPORTED (without recording an error) when the shape does not fit
 // the tile (K % 16, N % 256); the caller then uses the CUDA-core GEMM.
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
-                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0) {
+                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0, int lda) {
   if (K % pj::BK || N % pj::BN) return BBFMM_ERR_UNSUPPORTED;
   if (M <= 0) return BBFMM_OK;
   static bool attr = false;
@@ -137,7 +137,8 @@ int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, 
     attr = true;
   }
   dim3 grid((unsigned)((M + pj::BM - 1) / pj::BM), (unsigned)(N / pj::BN));
-  pj::proj_dmma_kernel<<<grid, 256, pj::SMEM_BYTES, s>>>(M, K, N, A, B, cs, scale, C, level, mapmode, row0);
+  pj::proj_dmma_kernel<<<grid, 256, pj::SMEM_BYTES, s>>>(M, K, N, A, B, cs, scale, C, level, mapmode, row0,
+                                                          lda > 0 ? lda : K);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_dmma", __FILE__, __LINE__);
 }
 

@@ -134,6 +134,17 @@ int Solver<T>::set_operators(const T *U, const T *E) {
     BBFMM_CUDA_OK(cudaMemcpy(Bup, bup.data(), sizeof(T) * bup.size(), cudaMemcpyHostToDevice));
     BBFMM_CUDA_OK(cudaMemcpy(Bdn, bdn.data(), sizeof(T) * bdn.size(), cudaMemcpyHostToDevice));
     BBFMM_CUDA_OK(cudaDeviceSynchronize());
+    if (mode == MODE_MIXED && r == 256 && sizeof(T) == 8) {
+      std::vector<T> b32((size_t)n3 * PROJ_LEAD);
+      for (int l = 0; l < n3; ++l)
+        for (int i = 0; i < PROJ_LEAD; ++i) b32[(size_t)l * PROJ_LEAD + i] = bup[(size_t)l * r + i];
+      if (!Bup32) TRY(dalloc(&Bup32, b32.size()));
+      BBFMM_CUDA_OK(cudaMemcpy(Bup32, b32.data(), sizeof(T) * b32.size(), cudaMemcpyHostToDevice));
+      if (tcproj) tc_free_projections(tcproj);
+      tcproj = nullptr;
+      TRY(tc_prepare_projections(n3, r, (const double *)Bup, (const double *)Bdn, PROJ_LEAD, &tcproj, stream));
+      BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
+    }
   }
   if (!E) return BBFMM_OK;
   std::vector<T> ert((size_t)BBFMM_NUM_OFFSETS * r * r);
@@ -164,13 +175,16 @@ int Solver<T>::share_operators(const Solver<T> &o) {
     return bbfmm_set_error(BBFMM_ERR_ARG, "operators can only be shared between solvers of the same n and mode");
   if (!o.Ert || !o.kw) return bbfmm_set_error(BBFMM_ERR_STATE, "the sharing solver has no operators");
   if (own_ops) {
-    void *mine[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol};
+    void *mine[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, Bup32};
     for (void *p : mine)
       if (p) cudaFree(p);
     if (tcops) tc_free_operators(tcops);
+    if (tcproj) tc_free_projections(tcproj);
   }
   tkz = o.tkz; cw = o.cw; kw = o.kw; Ert = o.Ert; Ecol = o.Ecol; Bup = o.Bup; Bdn = o.Bdn; kwcol = o.kwcol;
   tcops = o.tcops;
+  tcproj = o.tcproj;
+  Bup32 = o.Bup32;
   own_ops = false;
   return BBFMM_OK;
 }
@@ -227,6 +241,26 @@ int Solver<T>::alloc_work() {
   if (Lbuf) cudaFree(Lbuf);
   TRY(dalloc(&Lbuf, (size_t)nl * r));
   TRY(alloc_partials());
+  // bf16 copies of the projection inputs: the largest slab or level of S and of L rows
+  if (Ssplit) cudaFree(Ssplit);
+  if (Lsplit) cudaFree(Lsplit);
+  Ssplit = Lsplit = nullptr;
+  Ssplit_rows = Lsplit_rows = 0;
+  if (proj_tc()) {
+    int64_t sr = leaf_slab();
+    for (int l = BBFMM_MINLEV; l < maxlev; ++l)
+      if (cells(l) > sr) sr = cells(l);
+    const int64_t lr = sr;  // both are used per slab of the leaf level and per whole level above
+    unsigned char *p = nullptr;
+    TRY(dalloc(&p, (size_t)sr * n3 * 4));
+    Ssplit = p;
+    Ssplit_rows = sr;
+    if (lr > 0) {
+      TRY(dalloc(&p, (size_t)lr * r * 4));
+      Lsplit = p;
+      Lsplit_rows = lr;
+    }
+  }
   if (mode == MODE_MIXED && r == 256) {
     if (Msplit) cudaFree(Msplit);
     unsigned char *p = nullptr;
@@ -311,7 +345,7 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
     const int64_t c = nl - a < sl ? nl - a : sl;
     TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream, nsets, a, c));
     mark(ST_P2M);
-    TRY(proj(c, n3, r, Sl, Bup, nullptr, (T)1, Mall + Moff[maxlev], maxlev, MAP_OUT_CPG, a));
+    TRY(proj_up(c, Sl, maxlev, a));
     mark(ST_PROJ_UP);
     if (maxlev - 1 >= BBFMM_MINLEV) {
       TRY(launch_m2m<T>(n, Sl, S[(maxlev - 1) & 1], maxlev - 1, tb, stream, nsets, a / 8, c / 8));
@@ -323,7 +357,7 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
       TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream, nsets));
       mark(ST_M2M);
     }
-    TRY(proj(cells(l), n3, r, S[l & 1], Bup, nullptr, (T)1, Mall + Moff[l], l, MAP_OUT_CPG));
+    TRY(proj_up(cells(l), S[l & 1], l, 0));
     mark(ST_PROJ_UP);
   }
   if (mode == MODE_MIXED && tcops) {
@@ -355,6 +389,34 @@ int Solver<T>::proj(int64_t Mrows, int K, int Ncols, const T *A, const T *B, con
   return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream, row0);
 }
 
+// Up projection of `rows` S rows (Morton cells row0 .. of `level`) into the level's M (cpg).
+// Mixed mode: components j < PROJ_LEAD in FP64, the rest as split-BF16 tensor-core products.
+template <typename T>
+int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0) {
+  T *Mdst = Mall + Moff[level];
+  if (!proj_tc() || rows > Ssplit_rows)
+    return proj(rows, n3, r, S_rows, Bup, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, row0);
+  TRY(launch_proj<T>(rows, n3, PROJ_LEAD, S_rows, nullptr, Bup32, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, stream,
+                     row0, r));
+  TRY(tc_split_rows(rows, n3, (const double *)S_rows, 0, level, row0, Ssplit, stream));
+  return launch_proj_tc(tcproj, 0, Ssplit, rows, (double *)Mdst, level, row0, nullptr, 1.0, stream);
+}
+
+// Down projection of the level's M2L output (Lbuf, cpg) into `rows` F rows (Morton cells
+// row0 .., assign). Mixed mode: the contraction over j < PROJ_LEAD in FP64 (assign), then the
+// tensor cores add the rest, from L rows gathered into Morton order as split BF16.
+template <typename T>
+int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows) {
+  const T scale = (T)1 / cell_length<T>(level, (T)L);
+  if (!proj_tc() || rows > Lsplit_rows)
+    return proj(rows, r, n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0);
+  TRY(launch_proj_dmma(rows, PROJ_LEAD, n3, (const double *)Lbuf, (const double *)Bdn, (const double *)kw,
+                       (double)scale, (double *)F_rows, level, MAP_IN_CPG, stream, row0, r));
+  TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream));
+  return launch_proj_tc(tcproj, 1, Lsplit, rows, (double *)F_rows, level, 0, (const double *)kw, (double)scale,
+                        stream);
+}
+
 // Leaf level after the M2L: per slab, the down projection of the M2L output (assign), L2L
 // from the parents (add), then L2P (assign) -- the order of the whole-level path.
 template <typename T>
@@ -362,11 +424,10 @@ int Solver<T>::leaf_down(bool field) {
   const Tables tb = tables();
   T *Fl = F[maxlev & 1];
   const int64_t nl = cells(maxlev), sl = leaf_slab();
-  const T scale = (T)1 / cell_length<T>(maxlev, (T)L);
   for (int64_t a = 0; a < nl; a += sl) {
     const int64_t c = nl - a < sl ? nl - a : sl;
     if (slabbed()) {
-      TRY(proj(c, r, n3, Lbuf, Bdn, kw, scale, Fl, maxlev, MAP_IN_CPG, a));
+      TRY(proj_down(maxlev, c, a, Fl));
       mark(ST_PROJ_DOWN);
       if (maxlev > BBFMM_MINLEV) {
         TRY(launch_l2l<T>(n, F[(maxlev - 1) & 1], Fl, maxlev - 1, tb, stream, nsets, a / 8, c / 8));
@@ -419,8 +480,7 @@ int Solver<T>::m2l_post(int l) {
       mark(ST_M2L, g > 1 ? 2 : 1);  // groups add the partial sum
     }
     if (!(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
-      const T scale = (T)1 / cell_length<T>(l, (T)L);
-      TRY(proj(cells(l), r, n3, Lbuf, Bdn, kw, scale, F[l & 1], l, MAP_IN_CPG));
+      TRY(proj_down(l, cells(l), 0, F[l & 1]));
       mark(ST_PROJ_DOWN);
     }
   }
@@ -646,14 +706,15 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 template <typename T>
 void Solver<T>::release() {
   void *ptrs[] = {offs, perm, leaf_start, leafm, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
-                  phis, flds};
+                  phis, flds, Ssplit, Lsplit};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (own_ops) {
-    void *ops[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol};
+    void *ops[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, Bup32};
     for (void *p : ops)
       if (p) cudaFree(p);
     if (tcops) tc_free_operators(tcops);
+    if (tcproj) tc_free_projections(tcproj);
   }
   if (ev[ST_COUNT]) cudaEventDestroy(ev[ST_COUNT]);
   if (own_stream && stream) cudaStreamDestroy(stream);

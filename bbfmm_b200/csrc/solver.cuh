@@ -30,7 +30,7 @@ template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const
 template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 // rows are a slab of the level starting at cell row0 (the cpg side is indexed by level cell)
-template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0);
+template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int ldc = 0);
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
@@ -50,7 +50,7 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
 int dmma_default_groups(int level, int nsets);
 int64_t dmma_part_elems(int level, int nsets, int groups, int r);
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
-                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0);
+                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int lda = 0);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
 int launch_direct_field_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *pot,
                              double *fld, cudaStream_t s);
@@ -68,6 +68,14 @@ size_t tc_split_bytes(int r, int64_t ncell);
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3);
 int tc_status(int clear);
+// Tensor-core projections (m2l_tc.cu): the components j >= lead of the up projection and the
+// contraction over j >= lead of the down projection, as split-BF16 products.
+int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out, cudaStream_t s);
+void tc_free_projections(void *p);
+int launch_proj_tc(const void *p, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
+                   const double *cs, double scale, cudaStream_t s);
+int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
+                  cudaStream_t s);
 constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
 
 // Launch choices of one solver, per level (index = level): what the autotuner sets.
@@ -101,6 +109,14 @@ struct Solver {
   T *kwcol = nullptr;
   int4 *offs = nullptr;
   void *tcops = nullptr;  // mixed mode: split operators for the tensor-core kernel
+  // mixed mode, n = 8: projections with the leading PROJ_LEAD components in FP64 and the rest
+  // as split-BF16 tensor-core products (tcproj: split, transposed U operators)
+  static constexpr int PROJ_LEAD = 32;
+  bool mixed_proj = true;
+  void *tcproj = nullptr;
+  T *Bup32 = nullptr;  // [n3][PROJ_LEAD] leading columns of Bup
+  void *Ssplit = nullptr, *Lsplit = nullptr;  // bf16 [hi | lo] copies of S rows / L rows
+  int64_t Ssplit_rows = 0, Lsplit_rows = 0;
   // particles (sorted by leaf, Morton leaf order)
   int N = 0;
   int *perm = nullptr, *leaf_start = nullptr, *leafm = nullptr;
@@ -140,6 +156,9 @@ struct Solver {
   int share_operators(const Solver<T> &from);  // borrow tables and operators (same n, mode, lead)
   int alloc_partials();                          // Lpart for the current tuning
   int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
+  bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
+  int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0);  // S rows -> Mall (cpg)
+  int proj_down(int level, int64_t rows, int64_t row0, T *F_rows);    // Lbuf -> F rows (Morton, assign)
   // Times the launch choices of every level's M2L and of the near field on this solver's
   // own tree (after an upward pass with q_dev) and keeps the fastest; results are cached per
   // (mode, n, level, target tiles) and (mode, particles, leaves) for later solvers.
