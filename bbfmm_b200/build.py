@@ -26,6 +26,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcomp
 UNITS = [
     ("host_setup.cpp", [], "host_setup"),
     ("passes.cu", [], "passes"),
+    ("passes_dmma.cu", [], "passes_dmma"),
     ("p2p.cu", [], "p2p"),
     ("m2l_simt.cu", [], "m2l_simt"),
     ("m2l_tc.cu", [], "m2l_tc"),

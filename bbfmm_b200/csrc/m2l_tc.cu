@@ -425,11 +425,14 @@ __global__ void __launch_bounds__(192, 1)
 
 // dst = [hi | lo] split of rows x K values; row t comes from src row cpg(row0 + t) of
 // `level` when gather != 0 (Morton order from the class-major grid), else from row t.
+// One warp per row (grid-stride), 8 consecutive values per lane and step: two 32-byte
+// loads, one 16-byte store per plane. K is a multiple of 256.
 __global__ void split_rows_kernel(int64_t rows, int K, const double *__restrict__ src, int gather, int level,
                                   int64_t row0, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
-  const int64_t count = rows * K;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t t = e / K;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t t = warp; t < rows; t += nwarps) {
     int64_t sr = t;
     if (gather) {
       const int64_t m = row0 + t;
@@ -437,10 +440,20 @@ __global__ void split_rows_kernel(int64_t rows, int K, const double *__restrict_
       morton_to_grid(m, level, ix, iy, iz);
       sr = (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
     }
-    const double x = src[sr * K + (e - t * K)];
-    const __nv_bfloat16 h = __double2bfloat16(x);
-    hi[e] = h;
-    lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+    const double4 *in = reinterpret_cast<const double4 *>(src + sr * K);
+    uint4 *oh = reinterpret_cast<uint4 *>(hi + t * K), *ol = reinterpret_cast<uint4 *>(lo + t * K);
+    for (int c = lane; c < K / 8; c += 32) {
+      const double4 a = in[2 * c], b = in[2 * c + 1];
+      const double x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        h[i] = __double2bfloat16(x[i]);
+        l[i] = __double2bfloat16(x[i] - (double)__bfloat162float(h[i]));
+      }
+      oh[c] = *reinterpret_cast<const uint4 *>(h);
+      ol[c] = *reinterpret_cast<const uint4 *>(l);
+    }
   }
 }
 
@@ -639,8 +652,9 @@ int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, do
 // cell row0 + t of `level`.
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
                   cudaStream_t s) {
+  if (K % 256) return bbfmm_set_error(BBFMM_ERR_ARG, "split rows: K must be a multiple of 256");
   __nv_bfloat16 *hi = (__nv_bfloat16 *)dst;
-  tc::split_rows_kernel<<<148 * 8, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K);
+  tc::split_rows_kernel<<<148 * 16, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K);
   return bbfmm_set_cuda_error(cudaGetLastError(), "split", __FILE__, __LINE__);
 }
 

@@ -13,6 +13,10 @@
 
 namespace bbfmm {
 
+// FP64 tensor-path M2M / L2L for n = 8 (passes_dmma.cu).
+int launch_m2m_dmma(const double *Sc, double *Sp, const double *cw, int64_t first, int64_t count, cudaStream_t s);
+int launch_l2l_dmma(const double *Fp, double *Fc, const double *cw, int64_t first, int64_t count, cudaStream_t s);
+
 // Lane t < 3 NN of a warp: S(x_m, c) for axis t / NN (c = x, y, z) and node m = t % NN by
 // the Clenshaw recurrence of ComputeSn2 (bbfmm.c:1682-1690), S = 1/2 T_0(x_m) + sum_k
 // T_k(x_m) T_k(c) with Tkz[m n + k] = T_k(x_m); other lanes return 0. The warp shares the
@@ -454,6 +458,8 @@ int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream
   const size_t smem = sizeof(T) * 14 * n3;
   if (count < 0) count = nsets * pow8i(level) - first;
   if (count <= 0) return BBFMM_OK;
+  if (sizeof(T) == 8 && n == 8)
+    return launch_m2m_dmma((const double *)Sc, (double *)Sp, t.cw_d, first, count, s);
   const int grid = grid_for(count, 1, 148 * 8);
   if (n == 4) {
     m2m_kernel<T, 4><<<grid, 256, smem, s>>>(Sc, Sp, level, t, first, count);
@@ -471,6 +477,8 @@ int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream
   const size_t smem = sizeof(T) * 7 * n3;
   if (count < 0) count = nsets * pow8i(level) - first;
   if (count <= 0) return BBFMM_OK;
+  if (sizeof(T) == 8 && n == 8)
+    return launch_l2l_dmma((const double *)Fp, (double *)Fc, t.cw_d, first, count, s);
   const int grid = grid_for(count, 1, 148 * 8);
   if (n == 4) {
     l2l_kernel<T, 4><<<grid, 256, smem, s>>>(Fp, Fc, level, t, first, count);

@@ -396,8 +396,8 @@ int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0) {
   T *Mdst = Mall + Moff[level];
   if (!proj_tc() || rows > Ssplit_rows)
     return proj(rows, n3, r, S_rows, Bup, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, row0);
-  TRY(launch_proj<T>(rows, n3, PROJ_LEAD, S_rows, nullptr, Bup32, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, stream,
-                     row0, r));
+  TRY(launch_proj_narrow(rows, n3, (const double *)S_rows, (const double *)Bup32, (double *)Mdst, r, level,
+                         MAP_OUT_CPG, stream, row0));
   TRY(tc_split_rows(rows, n3, (const double *)S_rows, 0, level, row0, Ssplit, stream));
   return launch_proj_tc(tcproj, 0, Ssplit, rows, (double *)Mdst, level, row0, nullptr, 1.0, stream);
 }

@@ -51,6 +51,9 @@ int dmma_default_groups(int level, int nsets);
 int64_t dmma_part_elems(int level, int nsets, int groups, int r);
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
                      double *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int lda = 0);
+// C[out(m)][0:32] = sum_k A[m][k] B[k][0:32] on the FP64 tensor path (B: K x 32 contiguous).
+int launch_proj_narrow(int64_t M, int K, const double *A, const double *B, double *C, int ldc, int level,
+                       int mapmode, cudaStream_t s, int64_t row0);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
 int launch_direct_field_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *pot,
                              double *fld, cudaStream_t s);
