@@ -119,15 +119,20 @@ __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   return d;
 }
 
-// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = 256.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N columns
+// (a multiple of 16 up to 256; the accumulator columns [0, N) of the tile are updated).
+__host__ __device__ constexpr uint32_t idesc(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+constexpr uint32_t IDESC = idesc(BN);
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc,
+                                         uint32_t id = IDESC) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc)
+      "l"(adesc), "l"(bdesc), "r"(id), "r"(acc)
       : "memory");
 }
 
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(192, 1)
     m2l_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                   double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
-                  int nprod) {
+                  int split_chunks, int split_rows) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -221,11 +226,13 @@ __global__ void __launch_bounds__(192, 1)
       const int sc = (scx << 2) | (scy << 1) | scz;
       const int sx = bx0 + (gx - scx) / 2, sy = by0 + (gy - scy) / 2, sz = bz0 + (gz - scz) / 2;
       const uint32_t st = base + s * STAGE_BYTES;
-      // one product (hi x hi) needs only the hi halves of A and B
-      mbar_expect_tx(full_bar(s), nprod == 1 ? A_BYTES + B_BYTES : STAGE_BYTES);
+      // chunks kc < split_chunks take three products and need the lo halves (of B only its
+      // first split_rows rows, the box of mapBlo); the others take hi x hi alone
+      const bool three = kc < split_chunks;
+      mbar_expect_tx(full_bar(s), three ? 2 * A_BYTES + B_BYTES + (uint32_t)split_rows * BK * 2 : A_BYTES + B_BYTES);
       tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
       tma_load_3d(st + 2 * A_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
-      if (nprod != 1) {
+      if (three) {
         tma_load_5d(st + A_BYTES, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
         tma_load_3d(st + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
       }
@@ -240,14 +247,16 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_after();
       const uint32_t st = base + s * STAGE_BYTES;
       const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
+      const bool three = chunk0 + it % used_chunks < split_chunks;
+      const uint32_t id_part = idesc(split_rows);
       for (int ks = k0; ks < KS; ++ks) {
         const uint64_t ahi = sw64_desc(st + ks * 32), alo = sw64_desc(st + A_BYTES + ks * 32);
         const uint64_t bhi = sw64_desc(st + 2 * A_BYTES + ks * 32);
         const uint64_t blo = sw64_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
-        mma_bf16(tmem, ahi, bhi, acc);
-        if (nprod != 1) {
-          mma_bf16(tmem, ahi, blo, 1u);
-          mma_bf16(tmem, alo, bhi, 1u);
+        mma_bf16(tmem, ahi, bhi, acc);  // all 256 outputs (first MMA of the tile initialises them)
+        if (three) {                    // corrections for the outputs i < split_rows
+          mma_bf16(tmem, ahi, blo, 1u, id_part);
+          mma_bf16(tmem, alo, bhi, 1u, id_part);
         }
         acc = 1u;
       }
@@ -493,6 +502,7 @@ struct TcOps {
   int r = 0, lead = 0, lead_rows = 0;
   __nv_bfloat16 *Ehi = nullptr, *Elo = nullptr;
   CUtensorMap mapBhi, mapBlo;
+  CUtensorMap mapBlo_part;  // the first TC_SPLIT_ROWS rows i of the lo operator chunk
 };
 
 int tc_supported() {
@@ -544,6 +554,8 @@ int tc_prepare_operators(int r, const double *Ert, int lead, int lead_rows, void
   const cuuint32_t box[3] = {tc::BK, (cuuint32_t)tc::BN, 1};
   int rc = make_map(&ops->mapBhi, ops->Ehi, 3, dims, strides, box);
   if (rc == BBFMM_OK) rc = make_map(&ops->mapBlo, ops->Elo, 3, dims, strides, box);
+  const cuuint32_t box_part[3] = {tc::BK, (cuuint32_t)TC_SPLIT_ROWS, 1};
+  if (rc == BBFMM_OK) rc = make_map(&ops->mapBlo_part, ops->Elo, 3, dims, strides, box_part);
   if (rc != BBFMM_OK) {
     tc_free_operators(ops);
     return rc;
@@ -670,7 +682,11 @@ int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *M
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets, int nprod) {
   const TcOps *ops = (const TcOps *)opsv;
-  if (nprod != 1 && nprod != 3) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 1 or 3");
+  if (nprod != 0 && nprod != 1 && nprod != 3)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 0 (adaptive), 1 or 3");
+  // 3: three products everywhere; 1: one everywhere; 0: three only where one would not do
+  const int split_chunks = nprod == 3 ? tc::BN / tc::BK : (nprod == 1 ? 0 : TC_SPLIT_CHUNKS);
+  const int split_rows = nprod == 0 ? TC_SPLIT_ROWS : tc::BN;
   if (!ops || r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L needs r = 256 operators");
   const int P = 1 << (level - 1);
   if (P < tc::BOX_X) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs level >= 4");
@@ -695,8 +711,9 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   // with a full-width leading strip its K-steps are skipped; otherwise every K-step runs
   const int kfirst = ops->lead_rows >= r ? ops->lead / 16 : 0;
   const int ilead = ops->lead > 0 ? ops->lead_rows : 0;
-  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo, Lacc, level, offs,
-                                                       kfirst, ilead, nprod);
+  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi,
+                                                       split_rows < tc::BN ? ops->mapBlo_part : ops->mapBlo, Lacc,
+                                                       level, offs, kfirst, ilead, split_chunks, split_rows);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc", __FILE__, __LINE__);
 }
 

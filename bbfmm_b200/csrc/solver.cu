@@ -889,7 +889,8 @@ int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *h, long long cells) {
 }
 
 int bbfmm_b200_set_tc_products(bbfmm_b200_solver *h, int nprod) {
-  if (!h || (nprod != 1 && nprod != 3)) return bbfmm_set_error(BBFMM_ERR_ARG, "products must be 1 or 3");
+  if (!h || (nprod != 0 && nprod != 1 && nprod != 3))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "products must be 0 (adaptive), 1 or 3");
   if (h->f) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core products apply to the mixed mode");
   h->d->tc_products = nprod;
   return BBFMM_OK;

@@ -67,7 +67,12 @@ int tc_prepare_operators(int r, const double *Ert, int lead, int lead_rows, void
 void tc_free_operators(void *ops);
 int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *Msplit, cudaStream_t s);
 size_t tc_split_bytes(int r, int64_t ncell);
-// nprod: 3 = hi*hi + hi*lo + lo*hi (split BF16), 1 = hi*hi only (plain BF16 products).
+// nprod: 3 = hi*hi + hi*lo + lo*hi (split BF16) for every term, 1 = hi*hi only (plain BF16
+// products), 0 = adaptive: the three products for components j < 32 TC_SPLIT_CHUNKS and
+// outputs i < TC_SPLIT_ROWS, hi*hi alone elsewhere. With the SVD-ordered operators those
+// other terms are small enough that one BF16 product adds below 1e-8 of |L| (estimated
+// per 32 x 32 block from the operators and typical multipoles).
+constexpr int TC_SPLIT_CHUNKS = 3, TC_SPLIT_ROWS = 96;
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3);
 int tc_status(int clear);
@@ -102,7 +107,7 @@ struct Solver {
   bool own_stream = false;
   bool own_ops = true;  // false: tables and operators borrowed from another solver (share_operators)
   Tuning tune;
-  int tc_products = 3;  // mixed mode: products per term of the tensor-core M2L (3 split, 1 plain BF16)
+  int tc_products = 0;  // mixed mode: tensor-core M2L products (0 adaptive, 3 split everywhere, 1 plain BF16)
   // tables and operators (device)
   T *tkz = nullptr, *cw = nullptr, *kw = nullptr;
   T *Ert = nullptr;  // [316][r][r] row-major

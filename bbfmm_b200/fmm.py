@@ -131,7 +131,8 @@ class Solver:
         return phi
 
     def set_tc_products(self, nprod: int):
-        """Mixed mode: 3 (split BF16, default) or 1 (plain BF16) products per M2L term."""
+        """Mixed mode: 0 (adaptive, default: split BF16 where one product would not do),
+        3 (split BF16 for every term) or 1 (plain BF16) products per M2L term."""
         _lib.check(_lib.lib().bbfmm_b200_set_tc_products(self.h, int(nprod)))
 
     def set_leaf_slab(self, cells: int):
@@ -271,7 +272,8 @@ class Batch:
         return out
 
     def set_tc_products(self, nprod: int):
-        """Mixed mode: 3 (split BF16, default) or 1 (plain BF16) products per M2L term."""
+        """Mixed mode: 0 (adaptive, default: split BF16 where one product would not do),
+        3 (split BF16 for every term) or 1 (plain BF16) products per M2L term."""
         _lib.check(_lib.lib().bbfmm_b200_set_tc_products(self.h, int(nprod)))
 
     def set_leaf_slab(self, cells: int):

@@ -199,8 +199,11 @@ BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
  * and deeper). Reallocates the work buffers when particles are already set. */
 BBFMM_B200_API int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *s, long long cells);
 
-/* MIXED mode: products per term of the tensor-core M2L: 3 (default; hi*hi + hi*lo + lo*hi of
- * the split BF16 operands) or 1 (hi*hi: plain BF16 products, for precision comparisons). */
+/* MIXED mode: products per term of the tensor-core M2L. 0 (default, adaptive): the three
+ * split-BF16 products hi*hi + hi*lo + lo*hi for the contraction components j < 96 and the
+ * outputs i < 96 of every operator, hi*hi alone for the rest, whose terms are small enough
+ * (singular-value ordered operators) that one BF16 product adds below 1e-8 of |L|; 3: the
+ * three products everywhere; 1: hi*hi everywhere (plain BF16, for precision comparisons). */
 BBFMM_B200_API int bbfmm_b200_set_tc_products(bbfmm_b200_solver *s, int nprod);
 
 /* Autotuner (no counterpart in the reference): runs an upward pass with q_dev, then times the
