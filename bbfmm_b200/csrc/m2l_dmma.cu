@@ -145,13 +145,15 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   }
 }
 
-// Leading block only (outputs i < NI <= 64, components j < j1 <= 64): every warp owns one
-// 8-target fragment row and all NI/8 output fragments; a 4-stage cp.async pipeline over
-// the (offset, 16-component chunk) sequence keeps the small per-offset tiles in flight.
-// A is stored [target][j] (stride 20 doubles, conflict-free fragment reads, 16-byte copies).
+// Leading block only (outputs i < NI <= 64, components j < j1 <= 64): a tile of NT targets
+// of one class (NT = 64: a bw^3 box, bw = min(P, 4); NT = 128: an 8x4x4 box, P >= 8); every
+// warp owns NT/64 8-target fragment rows and all NI/8 output fragments, so each B fragment
+// feeds NT/64 DMMAs; a 4-stage cp.async pipeline over the (offset, 16-component chunk)
+// sequence keeps the small per-offset tiles in flight. A is stored [target][j] (stride 20
+// doubles, conflict-free fragment reads, 16-byte copies).
 namespace lead {
-constexpr int NT = 64, BK = 16, STAGES = 4, AST = BK + 4;
-template <int NI>
+constexpr int BK = 16, STAGES = 4, AST = BK + 4;
+template <int NI, int NT>
 struct Cfg {
   static constexpr int BST = NI + 4;
   static constexpr int STAGE = NT * AST + BK * BST;
@@ -159,21 +161,22 @@ struct Cfg {
 };
 }  // namespace lead
 
-template <int NI>
+template <int NI, int NT>
 __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict__ M, const double *__restrict__ Ecol,
                                                        double *__restrict__ Lout, int level, int j1,
                                                        const int4 *__restrict__ offs) {
-  constexpr int BST = lead::Cfg<NI>::BST, STAGE = lead::Cfg<NI>::STAGE, NF = NI / 8;
+  constexpr int BST = lead::Cfg<NI, NT>::BST, STAGE = lead::Cfg<NI, NT>::STAGE, NF = NI / 8, MF = NT / 64;
   extern __shared__ __align__(16) double smem[];
   const int P = 1 << (level - 1);
   const int bw = P < 4 ? P : 4;
-  const int nbox = P / bw;
-  const int tiles_per_class = nbox * nbox * nbox;
+  const int bwx = NT == 128 ? 8 : bw;  // box extent in x (y and z: bw)
+  const int nbx = P / bwx, nbox = P / bw;
+  const int tiles_per_class = nbx * nbox * nbox;
   const int c = blockIdx.x / tiles_per_class;
   const int tb = blockIdx.x % tiles_per_class;
-  const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
+  const int bxo = (tb % nbx) * bwx, byo = ((tb / nbx) % nbox) * bw, bzo = (tb / (nbx * nbox)) * bw;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int nt = bw * bw * bw;
+  const int nt = bwx * bw * bw;
   const int64_t P3 = (int64_t)P * P * P;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nchunk = (j1 + lead::BK - 1) / lead::BK;
@@ -189,10 +192,10 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
       const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
       const int sc = (scx << 2) | (scy << 1) | scz;
       const uint32_t sa = sbase + (uint32_t)((it % lead::STAGES) * STAGE) * 8u;
-      const uint32_t sb = sa + (uint32_t)(lead::NT * lead::AST) * 8u;
-      for (int e = tid; e < lead::NT * (lead::BK / 2); e += 256) {  // 64 targets x 8 pairs of j
+      const uint32_t sb = sa + (uint32_t)(NT * lead::AST) * 8u;
+      for (int e = tid; e < NT * (lead::BK / 2); e += 256) {  // NT targets x 8 pairs of j
         const int t = e / (lead::BK / 2), j2 = (e % (lead::BK / 2)) * 2;
-        const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
+        const int px = bxo + (t % bwx) + shx, py = byo + ((t / bwx) % bw) + shy, pz = bzo + (t / (bwx * bw)) + shz;
         const bool ok = t < nt && jc + j2 < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
         const double *src = ok ? M + ((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + j2 : M;
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa + (uint32_t)(t * lead::AST + j2) * 8u),
@@ -209,9 +212,11 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
     cp_commit();  // (possibly empty) group keeps the wait counts uniform
   };
 
-  double acc[NF][2];
+  double acc[MF][NF][2];
 #pragma unroll
-  for (int f = 0; f < NF; ++f) acc[f][0] = acc[f][1] = 0.0;
+  for (int m = 0; m < MF; ++m)
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
 #pragma unroll
   for (int s = 0; s < lead::STAGES - 1; ++s) issue(s);
   for (int it = 0; it < niter; ++it) {
@@ -219,23 +224,32 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
     __syncthreads();
     issue(it + lead::STAGES - 1);  // refills the stage consumed in iteration it - 1
     const double *A = smem + (it % lead::STAGES) * STAGE;
-    const double *B = A + lead::NT * lead::AST;
+    const double *B = A + NT * lead::AST;
 #pragma unroll
     for (int ks = 0; ks < lead::BK / 4; ++ks) {
       const int k = ks * 4 + (lane & 3);
-      const double af = A[(warp * 8 + (lane >> 2)) * lead::AST + k];
+      double af[MF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) dmma(acc[f][0], acc[f][1], af, B[k * BST + f * 8 + (lane >> 2)]);
+      for (int m = 0; m < MF; ++m) af[m] = A[(warp * 8 * MF + m * 8 + (lane >> 2)) * lead::AST + k];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const double bf = B[k * BST + f * 8 + (lane >> 2)];
+#pragma unroll
+        for (int m = 0; m < MF; ++m) dmma(acc[m][f][0], acc[m][f][1], af[m], bf);
+      }
     }
   }
   cp_wait_all();
-  const int t = warp * 8 + (lane >> 2);
-  if (t >= nt) return;
-  const int px = bxo + (t % bw), py = byo + ((t / bw) % bw), pz = bzo + (t / (bw * bw));
-  double *dst = Lout + ((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px) * R;
 #pragma unroll
-  for (int f = 0; f < NF; ++f)
-    *reinterpret_cast<double2 *>(dst + f * 8 + 2 * (lane & 3)) = make_double2(acc[f][0], acc[f][1]);
+  for (int m = 0; m < MF; ++m) {
+    const int t = warp * 8 * MF + m * 8 + (lane >> 2);
+    if (t >= nt) continue;
+    const int px = bxo + (t % bwx), py = byo + ((t / bwx) % bw), pz = bzo + (t / (bwx * bw));
+    double *dst = Lout + ((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px) * R;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      *reinterpret_cast<double2 *>(dst + f * 8 + 2 * (lane & 3)) = make_double2(acc[m][f][0], acc[m][f][1]);
+  }
 }
 
 // Lout[e] = sum_g part[g][e], in a fixed order.
@@ -285,14 +299,20 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
   if (j0 == 0 && j1 <= 64 && (ni == 32 || ni == 64)) {  // the FP64 leading block
     static bool lattr = false;
     if (!lattr) {
-      cudaFuncSetAttribute(dm::m2l_lead_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           dm::lead::Cfg<32>::SMEM);
-      cudaFuncSetAttribute(dm::m2l_lead_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           dm::lead::Cfg<64>::SMEM);
+      cudaFuncSetAttribute(dm::m2l_lead_kernel<32, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           dm::lead::Cfg<32, 64>::SMEM);
+      cudaFuncSetAttribute(dm::m2l_lead_kernel<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           dm::lead::Cfg<64, 64>::SMEM);
+      cudaFuncSetAttribute(dm::m2l_lead_kernel<32, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           dm::lead::Cfg<32, 128>::SMEM);
       lattr = true;
     }
-    if (ni == 32) dm::m2l_lead_kernel<32><<<grid, 256, dm::lead::Cfg<32>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
-    else dm::m2l_lead_kernel<64><<<grid, 256, dm::lead::Cfg<64>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
+    if (ni == 32 && P >= 8)  // 128-target tiles (8x4x4 boxes)
+      dm::m2l_lead_kernel<32, 128><<<grid / 2, 256, dm::lead::Cfg<32, 128>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
+    else if (ni == 32)
+      dm::m2l_lead_kernel<32, 64><<<grid, 256, dm::lead::Cfg<32, 64>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
+    else
+      dm::m2l_lead_kernel<64, 64><<<grid, 256, dm::lead::Cfg<64, 64>::SMEM, s>>>(M, Ecol, Lout, level, j1, offs);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_lead", __FILE__, __LINE__);
   }
   static bool attr = false;

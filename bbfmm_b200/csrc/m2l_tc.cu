@@ -296,6 +296,158 @@ __global__ void __launch_bounds__(192, 1)
   }
 }
 
+// Two target boxes per CTA for the adaptive product map: one 8x8x4 box of a class (256
+// targets) as two M = 128 halves, each with its own 128 x 256 FP32 accumulator in TMEM (all
+// 512 columns), so every operator chunk loaded into shared memory serves 256 targets and the
+// operator traffic from L2 is halved. The lo halves of B cover the first TC_SPLIT_ROWS rows.
+// Stage: A_hi 16 KB | A_lo 16 KB | B_hi 16 KB | B_lo 6 KB.
+constexpr int A2_BYTES = 2 * A_BYTES, BLO2_BYTES = TC_SPLIT_ROWS * BK * 2;
+constexpr int STAGE2_BYTES = 2 * A2_BYTES + B_BYTES + BLO2_BYTES;
+constexpr int SMEM2_BYTES = STAGES * STAGE2_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int BOX2_Y = 8;
+static_assert(SMEM2_BYTES <= 232448, "two-box stages exceed the shared memory of a CTA");
+
+__global__ void __launch_bounds__(192, 1)
+    m2l_tc2_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
+                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
+                   double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
+                   int split_chunks) {
+  constexpr int STAGE_BYTES = STAGE2_BYTES;
+  constexpr int split_rows = TC_SPLIT_ROWS;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *gbase = smem_raw + (base - raw);
+  const uint32_t bar_base = base + STAGES * STAGE_BYTES;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * STAGE_BYTES);
+  // bars[0..S-1] = full, bars[S..2S-1] = empty, bars[2S] = accumulator ready; tmem slot after
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 1);
+  auto full_bar = [&](int s) { return bar_base + 8u * s; };
+  auto empty_bar = [&](int s) { return bar_base + 8u * (STAGES + s); };
+  const uint32_t acc_bar = bar_base + 8u * (2 * STAGES);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int P = 1 << (level - 1);
+  const int nbx = P / BOX_X, nby = P / BOX2_Y, nbz = P / BOX_Z;
+  const int tiles_per_class = nbx * nby * nbz;
+  const int c = blockIdx.x / tiles_per_class;
+  const int tb = blockIdx.x % tiles_per_class;
+  const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX2_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
+  const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
+  const int nchunk = BN / BK;     // 8 K-chunks per offset (r = 256)
+  const int chunk0 = kfirst / KS;  // whole chunks skipped
+  const int kstep0 = kfirst % KS;  // K-steps skipped in the first used chunk
+  const int used_chunks = nchunk - chunk0;
+  const int niter = 189 * used_chunks;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(acc_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(empty_bar(s), ph ^ 1u, 1)) break;
+      const int o = it / used_chunks, kc = chunk0 + it % used_chunks;
+      const int4 ov = offs[(c & 7) * 189 + o];
+      const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
+      const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
+      const int sc = (scx << 2) | (scy << 1) | scz;
+      const int sx = bx0 + (gx - scx) / 2, sy = by0 + (gy - scy) / 2, sz = bz0 + (gz - scz) / 2;
+      const uint32_t st = base + s * STAGE_BYTES;
+      // chunks kc < split_chunks take three products and need the lo halves (of B only its
+      // first split_rows rows, the box of mapBlo); the others take hi x hi alone
+      const bool three = kc < split_chunks;
+      mbar_expect_tx(full_bar(s), three ? STAGE2_BYTES : A2_BYTES + B_BYTES);
+      tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
+      tma_load_3d(st + 2 * A2_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
+      if (three) {
+        tma_load_5d(st + A2_BYTES, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
+        tma_load_3d(st + 2 * A2_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    uint32_t acc = 0;
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(full_bar(s), ph, 2)) break;
+      tc_fence_after();
+      const uint32_t st = base + s * STAGE_BYTES;
+      const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
+      const bool three = chunk0 + it % used_chunks < split_chunks;
+      const uint32_t id_part = idesc(split_rows);
+      for (int ks = k0; ks < KS; ++ks) {
+        const uint64_t bhi = sw64_desc(st + 2 * A2_BYTES + ks * 32);
+        const uint64_t blo = sw64_desc(st + 2 * A2_BYTES + B_BYTES + ks * 32);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {  // the two 128-target halves of the box, accumulators h * 256
+          const uint64_t ahi = sw64_desc(st + h * A_BYTES + ks * 32);
+          const uint64_t alo = sw64_desc(st + A2_BYTES + h * A_BYTES + ks * 32);
+          mma_bf16(tmem + h * 256, ahi, bhi, acc);  // all 256 outputs (the first MMA initialises them)
+          if (three) {                              // corrections for the outputs i < split_rows
+            mma_bf16(tmem + h * 256, ahi, blo, 1u, id_part);
+            mma_bf16(tmem + h * 256, alo, bhi, 1u, id_part);
+          }
+        }
+        acc = 1u;
+      }
+      mma_commit(empty_bar(s));
+    }
+    mma_commit(acc_bar);  // also after an early exit: the epilogue must not wait forever
+  } else if (warp >= 2) {
+    // ---------------- epilogue: TMEM -> registers -> Lacc
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = q * 32 + lane;
+    const bool ok = mbar_wait(acc_bar, 0, 3);
+    tc_fence_after();
+    for (int h = 0; h < 2 && ok; ++h) {
+      const int rr = h * 128 + row;  // row of the 8x8x4 box: x fastest, then y, then z
+      const int tx = rr % BOX_X, ty = (rr / BOX_X) % BOX2_Y, tz = rr / (BOX_X * BOX2_Y);
+      const int64_t P3 = (int64_t)P * P * P;
+      const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
+      double *dst = Lacc + cell * BN;
+      for (int col = 0; col < BN; col += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 256 + col), v);
+        const bool add = col < ilead;  // ilead is a multiple of 32
+#pragma unroll
+        for (int i = 0; i < 32; i += 2) {
+          double2 o = add ? *reinterpret_cast<const double2 *>(dst + col + i) : make_double2(0.0, 0.0);
+          o.x += (double)v[i];
+          o.y += (double)v[i + 1];
+          *reinterpret_cast<double2 *>(dst + col + i) = o;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
 // ---------------------------------------------------------------- splitting
 // hi/lo bf16 split of src; for operators (r > 0) entries with i < zrows and j < zcols of
 // each row-major r x r block are zeroed (the FP64 leading block).
@@ -697,10 +849,28 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   const cuuint64_t dims[5] = {(cuuint64_t)r, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)8 * nsets};
   const cuuint64_t strides[4] = {(cuuint64_t)r * 2, (cuuint64_t)r * 2 * P, (cuuint64_t)r * 2 * P * P,
                                  (cuuint64_t)r * 2 * P * P * P};
-  const cuuint32_t box[5] = {tc::BK, tc::BOX_X, tc::BOX_Y, tc::BOX_Z, 1};
+  // the adaptive map runs two 128-target halves of an 8x8x4 box per CTA (m2l_tc2_kernel)
+  const bool two = nprod == 0;
+  const cuuint32_t box[5] = {tc::BK, tc::BOX_X, (cuuint32_t)(two ? tc::BOX2_Y : tc::BOX_Y), tc::BOX_Z, 1};
   int rc = make_map(&mapAhi, (void *)hi, 5, dims, strides, box);
   if (rc == BBFMM_OK) rc = make_map(&mapAlo, (void *)lo, 5, dims, strides, box);
   if (rc != BBFMM_OK) return rc;
+  // with a full-width leading strip its K-steps are skipped; otherwise every K-step runs
+  const int kfirst = ops->lead_rows >= r ? ops->lead / 16 : 0;
+  const int ilead = ops->lead > 0 ? ops->lead_rows : 0;
+  if (two) {
+    static bool attr2 = false;
+    if (!attr2) {
+      cudaError_t e =
+          cudaFuncSetAttribute(tc::m2l_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM2_BYTES);
+      if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc2 smem attribute", __FILE__, __LINE__);
+      attr2 = true;
+    }
+    const int tiles2 = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX2_Y) * (P / tc::BOX_Z);
+    tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo_part, Lacc,
+                                                            level, offs, kfirst, ilead, split_chunks);
+    return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
+  }
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(tc::m2l_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
@@ -708,9 +878,6 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     attr = true;
   }
   const int tiles = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
-  // with a full-width leading strip its K-steps are skipped; otherwise every K-step runs
-  const int kfirst = ops->lead_rows >= r ? ops->lead / 16 : 0;
-  const int ilead = ops->lead > 0 ? ops->lead_rows : 0;
   tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi,
                                                        split_rows < tc::BN ? ops->mapBlo_part : ops->mapBlo, Lacc,
                                                        level, offs, kfirst, ilead, split_chunks, split_rows);

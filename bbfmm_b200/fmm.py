@@ -124,9 +124,13 @@ class Solver:
         caller.wait_event(done)
         return pot, fld
 
-    def solve_host(self, q):
+    def solve_host(self, q, out=None):
+        """Host charges -> host q_i * phi_i (copies in, solves, copies out, synchronises).
+        out: an optional host array of the same size (pinned memory makes the copy direct)."""
         q = np.ascontiguousarray(np.asarray(q, dtype=self.np_dtype))
-        phi = np.empty_like(q)
+        phi = np.empty_like(q) if out is None else out
+        if phi.dtype != self.np_dtype or phi.size != q.size or not phi.flags.c_contiguous:
+            raise ValueError("out must be a contiguous array of the solver's dtype and q's size")
         _lib.check(_lib.lib().bbfmm_b200_solve_host(self.h, _ptr(q), _ptr(phi)))
         return phi
 
