@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_batch_destroy.argtypes = [vp]
         L.bbfmm_b200_batch_destroy.restype = None
         L.bbfmm_b200_device_status.argtypes = [i]
+        L.bbfmm_b200_wait_selftest.argtypes = [C.c_uint]
         L.bbfmm_b200_near_field.argtypes = [i, i, d, vp, vp, vp, i, vp]
         L.bbfmm_b200_near_field_noalloc.argtypes = [i, i, d, vp, vp, vp, i, vp]
         L.bbfmm_b200_stream.argtypes = [vp]

@@ -448,6 +448,25 @@ __global__ void __launch_bounds__(192, 1)
   }
 }
 
+// ---------------------------------------------------------------- wait probe
+// Failure detection without a fault: an mbarrier that nothing arrives at, waited on with the
+// bounded wait of the kernels above (at most `limit` try_wait polls). The wait must give up,
+// record `code` in the status word and return, leaving the context usable.
+__global__ void wait_probe_kernel(uint32_t limit, int code) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t i = 0; i < limit; ++i)
+      if (mbar_try(b, 0)) return;  // cannot happen: no thread arrives
+    atomicCAS(&g_tc_status, 0, code);
+  }
+}
+
 // ---------------------------------------------------------------- splitting
 // hi/lo bf16 split of src; for operators (r > 0) entries with i < zrows and j < zcols of
 // each row-major r x r block are zeroed (the FP64 leading block).
@@ -882,6 +901,14 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
                                                        split_rows < tc::BN ? ops->mapBlo_part : ops->mapBlo, Lacc,
                                                        level, offs, kfirst, ilead, split_chunks, split_rows);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc", __FILE__, __LINE__);
+}
+
+// Runs the wait probe; returns the status word it left (then cleared), or -1 on a CUDA error.
+int tc_wait_probe(unsigned limit, int code) {
+  tc_status(1);
+  tc::wait_probe_kernel<<<1, 32>>>(limit, code);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return -1;
+  return tc_status(1);
 }
 
 // Reads and clears the kernel status word (0 = every bounded wait completed).

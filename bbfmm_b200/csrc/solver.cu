@@ -862,6 +862,11 @@ int bbfmm_b200_time_m2l(bbfmm_b200_solver *h, int level, int reps, float *ms) {
 
 int bbfmm_b200_device_status(int clear) { return bbfmm::tc_status(clear); }
 
+int bbfmm_b200_wait_selftest(unsigned limit) {
+  if (limit == 0 || limit > (1u << 24)) return -bbfmm_set_error(BBFMM_ERR_ARG, "limit must be in [1, 2^24]");
+  return bbfmm::tc_wait_probe(limit, BBFMM_B200_WAIT_SELFTEST_CODE);
+}
+
 int bbfmm_b200_direct(int N, const double *xyz_dev, const double *q_dev, int ntarget, const int *targets_dev,
                       double *out_dev, void *stream) {
   if (N < 0 || ntarget < 0 || (ntarget > 0 && (!xyz_dev || !q_dev || !targets_dev || !out_dev)))

@@ -76,6 +76,7 @@ constexpr int TC_SPLIT_CHUNKS = 3, TC_SPLIT_ROWS = 96;
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3);
 int tc_status(int clear);
+int tc_wait_probe(unsigned limit, int code);
 // Tensor-core projections (m2l_tc.cu): the components j >= lead of the up projection and the
 // contraction over j >= lead of the down projection, as split-BF16 products.
 int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out, cudaStream_t s);

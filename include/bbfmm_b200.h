@@ -158,6 +158,15 @@ BBFMM_B200_API int bbfmm_b200_direct_field(int N, const double *xyz_dev, const d
  * remaining work and returned). Synchronises the device; clear != 0 resets the word. */
 BBFMM_B200_API int bbfmm_b200_device_status(int clear);
 
+/* Failure-detection self test (no counterpart in the reference): one kernel waits, with the
+ * bounded mbarrier wait of the tensor-core kernels (at most `limit` polls, 1 .. 2^24), on a
+ * barrier that nothing arrives at. The wait gives up, the kernel records
+ * BBFMM_B200_WAIT_SELFTEST_CODE in the status word and returns; the call synchronises,
+ * returns the status word it found (BBFMM_B200_WAIT_SELFTEST_CODE when the mechanism works)
+ * and clears it. No fault, trap or hang is involved; the context stays usable. */
+#define BBFMM_B200_WAIT_SELFTEST_CODE 99
+BBFMM_B200_API int bbfmm_b200_wait_selftest(unsigned limit);
+
 /* Near-field (P2P) part of the solve on caller-owned device arrays, the work of
  * anotherNearField (anotherNearField.c:219-346) and of the reference GPU kernel `direct`
  * (direct.cu:69-209): phi[k] += q_k sum_{B in N(A)} sum_{j in B, r != 0} q_j / r_kj over the
