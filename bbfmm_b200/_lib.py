@@ -53,6 +53,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_direct_field.argtypes = [i, vp, vp, i, vp, vp, vp, vp]
         L.bbfmm_b200_autotune.argtypes = [vp, vp]
         L.bbfmm_b200_set_tc_products.argtypes = [vp, i]
+        L.bbfmm_b200_set_rank.argtypes = [vp, i]
         L.bbfmm_b200_set_leaf_slab.argtypes = [vp, C.c_longlong]
         L.bbfmm_b200_tuning.argtypes = [vp, ip]
         L.bbfmm_b200_batch_create.argtypes = [C.POINTER(Config), i, ip, ip, ip, vp, vp, vp, vp, vp, i, C.POINTER(vp)]

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(192, 1)
     m2l_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                   double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
-                  int split_chunks, int split_rows) {
+                  int split_chunks, int split_rows, int ncols) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(192, 1)
   const int tb = blockIdx.x % tiles_per_class;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int nchunk = BN / BK;     // 8 K-chunks per offset (r = 256)
+  const int nchunk = ncols / BK;  // K-chunks per offset: the effective rank / 32 (8 for r = 256)
   const int chunk0 = kfirst / KS;  // whole chunks skipped
   const int kstep0 = kfirst % KS;  // K-steps skipped in the first used chunk
   const int used_chunks = nchunk - chunk0;
@@ -229,7 +229,8 @@ __global__ void __launch_bounds__(192, 1)
       // chunks kc < split_chunks take three products and need the lo halves (of B only its
       // first split_rows rows, the box of mapBlo); the others take hi x hi alone
       const bool three = kc < split_chunks;
-      mbar_expect_tx(full_bar(s), three ? 2 * A_BYTES + B_BYTES + (uint32_t)split_rows * BK * 2 : A_BYTES + B_BYTES);
+      const uint32_t bhi_bytes = (uint32_t)ncols * BK * 2;  // the B box holds the first ncols rows i
+      mbar_expect_tx(full_bar(s), three ? 2 * A_BYTES + bhi_bytes + (uint32_t)split_rows * BK * 2 : A_BYTES + bhi_bytes);
       tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
       tma_load_3d(st + 2 * A_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
       if (three) {
@@ -248,12 +249,12 @@ __global__ void __launch_bounds__(192, 1)
       const uint32_t st = base + s * STAGE_BYTES;
       const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
       const bool three = chunk0 + it % used_chunks < split_chunks;
-      const uint32_t id_part = idesc(split_rows);
+      const uint32_t id_part = idesc(split_rows), id_all = idesc(ncols);
       for (int ks = k0; ks < KS; ++ks) {
         const uint64_t ahi = sw64_desc(st + ks * 32), alo = sw64_desc(st + A_BYTES + ks * 32);
         const uint64_t bhi = sw64_desc(st + 2 * A_BYTES + ks * 32);
         const uint64_t blo = sw64_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
-        mma_bf16(tmem, ahi, bhi, acc);  // all 256 outputs (first MMA of the tile initialises them)
+        mma_bf16(tmem, ahi, bhi, acc, id_all);  // all ncols outputs (the first MMA initialises them)
         if (three) {                    // corrections for the outputs i < split_rows
           mma_bf16(tmem, ahi, blo, 1u, id_part);
           mma_bf16(tmem, alo, bhi, 1u, id_part);
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(192, 1)
       const int64_t P3 = (int64_t)P * P * P;
       const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
       double *dst = Lacc + cell * BN;
-      for (int col = 0; col < BN; col += 32) {
+      for (int col = 0; col < ncols; col += 32) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
         const bool add = col < ilead;  // ilead is a multiple of 32
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(192, 1)
     m2l_tc2_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                    const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                    double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
-                   int split_chunks) {
+                   int split_chunks, int ncols) {
   constexpr int STAGE_BYTES = STAGE2_BYTES;
   constexpr int split_rows = TC_SPLIT_ROWS;
   extern __shared__ uint8_t smem_raw[];
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(192, 1)
   const int tb = blockIdx.x % tiles_per_class;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX2_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int nchunk = BN / BK;     // 8 K-chunks per offset (r = 256)
+  const int nchunk = ncols / BK;  // K-chunks per offset: the effective rank / 32 (8 for r = 256)
   const int chunk0 = kfirst / KS;  // whole chunks skipped
   const int kstep0 = kfirst % KS;  // K-steps skipped in the first used chunk
   const int used_chunks = nchunk - chunk0;
@@ -376,7 +377,8 @@ __global__ void __launch_bounds__(192, 1)
       // chunks kc < split_chunks take three products and need the lo halves (of B only its
       // first split_rows rows, the box of mapBlo); the others take hi x hi alone
       const bool three = kc < split_chunks;
-      mbar_expect_tx(full_bar(s), three ? STAGE2_BYTES : A2_BYTES + B_BYTES);
+      const uint32_t bhi_bytes = (uint32_t)ncols * BK * 2;  // the B box holds the first ncols rows i
+      mbar_expect_tx(full_bar(s), three ? 2 * A2_BYTES + bhi_bytes + BLO2_BYTES : A2_BYTES + bhi_bytes);
       tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
       tma_load_3d(st + 2 * A2_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
       if (three) {
@@ -395,7 +397,7 @@ __global__ void __launch_bounds__(192, 1)
       const uint32_t st = base + s * STAGE_BYTES;
       const int k0 = (it % used_chunks == 0) ? kstep0 : 0;
       const bool three = chunk0 + it % used_chunks < split_chunks;
-      const uint32_t id_part = idesc(split_rows);
+      const uint32_t id_part = idesc(split_rows), id_all = idesc(ncols);
       for (int ks = k0; ks < KS; ++ks) {
         const uint64_t bhi = sw64_desc(st + 2 * A2_BYTES + ks * 32);
         const uint64_t blo = sw64_desc(st + 2 * A2_BYTES + B_BYTES + ks * 32);
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int h = 0; h < 2; ++h) {  // the two 128-target halves of the box, accumulators h * 256
           const uint64_t ahi = sw64_desc(st + h * A_BYTES + ks * 32);
           const uint64_t alo = sw64_desc(st + A2_BYTES + h * A_BYTES + ks * 32);
-          mma_bf16(tmem + h * 256, ahi, bhi, acc);  // all 256 outputs (the first MMA initialises them)
+          mma_bf16(tmem + h * 256, ahi, bhi, acc, id_all);  // all ncols outputs (the first initialises)
           if (three) {                              // corrections for the outputs i < split_rows
             mma_bf16(tmem + h * 256, ahi, blo, 1u, id_part);
             mma_bf16(tmem + h * 256, alo, bhi, 1u, id_part);
@@ -426,7 +428,7 @@ __global__ void __launch_bounds__(192, 1)
       const int64_t P3 = (int64_t)P * P * P;
       const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
       double *dst = Lacc + cell * BN;
-      for (int col = 0; col < BN; col += 32) {
+      for (int col = 0; col < ncols; col += 32) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 256 + col), v);
         const bool add = col < ilead;  // ilead is a multiple of 32
@@ -804,7 +806,7 @@ void tc_free_projections(void *v) {
 // Asplit = [hi | lo], rows x n3). Down (dir 1): F[t][l] += scale Kw[l] sum_{j >= lead} L'[t][j]
 // Bdn[j][l], t < rows, L' the split L rows in the order of F (Asplit, rows x r).
 int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
-                   const double *cs, double scale, cudaStream_t s) {
+                   const double *cs, double scale, cudaStream_t s, int rank) {
   const TcProj *p = (const TcProj *)pv;
   if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
   if (rows <= 0) return BBFMM_OK;
@@ -827,7 +829,8 @@ int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, do
                                                          0, p->n3 / tc::BK, p->lead, 0, nullptr, 1.0);
   else
     tc::proj_tc_kernel<<<grid, 192, tc::SMEM_BYTES, s>>>(ahi, alo, p->dn_hi, p->dn_lo, C, p->n3, rows, level, 0, 0,
-                                                         p->lead / tc::BK, p->r / tc::BK, 0, 1, cs, scale);
+                                                         p->lead / tc::BK, (rank > 0 ? rank : p->r) / tc::BK, 0, 1, cs,
+                                                         scale);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_tc", __FILE__, __LINE__);
 }
 
@@ -851,13 +854,18 @@ int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *M
 }
 
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
-                  int level, const int4 *offs, cudaStream_t s, int nsets, int nprod) {
+                  int level, const int4 *offs, cudaStream_t s, int nsets, int nprod, int rank) {
   const TcOps *ops = (const TcOps *)opsv;
   if (nprod != 0 && nprod != 1 && nprod != 3)
     return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 0 (adaptive), 1 or 3");
   // 3: three products everywhere; 1: one everywhere; 0: three only where one would not do
-  const int split_chunks = nprod == 3 ? tc::BN / tc::BK : (nprod == 1 ? 0 : TC_SPLIT_CHUNKS);
-  const int split_rows = nprod == 0 ? TC_SPLIT_ROWS : tc::BN;
+  if (rank <= 0) rank = tc::BN;
+  if (rank % tc::BK || rank > tc::BN) return bbfmm_set_error(BBFMM_ERR_ARG, "rank must be a multiple of 32 <= 256");
+  const int nchunk = rank / tc::BK;
+  int split_chunks = nprod == 3 ? nchunk : (nprod == 1 ? 0 : TC_SPLIT_CHUNKS);
+  if (split_chunks > nchunk) split_chunks = nchunk;
+  int split_rows = nprod == 0 ? TC_SPLIT_ROWS : rank;
+  if (split_rows > rank) split_rows = rank;
   if (!ops || r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L needs r = 256 operators");
   const int P = 1 << (level - 1);
   if (P < tc::BOX_X) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs level >= 4");
@@ -869,7 +877,7 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   const cuuint64_t strides[4] = {(cuuint64_t)r * 2, (cuuint64_t)r * 2 * P, (cuuint64_t)r * 2 * P * P,
                                  (cuuint64_t)r * 2 * P * P * P};
   // the adaptive map runs two 128-target halves of an 8x8x4 box per CTA (m2l_tc2_kernel)
-  const bool two = nprod == 0;
+  const bool two = nprod == 0 && split_rows == TC_SPLIT_ROWS;
   const cuuint32_t box[5] = {tc::BK, tc::BOX_X, (cuuint32_t)(two ? tc::BOX2_Y : tc::BOX_Y), tc::BOX_Z, 1};
   int rc = make_map(&mapAhi, (void *)hi, 5, dims, strides, box);
   if (rc == BBFMM_OK) rc = make_map(&mapAlo, (void *)lo, 5, dims, strides, box);
@@ -877,6 +885,22 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   // with a full-width leading strip its K-steps are skipped; otherwise every K-step runs
   const int kfirst = ops->lead_rows >= r ? ops->lead / 16 : 0;
   const int ilead = ops->lead > 0 ? ops->lead_rows : 0;
+  // B boxes of the first `rank` operator rows (the effective rank); the lo box keeps its
+  // split_rows rows (box maps built here when they differ from the prepared ones)
+  CUtensorMap mapBhi = ops->mapBhi, mapBlo = split_rows < tc::BN ? ops->mapBlo_part : ops->mapBlo;
+  {
+    const cuuint64_t bd[3] = {(cuuint64_t)r, (cuuint64_t)r, (cuuint64_t)BBFMM_NUM_OFFSETS};
+    const cuuint64_t bs[2] = {(cuuint64_t)r * 2, (cuuint64_t)r * r * 2};
+    if (rank != tc::BN) {
+      const cuuint32_t bb[3] = {tc::BK, (cuuint32_t)rank, 1};
+      rc = make_map(&mapBhi, ops->Ehi, 3, bd, bs, bb);
+    }
+    if (rc == BBFMM_OK && split_rows != tc::BN && split_rows != TC_SPLIT_ROWS) {
+      const cuuint32_t bl[3] = {tc::BK, (cuuint32_t)split_rows, 1};
+      rc = make_map(&mapBlo, ops->Elo, 3, bd, bs, bl);
+    }
+    if (rc != BBFMM_OK) return rc;
+  }
   if (two) {
     static bool attr2 = false;
     if (!attr2) {
@@ -886,8 +910,8 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
       attr2 = true;
     }
     const int tiles2 = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX2_Y) * (P / tc::BOX_Z);
-    tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi, ops->mapBlo_part, Lacc,
-                                                            level, offs, kfirst, ilead, split_chunks);
+    tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs,
+                                                            kfirst, ilead, split_chunks, rank);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
   }
   static bool attr = false;
@@ -897,9 +921,8 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     attr = true;
   }
   const int tiles = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
-  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, ops->mapBhi,
-                                                       split_rows < tc::BN ? ops->mapBlo_part : ops->mapBlo, Lacc,
-                                                       level, offs, kfirst, ilead, split_chunks, split_rows);
+  tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst,
+                                                       ilead, split_chunks, split_rows, rank);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc", __FILE__, __LINE__);
 }
 

@@ -337,7 +337,7 @@ template <typename T, int BN>
 __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N, const T *__restrict__ A,
                                                         const float *__restrict__ A2, const T *__restrict__ B,
                                                         const T *__restrict__ cs, T scale, T *__restrict__ C,
-                                                        int level, int mapmode, int64_t row0, int ldc) {
+                                                        int level, int mapmode, int64_t row0, int ldc, int lda) {
   constexpr int BM = 128, BK = 16, TN = BN / 16;
   __shared__ T sa[BK][BM + 1];
   __shared__ T sb[BK][BN];
@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N,
       T v = 0;
       if (m < M && k0 + c < K) {
         const int64_t ar = map_row(m, row0, level, MAP_IN_CPG, mapmode);
-        v = A[ar * K + k0 + c];
-        if (A2) v += (T)A2[ar * K + k0 + c];
+        v = A[ar * lda + k0 + c];
+        if (A2) v += (T)A2[ar * lda + k0 + c];
       }
       sa[c][r] = v;
     }
@@ -503,15 +503,16 @@ int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, con
 
 template <typename T>
 int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C,
-                int level, int mapmode, cudaStream_t s, int64_t row0, int ldc) {
+                int level, int mapmode, cudaStream_t s, int64_t row0, int ldc, int lda) {
   if (M <= 0) return BBFMM_OK;
   if (ldc <= 0) ldc = N;
+  if (lda <= 0) lda = K;
   if (N >= 64) {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 63) / 64));
-    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc);
+    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc, lda);
   } else {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 31) / 32));
-    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc);
+    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc, lda);
   }
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj", __FILE__, __LINE__);
 }
@@ -544,7 +545,7 @@ int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaS
   template int launch_l2p<T>(int, const T *, const int *, int, T, const Tables &, const T *, T *,          \
                              cudaStream_t, int, int64_t, int64_t);                                         \
   template int launch_proj<T>(int64_t, int, int, const T *, const float *, const T *, const T *, T, T *,   \
-                              int, int, cudaStream_t, int64_t, int);                                       \
+                              int, int, cudaStream_t, int64_t, int, int);                                  \
   template int launch_morton_cpg<T>(int, int, const T *, T *, int, cudaStream_t);
 INST(float)
 INST(double)

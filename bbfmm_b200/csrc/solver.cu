@@ -284,6 +284,9 @@ int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const
   const int64_t nl = cells(maxlev);
   if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(leafm); cudaFree(pos4); cudaFree(phis); }
   if (flds) cudaFree(flds);  // sized 3 N: reallocated by the next solve_fields
+  if (io_q) cudaFree(io_q);  // sized N: reallocated by the next host-buffer solve
+  if (io_phi) cudaFree(io_phi);
+  io_q = io_phi = nullptr;
   perm = leaf_start = leafm = nullptr; pos4 = phis = flds = nullptr;
   N = N_;
   TRY(dalloc(&perm, N > 0 ? N : 1));
@@ -380,13 +383,13 @@ int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
 
 template <typename T>
 int Solver<T>::proj(int64_t Mrows, int K, int Ncols, const T *A, const T *B, const T *cs, T scale, T *C, int level,
-                    int mapmode, int64_t row0) {
+                    int mapmode, int64_t row0, int lda) {
   if (sizeof(T) == 8) {
     int rc = launch_proj_dmma(Mrows, K, Ncols, (const double *)A, (const double *)B, (const double *)cs,
-                              (double)scale, (double *)C, level, mapmode, stream, row0);
+                              (double)scale, (double *)C, level, mapmode, stream, row0, lda);
     if (rc != BBFMM_ERR_UNSUPPORTED) return rc;
   }
-  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream, row0);
+  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream, row0, 0, lda);
 }
 
 // Up projection of `rows` S rows (Morton cells row0 .. of `level`) into the level's M (cpg).
@@ -408,13 +411,13 @@ int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0) {
 template <typename T>
 int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows) {
   const T scale = (T)1 / cell_length<T>(level, (T)L);
-  if (!proj_tc() || rows > Lsplit_rows)
-    return proj(rows, r, n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0);
+  if (!proj_tc() || rows > Lsplit_rows)  // contraction over the effective rank (j < rk())
+    return proj(rows, rk(), n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0, r);
   TRY(launch_proj_dmma(rows, PROJ_LEAD, n3, (const double *)Lbuf, (const double *)Bdn, (const double *)kw,
                        (double)scale, (double *)F_rows, level, MAP_IN_CPG, stream, row0, r));
   TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream));
   return launch_proj_tc(tcproj, 1, Lsplit, rows, (double *)F_rows, level, 0, (const double *)kw, (double)scale,
-                        stream);
+                        stream, rk());
 }
 
 // Leaf level after the M2L: per slab, the down projection of the M2L output (assign), L2L
@@ -466,15 +469,15 @@ int Solver<T>::m2l_post(int l) {
       if (lead > 0) {
         TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
-                          tc_products));
+                          tc_products, rk()));
         mark(ST_M2L, 2);
       } else {
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
-                          tc_products));
+                          tc_products, rk()));
         mark(ST_M2L, 1);
       }
     } else {
-      TRY(m2l_fp(Ml, l, 0, r, r));
+      TRY(m2l_fp(Ml, l, 0, rk(), rk()));
       int g = tune.m2l_groups[l] > 0 ? tune.m2l_groups[l] : dmma_default_groups(l, nsets);
       if ((int64_t)g * cells(l) * r > Lpart_elems) g = 1;
       mark(ST_M2L, g > 1 ? 2 : 1);  // groups add the partial sum
@@ -531,10 +534,10 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   for (int part = 0; part < (split ? 2 : 1) && rc == BBFMM_OK; ++part) {
     cudaEventRecord(a, stream);
     for (int i = 0; i < reps && rc == BBFMM_OK; ++i) {
-      if (!split) rc = m2l_fp(Ml, level, 0, r, r);
+      if (!split) rc = m2l_fp(Ml, level, 0, rk(), rk());
       else if (part == 0) rc = split ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf,
-                                                     level, offs, stream, nsets, tc_products)
-                                     : m2l_fp(Ml, level, 0, r, r);
+                                                     level, offs, stream, nsets, tc_products, rk())
+                                     : m2l_fp(Ml, level, 0, rk(), rk());
       else rc = split && lead > 0 ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
     }
     cudaEventRecord(b, stream);
@@ -706,7 +709,7 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 template <typename T>
 void Solver<T>::release() {
   void *ptrs[] = {offs, perm, leaf_start, leafm, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
-                  phis, flds, Ssplit, Lsplit};
+                  phis, flds, Ssplit, Lsplit, io_q, io_phi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (own_ops) {
@@ -818,9 +821,16 @@ int bbfmm_b200_solve_host(bbfmm_b200_solver *h, const void *q_host, void *phi_ho
   const size_t es = h->f ? sizeof(float) : sizeof(double);
   cudaStream_t st = h->f ? h->f->stream : h->d->stream;
   if (N == 0) return BBFMM_OK;
-  void *qd = nullptr, *pd = nullptr;
-  if (cudaMalloc(&qd, es * N) != cudaSuccess || cudaMalloc(&pd, es * N) != cudaSuccess) {
-    if (qd) cudaFree(qd);
+  // device staging kept by the solver (freed when the particles change), so repeated calls do
+  // not pay cudaMalloc / cudaFree and the device-wide synchronisation of the latter
+  void *&qd = h->f ? h->f->io_q : h->d->io_q;
+  void *&pd = h->f ? h->f->io_phi : h->d->io_phi;
+  if (!qd && cudaMalloc(&qd, es * N) != cudaSuccess) {
+    qd = nullptr;
+    return bbfmm_set_error(BBFMM_ERR_NOMEM, "device allocation for host solve failed");
+  }
+  if (!pd && cudaMalloc(&pd, es * N) != cudaSuccess) {
+    pd = nullptr;
     return bbfmm_set_error(BBFMM_ERR_NOMEM, "device allocation for host solve failed");
   }
   int rc = bbfmm_set_cuda_error(cudaMemcpyAsync(qd, q_host, es * N, cudaMemcpyHostToDevice, st), "h2d q", __FILE__,
@@ -830,8 +840,6 @@ int bbfmm_b200_solve_host(bbfmm_b200_solver *h, const void *q_host, void *phi_ho
     rc = bbfmm_set_cuda_error(cudaMemcpyAsync(phi_host, pd, es * N, cudaMemcpyDeviceToHost, st), "d2h phi",
                               __FILE__, __LINE__);
   if (rc == BBFMM_OK) rc = bbfmm_set_cuda_error(cudaStreamSynchronize(st), "sync", __FILE__, __LINE__);
-  cudaFree(qd);
-  cudaFree(pd);
   return rc;
 }
 
@@ -891,6 +899,16 @@ int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *h, long long cells) {
   }
   h->d->slab_request = cells;
   return h->d->pos4 ? h->d->alloc_work() : BBFMM_OK;
+}
+
+int bbfmm_b200_set_rank(bbfmm_b200_solver *h, int rank) {
+  if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
+  const int r = h->f ? h->f->r : h->d->r;
+  if (rank != 0 && (rank < 32 || rank > r || rank % 32))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "rank must be 0 or a multiple of 32 in [32, r]");
+  if (h->f) h->f->rank_eff = rank;
+  else h->d->rank_eff = rank;
+  return BBFMM_OK;
 }
 
 int bbfmm_b200_set_tc_products(bbfmm_b200_solver *h, int nprod) {

@@ -30,7 +30,7 @@ template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const
 template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 // rows are a slab of the level starting at cell row0 (the cpg side is indexed by level cell)
-template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int ldc = 0);
+template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int ldc = 0, int lda = 0);
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
@@ -73,8 +73,9 @@ size_t tc_split_bytes(int r, int64_t ncell);
 // other terms are small enough that one BF16 product adds below 1e-8 of |L| (estimated
 // per 32 x 32 block from the operators and typical multipoles).
 constexpr int TC_SPLIT_CHUNKS = 3, TC_SPLIT_ROWS = 96;
+// rank: the effective rank (outputs i and components j below it; 0 = r).
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
-                  int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3);
+                  int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0);
 int tc_status(int clear);
 int tc_wait_probe(unsigned limit, int code);
 // Tensor-core projections (m2l_tc.cu): the components j >= lead of the up projection and the
@@ -82,7 +83,7 @@ int tc_wait_probe(unsigned limit, int code);
 int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out, cudaStream_t s);
 void tc_free_projections(void *p);
 int launch_proj_tc(const void *p, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
-                   const double *cs, double scale, cudaStream_t s);
+                   const double *cs, double scale, cudaStream_t s, int rank = 0);
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
                   cudaStream_t s);
 constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
@@ -98,6 +99,11 @@ template <typename T>
 struct Solver {
   int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, lead_rows = 32, device = 0;
   int nsets = 1;  // particle sets of this depth stacked in every launch (set k = cells [k 8^l, (k+1) 8^l))
+  // Effective rank (0 = r): the operators hold a rank-rank_eff truncation zero-padded to r,
+  // and the M2L and the down projection skip the zero components j >= rank_eff and outputs
+  // i >= rank_eff (a tolerance-rank SVD cut, bbfmm_b200_set_rank).
+  int rank_eff = 0;
+  int rk() const { return rank_eff > 0 ? rank_eff : r; }
   // Leaf cells per slab of the leaf level (multiple of 64): P2M -> up projection -> M2M and
   // down projection -> L2L -> L2P run slab by slab through one slab-sized S / F buffer, so
   // the leaf level's n^3 arrays never exist in full. 0: automatic (slabs only when a full
@@ -141,6 +147,7 @@ struct Solver {
   void *Msplit = nullptr;
   T *phis = nullptr;
   T *flds = nullptr;  // 3 N, sorted field of the last solve_fields
+  void *io_q = nullptr, *io_phi = nullptr;  // device staging of the host-buffer solve (N each)
   // timing
   bool timing = false;
   cudaEvent_t ev[ST_COUNT + 1] = {};
@@ -184,7 +191,7 @@ struct Solver {
   int time_m2l(int level, int reps, float *ms);
   int m2l_fp(const T *Ml, int level, int j0, int j1, int ni);  // FP64 (DMMA) / FP32 (SIMT) M2L part
   int proj(int64_t M, int K, int N, const T *A, const T *B, const T *cs, T scale, T *C, int level, int mapmode,
-           int64_t row0 = 0);
+           int64_t row0 = 0, int lda = 0);
   void release();
 };
 

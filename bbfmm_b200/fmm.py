@@ -41,7 +41,8 @@ class Solver:
     components j < ``lead`` -- runs in FP64, FP32 compensated P2P)."""
 
     def __init__(self, n: int, maxlev: int, L: float = 1.0, mode: str = "d", lead: int = 16,
-                 lead_rows: int = 32, device: int = 0, operators=None, stream=None):
+                 lead_rows: int = 32, device: int = 0, operators=None, stream=None, rank: int | None = None,
+                 tol: float | None = None):
         import torch
         self.torch = torch
         self.n, self.maxlev, self.L, self.mode = n, maxlev, float(L), mode
@@ -55,6 +56,13 @@ class Solver:
             _, U, E = ops.load_operators(n, single=(mode == "s"))
         else:
             U, E = operators
+        # tolerance-rank mode: an SVD cut at relative singular value `tol` (or an explicit rank),
+        # the truncated operators zero-padded to r and the zero blocks skipped by the kernels
+        if tol is not None and rank is None:
+            rank = ops.tolerance_rank(n, tol)
+        self.rank = self.r if rank is None else int(rank)
+        if self.rank != self.r:
+            U, E = ops.truncate_operators(n, U, E, self.rank)
         U = np.ascontiguousarray(U)
         E = np.ascontiguousarray(E)
         fp32 = int(U.dtype == np.float32)
@@ -65,6 +73,8 @@ class Solver:
         _lib.check(_lib.lib().bbfmm_b200_create(C.byref(cfg), _ptr(U), _ptr(E), fp32, C.byref(h)))
         self.h = h
         self.N = 0
+        if self.rank != self.r:
+            _lib.check(_lib.lib().bbfmm_b200_set_rank(h, self.rank))
 
     def __del__(self):
         h = getattr(self, "h", None)

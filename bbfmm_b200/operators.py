@@ -191,6 +191,46 @@ def default_cache_dir() -> str:
         os.path.join(os.path.expanduser("~"), ".cache", "bbfmm_b200", "operators"))
 
 
+def singular_values(n: int, cache_dir: str | None = None) -> np.ndarray:
+    """Singular values of the FP64 kernel matrix K0 of order n, relative to the largest
+    (cached as sigma{n}.npy beside the operator files)."""
+    cache_dir = cache_dir or default_cache_dir()
+    path = os.path.join(cache_dir, f"sigma{n}.npy")
+    if os.path.exists(path):
+        return np.load(path)
+    K0 = kernel_matrix(n)
+    R = np.linalg.qr(K0.T, mode="r")
+    sv = np.linalg.svd(R.T, compute_uv=False)
+    sv = sv / sv[0]
+    os.makedirs(cache_dir, exist_ok=True)
+    np.save(path, sv)
+    return sv
+
+
+def tolerance_rank(n: int, tol: float, multiple: int = 32, cache_dir: str | None = None) -> int:
+    """Rank of an SVD cut at relative singular value `tol` (the number of sigma_j / sigma_0 >= tol),
+    rounded up to `multiple` (the kernels' component granularity) and capped at n^3 / 2."""
+    sv = singular_values(n, cache_dir)
+    r = int((sv >= tol).sum())
+    r = -(-r // multiple) * multiple
+    return max(multiple, min(r, n ** 3 // 2))
+
+
+def truncate_operators(n: int, Ucol: np.ndarray, Ecol: np.ndarray, rank: int):
+    """The rank-`rank` bbFMM operators inside the rank-r arrays: U keeps its leading `rank`
+    singular vectors (the rest zero) and E_k = U^T K_k U keeps its leading rank x rank block,
+    which is exactly U'^T K_k U' for the truncated basis U'. Zero padding keeps every array
+    layout (and kernel) of rank r = n^3 / 2."""
+    n3 = n ** 3
+    r = n3 // 2
+    U = np.array(Ucol, copy=True).reshape(r, n3)        # row j = column j of U
+    U[rank:] = 0
+    E = np.array(Ecol, copy=True).reshape(NUM_OFFSETS, r, r)  # [k][j][i]
+    E[:, rank:, :] = 0
+    E[:, :, rank:] = 0
+    return U.reshape(-1), E.reshape(-1)
+
+
 def load_operators(n: int, single: bool = False, cache_dir: str | None = None):
     """Cached operators for order n: returns (r, Ucol, Ecol) in the requested precision.
 

@@ -582,6 +582,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mixed", choices=["mixed", "d", "s"])
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--tol-rank", type=float, default=1e-8,
+                    help="also time mixed and plain FP64 with the SVD cut at this relative singular value (0: off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--N", type=int, default=N_FULL)
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
@@ -745,6 +747,28 @@ def main():
                  "err_ratio": err_mode / err_plain}
         pd.close()
 
+    # tolerance-rank mode: the SVD cut at relative singular value 1e-8 that the configuration
+    # names, mixed and plain FP64 at the same truncated rank (the reference fixes r = n^3/2)
+    tolr = None
+    if args.mode != "d" and args.tol_rank > 0 and args.plain_steps > 0:
+        res_t = {}
+        for m in ("mixed", "d"):
+            torch.cuda.empty_cache()
+            st = Solver(n, lev, 1.0, mode=m, device=local, tol=args.tol_rank)
+            st.set_particles(x)
+            qt = torch.as_tensor(q, device="cuda")
+            ot = torch.empty_like(qt)
+            st.solve(qt, out=ot)
+            reps = args.plain_steps if m == "d" else args.steps
+            tt = max_over_ranks(_device_time(lambda: st.solve(qt, out=ot), reps,
+                                             torch.cuda.ExternalStream(st.stream)))
+            res_t[m] = {"s_per_solve": tt, "err_vs_direct": rel(ot.double().cpu().numpy()), "rank": st.rank}
+            st.close()
+            del qt, ot
+        tolr = {"tol": args.tol_rank, "rank": res_t["d"]["rank"], "mixed": res_t["mixed"], "plain_fp64": res_t["d"],
+                "speedup": res_t["d"]["s_per_solve"] / res_t["mixed"]["s_per_solve"],
+                "err_ratio": res_t["mixed"]["err_vs_direct"] / res_t["d"]["err_vs_direct"]}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -770,6 +794,7 @@ def main():
                        "l2": "inputs and working set larger than L2 (operators 166 MB, expansions > 20 GB)"},
             "err_vs_fp64_direct": err_mode, "n_targets": N_TARGETS,
             "plain_fp64": plain,
+            "tolerance_rank": tolr,
             "stages_ms": stages,
             "e2e": {"value": world / t_e2e, "unit": "solve/s", "h2d_bytes_per_step": N * esz,
                     "d2h_bytes_per_step": N * esz},

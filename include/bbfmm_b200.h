@@ -122,7 +122,9 @@ BBFMM_B200_API int bbfmm_b200_solve(bbfmm_b200_solver *s, const void *q_dev, voi
  * new. Runs on the solver's stream without synchronising. */
 BBFMM_B200_API int bbfmm_b200_solve_fields(bbfmm_b200_solver *s, const void *q_dev, void *pot_dev, void *field_dev);
 
-/* The same with host buffers: copies q in, solves, copies phi out and synchronises. */
+/* The same with host buffers: copies q in, solves, copies phi out and synchronises. The
+ * device staging (2 N values) is allocated on the first call and kept until the particles
+ * change or the solver is destroyed; pinned host buffers make the copies direct. */
 BBFMM_B200_API int bbfmm_b200_solve_host(bbfmm_b200_solver *s, const void *q_host, void *phi_host);
 
 /* Per-stage device times (ms) of the last solve run with timing on; returns the number of
@@ -207,6 +209,14 @@ BBFMM_B200_API void bbfmm_b200_destroy(bbfmm_b200_solver *s);
  * Automatic: slabs of 16 GiB when a whole-level array would be larger (n = 8, FP64: depth 8
  * and deeper). Reallocates the work buffers when particles are already set. */
 BBFMM_B200_API int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *s, long long cells);
+
+/* Effective rank (0 = r, else a multiple of 32 in [32, r]): for operators that hold a rank-k
+ * truncation of the SVD basis zero-padded to r (the leading k singular vectors in U, the
+ * leading k x k block of every E_k; an SVD cut at a relative singular value), the M2L and the
+ * down projection skip the zero components j >= k and outputs i >= k. Results equal the
+ * rank-k bbFMM; the reference fixes r = n^3 / 2 (bbfmm.c:1340-1343), this tolerance-rank mode
+ * is new. */
+BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
 
 /* MIXED mode: products per term of the tensor-core M2L. 0 (default, adaptive): the three
  * split-BF16 products hi*hi + hi*lo + lo*hi for the contraction components j < 96 and the

@@ -157,3 +157,47 @@ def test_leaf_slabs_are_bitwise_identical(mode, n):
         p, f = s.solve_fields(qd)
         assert torch.equal(p, p0) and torch.equal(f, f0), cells
     s.close()
+
+
+def _compact(U, E, n, rank):
+    """Rank-`rank` operators in the compact reference layout (U: n^3 x rank, E: rank x rank blocks)."""
+    n3, r = n ** 3, n ** 3 // 2
+    Uc = np.ascontiguousarray(np.asarray(U).reshape(r, n3)[:rank]).reshape(-1)
+    Ec = np.ascontiguousarray(np.asarray(E).reshape(316, r, r)[:, :rank, :rank]).reshape(-1)
+    return Uc, Ec
+
+
+def test_tolerance_rank_matches_truncated_oracle(oracle_d):
+    """An SVD cut at relative singular value 1e-8 (rank 147 -> 160): the solver's zero-padded
+    rank-160 operators with the zero blocks skipped equal the oracle FMM run with the compact
+    rank-160 operators (FP64, 1e-12)."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200 import operators as ops
+    rank = ops.tolerance_rank(8, 1e-8)
+    assert rank == 160
+    x, q = uniform_inputs(20000, seed=14)
+    _, U, E = ops.load_operators(8, single=False)
+    want = oracle_d.fmm(x, q, 8, 3, *_compact(U, E, 8, rank))
+    s = Solver(8, 3, 1.0, mode="d", tol=1e-8)
+    assert s.rank == rank
+    s.set_particles(x)
+    got = s.solve(torch.as_tensor(q, device="cuda")).cpu().numpy()
+    assert rel_l2(got, want) < 1e-12
+    s.close()
+
+
+def test_tolerance_rank_mixed_matches_fp64_rank():
+    """Mixed precision at rank 160 (tensor-core M2L with N = 160, K-chunks up to 160; down
+    projection K = 160) against the FP64 solve at the same rank: 3e-7."""
+    import torch
+    from bbfmm_b200 import Solver
+    x, q = uniform_inputs(40000, seed=15)
+    qd = torch.as_tensor(q, device="cuda")
+    out = {}
+    for mode in ("mixed", "d"):
+        s = Solver(8, 4, 1.0, mode=mode, rank=160)
+        s.set_particles(x)
+        out[mode] = s.solve(qd).cpu().numpy()
+        s.close()
+    assert rel_l2(out["mixed"], out["d"]) < 3e-7
