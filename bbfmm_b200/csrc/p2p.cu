@@ -55,12 +55,7 @@ __device__ __forceinline__ float rsqrt_nr(float rr) {
   return y * fmaf(-0.5f * rr * y, y, 1.5f);
 }
 
-// QF: the FP32 charges come from qf (written once per solve) instead of converting the FP64
-// charge of every source pair by pair (a double -> float conversion per pair is the scarcest
-// instruction of the loop).
-template <bool QF>
 __global__ void __launch_bounds__(256) p2p_mixed_kernel(int N, const double4 *__restrict__ pos4,
-                                                        const float *__restrict__ qf,
                                                         const int *__restrict__ leaf_start,
                                                         const int *__restrict__ leafm, int maxlev,
                                                         double *__restrict__ phi) {
@@ -87,7 +82,7 @@ __global__ void __launch_bounds__(256) p2p_mixed_kernel(int N, const double4 *__
             const double ex = g.x - f.x, ey = g.y - f.y, ez = g.z - f.z;
             const double rr = fma(ex, ex, fma(ey, ey, ez * ez));
             if (rr != 0.0) {
-              const float t = (QF ? qf[s] : (float)g.w) * rsqrt_nr((float)rr);
+              const float t = (float)g.w * rsqrt_nr((float)rr);
               const float y = sum + t;
               comp += (fabsf(sum) >= fabsf(t)) ? ((sum - y) + t) : ((t - y) + sum);
               sum = y;
@@ -98,11 +93,6 @@ __global__ void __launch_bounds__(256) p2p_mixed_kernel(int N, const double4 *__
     }
     phi[i] += f.w * ((double)sum + (double)comp);
   }
-}
-
-// FP32 copy of the charges (the w of the sorted FP64 positions).
-__global__ void charges_f32_kernel(int N, const double4 *__restrict__ pos4, float *__restrict__ qf) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) qf[i] = (float)pos4[i].w;
 }
 
 // Per-particle leaf (Morton) index from the leaf ranges.
@@ -130,19 +120,12 @@ template int launch_p2p<double>(int, const double *, const int *, const int *, i
 template int launch_p2p<float>(int, const float *, const int *, const int *, int, float *, cudaStream_t, int);
 
 int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi,
-                     cudaStream_t s, int threads, const float *qf) {
+                     cudaStream_t s, int threads) {
   if (N <= 0) return BBFMM_OK;
   if (threads < 32 || threads > 256 || threads % 32) return bbfmm_set_error(BBFMM_ERR_ARG, "p2p threads per block");
-  const double4 *p4 = reinterpret_cast<const double4 *>(pos4);
-  if (qf) p2p_mixed_kernel<true><<<p2p_grid(N, threads), threads, 0, s>>>(N, p4, qf, leaf_start, leafm, maxlev, phi);
-  else p2p_mixed_kernel<false><<<p2p_grid(N, threads), threads, 0, s>>>(N, p4, qf, leaf_start, leafm, maxlev, phi);
+  p2p_mixed_kernel<<<p2p_grid(N, threads), threads, 0, s>>>(N, reinterpret_cast<const double4 *>(pos4), leaf_start,
+                                                            leafm, maxlev, phi);
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2p_mixed", __FILE__, __LINE__);
-}
-
-int launch_charges_f32(int N, const double *pos4, float *qf, cudaStream_t s) {
-  if (N <= 0) return BBFMM_OK;
-  charges_f32_kernel<<<p2p_grid(N), 256, 0, s>>>(N, reinterpret_cast<const double4 *>(pos4), qf);
-  return bbfmm_set_cuda_error(cudaGetLastError(), "charges_f32", __FILE__, __LINE__);
 }
 
 int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s, int nsets) {
@@ -203,9 +186,7 @@ __global__ void __launch_bounds__(256) p2p_field_kernel(int N, const T *__restri
 }
 
 // The same with the arithmetic of p2p_mixed_kernel; FP64 outputs.
-template <bool QF>
 __global__ void __launch_bounds__(256) p2p_mixed_field_kernel(int N, const double4 *__restrict__ pos4,
-                                                              const float *__restrict__ qf,
                                                               const int *__restrict__ leaf_start,
                                                               const int *__restrict__ leafm, int maxlev,
                                                               double *__restrict__ pot, double *__restrict__ fld) {
@@ -231,7 +212,7 @@ __global__ void __launch_bounds__(256) p2p_mixed_field_kernel(int N, const doubl
             const double ex = g.x - f.x, ey = g.y - f.y, ez = g.z - f.z;
             const double rr = fma(ex, ex, fma(ey, ey, ez * ez));
             if (rr != 0.0) {
-              const float rinv = rsqrt_nr((float)rr), t = (QF ? qf[s] : (float)g.w) * rinv, t3 = t * rinv * rinv;
+              const float rinv = rsqrt_nr((float)rr), t = (float)g.w * rinv, t3 = t * rinv * rinv;
               const float y = sum + t;
               comp += (fabsf(sum) >= fabsf(t)) ? ((sum - y) + t) : ((t - y) + sum);
               sum = y;
@@ -264,16 +245,11 @@ template int launch_p2p_field<float>(int, const float *, const int *, const int 
                                      cudaStream_t, int);
 
 int launch_p2p_mixed_field(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev,
-                           double *pot, double *fld, cudaStream_t s, int threads, const float *qf) {
+                           double *pot, double *fld, cudaStream_t s, int threads) {
   if (N <= 0) return BBFMM_OK;
   if (threads < 32 || threads > 256 || threads % 32) return bbfmm_set_error(BBFMM_ERR_ARG, "p2p threads per block");
-  const double4 *p4 = reinterpret_cast<const double4 *>(pos4);
-  if (qf)
-    p2p_mixed_field_kernel<true><<<p2p_grid(N, threads), threads, 0, s>>>(N, p4, qf, leaf_start, leafm, maxlev, pot,
-                                                                         fld);
-  else
-    p2p_mixed_field_kernel<false><<<p2p_grid(N, threads), threads, 0, s>>>(N, p4, qf, leaf_start, leafm, maxlev, pot,
-                                                                          fld);
+  p2p_mixed_field_kernel<<<p2p_grid(N, threads), threads, 0, s>>>(N, reinterpret_cast<const double4 *>(pos4),
+                                                                  leaf_start, leafm, maxlev, pot, fld);
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2p_mixed_field", __FILE__, __LINE__);
 }
 
@@ -292,8 +268,7 @@ int near_field_run(int N, int maxlev, const double *xyzq, const int *leaf_start,
                    cudaStream_t st, int *leafm) {
   int rc = bbfmm::launch_leaf_of(maxlev, leaf_start, leafm, st, 1);
   if (rc != BBFMM_OK) return rc;
-  if (mode == BBFMM_B200_MODE_MIXED)
-    return bbfmm::launch_p2p_mixed(N, xyzq, leaf_start, leafm, maxlev, phi, st, 256, nullptr);
+  if (mode == BBFMM_B200_MODE_MIXED) return bbfmm::launch_p2p_mixed(N, xyzq, leaf_start, leafm, maxlev, phi, st, 256);
   return bbfmm::launch_p2p<double>(N, xyzq, leaf_start, leafm, maxlev, phi, st, 256);
 }
 

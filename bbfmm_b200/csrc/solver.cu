@@ -286,9 +286,7 @@ int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const
   if (flds) cudaFree(flds);  // sized 3 N: reallocated by the next solve_fields
   if (io_q) cudaFree(io_q);  // sized N: reallocated by the next host-buffer solve
   if (io_phi) cudaFree(io_phi);
-  if (qf) cudaFree(qf);      // sized N: reallocated by the next near field
   io_q = io_phi = nullptr;
-  qf = nullptr;
   perm = leaf_start = leafm = nullptr; pos4 = phis = flds = nullptr;
   N = N_;
   TRY(dalloc(&perm, N > 0 ? N : 1));
@@ -558,12 +556,10 @@ template <typename T>
 int Solver<T>::near(T *pot, T *fld) {
   const int th = tune.p2p_threads;
   if (mode == MODE_MIXED) {
-    if (!qf) TRY(dalloc(&qf, N > 0 ? N : 1));
-    TRY(launch_charges_f32(N, (const double *)pos4, qf, stream));
     if (fld) TRY(launch_p2p_mixed_field(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot,
-                                        (double *)fld, stream, th, qf));
-    else TRY(launch_p2p_mixed(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot, stream, th, qf));
-    mark(ST_P2P, 2);
+                                        (double *)fld, stream, th));
+    else TRY(launch_p2p_mixed(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot, stream, th));
+    mark(ST_P2P);
   } else {
     if (fld) TRY(launch_p2p_field<T>(N, pos4, leaf_start, leafm, maxlev, pot, fld, stream, th));
     else TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, pot, stream, th));
@@ -713,7 +709,7 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
 template <typename T>
 void Solver<T>::release() {
   void *ptrs[] = {offs, perm, leaf_start, leafm, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
-                  phis, flds, Ssplit, Lsplit, io_q, io_phi, qf};
+                  phis, flds, Ssplit, Lsplit, io_q, io_phi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (own_ops) {

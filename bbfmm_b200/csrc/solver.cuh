@@ -35,13 +35,12 @@ template <typename T, typename TI> int launch_gather(int N, const int *perm, con
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
 template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s, int threads = 256);
-int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi, cudaStream_t s, int threads = 256, const float *qf = nullptr);
-int launch_charges_f32(int N, const double *pos4, float *qf, cudaStream_t s);
+int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi, cudaStream_t s, int threads = 256);
 int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s, int nsets = 1);
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
 template <typename T> int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld, cudaStream_t s, int threads = 256);
-int launch_p2p_mixed_field(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *pot, double *fld, cudaStream_t s, int threads = 256, const float *qf = nullptr);
+int launch_p2p_mixed_field(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *pot, double *fld, cudaStream_t s, int threads = 256);
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0);
 void build_offset_table(int *out);
 constexpr int DMMA_PARTS = 21;  // most offset groups of the FP64 M2L (189 = 9 x 21)
@@ -149,7 +148,6 @@ struct Solver {
   T *phis = nullptr;
   T *flds = nullptr;  // 3 N, sorted field of the last solve_fields
   void *io_q = nullptr, *io_phi = nullptr;  // device staging of the host-buffer solve (N each)
-  float *qf = nullptr;  // mixed mode: FP32 charges of the sorted particles (near field)
   // timing
   bool timing = false;
   cudaEvent_t ev[ST_COUNT + 1] = {};
