@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_set_rank.argtypes = [vp, i]
         L.bbfmm_b200_set_leaf_slab.argtypes = [vp, C.c_longlong]
         L.bbfmm_b200_tuning.argtypes = [vp, ip]
+        L.bbfmm_b200_set_tuning.argtypes = [vp, ip]
         L.bbfmm_b200_batch_create.argtypes = [C.POINTER(Config), i, ip, ip, ip, vp, vp, vp, vp, vp, i, C.POINTER(vp)]
         L.bbfmm_b200_batch_solve.argtypes = [vp, vp, vp, i]
         L.bbfmm_b200_batch_autotune.argtypes = [vp, vp]

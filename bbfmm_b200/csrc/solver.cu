@@ -924,6 +924,24 @@ int bbfmm_b200_autotune(bbfmm_b200_solver *h, const void *q_dev) {
   return h->f ? h->f->autotune(q_dev, 0) : h->d->autotune(q_dev, 1);
 }
 
+int bbfmm_b200_set_tuning(bbfmm_b200_solver *h, const int *info) {
+  if (!h || !info) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  const int th = info[0];
+  if (th != 64 && th != 128 && th != 256) return bbfmm_set_error(BBFMM_ERR_ARG, "P2P threads: 64, 128 or 256");
+  for (int l = 0; l <= 10; ++l)
+    if ((info[1 + l] != 0 && info[1 + l] != 1) || info[12 + l] < 0 || info[12 + l] > bbfmm::DMMA_PARTS)
+      return bbfmm_set_error(BBFMM_ERR_ARG, "M2L kind must be 0 or 1 and groups in [0, 21]");
+  auto apply = [&](auto &sv) -> int {
+    sv.tune.p2p_threads = th;
+    for (int l = 0; l <= 10; ++l) {
+      sv.tune.m2l_kind[l] = info[1 + l];
+      sv.tune.m2l_groups[l] = info[12 + l];
+    }
+    return sv.pos4 ? sv.alloc_partials() : BBFMM_OK;
+  };
+  return h->f ? apply(*h->f) : apply(*h->d);
+}
+
 int bbfmm_b200_tuning(const bbfmm_b200_solver *h, int *info) {
   if (!h || !info) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   const bbfmm::Tuning &t = h->f ? h->f->tune : h->d->tune;

@@ -79,8 +79,11 @@ class Solver:
     def __del__(self):
         h = getattr(self, "h", None)
         if h:
-            _lib.lib().bbfmm_b200_destroy(h)
             self.h = None
+            try:
+                _lib.lib().bbfmm_b200_destroy(h)
+            except (TypeError, AttributeError):  # interpreter shutdown: the module is gone
+                pass
 
     def close(self):
         self.__del__()
@@ -160,6 +163,12 @@ class Solver:
         self.torch.cuda.synchronize(q.device)
         _lib.check(_lib.lib().bbfmm_b200_autotune(self.h, C.c_void_p(q.data_ptr())))
         return self.tuning()
+
+    def set_tuning(self, choices):
+        """Set launch choices (the dict of tuning(): P2P threads, per-level M2L kind and groups)."""
+        v = [int(choices["p2p_threads"])] + [int(k) for k in choices["m2l_kind"]] + [int(g) for g in choices["m2l_groups"]]
+        info = (C.c_int * 23)(*v)
+        _lib.check(_lib.lib().bbfmm_b200_set_tuning(self.h, info))
 
     def tuning(self):
         info = (C.c_int * 23)()
@@ -252,8 +261,11 @@ class Batch:
     def __del__(self):
         h = getattr(self, "h", None)
         if h:
-            _lib.lib().bbfmm_b200_batch_destroy(h)
             self.h = None
+            try:
+                _lib.lib().bbfmm_b200_batch_destroy(h)
+            except (TypeError, AttributeError):  # interpreter shutdown: the module is gone
+                pass
 
     def close(self):
         self.__del__()

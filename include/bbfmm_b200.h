@@ -235,6 +235,8 @@ BBFMM_B200_API int bbfmm_b200_autotune(bbfmm_b200_solver *s, const void *q_dev);
 /* Current choices: info[0] = P2P threads per block, info[1 + l] = M2L kind of level l
  * (0 default, 1 FP64/SIMT), info[12 + l] = offset groups of level l (0 = default); 23 ints. */
 BBFMM_B200_API int bbfmm_b200_tuning(const bbfmm_b200_solver *s, int *info);
+/* Sets the choices (same 23 ints; for replaying a tuning or for tests). */
+BBFMM_B200_API int bbfmm_b200_set_tuning(bbfmm_b200_solver *s, const int *info);
 
 /* ---------------------------------------------------------------- batches
  * Many independent particle sets of uneven size, each with its own order n (4 or 8) and leaf

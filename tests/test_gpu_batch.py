@@ -133,3 +133,23 @@ def test_mixed_mode_order4_single_solver(oracle_d):
     got = s.solve(torch.as_tensor(q, device="cuda")).cpu().numpy()
     assert rel_l2(got, want) < 1e-6  # FP32 reciprocal distances in the near field
     s.close()
+
+
+
+def test_set_tuning_round_trip_and_groups_keep_results():
+    """Launch choices set by hand (offset groups of the FP64 M2L, near-field block size) are
+    reported back and keep the FP64 result to summation order (1e-13)."""
+    import torch
+    from bbfmm_b200 import Solver
+    sets, q = _sets(9, [(60000, 8, 3, "c")])
+    s = Solver(8, 3, 1.0, mode="d")
+    s.set_particles(sets[0][0])
+    qd = torch.as_tensor(q, device="cuda")
+    a = s.solve(qd).cpu().numpy()
+    t = s.tuning()
+    t2 = dict(t, p2p_threads=64, m2l_groups=[0, 0, 3, 7] + [0] * 7)
+    s.set_tuning(t2)
+    assert s.tuning() == t2
+    b = s.solve(qd).cpu().numpy()
+    assert rel_l2(b, a) < 1e-13
+    s.close()
