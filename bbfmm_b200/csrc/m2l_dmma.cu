@@ -183,6 +183,22 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
   const int niter = 189 * nchunk;
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
 
+  // the targets and component pairs this thread copies are the same for every (offset,
+  // chunk): their box coordinates and shared-memory slots are computed once
+  constexpr int PER = (NT * (lead::BK / 2) + 255) / 256;
+  int cx[PER], cy[PER], cz[PER], j2s[PER];
+  uint32_t soff[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = tid + 256 * k;
+    const int t = e / (lead::BK / 2);
+    j2s[k] = (e % (lead::BK / 2)) * 2;
+    const bool valid = e < NT * (lead::BK / 2) && t < nt;
+    cx[k] = valid ? bxo + (t % bwx) : -(1 << 20);  // invalid slots fall outside every grid
+    cy[k] = byo + ((t / bwx) % bw);
+    cz[k] = bzo + (t / (bwx * bw));
+    soff[k] = (uint32_t)(t * lead::AST + j2s[k]) * 8u;
+  }
   auto issue = [&](int it) {
     if (it < niter) {
       const int o = it / nchunk, jc = (it % nchunk) * lead::BK;
@@ -193,13 +209,16 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
       const int sc = (scx << 2) | (scy << 1) | scz;
       const uint32_t sa = sbase + (uint32_t)((it % lead::STAGES) * STAGE) * 8u;
       const uint32_t sb = sa + (uint32_t)(NT * lead::AST) * 8u;
-      for (int e = tid; e < NT * (lead::BK / 2); e += 256) {  // NT targets x 8 pairs of j
-        const int t = e / (lead::BK / 2), j2 = (e % (lead::BK / 2)) * 2;
-        const int px = bxo + (t % bwx) + shx, py = byo + ((t / bwx) % bw) + shy, pz = bzo + (t / (bwx * bw)) + shz;
-        const bool ok = t < nt && jc + j2 < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
-        const double *src = ok ? M + ((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + j2 : M;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa + (uint32_t)(t * lead::AST + j2) * 8u),
-                     "l"(src), "r"(ok ? 16 : 0)
+      const double *Mc = M + (int64_t)((c & ~7) + sc) * P3 * R + jc;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        if (tid + 256 * k >= NT * (lead::BK / 2)) break;
+        const int px = cx[k] + shx, py = cy[k] + shy, pz = cz[k] + shz;
+        const bool ok = jc + j2s[k] < j1 && (unsigned)px < (unsigned)P && (unsigned)py < (unsigned)P &&
+                        (unsigned)pz < (unsigned)P;
+        const double *src = ok ? Mc + (((int64_t)pz * P + py) * P + px) * R + j2s[k] : M;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa + soff[k]), "l"(src),
+                     "r"(ok ? 16 : 0)
                      : "memory");
       }
       const double *Ek = Ecol + (int64_t)ov.x * R * R;
