@@ -50,6 +50,9 @@ __global__ void __launch_bounds__(256) p2p_kernel(int N, const T *__restrict__ p
 }
 
 // 1/sqrt(rr) in FP32: the hardware estimate refined by one Newton step.
+// The compensated sums below form the term t = q * rsqrt_nr(rr) with __fmul_rn: were the
+// product contracted into the addition sum + t, the new sum would not be fl(sum + t) and the
+// compensation would no longer be the exact rounding error of that addition.
 __device__ __forceinline__ float rsqrt_nr(float rr) {
   const float y = rsqrtf(rr);
   return y * fmaf(-0.5f * rr * y, y, 1.5f);
@@ -82,7 +85,7 @@ __global__ void __launch_bounds__(256) p2p_mixed_kernel(int N, const double4 *__
             const double ex = g.x - f.x, ey = g.y - f.y, ez = g.z - f.z;
             const double rr = fma(ex, ex, fma(ey, ey, ez * ez));
             if (rr != 0.0) {
-              const float t = (float)g.w * rsqrt_nr((float)rr);
+              const float t = __fmul_rn((float)g.w, rsqrt_nr((float)rr));
               const float y = sum + t;
               comp += (fabsf(sum) >= fabsf(t)) ? ((sum - y) + t) : ((t - y) + sum);
               sum = y;
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(256) p2p_mixed_field_kernel(int N, const doubl
             const double ex = g.x - f.x, ey = g.y - f.y, ez = g.z - f.z;
             const double rr = fma(ex, ex, fma(ey, ey, ez * ez));
             if (rr != 0.0) {
-              const float rinv = rsqrt_nr((float)rr), t = (float)g.w * rinv, t3 = t * rinv * rinv;
+              const float rinv = rsqrt_nr((float)rr), t = __fmul_rn((float)g.w, rinv), t3 = t * rinv * rinv;
               const float y = sum + t;
               comp += (fabsf(sum) >= fabsf(t)) ? ((sum - y) + t) : ((t - y) + sum);
               sum = y;
