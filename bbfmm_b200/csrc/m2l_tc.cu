@@ -75,6 +75,14 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait: false (and the status word set) if the phase did not complete in time.
+// FP64 tensor-core step D += A B (m8n8k4): A row lane >> 2, column lane & 3; B row lane & 3,
+// column lane >> 2; D row lane >> 2, columns 2 (lane & 3) + {0, 1}.
+__device__ __forceinline__ void dmma_f64(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int code) {
   for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
     if (mbar_try(bar, parity)) return true;
@@ -302,6 +310,13 @@ __global__ void __launch_bounds__(192, 1)
 // 512 columns), so every operator chunk loaded into shared memory serves 256 targets and the
 // operator traffic from L2 is halved. The lo halves of B cover the first TC_SPLIT_ROWS rows.
 // Stage: A_hi 16 KB | A_lo 16 KB | B_hi 16 KB | B_lo 6 KB.
+// With Mlead and Erow given (leading block i < 32, j < 16), the four epilogue warps, idle
+// while the tensor cores run the ~1 ms mainloop of a CTA, compute that block in FP64 for the
+// rows they later read from tensor memory: DMMA m8n8k4 with fragments loaded straight from
+// global memory (shared memory is taken by the stages), k-slot u of step ks standing for
+// component 4u + ks so that each fragment load is one contiguous 32-byte run of M or of
+// Erow[k][i][j] = E_k(i, j). The block is written to Lacc (assign) before the accumulator
+// wait, and the tensor-memory epilogue adds to it as it adds to a separately computed block.
 constexpr int A2_BYTES = 2 * A_BYTES, BLO2_BYTES = TC_SPLIT_ROWS * BK * 2;
 constexpr int STAGE2_BYTES = 2 * A2_BYTES + B_BYTES + BLO2_BYTES;
 constexpr int SMEM2_BYTES = STAGES * STAGE2_BYTES + 1024 /*align*/ + 256 /*barriers*/;
@@ -312,7 +327,7 @@ __global__ void __launch_bounds__(192, 1)
     m2l_tc2_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                    const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                    double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
-                   int split_chunks, int ncols) {
+                   int split_chunks, int ncols, const double *__restrict__ Mlead, const double *__restrict__ Erow) {
   constexpr int STAGE_BYTES = STAGE2_BYTES;
   constexpr int split_rows = TC_SPLIT_ROWS;
   extern __shared__ uint8_t smem_raw[];
@@ -420,6 +435,69 @@ __global__ void __launch_bounds__(192, 1)
     // ---------------- epilogue: TMEM -> registers -> Lacc
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;
+    if (Mlead) {
+      // FP64 leading block of rows h * 128 + q * 32 + [0, 32): fragment m holds the 8 rows
+      // 8m .. 8m + 7 of that range (x = 0..7 at one y, z of the box)
+      const int64_t P3 = (int64_t)P * P * P;
+      const int u = lane & 3, tr = lane >> 2;
+      for (int h = 0; h < 2; ++h) {
+        double acc[4][4][2];
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
+        for (int o = 0; o < 189; ++o) {
+          const int4 ov = offs[(c & 7) * 189 + o];
+          const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
+          const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
+          const int sc = (scx << 2) | (scy << 1) | scz;
+          const int px = bx0 + tr + (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
+          const double *Mc = Mlead + (int64_t)((c & ~7) + sc) * P3 * BN + 4 * u;
+          double2 a[4][2], b[4][2];
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const int r0 = h * 128 + q * 32 + 8 * m;
+            const int py = by0 + ((r0 >> 3) & 7) + shy, pz = bz0 + (r0 >> 6) + shz;
+            if ((unsigned)px < (unsigned)P && (unsigned)py < (unsigned)P && (unsigned)pz < (unsigned)P) {
+              const double2 *src = reinterpret_cast<const double2 *>(Mc + (((int64_t)pz * P + py) * P + px) * BN);
+              a[m][0] = src[0];
+              a[m][1] = src[1];
+            } else {
+              a[m][0] = a[m][1] = make_double2(0.0, 0.0);
+            }
+          }
+          const double *Ek = Erow + (int64_t)ov.x * BN * BN + 4 * u;
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            const double2 *src = reinterpret_cast<const double2 *>(Ek + (int64_t)(8 * f + tr) * BN);
+            b[f][0] = src[0];
+            b[f][1] = src[1];
+          }
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+              const double av = (ks & 1) ? a[m][ks >> 1].y : a[m][ks >> 1].x;
+#pragma unroll
+              for (int f = 0; f < 4; ++f)
+                dmma_f64(acc[m][f][0], acc[m][f][1], av, (ks & 1) ? b[f][ks >> 1].y : b[f][ks >> 1].x);
+            }
+        }
+        // D fragment: row tr of fragment m, columns 8f + 2u + {0, 1}
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int rr = h * 128 + q * 32 + 8 * m + tr;
+          const int64_t cell =
+              (int64_t)c * P3 + ((int64_t)(bz0 + (rr >> 6)) * P + (by0 + ((rr >> 3) & 7))) * P + (bx0 + tr);
+          double *dst = Lacc + cell * BN;
+#pragma unroll
+          for (int f = 0; f < 4; ++f)
+            *reinterpret_cast<double2 *>(dst + 8 * f + 2 * u) = make_double2(acc[m][f][0], acc[m][f][1]);
+        }
+      }
+      __threadfence_block();
+      __syncwarp();  // the rows written here are read back below by other lanes of this warp
+    }
     const bool ok = mbar_wait(acc_bar, 0, 3);
     tc_fence_after();
     for (int h = 0; h < 2 && ok; ++h) {
@@ -853,8 +931,18 @@ int tc_split_multipoles(int r, int64_t ncell, const double *M, int lead, void *M
   return bbfmm_set_cuda_error(cudaGetLastError(), "split multipoles", __FILE__, __LINE__);
 }
 
+// Whether launch_m2l_tc runs the two-box kernel with the FP64 leading block inside it (given
+// the FP64 multipoles and operators): the adaptive product map at full split rows and a
+// leading block of i < 32, j < 16.
+bool tc_fuses_lead(const void *opsv, int nprod, int rank) {
+  const TcOps *ops = (const TcOps *)opsv;
+  if (rank <= 0) rank = tc::BN;
+  return ops && nprod == 0 && rank >= TC_SPLIT_ROWS && ops->lead == 16 && ops->lead_rows == 32;
+}
+
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
-                  int level, const int4 *offs, cudaStream_t s, int nsets, int nprod, int rank) {
+                  int level, const int4 *offs, cudaStream_t s, int nsets, int nprod, int rank, const double *Mlead,
+                  const double *Erow) {
   const TcOps *ops = (const TcOps *)opsv;
   if (nprod != 0 && nprod != 1 && nprod != 3)
     return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 0 (adaptive), 1 or 3");
@@ -910,8 +998,10 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
       attr2 = true;
     }
     const int tiles2 = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX2_Y) * (P / tc::BOX_Z);
+    const bool fuse = Mlead && Erow && tc_fuses_lead(ops, nprod, rank) && kfirst == 0 && ilead == 32;
     tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs,
-                                                            kfirst, ilead, split_chunks, rank);
+                                                            kfirst, ilead, split_chunks, rank,
+                                                            fuse ? Mlead : nullptr, fuse ? Erow : nullptr);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
   }
   static bool attr = false;

@@ -465,8 +465,13 @@ int Solver<T>::m2l_post(int l) {
     const bool split = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
     if (split) {
       // FP64 leading block (i < lead_rows, j < lead) on the FP64 tensor path, then the
-      // split-bf16 tensor-core kernel adds everything else into the same FP64 output
-      if (lead > 0) {
+      // split-bf16 tensor-core kernel adds everything else into the same FP64 output; the
+      // two-box kernel computes the block itself in its otherwise idle epilogue warps
+      if (lead > 0 && tc_fuses_lead(tcops, tc_products, rk())) {
+        TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
+                          tc_products, rk(), (const double *)Ml, (const double *)Ert));
+        mark(ST_M2L, 1);
+      } else if (lead > 0) {
         TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
                           tc_products, rk()));
@@ -529,16 +534,17 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   BBFMM_CUDA_OK(cudaEventCreate(&b));
   const T *Ml = Mall + Moff[level];
   const bool split = mode == MODE_MIXED && tcops && level >= TC_MIN_LEVEL && tune.m2l_kind[level] == 0;
+  const bool fused = split && lead > 0 && tc_fuses_lead(tcops, tc_products, rk());
   int rc = BBFMM_OK;
   float tot[2] = {0.f, 0.f};
   for (int part = 0; part < (split ? 2 : 1) && rc == BBFMM_OK; ++part) {
     cudaEventRecord(a, stream);
     for (int i = 0; i < reps && rc == BBFMM_OK; ++i) {
       if (!split) rc = m2l_fp(Ml, level, 0, rk(), rk());
-      else if (part == 0) rc = split ? launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf,
-                                                     level, offs, stream, nsets, tc_products, rk())
-                                     : m2l_fp(Ml, level, 0, rk(), rk());
-      else rc = split && lead > 0 ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
+      else if (part == 0) rc = launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf, level, offs,
+                                             stream, nsets, tc_products, rk(), fused ? (const double *)Ml : nullptr,
+                                             fused ? (const double *)Ert : nullptr);
+      else rc = lead > 0 && !fused ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
     }
     cudaEventRecord(b, stream);
     cudaEventSynchronize(b);

@@ -75,7 +75,9 @@ size_t tc_split_bytes(int r, int64_t ncell);
 constexpr int TC_SPLIT_CHUNKS = 3, TC_SPLIT_ROWS = 96;
 // rank: the effective rank (outputs i and components j below it; 0 = r).
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
-                  int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0);
+                  int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0,
+                  const double *Mlead = nullptr, const double *Erow = nullptr);
+bool tc_fuses_lead(const void *ops, int nprod, int rank);
 int tc_status(int clear);
 int tc_wait_probe(unsigned limit, int code);
 // Tensor-core projections (m2l_tc.cu): the components j >= lead of the up projection and the
