@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(192, 1)
 // targets) as two M = 128 halves, each with its own 128 x 256 FP32 accumulator in TMEM (all
 // 512 columns), so every operator chunk loaded into shared memory serves 256 targets and the
 // operator traffic from L2 is halved. The lo halves of B cover the first TC_SPLIT_ROWS rows.
-// Stage: A_hi 16 KB | A_lo 16 KB | B_hi 16 KB | B_lo 6 KB.
+// Stage: A_hi 16 KB | A_lo 16 KB | B_hi 16 KB | B_lo TC_SPLIT_ROWS x 32 BF16 (4 KB).
 // With Mlead and Erow given (leading block i < 32, j < 16), the four epilogue warps, idle
 // while the tensor cores run the ~1 ms mainloop of a CTA, compute that block in FP64 for the
 // rows they later read from tensor memory: DMMA m8n8k4 with fragments loaded straight from

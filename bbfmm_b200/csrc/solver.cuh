@@ -70,9 +70,11 @@ size_t tc_split_bytes(int r, int64_t ncell);
 // nprod: 3 = hi*hi + hi*lo + lo*hi (split BF16) for every term, 1 = hi*hi only (plain BF16
 // products), 0 = adaptive: the three products for components j < 32 TC_SPLIT_CHUNKS and
 // outputs i < TC_SPLIT_ROWS, hi*hi alone elsewhere. With the SVD-ordered operators those
-// other terms are small enough that one BF16 product adds below 1e-8 of |L| (estimated
-// per 32 x 32 block from the operators and typical multipoles).
-constexpr int TC_SPLIT_CHUNKS = 3, TC_SPLIT_ROWS = 96;
+// other terms are small enough for one BF16 product: on 4M uniform particles (n = 8, depth 7)
+// the error against the FP64 direct sum is 1.0453x that of the FP64 FMM with the 64 x 64
+// three-product block, 1.0450x with 96 x 96, 1.075x with 64 x 48 and 1.9x with 64 x 32 or
+// 32 x 64.
+constexpr int TC_SPLIT_CHUNKS = 2, TC_SPLIT_ROWS = 64;
 // rank: the effective rank (outputs i and components j below it; 0 = r).
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0,

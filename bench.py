@@ -714,15 +714,19 @@ def main():
         # (zero-filled out-of-grid sources included), per 32-component chunk hi*hi over the 256
         # outputs plus, for the first TC_SPLIT_CHUNKS chunks, the two corrections over the first
         # TC_SPLIT_ROWS outputs (the adaptive product map of the mixed mode)
-        split_chunks, split_rows, chunks = 3, 96, r // 32
+        split_chunks, split_rows, chunks = 2, 64, r // 32  # TC_SPLIT_CHUNKS, TC_SPLIT_ROWS
         macs_per_pair = 32 * (split_chunks * (256 + 2 * split_rows) + (chunks - split_chunks) * 256)
         exec_flop = 2.0 * macs_per_pair * 189 * 8 ** lev
         tc_flop = 2.0 * r * (r - sol.lead) * I_leaf           # algorithmic flops of the tensor-core part
         achieved = exec_flop / (m2l_ms / 1e3) / 1e12
-        roof = {"kernel": "m2l_tc (split-bf16 tcgen05 M2L, leaf level)", "bound": "tensor",
-                "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-                "peak_source": f"{peak_src} bf16 dense burst",
-                "achieved_note": "executed MMA flops (adaptive split-BF16 product map) / launch time",
+        # the launch is timed back to back inside a long power-capped step: sustained peak
+        roof = {"kernel": "m2l_tc2 (split-bf16 tcgen05 M2L with the FP64 leading block, leaf level)",
+                "bound": "tensor",
+                "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s", "frac": achieved / bf16_sus,
+                "peak_source": f"{peak_src} bf16 dense sustained",
+                "achieved_note": "executed BF16 MMA flops (adaptive split-BF16 product map) / launch time; "
+                                 "the same launch also runs the FP64 leading block (i < 32, j < 16) on DMMA",
+                "fp64_lead_flop": 2.0 * 32 * 16 * I_leaf,
                 "algorithmic_tflops": tc_flop / (m2l_ms / 1e3) / 1e12,
                 "traffic": TC_DRAM_BYTES_PER_CELL * 8 ** lev,
                 "traffic_note": "ncu dram bytes of the level-5 launch scaled by cells",

@@ -219,10 +219,10 @@ BBFMM_B200_API int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *s, long long cell
 BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
 
 /* MIXED mode: products per term of the tensor-core M2L. 0 (default, adaptive): the three
- * split-BF16 products hi*hi + hi*lo + lo*hi for the contraction components j < 96 and the
- * outputs i < 96 of every operator, hi*hi alone for the rest, whose terms are small enough
- * (singular-value ordered operators) that one BF16 product adds below 1e-8 of |L|; 3: the
- * three products everywhere; 1: hi*hi everywhere (plain BF16, for precision comparisons). */
+ * split-BF16 products hi*hi + hi*lo + lo*hi for the contraction components j < 64 and the
+ * outputs i < 64 of every operator, hi*hi alone for the rest, whose terms are small enough
+ * (singular-value ordered operators) for one BF16 product; 3: the three products
+ * everywhere; 1: hi*hi everywhere (plain BF16, for precision comparisons). */
 BBFMM_B200_API int bbfmm_b200_set_tc_products(bbfmm_b200_solver *s, int nprod);
 
 /* Autotuner (no counterpart in the reference): runs an upward pass with q_dev, then times the
