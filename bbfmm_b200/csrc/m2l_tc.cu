@@ -683,6 +683,214 @@ __global__ void __launch_bounds__(192, 1)
   }
 }
 
+// Down projection in one pass (mixed mode): for the rows t < rows of a level (or slab),
+//   F[t][n] = scale cs[n] (sum_{j < 32} L[cpg(row0 + t)][j] Dn(n, j)  +  sum_{32 <= j < 32 kc1} L'[t][j] Dn(n, j))
+// the first sum in FP64 (DMMA, the epilogue warps), the second from the split-BF16 rows L'
+// (Morton order) on the tensor cores, F written once. Persistent CTAs walk tiles of 128 rows
+// x 256 columns (tile = 2 row-tile + column block); two 256-column accumulators in tensor
+// memory let the MMA of a CTA's next tile run while its epilogue drains the previous one.
+// Epilogue warp q owns rows 32q .. 32q + 31 of the tile; per 32-column chunk it computes the
+// FP64 part as DMMA fragments (k-slot u of step ks standing for component 8u + ks, so that a
+// thread's A and B fragments are 64 contiguous bytes), stages them in shared memory, adds its
+// tensor-memory row and writes the chunk row by row (256 coalesced bytes per store).
+constexpr int PD_STAGES = 3, PD_SROW = 33;  // staging rows of 33 doubles: few bank conflicts
+constexpr int PD_STAGING = 4 * 32 * PD_SROW * 8;
+constexpr int PD_SMEM = PD_STAGES * STAGE_BYTES + PD_STAGING + 1024 /*align*/ + 256 /*barriers*/;
+static_assert(PD_SMEM <= 232448, "down-projection stages exceed the shared memory of a CTA");
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(192, 1)
+    proj_down_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
+                     const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
+                     const double *__restrict__ Lfp, int ldl, const double *__restrict__ Dlead,
+                     double *__restrict__ F, int ldf, int64_t rows, int level, int64_t row0, int kc0, int kc1,
+                     const double *__restrict__ cs, double scale, int64_t ntiles) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *gbase = smem_raw + (base - raw);
+  double *staging = reinterpret_cast<double *>(gbase + PD_STAGES * STAGE_BYTES);
+  const uint32_t bar_base = base + PD_STAGES * STAGE_BYTES + PD_STAGING;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + PD_STAGES * STAGE_BYTES + PD_STAGING);
+  // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the tmem slot
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * PD_STAGES + 4);
+  auto full_bar = [&](int st) { return bar_base + 8u * st; };
+  auto empty_bar = [&](int st) { return bar_base + 8u * (PD_STAGES + st); };
+  auto accf_bar = [&](int b) { return bar_base + 8u * (2 * PD_STAGES + b); };
+  auto acce_bar = [&](int b) { return bar_base + 8u * (2 * PD_STAGES + 2 + b); };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < PD_STAGES; ++st) {
+      mbar_init(full_bar(st), 1);
+      mbar_init(empty_bar(st), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf_bar(b), 1);  // tcgen05.commit of the tile's last MMA
+      mbar_init(acce_bar(b), 4);  // one arrival per epilogue warp
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nk = kc1 - kc0;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer
+    int it = 0;
+    bool alive = true;
+    for (int64_t tile = blockIdx.x; tile < ntiles && alive; tile += gridDim.x) {
+      const int t0 = (int)((tile >> 1) * BM), col0 = (int)(tile & 1) * BN;
+      for (int kc = kc0; kc < kc1; ++kc, ++it) {
+        const int st = it % PD_STAGES;
+        const uint32_t ph = (uint32_t)(it / PD_STAGES) & 1u;
+        if (!mbar_wait(empty_bar(st), ph ^ 1u, 21)) {
+          alive = false;
+          break;
+        }
+        const uint32_t sa = base + st * STAGE_BYTES;
+        mbar_expect_tx(full_bar(st), STAGE_BYTES);
+        tma_load_2d(sa, &mapAhi, full_bar(st), kc * BK, t0);
+        tma_load_2d(sa + A_BYTES, &mapAlo, full_bar(st), kc * BK, t0);
+        tma_load_2d(sa + 2 * A_BYTES, &mapBhi, full_bar(st), kc * BK, col0);
+        tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(st), kc * BK, col0);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    int it = 0, lt = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
+      const int b = lt & 1;
+      const uint32_t use = (uint32_t)(lt >> 1) & 1u;
+      if (!mbar_wait(acce_bar(b), use ^ 1u, 22)) break;  // the epilogue has drained accumulator b
+      tc_fence_after();
+      bool ok = true;
+      for (int kc = 0; kc < nk; ++kc, ++it) {
+        const int st = it % PD_STAGES;
+        const uint32_t ph = (uint32_t)(it / PD_STAGES) & 1u;
+        if (!mbar_wait(full_bar(st), ph, 23)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = base + st * STAGE_BYTES;
+        for (int ks = 0; ks < KS; ++ks) {
+          const uint64_t ahi = sw64_desc(sa + ks * 32), alo = sw64_desc(sa + A_BYTES + ks * 32);
+          const uint64_t bhi = sw64_desc(sa + 2 * A_BYTES + ks * 32);
+          const uint64_t blo = sw64_desc(sa + 2 * A_BYTES + B_BYTES + ks * 32);
+          const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
+          mma_bf16(tmem + b * BN, ahi, bhi, acc);
+          mma_bf16(tmem + b * BN, ahi, blo, 1u);
+          mma_bf16(tmem + b * BN, alo, bhi, 1u);
+        }
+        mma_commit(empty_bar(st));
+      }
+      mma_commit(accf_bar(b));
+      if (!ok) break;
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue: FP64 leading part + tensor-memory rows -> F
+    const int q = warp & 3;
+    const int u = lane & 3, tr = lane >> 2;
+    double *stg = staging + q * 32 * PD_SROW;
+    int lt = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
+      const int b = lt & 1;
+      const uint32_t use = (uint32_t)(lt >> 1) & 1u;
+      const int64_t t0 = (tile >> 1) * BM + q * 32;
+      const int col0 = (int)(tile & 1) * BN;
+      // A fragments: rows t0 + 8m + tr, components 8u .. 8u + 7 (FP64 L in cpg order)
+      double2 a[4][4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int64_t t = t0 + 8 * m + tr;
+        if (t < rows) {
+          const int64_t g = row0 + t;
+          int ix, iy, iz;
+          morton_to_grid(g, level, ix, iy, iz);
+          const int64_t crow = (g & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
+          const double2 *src = reinterpret_cast<const double2 *>(Lfp + crow * ldl + 8 * u);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) a[m][e] = src[e];
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) a[m][e] = make_double2(0.0, 0.0);
+        }
+      }
+      // warp-uniform: a wait that gave up (status word set) ends this warp's tiles
+      if (!__all_sync(0xffffffffu, mbar_wait(accf_bar(b), use, 24))) break;
+      tc_fence_after();
+      for (int cc = 0; cc < BN / 32; ++cc) {
+        const int n0 = col0 + cc * 32;
+        double acc[4][4][2];
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          const double2 *src = reinterpret_cast<const double2 *>(Dlead + (int64_t)(n0 + 8 * f + tr) * 32 + 8 * u);
+          double2 bf[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) bf[e] = src[e];
+#pragma unroll
+          for (int ks = 0; ks < 8; ++ks) {
+            const double bv = (ks & 1) ? bf[ks >> 1].y : bf[ks >> 1].x;
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+              dmma_f64(acc[m][f][0], acc[m][f][1], (ks & 1) ? a[m][ks >> 1].y : a[m][ks >> 1].x, bv);
+          }
+        }
+        // stage the FP64 part: row 8m + tr, columns 8f + 2u + {0, 1}
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            stg[(8 * m + tr) * PD_SROW + 8 * f + 2 * u] = acc[m][f][0];
+            stg[(8 * m + tr) * PD_SROW + 8 * f + 2 * u + 1] = acc[m][f][1];
+          }
+        __syncwarp();
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + cc * 32), v);  // every lane
+#pragma unroll
+        for (int c = 0; c < 32; ++c) stg[lane * PD_SROW + c] += (double)v[c];
+        __syncwarp();
+        const double sc = cs ? scale * cs[n0 + lane] : scale;
+        for (int rr = 0; rr < 32; ++rr)
+          if (t0 + rr < rows) F[(t0 + rr) * ldf + n0 + lane] = sc * stg[rr * PD_SROW + lane];
+        __syncwarp();
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce_bar(b));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+// Dlead[n][j] = B[j][n] for j < lead: the leading rows of a K x N operator, transposed.
+__global__ void lead_transpose_kernel(int K, int N, int lead, const double *__restrict__ B, double *__restrict__ Dlead) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N * lead; e += gridDim.x * blockDim.x)
+    Dlead[e] = B[(int64_t)(e % lead) * N + e / lead];
+}
+
 // dst = [hi | lo] split of rows x K values; row t comes from src row cpg(row0 + t) of
 // `level` when gather != 0 (Morton order from the class-major grid), else from row t.
 // One warp per row (grid-stride), 8 consecutive values per lane and step: two 32-byte
@@ -830,6 +1038,7 @@ struct TcProj {
   int n3 = 0, r = 0, lead = 0;
   __nv_bfloat16 *up = nullptr;  // [hi | lo] of Bup^T: r x n3, rows j < lead zero
   __nv_bfloat16 *dn = nullptr;  // [hi | lo] of Bdn^T: n3 x r
+  double *dn_lead = nullptr;    // FP64 Bdn^T for j < lead: n3 x lead
   CUtensorMap up_hi, up_lo, dn_hi, dn_lo;
 };
 
@@ -849,12 +1058,14 @@ int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, 
   TcProj *p = new TcProj();
   p->n3 = n3; p->r = r; p->lead = lead;
   const size_t cnt = (size_t)n3 * r;
-  if (cudaMalloc(&p->up, cnt * 4) != cudaSuccess || cudaMalloc(&p->dn, cnt * 4) != cudaSuccess) {
+  if (cudaMalloc(&p->up, cnt * 4) != cudaSuccess || cudaMalloc(&p->dn, cnt * 4) != cudaSuccess ||
+      cudaMalloc(&p->dn_lead, (size_t)n3 * lead * 8) != cudaSuccess) {
     tc_free_projections(p);
     return bbfmm_set_error(BBFMM_ERR_NOMEM, "projection operator split allocation failed");
   }
   tc::transpose_split_kernel<<<148, 256, 0, s>>>(n3, r, Bup, p->up, p->up + cnt, lead);  // Bup: n3 x r
   tc::transpose_split_kernel<<<148, 256, 0, s>>>(r, n3, Bdn, p->dn, p->dn + cnt, 0);     // Bdn: r x n3
+  tc::lead_transpose_kernel<<<64, 256, 0, s>>>(r, n3, lead, Bdn, p->dn_lead);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     tc_free_projections(p);
@@ -877,6 +1088,7 @@ void tc_free_projections(void *v) {
   if (!p) return;
   if (p->up) cudaFree(p->up);
   if (p->dn) cudaFree(p->dn);
+  if (p->dn_lead) cudaFree(p->dn_lead);
   delete p;
 }
 
@@ -910,6 +1122,36 @@ int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, do
                                                          p->lead / tc::BK, (rank > 0 ? rank : p->r) / tc::BK, 0, 1, cs,
                                                          scale);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_tc", __FILE__, __LINE__);
+}
+
+// Down projection of `rows` Morton rows (row0 ..) of `level` in one pass: F[t][l] = scale Kw[l]
+// (sum_{j < lead} L[cpg(row0 + t)][j] Bdn[j][l] in FP64 + sum_{lead <= j < rank} L'[t][j] Bdn[j][l]
+// from the split rows L' = Asplit), F rows ldf apart, assigned.
+int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int64_t rows, double *F, int level,
+                     int64_t row0, const double *cs, double scale, cudaStream_t s, int rank) {
+  const TcProj *p = (const TcProj *)pv;
+  if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
+  if (rows <= 0) return BBFMM_OK;
+  if (p->lead != 32 || p->n3 % tc::BN) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fused down projection: lead 32");
+  const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Asplit;
+  const __nv_bfloat16 *lo = hi + (size_t)rows * p->r;
+  CUtensorMap ahi, alo;
+  int rc = map2d(&ahi, hi, rows, p->r, tc::BM);
+  if (rc == BBFMM_OK) rc = map2d(&alo, lo, rows, p->r, tc::BM);
+  if (rc != BBFMM_OK) return rc;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc::proj_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::PD_SMEM);
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "proj_down smem attribute", __FILE__, __LINE__);
+    attr = true;
+  }
+  const int64_t ntiles = ((rows + tc::BM - 1) / tc::BM) * (p->n3 / tc::BN);
+  if (p->n3 / tc::BN != 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fused down projection: n3 = 512");
+  const int grid = (int)(ntiles < 148 ? ntiles : 148);
+  tc::proj_down_kernel<<<grid, 192, tc::PD_SMEM, s>>>(ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3,
+                                                      rows, level, row0, p->lead / tc::BK,
+                                                      (rank > 0 ? rank : p->r) / tc::BK, cs, scale, ntiles);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "proj_down", __FILE__, __LINE__);
 }
 
 // [hi | lo] split of rows x K FP64 values; gather != 0 reads row t from the cpg row of Morton

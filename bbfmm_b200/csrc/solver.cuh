@@ -86,6 +86,8 @@ int tc_wait_probe(unsigned limit, int code);
 // contraction over j >= lead of the down projection, as split-BF16 products.
 int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out, cudaStream_t s);
 void tc_free_projections(void *p);
+int launch_proj_down(const void *p, const void *Asplit, const double *Lfp, int64_t rows, double *F, int level,
+                     int64_t row0, const double *cs, double scale, cudaStream_t s, int rank = 0);
 int launch_proj_tc(const void *p, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
                    const double *cs, double scale, cudaStream_t s, int rank = 0);
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
