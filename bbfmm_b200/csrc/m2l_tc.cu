@@ -689,12 +689,17 @@ __global__ void __launch_bounds__(192, 1)
 // (Morton order) on the tensor cores, F written once. Persistent CTAs walk tiles of 128 rows
 // x 256 columns (tile = 2 row-tile + column block); two 256-column accumulators in tensor
 // memory let the MMA of a CTA's next tile run while its epilogue drains the previous one.
-// Epilogue warp q owns rows 32q .. 32q + 31 of the tile; per 32-column chunk it computes the
-// FP64 part as DMMA fragments (k-slot u of step ks standing for component 8u + ks, so that a
-// thread's A and B fragments are 64 contiguous bytes), stages them in shared memory, adds its
-// tensor-memory row and writes the chunk row by row (256 coalesced bytes per store).
+// Eight epilogue warps, two per tensor-memory lane quarter q (rows 32q .. 32q + 31 of the
+// tile), so that each SM sub-partition interleaves two of them: per 32-column chunk, warp half
+// h computes the FP64 part of rows 32q + 16h + [0, 16) as DMMA fragments (k-slot u of step ks
+// standing for component 8u + ks, so that a thread's A and B fragments are 64 contiguous
+// bytes) into the quarter's staging tile; after a barrier of the pair it adds the
+// tensor-memory columns 16h .. 16h + 15 of all 32 rows, and after a second barrier it writes
+// its 16 rows of the chunk (256 coalesced bytes per store). Two staging tiles alternate by
+// chunk.
 constexpr int PD_STAGES = 3, PD_SROW = 33;  // staging rows of 33 doubles: few bank conflicts
-constexpr int PD_STAGING = 4 * 32 * PD_SROW * 8;
+constexpr int PD_STAGING = 4 * 2 * 32 * PD_SROW * 8;
+constexpr int PD_THREADS = 320;
 constexpr int PD_SMEM = PD_STAGES * STAGE_BYTES + PD_STAGING + 1024 /*align*/ + 256 /*barriers*/;
 static_assert(PD_SMEM <= 232448, "down-projection stages exceed the shared memory of a CTA");
 
@@ -702,7 +707,24 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__global__ void __launch_bounds__(192, 1)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void pair_bar(int q) {  // the two epilogue warps of lane quarter q
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + q) : "memory");
+}
+
+__global__ void __launch_bounds__(PD_THREADS, 1)
     proj_down_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                      const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                      const double *__restrict__ Lfp, int ldl, const double *__restrict__ Dlead,
@@ -715,8 +737,9 @@ __global__ void __launch_bounds__(192, 1)
   double *staging = reinterpret_cast<double *>(gbase + PD_STAGES * STAGE_BYTES);
   const uint32_t bar_base = base + PD_STAGES * STAGE_BYTES + PD_STAGING;
   uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + PD_STAGES * STAGE_BYTES + PD_STAGING);
-  // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the tmem slot
+  // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the tmem slot and the pair flags
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * PD_STAGES + 4);
+  volatile int *pair_ok = reinterpret_cast<volatile int *>(tmem_slot + 4);
   auto full_bar = [&](int st) { return bar_base + 8u * st; };
   auto empty_bar = [&](int st) { return bar_base + 8u * (PD_STAGES + st); };
   auto accf_bar = [&](int b) { return bar_base + 8u * (2 * PD_STAGES + b); };
@@ -730,7 +753,7 @@ __global__ void __launch_bounds__(192, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf_bar(b), 1);  // tcgen05.commit of the tile's last MMA
-      mbar_init(acce_bar(b), 4);  // one arrival per epilogue warp
+      mbar_init(acce_bar(b), 8);  // one arrival per epilogue warp
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -802,20 +825,20 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else if (warp >= 2) {
     // ---------------- epilogue: FP64 leading part + tensor-memory rows -> F
-    const int q = warp & 3;
+    const int q = warp & 3, h = (warp - 2) >> 2;
     const int u = lane & 3, tr = lane >> 2;
-    double *stg = staging + q * 32 * PD_SROW;
+    double *stg0 = staging + q * 2 * 32 * PD_SROW;
     int lt = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
       const int b = lt & 1;
       const uint32_t use = (uint32_t)(lt >> 1) & 1u;
-      const int64_t t0 = (tile >> 1) * BM + q * 32;
+      const int64_t tq = (tile >> 1) * BM + q * 32;  // first row of the quarter
       const int col0 = (int)(tile & 1) * BN;
-      // A fragments: rows t0 + 8m + tr, components 8u .. 8u + 7 (FP64 L in cpg order)
-      double2 a[4][4];
+      // A fragments: rows tq + 16h + 8m + tr, components 8u .. 8u + 7 (FP64 L in cpg order)
+      double2 a[2][4];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int64_t t = t0 + 8 * m + tr;
+      for (int m = 0; m < 2; ++m) {
+        const int64_t t = tq + 16 * h + 8 * m + tr;
         if (t < rows) {
           const int64_t g = row0 + t;
           int ix, iy, iz;
@@ -829,14 +852,19 @@ __global__ void __launch_bounds__(192, 1)
           for (int e = 0; e < 4; ++e) a[m][e] = make_double2(0.0, 0.0);
         }
       }
-      // warp-uniform: a wait that gave up (status word set) ends this warp's tiles
-      if (!__all_sync(0xffffffffu, mbar_wait(accf_bar(b), use, 24))) break;
+      // a wait that gave up (status word set) ends the tiles of both warps of the pair
+      const bool okw = __all_sync(0xffffffffu, mbar_wait(accf_bar(b), use, 24));
+      if (lane == 0) pair_ok[2 * q + h] = okw ? 1 : 0;
+      pair_bar(q);
+      if (!(pair_ok[2 * q] && pair_ok[2 * q + 1])) break;
       tc_fence_after();
+      const int nrow = rows - tq < 32 ? (int)(rows - tq) : 32;  // valid rows of the quarter
       for (int cc = 0; cc < BN / 32; ++cc) {
         const int n0 = col0 + cc * 32;
-        double acc[4][4][2];
+        double *stg = stg0 + (cc & 1) * 32 * PD_SROW;
+        double acc[2][4][2];
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
+        for (int m = 0; m < 2; ++m)
 #pragma unroll
           for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
 #pragma unroll
@@ -849,28 +877,33 @@ __global__ void __launch_bounds__(192, 1)
           for (int ks = 0; ks < 8; ++ks) {
             const double bv = (ks & 1) ? bf[ks >> 1].y : bf[ks >> 1].x;
 #pragma unroll
-            for (int m = 0; m < 4; ++m)
+            for (int m = 0; m < 2; ++m)
               dmma_f64(acc[m][f][0], acc[m][f][1], (ks & 1) ? a[m][ks >> 1].y : a[m][ks >> 1].x, bv);
           }
         }
-        // stage the FP64 part: row 8m + tr, columns 8f + 2u + {0, 1}
+        // stage the FP64 part: row 16h + 8m + tr, columns 8f + 2u + {0, 1}
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
+        for (int m = 0; m < 2; ++m)
 #pragma unroll
           for (int f = 0; f < 4; ++f) {
-            stg[(8 * m + tr) * PD_SROW + 8 * f + 2 * u] = acc[m][f][0];
-            stg[(8 * m + tr) * PD_SROW + 8 * f + 2 * u + 1] = acc[m][f][1];
+            stg[(16 * h + 8 * m + tr) * PD_SROW + 8 * f + 2 * u] = acc[m][f][0];
+            stg[(16 * h + 8 * m + tr) * PD_SROW + 8 * f + 2 * u + 1] = acc[m][f][1];
           }
-        __syncwarp();
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + cc * 32), v);  // every lane
+        pair_bar(q);
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + cc * 32 + 16 * h), v);  // every lane
 #pragma unroll
-        for (int c = 0; c < 32; ++c) stg[lane * PD_SROW + c] += (double)v[c];
-        __syncwarp();
+        for (int c = 0; c < 16; ++c) stg[lane * PD_SROW + 16 * h + c] += (double)v[c];
+        pair_bar(q);
         const double sc = cs ? scale * cs[n0 + lane] : scale;
-        for (int rr = 0; rr < 32; ++rr)
-          if (t0 + rr < rows) F[(t0 + rr) * ldf + n0 + lane] = sc * stg[rr * PD_SROW + lane];
-        __syncwarp();
+        if (nrow == 32) {
+#pragma unroll
+          for (int rr = 0; rr < 16; ++rr)
+            F[(tq + 16 * h + rr) * ldf + n0 + lane] = sc * stg[(16 * h + rr) * PD_SROW + lane];
+        } else {
+          for (int rr = 0; rr < 16; ++rr)
+            if (16 * h + rr < nrow) F[(tq + 16 * h + rr) * ldf + n0 + lane] = sc * stg[(16 * h + rr) * PD_SROW + lane];
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -1148,7 +1181,7 @@ int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int6
   const int64_t ntiles = ((rows + tc::BM - 1) / tc::BM) * (p->n3 / tc::BN);
   if (p->n3 / tc::BN != 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fused down projection: n3 = 512");
   const int grid = (int)(ntiles < 148 ? ntiles : 148);
-  tc::proj_down_kernel<<<grid, 192, tc::PD_SMEM, s>>>(ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3,
+  tc::proj_down_kernel<<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3,
                                                       rows, level, row0, p->lead / tc::BK,
                                                       (rank > 0 ? rank : p->r) / tc::BK, cs, scale, ntiles);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_down", __FILE__, __LINE__);
