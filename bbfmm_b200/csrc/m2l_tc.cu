@@ -684,7 +684,7 @@ __global__ void __launch_bounds__(192, 1)
 }
 
 // Down projection in one pass (mixed mode): for the rows t < rows of a level (or slab),
-//   F[t][n] = scale cs[n] (sum_{j < 32} L[cpg(row0 + t)][j] Dn(n, j)  +  sum_{32 <= j < 32 kc1} L'[t][j] Dn(n, j))
+//   F[t][n] = scale cs[n] (sum_{j < 16} L[cpg(row0 + t)][j] Dn(n, j)  +  sum_{16 <= j < 32 kc1} L'[t][j] Dn(n, j))
 // the first sum in FP64 (DMMA, the epilogue warps), the second from the split-BF16 rows L'
 // (Morton order) on the tensor cores, F written once. Persistent CTAs walk tiles of 128 rows
 // x 256 columns (tile = 2 row-tile + column block); two 256-column accumulators in tensor
@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(192, 1)
 // Eight epilogue warps, two per tensor-memory lane quarter q (rows 32q .. 32q + 31 of the
 // tile), so that each SM sub-partition interleaves two of them: per 32-column chunk, warp half
 // h computes the FP64 part of rows 32q + 16h + [0, 16) as DMMA fragments (k-slot u of step ks
-// standing for component 8u + ks, so that a thread's A and B fragments are 64 contiguous
+// standing for component 4u + ks, so that a thread's A and B fragments are 32 contiguous
 // bytes) into the quarter's staging tile; after a barrier of the pair it adds the
 // tensor-memory columns 16h .. 16h + 15 of all 32 rows, and after a second barrier it writes
 // its 16 rows of the chunk (256 coalesced bytes per store). Two staging tiles alternate by
@@ -700,6 +700,7 @@ __global__ void __launch_bounds__(192, 1)
 constexpr int PD_STAGES = 3, PD_SROW = 33;  // staging rows of 33 doubles: few bank conflicts
 constexpr int PD_STAGING = 4 * 2 * 32 * PD_SROW * 8;
 constexpr int PD_THREADS = 320;
+constexpr int DN_LEAD = 16;  // FP64 components of the down projection (the split rows zero them)
 constexpr int PD_SMEM = PD_STAGES * STAGE_BYTES + PD_STAGING + 1024 /*align*/ + 256 /*barriers*/;
 static_assert(PD_SMEM <= 232448, "down-projection stages exceed the shared memory of a CTA");
 
@@ -834,8 +835,8 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
       const uint32_t use = (uint32_t)(lt >> 1) & 1u;
       const int64_t tq = (tile >> 1) * BM + q * 32;  // first row of the quarter
       const int col0 = (int)(tile & 1) * BN;
-      // A fragments: rows tq + 16h + 8m + tr, components 8u .. 8u + 7 (FP64 L in cpg order)
-      double2 a[2][4];
+      // A fragments: rows tq + 16h + 8m + tr, components 4u .. 4u + 3 (FP64 L in cpg order)
+      double2 a[2][2];
 #pragma unroll
       for (int m = 0; m < 2; ++m) {
         const int64_t t = tq + 16 * h + 8 * m + tr;
@@ -844,12 +845,11 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
           int ix, iy, iz;
           morton_to_grid(g, level, ix, iy, iz);
           const int64_t crow = (g & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
-          const double2 *src = reinterpret_cast<const double2 *>(Lfp + crow * ldl + 8 * u);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) a[m][e] = src[e];
+          const double2 *src = reinterpret_cast<const double2 *>(Lfp + crow * ldl + 4 * u);
+          a[m][0] = src[0];
+          a[m][1] = src[1];
         } else {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) a[m][e] = make_double2(0.0, 0.0);
+          a[m][0] = a[m][1] = make_double2(0.0, 0.0);
         }
       }
       // a wait that gave up (status word set) ends the tiles of both warps of the pair
@@ -869,12 +869,11 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
           for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-          const double2 *src = reinterpret_cast<const double2 *>(Dlead + (int64_t)(n0 + 8 * f + tr) * 32 + 8 * u);
-          double2 bf[4];
+          const double2 *src =
+              reinterpret_cast<const double2 *>(Dlead + (int64_t)(n0 + 8 * f + tr) * DN_LEAD + 4 * u);
+          const double2 bf[2] = {src[0], src[1]};
 #pragma unroll
-          for (int e = 0; e < 4; ++e) bf[e] = src[e];
-#pragma unroll
-          for (int ks = 0; ks < 8; ++ks) {
+          for (int ks = 0; ks < 4; ++ks) {
             const double bv = (ks & 1) ? bf[ks >> 1].y : bf[ks >> 1].x;
 #pragma unroll
             for (int m = 0; m < 2; ++m)
@@ -929,7 +928,8 @@ __global__ void lead_transpose_kernel(int K, int N, int lead, const double *__re
 // One warp per row (grid-stride), 8 consecutive values per lane and step: two 32-byte
 // loads, one 16-byte store per plane. K is a multiple of 256.
 __global__ void split_rows_kernel(int64_t rows, int K, const double *__restrict__ src, int gather, int level,
-                                  int64_t row0, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+                                  int64_t row0, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
+                                  int zlead) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -945,7 +945,11 @@ __global__ void split_rows_kernel(int64_t rows, int K, const double *__restrict_
     uint4 *oh = reinterpret_cast<uint4 *>(hi + t * K), *ol = reinterpret_cast<uint4 *>(lo + t * K);
     for (int c = lane; c < K / 8; c += 32) {
       const double4 a = in[2 * c], b = in[2 * c + 1];
-      const double x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      double x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      if (8 * c < zlead) {  // components below zlead are computed elsewhere (FP64)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = 8 * c + i < zlead ? 0.0 : x[i];
+      }
       __align__(16) __nv_bfloat16 h[8], l[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
@@ -1071,7 +1075,7 @@ struct TcProj {
   int n3 = 0, r = 0, lead = 0;
   __nv_bfloat16 *up = nullptr;  // [hi | lo] of Bup^T: r x n3, rows j < lead zero
   __nv_bfloat16 *dn = nullptr;  // [hi | lo] of Bdn^T: n3 x r
-  double *dn_lead = nullptr;    // FP64 Bdn^T for j < lead: n3 x lead
+  double *dn_lead = nullptr;    // FP64 Bdn^T for j < DN_LEAD: n3 x DN_LEAD
   CUtensorMap up_hi, up_lo, dn_hi, dn_lo;
 };
 
@@ -1092,13 +1096,13 @@ int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, 
   p->n3 = n3; p->r = r; p->lead = lead;
   const size_t cnt = (size_t)n3 * r;
   if (cudaMalloc(&p->up, cnt * 4) != cudaSuccess || cudaMalloc(&p->dn, cnt * 4) != cudaSuccess ||
-      cudaMalloc(&p->dn_lead, (size_t)n3 * lead * 8) != cudaSuccess) {
+      cudaMalloc(&p->dn_lead, (size_t)n3 * tc::DN_LEAD * 8) != cudaSuccess) {
     tc_free_projections(p);
     return bbfmm_set_error(BBFMM_ERR_NOMEM, "projection operator split allocation failed");
   }
   tc::transpose_split_kernel<<<148, 256, 0, s>>>(n3, r, Bup, p->up, p->up + cnt, lead);  // Bup: n3 x r
   tc::transpose_split_kernel<<<148, 256, 0, s>>>(r, n3, Bdn, p->dn, p->dn + cnt, 0);     // Bdn: r x n3
-  tc::lead_transpose_kernel<<<64, 256, 0, s>>>(r, n3, lead, Bdn, p->dn_lead);
+  tc::lead_transpose_kernel<<<64, 256, 0, s>>>(r, n3, tc::DN_LEAD, Bdn, p->dn_lead);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     tc_free_projections(p);
@@ -1158,14 +1162,14 @@ int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, do
 }
 
 // Down projection of `rows` Morton rows (row0 ..) of `level` in one pass: F[t][l] = scale Kw[l]
-// (sum_{j < lead} L[cpg(row0 + t)][j] Bdn[j][l] in FP64 + sum_{lead <= j < rank} L'[t][j] Bdn[j][l]
-// from the split rows L' = Asplit), F rows ldf apart, assigned.
+// (sum_{j < 16} L[cpg(row0 + t)][j] Bdn[j][l] in FP64 + sum_{16 <= j < rank} L'[t][j] Bdn[j][l]
+// from the split rows L' = Asplit, whose components j < 16 are zero), F rows n3 apart, assigned.
 int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int64_t rows, double *F, int level,
                      int64_t row0, const double *cs, double scale, cudaStream_t s, int rank) {
   const TcProj *p = (const TcProj *)pv;
   if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
   if (rows <= 0) return BBFMM_OK;
-  if (p->lead != 32 || p->n3 % tc::BN) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fused down projection: lead 32");
+  if (p->n3 != 2 * tc::BN) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fused down projection: n3 = 512");
   const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Asplit;
   const __nv_bfloat16 *lo = hi + (size_t)rows * p->r;
   CUtensorMap ahi, alo;
@@ -1179,21 +1183,20 @@ int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int6
     attr = true;
   }
   const int64_t ntiles = ((rows + tc::BM - 1) / tc::BM) * (p->n3 / tc::BN);
-  if (p->n3 / tc::BN != 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fused down projection: n3 = 512");
   const int grid = (int)(ntiles < 148 ? ntiles : 148);
   tc::proj_down_kernel<<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3,
-                                                      rows, level, row0, p->lead / tc::BK,
-                                                      (rank > 0 ? rank : p->r) / tc::BK, cs, scale, ntiles);
+                                                      rows, level, row0, 0, (rank > 0 ? rank : p->r) / tc::BK, cs,
+                                                      scale, ntiles);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_down", __FILE__, __LINE__);
 }
 
 // [hi | lo] split of rows x K FP64 values; gather != 0 reads row t from the cpg row of Morton
 // cell row0 + t of `level`.
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
-                  cudaStream_t s) {
+                  cudaStream_t s, int zlead) {
   if (K % 256) return bbfmm_set_error(BBFMM_ERR_ARG, "split rows: K must be a multiple of 256");
   __nv_bfloat16 *hi = (__nv_bfloat16 *)dst;
-  tc::split_rows_kernel<<<148 * 16, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K);
+  tc::split_rows_kernel<<<148 * 16, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K, zlead);
   return bbfmm_set_cuda_error(cudaGetLastError(), "split", __FILE__, __LINE__);
 }
 

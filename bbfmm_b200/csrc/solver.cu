@@ -413,8 +413,8 @@ int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows) {
   const T scale = (T)1 / cell_length<T>(level, (T)L);
   if (!proj_tc() || rows > Lsplit_rows)  // contraction over the effective rank (j < rk())
     return proj(rows, rk(), n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0, r);
-  // components j < PROJ_LEAD in FP64 and the rest as split-BF16 tensor-core products, one pass
-  TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream));
+  // components j < 16 in FP64 and the rest as split-BF16 tensor-core products, one pass
+  TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream, 16));
   return launch_proj_down(tcproj, Lsplit, (const double *)Lbuf, rows, (double *)F_rows, level, row0,
                           (const double *)kw, (double)scale, stream, rk());
 }

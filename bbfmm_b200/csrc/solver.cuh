@@ -91,7 +91,7 @@ int launch_proj_down(const void *p, const void *Asplit, const double *Lfp, int64
 int launch_proj_tc(const void *p, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
                    const double *cs, double scale, cudaStream_t s, int rank = 0);
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
-                  cudaStream_t s);
+                  cudaStream_t s, int zlead = 0);
 constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
 
 // Launch choices of one solver, per level (index = level): what the autotuner sets.
