@@ -565,130 +565,16 @@ __global__ void split_kernel(int64_t count, const double *__restrict__ src, __nv
 }
 
 // ---------------------------------------------------------------- projections
-// The U-projections around the M2L with the same split-BF16 tensor-core machinery:
-//   C[out(t)][col0 + n] (=, or += when `add`) scale * cs[col0 + n] * sum_k A[t][k] B[col0 + n][k]
-// for one tile of 128 consecutive rows t of A (its storage order) and 256 columns (blockIdx.y
-// selects the 256-column block), K-chunks kc0 .. kc1-1 of 32. Columns below col_skip are not
-// written (the FP64 leading part owns them). outmap: 1 = A rows are Morton cells row0 + t
-// of `level` and C rows their cpg index (up projection); 0 = same row (down projection, whose
-// A rows were gathered into Morton order). Rows t >= rows are zero-filled by TMA and skipped.
-__global__ void __launch_bounds__(192, 1)
-    proj_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
-                   const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
-                   double *__restrict__ C, int ldc, int64_t rows, int level, int outmap, int64_t row0, int kc0,
-                   int kc1, int col_skip, int add, const double *__restrict__ cs, double scale) {
-  extern __shared__ uint8_t smem_raw[];
-  const uint32_t raw = smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;
-  uint8_t *gbase = smem_raw + (base - raw);
-  const uint32_t bar_base = base + STAGES * STAGE_BYTES;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * STAGE_BYTES);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 1);
-  auto full_bar = [&](int s) { return bar_base + 8u * s; };
-  auto empty_bar = [&](int s) { return bar_base + 8u * (STAGES + s); };
-  const uint32_t acc_bar = bar_base + 8u * (2 * STAGES);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t t0 = (int64_t)blockIdx.x * BM;
-  const int col0 = blockIdx.y * BN;
-  const int niter = kc1 - kc0;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(full_bar(s), 1);
-      mbar_init(empty_bar(s), 1);
-    }
-    mbar_init(acc_bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(256)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-
-  if (warp == 0 && lane == 0) {
-    for (int it = 0; it < niter; ++it) {
-      const int s = it % STAGES;
-      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
-      if (!mbar_wait(empty_bar(s), ph ^ 1u, 11)) break;
-      const int k = (kc0 + it) * BK;
-      const uint32_t st = base + s * STAGE_BYTES;
-      mbar_expect_tx(full_bar(s), STAGE_BYTES);
-      tma_load_2d(st, &mapAhi, full_bar(s), k, (int)t0);
-      tma_load_2d(st + A_BYTES, &mapAlo, full_bar(s), k, (int)t0);
-      tma_load_2d(st + 2 * A_BYTES, &mapBhi, full_bar(s), k, col0);
-      tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mapBlo, full_bar(s), k, col0);
-    }
-  } else if (warp == 1 && lane == 0) {
-    uint32_t acc = 0;
-    for (int it = 0; it < niter; ++it) {
-      const int s = it % STAGES;
-      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
-      if (!mbar_wait(full_bar(s), ph, 12)) break;
-      tc_fence_after();
-      const uint32_t st = base + s * STAGE_BYTES;
-      for (int ks = 0; ks < KS; ++ks) {
-        const uint64_t ahi = sw64_desc(st + ks * 32), alo = sw64_desc(st + A_BYTES + ks * 32);
-        const uint64_t bhi = sw64_desc(st + 2 * A_BYTES + ks * 32);
-        const uint64_t blo = sw64_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
-        mma_bf16(tmem, ahi, bhi, acc);
-        mma_bf16(tmem, ahi, blo, 1u);
-        mma_bf16(tmem, alo, bhi, 1u);
-        acc = 1u;
-      }
-      mma_commit(empty_bar(s));
-    }
-    mma_commit(acc_bar);  // also after an early exit: the epilogue must not wait forever
-  } else if (warp >= 2) {
-    const int q = warp & 3;  // TMEM lane quarter this warp may access
-    const int row = q * 32 + lane;
-    const bool ok = mbar_wait(acc_bar, 0, 13);
-    tc_fence_after();
-    const int64_t t = t0 + row;
-    if (ok) {
-      int64_t orow = t;
-      if (outmap == 1) {
-        const int64_t m = row0 + t;
-        int ix, iy, iz;
-        morton_to_grid(m, level, ix, iy, iz);
-        orow = (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
-      }
-      double *dst = C + orow * ldc + col0;
-      for (int col = 0; col < BN; col += 32) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);  // every lane takes part
-        if (t >= rows || col0 + col < col_skip) continue;
-#pragma unroll
-        for (int i = 0; i < 32; i += 2) {
-          const double c0 = cs ? scale * cs[col0 + col + i] : scale, c1 = cs ? scale * cs[col0 + col + i + 1] : scale;
-          double2 o = add ? *reinterpret_cast<const double2 *>(dst + col + i) : make_double2(0.0, 0.0);
-          o.x += c0 * (double)v[i];
-          o.y += c1 * (double)v[i + 1];
-          *reinterpret_cast<double2 *>(dst + col + i) = o;
-        }
-      }
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
-  }
-}
-
-// Down projection in one pass (mixed mode): for the rows t < rows of a level (or slab),
+// Projection passes with double-buffered accumulators (mixed mode). Down projection in one
+// pass: for the rows t < rows of a level (or slab),
 //   F[t][n] = scale cs[n] (sum_{j < 16} L[cpg(row0 + t)][j] Dn(n, j)  +  sum_{16 <= j < 32 kc1} L'[t][j] Dn(n, j))
 // the first sum in FP64 (DMMA, the epilogue warps), the second from the split-BF16 rows L'
 // (Morton order) on the tensor cores, F written once. Persistent CTAs walk tiles of 128 rows
 // x 256 columns (tile = 2 row-tile + column block); two 256-column accumulators in tensor
 // memory let the MMA of a CTA's next tile run while its epilogue drains the previous one.
+// The up projection (UP) runs the same kernel without the FP64 part (its FP64 columns come
+// from proj_narrow_kernel): M[cpg(row0 + t)][j] for j >= col_skip from the split S rows, one
+// 256-column block, output rows in the class-major parent grid.
 // Eight epilogue warps, two per tensor-memory lane quarter q (rows 32q .. 32q + 31 of the
 // tile), so that each SM sub-partition interleaves two of them: per 32-column chunk, warp half
 // h computes the FP64 part of rows 32q + 16h + [0, 16) as DMMA fragments (k-slot u of step ks
@@ -725,12 +611,14 @@ __device__ __forceinline__ void pair_bar(int q) {  // the two epilogue warps of 
   asm volatile("bar.sync %0, 64;" ::"r"(1 + q) : "memory");
 }
 
+template <bool UP>
 __global__ void __launch_bounds__(PD_THREADS, 1)
-    proj_down_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
-                     const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
-                     const double *__restrict__ Lfp, int ldl, const double *__restrict__ Dlead,
-                     double *__restrict__ F, int ldf, int64_t rows, int level, int64_t row0, int kc0, int kc1,
-                     const double *__restrict__ cs, double scale, int64_t ntiles) {
+    proj_fused_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
+                      const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
+                      const double *__restrict__ Lfp, int ldl, const double *__restrict__ Dlead,
+                      double *__restrict__ F, int ldf, int64_t rows, int level, int64_t row0, int kc0, int kc1,
+                      const double *__restrict__ cs, double scale, int64_t ntiles, int col_skip) {
+  constexpr int ncb = UP ? 1 : 2;  // 256-column blocks: r = 256 outputs up, n3 = 512 down
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -776,7 +664,7 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
     int it = 0;
     bool alive = true;
     for (int64_t tile = blockIdx.x; tile < ntiles && alive; tile += gridDim.x) {
-      const int t0 = (int)((tile >> 1) * BM), col0 = (int)(tile & 1) * BN;
+      const int t0 = (int)((tile / ncb) * BM), col0 = (int)(tile % ncb) * BN;
       for (int kc = kc0; kc < kc1; ++kc, ++it) {
         const int st = it % PD_STAGES;
         const uint32_t ph = (uint32_t)(it / PD_STAGES) & 1u;
@@ -833,14 +721,22 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
       const int b = lt & 1;
       const uint32_t use = (uint32_t)(lt >> 1) & 1u;
-      const int64_t tq = (tile >> 1) * BM + q * 32;  // first row of the quarter
-      const int col0 = (int)(tile & 1) * BN;
+      const int64_t tq = (tile / ncb) * BM + q * 32;  // first row of the quarter
+      const int col0 = (int)(tile % ncb) * BN;
+      // output row of row 16h + (lane & 15) of the quarter (up: read back by shuffles)
+      int64_t orow = tq + 16 * h + (lane & 15);
+      if (UP) {
+        const int64_t g = row0 + orow;
+        int ix, iy, iz;
+        morton_to_grid(g, level, ix, iy, iz);
+        orow = (g & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
+      }
       // A fragments: rows tq + 16h + 8m + tr, components 4u .. 4u + 3 (FP64 L in cpg order)
       double2 a[2][2];
 #pragma unroll
       for (int m = 0; m < 2; ++m) {
         const int64_t t = tq + 16 * h + 8 * m + tr;
-        if (t < rows) {
+        if (!UP && t < rows) {
           const int64_t g = row0 + t;
           int ix, iy, iz;
           morton_to_grid(g, level, ix, iy, iz);
@@ -861,6 +757,7 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
       const int nrow = rows - tq < 32 ? (int)(rows - tq) : 32;  // valid rows of the quarter
       for (int cc = 0; cc < BN / 32; ++cc) {
         const int n0 = col0 + cc * 32;
+        if (n0 + 32 <= col_skip) continue;  // the same for both warps of the pair
         double *stg = stg0 + (cc & 1) * 32 * PD_SROW;
         double acc[2][4][2];
 #pragma unroll
@@ -868,7 +765,7 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
 #pragma unroll
           for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < (UP ? 0 : 4); ++f) {
           const double2 *src =
               reinterpret_cast<const double2 *>(Dlead + (int64_t)(n0 + 8 * f + tr) * DN_LEAD + 4 * u);
           const double2 bf[2] = {src[0], src[1]};
@@ -897,11 +794,15 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
         const double sc = cs ? scale * cs[n0 + lane] : scale;
         if (nrow == 32) {
 #pragma unroll
-          for (int rr = 0; rr < 16; ++rr)
-            F[(tq + 16 * h + rr) * ldf + n0 + lane] = sc * stg[(16 * h + rr) * PD_SROW + lane];
+          for (int rr = 0; rr < 16; ++rr) {
+            const int64_t o = UP ? __shfl_sync(0xffffffffu, orow, rr) : tq + 16 * h + rr;
+            F[o * ldf + n0 + lane] = sc * stg[(16 * h + rr) * PD_SROW + lane];
+          }
         } else {
-          for (int rr = 0; rr < 16; ++rr)
-            if (16 * h + rr < nrow) F[(tq + 16 * h + rr) * ldf + n0 + lane] = sc * stg[(16 * h + rr) * PD_SROW + lane];
+          for (int rr = 0; rr < 16; ++rr) {
+            const int64_t o = UP ? __shfl_sync(0xffffffffu, orow, rr) : tq + 16 * h + rr;
+            if (16 * h + rr < nrow) F[o * ldf + n0 + lane] = sc * stg[(16 * h + rr) * PD_SROW + lane];
+          }
         }
       }
       tc_fence_before();
@@ -1070,7 +971,7 @@ void tc_free_operators(void *p) {
 
 size_t tc_split_bytes(int r, int64_t ncell) { return (size_t)ncell * r * 2 * 2; }
 
-// Split, transposed copies of the projection operators for proj_tc_kernel.
+// Split, transposed copies of the projection operators for proj_fused_kernel.
 struct TcProj {
   int n3 = 0, r = 0, lead = 0;
   __nv_bfloat16 *up = nullptr;  // [hi | lo] of Bup^T: r x n3, rows j < lead zero
@@ -1089,7 +990,7 @@ static int map2d(CUtensorMap *m, const void *ptr, int64_t rows, int K, int box_r
 int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out,
                            cudaStream_t s) {
   *out = nullptr;
-  if (r != tc::BN || n3 % tc::BN || lead % 32 || lead <= 0 || lead >= r)
+  if (r != tc::BN || n3 % tc::BN || lead % 16 || lead <= 0 || lead >= r)
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core projections need n = 8 (r = 256)");
   if (!encode_fn()) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   TcProj *p = new TcProj();
@@ -1129,38 +1030,6 @@ void tc_free_projections(void *v) {
   delete p;
 }
 
-// Up (dir 0): M[cpg(row0 + t)][j] = sum_l S[t][l] Bup[l][j] for j >= lead, t < rows (S split in
-// Asplit = [hi | lo], rows x n3). Down (dir 1): F[t][l] += scale Kw[l] sum_{j >= lead} L'[t][j]
-// Bdn[j][l], t < rows, L' the split L rows in the order of F (Asplit, rows x r).
-int launch_proj_tc(const void *pv, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
-                   const double *cs, double scale, cudaStream_t s, int rank) {
-  const TcProj *p = (const TcProj *)pv;
-  if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
-  if (rows <= 0) return BBFMM_OK;
-  const int K = dir == 0 ? p->n3 : p->r;
-  const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Asplit;
-  const __nv_bfloat16 *lo = hi + (size_t)rows * K;
-  CUtensorMap ahi, alo;
-  int rc = map2d(&ahi, hi, rows, K, tc::BM);
-  if (rc == BBFMM_OK) rc = map2d(&alo, lo, rows, K, tc::BM);
-  if (rc != BBFMM_OK) return rc;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(tc::proj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
-    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "proj_tc smem attribute", __FILE__, __LINE__);
-    attr = true;
-  }
-  const dim3 grid((unsigned)((rows + tc::BM - 1) / tc::BM), dir == 0 ? 1 : p->n3 / tc::BN);
-  if (dir == 0)
-    tc::proj_tc_kernel<<<grid, 192, tc::SMEM_BYTES, s>>>(ahi, alo, p->up_hi, p->up_lo, C, p->r, rows, level, 1, row0,
-                                                         0, p->n3 / tc::BK, p->lead, 0, nullptr, 1.0);
-  else
-    tc::proj_tc_kernel<<<grid, 192, tc::SMEM_BYTES, s>>>(ahi, alo, p->dn_hi, p->dn_lo, C, p->n3, rows, level, 0, 0,
-                                                         p->lead / tc::BK, (rank > 0 ? rank : p->r) / tc::BK, 0, 1, cs,
-                                                         scale);
-  return bbfmm_set_cuda_error(cudaGetLastError(), "proj_tc", __FILE__, __LINE__);
-}
-
 // Down projection of `rows` Morton rows (row0 ..) of `level` in one pass: F[t][l] = scale Kw[l]
 // (sum_{j < 16} L[cpg(row0 + t)][j] Bdn[j][l] in FP64 + sum_{16 <= j < rank} L'[t][j] Bdn[j][l]
 // from the split rows L' = Asplit, whose components j < 16 are zero), F rows n3 apart, assigned.
@@ -1178,16 +1047,46 @@ int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int6
   if (rc != BBFMM_OK) return rc;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(tc::proj_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::PD_SMEM);
-    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "proj_down smem attribute", __FILE__, __LINE__);
+    cudaError_t e = cudaFuncSetAttribute(tc::proj_fused_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tc::PD_SMEM);
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "proj_fused smem attribute", __FILE__, __LINE__);
     attr = true;
   }
   const int64_t ntiles = ((rows + tc::BM - 1) / tc::BM) * (p->n3 / tc::BN);
   const int grid = (int)(ntiles < 148 ? ntiles : 148);
-  tc::proj_down_kernel<<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3,
-                                                      rows, level, row0, 0, (rank > 0 ? rank : p->r) / tc::BK, cs,
-                                                      scale, ntiles);
+  tc::proj_fused_kernel<false><<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(
+      ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3, rows, level, row0, 0,
+      (rank > 0 ? rank : p->r) / tc::BK, cs, scale, ntiles, 0);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_down", __FILE__, __LINE__);
+}
+
+// Up projection of `rows` Morton rows (row0 ..) of `level`: M[cpg(row0 + t)][j] = sum_l S'[t][l]
+// Bup[l][j] from the split S rows (Asplit, rows x n3), assigned for every j; the split operator
+// is zero for j < lead, whose FP64 values proj_narrow_kernel writes afterwards.
+int launch_proj_up(const void *pv, const void *Asplit, int64_t rows, double *M, int level, int64_t row0,
+                   cudaStream_t s) {
+  const TcProj *p = (const TcProj *)pv;
+  if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
+  if (rows <= 0) return BBFMM_OK;
+  const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Asplit;
+  const __nv_bfloat16 *lo = hi + (size_t)rows * p->n3;
+  CUtensorMap ahi, alo;
+  int rc = map2d(&ahi, hi, rows, p->n3, tc::BM);
+  if (rc == BBFMM_OK) rc = map2d(&alo, lo, rows, p->n3, tc::BM);
+  if (rc != BBFMM_OK) return rc;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc::proj_fused_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tc::PD_SMEM);
+    if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "proj_fused smem attribute", __FILE__, __LINE__);
+    attr = true;
+  }
+  const int64_t ntiles = (rows + tc::BM - 1) / tc::BM;
+  const int grid = (int)(ntiles < 148 ? ntiles : 148);
+  tc::proj_fused_kernel<true><<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(
+      ahi, alo, p->up_hi, p->up_lo, nullptr, 0, nullptr, M, p->r, rows, level, row0, 0, p->n3 / tc::BK, nullptr, 1.0,
+      ntiles, 0);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "proj_up", __FILE__, __LINE__);
 }
 
 // [hi | lo] split of rows x K FP64 values; gather != 0 reads row t from the cpg row of Morton

@@ -122,10 +122,10 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
 }
 
 // Narrow form for the FP64 leading columns of the mixed-mode up projection:
-// C[out(m)][0:32] = sum_k A[m][k] B[k][0:32], CTA tile 128 rows x 32 columns, 8 warps of
+// C[out(m)][0:16] = sum_k A[m][k] B[k][0:16], CTA tile 128 rows x 16 columns, 8 warps of
 // 16 rows, K-chunks of 16 double-buffered with cp.async; rows of C ldc apart.
 namespace nw {
-constexpr int BM = 128, BN = 32, BK = 16, AST = BK + 4, BST = BN + 8;
+constexpr int BM = 128, BN = 16, BK = 16, AST = BK + 4, BST = BN + 8;
 constexpr int STAGE = BM * AST + BK * BST;
 constexpr int SMEM_BYTES = 2 * STAGE * 8;
 }  // namespace nw
@@ -148,17 +148,18 @@ __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, cons
       const int64_t ar = m < M ? remap(m, row0, level, mapmode == MAP_IN_CPG) : -1;
       cp_async16(sa + (uint32_t)(row * nw::AST + k2) * 8u, ar >= 0 ? A + ar * K + k0 + k2 : A, ar >= 0);
     }
-    for (int e = tid; e < nw::BK * (nw::BN / 2); e += 256) {  // 16 rows x 16 pairs
+    for (int e = tid; e < nw::BK * (nw::BN / 2); e += 256) {  // 16 rows x 8 pairs
       const int k = e / (nw::BN / 2), n2 = (e % (nw::BN / 2)) * 2;
       cp_async16(sb + (uint32_t)(k * nw::BST + n2) * 8u, B + (int64_t)(k0 + k) * nw::BN + n2, true);
     }
     cp_commit();
   };
-  double acc[2][4][2];
+  constexpr int NF = nw::BN / 8;
+  double acc[2][NF][2];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int b = 0; b < NF; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   issue(0, 0);
   for (int kc = 0; kc < nk; ++kc) {
     const int buf = kc & 1;
@@ -174,15 +175,15 @@ __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, cons
 #pragma unroll
     for (int ks = 0; ks < nw::BK / 4; ++ks) {
       const int k = ks * 4 + c4;
-      double af[2], bf[4];
+      double af[2], bf[NF];
 #pragma unroll
       for (int mf = 0; mf < 2; ++mf) af[mf] = As[(warp * 16 + mf * 8 + r8) * nw::AST + k];
 #pragma unroll
-      for (int nf = 0; nf < 4; ++nf) bf[nf] = Bs[k * nw::BST + nf * 8 + r8];
+      for (int nf = 0; nf < NF; ++nf) bf[nf] = Bs[k * nw::BST + nf * 8 + r8];
 #pragma unroll
       for (int mf = 0; mf < 2; ++mf)
 #pragma unroll
-        for (int nf = 0; nf < 4; ++nf) dmma(acc[mf][nf][0], acc[mf][nf][1], af[mf], bf[nf]);
+        for (int nf = 0; nf < NF; ++nf) dmma(acc[mf][nf][0], acc[mf][nf][1], af[mf], bf[nf]);
     }
     __syncthreads();
   }
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, cons
     if (m >= M) continue;
     double *dst = C + remap(m, row0, level, mapmode == MAP_OUT_CPG) * ldc;
 #pragma unroll
-    for (int nf = 0; nf < 4; ++nf)
+    for (int nf = 0; nf < NF; ++nf)
       *reinterpret_cast<double2 *>(dst + nf * 8 + 2 * c4) = make_double2(acc[mf][nf][0], acc[mf][nf][1]);
   }
 }
@@ -203,7 +204,7 @@ int launch_proj_narrow(int64_t M, int K, const double *A, const double *B, doubl
                        int mapmode, cudaStream_t s, int64_t row0) {
   if (K % pj::nw::BK) return bbfmm_set_error(BBFMM_ERR_ARG, "narrow projection: K must be a multiple of 16");
   if (M <= 0) return BBFMM_OK;
-  static bool attr = false;  // 50 KB of dynamic shared memory
+  static bool attr = false;  // 47 KB of dynamic shared memory
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(pj::proj_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          pj::nw::SMEM_BYTES);

@@ -135,11 +135,11 @@ int Solver<T>::set_operators(const T *U, const T *E) {
     BBFMM_CUDA_OK(cudaMemcpy(Bdn, bdn.data(), sizeof(T) * bdn.size(), cudaMemcpyHostToDevice));
     BBFMM_CUDA_OK(cudaDeviceSynchronize());
     if (mode == MODE_MIXED && r == 256 && sizeof(T) == 8) {
-      std::vector<T> b32((size_t)n3 * PROJ_LEAD);
+      std::vector<T> blead((size_t)n3 * PROJ_LEAD);
       for (int l = 0; l < n3; ++l)
-        for (int i = 0; i < PROJ_LEAD; ++i) b32[(size_t)l * PROJ_LEAD + i] = bup[(size_t)l * r + i];
-      if (!Bup32) TRY(dalloc(&Bup32, b32.size()));
-      BBFMM_CUDA_OK(cudaMemcpy(Bup32, b32.data(), sizeof(T) * b32.size(), cudaMemcpyHostToDevice));
+        for (int i = 0; i < PROJ_LEAD; ++i) blead[(size_t)l * PROJ_LEAD + i] = bup[(size_t)l * r + i];
+      if (!Bup_lead) TRY(dalloc(&Bup_lead, blead.size()));
+      BBFMM_CUDA_OK(cudaMemcpy(Bup_lead, blead.data(), sizeof(T) * blead.size(), cudaMemcpyHostToDevice));
       if (tcproj) tc_free_projections(tcproj);
       tcproj = nullptr;
       TRY(tc_prepare_projections(n3, r, (const double *)Bup, (const double *)Bdn, PROJ_LEAD, &tcproj, stream));
@@ -175,7 +175,7 @@ int Solver<T>::share_operators(const Solver<T> &o) {
     return bbfmm_set_error(BBFMM_ERR_ARG, "operators can only be shared between solvers of the same n and mode");
   if (!o.Ert || !o.kw) return bbfmm_set_error(BBFMM_ERR_STATE, "the sharing solver has no operators");
   if (own_ops) {
-    void *mine[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, Bup32};
+    void *mine[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, Bup_lead};
     for (void *p : mine)
       if (p) cudaFree(p);
     if (tcops) tc_free_operators(tcops);
@@ -184,7 +184,7 @@ int Solver<T>::share_operators(const Solver<T> &o) {
   tkz = o.tkz; cw = o.cw; kw = o.kw; Ert = o.Ert; Ecol = o.Ecol; Bup = o.Bup; Bdn = o.Bdn; kwcol = o.kwcol;
   tcops = o.tcops;
   tcproj = o.tcproj;
-  Bup32 = o.Bup32;
+  Bup_lead = o.Bup_lead;
   own_ops = false;
   return BBFMM_OK;
 }
@@ -399,15 +399,17 @@ int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0) {
   T *Mdst = Mall + Moff[level];
   if (!proj_tc() || rows > Ssplit_rows)
     return proj(rows, n3, r, S_rows, Bup, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, row0);
-  TRY(launch_proj_narrow(rows, n3, (const double *)S_rows, (const double *)Bup32, (double *)Mdst, r, level,
-                         MAP_OUT_CPG, stream, row0));
+  // the tensor cores write all r columns (zero for j < PROJ_LEAD: those operator rows are
+  // zero in the split copy), then the FP64 pass overwrites the leading columns
   TRY(tc_split_rows(rows, n3, (const double *)S_rows, 0, level, row0, Ssplit, stream));
-  return launch_proj_tc(tcproj, 0, Ssplit, rows, (double *)Mdst, level, row0, nullptr, 1.0, stream);
+  TRY(launch_proj_up(tcproj, Ssplit, rows, (double *)Mdst, level, row0, stream));
+  return launch_proj_narrow(rows, n3, (const double *)S_rows, (const double *)Bup_lead, (double *)Mdst, r, level,
+                            MAP_OUT_CPG, stream, row0);
 }
 
 // Down projection of the level's M2L output (Lbuf, cpg) into `rows` F rows (Morton cells
-// row0 .., assign). Mixed mode: the contraction over j < PROJ_LEAD in FP64 (assign), then the
-// tensor cores add the rest, from L rows gathered into Morton order as split BF16.
+// row0 .., assign). Mixed mode: one pass, the contraction over j < 16 in FP64 and the rest on
+// the tensor cores from L rows gathered into Morton order as split BF16.
 template <typename T>
 int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows) {
   const T scale = (T)1 / cell_length<T>(level, (T)L);
@@ -718,7 +720,7 @@ void Solver<T>::release() {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (own_ops) {
-    void *ops[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, Bup32};
+    void *ops[] = {tkz, cw, kw, Ert, Ecol, Bup, Bdn, kwcol, Bup_lead};
     for (void *p : ops)
       if (p) cudaFree(p);
     if (tcops) tc_free_operators(tcops);

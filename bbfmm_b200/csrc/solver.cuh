@@ -88,8 +88,7 @@ int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, 
 void tc_free_projections(void *p);
 int launch_proj_down(const void *p, const void *Asplit, const double *Lfp, int64_t rows, double *F, int level,
                      int64_t row0, const double *cs, double scale, cudaStream_t s, int rank = 0);
-int launch_proj_tc(const void *p, int dir, const void *Asplit, int64_t rows, double *C, int level, int64_t row0,
-                   const double *cs, double scale, cudaStream_t s, int rank = 0);
+int launch_proj_up(const void *p, const void *Asplit, int64_t rows, double *M, int level, int64_t row0, cudaStream_t s);
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
                   cudaStream_t s, int zlead = 0);
 constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
@@ -132,10 +131,10 @@ struct Solver {
   void *tcops = nullptr;  // mixed mode: split operators for the tensor-core kernel
   // mixed mode, n = 8: projections with the leading PROJ_LEAD components in FP64 and the rest
   // as split-BF16 tensor-core products (tcproj: split, transposed U operators)
-  static constexpr int PROJ_LEAD = 32;
+  static constexpr int PROJ_LEAD = 16;
   bool mixed_proj = true;
   void *tcproj = nullptr;
-  T *Bup32 = nullptr;  // [n3][PROJ_LEAD] leading columns of Bup
+  T *Bup_lead = nullptr;  // [n3][PROJ_LEAD] leading columns of Bup
   void *Ssplit = nullptr, *Lsplit = nullptr;  // bf16 [hi | lo] copies of S rows / L rows
   int64_t Ssplit_rows = 0, Lsplit_rows = 0;
   // particles (sorted by leaf, Morton leaf order)
