@@ -9,6 +9,8 @@
 //   L2L  anotherDownwardPassX.c:40-211  x, then y, then z interpolation, accumulated
 //   L2P  anotherDownwardPassX.c:226-331  phi_p = q_p (2/n)^3 sum F Sx Sy Sz
 // The summation order of each output follows the reference loops.
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace bbfmm {
@@ -48,11 +50,13 @@ template <> __device__ __forceinline__ const float *tab_cw<float>(const Tables &
 
 // ----------------------------------------------------------------------------- P2M
 // One warp per leaf (grid-stride). pos4 = (x, y, z, q) in leaf-sorted order.
-// S_leaf[m * n3 + l], Morton order at maxlev.
+// S_leaf[m * n3 + l], Morton order at maxlev. With Ssplit (mixed mode) the kernel also writes
+// the [hi | lo] BF16 split of the same rows (hi plane count x n3, then the lo plane), as
+// split_rows_kernel would from S, for the tensor-core up projection.
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   int maxlev, T L, Tables tabs, T *__restrict__ S, int64_t m0,
-                                                  int64_t count) {
+                                                  int64_t count, __nv_bfloat16 *__restrict__ Ssplit) {
   constexpr int N3 = NN * NN * NN;
   constexpr int PER = (N3 + 31) / 32;
   __shared__ T s_tkz[NN * NN];
@@ -94,6 +98,16 @@ __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, co
     T *out = S + mm * N3;
 #pragma unroll
     for (int k = 0; k < PER; ++k) out[lane + 32 * k] = pre3 * acc[k];
+    if (Ssplit) {
+      __nv_bfloat16 *hi = Ssplit + mm * N3, *lo = Ssplit + (count + mm) * N3;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const double x = (double)(pre3 * acc[k]);
+        const __nv_bfloat16 h = __double2bfloat16(x);
+        hi[lane + 32 * k] = h;
+        lo[lane + 32 * k] = __double2bfloat16(x - (double)__bfloat162float(h));
+      }
+    }
   }
 }
 
@@ -441,12 +455,13 @@ static int grid_for(int64_t work, int per_block, int cap) {
 
 template <typename T>
 int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s,
-               int nsets, int64_t first, int64_t count) {
+               int nsets, int64_t first, int64_t count, void *Ssplit) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
   const int grid = grid_for(count, 4, 148 * 64);
-  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count);
-  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count);
+  __nv_bfloat16 *sp = (__nv_bfloat16 *)Ssplit;
+  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count, sp);
+  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count, sp);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2m", __FILE__, __LINE__);
 }
@@ -539,7 +554,7 @@ int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaS
 
 #define INST(T)                                                                                           \
   template int launch_p2m<T>(int, const T *, const int *, int, T, const Tables &, T *, cudaStream_t, int,   \
-                             int64_t, int64_t);                                                            \
+                             int64_t, int64_t, void *);                                                    \
   template int launch_m2m<T>(int, const T *, T *, int, const Tables &, cudaStream_t, int, int64_t, int64_t); \
   template int launch_l2l<T>(int, const T *, T *, int, const Tables &, cudaStream_t, int, int64_t, int64_t); \
   template int launch_l2p<T>(int, const T *, const int *, int, T, const Tables &, const T *, T *,          \

@@ -346,9 +346,11 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
   const int64_t nl = cells(maxlev), sl = leaf_slab();
   for (int64_t a = 0; a < nl; a += sl) {
     const int64_t c = nl - a < sl ? nl - a : sl;
-    TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream, nsets, a, c));
+    // mixed mode: P2M also writes the BF16 split of S that the tensor-core up projection reads
+    void *sp = proj_tc() && c <= Ssplit_rows ? Ssplit : nullptr;
+    TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream, nsets, a, c, sp));
     mark(ST_P2M);
-    TRY(proj_up(c, Sl, maxlev, a));
+    TRY(proj_up(c, Sl, maxlev, a, sp != nullptr));
     mark(ST_PROJ_UP);
     if (maxlev - 1 >= BBFMM_MINLEV) {
       TRY(launch_m2m<T>(n, Sl, S[(maxlev - 1) & 1], maxlev - 1, tb, stream, nsets, a / 8, c / 8));
@@ -395,13 +397,13 @@ int Solver<T>::proj(int64_t Mrows, int K, int Ncols, const T *A, const T *B, con
 // Up projection of `rows` S rows (Morton cells row0 .. of `level`) into the level's M (cpg).
 // Mixed mode: components j < PROJ_LEAD in FP64, the rest as split-BF16 tensor-core products.
 template <typename T>
-int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0) {
+int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit) {
   T *Mdst = Mall + Moff[level];
   if (!proj_tc() || rows > Ssplit_rows)
     return proj(rows, n3, r, S_rows, Bup, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, row0);
   // the tensor cores write all r columns (zero for j < PROJ_LEAD: those operator rows are
   // zero in the split copy), then the FP64 pass overwrites the leading columns
-  TRY(tc_split_rows(rows, n3, (const double *)S_rows, 0, level, row0, Ssplit, stream));
+  if (!presplit) TRY(tc_split_rows(rows, n3, (const double *)S_rows, 0, level, row0, Ssplit, stream));
   TRY(launch_proj_up(tcproj, Ssplit, rows, (double *)Mdst, level, row0, stream));
   return launch_proj_narrow(rows, n3, (const double *)S_rows, (const double *)Bup_lead, (double *)Mdst, r, level,
                             MAP_OUT_CPG, stream, row0);

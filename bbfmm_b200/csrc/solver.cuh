@@ -25,7 +25,7 @@ enum Stage {
 // first, count: a range of cells (P2M, L2P: leaves; M2M, L2L: parents) whose per-cell n^3
 // arrays (S of P2M, F of L2P; the children in M2M and L2L) start at the pointer given, so a
 // level can be processed in slabs; count < 0 means every cell from `first` on.
-template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, void *Ssplit = nullptr);
 template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
@@ -178,7 +178,7 @@ struct Solver {
   int alloc_partials();                          // Lpart for the current tuning
   int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
   bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
-  int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0);  // S rows -> Mall (cpg)
+  int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false);  // S rows -> Mall (cpg)
   int proj_down(int level, int64_t rows, int64_t row0, T *F_rows);    // Lbuf -> F rows (Morton, assign)
   // Times the launch choices of every level's M2L and of the near field on this solver's
   // own tree (after an upward pass with q_dev) and keeps the fastest; results are cached per
