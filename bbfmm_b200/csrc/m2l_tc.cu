@@ -317,6 +317,10 @@ __global__ void __launch_bounds__(192, 1)
 // component 4u + ks so that each fragment load is one contiguous 32-byte run of M or of
 // Erow[k][i][j] = E_k(i, j). The block is written to Lacc (assign) before the accumulator
 // wait, and the tensor-memory epilogue adds to it as it adds to a separately computed block.
+// With Lsplit (one whole level, mixed projections) the epilogue writes the FP64 output only
+// for i < 32 and, for every i < ncols, its [hi | lo] BF16 split into the Morton row of the
+// cell (planes of `nrows` rows of 256), components i < DNZ zero: the input of the fused down
+// projection, which otherwise gathers and splits the rows in a separate pass.
 constexpr int A2_BYTES = 2 * A_BYTES, BLO2_BYTES = TC_SPLIT_ROWS * BK * 2;
 constexpr int STAGE2_BYTES = 2 * A2_BYTES + B_BYTES + BLO2_BYTES;
 constexpr int SMEM2_BYTES = STAGES * STAGE2_BYTES + 1024 /*align*/ + 256 /*barriers*/;
@@ -327,8 +331,10 @@ __global__ void __launch_bounds__(192, 1)
     m2l_tc2_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                    const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                    double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
-                   int split_chunks, int ncols, const double *__restrict__ Mlead, const double *__restrict__ Erow) {
+                   int split_chunks, int ncols, const double *__restrict__ Mlead, const double *__restrict__ Erow,
+                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows) {
   constexpr int STAGE_BYTES = STAGE2_BYTES;
+  constexpr int DNZ = 16;  // components the fused down projection takes in FP64
   constexpr int split_rows = TC_SPLIT_ROWS;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -506,16 +512,36 @@ __global__ void __launch_bounds__(192, 1)
       const int64_t P3 = (int64_t)P * P * P;
       const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
       double *dst = Lacc + cell * BN;
+      int64_t mrow = 0;  // Morton row of the cell: set base + Morton index of its grid position
+      if (Lsplit)
+        mrow = (int64_t)(c >> 3) * 8 * P3 +
+               grid_to_morton(2 * (bx0 + tx) + cbx, 2 * (by0 + ty) + cby, 2 * (bz0 + tz) + cbz, level);
       for (int col = 0; col < ncols; col += 32) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 256 + col), v);
         const bool add = col < ilead;  // ilead is a multiple of 32
+        const bool fp = !Lsplit || col < 32;
+        __align__(16) __nv_bfloat16 sh[32], sl[32];
 #pragma unroll
         for (int i = 0; i < 32; i += 2) {
           double2 o = add ? *reinterpret_cast<const double2 *>(dst + col + i) : make_double2(0.0, 0.0);
           o.x += (double)v[i];
           o.y += (double)v[i + 1];
-          *reinterpret_cast<double2 *>(dst + col + i) = o;
+          if (fp) *reinterpret_cast<double2 *>(dst + col + i) = o;
+          const double x0 = col + i < DNZ ? 0.0 : o.x, x1 = col + i + 1 < DNZ ? 0.0 : o.y;
+          sh[i] = __double2bfloat16(x0);
+          sl[i] = __double2bfloat16(x0 - (double)__bfloat162float(sh[i]));
+          sh[i + 1] = __double2bfloat16(x1);
+          sl[i + 1] = __double2bfloat16(x1 - (double)__bfloat162float(sh[i + 1]));
+        }
+        if (Lsplit) {
+          uint4 *oh = reinterpret_cast<uint4 *>(Lsplit + mrow * BN + col);
+          uint4 *ol = reinterpret_cast<uint4 *>(Lsplit + (nrows + mrow) * BN + col);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            oh[e] = reinterpret_cast<const uint4 *>(sh)[e];
+            ol[e] = reinterpret_cast<const uint4 *>(sl)[e];
+          }
         }
       }
     }
@@ -1119,7 +1145,7 @@ bool tc_fuses_lead(const void *opsv, int nprod, int rank) {
 
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets, int nprod, int rank, const double *Mlead,
-                  const double *Erow) {
+                  const double *Erow, void *Lsplit) {
   const TcOps *ops = (const TcOps *)opsv;
   if (nprod != 0 && nprod != 1 && nprod != 3)
     return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 0 (adaptive), 1 or 3");
@@ -1176,9 +1202,10 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     }
     const int tiles2 = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX2_Y) * (P / tc::BOX_Z);
     const bool fuse = Mlead && Erow && tc_fuses_lead(ops, nprod, rank) && kfirst == 0 && ilead == 32;
-    tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs,
-                                                            kfirst, ilead, split_chunks, rank,
-                                                            fuse ? Mlead : nullptr, fuse ? Erow : nullptr);
+    if (Lsplit && !fuse) return bbfmm_set_error(BBFMM_ERR_ARG, "split M2L output needs the fused leading block");
+    tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(
+        mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst, ilead, split_chunks, rank, fuse ? Mlead : nullptr,
+        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
   }
   static bool attr = false;

@@ -413,12 +413,12 @@ int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, b
 // row0 .., assign). Mixed mode: one pass, the contraction over j < 16 in FP64 and the rest on
 // the tensor cores from L rows gathered into Morton order as split BF16.
 template <typename T>
-int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows) {
+int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit) {
   const T scale = (T)1 / cell_length<T>(level, (T)L);
   if (!proj_tc() || rows > Lsplit_rows)  // contraction over the effective rank (j < rk())
     return proj(rows, rk(), n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0, r);
   // components j < 16 in FP64 and the rest as split-BF16 tensor-core products, one pass
-  TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream, 16));
+  if (!presplit) TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream, 16));
   return launch_proj_down(tcproj, Lsplit, (const double *)Lbuf, rows, (double *)F_rows, level, row0,
                           (const double *)kw, (double)scale, stream, rk());
 }
@@ -465,14 +465,18 @@ template <typename T>
 int Solver<T>::m2l_post(int l) {
   {
     const T *Ml = Mall + Moff[l];
+    bool presplit = false;  // the M2L kernel wrote the split rows of the down projection
     const bool split = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
     if (split) {
       // FP64 leading block (i < lead_rows, j < lead) on the FP64 tensor path, then the
       // split-bf16 tensor-core kernel adds everything else into the same FP64 output; the
       // two-box kernel computes the block itself in its otherwise idle epilogue warps
       if (lead > 0 && tc_fuses_lead(tcops, tc_products, rk())) {
+        // whole level with mixed projections: the kernel also writes the split rows that the
+        // down projection reads (and the FP64 output only where that pass reads it)
+        presplit = proj_tc() && cells(l) <= Lsplit_rows && !(l == maxlev && slabbed());
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
-                          tc_products, rk(), (const double *)Ml, (const double *)Ert));
+                          tc_products, rk(), (const double *)Ml, (const double *)Ert, presplit ? Lsplit : nullptr));
         mark(ST_M2L, 1);
       } else if (lead > 0) {
         TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
@@ -491,7 +495,7 @@ int Solver<T>::m2l_post(int l) {
       mark(ST_M2L, g > 1 ? 2 : 1);  // groups add the partial sum
     }
     if (!(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
-      TRY(proj_down(l, cells(l), 0, F[l & 1]));
+      TRY(proj_down(l, cells(l), 0, F[l & 1], presplit));
       mark(ST_PROJ_DOWN);
     }
   }

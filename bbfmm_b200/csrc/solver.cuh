@@ -78,7 +78,7 @@ constexpr int TC_SPLIT_CHUNKS = 2, TC_SPLIT_ROWS = 64;
 // rank: the effective rank (outputs i and components j below it; 0 = r).
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0,
-                  const double *Mlead = nullptr, const double *Erow = nullptr);
+                  const double *Mlead = nullptr, const double *Erow = nullptr, void *Lsplit = nullptr);
 bool tc_fuses_lead(const void *ops, int nprod, int rank);
 int tc_status(int clear);
 int tc_wait_probe(unsigned limit, int code);
@@ -179,7 +179,7 @@ struct Solver {
   int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
   bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
   int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false);  // S rows -> Mall (cpg)
-  int proj_down(int level, int64_t rows, int64_t row0, T *F_rows);    // Lbuf -> F rows (Morton, assign)
+  int proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit = false);    // Lbuf -> F rows (Morton, assign)
   // Times the launch choices of every level's M2L and of the near field on this solver's
   // own tree (after an upward pass with q_dev) and keeps the fastest; results are cached per
   // (mode, n, level, target tiles) and (mode, particles, leaves) for later solvers.
