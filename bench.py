@@ -35,7 +35,7 @@ METRIC = "FMM solves/s at N=4,194,304, n=8, depth 7 (1 GPU; err <= 1.2x FP64 req
 # DRAM bytes of one m2l_tc2_kernel launch per cell of its level, from an ncu capture of the
 # level-5 launch (32,768 cells: 82.9 MB read + 14.5 MB written); the traffic scales with
 # the number of cells (multipole split in, FP64 M2L output read-modify-written).
-TC_DRAM_BYTES_PER_CELL = (77.903872e6 + 14.111232e6) / 32768
+TC_DRAM_BYTES_PER_CELL = (77.765632e6 + 4.091136e6) / 32768
 
 
 def interactions_per_level(level: int) -> int:
