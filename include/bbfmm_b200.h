@@ -51,9 +51,12 @@ extern "C" {
  *  D      FP64 storage and arithmetic in every stage (the reference's double build).
  *  S      FP32 storage and arithmetic in every stage (the reference's SINGLE build).
  *  MIXED  FP64 passes; M2L with the leading block of every operator (outputs i < lead_rows,
- *         contraction components j < lead) in FP64 and everything else as three-term split
- *         BF16 products on tcgen05 tensor cores accumulated in FP32; P2P in FP32 on
- *         leaf-local coordinates with compensated sums. */
+ *         contraction components j < lead) in FP64 and everything else as split-BF16
+ *         products on tcgen05 tensor cores accumulated in FP32 (three products for the
+ *         leading 64 x 64 block, one elsewhere; bbfmm_b200_set_tc_products); U-projections
+ *         with their 16 leading components in FP64 and the rest as split-BF16 products;
+ *         P2P with FP64 pair separations, FP32 reciprocal distances and compensated FP32
+ *         sums added to FP64 potentials. */
 #define BBFMM_B200_MODE_D 0
 #define BBFMM_B200_MODE_S 1
 #define BBFMM_B200_MODE_MIXED 2
