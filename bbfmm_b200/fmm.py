@@ -38,7 +38,8 @@ class Solver:
 
     mode: "d" (FP64 everywhere), "s" (FP32 everywhere), "mixed" (FP64 passes,
     split-precision tensor-core M2L whose leading operator block -- outputs i < ``lead_rows``,
-    components j < ``lead`` -- runs in FP64, FP32 compensated P2P)."""
+    components j < ``lead`` -- runs in FP64, split-precision tensor-core projections with 16
+    FP64 components, P2P with FP64 separations and compensated FP32 sums)."""
 
     def __init__(self, n: int, maxlev: int, L: float = 1.0, mode: str = "d", lead: int = 16,
                  lead_rows: int = 32, device: int = 0, operators=None, stream=None, rank: int | None = None,
