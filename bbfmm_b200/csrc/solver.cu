@@ -378,7 +378,10 @@ int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
   if (sizeof(T) == 8 && r == 256)
     return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
                            (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level]);
-  if (ni != r) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
+  // the SIMT kernel writes all r outputs; in the rank mode (ni = rk()) the outputs i >= rank
+  // of the zero-padded operators come out as zeros, so only other partial ranges are refused
+  if (ni != r && ni != rk())
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
   const int g = tune.m2l_groups[level] > 0 ? tune.m2l_groups[level] : dmma_default_groups(level, nsets);
   return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets, g, Lpart, Lpart_elems);
 }

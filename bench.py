@@ -256,6 +256,61 @@ def run_uniform_32k(args):
     return 0
 
 
+def run_uniform_4m_variants(args):
+    """The other precision/order forms of the 4M-particle uniform workload (N = 4,194,304,
+    maxlev 7, seeded like the headline line): n in {4, 8} x modes d / s / mixed, and the FP32
+    tolerance-rank form (SVD cut at 1e-5), each timed over `steps` device-resident solves and
+    checked against the FP64 direct sum on the headline's 4,096 seeded targets; the
+    reference CPU code for n = 4 on a bounded sample beside them."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.fmm import direct
+    N, lev = args.N, args.maxlev
+    x, q = make_inputs(N, 2)
+    targets = np.random.default_rng(1234).choice(N, N_TARGETS, replace=False).astype(np.int32)
+    dref = direct(torch.as_tensor(x, device="cuda"), torch.as_tensor(q, device="cuda"),
+                  torch.as_tensor(targets, device="cuda")).cpu().numpy()
+    forms = [(4, "d", None), (4, "s", None), (4, "mixed", None), (8, "d", None), (8, "s", None),
+             (8, "mixed", None), (8, "s", 1e-5)]
+    out = []
+    for n, mode, tol in forms:
+        sol = Solver(n, lev, 1.0, mode=mode, tol=tol)
+        sol.set_particles(x)
+        dt = torch.float32 if mode == "s" else torch.float64
+        qd = torch.as_tensor(q, dtype=dt, device="cuda")
+        ph = torch.empty_like(qd)
+        stream = torch.cuda.ExternalStream(sol.stream)
+        steps = args.steps if n == 4 or mode == "mixed" else min(args.steps, 2)
+        sol.solve(qd, out=ph)
+        t = _device_time(lambda: sol.solve(qd, out=ph), steps, stream)
+        a = ph.double().cpu().numpy()[targets]
+        err = float(np.sqrt(((a - dref) ** 2).sum() / (dref ** 2).sum()))
+        out.append({"n": n, "mode": mode, "tol": tol, "rank": sol.rank if tol else n ** 3 // 2,
+                    "s_per_solve": t, "steps": steps, "err_vs_fp64_direct": err})
+        sol.close()
+        del sol
+        torch.cuda.empty_cache()
+    base = {(o["n"], o["mode"]): o for o in out if o["tol"] is None}
+    for o in out:
+        d = base.get((o["n"], "d"))
+        o["speedup_vs_fp64_gpu"] = d["s_per_solve"] / o["s_per_solve"] if d else None
+        o["err_ratio_vs_fp64_gpu"] = o["err_vs_fp64_direct"] / d["err_vs_fp64_direct"] if d else None
+    t_ref, cores, kind = (reference_sample(65536, 5, n=4) if not args.no_cpu_baseline else (None, 0, None))
+    head = base[(4, "mixed")]
+    line = {"metric": "FMM solves/s at N=4,194,304 uniform, depth 7: n = 4 / 8, FP64 / FP32 / mixed",
+            "value": 1.0 / head["s_per_solve"], "unit": "solve/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": head["s_per_solve"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform [0,1)^3, q~U[-1,1])",
+            "config": {"workload": "bbFMM Laplace 1/r, N=4,194,304 uniform, maxlev 7, order and precision forms",
+                       "N": N, "maxlev": lev, "headline_form": "n=4 mixed"},
+            "forms": out,
+            "cpu_baseline": None if t_ref is None else {
+                "value": 1.0 / (t_ref * N / 65536), "unit": "solve/s", "cores": cores, "kind": kind,
+                "sample": "one CPU solve of N=65536, n=4, maxlev 5 (2 particles/leaf), scaled by N"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def _gradient_case(mode, x, q, w, args):
     """Forward and forward + backward of L = sum_i w_i phi_i in one precision mode: timings,
     bytes kept for the backward, and the gradients (of the last save mode)."""
@@ -602,11 +657,14 @@ def main():
     ap.add_argument("--N", type=int, default=N_FULL)
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
     ap.add_argument("--workload", default="uniform-4m",
-                    choices=["uniform-4m", "uniform-32k", "gradient-1m", "batch-256", "clustered-16m"],
+                    choices=["uniform-4m", "uniform-4m-variants", "uniform-32k", "gradient-1m", "batch-256",
+                             "clustered-16m"],
                     help="uniform-4m: the headline line; the others measure further configurations")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "uniform-4m-variants":
+        return run_uniform_4m_variants(args)
     if args.workload == "uniform-32k":
         return run_uniform_32k(args)
     if args.workload == "gradient-1m":

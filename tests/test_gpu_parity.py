@@ -201,3 +201,24 @@ def test_tolerance_rank_mixed_matches_fp64_rank():
         out[mode] = s.solve(qd).cpu().numpy()
         s.close()
     assert rel_l2(out["mixed"], out["d"]) < 3e-7
+
+
+def test_tolerance_rank_fp32_matches_fp64_rank():
+    """FP32 mode with an SVD cut at 1e-5 (the FP32 tolerance of the 4M-particle workload): the
+    CUDA-core M2L contracts over the rank and writes zeros above it; against the FP64 solve at
+    the same rank: 2e-5 (FP32 arithmetic throughout)."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200 import operators as ops
+    rank = ops.tolerance_rank(8, 1e-5)
+    assert rank < 256
+    x, q = uniform_inputs(20000, seed=16)
+    out = {}
+    for mode in ("s", "d"):
+        s = Solver(8, 3, 1.0, mode=mode, tol=1e-5)
+        assert s.rank == rank
+        s.set_particles(x)
+        dt = torch.float32 if mode == "s" else torch.float64
+        out[mode] = s.solve(torch.as_tensor(q, dtype=dt, device="cuda")).double().cpu().numpy()
+        s.close()
+    assert rel_l2(out["s"], out["d"]) < 2e-5
