@@ -25,13 +25,15 @@ struct OffsetTable {
   const int4 *offs;
 };
 
+// TM x TN outputs per thread; the CTA has (64 / TM) (R / TN) threads (256 at r = 256 with an
+// 8 x 8 tile, 128 at r = 32 with a 4 x 4 tile: 8 shared-memory loads per 16 FMAs).
 template <typename T, int R, int TM, int TN>
-__global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, const T *__restrict__ Ert,
+__global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T *__restrict__ M, const T *__restrict__ Ert,
                                                        T *__restrict__ Lout, int level, int j0, int j1,
                                                        const int4 *__restrict__ offs, int accumulate) {
   constexpr int BK = 16;
   constexpr int NT = 64;  // targets per tile (4x4x4 box)
-  static_assert((NT / TM) * (R / TN) == 256, "thread tile must cover the CTA tile");
+  constexpr int THREADS = (NT / TM) * (R / TN);
   constexpr int TGX = NT / TM;  // thread groups along targets
   __shared__ T sa[BK][NT];
   __shared__ T sb[BK][R + (sizeof(T) == 8 ? 1 : 0)];
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, 
     const int sc = (scx << 2) | (scy << 1) | scz;
     for (int jc = j0; jc < j1; jc += BK) {
       __syncthreads();
-      for (int e = tid; e < NT * BK; e += 256) {
+      for (int e = tid; e < NT * BK; e += THREADS) {
         const int t = e / BK, jj = e % BK;
         T v = 0;
         if (t < nt && jc + jj < j1) {
@@ -78,7 +80,7 @@ __global__ void __launch_bounds__(256) m2l_simt_kernel(const T *__restrict__ M, 
         sa[jj][t] = v;
       }
       const T *Ek = Ert + (int64_t)k * R * R;
-      for (int e = tid; e < R * BK; e += 256) {
+      for (int e = tid; e < R * BK; e += THREADS) {
         const int i = e / BK, jj = e % BK;
         sb[jj][i] = (jc + jj < j1) ? Ek[(int64_t)i * R + jc + jj] : (T)0;
       }
@@ -148,7 +150,7 @@ int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0,
   if (r == 256) {
     m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
   } else if (r == 32) {
-    m2l_simt_kernel<T, 32, 2, 4><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
+    m2l_simt_kernel<T, 32, 4, 4><<<grid, 128, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
   } else {
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L rank must be 32 or 256 (n = 4 or 8)");
   }
