@@ -36,6 +36,7 @@ UNITS = [
     ("solver.cu", [], "solver"),
     ("reference_abi.cu", [], "reference_abi"),
     ("batch.cu", [], "batch"),
+    ("tree.cu", [], "tree"),
 ]
 
 

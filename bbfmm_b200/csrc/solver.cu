@@ -312,6 +312,33 @@ int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const
   return BBFMM_OK;
 }
 
+// The same state as set_particles_sorted for one set, with the octree built on the device from
+// positions there (build_tree_device: the host sort's perm and leaf_start, bit for bit).
+template <typename T>
+int Solver<T>::set_particles_device(int N_, const T *xyz_d) {
+  if (N_ < 0 || (N_ > 0 && !xyz_d)) return bbfmm_set_error(BBFMM_ERR_ARG, "bad particle arguments");
+  nsets = 1;
+  const int64_t nl = cells(maxlev);
+  if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(leafm); cudaFree(pos4); cudaFree(phis); }
+  if (flds) cudaFree(flds);
+  if (io_q) cudaFree(io_q);
+  if (io_phi) cudaFree(io_phi);
+  io_q = io_phi = nullptr;
+  perm = leaf_start = leafm = nullptr; pos4 = phis = flds = nullptr;
+  N = N_;
+  TRY(dalloc(&perm, N > 0 ? N : 1));
+  TRY(dalloc(&leaf_start, nl + 1));
+  TRY(dalloc(&leafm, N > 0 ? N : 1));
+  TRY(dalloc(&pos4, 4 * (size_t)(N > 0 ? N : 1)));
+  TRY(dalloc(&phis, N > 0 ? N : 1));
+  TRY(build_tree_device<T>(N, xyz_d, (T)L, maxlev, perm, leaf_start, stream));
+  TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream, 1));
+  if (N > 0) TRY((launch_gather<T, T>(N, perm, xyz_d, nullptr, pos4, stream)));
+  TRY(alloc_work());
+  BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
+  return BBFMM_OK;
+}
+
 template <typename T>
 void Solver<T>::mark(int stage, int launches) {
   kernel_launches += launches;
@@ -817,6 +844,12 @@ int bbfmm_b200_set_particles(bbfmm_b200_solver *h, int N, const void *xyz) {
   int rc = bbfmm_sort_particles<double>(N, (const double *)xyz, s.L, s.maxlev, perm.data(), ls.data());
   if (rc != BBFMM_OK) return rc;
   return s.set_particles_sorted(N, perm.data(), ls.data(), (const double *)xyz);
+}
+
+int bbfmm_b200_set_particles_device(bbfmm_b200_solver *h, int N, const void *xyz_dev) {
+  if (!h || (N > 0 && !xyz_dev) || N < 0) return bbfmm_set_error(BBFMM_ERR_ARG, "bad particle arguments");
+  if (h->f) return h->f->set_particles_device(N, (const float *)xyz_dev);
+  return h->d->set_particles_device(N, (const double *)xyz_dev);
 }
 
 int bbfmm_b200_solve(bbfmm_b200_solver *h, const void *q_dev, void *phi_dev) {

@@ -25,6 +25,8 @@ enum Stage {
 // first, count: a range of cells (P2M, L2P: leaves; M2M, L2L: parents) whose per-cell n^3
 // arrays (S of P2M, F of L2P; the children in M2M and L2L) start at the pointer given, so a
 // level can be processed in slabs; count < 0 means every cell from `first` on.
+template <typename T>
+int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf_start, cudaStream_t s);
 template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, void *Ssplit = nullptr);
 template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
@@ -168,6 +170,8 @@ struct Solver {
   int init(int n_, int maxlev_, double L_, int mode_, int lead_, int lead_rows_, int device_, cudaStream_t s);
   int set_tables(const T *Tkz, const T *Cweights, const T *Kweights);  // host arrays
   int set_operators(const T *U, const T *E);                              // host, reference layout
+  // positions already on the device ([N][3], this solver's precision): the tree is built there
+  int set_particles_device(int N_, const T *xyz_dev);
   int set_particles_sorted(int N_, const int *perm_host, const int *leaf_start_host, const T *xyz_host);
   // N_ particles of nsets_ stacked sets: perm_host[k] indexes the caller's arrays of Nxyz
   // particles (positions xyz_host, and later q and phi); leaf_start_host has nsets_ 8^maxlev + 1

@@ -94,7 +94,15 @@ class Solver:
         return _lib.lib().bbfmm_b200_stream(self.h)
 
     def set_particles(self, xyz):
-        """Particle positions, N x 3 inside [-L/2, L/2]^3 (host array)."""
+        """Particle positions, N x 3 inside [-L/2, L/2]^3: a host array (the tree is built on
+        the host), or a CUDA tensor (the tree is built on the GPU; same particle order)."""
+        torch = self.torch
+        if isinstance(xyz, torch.Tensor) and xyz.is_cuda:
+            x = xyz.to(device=f"cuda:{self.device}", dtype=self.dtype).reshape(-1, 3).contiguous()
+            self.N = x.shape[0]
+            torch.cuda.synchronize(x.device)  # the solver's stream reads x
+            _lib.check(_lib.lib().bbfmm_b200_set_particles_device(self.h, self.N, C.c_void_p(x.data_ptr())))
+            return
         xyz = np.ascontiguousarray(np.asarray(xyz, dtype=self.np_dtype).reshape(-1, 3))
         self.N = xyz.shape[0]
         _lib.check(_lib.lib().bbfmm_b200_set_particles(self.h, self.N, _ptr(xyz)))

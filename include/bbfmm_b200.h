@@ -110,6 +110,11 @@ BBFMM_B200_API int bbfmm_b200_create(const bbfmm_b200_config *cfg, const void *U
 /* Positions (host, N x 3; FP32 in mode S, FP64 otherwise), inside [-L/2, L/2]^3. Builds
  * the leaf order on the host and keeps the sorted particles on the device. */
 BBFMM_B200_API int bbfmm_b200_set_particles(bbfmm_b200_solver *s, int N, const void *xyz);
+/* The same for positions already on the solver's device (xyz_dev: N x 3 in the solver's
+ * precision, float in mode S, double otherwise): the octree is built on the GPU (leaf
+ * assignment and a stable radix sort by Morton leaf), with the same particle order and leaf
+ * ranges as bbfmm_b200_set_particles (anotherFMMDistribute.c:258-298, 431-473). */
+BBFMM_B200_API int bbfmm_b200_set_particles_device(bbfmm_b200_solver *s, int N, const void *xyz_dev);
 
 /* One solve with device-resident charges and result (original particle order; FP32 in
  * mode S, FP64 otherwise): phi[i] = q_i * sum_{j != i} q_j / |x_i - x_j| (FMM-approximated).
