@@ -1,4 +1,5 @@
-"""Chebyshev tables and SVD-compressed M2L operators for the 1/r kernel (host, FP64).
+"""Chebyshev tables and SVD-compressed M2L operators (host, FP64) for the reference's
+homogeneous kernels: 1/r (LAPLACIAN, the default) and 1/r^4 (ONEOVERR4).
 
 This is set-up work, not the solve: it runs once per interpolation order ``n`` and
 its output is cached in the reference's operator-file format so that the same
@@ -30,6 +31,24 @@ from dataclasses import dataclass
 import numpy as np
 
 NUM_OFFSETS = 316  # |[-3,3]^3 \ [-1,1]^3|
+
+# The reference's compile-time kernels (bbfmm.c:109-144, 798-849): name -> (degree of
+# homogeneity, kernel id of the C-ABI). LAPLACIANFORCE (x / r^3, homogeneity 2) is not
+# provided: it is antisymmetric, so the E_k = U^T K_k U form used for the M2L does not hold.
+KERNELS = {"laplacian": (1, 0), "oneoverr4": (4, 2)}
+
+
+def homogeneity(kernel: str) -> int:
+    return KERNELS[kernel][0]
+
+
+def _kernel_values(kernel: str, r: np.ndarray) -> np.ndarray:
+    if kernel == "laplacian":
+        return 1.0 / r
+    if kernel == "oneoverr4":
+        rinv = 1.0 / r
+        return rinv * rinv * rinv * rinv
+    raise ValueError(f"unknown kernel {kernel!r} (laplacian or oneoverr4)")
 
 
 def ktable() -> np.ndarray:
@@ -110,12 +129,12 @@ def chebyshev_tables(n: int) -> ChebTables:
     return ChebTables(n, nodes, Tkz, Kweights, C.reshape(-1), ktable())
 
 
-def kernel_matrix(n: int) -> np.ndarray:
-    """K0 (n^3 x 316 n^3): weighted 1/r between unit-cell field nodes and the nodes of
+def kernel_matrix(n: int, kernel: str = "laplacian") -> np.ndarray:
+    """K0 (n^3 x 316 n^3): the weighted kernel between unit-cell field nodes and the nodes of
     the 316 well-separated unit cells, block k = columns [k n^3, (k+1) n^3).
 
-    Entry (i, k n^3 + j) = 1/|f_i - s_j| / (w_i w_j) with f at 0.5*nodes and s at
-    offset_k + 0.5*nodes (bbfmm.c:1247-1324)."""
+    Entry (i, k n^3 + j) = K(|f_i - s_j|) / (w_i w_j) with f at 0.5*nodes and s at
+    offset_k + 0.5*nodes (bbfmm.c:1247-1324), K = 1/r or 1/r^4."""
     tab = chebyshev_tables(n)
     h = 0.5 * tab.nodes
     g = np.stack(np.meshgrid(h, h, h, indexing="ij"), axis=-1).reshape(-1, 3)  # (n3, 3)
@@ -128,11 +147,11 @@ def kernel_matrix(n: int) -> np.ndarray:
         src = offs[k][None, :] + g                      # (n3, 3)
         d = g[:, None, :] - src[None, :, :]             # (n3 field, n3 source, 3)
         r = np.sqrt(np.einsum("fsx,fsx->fs", d, d))
-        K[:, k * n3:(k + 1) * n3] = 1.0 / r / ww
+        K[:, k * n3:(k + 1) * n3] = _kernel_values(kernel, r) / ww
     return K
 
 
-def kernel_svd(n: int, rank: int | None = None):
+def kernel_svd(n: int, rank: int | None = None, kernel: str = "laplacian"):
     """Returns (U, E, sigma): U column-major (n^3, r) flattened, E (316, r, r) as
     column-major blocks flattened, sigma all n^3 singular values.
 
@@ -141,7 +160,7 @@ def kernel_svd(n: int, rank: int | None = None):
     right factor reuses U, bbfmm.c:1384-1405)."""
     n3 = n ** 3
     r = n3 // 2 if rank is None else rank
-    K0 = kernel_matrix(n)
+    K0 = kernel_matrix(n, kernel)
     R = np.linalg.qr(K0.T, mode="r")          # (n3, n3), K0 = R^T Q^T
     Ul, s, _ = np.linalg.svd(R.T)
     U = np.ascontiguousarray(Ul[:, :r])       # (n3, r)
@@ -155,15 +174,20 @@ def kernel_svd(n: int, rank: int | None = None):
     return Ucol, Ecol, s
 
 
-def operator_file_names(n: int, single: bool) -> tuple[str, str]:
+def operator_file_names(n: int, single: bool, kernel: str = "laplacian") -> tuple[str, str]:
+    """The reference's file names (bbfmm.c:109-144): [s]laplacian{K,U}{n}.bin,
+    [s]oneoverr4{K,U}{n}.bin."""
+    if kernel not in KERNELS:
+        raise ValueError(f"unknown kernel {kernel!r} (laplacian or oneoverr4)")
     p = "s" if single else ""
-    return f"{p}laplacianK{n}.bin", f"{p}laplacianU{n}.bin"
+    return f"{p}{kernel}K{n}.bin", f"{p}{kernel}U{n}.bin"
 
 
-def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarray, single: bool):
-    """Write ``[s]laplacian{K,U}{n}.bin`` in the reference layout (bbfmm.c:1361-1405)."""
+def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarray, single: bool,
+                         kernel: str = "laplacian"):
+    """Write ``[s]<kernel>{K,U}{n}.bin`` in the reference layout (bbfmm.c:1361-1405)."""
     os.makedirs(dirpath, exist_ok=True)
-    kname, uname = operator_file_names(n, single)
+    kname, uname = operator_file_names(n, single, kernel)
     dt = np.float32 if single else np.float64
     r = Ucol.size // n ** 3
     with open(os.path.join(dirpath, uname), "wb") as f:
@@ -173,9 +197,9 @@ def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarra
         f.write(np.asarray(Ecol, dtype=dt).tobytes())
 
 
-def read_operator_files(dirpath: str, n: int, single: bool):
-    """Read ``[s]laplacian{K,U}{n}.bin`` (bbfmm.c:216-254). Returns (r, Ucol, Ecol)."""
-    kname, uname = operator_file_names(n, single)
+def read_operator_files(dirpath: str, n: int, single: bool, kernel: str = "laplacian"):
+    """Read ``[s]<kernel>{K,U}{n}.bin`` (bbfmm.c:216-254). Returns (r, Ucol, Ecol)."""
+    kname, uname = operator_file_names(n, single, kernel)
     dt = np.float32 if single else np.float64
     with open(os.path.join(dirpath, uname), "rb") as f:
         r = struct.unpack("i", f.read(4))[0]
@@ -191,14 +215,16 @@ def default_cache_dir() -> str:
         os.path.join(os.path.expanduser("~"), ".cache", "bbfmm_b200", "operators"))
 
 
-def singular_values(n: int, cache_dir: str | None = None) -> np.ndarray:
+def singular_values(n: int, cache_dir: str | None = None, kernel: str = "laplacian") -> np.ndarray:
     """Singular values of the FP64 kernel matrix K0 of order n, relative to the largest
-    (cached as sigma{n}.npy beside the operator files)."""
+    (cached as sigma{n}.npy, sigma_<kernel>{n}.npy for other kernels, beside the operator
+    files)."""
     cache_dir = cache_dir or default_cache_dir()
-    path = os.path.join(cache_dir, f"sigma{n}.npy")
+    tag = "" if kernel == "laplacian" else f"_{kernel}"
+    path = os.path.join(cache_dir, f"sigma{tag}{n}.npy")
     if os.path.exists(path):
         return np.load(path)
-    K0 = kernel_matrix(n)
+    K0 = kernel_matrix(n, kernel)
     R = np.linalg.qr(K0.T, mode="r")
     sv = np.linalg.svd(R.T, compute_uv=False)
     sv = sv / sv[0]
@@ -207,10 +233,11 @@ def singular_values(n: int, cache_dir: str | None = None) -> np.ndarray:
     return sv
 
 
-def tolerance_rank(n: int, tol: float, multiple: int = 32, cache_dir: str | None = None) -> int:
+def tolerance_rank(n: int, tol: float, multiple: int = 32, cache_dir: str | None = None,
+                   kernel: str = "laplacian") -> int:
     """Rank of an SVD cut at relative singular value `tol` (the number of sigma_j / sigma_0 >= tol),
     rounded up to `multiple` (the kernels' component granularity) and capped at n^3 / 2."""
-    sv = singular_values(n, cache_dir)
+    sv = singular_values(n, cache_dir, kernel)
     r = int((sv >= tol).sum())
     r = -(-r // multiple) * multiple
     return max(multiple, min(r, n ** 3 // 2))
@@ -231,21 +258,22 @@ def truncate_operators(n: int, Ucol: np.ndarray, Ecol: np.ndarray, rank: int):
     return U.reshape(-1), E.reshape(-1)
 
 
-def load_operators(n: int, single: bool = False, cache_dir: str | None = None):
-    """Cached operators for order n: returns (r, Ucol, Ecol) in the requested precision.
+def load_operators(n: int, single: bool = False, cache_dir: str | None = None, kernel: str = "laplacian"):
+    """Cached operators for order n and a kernel: returns (r, Ucol, Ecol) in the requested
+    precision.
 
     The FP64 SVD is always the source; single-precision files hold its rounding
     (operators are FP64-derived in every mode)."""
     cache_dir = cache_dir or default_cache_dir()
-    kname, uname = operator_file_names(n, single)
+    kname, uname = operator_file_names(n, single, kernel)
     if not (os.path.exists(os.path.join(cache_dir, kname))
             and os.path.exists(os.path.join(cache_dir, uname))):
-        dk, du = operator_file_names(n, False)
+        dk, du = operator_file_names(n, False, kernel)
         if os.path.exists(os.path.join(cache_dir, dk)) and os.path.exists(os.path.join(cache_dir, du)):
-            _, Ucol, Ecol = read_operator_files(cache_dir, n, False)
+            _, Ucol, Ecol = read_operator_files(cache_dir, n, False, kernel)
         else:
-            Ucol, Ecol, _ = kernel_svd(n)
-            write_operator_files(cache_dir, n, Ucol, Ecol, False)
+            Ucol, Ecol, _ = kernel_svd(n, kernel=kernel)
+            write_operator_files(cache_dir, n, Ucol, Ecol, False, kernel)
         if single:
-            write_operator_files(cache_dir, n, Ucol, Ecol, True)
-    return read_operator_files(cache_dir, n, single)
+            write_operator_files(cache_dir, n, Ucol, Ecol, True, kernel)
+    return read_operator_files(cache_dir, n, single, kernel)

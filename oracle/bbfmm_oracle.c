@@ -40,6 +40,7 @@
 typedef float real;
 #define SFX(name) name##_s
 #define SQRT(x) sqrtf(x)
+#define POW(x, y) powf(x, y)
 #define COS(x) cosf(x)
 #define RINT(x) rintf(x)
 #define ZERO 0.0f
@@ -49,6 +50,7 @@ typedef float real;
 typedef double real;
 #define SFX(name) name##_d
 #define SQRT(x) sqrt(x)
+#define POW(x, y) pow(x, y)
 #define COS(x) cos(x)
 #define RINT(x) rint(x)
 #define ZERO 0.0
@@ -61,6 +63,12 @@ typedef double real;
 #define MINLEV 2
 
 static int pow8(int i) { return 1 << (3 * i); }
+
+/* Kernel: degree of homogeneity 1 (1/r, LAPLACIAN) or 4 (1/r^4, ONEOVERR4); the pair value as
+   the reference's near field forms it from rinv = 1/r (anotherNearField.c:111-124). */
+static int g_homogen = 1;
+void SFX(orc_set_kernel)(int homogen) { g_homogen = homogen; }
+static real kern(real rinv) { return g_homogen == 4 ? rinv * rinv * rinv * rinv : rinv; }
 
 int SFX(orc_ncell)(int maxlev) { return (pow8(maxlev + 1) - 1) / 7; }
 int SFX(orc_levsta)(int level) { return (pow8(level) - 1) / 7; }
@@ -372,8 +380,8 @@ void SFX(orc_m2l)(int maxlev, int r, const real *E, const real *M, const real *c
   free(acc);
 }
 
-/* fieldval[n3 A + i] = (scale * Kweights[i]) * sum_j U(i, j) PF[r A + j], scale = 1/L_level
-   (homogeneity 1), for levels minlev..maxlev. */
+/* fieldval[n3 A + i] = (scale * Kweights[i]) * sum_j U(i, j) PF[r A + j], scale =
+   (1/L_level)^homogeneity (anotherFMMInteraction.c:7545-7549), for levels minlev..maxlev. */
 void SFX(orc_postm2l)(int maxlev, int n, int r, const real *U, const real *Kweights,
                       const real *PF, real L, real *fieldval)
 {
@@ -381,7 +389,7 @@ void SFX(orc_postm2l)(int maxlev, int n, int r, const real *U, const real *Kweig
   for (int level = MINLEV; level <= maxlev; level++) {
     real Lc = L;
     for (int i = 0; i < level; i++) Lc *= 0.5;
-    real scale = ONE / Lc;
+    real scale = POW(ONE / Lc, (real)g_homogen);
     for (int A = SFX(orc_levsta)(level); A < SFX(orc_levsta)(level + 1); A++)
       for (int i = 0; i < n3; i++) {
         real sum = ZERO;
@@ -506,7 +514,7 @@ void SFX(orc_nearfield)(int maxlev, int N, const real *xyz, const real *q, const
           real dx = x[jsta + j] - fx, dy = y[jsta + j] - fy, dz = z[jsta + j] - fz;
           real rr = dx * dx + dy * dy + dz * dz;
           real rinv = (rr != ZERO ? ONE / SQRT(rr) : ZERO);
-          v += rinv * qs[jsta + j];
+          v += kern(rinv) * qs[jsta + j];
         }
       }
       p[i] += qs[i] * v;
@@ -563,7 +571,8 @@ void SFX(orc_direct_fp64)(int N, const double *xyz, const double *q, int ntarget
     for (int j = 0; j < N; j++) {
       double dx = xyz[3 * j] - fx, dy = xyz[3 * j + 1] - fy, dz = xyz[3 * j + 2] - fz;
       if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
-      double v = q[j] / sqrt(dx * dx + dy * dy + dz * dz);
+      double rr = dx * dx + dy * dy + dz * dz;
+      double v = g_homogen == 4 ? q[j] * (1.0 / rr) * (1.0 / rr) : q[j] / sqrt(rr);
       double tsum = s + v;
       if (fabs(s) >= fabs(v)) c += (s - tsum) + v; else c += (v - tsum) + s;
       s = tsum;

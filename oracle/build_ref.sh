@@ -25,17 +25,18 @@ SRCS="bbfmm.c options.c checks.c opts.c envs.c output.c timer.c elapsed.c anothe
       anotherFMMInteraction.c anotherDownwardPassX.c anotherDownwardPass.c anotherUpwardPass.c
       anotherFMMDistribute.c anotherInteractionList.c anotherNearField.c m2l_aux.c
       auxAnotherFMMInteraction.c anotherBuildFMMHierachy.c xdot.c atransx.c m2l_aux_cpu.c"
+KDEF=-DLAPLACIAN  # the kernel of the build (bbfmm.c:109-144)
 build() {  # $1 = output name, rest = extra defines
   local name=$1; shift
   local objdir="$OUT/obj_$name"
   mkdir -p "$objdir"
   local objs=""
   for s in $SRCS; do
-    gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE \
+    gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w $KDEF -DFAST_HOST_CODE \
         -DENABLE_GETTIMEOFDAY "$@" -I"$REF" -c "$REF/$s" -o "$objdir/${s%.c}.o" &
     objs="$objs $objdir/${s%.c}.o"
   done
-  gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE "$@" -I"$REF" \
+  gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w $KDEF -DFAST_HOST_CODE "$@" -I"$REF" \
       -c "$HERE/ref_harness.c" -o "$objdir/ref_harness.o" &
   wait
   gcc -shared -fopenmp -o "$OUT/$name.so" $objs "$objdir/ref_harness.o" \
@@ -46,6 +47,8 @@ build libref_cpu8a_d -DCPU8 -DCPU8A
 build libref_cpu8a_s -DCPU8 -DCPU8A -DSINGLE
 build libref_cpu9a_d -DCPU9 -DCPU9A
 build libref_cpu9a_s -DCPU9 -DCPU9A -DSINGLE
+KDEF=-DONEOVERR4 build libref_cpu8a_d_r4 -DCPU8 -DCPU8A  # the 1/r^4 kernel (homogeneity 4)
+KDEF=-DLAPLACIAN
 # Drop-in build: the reference's own code with its pass objects (anotherFMMCompute,
 # anotherUpwardPass, anotherFMMInteraction, anotherDownwardPass[X], anotherNearField) left
 # out and resolved from the B200 library's reference-name shims instead.

@@ -129,14 +129,20 @@ class Oracle:
                                  _p(tree.neighbors), _p(phi))
         return phi
 
-    def fmm(self, xyz, q, n, maxlev, U, E, L=1.0):
+    def fmm(self, xyz, q, n, maxlev, U, E, L=1.0, homogen=1):
+        """homogen: the kernel's degree of homogeneity, 1 (1/r) or 4 (1/r^4); U, E must be
+        that kernel's operators."""
         xyz = self._arr(xyz).reshape(-1)
         q = self._arr(q)
         N = q.size
         r = U.size // n ** 3
         phi = np.zeros(N, self.dt)
-        self._f("orc_fmm")(N, _p(xyz), _p(q), self.R(L), n, r, maxlev, _p(self._arr(E)),
-                           _p(self._arr(U)), _p(phi))
+        self._f("orc_set_kernel")(int(homogen))
+        try:
+            self._f("orc_fmm")(N, _p(xyz), _p(q), self.R(L), n, r, maxlev, _p(self._arr(E)),
+                               _p(self._arr(U)), _p(phi))
+        finally:
+            self._f("orc_set_kernel")(1)
         return phi
 
     def ref_sources(self, N, L=1.0):
@@ -156,27 +162,34 @@ class Oracle:
         self._f("orc_direct_field_fp64")(q.size, _p(xyz), _p(q), targets.size, _p(targets), _p(pot), _p(fld))
         return pot, fld.reshape(-1, 3)
 
-    def direct_fp64(self, xyz, q, targets):
+    def direct_fp64(self, xyz, q, targets, homogen=1):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
         q = np.ascontiguousarray(q, dtype=np.float64)
         targets = np.ascontiguousarray(targets, dtype=np.int32)
         out = np.zeros(targets.size)
-        self._f("orc_direct_fp64")(q.size, _p(xyz), _p(q), targets.size, _p(targets), _p(out))
+        self._f("orc_set_kernel")(int(homogen))
+        try:
+            self._f("orc_direct_fp64")(q.size, _p(xyz), _p(q), targets.size, _p(targets), _p(out))
+        finally:
+            self._f("orc_set_kernel")(1)
         return out
 
 
-def reference_available(prec="d", variant="cpu8a") -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", f"libref_{variant}_{prec}.so"))
+def reference_available(prec="d", variant="cpu8a", kernel="laplacian") -> bool:
+    tag = "" if kernel == "laplacian" else "_r4"
+    return os.path.exists(os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{tag}.so"))
 
 
 class Reference:
-    """The reference's own CPU implementation (oracle/_ref, built by build_ref.sh)."""
+    """The reference's own CPU implementation (oracle/_ref, built by build_ref.sh); kernel
+    "oneoverr4" is its -DONEOVERR4 build."""
 
-    def __init__(self, prec="d", variant="cpu8a"):
+    def __init__(self, prec="d", variant="cpu8a", kernel="laplacian"):
         self.prec = prec
         self.dt = np.float64 if prec == "d" else np.float32
         self.R = C.c_double if prec == "d" else C.c_float
-        path = os.path.join(HERE, "_ref", f"libref_{variant}_{prec}.so")
+        tag = "" if kernel == "laplacian" else "_r4"
+        path = os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{tag}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run oracle/build_ref.sh")
         self.lib = C.CDLL(path)

@@ -129,7 +129,11 @@ int ref_fmm(int N, real *xyz, real *q, real L, int n, int maxlev, char *Kpath, c
   FMMReadMatrices(K, U, cutoff, n, 1, Kpath, Upath);
   anotherTree *atree;
   anotherBuildFMMHierachy(L, n, 1, maxlev, cutoff, &atree, N, N, (real3 *)xyz, (real3 *)xyz);
+#ifdef ONEOVERR4
+  real homogen = 4;  /* bbfmm.c:133-143 */
+#else
   real homogen = 1;
+#endif
   anotherUpwardPass(&atree, (real3 *)xyz, Cweights, Tkz, q, U, Kweights, cutoff, n, 1);
   if (proxysval_out) memcpy(proxysval_out, atree->proxysval, sizeof(real) * atree->ncell * cutoff);
   anotherFMMInteraction(&atree, K, Ktable, U, Kweights, n, 1, cutoff, homogen);
