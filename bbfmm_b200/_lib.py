@@ -43,6 +43,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_create.argtypes = [C.POINTER(Config), vp, vp, i, C.POINTER(vp)]
         L.bbfmm_b200_set_particles.argtypes = [vp, i, vp]
         L.bbfmm_b200_set_particles_device.argtypes = [vp, i, vp]
+        L.bbfmm_b200_set_kernel.argtypes = [vp, i]
         L.bbfmm_b200_solve.argtypes = [vp, vp, vp]
         L.bbfmm_b200_solve_host.argtypes = [vp, vp, vp]
         L.bbfmm_b200_solve_fields.argtypes = [vp, vp, vp, vp]

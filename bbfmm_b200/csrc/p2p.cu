@@ -14,7 +14,9 @@
 
 namespace bbfmm {
 
-template <typename T>
+// H: the kernel's degree of homogeneity, 1 (1/r) or 4 (1/r^4 = rinv rinv rinv rinv, as the
+// reference's near field forms it, anotherNearField.c:111-124).
+template <typename T, int H>
 __global__ void __launch_bounds__(256) p2p_kernel(int N, const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   const int *__restrict__ leafm, int maxlev, T *__restrict__ phi) {
   const int ncpd = 1 << maxlev;
@@ -40,7 +42,10 @@ __global__ void __launch_bounds__(256) p2p_kernel(int N, const T *__restrict__ p
             const T ex = pos4[4 * (int64_t)s] - fx, ey = pos4[4 * (int64_t)s + 1] - fy,
                     ez = pos4[4 * (int64_t)s + 2] - fz;
             const T rr = ex * ex + ey * ey + ez * ez;
-            if (rr != (T)0) v += pos4[4 * (int64_t)s + 3] * ((T)1 / sqrt(rr));
+            if (rr != (T)0) {
+              const T rinv = (T)1 / sqrt(rr);
+              v += pos4[4 * (int64_t)s + 3] * (H == 4 ? rinv * rinv * rinv * rinv : rinv);
+            }
           }
         }
       }
@@ -113,14 +118,19 @@ static int p2p_grid(int64_t n, int threads = 256) {
 
 template <typename T>
 int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s,
-               int threads) {
+               int threads, int homogen) {
   if (N <= 0) return BBFMM_OK;
   if (threads < 32 || threads > 256 || threads % 32) return bbfmm_set_error(BBFMM_ERR_ARG, "p2p threads per block");
-  p2p_kernel<T><<<p2p_grid(N, threads), threads, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
+  if (homogen == 4)
+    p2p_kernel<T, 4><<<p2p_grid(N, threads), threads, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
+  else if (homogen == 1)
+    p2p_kernel<T, 1><<<p2p_grid(N, threads), threads, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
+  else
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "near field: kernel homogeneity 1 (1/r) or 4 (1/r^4)");
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2p", __FILE__, __LINE__);
 }
-template int launch_p2p<double>(int, const double *, const int *, const int *, int, double *, cudaStream_t, int);
-template int launch_p2p<float>(int, const float *, const int *, const int *, int, float *, cudaStream_t, int);
+template int launch_p2p<double>(int, const double *, const int *, const int *, int, double *, cudaStream_t, int, int);
+template int launch_p2p<float>(int, const float *, const int *, const int *, int, float *, cudaStream_t, int, int);
 
 int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi,
                      cudaStream_t s, int threads) {
@@ -272,7 +282,7 @@ int near_field_run(int N, int maxlev, const double *xyzq, const int *leaf_start,
   int rc = bbfmm::launch_leaf_of(maxlev, leaf_start, leafm, st, 1);
   if (rc != BBFMM_OK) return rc;
   if (mode == BBFMM_B200_MODE_MIXED) return bbfmm::launch_p2p_mixed(N, xyzq, leaf_start, leafm, maxlev, phi, st, 256);
-  return bbfmm::launch_p2p<double>(N, xyzq, leaf_start, leafm, maxlev, phi, st, 256);
+  return bbfmm::launch_p2p<double>(N, xyzq, leaf_start, leafm, maxlev, phi, st, 256, 1);
 }
 
 int near_field_check(int N, int maxlev, double L, const void *xyzq, const void *leaf_start, const void *phi,

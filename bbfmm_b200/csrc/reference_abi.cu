@@ -228,6 +228,13 @@ int upward(Tree<T> **atree, const Real3<T> *source, const T *Cweights, const T *
   return rc;
 }
 
+// The reference's kernels the passes provide: homogeneity 1 (LAPLACIAN) and 4 (ONEOVERR4);
+// 0 for any other (LAPLACIANFORCE, homogen 2, is antisymmetric and not provided).
+template <typename T>
+int kernel_homogen(T homogen) {
+  return homogen == (T)1 ? 1 : (homogen == (T)4 ? 4 : 0);
+}
+
 template <typename T>
 int interaction(Tree<T> **atree, const T *E, const int *Ktable, const T *U, const T *Kweights, int n, int dof,
                 int cutoff, T homogen, double *secs) {
@@ -236,10 +243,12 @@ int interaction(Tree<T> **atree, const T *E, const int *Ktable, const T *U, cons
   TRY(check_tree(t, n, dof));
   if (cutoff != n * n * n / 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cutoff must be n^3/2");
   if (!t->proxysval) return bbfmm_set_error(BBFMM_ERR_STATE, "proxysval missing: run the upward pass first");
-  if (homogen != (T)1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "only the 1/r kernel (homogen = 1)");
+  if (!kernel_homogen(homogen))
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r) or 4 (1/r^4) only");
   const int n3 = n * n * n;
   Solver<T> s;
   int rc = make_solver(s, n, t->maxlev, (double)t->celeng[0], (const T *)nullptr, (const T *)nullptr, Kweights);
+  s.homogen = kernel_homogen(homogen);
   if (rc == BBFMM_OK) rc = s.set_operators(U, E);
   if (rc == BBFMM_OK) rc = s.alloc_work();
   if (rc == BBFMM_OK) rc = upload_multipoles(s, t->proxysval, BBFMM_MINLEV, t->maxlev);
@@ -284,9 +293,11 @@ int interaction(Tree<T> **atree, const T *E, const int *Ktable, const T *U, cons
 // near: add the near field; far: L2L + L2P from fieldval (which is then freed).
 template <typename T>
 int downward(Tree<T> **atree, const Real3<T> *field, const T *Cweights, const T *Tkz, const T *q, int n, int dof,
-             T *phi, bool far, bool near) {
+             T *phi, bool far, bool near, T homogen) {
   Tree<T> *t = atree ? *atree : nullptr;
   TRY(check_tree(t, n, dof));
+  if (near && !kernel_homogen(homogen))
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r) or 4 (1/r^4) only");
   if (far && !t->fieldval) return bbfmm_set_error(BBFMM_ERR_STATE, "fieldval missing: run the interaction first");
   const int n3 = n * n * n, maxlev = t->maxlev;
   Solver<T> s;
@@ -313,7 +324,8 @@ int downward(Tree<T> **atree, const Real3<T> *field, const T *Cweights, const T 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
     rc = bbfmm_set_cuda_error(e, "h2d phi", __FILE__, __LINE__);
   }
-  if (near && rc == BBFMM_OK) rc = launch_p2p<T>(s.N, s.pos4, s.leaf_start, s.leafm, maxlev, s.phis, s.stream);
+  if (near && rc == BBFMM_OK)
+    rc = launch_p2p<T>(s.N, s.pos4, s.leaf_start, s.leafm, maxlev, s.phis, s.stream, 256, kernel_homogen(homogen));
   if (rc == BBFMM_OK && s.N > 0) {
     std::vector<T> ps(s.N);
     cudaError_t e = cudaMemcpyAsync(ps.data(), s.phis, sizeof(T) * s.N, cudaMemcpyDeviceToHost, s.stream);
@@ -341,10 +353,12 @@ int compute(Tree<T> **atree, const Real3<T> *field, const Real3<T> *source, cons
   TRY(check_tree(t, n, dof));
   if (field != source) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "field points must equal the sources");
   if (cutoff != n * n * n / 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cutoff must be n^3/2");
-  if (homogen != (T)1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "only the 1/r kernel (homogen = 1)");
+  if (!kernel_homogen(homogen))
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r) or 4 (1/r^4) only");
   Solver<T> s;
   T *qd = nullptr, *pd = nullptr;
   int rc = make_solver(s, n, t->maxlev, (double)t->celeng[0], Tkz, Cweights, Kweights);
+  s.homogen = kernel_homogen(homogen);
   if (rc == BBFMM_OK) rc = s.set_operators(U, K);
   if (rc == BBFMM_OK) rc = load_particles(s, t, source);
   if (rc == BBFMM_OK) rc = upload_q(s, q, &qd);
@@ -396,22 +410,24 @@ using namespace bbfmm::ref;
   }                                                                                                               \
   API int bbfmm_b200_ref_downward_##SFX(void *atree, void *field, void *source, T *Cweights, T *Tkz, T *q, T *U, \
                                         int cutoff, int n, int dof, T homogen, T *phi) {                          \
-    (void)source; (void)U; (void)cutoff; (void)homogen;                                                           \
-    return downward<T>((Tree<T> **)atree, (const Real3<T> *)field, Cweights, Tkz, q, n, dof, phi, true, true);   \
+    (void)source; (void)U; (void)cutoff;                                                                          \
+    return downward<T>((Tree<T> **)atree, (const Real3<T> *)field, Cweights, Tkz, q, n, dof, phi, true, true,    \
+                       homogen);                                                                                  \
   }                                                                                                               \
   API int bbfmm_b200_ref_downward_far_##SFX(void *atree, void *field, T *Cweights, T *Tkz, T *q, T *U,           \
                                             int cutoff, int n, int dof, T homogen, T *phi) {                      \
-    (void)U; (void)cutoff; (void)homogen;                                                                         \
-    return downward<T>((Tree<T> **)atree, (const Real3<T> *)field, Cweights, Tkz, q, n, dof, phi, true, false);  \
+    (void)U; (void)cutoff;                                                                                        \
+    return downward<T>((Tree<T> **)atree, (const Real3<T> *)field, Cweights, Tkz, q, n, dof, phi, true, false,   \
+                       homogen);                                                                                  \
   }                                                                                                               \
   API int bbfmm_b200_ref_near_field_##SFX(void *atree, int dof, T homogen, void *field, void *source, T *phi,    \
                                           T *q) {                                                                 \
-    (void)source; (void)homogen;                                                                                  \
+    (void)source;                                                                                                 \
     Tree<T> *t = atree ? *(Tree<T> **)atree : nullptr;                                                            \
     if (!t) return bbfmm_set_error(BBFMM_ERR_ARG, "null tree");                                                   \
     const int n = 4; /* the order does not enter the near field */                                                \
     return downward<T>((Tree<T> **)atree, (const Real3<T> *)field, nullptr, nullptr, q, n, dof, phi, false,      \
-                       true);                                                                                     \
+                       true, homogen);                                                                            \
   }                                                                                                               \
   API int bbfmm_b200_ref_compute_##SFX(void *atree, void *field, void *source, T *q, T *K, T *U, T *Tkz,         \
                                        int *Ktable, T *Kweights, T *Cweights, T homogen, int cutoff, int n,       \

@@ -5,6 +5,7 @@
 //   gather q -> P2M (maxlev) -> [U-projection, M2M] up to level 2      (upward)
 //   per level 2..maxlev: M2L -> post projection (assign) -> L2L from the parent level
 //   L2P (assign) -> P2P (add) -> scatter phi to the caller's particle order
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -444,7 +445,9 @@ int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, b
 // the tensor cores from L rows gathered into Morton order as split BF16.
 template <typename T>
 int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit) {
-  const T scale = (T)1 / cell_length<T>(level, (T)L);
+  // (1/L_l)^homogen in T, as the reference's POW(iL, homogen) (anotherFMMInteraction.c:7545-7549)
+  const T iL = (T)1 / cell_length<T>(level, (T)L);
+  const T scale = homogen == 1 ? iL : (T)std::pow(iL, (T)homogen);
   if (!proj_tc() || rows > Lsplit_rows)  // contraction over the effective rank (j < rk())
     return proj(rows, rk(), n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0, r);
   // components j < 16 in FP64 and the rest as split-BF16 tensor-core products, one pass
@@ -605,7 +608,7 @@ int Solver<T>::near(T *pot, T *fld) {
     mark(ST_P2P);
   } else {
     if (fld) TRY(launch_p2p_field<T>(N, pos4, leaf_start, leafm, maxlev, pot, fld, stream, th));
-    else TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, pot, stream, th));
+    else TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, pot, stream, th, homogen));
     mark(ST_P2P);
   }
   return BBFMM_OK;
@@ -616,6 +619,7 @@ int Solver<T>::near(T *pot, T *fld) {
 template <typename T>
 int Solver<T>::solve_fields(const void *q_dev, void *pot_dev, void *fld_dev) {
   if (!pos4) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
+  if (homogen != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fields are computed for the 1/r kernel");
   if (!Ert) return bbfmm_set_error(BBFMM_ERR_STATE, "operators not set");
   if (!flds) TRY(dalloc(&flds, 3 * (size_t)(N > 0 ? N : 1)));
   kernel_launches = 0;
@@ -948,6 +952,21 @@ int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *h, long long cells) {
   }
   h->d->slab_request = cells;
   return h->d->pos4 ? h->d->alloc_work() : BBFMM_OK;
+}
+
+int bbfmm_b200_set_kernel(bbfmm_b200_solver *h, int kernel) {
+  if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
+  if (kernel == BBFMM_B200_KERNEL_LAPLACIAN_FORCE)
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "the x / r^3 kernel is antisymmetric: not provided");
+  if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && kernel != BBFMM_B200_KERNEL_ONEOVERR4)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "unknown kernel");
+  const int mode = h->f ? h->f->mode : h->d->mode;
+  if (kernel == BBFMM_B200_KERNEL_ONEOVERR4 && mode == bbfmm::MODE_MIXED)
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "the 1/r^4 kernel runs in modes D and S");
+  const int hg = kernel == BBFMM_B200_KERNEL_ONEOVERR4 ? 4 : 1;
+  if (h->f) h->f->homogen = hg;
+  else h->d->homogen = hg;
+  return BBFMM_OK;
 }
 
 int bbfmm_b200_set_rank(bbfmm_b200_solver *h, int rank) {

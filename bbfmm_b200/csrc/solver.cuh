@@ -36,7 +36,7 @@ template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
-template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s, int threads = 256);
+template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s, int threads = 256, int homogen = 1);
 int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi, cudaStream_t s, int threads = 256);
 int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s, int nsets = 1);
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
@@ -106,6 +106,9 @@ template <typename T>
 struct Solver {
   int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, lead_rows = 32, device = 0;
   int nsets = 1;  // particle sets of this depth stacked in every launch (set k = cells [k 8^l, (k+1) 8^l))
+  // kernel: degree of homogeneity, 1 (1/r, LAPLACIAN) or 4 (1/r^4, ONEOVERR4; modes D and S):
+  // the near-field pair value and the per-level scale (1/L_l)^homogen after the M2L
+  int homogen = 1;
   // Effective rank (0 = r): the operators hold a rank-rank_eff truncation zero-padded to r,
   // and the M2L and the down projection skip the zero components j >= rank_eff and outputs
   // i >= rank_eff (a tolerance-rank SVD cut, bbfmm_b200_set_rank).

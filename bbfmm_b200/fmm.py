@@ -39,11 +39,13 @@ class Solver:
     mode: "d" (FP64 everywhere), "s" (FP32 everywhere), "mixed" (FP64 passes,
     split-precision tensor-core M2L whose leading operator block -- outputs i < ``lead_rows``,
     components j < ``lead`` -- runs in FP64, split-precision tensor-core projections with 16
-    FP64 components, P2P with FP64 separations and compensated FP32 sums)."""
+    FP64 components, P2P with FP64 separations and compensated FP32 sums).
+    kernel: "laplacian" (1/r) or "oneoverr4" (1/r^4, modes "d" and "s"), the reference's
+    LAPLACIAN and ONEOVERR4 builds."""
 
     def __init__(self, n: int, maxlev: int, L: float = 1.0, mode: str = "d", lead: int = 16,
                  lead_rows: int = 32, device: int = 0, operators=None, stream=None, rank: int | None = None,
-                 tol: float | None = None):
+                 tol: float | None = None, kernel: str = "laplacian"):
         import torch
         self.torch = torch
         self.n, self.maxlev, self.L, self.mode = n, maxlev, float(L), mode
@@ -53,14 +55,17 @@ class Solver:
         self.device = device
         self.dtype = torch.float32 if mode == "s" else torch.float64
         self.np_dtype = np.float32 if mode == "s" else np.float64
+        if kernel != "laplacian" and mode == "mixed":
+            raise ValueError("the mixed mode is built for the 1/r kernel; use mode 'd' or 's'")
+        self.kernel = kernel
         if operators is None:
-            _, U, E = ops.load_operators(n, single=(mode == "s"))
+            _, U, E = ops.load_operators(n, single=(mode == "s"), kernel=kernel)
         else:
             U, E = operators
         # tolerance-rank mode: an SVD cut at relative singular value `tol` (or an explicit rank),
         # the truncated operators zero-padded to r and the zero blocks skipped by the kernels
         if tol is not None and rank is None:
-            rank = ops.tolerance_rank(n, tol)
+            rank = ops.tolerance_rank(n, tol, kernel=kernel)
         self.rank = self.r if rank is None else int(rank)
         if self.rank != self.r:
             U, E = ops.truncate_operators(n, U, E, self.rank)
@@ -76,6 +81,8 @@ class Solver:
         self.N = 0
         if self.rank != self.r:
             _lib.check(_lib.lib().bbfmm_b200_set_rank(h, self.rank))
+        if kernel != "laplacian":
+            _lib.check(_lib.lib().bbfmm_b200_set_kernel(h, ops.KERNELS[kernel][1]))
 
     def __del__(self):
         h = getattr(self, "h", None)

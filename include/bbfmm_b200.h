@@ -226,6 +226,17 @@ BBFMM_B200_API int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *s, long long cell
  * is new. */
 BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
 
+/* Kernel of the solver (the reference's compile-time kernels, bbfmm.c:109-144, 798-849):
+ * BBFMM_B200_KERNEL_LAPLACIAN (1/r, the default) or BBFMM_B200_KERNEL_ONEOVERR4 (1/r^4,
+ * modes D and S; the operators given at create must be that kernel's, e.g. the reference's
+ * oneoverr4{K,U}{n}.bin). It sets the near-field pair value and the per-level scale
+ * (1/L_l)^homogeneity after the M2L. BBFMM_B200_KERNEL_LAPLACIAN_FORCE (x / r^3) is
+ * antisymmetric and not provided (BBFMM_B200_ERR_UNSUPPORTED). Field solves are for 1/r. */
+#define BBFMM_B200_KERNEL_LAPLACIAN 0
+#define BBFMM_B200_KERNEL_LAPLACIAN_FORCE 1
+#define BBFMM_B200_KERNEL_ONEOVERR4 2
+BBFMM_B200_API int bbfmm_b200_set_kernel(bbfmm_b200_solver *s, int kernel);
+
 /* MIXED mode: products per term of the tensor-core M2L. 0 (default, adaptive): the three
  * split-BF16 products hi*hi + hi*lo + lo*hi for the contraction components j < 64 and the
  * outputs i < 64 of every operator, hi*hi alone for the rest, whose terms are small enough

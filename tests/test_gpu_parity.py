@@ -222,3 +222,37 @@ def test_tolerance_rank_fp32_matches_fp64_rank():
         out[mode] = s.solve(torch.as_tensor(q, dtype=dt, device="cuda")).double().cpu().numpy()
         s.close()
     assert rel_l2(out["s"], out["d"]) < 2e-5
+
+
+@pytest.mark.parametrize("mode,tol", [("d", 1e-12), ("s", 2e-5)])
+def test_oneoverr4_kernel_matches_oracle(oracle_d, oracle_s, mode, tol):
+    """The 1/r^4 kernel (the reference's ONEOVERR4 build; homogeneity 4: near field
+    q / r^4 and the per-level scale (1/L_l)^4) against the oracle with the same operators."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200 import operators as ops
+    single = mode == "s"
+    _, U, E = ops.load_operators(4, single=single, kernel="oneoverr4")
+    x, q = uniform_inputs(30000, seed=17)
+    O = oracle_s if single else oracle_d
+    want = O.fmm(x, q, 4, 3, U, E, homogen=4)
+    s = Solver(4, 3, 1.0, mode=mode, kernel="oneoverr4")
+    s.set_particles(x)
+    dt = torch.float32 if single else torch.float64
+    got = s.solve(torch.as_tensor(q, dtype=dt, device="cuda")).double().cpu().numpy()
+    assert rel_l2(got, want) < tol
+    s.close()
+
+
+def test_oneoverr4_refuses_mixed_and_fields():
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200._lib import BBFMMError
+    with pytest.raises(ValueError):
+        Solver(8, 3, 1.0, mode="mixed", kernel="oneoverr4")
+    x, q = uniform_inputs(2000, seed=18)
+    s = Solver(4, 3, 1.0, mode="d", kernel="oneoverr4")
+    s.set_particles(x)
+    with pytest.raises(BBFMMError):
+        s.solve_fields(torch.as_tensor(q, device="cuda"))
+    s.close()
