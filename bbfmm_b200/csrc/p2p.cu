@@ -1,6 +1,7 @@
-// Near-field P2P: phi_i += q_i * sum_{B in N(A)} sum_{j in B, r_ij != 0} q_j / r_ij over
-// the <= 27 neighbour leaves of each leaf (reference: anotherNearField.c:141-206 on the
-// CPU, direct.cu:69-209 on the GPU).
+// Near-field P2P: phi_i += q_i * sum_{B in N(A)} sum_{j in B, r_ij != 0} q_j K(r_ij) over
+// the <= 27 neighbour leaves of each leaf, K = 1/r (and 1/r^4 in p2p_kernel<T, 4>, the
+// reference's ONEOVERR4 build) (reference: anotherNearField.c:141-206 on the CPU,
+// direct.cu:69-209 on the GPU).
 //
 // One thread per target particle; particles are leaf-sorted, so a warp covers a run of
 // neighbouring leaves and the source particles it streams are shared through L1.
