@@ -46,3 +46,26 @@ def test_operator_files_roundtrip(tmp_path):
     ops.write_operator_files(str(tmp_path), 4, U, E, False)
     r, U2, E2 = ops.read_operator_files(str(tmp_path), 4, False)
     assert r == 32 and np.array_equal(U, U2) and np.array_equal(E, E2)
+
+
+def test_kernel_operator_files_round_trip(tmp_path):
+    """The 1/r^4 operators (the reference's ONEOVERR4 build) use the reference's file names
+    and layout, stay apart from the 1/r files in one directory, and differ from them."""
+    import numpy as np
+    import pytest
+    from bbfmm_b200 import operators as ops
+    assert ops.operator_file_names(4, False, "oneoverr4") == ("oneoverr4K4.bin", "oneoverr4U4.bin")
+    assert ops.operator_file_names(8, True, "oneoverr4") == ("soneoverr4K8.bin", "soneoverr4U8.bin")
+    assert ops.operator_file_names(4, False) == ("laplacianK4.bin", "laplacianU4.bin")
+    assert ops.homogeneity("laplacian") == 1 and ops.homogeneity("oneoverr4") == 4
+    with pytest.raises(ValueError):
+        ops.operator_file_names(4, False, "laplacianforce")
+    r4, U4, E4 = ops.load_operators(4, cache_dir=str(tmp_path), kernel="oneoverr4")
+    r1, U1, E1 = ops.load_operators(4, cache_dir=str(tmp_path))
+    assert r4 == r1 == 32
+    assert (tmp_path / "oneoverr4K4.bin").exists() and (tmp_path / "laplacianK4.bin").exists()
+    r, U, E = ops.read_operator_files(str(tmp_path), 4, False, "oneoverr4")
+    assert np.array_equal(U, U4) and np.array_equal(E, E4)
+    assert not np.allclose(np.abs(E4), np.abs(E1))
+    _, Us, _ = ops.load_operators(4, single=True, cache_dir=str(tmp_path), kernel="oneoverr4")
+    assert Us.dtype == np.float32 and np.allclose(Us, U4, rtol=1e-6, atol=1e-7)
