@@ -56,19 +56,21 @@ LIBDIR="$HERE/../bbfmm_b200/lib"
 if [ -f "$LIBDIR/libbbfmm_b200_ref_d.so" ]; then
   DROP="anotherFMMCompute.c anotherFMMInteraction.c anotherDownwardPassX.c anotherDownwardPass.c
         anotherUpwardPass.c anotherNearField.c"
-  for prec in d s; do
+  # d, s and the 1/r^4 kernel (ONEOVERR4, double)
+  for var in d s d_r4; do
+    prec=${var%%_*}; kdef=-DLAPLACIAN; [ $var = d_r4 ] && kdef=-DONEOVERR4
     def=""; [ $prec = s ] && def="-DSINGLE"
-    objdir="$OUT/obj_dropin_$prec"; mkdir -p "$objdir"; objs=""
+    objdir="$OUT/obj_dropin_$var"; mkdir -p "$objdir"; objs=""
     for src in $SRCS; do
       case " $(echo $DROP) " in *" $src "*) continue;; esac
-      gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE -DENABLE_GETTIMEOFDAY \
+      gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w $kdef -DFAST_HOST_CODE -DENABLE_GETTIMEOFDAY \
           -DCPU8 -DCPU8A $def -I"$REF" -c "$REF/$src" -o "$objdir/${src%.c}.o" &
       objs="$objs $objdir/${src%.c}.o"
     done
-    gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w -DLAPLACIAN -DFAST_HOST_CODE -DCPU8 -DCPU8A $def -I"$REF" \
+    gcc -std=gnu99 -O3 -fopenmp -fcommon -fPIC -w $kdef -DFAST_HOST_CODE -DCPU8 -DCPU8A $def -I"$REF" \
         -c "$HERE/ref_harness.c" -o "$objdir/ref_harness.o" &
     wait
-    gcc -shared -fopenmp -o "$OUT/libref_dropin_$prec.so" $objs "$objdir/ref_harness.o" \
+    gcc -shared -fopenmp -o "$OUT/libref_dropin_$var.so" $objs "$objdir/ref_harness.o" \
         -L"$LIBDIR" -l:libbbfmm_b200_ref_$prec.so -Wl,--disable-new-dtags,-rpath,'$ORIGIN/../../bbfmm_b200/lib' \
         -L"$BL" -l:"$BLAS" -Wl,-rpath,"$BL" -lm
     rm -rf "$objdir"

@@ -45,6 +45,27 @@ def test_reference_pipeline_with_b200_passes(prec, lev, tol, opdir):
     assert rel_l2(pd, pr) < tol
 
 
+
+@pytest.mark.skipif(not reference_available("d", "dropin", kernel="oneoverr4"),
+                    reason="1/r^4 drop-in reference build absent")
+def test_reference_pipeline_with_b200_passes_oneoverr4():
+    """The same drop-in check for the reference's -DONEOVERR4 build (homogen 4 through the
+    shims: the near field q / r^4 and the per-level scale (1/L_l)^4), on the operators that
+    build computes itself: 1e-12."""
+    ref = Reference("d", "cpu8a", kernel="oneoverr4")
+    drop = Reference("d", "dropin", kernel="oneoverr4")
+    d = tempfile.mkdtemp()
+    kp, up = os.path.join(d, "oneoverr4K4.bin"), os.path.join(d, "oneoverr4U4.bin")
+    ref.lib.ref_compute_operators(4, C.c_char_p(kp.encode()), C.c_char_p(up.encode()))
+    x, q = uniform_inputs(30000, seed=43)
+    pr, Pr, Fr = ref.fmm(x, q, 4, 3, kp, up, want_intermediates=True)
+    pd, Pd, Fd = drop.fmm(x, q, 4, 3, kp, up, want_intermediates=True)
+    lo32, lo64 = 9 * 32, 9 * 64
+    assert rel_l2(Pd[lo32:], Pr[lo32:]) < 1e-12
+    assert rel_l2(Fd[lo64:], Fr[lo64:]) < 1e-12
+    assert rel_l2(pd, pr) < 1e-12
+
+
 class Cell(C.Structure):
     _fields_ = [("neighbors", C.c_void_p), ("interaction", C.c_void_p), ("center", C.c_void_p),
                 ("fieldsta", C.c_void_p), ("fieldend", C.c_void_p), ("sourcesta", C.c_void_p),
