@@ -1,7 +1,7 @@
-// Near-field P2P: phi_i += q_i * sum_{B in N(A)} sum_{j in B, r_ij != 0} q_j K(r_ij) over
-// the <= 27 neighbour leaves of each leaf, K = 1/r (and 1/r^4 in p2p_kernel<T, 4>, the
-// reference's ONEOVERR4 build) (reference: anotherNearField.c:141-206 on the CPU,
-// direct.cu:69-209 on the GPU).
+// Near-field P2P: phi_i += q_i * sum_{B in N(A)} sum_{j in B, r_ij != 0} q_j K(x_j - x_i) over
+// the <= 27 neighbour leaves of each leaf, K = 1/r (and, in p2p_kernel<T, H>, x/r^3 for H = 2
+// and 1/r^4 for H = 4: the reference's LAPLACIANFORCE and ONEOVERR4 builds) (reference:
+// anotherNearField.c:141-206 on the CPU, direct.cu:69-209 on the GPU).
 //
 // One thread per target particle; particles are leaf-sorted, so a warp covers a run of
 // neighbouring leaves and the source particles it streams are shared through L1.
@@ -15,8 +15,9 @@
 
 namespace bbfmm {
 
-// H: the kernel's degree of homogeneity, 1 (1/r) or 4 (1/r^4 = rinv rinv rinv rinv, as the
-// reference's near field forms it, anotherNearField.c:111-124).
+// H: the kernel's degree of homogeneity, 1 (1/r), 2 (x/r^3 = dx rinv rinv rinv with dx the
+// x component of source - target) or 4 (1/r^4 = rinv rinv rinv rinv), each formed as the
+// reference's near field forms it (anotherNearField.c:111-124).
 template <typename T, int H>
 __global__ void __launch_bounds__(256) p2p_kernel(int N, const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   const int *__restrict__ leafm, int maxlev, T *__restrict__ phi) {
@@ -45,7 +46,8 @@ __global__ void __launch_bounds__(256) p2p_kernel(int N, const T *__restrict__ p
             const T rr = ex * ex + ey * ey + ez * ez;
             if (rr != (T)0) {
               const T rinv = (T)1 / sqrt(rr);
-              v += pos4[4 * (int64_t)s + 3] * (H == 4 ? rinv * rinv * rinv * rinv : rinv);
+              const T kern = H == 4 ? rinv * rinv * rinv * rinv : (H == 2 ? ex * rinv * rinv * rinv : rinv);
+              v += pos4[4 * (int64_t)s + 3] * kern;
             }
           }
         }
@@ -124,10 +126,13 @@ int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, in
   if (threads < 32 || threads > 256 || threads % 32) return bbfmm_set_error(BBFMM_ERR_ARG, "p2p threads per block");
   if (homogen == 4)
     p2p_kernel<T, 4><<<p2p_grid(N, threads), threads, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
+  else if (homogen == 2)
+    p2p_kernel<T, 2><<<p2p_grid(N, threads), threads, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
   else if (homogen == 1)
     p2p_kernel<T, 1><<<p2p_grid(N, threads), threads, 0, s>>>(N, pos4, leaf_start, leafm, maxlev, phi);
   else
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "near field: kernel homogeneity 1 (1/r) or 4 (1/r^4)");
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED,
+                           "near field: kernel homogeneity 1 (1/r), 2 (x/r^3) or 4 (1/r^4)");
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2p", __FILE__, __LINE__);
 }
 template int launch_p2p<double>(int, const double *, const int *, const int *, int, double *, cudaStream_t, int, int);

@@ -228,11 +228,11 @@ int upward(Tree<T> **atree, const Real3<T> *source, const T *Cweights, const T *
   return rc;
 }
 
-// The reference's kernels the passes provide: homogeneity 1 (LAPLACIAN) and 4 (ONEOVERR4);
-// 0 for any other (LAPLACIANFORCE, homogen 2, is antisymmetric and not provided).
+// The reference's kernels (bbfmm.c:109-144), told apart by the homogen argument it passes:
+// 1 (LAPLACIAN, 1/r), 2 (LAPLACIANFORCE, x/r^3) and 4 (ONEOVERR4, 1/r^4); 0 for any other.
 template <typename T>
 int kernel_homogen(T homogen) {
-  return homogen == (T)1 ? 1 : (homogen == (T)4 ? 4 : 0);
+  return homogen == (T)1 ? 1 : (homogen == (T)2 ? 2 : (homogen == (T)4 ? 4 : 0));
 }
 
 template <typename T>
@@ -244,7 +244,7 @@ int interaction(Tree<T> **atree, const T *E, const int *Ktable, const T *U, cons
   if (cutoff != n * n * n / 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cutoff must be n^3/2");
   if (!t->proxysval) return bbfmm_set_error(BBFMM_ERR_STATE, "proxysval missing: run the upward pass first");
   if (!kernel_homogen(homogen))
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r) or 4 (1/r^4) only");
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r), 2 (x/r^3) or 4 (1/r^4) only");
   const int n3 = n * n * n;
   Solver<T> s;
   int rc = make_solver(s, n, t->maxlev, (double)t->celeng[0], (const T *)nullptr, (const T *)nullptr, Kweights);
@@ -297,7 +297,7 @@ int downward(Tree<T> **atree, const Real3<T> *field, const T *Cweights, const T 
   Tree<T> *t = atree ? *atree : nullptr;
   TRY(check_tree(t, n, dof));
   if (near && !kernel_homogen(homogen))
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r) or 4 (1/r^4) only");
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r), 2 (x/r^3) or 4 (1/r^4) only");
   if (far && !t->fieldval) return bbfmm_set_error(BBFMM_ERR_STATE, "fieldval missing: run the interaction first");
   const int n3 = n * n * n, maxlev = t->maxlev;
   Solver<T> s;
@@ -354,7 +354,7 @@ int compute(Tree<T> **atree, const Real3<T> *field, const Real3<T> *source, cons
   if (field != source) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "field points must equal the sources");
   if (cutoff != n * n * n / 2) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "cutoff must be n^3/2");
   if (!kernel_homogen(homogen))
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r) or 4 (1/r^4) only");
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "kernels with homogen 1 (1/r), 2 (x/r^3) or 4 (1/r^4) only");
   Solver<T> s;
   T *qd = nullptr, *pd = nullptr;
   int rc = make_solver(s, n, t->maxlev, (double)t->celeng[0], Tkz, Cweights, Kweights);

@@ -956,14 +956,13 @@ int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *h, long long cells) {
 
 int bbfmm_b200_set_kernel(bbfmm_b200_solver *h, int kernel) {
   if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
-  if (kernel == BBFMM_B200_KERNEL_LAPLACIAN_FORCE)
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "the x / r^3 kernel is antisymmetric: not provided");
-  if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && kernel != BBFMM_B200_KERNEL_ONEOVERR4)
+  if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && kernel != BBFMM_B200_KERNEL_LAPLACIAN_FORCE &&
+      kernel != BBFMM_B200_KERNEL_ONEOVERR4)
     return bbfmm_set_error(BBFMM_ERR_ARG, "unknown kernel");
   const int mode = h->f ? h->f->mode : h->d->mode;
-  if (kernel == BBFMM_B200_KERNEL_ONEOVERR4 && mode == bbfmm::MODE_MIXED)
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "the 1/r^4 kernel runs in modes D and S");
-  const int hg = kernel == BBFMM_B200_KERNEL_ONEOVERR4 ? 4 : 1;
+  if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && mode == bbfmm::MODE_MIXED)
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "the x / r^3 and 1/r^4 kernels run in modes D and S");
+  const int hg = kernel == BBFMM_B200_KERNEL_ONEOVERR4 ? 4 : (kernel == BBFMM_B200_KERNEL_LAPLACIAN_FORCE ? 2 : 1);
   if (h->f) h->f->homogen = hg;
   else h->d->homogen = hg;
   return BBFMM_OK;

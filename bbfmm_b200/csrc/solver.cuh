@@ -106,8 +106,9 @@ template <typename T>
 struct Solver {
   int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, lead_rows = 32, device = 0;
   int nsets = 1;  // particle sets of this depth stacked in every launch (set k = cells [k 8^l, (k+1) 8^l))
-  // kernel: degree of homogeneity, 1 (1/r, LAPLACIAN) or 4 (1/r^4, ONEOVERR4; modes D and S):
-  // the near-field pair value and the per-level scale (1/L_l)^homogen after the M2L
+  // kernel: degree of homogeneity, 1 (1/r, LAPLACIAN), 2 (x/r^3, LAPLACIANFORCE) or 4 (1/r^4,
+  // ONEOVERR4); 2 and 4 in modes D and S: the near-field pair value and the per-level scale
+  // (1/L_l)^homogen after the M2L
   int homogen = 1;
   // Effective rank (0 = r): the operators hold a rank-rank_eff truncation zero-padded to r,
   // and the M2L and the down projection skip the zero components j >= rank_eff and outputs

@@ -40,8 +40,9 @@ class Solver:
     split-precision tensor-core M2L whose leading operator block -- outputs i < ``lead_rows``,
     components j < ``lead`` -- runs in FP64, split-precision tensor-core projections with 16
     FP64 components, P2P with FP64 separations and compensated FP32 sums).
-    kernel: "laplacian" (1/r) or "oneoverr4" (1/r^4, modes "d" and "s"), the reference's
-    LAPLACIAN and ONEOVERR4 builds."""
+    kernel: "laplacian" (1/r), "laplacianforce" (x/r^3, x the first component of source -
+    target; modes "d" and "s") or "oneoverr4" (1/r^4, modes "d" and "s"), the reference's
+    LAPLACIAN, LAPLACIANFORCE and ONEOVERR4 builds."""
 
     def __init__(self, n: int, maxlev: int, L: float = 1.0, mode: str = "d", lead: int = 16,
                  lead_rows: int = 32, device: int = 0, operators=None, stream=None, rank: int | None = None,
@@ -55,6 +56,8 @@ class Solver:
         self.device = device
         self.dtype = torch.float32 if mode == "s" else torch.float64
         self.np_dtype = np.float32 if mode == "s" else np.float64
+        if kernel not in ops.KERNELS:
+            raise ValueError(f"unknown kernel {kernel!r} ({', '.join(ops.KERNELS)})")
         if kernel != "laplacian" and mode == "mixed":
             raise ValueError("the mixed mode is built for the 1/r kernel; use mode 'd' or 's'")
         self.kernel = kernel

@@ -1,5 +1,6 @@
 """Chebyshev tables and SVD-compressed M2L operators (host, FP64) for the reference's
-homogeneous kernels: 1/r (LAPLACIAN, the default) and 1/r^4 (ONEOVERR4).
+homogeneous kernels: 1/r (LAPLACIAN, the default), x/r^3 (LAPLACIANFORCE) and 1/r^4
+(ONEOVERR4).
 
 This is set-up work, not the solve: it runs once per interpolation order ``n`` and
 its output is cached in the reference's operator-file format so that the same
@@ -33,22 +34,29 @@ import numpy as np
 NUM_OFFSETS = 316  # |[-3,3]^3 \ [-1,1]^3|
 
 # The reference's compile-time kernels (bbfmm.c:109-144, 798-849): name -> (degree of
-# homogeneity, kernel id of the C-ABI). LAPLACIANFORCE (x / r^3, homogeneity 2) is not
-# provided: it is antisymmetric, so the E_k = U^T K_k U form used for the M2L does not hold.
-KERNELS = {"laplacian": (1, 0), "oneoverr4": (4, 2)}
+# homogeneity, kernel id of the C-ABI). "laplacianforce" is x / r^3 with x the first component
+# of source - field (LAPLACIANFORCE). It is odd in the separation, so K_{-k} = -K_k^T over the
+# symmetric set of 316 offsets: the field-side singular vectors of [K_0 ... K_315] also span
+# every K_k's source side, and E_k = U^T K_k U compresses it as it does the even kernels.
+KERNELS = {"laplacian": (1, 0), "laplacianforce": (2, 1), "oneoverr4": (4, 2)}
 
 
 def homogeneity(kernel: str) -> int:
     return KERNELS[kernel][0]
 
 
-def _kernel_values(kernel: str, r: np.ndarray) -> np.ndarray:
+def _kernel_values(kernel: str, d: np.ndarray) -> np.ndarray:
+    """K at separations d = source - field (..., 3), as the reference's EvaluateKernel
+    (bbfmm.c:798-849)."""
+    r = np.sqrt(np.einsum("...x,...x->...", d, d))
+    rinv = 1.0 / r
     if kernel == "laplacian":
-        return 1.0 / r
+        return rinv
+    if kernel == "laplacianforce":
+        return d[..., 0] * rinv * rinv * rinv
     if kernel == "oneoverr4":
-        rinv = 1.0 / r
         return rinv * rinv * rinv * rinv
-    raise ValueError(f"unknown kernel {kernel!r} (laplacian or oneoverr4)")
+    raise ValueError(f"unknown kernel {kernel!r} ({', '.join(KERNELS)})")
 
 
 def ktable() -> np.ndarray:
@@ -133,8 +141,8 @@ def kernel_matrix(n: int, kernel: str = "laplacian") -> np.ndarray:
     """K0 (n^3 x 316 n^3): the weighted kernel between unit-cell field nodes and the nodes of
     the 316 well-separated unit cells, block k = columns [k n^3, (k+1) n^3).
 
-    Entry (i, k n^3 + j) = K(|f_i - s_j|) / (w_i w_j) with f at 0.5*nodes and s at
-    offset_k + 0.5*nodes (bbfmm.c:1247-1324), K = 1/r or 1/r^4."""
+    Entry (i, k n^3 + j) = K(s_j - f_i) / (w_i w_j) with f at 0.5*nodes and s at
+    offset_k + 0.5*nodes (bbfmm.c:1247-1324), K = 1/r, x/r^3 or 1/r^4."""
     tab = chebyshev_tables(n)
     h = 0.5 * tab.nodes
     g = np.stack(np.meshgrid(h, h, h, indexing="ij"), axis=-1).reshape(-1, 3)  # (n3, 3)
@@ -145,9 +153,8 @@ def kernel_matrix(n: int, kernel: str = "laplacian") -> np.ndarray:
     K = np.empty((n3, NUM_OFFSETS * n3))
     for k in range(NUM_OFFSETS):
         src = offs[k][None, :] + g                      # (n3, 3)
-        d = g[:, None, :] - src[None, :, :]             # (n3 field, n3 source, 3)
-        r = np.sqrt(np.einsum("fsx,fsx->fs", d, d))
-        K[:, k * n3:(k + 1) * n3] = _kernel_values(kernel, r) / ww
+        d = src[None, :, :] - g[:, None, :]             # (n3 field, n3 source, 3)
+        K[:, k * n3:(k + 1) * n3] = _kernel_values(kernel, d) / ww
     return K
 
 
@@ -156,8 +163,8 @@ def kernel_svd(n: int, rank: int | None = None, kernel: str = "laplacian"):
     column-major blocks flattened, sigma all n^3 singular values.
 
     Restates ``ComputeKernelSVD`` (bbfmm.c:1209-1421): SVD of K0, keep r = n^3/2
-    leading left singular vectors, E_k = U^T K_k U (the kernel is symmetric so the
-    right factor reuses U, bbfmm.c:1384-1405)."""
+    leading left singular vectors, E_k = U^T K_k U (the right factor reuses U,
+    bbfmm.c:1384-1405; for the odd x / r^3 kernel too, see KERNELS)."""
     n3 = n ** 3
     r = n3 // 2 if rank is None else rank
     K0 = kernel_matrix(n, kernel)
@@ -176,9 +183,9 @@ def kernel_svd(n: int, rank: int | None = None, kernel: str = "laplacian"):
 
 def operator_file_names(n: int, single: bool, kernel: str = "laplacian") -> tuple[str, str]:
     """The reference's file names (bbfmm.c:109-144): [s]laplacian{K,U}{n}.bin,
-    [s]oneoverr4{K,U}{n}.bin."""
+    [s]laplacianforce{K,U}{n}.bin, [s]oneoverr4{K,U}{n}.bin."""
     if kernel not in KERNELS:
-        raise ValueError(f"unknown kernel {kernel!r} (laplacian or oneoverr4)")
+        raise ValueError(f"unknown kernel {kernel!r} ({', '.join(KERNELS)})")
     p = "s" if single else ""
     return f"{p}{kernel}K{n}.bin", f"{p}{kernel}U{n}.bin"
 

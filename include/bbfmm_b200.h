@@ -227,11 +227,12 @@ BBFMM_B200_API int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *s, long long cell
 BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
 
 /* Kernel of the solver (the reference's compile-time kernels, bbfmm.c:109-144, 798-849):
- * BBFMM_B200_KERNEL_LAPLACIAN (1/r, the default) or BBFMM_B200_KERNEL_ONEOVERR4 (1/r^4,
- * modes D and S; the operators given at create must be that kernel's, e.g. the reference's
- * oneoverr4{K,U}{n}.bin). It sets the near-field pair value and the per-level scale
- * (1/L_l)^homogeneity after the M2L. BBFMM_B200_KERNEL_LAPLACIAN_FORCE (x / r^3) is
- * antisymmetric and not provided (BBFMM_B200_ERR_UNSUPPORTED). Field solves are for 1/r. */
+ * BBFMM_B200_KERNEL_LAPLACIAN (1/r, the default), BBFMM_B200_KERNEL_LAPLACIAN_FORCE (x / r^3,
+ * x the first component of source - target, homogeneity 2) or BBFMM_B200_KERNEL_ONEOVERR4
+ * (1/r^4, homogeneity 4). The last two run in modes D and S (BBFMM_B200_ERR_UNSUPPORTED in
+ * MIXED mode), and the operators given at create must be that kernel's, e.g. the reference's
+ * laplacianforce{K,U}{n}.bin or oneoverr4{K,U}{n}.bin. It sets the near-field pair value and
+ * the per-level scale (1/L_l)^homogeneity after the M2L. Field solves are for 1/r. */
 #define BBFMM_B200_KERNEL_LAPLACIAN 0
 #define BBFMM_B200_KERNEL_LAPLACIAN_FORCE 1
 #define BBFMM_B200_KERNEL_ONEOVERR4 2

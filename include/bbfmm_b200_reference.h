@@ -16,8 +16,8 @@
  * M2L_EXIT_SUCCESS (0) or M2L_EXIT_FAIL (1) (m2l_drv.h:4-5) and accepts schemes 0-3, all of
  * which run the same B200 M2L. Differences: the tree must be the full uniform octree the
  * reference builds (its lists are implied and not read); dof = 1; the kernels with homogen 1
- * (LAPLACIAN, 1/r) and 4 (ONEOVERR4, 1/r^4; the caller's K and U files must be that kernel's),
- * not LAPLACIANFORCE;
+ * (LAPLACIAN, 1/r), 2 (LAPLACIANFORCE, x/r^3) and 4 (ONEOVERR4, 1/r^4), the caller's K and U
+ * files being that kernel's;
  * void entry points report failures on stderr and through bbfmm_b200_last_error() instead
  * of aborting.
  */

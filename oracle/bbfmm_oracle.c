@@ -64,11 +64,18 @@ typedef double real;
 
 static int pow8(int i) { return 1 << (3 * i); }
 
-/* Kernel: degree of homogeneity 1 (1/r, LAPLACIAN) or 4 (1/r^4, ONEOVERR4); the pair value as
-   the reference's near field forms it from rinv = 1/r (anotherNearField.c:111-124). */
+/* Kernel: degree of homogeneity 1 (1/r, LAPLACIAN), 2 (x / r^3, LAPLACIANFORCE: the x
+   component of the separation source - field over r^3) or 4 (1/r^4, ONEOVERR4); the pair value
+   as the reference's near field forms it from rinv = 1/r and dx = x_s - x_f
+   (anotherNearField.c:111-124). */
 static int g_homogen = 1;
 void SFX(orc_set_kernel)(int homogen) { g_homogen = homogen; }
-static real kern(real rinv) { return g_homogen == 4 ? rinv * rinv * rinv * rinv : rinv; }
+static real kern(real rinv, real dx)
+{
+  if (g_homogen == 4) return rinv * rinv * rinv * rinv;
+  if (g_homogen == 2) return dx * rinv * rinv * rinv;
+  return rinv;
+}
 
 int SFX(orc_ncell)(int maxlev) { return (pow8(maxlev + 1) - 1) / 7; }
 int SFX(orc_levsta)(int level) { return (pow8(level) - 1) / 7; }
@@ -487,7 +494,8 @@ void SFX(orc_downward)(int maxlev, int n, const real *xyz, const real *q, const 
 
 /* -------------------------------------------------------------------- P2P --- */
 
-/* phi[k] += q_k sum_{B in N(A)} sum_{j in B, r != 0} q_j / r  (anotherNearField.c). */
+/* phi[k] += q_k sum_{B in N(A)} sum_{j in B, r != 0} q_j K(x_j - x_k), K = kern() above
+   (anotherNearField.c). */
 void SFX(orc_nearfield)(int maxlev, int N, const real *xyz, const real *q, const int *fieldlist,
                         const int *sta, const int *end, const int *ineigh, const int *neighbors,
                         real *phi)
@@ -514,7 +522,7 @@ void SFX(orc_nearfield)(int maxlev, int N, const real *xyz, const real *q, const
           real dx = x[jsta + j] - fx, dy = y[jsta + j] - fy, dz = z[jsta + j] - fz;
           real rr = dx * dx + dy * dy + dz * dz;
           real rinv = (rr != ZERO ? ONE / SQRT(rr) : ZERO);
-          v += kern(rinv) * qs[jsta + j];
+          v += kern(rinv, dx) * qs[jsta + j];
         }
       }
       p[i] += qs[i] * v;
@@ -558,7 +566,8 @@ void SFX(orc_fmm)(int N, const real *xyz, const real *q, real L, int n, int r, i
   free(neighbors); free(interaction); free(sourceval); free(proxysval); free(PF); free(fieldval);
 }
 
-/* FP64 direct sum on sampled targets: out[t] = q_i sum_{x_j != x_i} q_j / |x_j - x_i|,
+/* FP64 direct sum on sampled targets: out[t] = q_i sum_{x_j != x_i} q_j K(x_j - x_i) (K = 1/r,
+   x/r^3 or 1/r^4 as set by orc_set_kernel),
    i = targets[t], with Neumaier-compensated summation. Positions are given in FP64
    whatever the build precision. */
 void SFX(orc_direct_fp64)(int N, const double *xyz, const double *q, int ntarget,
@@ -572,7 +581,9 @@ void SFX(orc_direct_fp64)(int N, const double *xyz, const double *q, int ntarget
       double dx = xyz[3 * j] - fx, dy = xyz[3 * j + 1] - fy, dz = xyz[3 * j + 2] - fz;
       if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
       double rr = dx * dx + dy * dy + dz * dz;
-      double v = g_homogen == 4 ? q[j] * (1.0 / rr) * (1.0 / rr) : q[j] / sqrt(rr);
+      double v = g_homogen == 4   ? q[j] * (1.0 / rr) * (1.0 / rr)
+                 : g_homogen == 2 ? q[j] * dx / (rr * sqrt(rr))
+                                  : q[j] / sqrt(rr);
       double tsum = s + v;
       if (fabs(s) >= fabs(v)) c += (s - tsum) + v; else c += (v - tsum) + s;
       s = tsum;

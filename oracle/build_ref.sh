@@ -5,6 +5,8 @@
 #
 #   libref_cpu8a_{d,s}.so  default CPU path: sibling-blocking M2L (CPU8A)
 #   libref_cpu9a_{d,s}.so  ij-blocking CPU M2L (CPU9A, the aux_CPU9* family)
+#   libref_cpu8a_d_{r4,force}.so  the 1/r^4 (ONEOVERR4) and x / r^3 (LAPLACIANFORCE) builds
+#   libref_dropin_*.so  the same code with the pass objects taken from the B200 library
 #
 # Flags follow the reference's own recipes (www.sh:23-36, zzz.sh:209-212) with gcc,
 # -fcommon (bbfmm.h defines globals in a header) and gettimeofday timers. BLAS/LAPACK
@@ -48,6 +50,7 @@ build libref_cpu8a_s -DCPU8 -DCPU8A -DSINGLE
 build libref_cpu9a_d -DCPU9 -DCPU9A
 build libref_cpu9a_s -DCPU9 -DCPU9A -DSINGLE
 KDEF=-DONEOVERR4 build libref_cpu8a_d_r4 -DCPU8 -DCPU8A  # the 1/r^4 kernel (homogeneity 4)
+KDEF=-DLAPLACIANFORCE build libref_cpu8a_d_force -DCPU8 -DCPU8A  # x / r^3 (homogeneity 2)
 KDEF=-DLAPLACIAN
 # Drop-in build: the reference's own code with its pass objects (anotherFMMCompute,
 # anotherUpwardPass, anotherFMMInteraction, anotherDownwardPass[X], anotherNearField) left
@@ -56,9 +59,11 @@ LIBDIR="$HERE/../bbfmm_b200/lib"
 if [ -f "$LIBDIR/libbbfmm_b200_ref_d.so" ]; then
   DROP="anotherFMMCompute.c anotherFMMInteraction.c anotherDownwardPassX.c anotherDownwardPass.c
         anotherUpwardPass.c anotherNearField.c"
-  # d, s and the 1/r^4 kernel (ONEOVERR4, double)
-  for var in d s d_r4; do
-    prec=${var%%_*}; kdef=-DLAPLACIAN; [ $var = d_r4 ] && kdef=-DONEOVERR4
+  # d, s, the 1/r^4 kernel (ONEOVERR4, double) and x / r^3 (LAPLACIANFORCE, double)
+  for var in d s d_r4 d_force; do
+    prec=${var%%_*}; kdef=-DLAPLACIAN
+    [ $var = d_r4 ] && kdef=-DONEOVERR4
+    [ $var = d_force ] && kdef=-DLAPLACIANFORCE
     def=""; [ $prec = s ] && def="-DSINGLE"
     objdir="$OUT/obj_dropin_$var"; mkdir -p "$objdir"; objs=""
     for src in $SRCS; do

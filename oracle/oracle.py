@@ -130,8 +130,8 @@ class Oracle:
         return phi
 
     def fmm(self, xyz, q, n, maxlev, U, E, L=1.0, homogen=1):
-        """homogen: the kernel's degree of homogeneity, 1 (1/r) or 4 (1/r^4); U, E must be
-        that kernel's operators."""
+        """homogen: the kernel's degree of homogeneity, 1 (1/r), 2 (x/r^3) or 4 (1/r^4); U, E
+        must be that kernel's operators."""
         xyz = self._arr(xyz).reshape(-1)
         q = self._arr(q)
         N = q.size
@@ -175,21 +175,23 @@ class Oracle:
         return out
 
 
+# File tag of the reference's build for each kernel (oracle/build_ref.sh).
+_KERNEL_TAG = {"laplacian": "", "oneoverr4": "_r4", "laplacianforce": "_force"}
+
+
 def reference_available(prec="d", variant="cpu8a", kernel="laplacian") -> bool:
-    tag = "" if kernel == "laplacian" else "_r4"
-    return os.path.exists(os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{tag}.so"))
+    return os.path.exists(os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{_KERNEL_TAG[kernel]}.so"))
 
 
 class Reference:
     """The reference's own CPU implementation (oracle/_ref, built by build_ref.sh); kernel
-    "oneoverr4" is its -DONEOVERR4 build."""
+    "oneoverr4" is its -DONEOVERR4 build, "laplacianforce" its -DLAPLACIANFORCE build."""
 
     def __init__(self, prec="d", variant="cpu8a", kernel="laplacian"):
         self.prec = prec
         self.dt = np.float64 if prec == "d" else np.float32
         self.R = C.c_double if prec == "d" else C.c_float
-        tag = "" if kernel == "laplacian" else "_r4"
-        path = os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{tag}.so")
+        path = os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{_KERNEL_TAG[kernel]}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run oracle/build_ref.sh")
         self.lib = C.CDLL(path)

@@ -129,8 +129,10 @@ int ref_fmm(int N, real *xyz, real *q, real L, int n, int maxlev, char *Kpath, c
   FMMReadMatrices(K, U, cutoff, n, 1, Kpath, Upath);
   anotherTree *atree;
   anotherBuildFMMHierachy(L, n, 1, maxlev, cutoff, &atree, N, N, (real3 *)xyz, (real3 *)xyz);
-#ifdef ONEOVERR4
+#if defined(ONEOVERR4)
   real homogen = 4;  /* bbfmm.c:133-143 */
+#elif defined(LAPLACIANFORCE)
+  real homogen = 2;  /* bbfmm.c:122-131 */
 #else
   real homogen = 1;
 #endif

@@ -57,9 +57,14 @@ def test_kernel_operator_files_round_trip(tmp_path):
     assert ops.operator_file_names(4, False, "oneoverr4") == ("oneoverr4K4.bin", "oneoverr4U4.bin")
     assert ops.operator_file_names(8, True, "oneoverr4") == ("soneoverr4K8.bin", "soneoverr4U8.bin")
     assert ops.operator_file_names(4, False) == ("laplacianK4.bin", "laplacianU4.bin")
+    assert ops.operator_file_names(4, False, "laplacianforce") == ("laplacianforceK4.bin",
+                                                                   "laplacianforceU4.bin")
     assert ops.homogeneity("laplacian") == 1 and ops.homogeneity("oneoverr4") == 4
+    assert ops.homogeneity("laplacianforce") == 2
+    # kernel ids of bbfmm_b200_set_kernel (include/bbfmm_b200.h)
+    assert [ops.KERNELS[k][1] for k in ("laplacian", "laplacianforce", "oneoverr4")] == [0, 1, 2]
     with pytest.raises(ValueError):
-        ops.operator_file_names(4, False, "laplacianforce")
+        ops.operator_file_names(4, False, "yukawa")
     r4, U4, E4 = ops.load_operators(4, cache_dir=str(tmp_path), kernel="oneoverr4")
     r1, U1, E1 = ops.load_operators(4, cache_dir=str(tmp_path))
     assert r4 == r1 == 32
@@ -69,3 +74,26 @@ def test_kernel_operator_files_round_trip(tmp_path):
     assert not np.allclose(np.abs(E4), np.abs(E1))
     _, Us, _ = ops.load_operators(4, single=True, cache_dir=str(tmp_path), kernel="oneoverr4")
     assert Us.dtype == np.float32 and np.allclose(Us, U4, rtol=1e-6, atol=1e-7)
+
+
+def test_force_kernel_matrix_is_odd_and_compressed_by_one_basis():
+    """x / r^3 (LAPLACIANFORCE) is odd in the separation, so over the symmetric offset set
+    K_{-k} = -K_k^T (to rounding of the node coordinates), and the field-side singular
+    vectors U of [K_0 ... K_315] also capture each K_k's source side: U U^T K_k U U^T keeps
+    K_k to the size of the first dropped singular value, as it does for 1/r."""
+    import numpy as np
+    from bbfmm_b200 import operators as ops
+    n, n3, r = 4, 64, 32
+    offs = [tuple(o) for o in ops.offsets()]
+    for kern in ("laplacianforce", "laplacian"):
+        K0 = ops.kernel_matrix(n, kern)
+        blk = lambda k: K0[:, k * n3:(k + 1) * n3]
+        sign = -1.0 if kern == "laplacianforce" else 1.0
+        for k in (0, 100, 200, 315):
+            mk = offs.index(tuple(-v for v in offs[k]))
+            assert np.allclose(blk(mk), sign * blk(k).T, rtol=1e-12, atol=1e-14 * np.abs(blk(k)).max())
+        U = np.fromiter(ops.kernel_svd(n, kernel=kern)[0], float).reshape(r, n3).T  # (n3, r)
+        _, sv, _ = np.linalg.svd(K0, full_matrices=False)
+        P = U @ U.T
+        worst = max(np.linalg.norm(blk(k) - P @ blk(k) @ P, 2) for k in range(316))
+        assert worst < 2 * sv[r], (kern, worst / sv[r])  # ~0.3; a random basis gives ~300

@@ -224,19 +224,24 @@ def test_tolerance_rank_fp32_matches_fp64_rank():
     assert rel_l2(out["s"], out["d"]) < 2e-5
 
 
-@pytest.mark.parametrize("mode,tol", [("d", 1e-12), ("s", 2e-5)])
-def test_oneoverr4_kernel_matches_oracle(oracle_d, oracle_s, mode, tol):
-    """The 1/r^4 kernel (the reference's ONEOVERR4 build; homogeneity 4: near field
-    q / r^4 and the per-level scale (1/L_l)^4) against the oracle with the same operators."""
+@pytest.mark.parametrize("kernel,mode,tol", [("oneoverr4", "d", 1e-12), ("oneoverr4", "s", 2e-5),
+                                             ("laplacianforce", "d", 1e-12), ("laplacianforce", "s", 1e-4)])
+def test_other_kernels_match_oracle(oracle_d, oracle_s, kernel, mode, tol):
+    """The reference's other kernels against the oracle with the same operators: 1/r^4
+    (ONEOVERR4; homogeneity 4: near field q / r^4 and the per-level scale (1/L_l)^4) and
+    x / r^3 (LAPLACIANFORCE; homogeneity 2: near field q dx / r^3 with dx = x_source -
+    x_target, scale (1/L_l)^2). FP32 tolerance for x / r^3: the FP32 oracle itself is 1.8e-5
+    from the FP64 oracle on this input (odd kernel, cancelling near-field sums), so two FP32
+    summation orders may differ by about that much."""
     import torch
     from bbfmm_b200 import Solver
     from bbfmm_b200 import operators as ops
     single = mode == "s"
-    _, U, E = ops.load_operators(4, single=single, kernel="oneoverr4")
+    _, U, E = ops.load_operators(4, single=single, kernel=kernel)
     x, q = uniform_inputs(30000, seed=17)
     O = oracle_s if single else oracle_d
-    want = O.fmm(x, q, 4, 3, U, E, homogen=4)
-    s = Solver(4, 3, 1.0, mode=mode, kernel="oneoverr4")
+    want = O.fmm(x, q, 4, 3, U, E, homogen=ops.homogeneity(kernel))
+    s = Solver(4, 3, 1.0, mode=mode, kernel=kernel)
     s.set_particles(x)
     dt = torch.float32 if single else torch.float64
     got = s.solve(torch.as_tensor(q, dtype=dt, device="cuda")).double().cpu().numpy()
@@ -244,14 +249,15 @@ def test_oneoverr4_kernel_matches_oracle(oracle_d, oracle_s, mode, tol):
     s.close()
 
 
-def test_oneoverr4_refuses_mixed_and_fields():
+@pytest.mark.parametrize("kernel", ["oneoverr4", "laplacianforce"])
+def test_other_kernels_refuse_mixed_and_fields(kernel):
     import torch
     from bbfmm_b200 import Solver
     from bbfmm_b200._lib import BBFMMError
     with pytest.raises(ValueError):
-        Solver(8, 3, 1.0, mode="mixed", kernel="oneoverr4")
+        Solver(8, 3, 1.0, mode="mixed", kernel=kernel)
     x, q = uniform_inputs(2000, seed=18)
-    s = Solver(4, 3, 1.0, mode="d", kernel="oneoverr4")
+    s = Solver(4, 3, 1.0, mode="d", kernel=kernel)
     s.set_particles(x)
     with pytest.raises(BBFMMError):
         s.solve_fields(torch.as_tensor(q, device="cuda"))

@@ -45,17 +45,17 @@ def test_reference_pipeline_with_b200_passes(prec, lev, tol, opdir):
     assert rel_l2(pd, pr) < tol
 
 
-
-@pytest.mark.skipif(not reference_available("d", "dropin", kernel="oneoverr4"),
-                    reason="1/r^4 drop-in reference build absent")
-def test_reference_pipeline_with_b200_passes_oneoverr4():
-    """The same drop-in check for the reference's -DONEOVERR4 build (homogen 4 through the
-    shims: the near field q / r^4 and the per-level scale (1/L_l)^4), on the operators that
-    build computes itself: 1e-12."""
-    ref = Reference("d", "cpu8a", kernel="oneoverr4")
-    drop = Reference("d", "dropin", kernel="oneoverr4")
+@pytest.mark.parametrize("kernel", ["oneoverr4", "laplacianforce"])
+def test_reference_pipeline_with_b200_passes_other_kernels(kernel):
+    """The same drop-in check for the reference's -DONEOVERR4 and -DLAPLACIANFORCE builds
+    (homogen 4 and 2 through the shims: the near field q / r^4 or q dx / r^3 and the per-level
+    scale (1/L_l)^homogen), on the operators that build computes itself: 1e-12."""
+    if not reference_available("d", "dropin", kernel=kernel):
+        pytest.skip(f"{kernel} drop-in reference build absent")
+    ref = Reference("d", "cpu8a", kernel=kernel)
+    drop = Reference("d", "dropin", kernel=kernel)
     d = tempfile.mkdtemp()
-    kp, up = os.path.join(d, "oneoverr4K4.bin"), os.path.join(d, "oneoverr4U4.bin")
+    kp, up = os.path.join(d, f"{kernel}K4.bin"), os.path.join(d, f"{kernel}U4.bin")
     ref.lib.ref_compute_operators(4, C.c_char_p(kp.encode()), C.c_char_p(up.encode()))
     x, q = uniform_inputs(30000, seed=43)
     pr, Pr, Fr = ref.fmm(x, q, 4, 3, kp, up, want_intermediates=True)
