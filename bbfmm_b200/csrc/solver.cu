@@ -225,9 +225,10 @@ int Solver<T>::alloc_work() {
     const int64_t c = l == maxlev ? leaf_slab() : cells(l);
     if (c > smax[l & 1]) smax[l & 1] = c;
   }
-  for (int b = 0; b < 2; ++b) {
+  for (int b = 0; b < 2; ++b) {  // freed and cleared first: a failed allocation leaves no stale pointer
     if (S[b]) cudaFree(S[b]);
     if (F[b]) cudaFree(F[b]);
+    S[b] = F[b] = nullptr;
     TRY(dalloc(&S[b], (size_t)smax[b] * n3));
     TRY(dalloc(&F[b], (size_t)smax[b] * n3));
   }
@@ -264,6 +265,7 @@ int Solver<T>::alloc_work() {
   }
   if (mode == MODE_MIXED && r == 256) {
     if (Msplit) cudaFree(Msplit);
+    Msplit = nullptr;
     unsigned char *p = nullptr;
     TRY(dalloc(&p, tc_split_bytes(r, tot / r)));
     Msplit = p;
@@ -647,8 +649,12 @@ int bucket(int64_t v) {  // power-of-two bucket
 template <typename T>
 int Solver<T>::autotune(const void *q_dev, int io_double) {
   if (!pos4) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
-  const bool was_timing = timing;
-  timing = false;
+  struct TimingOff {  // stage timing off while tuning, restored on every return path
+    bool &t;
+    const bool was;
+    explicit TimingOff(bool &x) : t(x), was(x) { t = false; }
+    ~TimingOff() { t = was; }
+  } timing_off(timing);
   TRY(upward(q_dev, io_double));
   BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
   for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
@@ -732,7 +738,6 @@ int Solver<T>::autotune(const void *q_dev, int io_double) {
     std::lock_guard<std::mutex> g(g_tune_mutex);
     g_tune_cache[key] = {pick, 0};
   }
-  timing = was_timing;
   BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
   return BBFMM_OK;
 }
