@@ -33,6 +33,18 @@ def _ptr(a):
     return C.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else C.c_void_p(a.data_ptr())
 
 
+def _check_count(what: str, got: int, want: int):
+    """The C-ABI takes bare pointers sized by the particle count it holds: a shorter buffer
+    would be read or written past its end, so sizes are checked here, before any copy."""
+    if got != want:
+        raise ValueError(f"{what} has {got} entries; {want} expected")
+
+
+def _check_out(out, like):
+    if out.dtype != like.dtype or out.device != like.device or out.numel() != like.numel() or not out.is_contiguous():
+        raise ValueError("out must be a contiguous tensor of q's dtype, device and size")
+
+
 class Solver:
     """Device-resident FMM for one particle set.
 
@@ -120,9 +132,11 @@ class Solver:
     def solve(self, q, out=None):
         """q: CUDA tensor (N,) -> q_i * phi_i as a CUDA tensor, on the solver's stream."""
         torch = self.torch
+        _check_count("q", q.numel(), self.N)
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         if out is None:
             out = torch.empty_like(q)
+        _check_out(out, q)
         # order the solver's stream after the caller's work on q, and the caller's stream
         # after the solve: both buffers belong to the caller's stream, which cannot reuse
         # them before the solve has finished with them
@@ -141,6 +155,7 @@ class Solver:
         """q: CUDA tensor (N,) -> (pot, field): pot_i = sum_j q_j / r_ij and field = grad pot
         at every particle, (N,) and (N, 3) CUDA tensors (field None unless want_field)."""
         torch = self.torch
+        _check_count("q", q.numel(), self.N)
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         pot = torch.empty_like(q)
         fld = torch.empty((q.numel(), 3), dtype=self.dtype, device=q.device) if want_field else None
@@ -160,6 +175,7 @@ class Solver:
         """Host charges -> host q_i * phi_i (copies in, solves, copies out, synchronises).
         out: an optional host array of the same size (pinned memory makes the copy direct)."""
         q = np.ascontiguousarray(np.asarray(q, dtype=self.np_dtype))
+        _check_count("q", q.size, self.N)
         phi = np.empty_like(q) if out is None else out
         if phi.dtype != self.np_dtype or phi.size != q.size or not phi.flags.c_contiguous:
             raise ValueError("out must be a contiguous array of the solver's dtype and q's size")
@@ -178,6 +194,7 @@ class Solver:
     def autotune(self, q):
         """Time the per-level M2L and near-field launch choices on this tree (an upward pass
         with charges q, a CUDA tensor) and keep the fastest; returns the choices."""
+        _check_count("q", q.numel(), self.N)
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         self.torch.cuda.synchronize(q.device)
         _lib.check(_lib.lib().bbfmm_b200_autotune(self.h, C.c_void_p(q.data_ptr())))
@@ -305,9 +322,11 @@ class Batch:
     def solve(self, q, out=None, graph: bool = True):
         """q: CUDA tensor (N_total,) -> q_i * phi_i of every set (same layout)."""
         torch = self.torch
+        _check_count("q", q.numel(), self.N)
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         if out is None:
             out = torch.empty_like(q)
+        _check_out(out, q)
         caller, mine = self._order(q)
         _lib.check(_lib.lib().bbfmm_b200_batch_solve(self.h, C.c_void_p(q.data_ptr()), C.c_void_p(out.data_ptr()),
                                                       int(graph)))
@@ -326,6 +345,7 @@ class Batch:
         _lib.check(_lib.lib().bbfmm_b200_set_leaf_slab(self.h, int(cells)))
 
     def autotune(self, q):
+        _check_count("q", q.numel(), self.N)
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         self.torch.cuda.synchronize(q.device)
         _lib.check(_lib.lib().bbfmm_b200_batch_autotune(self.h, C.c_void_p(q.data_ptr())))
@@ -343,6 +363,7 @@ class Batch:
 
     def group_stage_times(self, q, g: int):
         """Stage times (ms) of group g solved alone (q: CUDA tensor of all sets)."""
+        _check_count("q", q.numel(), self.N)
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         out = self.torch.empty_like(q)
         ms = (C.c_float * len(_lib.STAGES))()
@@ -355,6 +376,16 @@ class Batch:
         return int(_lib.lib().bbfmm_b200_batch_graph_nodes(self.h))
 
 
+def _check_direct(xyz, q, targets):
+    """Sizes, devices and target indices of a direct sum: the kernel reads xyz[3 t + k] and
+    q[t] for every target t, so each must lie in [0, N)."""
+    _check_count("xyz", xyz.numel(), 3 * q.numel())
+    if not (xyz.device == q.device == targets.device) or q.device.type != "cuda":
+        raise ValueError("xyz, q and targets must be CUDA tensors on one device")
+    if targets.numel() and (int(targets.min()) < 0 or int(targets.max()) >= q.numel()):
+        raise ValueError("targets must be particle indices in [0, N)")
+
+
 def direct(xyz, q, targets, stream=None):
     """FP64 direct sum q_i sum_{j != i} q_j / r_ij on the GPU for the given targets
     (torch CUDA tensors: xyz (N,3) float64, q (N,) float64, targets (T,) int32)."""
@@ -362,6 +393,7 @@ def direct(xyz, q, targets, stream=None):
     xyz = xyz.to(torch.float64).contiguous()
     q = q.to(torch.float64).contiguous()
     targets = targets.to(torch.int32).contiguous()
+    _check_direct(xyz, q, targets)
     out = torch.empty(targets.numel(), dtype=torch.float64, device=q.device)
     st = torch.cuda.current_stream(q.device).cuda_stream if stream is None else stream
     _lib.check(_lib.lib().bbfmm_b200_direct(q.numel(), C.c_void_p(xyz.data_ptr()), C.c_void_p(q.data_ptr()),
@@ -377,6 +409,7 @@ def direct_field(xyz, q, targets, stream=None):
     xyz = xyz.to(torch.float64).contiguous()
     q = q.to(torch.float64).contiguous()
     targets = targets.to(torch.int32).contiguous()
+    _check_direct(xyz, q, targets)
     pot = torch.empty(targets.numel(), dtype=torch.float64, device=q.device)
     fld = torch.empty((targets.numel(), 3), dtype=torch.float64, device=q.device)
     st = torch.cuda.current_stream(q.device).cuda_stream if stream is None else stream

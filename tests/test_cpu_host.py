@@ -97,3 +97,32 @@ def test_force_kernel_matrix_is_odd_and_compressed_by_one_basis():
         P = U @ U.T
         worst = max(np.linalg.norm(blk(k) - P @ blk(k) @ P, 2) for k in range(316))
         assert worst < 2 * sv[r], (kern, worst / sv[r])  # ~0.3; a random basis gives ~300
+
+
+def test_python_api_checks_buffer_sizes_before_the_c_abi():
+    """The C-ABI takes bare pointers sized by the particle count the solver holds: the Python
+    layer refuses shorter or longer charge arrays before any copy or launch (a bare solver
+    object stands in for one on a GPU; nothing reaches the library)."""
+    import torch
+    from bbfmm_b200 import Batch, Solver
+    from bbfmm_b200.fmm import direct
+    s = Solver.__new__(Solver)
+    s.torch, s.N, s.device, s.dtype, s.np_dtype, s.h = torch, 100, 0, torch.float64, np.float64, None
+    for bad in (99, 101):
+        with pytest.raises(ValueError, match="q has"):
+            s.solve(torch.zeros(bad, dtype=torch.float64))
+        with pytest.raises(ValueError, match="q has"):
+            s.solve_fields(torch.zeros(bad, dtype=torch.float64))
+        with pytest.raises(ValueError, match="q has"):
+            s.solve_host(np.zeros(bad))
+        with pytest.raises(ValueError, match="q has"):
+            s.autotune(torch.zeros(bad, dtype=torch.float64))
+    b = Batch.__new__(Batch)
+    b.torch, b.N, b.device, b.dtype, b.h = torch, 50, 0, torch.float64, None
+    with pytest.raises(ValueError, match="q has"):
+        b.solve(torch.zeros(49, dtype=torch.float64))
+    x, q, t = torch.zeros(10, 3, dtype=torch.float64), torch.zeros(10, dtype=torch.float64), torch.zeros(2)
+    with pytest.raises(ValueError, match="xyz has"):
+        direct(x[:9], q, t)
+    with pytest.raises(ValueError, match="CUDA tensors"):
+        direct(x, q, t)
