@@ -106,9 +106,15 @@ int load_particles(Solver<T> &s, Tree<T> *t, const Real3<T> *xyz) {
   std::vector<int> ls(nl + 1);
   for (int64_t k = 0; k < nl; ++k) ls[k] = t->c->fieldsta[A0 + k];
   ls[nl] = N;
+  if (N < 0 || (N > 0 && (!t->fieldlist || !xyz)) || ls[0] != 0)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "tree particle arrays missing or not starting at leaf 0");
   for (int64_t k = 0; k < nl; ++k)
-    if (t->c->fieldend[A0 + k] - t->c->fieldsta[A0 + k] + 1 != ls[k + 1] - ls[k])
+    if (ls[k + 1] < ls[k] || t->c->fieldend[A0 + k] - t->c->fieldsta[A0 + k] + 1 != ls[k + 1] - ls[k])
       return bbfmm_set_error(BBFMM_ERR_ARG, "leaf particle ranges are not contiguous in leaf order");
+  // the device gathers positions and charges through fieldlist: every entry must index a particle
+  for (int i = 0; i < N; ++i)
+    if (t->fieldlist[i] < 0 || t->fieldlist[i] >= N)
+      return bbfmm_set_error(BBFMM_ERR_ARG, "fieldlist entry outside [0, Nf)");
   return s.set_particles_sorted(N, t->fieldlist, ls.data(), reinterpret_cast<const T *>(xyz));
 }
 
