@@ -22,6 +22,9 @@
  *   P2P            anotherNearField.c:141-206 (CPU8A) and 219-316 (driver)
  *   direct         bbfmm.c:880-913 semantics (q_i * sum_{x_j != x_i} q_j / r_ij),
  *                  evaluated here in FP64 with compensated summation on sampled targets.
+ *   kernels        1/r (LAPLACIAN), x/r^3 (LAPLACIANFORCE) and 1/r^4 (ONEOVERR4):
+ *                  bbfmm.c:109-144 (homogeneity), anotherNearField.c:111-124 (pair value),
+ *                  selected at run time by orc_set_kernel.
  *
  * Compiled twice: -DORC_SINGLE gives real = float (the reference's SINGLE build),
  * otherwise real = double. Every exported symbol carries the suffix _s or _d.

@@ -6,7 +6,9 @@ TEST INFRASTRUCTURE ONLY. Tests, ``__graft_entry__.smoke()`` and the CPU-baselin
 * ``Oracle(prec)``      -- our CPU restatement, ``prec`` in {"d", "s"}.
 * ``Reference(prec, variant)`` -- the reference's own CPU code built from its sources by
   ``oracle/build_ref.sh`` into ``oracle/_ref/`` (variant "cpu8a" = default sibling-blocking
-  M2L, "cpu9a" = ij-blocking CPU M2L). Present only where that build ran.
+  M2L, "cpu9a" = ij-blocking CPU M2L, "dropin" = the same code with its pass objects taken
+  from the B200 library; ``kernel`` "oneoverr4" / "laplacianforce" for the -DONEOVERR4 /
+  -DLAPLACIANFORCE builds). Present only where that build ran.
 """
 from __future__ import annotations
 
