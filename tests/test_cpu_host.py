@@ -7,7 +7,7 @@ from bbfmm_b200.fmm import reference_depth
 
 
 def test_reference_depth_formula():
-    # (int)log(N)/log(8) binds the cast to log(N) only (bbfmm.c:151-160; SURVEY F4)
+    # (int)log(N)/log(8) binds the cast to log(N) only (bbfmm.c:151-160)
     assert reference_depth(32768) == 3 and reference_depth(32768, 1) == 4
     assert reference_depth(4194304) == 6 and reference_depth(4194304, 1) == 7
     assert reference_depth(10) == 2 and reference_depth(1) == 2
