@@ -25,6 +25,7 @@ the left singular vectors are taken from an R factor of the transposed kernel ma
 """
 from __future__ import annotations
 
+import io
 import os
 import struct
 from dataclasses import dataclass
@@ -190,6 +191,16 @@ def operator_file_names(n: int, single: bool, kernel: str = "laplacian") -> tupl
     return f"{p}{kernel}K{n}.bin", f"{p}{kernel}U{n}.bin"
 
 
+def _write_atomic(path: str, *chunks: bytes):
+    """Write a file under a private name, then rename it into place: processes that share the
+    cache (one per GPU) see either no file or a complete one."""
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "wb") as f:
+        for c in chunks:
+            f.write(c)
+    os.replace(tmp, path)
+
+
 def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarray, single: bool,
                          kernel: str = "laplacian"):
     """Write ``[s]<kernel>{K,U}{n}.bin`` in the reference layout (bbfmm.c:1361-1405)."""
@@ -197,11 +208,8 @@ def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarra
     kname, uname = operator_file_names(n, single, kernel)
     dt = np.float32 if single else np.float64
     r = Ucol.size // n ** 3
-    with open(os.path.join(dirpath, uname), "wb") as f:
-        f.write(struct.pack("i", r))
-        f.write(np.asarray(Ucol, dtype=dt).tobytes())
-    with open(os.path.join(dirpath, kname), "wb") as f:
-        f.write(np.asarray(Ecol, dtype=dt).tobytes())
+    _write_atomic(os.path.join(dirpath, uname), struct.pack("i", r), np.asarray(Ucol, dtype=dt).tobytes())
+    _write_atomic(os.path.join(dirpath, kname), np.asarray(Ecol, dtype=dt).tobytes())
 
 
 def read_operator_files(dirpath: str, n: int, single: bool, kernel: str = "laplacian"):
@@ -236,7 +244,9 @@ def singular_values(n: int, cache_dir: str | None = None, kernel: str = "laplaci
     sv = np.linalg.svd(R.T, compute_uv=False)
     sv = sv / sv[0]
     os.makedirs(cache_dir, exist_ok=True)
-    np.save(path, sv)
+    buf = io.BytesIO()
+    np.save(buf, sv)
+    _write_atomic(path, buf.getvalue())
     return sv
 
 

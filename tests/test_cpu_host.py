@@ -126,3 +126,15 @@ def test_python_api_checks_buffer_sizes_before_the_c_abi():
         direct(x[:9], q, t)
     with pytest.raises(ValueError, match="CUDA tensors"):
         direct(x, q, t)
+
+
+def test_operator_cache_is_written_atomically(tmp_path):
+    """Files appear complete or not at all (rename into place), and no temporaries remain."""
+    from bbfmm_b200 import operators as ops
+    r, U, E = ops.load_operators(4, single=True, cache_dir=str(tmp_path))
+    sv = ops.singular_values(4, cache_dir=str(tmp_path))
+    names = sorted(p.name for p in tmp_path.iterdir())
+    assert names == ["laplacianK4.bin", "laplacianU4.bin", "sigma4.npy", "slaplacianK4.bin", "slaplacianU4.bin"]
+    assert np.array_equal(ops.singular_values(4, cache_dir=str(tmp_path)), sv) and sv[0] == 1.0
+    r2, U2, E2 = ops.read_operator_files(str(tmp_path), 4, True)
+    assert r2 == r == 32 and np.array_equal(U2, U) and np.array_equal(E2, E)
