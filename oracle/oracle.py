@@ -193,6 +193,7 @@ class Reference:
         self.prec = prec
         self.dt = np.float64 if prec == "d" else np.float32
         self.R = C.c_double if prec == "d" else C.c_float
+        self.kernel = kernel
         path = os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{_KERNEL_TAG[kernel]}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run oracle/build_ref.sh")
@@ -203,10 +204,10 @@ class Reference:
         return np.ascontiguousarray(a, dtype=self.dt)
 
     def compute_operators(self, n, dirpath):
-        from_names = {"d": ("laplacianK%d.bin", "laplacianU%d.bin"),
-                      "s": ("slaplacianK%d.bin", "slaplacianU%d.bin")}[self.prec]
-        kp = os.path.join(dirpath, from_names[0] % n).encode()
-        up = os.path.join(dirpath, from_names[1] % n).encode()
+        """The reference's own SVD (ComputeKernelSVD) into [s]<kernel>{K,U}{n}.bin."""
+        pre = ("s" if self.prec == "s" else "") + self.kernel
+        kp = os.path.join(dirpath, f"{pre}K{n}.bin").encode()
+        up = os.path.join(dirpath, f"{pre}U{n}.bin").encode()
         os.makedirs(dirpath, exist_ok=True)
         self.lib.ref_compute_operators(n, C.c_char_p(kp), C.c_char_p(up))
         return kp.decode(), up.decode()

@@ -1,7 +1,9 @@
 """Generates the golden fixtures in tests/golden/ from the REFERENCE CPU code built from its
 own sources by oracle/build_ref.sh (oracle/_ref). Run once where the reference is present:
 
-    oracle/build_ref.sh && python tests/golden/make_golden.py
+    oracle/build_ref.sh && python tests/golden/make_golden.py            # everything
+    oracle/build_ref.sh && python tests/golden/make_golden.py kernels    # add the kernel
+                                                                         # fixtures only
 
 Fixtures (all produced by the reference itself):
   refU4_d.bin, refU4_s.bin, refU8_d.bin  U files of the reference's own SVD
@@ -13,6 +15,9 @@ Fixtures (all produced by the reference itself):
       arithmetic with FP64 sums), reference inputs, N = 32768, and the first 32 values
       of the reference FMM output for n = 4, depth 3, d
     * the reference direct code's output at 64 fixed targets (N = 32768, d)
+  For the reference's -DONEOVERR4 and -DLAPLACIANFORCE builds (d, n = 4, N = 32768, depth 3):
+  refU4_d_<kernel>.bin (its U file), and in golden.json kat_d_n4_l3_<kernel>,
+  fmm_d_n4_l3_<kernel>_first32 and direct_d_N32768_<kernel>_first64.
 """
 import hashlib
 import json
@@ -77,9 +82,40 @@ def main():
                 print(prec, n, lev, out[f"kat_{prec}_n{n}_l{lev}"], flush=True)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+    kernel_fixtures(out)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1)
 
 
+def kernel_fixtures(out):
+    """Known answers of the reference's other kernels (1/r^4, x/r^3), FP64, n = 4, depth 3."""
+    tmp = tempfile.mkdtemp()
+    try:
+        for kernel in ("oneoverr4", "laplacianforce"):
+            R = Reference("d", kernel=kernel)
+            kp, up = R.compute_operators(4, tmp)
+            shutil.copy(up, os.path.join(HERE, f"refU4_d_{kernel}.bin"))
+            xyz, q = R.set_sources(32768)
+            pd = R.direct(xyz, q)
+            phi = R.fmm(xyz, q, 4, 3, kp, up)
+            out[f"kat_d_n4_l3_{kernel}"] = rel_l2(phi, pd)
+            out[f"fmm_d_n4_l3_{kernel}_first32"] = [float(v).hex() for v in phi[:32]]
+            out[f"direct_d_N32768_{kernel}_first64"] = [float(v).hex() for v in pd[:64]]
+            print(kernel, out[f"kat_d_n4_l3_{kernel}"], flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def add_kernel_fixtures():
+    path = os.path.join(HERE, "golden.json")
+    out = json.load(open(path))
+    kernel_fixtures(out)
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["kernels"]:
+        add_kernel_fixtures()
+    else:
+        main()

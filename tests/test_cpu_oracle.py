@@ -27,16 +27,17 @@ def _hexarr(v, dt):
     return np.array([float.fromhex(x) for x in v]).astype(dt)
 
 
-def ref_operators(n, prec):
+def ref_operators(n, prec, kernel="laplacian"):
     """U from the reference's own SVD file; E = U^T K_k U in FP64 (bbfmm.c:1384-1405)."""
     from bbfmm_b200 import operators as ops
     dt = np.float64 if prec == "d" else np.float32
-    raw = open(os.path.join(GOLD, f"refU{n}_{prec}.bin"), "rb").read()
+    tag = "" if kernel == "laplacian" else f"_{kernel}"
+    raw = open(os.path.join(GOLD, f"refU{n}_{prec}{tag}.bin"), "rb").read()
     r = struct.unpack("i", raw[:4])[0]
     Ucol = np.frombuffer(raw[4:], dtype=dt).astype(np.float64)
     n3 = n ** 3
     U = Ucol.reshape(r, n3).T
-    K0 = ops.kernel_matrix(n)
+    K0 = ops.kernel_matrix(n, kernel)
     E = np.stack([U.T @ K0[:, k * n3:(k + 1) * n3] @ U for k in range(316)])
     Ecol = np.ascontiguousarray(E.transpose(0, 2, 1)).reshape(-1)
     return Ucol.astype(dt), Ecol.astype(dt)
@@ -88,3 +89,22 @@ def test_known_answers(n, lev, prec, rtol, oracle_d, oracle_s):
     if (n, lev, prec) == (4, 3, "d"):
         first = _hexarr(G["fmm_d_n4_l3_first32"], np.float64)
         assert rel_l2(phi[:32], first) < 1e-10
+
+
+@pytest.mark.parametrize("kernel", ["oneoverr4", "laplacianforce"])
+def test_known_answers_other_kernels(kernel, oracle_d):
+    """The reference's -DONEOVERR4 and -DLAPLACIANFORCE builds on their own particles (N =
+    32768, n = 4, depth 3, their own U files): the oracle's direct sum and FMM reproduce the
+    reference's direct values, FMM values and FMM-vs-direct error. Measured: FMM values equal
+    to 1e-16, direct values to 1e-15, the error to 2e-9 relative (1/r^4, whose error of 2e-9
+    is itself near rounding: the near field dominates the norm) and 1e-14 (x/r^3)."""
+    from bbfmm_b200 import operators as ops
+    U, E = ref_operators(4, "d", kernel)
+    h = ops.homogeneity(kernel)
+    xyz, q = oracle_d.ref_sources(32768)
+    phi = oracle_d.fmm(xyz, q, 4, 3, U, E, homogen=h)
+    assert rel_l2(phi[:32], _hexarr(G[f"fmm_d_n4_l3_{kernel}_first32"], np.float64)) < 1e-13
+    dref = oracle_d.direct_fp64(xyz, q, np.arange(32768), homogen=h)
+    assert rel_l2(dref[:64], _hexarr(G[f"direct_d_N32768_{kernel}_first64"], np.float64)) < 1e-13
+    want = G[f"kat_d_n4_l3_{kernel}"]
+    assert abs(rel_l2(phi, dref) - want) <= 1e-7 * want
