@@ -119,3 +119,24 @@ def test_oracle_equals_reference_laplacianforce(oracle_d, lev):
     # the kernel matters: the 1/r operators with the x / r^3 near field and scale are wrong
     _, Ul, El = ops.load_operators(4, single=False)
     assert rel_l2(oracle_d.fmm(x, q, 4, lev, Ul, El, homogen=2)[tg], dref) > 50 * e_ref
+
+
+@pytest.mark.parametrize("kernel", ["oneoverr4", "laplacianforce"])
+@pytest.mark.parametrize("lev", [3, 4])
+def test_fp32_oracle_equals_fp32_reference_other_kernels(oracle_s, kernel, lev):
+    """The FP32 oracle (the checker of the GPU's FP32 solve) against the reference's -DSINGLE
+    builds of the 1/r^4 and x / r^3 kernels on their own operators: relative L2 < 1e-6
+    (measured 5e-12 and 2e-8: summation order)."""
+    from bbfmm_b200 import operators as ops
+    if not reference_available("s", kernel=kernel):
+        pytest.skip(f"FP32 {kernel} reference build absent")
+    R = Reference("s", "cpu8a", kernel=kernel)
+    kp, up = R.compute_operators(4, tempfile.mkdtemp())
+    U = np.fromfile(up, dtype=np.float32, offset=4)
+    E = np.fromfile(kp, dtype=np.float32)
+    rng = np.random.default_rng(6)
+    x = (rng.random((20000, 3)) - 0.5).astype(np.float32)
+    q = rng.uniform(-1, 1, 20000).astype(np.float32)
+    phir = R.fmm(x, q, 4, lev, kp, up)
+    phio = oracle_s.fmm(x, q, 4, lev, U, E, homogen=ops.homogeneity(kernel))
+    assert rel_l2(phio, phir) < 1e-6
