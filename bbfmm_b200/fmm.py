@@ -421,14 +421,15 @@ def direct_field(xyz, q, targets, stream=None):
 
 
 def bbfmm(xyz, q, L: float = 1.0, n: int = 4, level_modifier: int = 0, mode: str = "d", maxlev=None,
-          operators=None):
-    """One solve from host arrays, like the reference's ``bbfmm()`` with field = source.
+          operators=None, kernel: str = "laplacian"):
+    """One solve from host arrays, like the reference's ``bbfmm()`` with field = source; the
+    kernel, a compile-time choice there (bbfmm.c:109-144), is an argument here.
 
     Returns q_i * phi_i in the input order."""
     xyz = np.asarray(xyz)
     N = xyz.shape[0]
     lev = maxlev if maxlev is not None else reference_depth(N, level_modifier)
-    s = Solver(n, lev, L, mode=mode, operators=operators)
+    s = Solver(n, lev, L, mode=mode, operators=operators, kernel=kernel)
     try:
         s.set_particles(xyz)
         return s.solve_host(q)
