@@ -182,13 +182,20 @@ def kernel_svd(n: int, rank: int | None = None, kernel: str = "laplacian"):
     return Ucol, Ecol, s
 
 
-def operator_file_names(n: int, single: bool, kernel: str = "laplacian") -> tuple[str, str]:
-    """The reference's file names (bbfmm.c:109-144): [s]laplacian{K,U}{n}.bin,
-    [s]laplacianforce{K,U}{n}.bin, [s]oneoverr4{K,U}{n}.bin."""
+def operator_file_names(n: int, single: bool, kernel: str = "laplacian", ascii: bool = False) -> tuple[str, str]:
+    """The reference's file names (bbfmm.c:96-144): [s]laplacian{K,U}{n}.bin,
+    [s]laplacianforce{K,U}{n}.bin, [s]oneoverr4{K,U}{n}.bin; extension .out for the text
+    form of its ENABLE_ASCII_IO builds."""
     if kernel not in KERNELS:
         raise ValueError(f"unknown kernel {kernel!r} ({', '.join(KERNELS)})")
     p = "s" if single else ""
-    return f"{p}{kernel}K{n}.bin", f"{p}{kernel}U{n}.bin"
+    ext = "out" if ascii else "bin"
+    return f"{p}{kernel}K{n}.{ext}", f"{p}{kernel}U{n}.{ext}"
+
+
+def _ascii_lines(values) -> bytes:
+    # one "%18.12e" line per value, as the reference's fprintf (bbfmm.c:1366-1370, 1398-1400)
+    return "".join("%18.12e\n" % v for v in np.asarray(values, np.float64).tolist()).encode()
 
 
 def _write_atomic(path: str, *chunks: bytes):
@@ -202,20 +209,39 @@ def _write_atomic(path: str, *chunks: bytes):
 
 
 def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarray, single: bool,
-                         kernel: str = "laplacian"):
-    """Write ``[s]<kernel>{K,U}{n}.bin`` in the reference layout (bbfmm.c:1361-1405)."""
+                         kernel: str = "laplacian", ascii: bool = False):
+    """Write ``[s]<kernel>{K,U}{n}.bin`` in the reference layout (bbfmm.c:1361-1405); with
+    ``ascii`` the text form ``.out`` of its ENABLE_ASCII_IO builds (the cutoff, then one value
+    per line; values rounded to 13 significant digits, as that form holds them)."""
     os.makedirs(dirpath, exist_ok=True)
-    kname, uname = operator_file_names(n, single, kernel)
+    kname, uname = operator_file_names(n, single, kernel, ascii)
     dt = np.float32 if single else np.float64
     r = Ucol.size // n ** 3
-    _write_atomic(os.path.join(dirpath, uname), struct.pack("i", r), np.asarray(Ucol, dtype=dt).tobytes())
-    _write_atomic(os.path.join(dirpath, kname), np.asarray(Ecol, dtype=dt).tobytes())
+    U = np.asarray(Ucol, dtype=dt)
+    E = np.asarray(Ecol, dtype=dt)
+    if ascii:
+        _write_atomic(os.path.join(dirpath, uname), b"%d\n" % r, _ascii_lines(U))
+        _write_atomic(os.path.join(dirpath, kname), _ascii_lines(E))
+        return
+    _write_atomic(os.path.join(dirpath, uname), struct.pack("i", r), U.tobytes())
+    _write_atomic(os.path.join(dirpath, kname), E.tobytes())
 
 
-def read_operator_files(dirpath: str, n: int, single: bool, kernel: str = "laplacian"):
-    """Read ``[s]<kernel>{K,U}{n}.bin`` (bbfmm.c:216-254). Returns (r, Ucol, Ecol)."""
-    kname, uname = operator_file_names(n, single, kernel)
+def read_operator_files(dirpath: str, n: int, single: bool, kernel: str = "laplacian", ascii: bool = False):
+    """Read ``[s]<kernel>{K,U}{n}.bin`` (bbfmm.c:216-254), or with ``ascii`` the ``.out`` text
+    form of the reference's ENABLE_ASCII_IO builds. Returns (r, Ucol, Ecol)."""
+    kname, uname = operator_file_names(n, single, kernel, ascii)
     dt = np.float32 if single else np.float64
+    if ascii:
+        u = open(os.path.join(dirpath, uname)).read().split()
+        r = int(u[0])
+        # text to FP64, then to the file's precision, as fscanf "%f" / "%lf" read it
+        Ucol = np.array(u[1:1 + n ** 3 * r], dtype=np.float64).astype(dt)
+        e = open(os.path.join(dirpath, kname)).read().split()
+        Ecol = np.array(e[:NUM_OFFSETS * r * r], dtype=np.float64).astype(dt)
+        if Ucol.size != n ** 3 * r or Ecol.size != NUM_OFFSETS * r * r:
+            raise ValueError("operator text files are shorter than their cutoff implies")
+        return r, Ucol, Ecol
     with open(os.path.join(dirpath, uname), "rb") as f:
         r = struct.unpack("i", f.read(4))[0]
         Ucol = np.frombuffer(f.read(), dtype=dt, count=n ** 3 * r).copy()

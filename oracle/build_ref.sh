@@ -6,6 +6,7 @@
 #   libref_cpu8a_{d,s}.so  default CPU path: sibling-blocking M2L (CPU8A)
 #   libref_cpu9a_{d,s}.so  ij-blocking CPU M2L (CPU9A, the aux_CPU9* family)
 #   libref_cpu8a_{d,s}_{r4,force}.so  the 1/r^4 (ONEOVERR4) and x / r^3 (LAPLACIANFORCE) builds
+#   libref_cpu8a_ascii_d.so  the ENABLE_ASCII_IO build (operator files as text)
 #   libref_dropin_*.so  the same code with the pass objects taken from the B200 library
 #
 # Flags follow the reference's own recipes (www.sh:23-36, zzz.sh:209-212) with gcc,
@@ -53,6 +54,7 @@ KDEF=-DONEOVERR4 build libref_cpu8a_d_r4 -DCPU8 -DCPU8A  # the 1/r^4 kernel (hom
 KDEF=-DONEOVERR4 build libref_cpu8a_s_r4 -DCPU8 -DCPU8A -DSINGLE
 KDEF=-DLAPLACIANFORCE build libref_cpu8a_d_force -DCPU8 -DCPU8A  # x / r^3 (homogeneity 2)
 KDEF=-DLAPLACIANFORCE build libref_cpu8a_s_force -DCPU8 -DCPU8A -DSINGLE
+build libref_cpu8a_ascii_d -DCPU8 -DCPU8A -DENABLE_ASCII_IO  # operator files as text (.out)
 KDEF=-DLAPLACIAN
 # Drop-in build: the reference's own code with its pass objects (anotherFMMCompute,
 # anotherUpwardPass, anotherFMMInteraction, anotherDownwardPass[X], anotherNearField) left

@@ -6,8 +6,8 @@ TEST INFRASTRUCTURE ONLY. Tests, ``__graft_entry__.smoke()`` and the CPU-baselin
 * ``Oracle(prec)``      -- our CPU restatement, ``prec`` in {"d", "s"}.
 * ``Reference(prec, variant)`` -- the reference's own CPU code built from its sources by
   ``oracle/build_ref.sh`` into ``oracle/_ref/`` (variant "cpu8a" = default sibling-blocking
-  M2L, "cpu9a" = ij-blocking CPU M2L, "dropin" = the same code with its pass objects taken
-  from the B200 library; ``kernel`` "oneoverr4" / "laplacianforce" for the -DONEOVERR4 /
+  M2L, "cpu9a" = ij-blocking CPU M2L, "cpu8a_ascii" = its operator files as text, "dropin" =
+  the same code with its pass objects taken from the B200 library; ``kernel`` "oneoverr4" / "laplacianforce" for the -DONEOVERR4 /
   -DLAPLACIANFORCE builds). Present only where that build ran.
 """
 from __future__ import annotations
@@ -193,7 +193,7 @@ class Reference:
         self.prec = prec
         self.dt = np.float64 if prec == "d" else np.float32
         self.R = C.c_double if prec == "d" else C.c_float
-        self.kernel = kernel
+        self.kernel, self.variant = kernel, variant
         path = os.path.join(HERE, "_ref", f"libref_{variant}_{prec}{_KERNEL_TAG[kernel]}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run oracle/build_ref.sh")
@@ -204,10 +204,12 @@ class Reference:
         return np.ascontiguousarray(a, dtype=self.dt)
 
     def compute_operators(self, n, dirpath):
-        """The reference's own SVD (ComputeKernelSVD) into [s]<kernel>{K,U}{n}.bin."""
+        """The reference's own SVD (ComputeKernelSVD) into [s]<kernel>{K,U}{n}.bin (.out, as
+        text, for the ENABLE_ASCII_IO build)."""
         pre = ("s" if self.prec == "s" else "") + self.kernel
-        kp = os.path.join(dirpath, f"{pre}K{n}.bin").encode()
-        up = os.path.join(dirpath, f"{pre}U{n}.bin").encode()
+        ext = "out" if self.variant.endswith("ascii") else "bin"
+        kp = os.path.join(dirpath, f"{pre}K{n}.{ext}").encode()
+        up = os.path.join(dirpath, f"{pre}U{n}.{ext}").encode()
         os.makedirs(dirpath, exist_ok=True)
         self.lib.ref_compute_operators(n, C.c_char_p(kp), C.c_char_p(up))
         return kp.decode(), up.decode()

@@ -122,8 +122,14 @@ int ref_fmm(int N, real *xyz, real *q, real L, int n, int maxlev, char *Kpath, c
   ComputeWeights(Tkz, Ktable, Kweights, Cweights, n);
   FILE *f = fopen(Upath, "rb");
   if (!f) { harness_end(); return 1; }
+#ifdef ENABLE_ASCII_IO
+  /* the text form starts with the cutoff on its own line (bbfmm.c:1361-1364) */
+  if (fscanf(f, "%d", &cutoff) != 1) { fclose(f); harness_end(); return 1; }
+#else
   if (fread(&cutoff, sizeof(int), 1, f) != 1) { fclose(f); harness_end(); return 1; }
+#endif
   fclose(f);
+  if (cutoff < 1 || cutoff > n3) { harness_end(); return 1; }
   real *K = (real *)malloc((size_t)316 * cutoff * cutoff * sizeof(real));
   real *U = (real *)malloc((size_t)cutoff * n3 * sizeof(real));
   FMMReadMatrices(K, U, cutoff, n, 1, Kpath, Upath);

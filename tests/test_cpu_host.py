@@ -138,3 +138,21 @@ def test_operator_cache_is_written_atomically(tmp_path):
     assert np.array_equal(ops.singular_values(4, cache_dir=str(tmp_path)), sv) and sv[0] == 1.0
     r2, U2, E2 = ops.read_operator_files(str(tmp_path), 4, True)
     assert r2 == r == 32 and np.array_equal(U2, U) and np.array_equal(E2, E)
+
+
+def test_operator_text_files(tmp_path):
+    """The text form of the operator files (the reference's ENABLE_ASCII_IO builds, .out):
+    the cutoff on the first line of the U file, one %18.12e value per line, read back to
+    13 significant digits."""
+    from bbfmm_b200 import operators as ops
+    assert ops.operator_file_names(8, True, "oneoverr4", ascii=True) == ("soneoverr4K8.out", "soneoverr4U8.out")
+    U, E, _ = ops.kernel_svd(4)
+    ops.write_operator_files(str(tmp_path), 4, U, E, False, ascii=True)
+    lines = (tmp_path / "laplacianU4.out").read_text().splitlines()
+    assert lines[0] == "32" and len(lines) == 1 + 64 * 32 and lines[1] == "%18.12e" % U[0]
+    assert len((tmp_path / "laplacianK4.out").read_text().splitlines()) == 316 * 32 * 32
+    r, U2, E2 = ops.read_operator_files(str(tmp_path), 4, False, ascii=True)
+    assert r == 32 and np.allclose(U2, U, rtol=1e-12, atol=1e-15) and np.allclose(E2, E, rtol=1e-12, atol=1e-15)
+    ops.write_operator_files(str(tmp_path), 4, U2, E2, True, ascii=True)
+    _, Us, _ = ops.read_operator_files(str(tmp_path), 4, True, ascii=True)
+    assert Us.dtype == np.float32 and np.array_equal(Us, U2.astype(np.float32))

@@ -140,3 +140,28 @@ def test_fp32_oracle_equals_fp32_reference_other_kernels(oracle_s, kernel, lev):
     phir = R.fmm(x, q, 4, lev, kp, up)
     phio = oracle_s.fmm(x, q, 4, lev, U, E, homogen=ops.homogeneity(kernel))
     assert rel_l2(phio, phir) < 1e-6
+
+
+@pytest.mark.skipif(not reference_available("d", "cpu8a_ascii"), reason="ENABLE_ASCII_IO reference build absent")
+def test_operator_text_files_match_the_reference(oracle_d):
+    """The reference's ENABLE_ASCII_IO build: its text operator files, read and written again by
+    bbfmm_b200.operators, come out byte for byte the same; and that build's FMM, reading text
+    files written by bbfmm_b200.operators, equals the oracle on the values read back
+    (relative L2 < 1e-14)."""
+    import filecmp
+    from bbfmm_b200 import operators as ops
+    R = Reference("d", "cpu8a_ascii")
+    d, d2, d3 = tempfile.mkdtemp(), tempfile.mkdtemp(), tempfile.mkdtemp()
+    kp, up = R.compute_operators(4, d)
+    r, U, E = ops.read_operator_files(d, 4, False, ascii=True)
+    ops.write_operator_files(d2, 4, U, E, False, ascii=True)
+    assert filecmp.cmp(kp, os.path.join(d2, "laplacianK4.out"), shallow=False)
+    assert filecmp.cmp(up, os.path.join(d2, "laplacianU4.out"), shallow=False)
+    Uo, Eo, _ = ops.kernel_svd(4)
+    ops.write_operator_files(d3, 4, Uo, Eo, False, ascii=True)
+    rng = np.random.default_rng(6)
+    x = rng.random((20000, 3)) - 0.5
+    q = rng.uniform(-1, 1, 20000)
+    phir = R.fmm(x, q, 4, 3, os.path.join(d3, "laplacianK4.out"), os.path.join(d3, "laplacianU4.out"))
+    _, U3, E3 = ops.read_operator_files(d3, 4, False, ascii=True)
+    assert rel_l2(oracle_d.fmm(x, q, 4, 3, U3, E3), phir) < 1e-14
