@@ -95,3 +95,17 @@ def test_near_field_argument_checks():
     assert L.bbfmm_b200_near_field_noalloc(262145, 3, 1.0, C.c_void_p(16), C.c_void_p(16), C.c_void_p(16), 0,
                                            None) == 1
     assert L.bbfmm_b200_near_field(0, 3, 1.0, None, None, None, 0, None) == 0
+
+
+def test_handle_setters_reject_null_handles_and_bad_values():
+    """Argument checks of the handle setters that run before any device work."""
+    L = _lib.lib()  # argument types as declared by bbfmm_b200._lib
+    for k in (0, 1, 2):  # LAPLACIAN, LAPLACIAN_FORCE, ONEOVERR4
+        assert L.bbfmm_b200_set_kernel(None, k) == 1
+    assert L.bbfmm_b200_set_rank(None, 64) == 1
+    assert L.bbfmm_b200_set_tc_products(None, 0) == 1
+    assert L.bbfmm_b200_set_leaf_slab(None, 64) == 1
+    assert L.bbfmm_b200_solve(None, None, None) == 1
+    assert L.bbfmm_b200_set_particles(None, 10, None) == 1
+    assert L.bbfmm_b200_set_particles_device(None, 10, None) == 1
+    assert b"null" in L.bbfmm_b200_last_error() or b"bad" in L.bbfmm_b200_last_error()
