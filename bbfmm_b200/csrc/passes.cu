@@ -266,12 +266,57 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
 }
 
 // ----------------------------------------------------------------------------- L2P
-// One warp per leaf; phi_sorted[p] = q_p (2/n)^3 sum_l F[l] Sx Sy Sz (assign).
+// Lane share of a leaf's F (n^3 values, l = (l1 n + l2) n + l3) when a warp loads it
+// coalesced, lane + 32 k for k < n^3 / 32: l3 = lane % n for every k (32 % n == 0); for n = 8,
+// l1 = k / 2 and l2 = 4 (k % 2) + lane / 8; for n = 4, l1 = 2 k + lane / 16 and
+// l2 = (lane / 4) % 4.
+template <int NN> __device__ __forceinline__ int f_l1(int k, int lane) { return NN == 8 ? k >> 1 : 2 * k + (lane >> 4); }
+template <int NN> __device__ __forceinline__ int f_l2(int k, int lane) {
+  return NN == 8 ? 4 * (k & 1) + (lane >> 3) : (lane >> 2) & 3;
+}
+
+// Warp-per-leaf pipeline shared by the L2P kernels: the leaf offsets are loaded two leaves
+// ahead and the next leaf's F (coalesced, n^3 / 32 values per lane; skipped for empty
+// leaves) one leaf ahead, so the HBM loads of the next leaf are in flight while the current
+// one is evaluated. body(leaf m, local index mm, p0, p1, F registers) does the arithmetic.
+template <typename T, int NN, typename Body>
+__device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start, const T *__restrict__ F, int64_t m0,
+                                             int64_t count, Body body) {
+  constexpr int PER = NN * NN * NN / 32;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  T fc[PER], fn[PER];
+  int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+  if (warp < count) { a0 = leaf_start[m0 + warp]; a1 = leaf_start[m0 + warp + 1]; }
+  if (warp + nwarps < count) { b0 = leaf_start[m0 + warp + nwarps]; b1 = leaf_start[m0 + warp + nwarps + 1]; }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) fc[k] = a1 > a0 ? F[warp * (NN * NN * NN) + lane + 32 * k] : (T)0;
+  for (int64_t mm = warp; mm < count; mm += nwarps) {
+    int c0 = 0, c1 = 0;
+    if (mm + 2 * nwarps < count) { c0 = leaf_start[m0 + mm + 2 * nwarps]; c1 = leaf_start[m0 + mm + 2 * nwarps + 1]; }
+    const bool nxt = mm + nwarps < count && b1 > b0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) fn[k] = nxt ? F[(mm + nwarps) * (NN * NN * NN) + lane + 32 * k] : (T)0;
+    if (a1 > a0) body(m0 + mm, a0, a1, fc);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) fc[k] = fn[k];
+    a0 = b0; a1 = b1; b0 = c0; b1 = c1;
+  }
+}
+
+template <typename T> struct Vec4;
+template <> struct Vec4<double> { using type = double4; };
+template <> struct Vec4<float> { using type = float4; };
+
+// One warp per leaf; phi_sorted[p] = q_p (2/n)^3 sum_l F[l] Sx Sy Sz (assign). A leaf's
+// particles are loaded by its lanes at once and broadcast one by one; the S values of a
+// particle come from sn_lane (one Clenshaw evaluation per lane) by shuffles.
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                   T *__restrict__ phi, int64_t m0, int64_t count) {
-  constexpr int N2 = NN * NN, N3 = N2 * NN;
+  constexpr int PER = NN * NN * NN / 32;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
   for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
@@ -281,53 +326,41 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
   const T ihalf = (T)1 / (len / (T)2);
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t mm = warp; mm < count; mm += nwarps) {
-    const int64_t m = m0 + mm;  // leaf; F holds leaves m0 .. m0 + count - 1
-    const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
-    if (p1 == p0) continue;
+  using V4 = typename Vec4<T>::type;
+  const V4 *p4 = reinterpret_cast<const V4 *>(pos4);
+  l2p_pipeline<T, NN>(leaf_start, F, m0, count, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
-    // lanes split the (l1, l2) rows of the leaf's F; each lane keeps its rows in registers
-    constexpr int NIT = (N2 + 31) / 32;
-    const T *Fm = F + mm * N3;
-    T fr[NIT][NN];
+    for (int pb = p0; pb < p1; pb += 32) {
+      const int np = min(32, p1 - pb);
+      V4 mine = {};
+      if (lane < np) mine = p4[pb + lane];
+      T res = 0;
+      for (int k = 0; k < np; ++k) {
+        const T x = ihalf * (wshfl(mine.x, k) - cx), y = ihalf * (wshfl(mine.y, k) - cy),
+                z = ihalf * (wshfl(mine.z, k) - cz);
+        const T val = sn_lane<T, NN>(s_tkz, lane, x, y, z);
+        // sum over the lane's F values of F Sx[l1] Sy[l2], then times Sz[l3]
+        T part = 0;
+        if constexpr (NN == 8) {
+          const T sya = wshfl(val, NN + (lane >> 3)), syb = wshfl(val, NN + 4 + (lane >> 3));
 #pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int l12 = lane + 32 * it;
+          for (int a = 0; a < NN; ++a) part += wshfl(val, a) * (fr[2 * a] * sya + fr[2 * a + 1] * syb);
+        } else {
+          const T sy = wshfl(val, NN + f_l2<NN>(0, lane));
 #pragma unroll
-      for (int l3 = 0; l3 < NN; ++l3) fr[it][l3] = l12 < N2 ? Fm[l12 * NN + l3] : (T)0;
-    }
-    for (int p = p0; p < p1; ++p) {
-      const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
-      const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
-      const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
-      const T q = pos4[4 * (int64_t)p + 3];
-      const T val = sn_lane<T, NN>(s_tkz, lane, x, y, z);
-      T sz[NN];
-#pragma unroll
-      for (int l3 = 0; l3 < NN; ++l3) sz[l3] = wshfl(val, 2 * NN + l3);
-      // each lane sums its l3 rows (shuffles by every lane)
-      T part = 0;
-#pragma unroll
-      for (int it = 0; it < NIT; ++it) {
-        const int l12 = lane + 32 * it, l12c = l12 < N2 ? l12 : 0;
-        const T a = wshfl(val, l12c / NN), b = wshfl(val, NN + l12c % NN);
-        if (l12 < N2) {
-          T inner = 0;
-#pragma unroll
-          for (int l3 = 0; l3 < NN; ++l3) inner += sz[l3] * fr[it][l3];
-          part += a * b * inner;
+          for (int kk = 0; kk < PER; ++kk) part += fr[kk] * wshfl(val, f_l1<NN>(kk, lane)) * sy;
         }
-      }
+        part *= wshfl(val, 2 * NN + (lane & (NN - 1)));
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-      if (lane == 0) phi[p] = q * pre3 * part;
+        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+        if (lane == k) res = mine.w * pre3 * part;
+      }
+      if (lane < np) phi[pb + lane] = res;
     }
-  }
+  });
 }
 
 // --------------------------------------------------------------- projections (GEMM)
@@ -453,6 +486,21 @@ static int grid_for(int64_t work, int per_block, int cap) {
   return (int)g;
 }
 
+// One wave of `kernel` at `threads` per CTA: SMs x resident CTAs per SM (looked up once per
+// kernel), so that grid-stride pipelines run for the whole launch.
+template <auto Kernel>
+static int resident_grid(int threads) {
+  static int blocks = 0;  // one cache per kernel
+  if (!blocks) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, Kernel, threads, 0);
+    blocks = sms * (per > 0 ? per : 1);
+  }
+  return blocks;
+}
+
 template <typename T>
 int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s,
                int nsets, int64_t first, int64_t count, void *Ssplit) {
@@ -509,9 +557,12 @@ int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, con
                cudaStream_t s, int nsets, int64_t first, int64_t count) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
-  const int grid = grid_for(count, 4, 148 * 64);
-  if (n == 4) l2p_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi, first, count);
-  else if (n == 8) l2p_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, phi, first, count);
+  if (n == 4)
+    l2p_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 4>>(128)), 128, 0, s>>>(
+        pos4, leaf_start, maxlev, L, t, F, phi, first, count);
+  else if (n == 8)
+    l2p_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 8>>(128)), 128, 0, s>>>(
+        pos4, leaf_start, maxlev, L, t, F, phi, first, count);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p", __FILE__, __LINE__);
 }
@@ -598,13 +649,14 @@ __device__ __forceinline__ void sn_lane_d(const T *__restrict__ tkz, int lane, T
 }
 
 // One warp per leaf: pot[p] = (2/n)^3 sum_l F[l] Sx Sy Sz (no target factor) and
-// fld[3p + a] = d pot / d x_a, with the chain factor 2 / leaf length of the leaf map.
+// fld[3p + a] = d pot / d x_a, with the chain factor 2 / leaf length of the leaf map; the
+// same load pipeline as l2p_kernel.
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                         int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                         T *__restrict__ pot, T *__restrict__ fld, int64_t m0,
                                                         int64_t count) {
-  constexpr int N2 = NN * NN, N3 = N2 * NN;
+  constexpr int PER = NN * NN * NN / 32;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
   for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
@@ -614,64 +666,78 @@ __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ po
   const T ihalf = (T)1 / (len / (T)2);
   const T prefac = (T)2 / (T)NN;
   const T pre3 = prefac * prefac * prefac;
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t mm = warp; mm < count; mm += nwarps) {
-    const int64_t m = m0 + mm;  // leaf; F holds leaves m0 .. m0 + count - 1
-    const int p0 = leaf_start[m], p1 = leaf_start[m + 1];
-    if (p1 == p0) continue;
+  using V4 = typename Vec4<T>::type;
+  const V4 *p4 = reinterpret_cast<const V4 *>(pos4);
+  l2p_pipeline<T, NN>(leaf_start, F, m0, count, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
-    const T *Fm = F + mm * N3;
-    for (int p = p0; p < p1; ++p) {
-      const T x = ihalf * (pos4[4 * (int64_t)p] - cx);
-      const T y = ihalf * (pos4[4 * (int64_t)p + 1] - cy);
-      const T z = ihalf * (pos4[4 * (int64_t)p + 2] - cz);
-      T vs, vd;
-      sn_lane_d<T, NN>(s_tkz, lane, x, y, z, vs, vd);
-      T sz[NN], dz[NN];
+    for (int pb = p0; pb < p1; pb += 32) {
+      const int np = min(32, p1 - pb);
+      V4 mine = {};
+      if (lane < np) mine = p4[pb + lane];
+      T rv = 0, rx = 0, ry = 0, rz = 0;
+      for (int k = 0; k < np; ++k) {
+        const T x = ihalf * (wshfl(mine.x, k) - cx), y = ihalf * (wshfl(mine.y, k) - cy),
+                z = ihalf * (wshfl(mine.z, k) - cz);
+        T vs, vd;
+        sn_lane_d<T, NN>(s_tkz, lane, x, y, z, vs, vd);
+        // per l1 row: A = sum F Sy[l2], B = sum F dSy[l2]; then v = sum Sx A, gx = sum dSx A,
+        // gy = sum Sx B (times Sz or dSz below)
+        T v = 0, gx = 0, gy = 0;
+        if constexpr (NN == 8) {
+          const int ba = NN + (lane >> 3), bb = NN + 4 + (lane >> 3);
+          const T sya = wshfl(vs, ba), syb = wshfl(vs, bb), dya = wshfl(vd, ba), dyb = wshfl(vd, bb);
 #pragma unroll
-      for (int l3 = 0; l3 < NN; ++l3) {
-        sz[l3] = wshfl(vs, 2 * NN + l3);
-        dz[l3] = wshfl(vd, 2 * NN + l3);
-      }
-      T v = 0, gx = 0, gy = 0, gz = 0;
-#pragma unroll
-      for (int it = 0; it < (N2 + 31) / 32; ++it) {
-        const int l12 = lane + 32 * it, l12c = l12 < N2 ? l12 : 0;
-        const int l1 = l12c / NN, l2 = l12c % NN;
-        const T sx = wshfl(vs, l1), dx = wshfl(vd, l1), sy = wshfl(vs, NN + l2), dy = wshfl(vd, NN + l2);
-        if (l12 < N2) {
-          const T *f = Fm + l12 * NN;
-          T in0 = 0, in1 = 0;
-#pragma unroll
-          for (int l3 = 0; l3 < NN; ++l3) {
-            in0 += sz[l3] * f[l3];
-            in1 += dz[l3] * f[l3];
+          for (int a = 0; a < NN; ++a) {
+            const T A = fr[2 * a] * sya + fr[2 * a + 1] * syb, B = fr[2 * a] * dya + fr[2 * a + 1] * dyb;
+            const T sx = wshfl(vs, a), dx = wshfl(vd, a);
+            v += sx * A;
+            gx += dx * A;
+            gy += sx * B;
           }
-          v += sx * sy * in0;
-          gx += dx * sy * in0;
-          gy += sx * dy * in0;
-          gz += sx * sy * in1;
+        } else {
+          const int b = NN + f_l2<NN>(0, lane);
+          const T sy = wshfl(vs, b), dy = wshfl(vd, b);
+#pragma unroll
+          for (int kk = 0; kk < PER; ++kk) {
+            const int a = f_l1<NN>(kk, lane);
+            const T sx = wshfl(vs, a), dx = wshfl(vd, a);
+            v += fr[kk] * sx * sy;
+            gx += fr[kk] * dx * sy;
+            gy += fr[kk] * sx * dy;
+          }
+        }
+        const int c = 2 * NN + (lane & (NN - 1));
+        const T sz = wshfl(vs, c), dz = wshfl(vd, c);
+        T gz = v * dz;
+        v *= sz;
+        gx *= sz;
+        gy *= sz;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          v += __shfl_xor_sync(0xffffffffu, v, off);
+          gx += __shfl_xor_sync(0xffffffffu, gx, off);
+          gy += __shfl_xor_sync(0xffffffffu, gy, off);
+          gz += __shfl_xor_sync(0xffffffffu, gz, off);
+        }
+        if (lane == k) {
+          rv = pre3 * v;
+          rx = pre3 * ihalf * gx;
+          ry = pre3 * ihalf * gy;
+          rz = pre3 * ihalf * gz;
         }
       }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        v += __shfl_xor_sync(0xffffffffu, v, off);
-        gx += __shfl_xor_sync(0xffffffffu, gx, off);
-        gy += __shfl_xor_sync(0xffffffffu, gy, off);
-        gz += __shfl_xor_sync(0xffffffffu, gz, off);
-      }
-      if (lane == 0) {
-        pot[p] = pre3 * v;
-        fld[3 * (int64_t)p] = pre3 * ihalf * gx;
-        fld[3 * (int64_t)p + 1] = pre3 * ihalf * gy;
-        fld[3 * (int64_t)p + 2] = pre3 * ihalf * gz;
+      if (lane < np) {
+        const int64_t p = pb + lane;
+        pot[p] = rv;
+        fld[3 * p] = rx;
+        fld[3 * p + 1] = ry;
+        fld[3 * p + 2] = rz;
       }
     }
-  }
+  });
 }
 
 // Sorted (potential, field) -> caller's order.
@@ -694,10 +760,12 @@ int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T 
                      T *pot, T *fld, cudaStream_t s, int nsets, int64_t first, int64_t count) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
-  const int grid = grid_for(count, 4, 148 * 64);
-  if (n == 4) l2p_field_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
+  if (n == 4)
+    l2p_field_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 4>>(128)), 128, 0, s>>>(
+        pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
   else if (n == 8)
-    l2p_field_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
+    l2p_field_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 8>>(128)), 128, 0, s>>>(
+        pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p_field", __FILE__, __LINE__);
 }

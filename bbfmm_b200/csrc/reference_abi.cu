@@ -330,8 +330,10 @@ int downward(Tree<T> **atree, const Real3<T> *field, const T *Cweights, const T 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
     rc = bbfmm_set_cuda_error(e, "h2d phi", __FILE__, __LINE__);
   }
-  if (near && rc == BBFMM_OK)
-    rc = launch_p2p<T>(s.N, s.pos4, s.leaf_start, s.leafm, maxlev, s.phis, s.stream, 256, kernel_homogen(homogen));
+  if (near && rc == BBFMM_OK) {
+    s.homogen = kernel_homogen(homogen);
+    rc = s.near(s.phis, nullptr);
+  }
   if (rc == BBFMM_OK && s.N > 0) {
     std::vector<T> ps(s.N);
     cudaError_t e = cudaMemcpyAsync(ps.data(), s.phis, sizeof(T) * s.N, cudaMemcpyDeviceToHost, s.stream);

@@ -285,22 +285,24 @@ int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const
     return bbfmm_set_error(BBFMM_ERR_ARG, "number of stacked sets out of range");
   nsets = nsets_;
   const int64_t nl = cells(maxlev);
-  if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(leafm); cudaFree(pos4); cudaFree(phis); }
+  if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(pos4); cudaFree(phis); }
+  if (near_work) cudaFree(near_work);
+  near_work = nullptr;
+  near_items = near_threads = 0;
   if (flds) cudaFree(flds);  // sized 3 N: reallocated by the next solve_fields
   if (io_q) cudaFree(io_q);  // sized N: reallocated by the next host-buffer solve
   if (io_phi) cudaFree(io_phi);
   io_q = io_phi = nullptr;
-  perm = leaf_start = leafm = nullptr; pos4 = phis = flds = nullptr;
+  perm = leaf_start = nullptr; pos4 = phis = flds = nullptr;
   N = N_;
   TRY(dalloc(&perm, N > 0 ? N : 1));
   TRY(dalloc(&leaf_start, nl + 1));
-  TRY(dalloc(&leafm, N > 0 ? N : 1));
   TRY(dalloc(&pos4, 4 * (size_t)(N > 0 ? N : 1)));
   TRY(dalloc(&phis, N > 0 ? N : 1));
   if (N > 0) BBFMM_CUDA_OK(cudaMemcpy(perm, perm_h, sizeof(int) * N, cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaMemcpy(leaf_start, leaf_start_h, sizeof(int) * (nl + 1), cudaMemcpyHostToDevice));
   BBFMM_CUDA_OK(cudaDeviceSynchronize());
-  TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream, nsets));
+  TRY(build_near_work());
   if (N > 0) {
     T *xyz_d = nullptr;
     TRY(dalloc(&xyz_d, 3 * (size_t)Nxyz));
@@ -322,20 +324,22 @@ int Solver<T>::set_particles_device(int N_, const T *xyz_d) {
   if (N_ < 0 || (N_ > 0 && !xyz_d)) return bbfmm_set_error(BBFMM_ERR_ARG, "bad particle arguments");
   nsets = 1;
   const int64_t nl = cells(maxlev);
-  if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(leafm); cudaFree(pos4); cudaFree(phis); }
+  if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(pos4); cudaFree(phis); }
+  if (near_work) cudaFree(near_work);
+  near_work = nullptr;
+  near_items = near_threads = 0;
   if (flds) cudaFree(flds);
   if (io_q) cudaFree(io_q);
   if (io_phi) cudaFree(io_phi);
   io_q = io_phi = nullptr;
-  perm = leaf_start = leafm = nullptr; pos4 = phis = flds = nullptr;
+  perm = leaf_start = nullptr; pos4 = phis = flds = nullptr;
   N = N_;
   TRY(dalloc(&perm, N > 0 ? N : 1));
   TRY(dalloc(&leaf_start, nl + 1));
-  TRY(dalloc(&leafm, N > 0 ? N : 1));
   TRY(dalloc(&pos4, 4 * (size_t)(N > 0 ? N : 1)));
   TRY(dalloc(&phis, N > 0 ? N : 1));
   TRY(build_tree_device<T>(N, xyz_d, (T)L, maxlev, perm, leaf_start, stream));
-  TRY(launch_leaf_of(maxlev, leaf_start, leafm, stream, 1));
+  TRY(build_near_work());
   if (N > 0) TRY((launch_gather<T, T>(N, perm, xyz_d, nullptr, pos4, stream)));
   TRY(alloc_work());
   BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
@@ -602,17 +606,22 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
 // Near field into the sorted potential (and field when fld != null), added.
 template <typename T>
 int Solver<T>::near(T *pot, T *fld) {
-  const int th = tune.p2p_threads;
-  if (mode == MODE_MIXED) {
-    if (fld) TRY(launch_p2p_mixed_field(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot,
-                                        (double *)fld, stream, th));
-    else TRY(launch_p2p_mixed(N, (const double *)pos4, leaf_start, leafm, maxlev, (double *)pot, stream, th));
-    mark(ST_P2P);
-  } else {
-    if (fld) TRY(launch_p2p_field<T>(N, pos4, leaf_start, leafm, maxlev, pot, fld, stream, th));
-    else TRY(launch_p2p<T>(N, pos4, leaf_start, leafm, maxlev, pot, stream, th, homogen));
-    mark(ST_P2P);
-  }
+  if (near_threads != tune.p2p_threads) TRY(build_near_work());
+  TRY(launch_near(mode, homogen, N, pos4, leaf_start, maxlev, near_work, nsets, near_items, near_threads, pot, fld,
+                  stream));
+  mark(ST_P2P);
+  return BBFMM_OK;
+}
+
+// The near-field work list of the current tree for tune.p2p_threads threads per CTA (one
+// synchronisation: the item count sizes the launch).
+template <typename T>
+int Solver<T>::build_near_work() {
+  if (!near_work) TRY(dalloc((unsigned char **)&near_work, near_work_bytes(N, maxlev, nsets)));
+  int flag = 0;
+  TRY(near_work_build(N, leaf_start, maxlev, nsets, tune.p2p_threads, near_work, stream, &near_items, &flag));
+  if (flag) return bbfmm_set_error(BBFMM_ERR_ARG, "leaf offsets must rise from 0 to N without decreasing");
+  near_threads = tune.p2p_threads;
   return BBFMM_OK;
 }
 
@@ -718,7 +727,7 @@ int Solver<T>::autotune(const void *q_dev, int io_double) {
     int rc = BBFMM_OK;
     for (int th : {64, 128, 256}) {
       tune.p2p_threads = th;
-      rc = near(phis, nullptr);  // warm; phis is scratch that the next solve assigns
+      rc = near(phis, nullptr);  // builds the list for th, warm; phis is scratch that the next solve assigns
       if (rc != BBFMM_OK) break;
       cudaEventRecord(a, stream);
       for (int i = 0; i < 3 && rc == BBFMM_OK; ++i) rc = near(phis, nullptr);
@@ -738,6 +747,8 @@ int Solver<T>::autotune(const void *q_dev, int io_double) {
     std::lock_guard<std::mutex> g(g_tune_mutex);
     g_tune_cache[key] = {pick, 0};
   }
+  // the list for the choice now, so that no later (possibly captured) solve rebuilds it
+  if (near_threads != tune.p2p_threads) TRY(build_near_work());
   BBFMM_CUDA_OK(cudaStreamSynchronize(stream));
   return BBFMM_OK;
 }
@@ -758,9 +769,40 @@ int Solver<T>::copy_multipoles_morton(int level, T *host_out) {
   return rc;
 }
 
+// The M2L output of one level (L = sum E_k M over the interaction lists, before the post-M2L
+// projection and its scale), recomputed from the multipoles of the last solve with the launch
+// choices of the solve (the mixed mode's tensor-core kernel writing its full FP64 output), r
+// values per cell in the reference's Morton order.
+template <typename T>
+int Solver<T>::copy_m2l_morton(int level, T *host_out) {
+  if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "level out of range");
+  if (nsets != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L copies are per single-set solver");
+  if (!pos4 || !Lbuf) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
+  const T *Ml = Mall + Moff[level];
+  const bool split = mode == MODE_MIXED && tcops && level >= TC_MIN_LEVEL && tune.m2l_kind[level] == 0;
+  if (split) {
+    const bool fused = lead > 0 && tc_fuses_lead(tcops, tc_products, rk());
+    if (lead > 0 && !fused) TRY(m2l_fp(Ml, level, 0, lead, lead_rows));
+    TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf, level, offs, stream, nsets,
+                      tc_products, rk(), fused ? (const double *)Ml : nullptr, fused ? (const double *)Ert : nullptr));
+  } else {
+    TRY(m2l_fp(Ml, level, 0, rk(), rk()));
+  }
+  T *tmp = nullptr;
+  TRY(dalloc(&tmp, (size_t)pow8i(level) * r));
+  int rc = launch_morton_cpg<T>(level, r, Lbuf, tmp, 1, stream);
+  if (rc == BBFMM_OK) {
+    cudaError_t e = cudaMemcpyAsync(host_out, tmp, sizeof(T) * pow8i(level) * r, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    rc = bbfmm_set_cuda_error(e, "copy M2L output", __FILE__, __LINE__);
+  }
+  cudaFree(tmp);
+  return rc;
+}
+
 template <typename T>
 void Solver<T>::release() {
-  void *ptrs[] = {offs, perm, leaf_start, leafm, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
+  void *ptrs[] = {offs, perm, leaf_start, near_work, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
                   phis, flds, Ssplit, Lsplit, io_q, io_phi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -921,12 +963,21 @@ int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *h, int level, void *host_out) 
   return h->d->copy_multipoles_morton(level, (double *)host_out);
 }
 
+int bbfmm_b200_copy_m2l(bbfmm_b200_solver *h, int level, void *host_out) {
+  if (!h || !host_out) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  if (h->f) return h->f->copy_m2l_morton(level, (float *)host_out);
+  return h->d->copy_m2l_morton(level, (double *)host_out);
+}
+
 int bbfmm_b200_time_m2l(bbfmm_b200_solver *h, int level, int reps, float *ms) {
   if (!h || !ms) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   return h->f ? h->f->time_m2l(level, reps, ms) : h->d->time_m2l(level, reps, ms);
 }
 
-int bbfmm_b200_device_status(int clear) { return bbfmm::tc_status(clear); }
+int bbfmm_b200_device_status(int clear) {
+  const int a = bbfmm::tc_status(clear), b = bbfmm::near_status(clear);
+  return a != 0 ? a : b;
+}
 
 int bbfmm_b200_wait_selftest(unsigned limit) {
   if (limit == 0 || limit > (1u << 24)) return -bbfmm_set_error(BBFMM_ERR_ARG, "limit must be in [1, 2^24]");
@@ -1009,7 +1060,9 @@ int bbfmm_b200_set_tuning(bbfmm_b200_solver *h, const int *info) {
       sv.tune.m2l_kind[l] = info[1 + l];
       sv.tune.m2l_groups[l] = info[12 + l];
     }
-    return sv.pos4 ? sv.alloc_partials() : BBFMM_OK;
+    if (!sv.pos4) return BBFMM_OK;
+    if (sv.near_threads != th) TRY(sv.build_near_work());
+    return sv.alloc_partials();
   };
   return h->f ? apply(*h->f) : apply(*h->d);
 }

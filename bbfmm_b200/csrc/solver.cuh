@@ -36,13 +36,20 @@ template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
-template <typename T> int launch_p2p(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *phi, cudaStream_t s, int threads = 256, int homogen = 1);
-int launch_p2p_mixed(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *phi, cudaStream_t s, int threads = 256);
-int launch_leaf_of(int maxlev, const int *leaf_start, int *leafm, cudaStream_t s, int nsets = 1);
+// Near field (p2p.cu): a work list built on the device from the leaf offsets (near_work_build,
+// into near_work_bytes of scratch), then one CTA per item of `threads` threads (64, 128 or
+// 256; the list depends on it). mode: MODE_D / MODE_S / MODE_MIXED (pos4 and pot in FP64,
+// FP32, FP64); homogen 1, 2 or 4; fld != null adds the gradient (1/r only, no target factor
+// on pot then). nitems_host / flag_host: synchronise and return the item count and whether
+// the offsets were malformed.
+size_t near_work_bytes(int N, int maxlev, int nsets);
+int near_work_build(int N, const int *leaf_start, int maxlev, int nsets, int threads, void *scratch, cudaStream_t s,
+                    int *nitems_host, int *flag_host);
+int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_start, int maxlev, const void *work,
+                int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s);
+int near_status(int clear);
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
-template <typename T> int launch_p2p_field(int N, const T *pos4, const int *leaf_start, const int *leafm, int maxlev, T *pot, T *fld, cudaStream_t s, int threads = 256);
-int launch_p2p_mixed_field(int N, const double *pos4, const int *leaf_start, const int *leafm, int maxlev, double *pot, double *fld, cudaStream_t s, int threads = 256);
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0);
 void build_offset_table(int *out);
 constexpr int DMMA_PARTS = 21;  // most offset groups of the FP64 M2L (189 = 9 x 21)
@@ -99,7 +106,7 @@ constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid
 struct Tuning {
   int m2l_kind[11] = {};    // 0: default (tensor-core split M2L where the mode has it), 1: FP64/SIMT M2L
   int m2l_groups[11] = {};  // offset groups of the FP64 DMMA M2L (0: dmma_default_groups)
-  int p2p_threads = 256;    // threads per block of the near-field kernels
+  int p2p_threads = 128;    // threads per block of the near-field kernel
 };
 
 template <typename T>
@@ -145,7 +152,9 @@ struct Solver {
   int64_t Ssplit_rows = 0, Lsplit_rows = 0;
   // particles (sorted by leaf, Morton leaf order)
   int N = 0;
-  int *perm = nullptr, *leaf_start = nullptr, *leafm = nullptr;
+  int *perm = nullptr, *leaf_start = nullptr;
+  void *near_work = nullptr;  // near-field work list (near_work_build) for near_threads
+  int near_items = 0, near_threads = 0;
   T *pos4 = nullptr;
   // expansions
   T *S[2] = {nullptr, nullptr};
@@ -185,6 +194,7 @@ struct Solver {
   int share_operators(const Solver<T> &from);  // borrow tables and operators (same n, mode, lead)
   int alloc_partials();                          // Lpart for the current tuning
   int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
+  int build_near_work();                         // the work list for tune.p2p_threads
   bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
   int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false);  // S rows -> Mall (cpg)
   int proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit = false);    // Lbuf -> F rows (Morton, assign)
@@ -200,6 +210,7 @@ struct Solver {
   int solve(const void *q_dev, void *phi_dev, int io_double);
   int solve_fields(const void *q_dev, void *pot_dev, void *fld_dev);  // potential and its gradient
   int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order
+  int copy_m2l_morton(int level, T *host_out);         // level's M2L output, recomputed, Morton order
   void mark(int stage, int launches = 1);
   int time_m2l(int level, int reps, float *ms);
   int m2l_fp(const T *Ml, int level, int j0, int j1, int ni);  // FP64 (DMMA) / FP32 (SIMT) M2L part

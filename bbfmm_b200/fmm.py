@@ -230,6 +230,13 @@ class Solver:
         _lib.check(_lib.lib().bbfmm_b200_copy_multipoles(self.h, level, _ptr(out)))
         return out
 
+    def m2l_output(self, level: int):
+        """The level's M2L output L = sum E_k M (before the post-M2L projection), recomputed
+        from the multipoles of the last solve; shape (8^level, r), Morton cell order."""
+        out = np.empty(8 ** level * self.r, dtype=self.np_dtype)
+        _lib.check(_lib.lib().bbfmm_b200_copy_m2l(self.h, level, _ptr(out)))
+        return out.reshape(8 ** level, self.r)
+
 
 def batch_depth(N: int, per_leaf: float = 32.0) -> int:
     """Leaf depth for about `per_leaf` particles per leaf: round(log8(N / per_leaf)), >= 2."""

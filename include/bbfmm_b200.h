@@ -144,6 +144,13 @@ BBFMM_B200_API int bbfmm_b200_stage_times(const bbfmm_b200_solver *s, float *ms,
  * the reference's Morton cell order (the level's slice of proxysval). */
 BBFMM_B200_API int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *s, int level, void *host_out);
 
+/* The M2L output of one level -- the level's slice of what the reference's m2l_drv writes
+ * into L (m2l_drv.cu:14-19; PF of anotherFMMInteraction): L(F) = sum_{S in IL(F)} E_k M(S),
+ * before the post-M2L projection and its (1/L_l)^homogeneity scale -- recomputed from the
+ * multipoles of the last solve with that solve's kernels (MIXED: the tensor-core kernel with
+ * its full FP64 output), r values per cell in the reference's Morton cell order. */
+BBFMM_B200_API int bbfmm_b200_copy_m2l(bbfmm_b200_solver *s, int level, void *host_out);
+
 /* Re-run the M2L of one level `reps` times (inputs of the last solve) between CUDA events
  * on the solver's stream: ms[0] = mean time of the main M2L kernel per launch, ms[1] =
  * mean time of the FP64 leading-component kernel (MIXED only, else 0). */
@@ -163,9 +170,14 @@ BBFMM_B200_API int bbfmm_b200_direct_field(int N, const double *xyz_dev, const d
                                            const int *targets_dev, double *pot_dev, double *field_dev,
                                            void *stream);
 
-/* Status word of the tensor-core kernels: 0 when every bounded wait of every launch so far
- * completed, else the code of the first wait that gave up (the launch then skipped its
- * remaining work and returned). Synchronises the device; clear != 0 resets the word. */
+/* Status word of the device kernels: 0 when every bounded wait of every tensor-core launch so
+ * far completed and every near-field launch found well-formed leaf offsets, else the code of
+ * the first failure: the code of a wait that gave up (the launch then skipped its remaining
+ * work and returned), or BBFMM_B200_LEAF_RANGE_CODE when a near-field call was given leaf
+ * offsets that are out of [0, N] or decrease (the kernels clamp every offset, so nothing was
+ * read or written outside the caller's arrays). Synchronises the device; clear != 0 resets
+ * the word. */
+#define BBFMM_B200_LEAF_RANGE_CODE 98
 BBFMM_B200_API int bbfmm_b200_device_status(int clear);
 
 /* Failure-detection self test (no counterpart in the reference): one kernel waits, with the
@@ -182,11 +194,15 @@ BBFMM_B200_API int bbfmm_b200_wait_selftest(unsigned limit);
  * (direct.cu:69-209): phi[k] += q_k sum_{B in N(A)} sum_{j in B, r != 0} q_j / r_kj over the
  * <= 27 neighbour leaves. xyzq is N x 4 (x, y, z, q) FP64 sorted by leaf in Morton order
  * (as bbfmm_b200_sort_particles orders them), leaf_start holds the 8^maxlev + 1 leaf
- * offsets, phi is added to; all three are device pointers. mode BBFMM_B200_MODE_D computes
- * in FP64 like the reference; BBFMM_B200_MODE_MIXED takes each pair's separation in FP64 and
- * the reciprocal distance, product and compensated sum in FP32. L is checked (> 0) but the
- * leaf geometry needs only maxlev. Allocates N * 4 bytes of device scratch for the call, runs
- * on `stream` (cudaStream_t, may be NULL) and synchronises it before freeing the scratch. */
+ * offsets, phi is added to; all three are device pointers. The offsets must start at
+ * leaf_start[0] = 0, never decrease and end at leaf_start[8^maxlev] = N; other offsets make
+ * the call return BBFMM_B200_ERR_ARG (and set BBFMM_B200_LEAF_RANGE_CODE in the status word)
+ * without any access outside the arrays, phi then being unspecified. mode BBFMM_B200_MODE_D
+ * computes in FP64 like the reference; BBFMM_B200_MODE_MIXED takes each pair's separation in
+ * FP64 and the reciprocal distance, product and compensated sum in FP32. L is checked (> 0)
+ * but the leaf geometry needs only maxlev. Allocates a device work list for the call (8 bytes
+ * per particle plus 8 bytes per 256 cells of level maxlev - 2), runs on `stream`
+ * (cudaStream_t, may be NULL) and synchronises it. */
 BBFMM_B200_API int bbfmm_b200_near_field(int N, int maxlev, double L, const double *xyzq, const int *leaf_start,
                                          double *phi, int mode, void *stream);
 
@@ -194,16 +210,19 @@ BBFMM_B200_API int bbfmm_b200_near_field(int N, int maxlev, double L, const doub
  * in the reference. It is for callers that must not call cudaMalloc: code whose device
  * memory is handed out by another framework's allocator (which may hold all of it), and
  * time-critical loops that cannot afford the device-wide synchronisation cudaMalloc and
- * cudaFree imply. Inputs and output are the caller's, as above; the per-particle scratch
- * lives in one fixed array of device memory inside the library, sized for
- * BBFMM_B200_NOALLOC_MAX_PARTICLES particles (1 MiB), which every GPU that loads the library
- * keeps until the process exits. Larger N is rejected with BBFMM_B200_ERR_ARG.
- * The first call on a device looks up that array's device address (with the device
- * current), so make the first call on each device before any stream capture. All calls
- * share the array: calls that overlap on the GPU (other streams, other host threads) race
- * on it, so order them. Each call rewrites the scratch before reading it. Runs on `stream`
- * and returns without synchronising. */
+ * cudaFree imply. Inputs, output and the leaf-offset rules are as above; the work list
+ * lives in one fixed array of device memory inside the library,
+ * BBFMM_B200_NOALLOC_SCRATCH_BYTES (2.5 MiB) long, room for BBFMM_B200_NOALLOC_MAX_PARTICLES
+ * particles at any maxlev up to 10, which every GPU that loads the library keeps until the
+ * process exits. Larger N is rejected with BBFMM_B200_ERR_ARG. The first call on a device
+ * looks up that array's device address (with the device current), so make the first call
+ * on each device before any stream capture; the address stays valid for the life of the
+ * device's primary context, so do not call it across a cudaDeviceReset. All calls share
+ * the array: calls that overlap on the GPU (other streams, other host threads) race on it,
+ * so order them. Each call clears the list's counters and rewrites every entry it reads. Runs
+ * on `stream` and synchronises that stream (not the device) to check the leaf offsets. */
 #define BBFMM_B200_NOALLOC_MAX_PARTICLES 262144
+#define BBFMM_B200_NOALLOC_SCRATCH_BYTES 2621696
 BBFMM_B200_API int bbfmm_b200_near_field_noalloc(int N, int maxlev, double L, const double *xyzq,
                                                  const int *leaf_start, double *phi, int mode, void *stream);
 

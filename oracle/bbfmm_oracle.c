@@ -237,13 +237,17 @@ static void sn2(const real *xt, int Ns, const real *Tkz, int n, real *Sx, real *
     }
 }
 
-/* y[i] = 0 + sum_j A^T ... (atransx.c:48-86 with y zero on entry). */
-static void atransx(int m, int nn, const real *at, const real *x, real *y)
+/* y[i] = 0 + sum_j A^T ... (atransx.c:48-86 with y zero on entry), from the transposed
+   copy ut[nn j + i] = at[m i + j]: every y[i] still sums its terms in the order j = 0 .. m-1
+   from +0 (a sum started at +0 is never -0 under round-to-nearest, so the final 0 + sum of
+   the reference changes nothing), and the inner loop runs over contiguous i. */
+static void atransx_t(int m, int nn, const real *ut, const real *x, real *y)
 {
-  for (int i = 0; i < nn; i++) {
-    real sum = ZERO;
-    for (int j = 0; j < m; j++) sum += at[m * i + j] * x[j];
-    y[i] = ZERO + sum;
+  for (int i = 0; i < nn; i++) y[i] = ZERO;
+  for (int j = 0; j < m; j++) {
+    const real xj = x[j];
+    const real *u = &ut[(size_t)nn * j];
+    for (int i = 0; i < nn; i++) y[i] += u[i] * xj;
   }
 }
 
@@ -270,6 +274,9 @@ void SFX(orc_upward)(int maxlev, int n, int r, const real *xyz, const real *q,
     length *= 0.5;
   }
   real *Sw = (real *)malloc(sizeof(real) * n3);
+  real *Ut = (real *)malloc(sizeof(real) * (size_t)n3 * r);  /* Ut[r l + i] = U[n3 i + l] */
+  for (int i = 0; i < r; i++)
+    for (int l = 0; l < n3; l++) Ut[(size_t)r * l + i] = U[(size_t)n3 * i + l];
   {
     real Lc = celeng[maxlev], halfL = Lc / TWO, ihalfL = ONE / halfL;
     for (int A = SFX(orc_levsta)(maxlev); A < SFX(orc_levsta)(maxlev + 1); A++) {
@@ -301,7 +308,7 @@ void SFX(orc_upward)(int maxlev, int n, int r, const real *xyz, const real *q,
             Sw[l] = S[l] * Kweights[l];
             l++;
           }
-      atransx(n3, r, U, Sw, &proxysval[(size_t)r * A]);
+      atransx_t(n3, r, Ut, Sw, &proxysval[(size_t)r * A]);
       free(xt); free(qt); free(Sx); free(Sy); free(Sz);
     }
   }
@@ -347,12 +354,13 @@ void SFX(orc_upward)(int maxlev, int n, int r, const real *xyz, const real *q,
         S[l] *= prefac3;
         Sw[l] = S[l] * Kweights[l];
       }
-      atransx(n3, r, U, Sw, &proxysval[(size_t)r * A]);
+      atransx_t(n3, r, Ut, Sw, &proxysval[(size_t)r * A]);
     }
   }
   free(Sy);
   free(Sz);
   free(Sw);
+  free(Ut);
 }
 
 /* -------------------------------------------------------------------- M2L --- */
@@ -363,7 +371,7 @@ void SFX(orc_m2l)(int maxlev, int r, const real *E, const real *M, const real *c
                   const int *iinter, const int *interaction, const int *Ktable, real L,
                   real *PF)
 {
-  real *acc = (real *)malloc(sizeof(real) * r);
+  real *acc = (real *)malloc(sizeof(real) * r), *tmp = (real *)malloc(sizeof(real) * r);
   for (int level = MINLEV; level <= maxlev; level++) {
     real Lc = L;
     for (int i = 0; i < level; i++) Lc *= 0.5;
@@ -378,16 +386,44 @@ void SFX(orc_m2l)(int maxlev, int r, const real *E, const real *M, const real *c
         int k = Ktable[49 * (vx + 3) + 7 * (vy + 3) + (vz + 3)];
         const real *Ek = &E[(size_t)r * r * k];
         const real *Ms = &M[(size_t)r * S];
-        for (int i = 0; i < r; i++) {
-          real sum = ZERO;
-          for (int j = 0; j < r; j++) sum += Ek[(size_t)j * r + i] * Ms[j];
-          acc[i] += sum;
+        /* sum_j Ek(i, j) M_S[j] for every i, each in the order j = 0 .. r-1, then added to
+           acc[i]; the loop over i is the inner one so that it reads Ek contiguously */
+        for (int i = 0; i < r; i++) tmp[i] = ZERO;
+        for (int j = 0; j < r; j++) {
+          const real mj = Ms[j];
+          const real *col = &Ek[(size_t)j * r];
+          for (int i = 0; i < r; i++) tmp[i] += col[i] * mj;
         }
+        for (int i = 0; i < r; i++) acc[i] += tmp[i];
       }
       for (int i = 0; i < r; i++) PF[(size_t)r * F + i] = acc[i];
     }
   }
   free(acc);
+  free(tmp);
+}
+
+/* The same (target, source) products from a list of pairs: acc[r cell[p] + i] += sum_j
+   E_{k[p]}(i, j) M[r src[p] + j], the pairs taken in the order given (a caller that sorts them
+   by operator reads each r x r block once per run of equal k). Each product sums over j in
+   order, as orc_m2l; only the order in which a cell's products are added can differ. */
+void SFX(orc_m2l_pairs)(int r, const real *E, const real *M, long long npairs, const int *cell,
+                        const long long *src, const int *k, real *acc)
+{
+  real *tmp = (real *)malloc(sizeof(real) * r);
+  for (long long p = 0; p < npairs; p++) {
+    const real *Ek = &E[(size_t)r * r * k[p]];
+    const real *Ms = &M[(size_t)r * src[p]];
+    for (int i = 0; i < r; i++) tmp[i] = ZERO;
+    for (int j = 0; j < r; j++) {
+      const real mj = Ms[j];
+      const real *col = &Ek[(size_t)j * r];
+      for (int i = 0; i < r; i++) tmp[i] += col[i] * mj;
+    }
+    real *a = &acc[(size_t)r * cell[p]];
+    for (int i = 0; i < r; i++) a[i] += tmp[i];
+  }
+  free(tmp);
 }
 
 /* fieldval[n3 A + i] = (scale * Kweights[i]) * sum_j U(i, j) PF[r A + j], scale =
@@ -396,17 +432,23 @@ void SFX(orc_postm2l)(int maxlev, int n, int r, const real *U, const real *Kweig
                       const real *PF, real L, real *fieldval)
 {
   int n3 = n * n * n;
+  real *tmp = (real *)malloc(sizeof(real) * n3);
   for (int level = MINLEV; level <= maxlev; level++) {
     real Lc = L;
     for (int i = 0; i < level; i++) Lc *= 0.5;
     real scale = POW(ONE / Lc, (real)g_homogen);
-    for (int A = SFX(orc_levsta)(level); A < SFX(orc_levsta)(level + 1); A++)
-      for (int i = 0; i < n3; i++) {
-        real sum = ZERO;
-        for (int j = 0; j < r; j++) sum += U[i + (size_t)n3 * j] * PF[(size_t)r * A + j];
-        fieldval[(size_t)n3 * A + i] = scale * Kweights[i] * sum;
+    for (int A = SFX(orc_levsta)(level); A < SFX(orc_levsta)(level + 1); A++) {
+      /* every sum over j in order, the loop over i inner (contiguous columns of U) */
+      for (int i = 0; i < n3; i++) tmp[i] = ZERO;
+      for (int j = 0; j < r; j++) {
+        const real pj = PF[(size_t)r * A + j];
+        const real *col = &U[(size_t)n3 * j];
+        for (int i = 0; i < n3; i++) tmp[i] += col[i] * pj;
       }
+      for (int i = 0; i < n3; i++) fieldval[(size_t)n3 * A + i] = scale * Kweights[i] * tmp[i];
+    }
   }
+  free(tmp);
 }
 
 /* --------------------------------------------------------------- downward --- */

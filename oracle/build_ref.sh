@@ -12,7 +12,9 @@
 # Flags follow the reference's own recipes (www.sh:23-36, zzz.sh:209-212) with gcc,
 # -fcommon (bbfmm.h defines globals in a header) and gettimeofday timers. BLAS/LAPACK
 # (?gesvd, ?gemm, ?dot) come from the OpenBLAS that ships inside the opencv wheel of
-# this image. Usage: oracle/build_ref.sh [reference-dir]
+# this image. Usage: oracle/build_ref.sh [reference-dir]; without an argument the
+# directory comes from BBFMM_REFERENCE_DIR, else the reference checkout's location in the
+# build container. Exit code 2: no reference sources there (nothing built).
 set -euo pipefail
 REF=${1:-${BBFMM_REFERENCE_DIR:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)

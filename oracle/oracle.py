@@ -106,6 +106,91 @@ class Oracle:
                            _p(tree.iinter), _p(tree.interaction), _p(Kt), self.R(L), _p(PF))
         return PF
 
+    def m2l_pairs(self, r, E, M, cell, src, k, acc):
+        """acc[cell[p]] += E_{k[p]} M[src[p]] for the pairs in order (orc_m2l_pairs)."""
+        cell = np.ascontiguousarray(cell, np.int32)
+        src = np.ascontiguousarray(src, np.int64)
+        k = np.ascontiguousarray(k, np.int32)
+        self._f("orc_m2l_pairs")(r, _p(E), _p(M), C.c_longlong(cell.size), _p(cell), _p(src), _p(k), _p(acc))
+
+    def _pairs_threaded(self, r, E, M, cell, src, k, acc, threads):
+        """Runs the pairs in `threads` chunks of whole target cells (disjoint rows of acc),
+        each chunk sorted by operator so that every E_k block is read once per chunk. ctypes
+        releases the GIL during the C call, so the chunks run in parallel."""
+        from concurrent.futures import ThreadPoolExecutor
+        E = self._arr(E)
+        M = self._arr(M)
+        order = np.argsort(cell, kind="stable")
+        cell, src, k = cell[order], src[order], k[order]
+        cuts = np.linspace(0, cell.size, threads + 1).astype(np.int64)
+        # move each cut to a cell boundary so that no cell is split between chunks
+        cuts = np.unique(np.searchsorted(cell, cell[np.minimum(cuts, cell.size - 1)], side="left").tolist()
+                         + [0, cell.size])
+        jobs = []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            o = np.argsort(k[a:b], kind="stable")
+            jobs.append((cell[a:b][o], src[a:b][o], k[a:b][o]))
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(lambda j: self.m2l_pairs(r, E, M, *j, acc), jobs))
+
+    def m2l_parallel(self, tree, r, E, M, L=1.0, threads=None):
+        """PF of orc_m2l (every level's M2L over the tree's interaction lists), computed with
+        orc_m2l_pairs on all host cores: the same products, summed in operator order per cell
+        instead of list order (agrees with orc_m2l to rounding)."""
+        threads = threads or os.cpu_count() or 1
+        _, Kt, _, _ = self.weights(4)
+        PF = np.zeros(ncell(tree.maxlev) * r, self.dt)
+        for level in range(2, tree.maxlev + 1):
+            lo, hi = levsta(level), levsta(level + 1)
+            cnt = tree.iinter[lo:hi].astype(np.int64)
+            F = np.repeat(np.arange(lo, hi, dtype=np.int64), cnt)
+            slot = np.arange(F.size) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+            S = tree.interaction[F * PITCH_INTERACTION + slot].astype(np.int64)
+            cen = tree.center.reshape(-1, 3).astype(np.float64)
+            Lc = L * 0.5 ** level
+            v = np.rint((cen[S] - cen[F]) / Lc).astype(np.int64)
+            k = Kt[49 * (v[:, 0] + 3) + 7 * (v[:, 1] + 3) + (v[:, 2] + 3)]
+            self._pairs_threaded(r, E, M, F.astype(np.int32), S, k, PF, threads)
+        return PF
+
+    def fmm_staged(self, xyz, q, n, maxlev, U, E, L=1.0, threads=None):
+        """The oracle FMM (orc_fmm's stages: tree, upward, M2L, post-M2L, downward, near field)
+        with the M2L of m2l_parallel, for depths where the single-threaded M2L is too slow."""
+        r = U.size // n ** 3
+        tree = self.build_tree(xyz, maxlev, L)
+        _, P = self.upward(tree, xyz, q, n, U, L)
+        PF = self.m2l_parallel(tree, r, E, P, L, threads)
+        F = self.postm2l(tree, n, U, PF, L)
+        phi, _ = self.downward(tree, xyz, q, n, F, L)
+        return self.nearfield(tree, xyz, q, phi)
+
+    def m2l_sample(self, level, r, E, M_level, cells, threads=None):
+        """M2L output rows of the given cells of `level` (Morton indices within the level) from
+        that level's multipoles M_level (Morton order, r per cell): each cell's interaction list
+        (the children of its parent's neighbours that are not its own neighbours, as
+        anotherInteractionList.c:11-111 forms it) is enumerated from the grid, so no tree arrays
+        are needed at any depth. Rows in the order of `cells`."""
+        threads = threads or os.cpu_count() or 1
+        _, Kt, _, _ = self.weights(4)
+        cells = np.asarray(cells, np.int64)
+        ix, iy, iz = morton_to_grid(cells, level)
+        m = 2 ** level
+        d = np.arange(-2, 4)
+        dx, dy, dz = [a.reshape(-1) for a in np.meshgrid(d, d, d, indexing="ij")]
+        # source grid coordinates: children of the parent's 3 x 3 x 3 neighbourhood
+        jx = (ix[:, None] // 2) * 2 + dx[None, :]
+        jy = (iy[:, None] // 2) * 2 + dy[None, :]
+        jz = (iz[:, None] // 2) * 2 + dz[None, :]
+        vx, vy, vz = jx - ix[:, None], jy - iy[:, None], jz - iz[:, None]
+        ok = ((jx >= 0) & (jx < m) & (jy >= 0) & (jy < m) & (jz >= 0) & (jz < m)
+              & (np.maximum(np.maximum(abs(vx), abs(vy)), abs(vz)) > 1))
+        row = np.broadcast_to(np.arange(cells.size)[:, None], ok.shape)[ok]
+        src = grid_to_morton(jx[ok], jy[ok], jz[ok], level)
+        k = Kt[49 * (vx[ok] + 3) + 7 * (vy[ok] + 3) + (vz[ok] + 3)]
+        acc = np.zeros(cells.size * r, self.dt)
+        self._pairs_threaded(r, E, M_level, row.astype(np.int32), src, k, acc, threads)
+        return acc.reshape(cells.size, r)
+
     def postm2l(self, tree, n, U, PF, L=1.0):
         r = U.size // n ** 3
         _, _, Kw, _ = self.weights(n)
@@ -256,6 +341,26 @@ class Reference:
         phi = np.zeros(q.size, self.dt)
         self.lib.ref_direct(q.size, _p(xyz), _p(q), self.R(L), _p(phi))
         return phi
+
+
+def morton_to_grid(m, level):
+    """Grid coordinates of Morton cell indices (anotherFMMDistribute.c:239-253 bit order)."""
+    m = np.asarray(m, np.int64)
+    ix = np.zeros_like(m); iy = np.zeros_like(m); iz = np.zeros_like(m)
+    for b in range(level):
+        t = (m >> (3 * b)) & 7
+        ix |= ((t >> 2) & 1) << b
+        iy |= ((t >> 1) & 1) << b
+        iz |= (t & 1) << b
+    return ix, iy, iz
+
+
+def grid_to_morton(ix, iy, iz, level):
+    ix, iy, iz = (np.asarray(a, np.int64) for a in (ix, iy, iz))
+    m = np.zeros_like(ix)
+    for b in range(level):
+        m |= (((ix >> b) & 1) << (3 * b + 2)) | (((iy >> b) & 1) << (3 * b + 1)) | (((iz >> b) & 1) << (3 * b))
+    return m
 
 
 def rel_l2(a, b) -> float:

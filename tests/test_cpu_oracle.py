@@ -108,3 +108,27 @@ def test_known_answers_other_kernels(kernel, oracle_d):
     assert rel_l2(dref[:64], _hexarr(G[f"direct_d_N32768_{kernel}_first64"], np.float64)) < 1e-13
     want = G[f"kat_d_n4_l3_{kernel}"]
     assert abs(rel_l2(phi, dref) - want) <= 1e-7 * want
+
+
+@pytest.mark.parametrize("n,lev", [(4, 3), (4, 4), (8, 3)])
+def test_staged_oracle_and_sampled_m2l(oracle_d, n, lev):
+    """The oracle's threaded, operator-sorted M2L (fmm_staged) agrees with orc_fmm to rounding,
+    and the M2L of sampled cells with interaction lists enumerated from the grid
+    (m2l_sample, used at depths whose explicit lists are too large) agrees with the M2L over
+    the tree's explicit lists, which equal the reference's bitwise."""
+    from bbfmm_b200 import operators as ops
+    from oracle.oracle import levsta, rel_l2
+    _, U, E = ops.load_operators(n, single=False)
+    rng = np.random.default_rng(n + lev)
+    N = 8000 * lev
+    x = rng.random((N, 3)) - 0.5
+    q = rng.uniform(-1, 1, N)
+    assert rel_l2(oracle_d.fmm_staged(x, q, n, lev, U, E), oracle_d.fmm(x, q, n, lev, U, E)) < 1e-14
+    r = n ** 3 // 2
+    tree = oracle_d.build_tree(x, lev)
+    _, P = oracle_d.upward(tree, x, q, n, U)
+    PF = oracle_d.m2l(tree, r, E, P)
+    lo = levsta(lev)
+    cells = rng.choice(8 ** lev, 40, replace=False)
+    got = oracle_d.m2l_sample(lev, r, E, P[lo * r:(lo + 8 ** lev) * r], cells)
+    assert rel_l2(got, PF[lo * r:(lo + 8 ** lev) * r].reshape(-1, r)[cells]) < 1e-14

@@ -50,6 +50,40 @@ def test_oracle_equals_reference(prec, variant, tol, opdir, oracle_d, oracle_s):
     assert rel_l2(phio, phir) < tol
 
 
+@pytest.mark.parametrize("prec,variant,tol", [("d", "cpu8a", 1e-14), ("d", "cpu9a", 1e-14),
+                                              ("s", "cpu8a", 1e-6), ("s", "cpu9a", 1e-6)])
+def test_oracle_equals_reference_n8(prec, variant, tol, oracle_d, oracle_s):
+    """n = 8 (r = 256) at depth 3, on operator files written by bbfmm_b200.operators in the
+    reference's format and read by the reference itself: tree and lists bitwise, upward-pass
+    multipoles bitwise, potentials within tol (M2L summation order; the oracle's M2L here is
+    the operator-sorted threaded form, Oracle.fmm_staged)."""
+    if not reference_available(prec, variant):
+        pytest.skip("variant not built")
+    from bbfmm_b200 import operators as ops
+    R = Reference(prec, variant)
+    O = oracle_d if prec == "d" else oracle_s
+    single = prec == "s"
+    _, U, E = ops.load_operators(8, single=single)
+    d = tempfile.mkdtemp()
+    ops.write_operator_files(d, 8, U, E, single)
+    kp, up = (os.path.join(d, f) for f in ops.operator_file_names(8, single))
+    U = np.fromfile(up, dtype=O.dt, offset=4)
+    E = np.fromfile(kp, dtype=O.dt)
+    rng = np.random.default_rng(8)
+    x = (rng.random((20000, 3)) - 0.5).astype(O.dt)
+    q = rng.uniform(-1, 1, 20000).astype(O.dt)
+    lev = 3
+    tr, to = R.build_tree(x, 8, lev), O.build_tree(x, lev)
+    for k in ("center", "fieldlist", "sta", "end", "ineigh", "neighbors", "iinter", "interaction"):
+        assert np.array_equal(getattr(tr, k), getattr(to, k)), k
+    phir, Pr, _ = R.fmm(x, q, 8, lev, kp, up, want_intermediates=True)
+    _, Po = O.upward(to, x, q, 8, U)
+    lo = 9 * 256  # levels >= 2
+    assert np.array_equal(Pr[lo:], Po[lo:])
+    phio = O.fmm_staged(x, q, 8, lev, U, E)
+    assert rel_l2(phio, phir) < tol, rel_l2(phio, phir)
+
+
 @pytest.mark.skipif(not reference_available("d", kernel="oneoverr4"), reason="1/r^4 reference build absent")
 def test_oracle_equals_reference_oneoverr4(oracle_d):
     """The 1/r^4 kernel (ONEOVERR4, homogeneity 4): the oracle against the reference's

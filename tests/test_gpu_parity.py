@@ -109,15 +109,27 @@ def test_host_entry_matches_device_entry():
     s.close()
 
 
+def _clustered(N, seed, k=4, sigma=0.02):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-0.4, 0.4, (k, 3))
+    x = np.clip(c[rng.integers(0, k, N)] + sigma * rng.standard_normal((N, 3)), -0.5, np.nextafter(0.5, 0))
+    return x, rng.uniform(-1.0, 1.0, N)
+
+
 @pytest.mark.parametrize("mode,tol", [(0, 1e-13), (2, 1e-6)])
-def test_near_field_entry_matches_oracle(oracle_d, mode, tol):
+@pytest.mark.parametrize("layout", ["dense", "sparse", "clustered"])
+def test_near_field_entry_matches_oracle(oracle_d, mode, tol, layout):
     """bbfmm_b200_near_field on caller-owned device arrays vs the oracle's P2P
-    (anotherNearField semantics). FP64 mode: 1e-13; mixed mode (FP32 reciprocal distances): 1e-6."""
+    (anotherNearField semantics). FP64 mode: 1e-13; mixed mode (FP32 reciprocal distances): 1e-6.
+    Layouts: ~12 particles per leaf (every 4 x 4 x 4 block is split into per-leaf chunks),
+    ~1.5 per leaf (whole blocks staged at once), and 4 tight clusters at depth 5 (both kinds,
+    empty blocks, and leaves of several hundred particles whose neighbourhoods stream through
+    shared memory in many tiles)."""
     import ctypes as C
     import torch
     from bbfmm_b200 import _lib
-    N, lev = 50000, 4
-    x, q = uniform_inputs(N, seed=31)
+    N, lev = 50000, {"dense": 4, "sparse": 5, "clustered": 5}[layout]
+    x, q = _clustered(N, 32) if layout == "clustered" else uniform_inputs(N, seed=31)
     tree = oracle_d.build_tree(x, lev)
     want = oracle_d.nearfield(tree, x, q, np.zeros(N))
     perm = np.zeros(N, dtype=np.int32)

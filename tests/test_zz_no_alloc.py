@@ -61,7 +61,8 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("mode", [0, 2])  # BBFMM_B200_MODE_D, BBFMM_B200_MODE_MIXED
 def test_noalloc_matches_allocating_entry_twice(mode):
-    for call, (N, seed) in enumerate([(200_000, 1), (150_000, 2)]):
+    # the last call fills the static scratch to its stated capacity
+    for call, (N, seed) in enumerate([(200_000, 1), (150_000, 2), (262_144, 3)]):
         xyzq, ls = _sorted_inputs(N, seed)
         want = _near("bbfmm_b200_near_field", xyzq, ls, mode)
         got = _near("bbfmm_b200_near_field_noalloc", xyzq, ls, mode)
@@ -79,3 +80,40 @@ def test_noalloc_rejects_oversize():
                                                   C.c_void_p(ls.data_ptr()), C.c_void_p(buf.data_ptr()), 0, None)
     assert rc == 1
     assert b"262144" in _lib.lib().bbfmm_b200_last_error()
+
+
+@pytest.mark.parametrize("entry", ["bbfmm_b200_near_field", "bbfmm_b200_near_field_noalloc"])
+@pytest.mark.parametrize("fault", ["past_n", "decreasing"])
+def test_malformed_leaf_offsets_are_refused(entry, fault):
+    """Leaf offsets that end past N or decrease are refused with BBFMM_B200_ERR_ARG and the
+    leaf-range code in the status word. The arrays are sized for N + 16 particles, so even an
+    access the clamps failed to stop would stay inside memory the test owns."""
+    import torch
+    from bbfmm_b200 import _lib
+    N = 5000
+    xyzq, ls = _sorted_inputs(N + 16, 4)
+    ls = ls.copy()
+    if fault == "past_n":
+        pass                                   # offsets end at N + 16 but the call says N
+    else:
+        k = int(np.searchsorted(ls, N // 2))
+        ls[k] = ls[k + 1] + 3                  # one offset above its successor
+        ls[-1] = N
+        ls = np.minimum(ls, N)
+    dx = torch.as_tensor(xyzq, device="cuda")
+    dl = torch.as_tensor(ls, device="cuda")
+    phi = torch.zeros(N + 16, dtype=torch.float64, device="cuda")
+    lib = _lib.lib()
+    lib.bbfmm_b200_device_status(1)
+    rc = getattr(lib, entry)(N, MAXLEV, L, C.c_void_p(dx.data_ptr()), C.c_void_p(dl.data_ptr()),
+                             C.c_void_p(phi.data_ptr()), 0, None)
+    torch.cuda.synchronize()
+    assert rc == 1, rc
+    assert b"leaf_start" in lib.bbfmm_b200_last_error()
+    assert lib.bbfmm_b200_device_status(1) == 98       # BBFMM_B200_LEAF_RANGE_CODE
+    assert float(phi[N:].abs().max()) == 0.0           # nothing written past N
+    # the context stays usable: a well-formed call right after succeeds
+    xyzq2, ls2 = _sorted_inputs(N, 5)
+    got = _near(entry, xyzq2, ls2, 0)
+    assert np.all(np.isfinite(got))
+    assert lib.bbfmm_b200_device_status(1) == 0
