@@ -50,8 +50,11 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   const int bw = P < 4 ? P : 4;
   const int nbox = P / bw;
   const int tiles_per_class = nbox * nbox * nbox;
-  const int c = blockIdx.x / tiles_per_class;
-  const int tb = blockIdx.x % tiles_per_class;
+  // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
+  // of neighbouring boxes, which read one source region that stays in L2
+  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int c = set_ * 8 + loc_ % 8;
+  const int tb = loc_ / 8;
   const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
   const int nt = bw * bw * bw;
@@ -172,8 +175,11 @@ __global__ void __launch_bounds__(256) m2l_lead_kernel(const double *__restrict_
   const int bwx = NT == 128 ? 8 : bw;  // box extent in x (y and z: bw)
   const int nbx = P / bwx, nbox = P / bw;
   const int tiles_per_class = nbx * nbox * nbox;
-  const int c = blockIdx.x / tiles_per_class;
-  const int tb = blockIdx.x % tiles_per_class;
+  // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
+  // of neighbouring boxes, which read one source region that stays in L2
+  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int c = set_ * 8 + loc_ % 8;
+  const int tb = loc_ / 8;
   const int bxo = (tb % nbx) * bwx, byo = ((tb / nbx) % nbox) * bw, bzo = (tb / (nbx * nbox)) * bw;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
   const int nt = bwx * bw * bw;

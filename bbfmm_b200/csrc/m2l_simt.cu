@@ -41,8 +41,11 @@ __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T 
   const int bw = P < 4 ? P : 4;  // box width per dimension
   const int nbox = P / bw;
   const int tiles_per_class = nbox * nbox * nbox;
-  const int c = blockIdx.x / tiles_per_class;
-  const int tb = blockIdx.x % tiles_per_class;
+  // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
+  // of neighbouring boxes, which read one source region that stays in L2
+  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int c = set_ * 8 + loc_ % 8;
+  const int tb = loc_ / 8;
   const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
   const int nt = bw * bw * bw;

@@ -191,8 +191,11 @@ __global__ void __launch_bounds__(192, 1)
   const int P = 1 << (level - 1);
   const int nbx = P / BOX_X, nby = P / BOX_Y, nbz = P / BOX_Z;
   const int tiles_per_class = nbx * nby * nbz;
-  const int c = blockIdx.x / tiles_per_class;
-  const int tb = blockIdx.x % tiles_per_class;
+  // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
+  // of neighbouring boxes, which read one source region that stays in L2
+  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int c = set_ * 8 + loc_ % 8;
+  const int tb = loc_ / 8;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
   const int nchunk = ncols / BK;  // K-chunks per offset: the effective rank / 32 (8 for r = 256)
@@ -352,8 +355,11 @@ __global__ void __launch_bounds__(192, 1)
   const int P = 1 << (level - 1);
   const int nbx = P / BOX_X, nby = P / BOX2_Y, nbz = P / BOX_Z;
   const int tiles_per_class = nbx * nby * nbz;
-  const int c = blockIdx.x / tiles_per_class;
-  const int tb = blockIdx.x % tiles_per_class;
+  // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
+  // of neighbouring boxes, which read one source region that stays in L2
+  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int c = set_ * 8 + loc_ % 8;
+  const int tb = loc_ / 8;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX2_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
   const int nchunk = ncols / BK;  // K-chunks per offset: the effective rank / 32 (8 for r = 256)

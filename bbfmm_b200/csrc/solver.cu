@@ -581,6 +581,9 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   const T *Ml = Mall + Moff[level];
   const bool split = mode == MODE_MIXED && tcops && level >= TC_MIN_LEVEL && tune.m2l_kind[level] == 0;
   const bool fused = split && lead > 0 && tc_fuses_lead(tcops, tc_products, rk());
+  // the launch as the solve makes it: a whole level with the mixed projections also writes
+  // the split rows of the down projection (m2l_post)
+  const bool presplit = fused && proj_tc() && cells(level) <= Lsplit_rows && !(level == maxlev && slabbed());
   int rc = BBFMM_OK;
   float tot[2] = {0.f, 0.f};
   for (int part = 0; part < (split ? 2 : 1) && rc == BBFMM_OK; ++part) {
@@ -589,7 +592,7 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
       if (!split) rc = m2l_fp(Ml, level, 0, rk(), rk());
       else if (part == 0) rc = launch_m2l_tc(r, Msplit, Mcells(), Moff[level] / r, tcops, (double *)Lbuf, level, offs,
                                              stream, nsets, tc_products, rk(), fused ? (const double *)Ml : nullptr,
-                                             fused ? (const double *)Ert : nullptr);
+                                             fused ? (const double *)Ert : nullptr, presplit ? Lsplit : nullptr);
       else rc = lead > 0 && !fused ? m2l_fp(Ml, level, 0, lead, lead_rows) : BBFMM_OK;
     }
     cudaEventRecord(b, stream);
@@ -607,8 +610,12 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
 template <typename T>
 int Solver<T>::near(T *pot, T *fld) {
   if (near_threads != tune.p2p_threads) TRY(build_near_work());
-  TRY(launch_near(mode, homogen, N, pos4, leaf_start, maxlev, near_work, nsets, near_items, near_threads, pot, fld,
-                  stream));
+  // The mixed mode's 1/r^4 near field runs in FP64: that kernel's potentials are near-field
+  // dominated and its FP64 FMM error (3e-11 against the direct sum at n = 8) is far below the
+  // ~1e-7 relative rounding of FP32 pair terms; its M2L and projections stay split-BF16.
+  const int near_mode = mode == MODE_MIXED && homogen == 4 ? (int)MODE_D : mode;
+  TRY(launch_near(near_mode, homogen, N, pos4, leaf_start, maxlev, near_work, nsets, near_items, near_threads, pot,
+                  fld, stream));
   mark(ST_P2P);
   return BBFMM_OK;
 }
@@ -1015,9 +1022,6 @@ int bbfmm_b200_set_kernel(bbfmm_b200_solver *h, int kernel) {
   if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && kernel != BBFMM_B200_KERNEL_LAPLACIAN_FORCE &&
       kernel != BBFMM_B200_KERNEL_ONEOVERR4)
     return bbfmm_set_error(BBFMM_ERR_ARG, "unknown kernel");
-  const int mode = h->f ? h->f->mode : h->d->mode;
-  if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && mode == bbfmm::MODE_MIXED)
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "the x / r^3 and 1/r^4 kernels run in modes D and S");
   const int hg = kernel == BBFMM_B200_KERNEL_ONEOVERR4 ? 4 : (kernel == BBFMM_B200_KERNEL_LAPLACIAN_FORCE ? 2 : 1);
   if (h->f) h->f->homogen = hg;
   else h->d->homogen = hg;

@@ -70,8 +70,6 @@ class Solver:
         self.np_dtype = np.float32 if mode == "s" else np.float64
         if kernel not in ops.KERNELS:
             raise ValueError(f"unknown kernel {kernel!r} ({', '.join(ops.KERNELS)})")
-        if kernel != "laplacian" and mode == "mixed":
-            raise ValueError("the mixed mode is built for the 1/r kernel; use mode 'd' or 's'")
         self.kernel = kernel
         if operators is None:
             _, U, E = ops.load_operators(n, single=(mode == "s"), kernel=kernel)

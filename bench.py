@@ -33,9 +33,74 @@ MAXLEV = 7
 N_TARGETS = 4096
 METRIC = "FMM solves/s at N=4,194,304, n=8, depth 7 (1 GPU; err <= 1.2x FP64 required)"
 # DRAM bytes of one m2l_tc2_kernel launch per cell of its level, from an ncu capture of the
-# level-5 launch (32,768 cells: 82.9 MB read + 14.5 MB written); the traffic scales with
-# the number of cells (multipole split in, FP64 M2L output read-modify-written).
-TC_DRAM_BYTES_PER_CELL = (77.765632e6 + 4.091136e6) / 32768
+# level-6 launch of a depth-6 solve in the form the solve makes it (split rows of the down
+# projection written; profiles/m2l_tc2_n8_level6_traffic.md); the traffic scales with the
+# number of cells (multipoles in, FP64 output and split rows out): 885.2 MB read + 299.2 MB
+# written for 262,144 cells.
+TC_DRAM_BYTES_PER_CELL = (885159936 + 299155712) / 262144
+SMS, MAX_SM_MHZ = 148, 1965.0
+# FP64 tensor (DMMA) peak: 128 FP64 flops per clock per SM (profiles/m2l_lead_n8_level5.md)
+DMMA_TFLOPS = SMS * 128 * MAX_SM_MHZ * 1e6 / 1e12
+# FP32 SIMT peak (an FMA as two flops per lane, 128 lanes per SM)
+FP32_TFLOPS = SMS * 256 * MAX_SM_MHZ * 1e6 / 1e12
+# Near-field roof of the survey: min(FP32 issue / 7 FP32 operations per pair, reciprocal
+# square roots at 16 per clock per SM), in pairs/s at the maximum SM clock
+P2P_ROOF_PAIRS = min(SMS * 128 * MAX_SM_MHZ * 1e6 / 7, SMS * 16 * MAX_SM_MHZ * 1e6)
+
+
+def morton_to_grid(m, level):
+    m = np.asarray(m, np.int64)
+    ix, iy, iz = (np.zeros_like(m) for _ in range(3))
+    for b in range(level):
+        t = (m >> (3 * b)) & 7
+        ix |= ((t >> 2) & 1) << b
+        iy |= ((t >> 1) & 1) << b
+        iz |= (t & 1) << b
+    return ix, iy, iz
+
+
+def leaf_counts(x, maxlev, L=1.0):
+    """Particles per leaf on the (2^maxlev)^3 grid, from the library's own leaf sort."""
+    import ctypes as C
+    from bbfmm_b200 import _lib
+    x = np.ascontiguousarray(x, np.float64)
+    N = x.shape[0]
+    perm = np.zeros(N, np.int32)
+    ls = np.zeros(8 ** maxlev + 1, np.int32)
+    _lib.check(_lib.lib().bbfmm_b200_sort_particles(N, 0, C.c_void_p(x.ctypes.data), L, maxlev,
+                                                    perm.ctypes.data_as(C.POINTER(C.c_int)),
+                                                    ls.ctypes.data_as(C.POINTER(C.c_int))))
+    m = 2 ** maxlev
+    g = np.zeros((m, m, m), np.int64)
+    ix, iy, iz = morton_to_grid(np.arange(8 ** maxlev), maxlev)
+    g[ix, iy, iz] = np.diff(ls)
+    return g
+
+
+def near_pairs(counts):
+    """Pair evaluations of the near field, exact from the tree: sum_A n_A sum_{B in N(A)} n_B
+    over the leaves and their <= 27 neighbours (anotherNearField.c:326-336; self pairs, which
+    the kernels skip, included)."""
+    m = counts.shape[0]
+    p = np.pad(counts, 1)
+    nb = sum(p[1 + dx:1 + dx + m, 1 + dy:1 + dy + m, 1 + dz:1 + dz + m]
+             for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1))
+    return int((counts * nb).sum())
+
+
+def pass_bytes(n, maxlev, N, nonempty, mixed):
+    """Algorithmic HBM bytes of the passes of one solve (FP64 node values, 8 B each):
+    P2M reads the particles (32 B) and writes the leaves' n^3 values (plus their BF16 hi/lo
+    split in the mixed mode); M2M reads 8 children and writes the parent per parent cell;
+    L2L reads the parent and reads and writes the 8 children; L2P reads the n^3 values of the
+    non-empty leaves and the particles and writes phi."""
+    n3b = n ** 3 * 8
+    leaves = 8 ** maxlev
+    par = sum(8 ** l for l in range(2, maxlev))  # parents of levels 3 .. maxlev
+    return {"p2m": 32 * N + leaves * n3b + (leaves * n ** 3 * 4 if mixed else 0),
+            "m2m": par * (8 * n3b + n3b),
+            "l2l": par * (n3b + 2 * 8 * n3b),
+            "l2p": nonempty * n3b + 40 * N}
 
 
 def interactions_per_level(level: int) -> int:
@@ -623,6 +688,87 @@ def run_batch_256(args):
     return 0
 
 
+def layout_inputs(N, layout, seed=2):
+    """Seeded positions in the origin-centred unit root cell and charges U[-1, 1]: "uniform",
+    or "clustered" (4 Gaussian clusters, sigma 0.04, centres U[0.1, 0.9]^3, clipped -- the
+    clustered sets of the 256-set batch)."""
+    rng = np.random.default_rng(seed)
+    if layout == "uniform":
+        x = rng.random((N, 3))
+    else:
+        c = rng.uniform(0.1, 0.9, (4, 3))
+        x = np.clip(c[rng.integers(0, 4, N)] + 0.04 * rng.standard_normal((N, 3)), 0.0, np.nextafter(1.0, 0.0))
+    return np.ascontiguousarray(x - 0.5), rng.uniform(-1.0, 1.0, N)
+
+
+def run_near_field(args):
+    """The near field alone through the caller-owned entry point bbfmm_b200_near_field (mode
+    MIXED; leaf-sorted FP64 particles and leaf offsets on the device), timed per call with CUDA
+    events around the call (it builds its work list and synchronises); pairs exact from the tree."""
+    import ctypes as C
+    import torch
+    from bbfmm_b200 import _lib
+    N, lev = args.N, args.maxlev
+    x, q = layout_inputs(N, args.layout)
+    perm = np.zeros(N, np.int32)
+    ls = np.zeros(8 ** lev + 1, np.int32)
+    L = _lib.lib()
+    _lib.check(L.bbfmm_b200_sort_particles(N, 0, C.c_void_p(x.ctypes.data), 1.0, lev,
+                                           perm.ctypes.data_as(C.POINTER(C.c_int)),
+                                           ls.ctypes.data_as(C.POINTER(C.c_int))))
+    dx = torch.as_tensor(np.concatenate([x[perm], q[perm, None]], axis=1), device="cuda")
+    dl = torch.as_tensor(ls, device="cuda")
+    phi = torch.zeros(N, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def call():
+        _lib.check(L.bbfmm_b200_near_field(N, lev, 1.0, C.c_void_p(dx.data_ptr()), C.c_void_p(dl.data_ptr()),
+                                           C.c_void_p(phi.data_ptr()), 2, C.c_void_p(stream.cuda_stream)))
+    for _ in range(args.warmup):
+        call()
+    t = _device_time(call, max(args.steps, 1), stream)
+    pairs = near_pairs(leaf_counts(x, lev))
+    line = {"metric": f"near-field pair evaluations/s, N={N} {args.layout}, depth {lev}",
+            "value": pairs / t, "unit": "pair/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 separation + f32 terms", "data": f"synthetic ({args.layout}, seeded)",
+            "config": {"workload": "bbfmm_b200_near_field (MIXED)", "N": N, "maxlev": lev, "layout": args.layout},
+            "pairs": pairs, "frac_of_roof": pairs / t / P2P_ROOF_PAIRS}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_stages(args):
+    """Per-stage device times (CUDA events between stages) of one solver configuration: the
+    best of `steps` timed solves after `warmup` plain ones."""
+    import torch
+    from bbfmm_b200 import Solver
+    x, q = layout_inputs(args.N, args.layout)
+    s = Solver(N_ORDER, args.maxlev, 1.0, mode=args.mode)
+    s.set_particles(x)
+    qd = torch.as_tensor(q, dtype=s.dtype, device="cuda")
+    out = torch.empty_like(qd)
+    for _ in range(args.warmup):
+        s.solve(qd, out=out)
+    s.set_timing(True)
+    best = {}
+    for _ in range(max(args.steps, 1)):
+        s.solve(qd, out=out)
+        torch.cuda.synchronize()
+        st, launches = s.stage_times()
+        best = {k: min(best.get(k, 1e30), v) for k, v in st.items()}
+    line = {"metric": f"stage times of one solve, N={args.N} {args.layout}, n={N_ORDER}, depth {args.maxlev}",
+            "value": sum(best.values()), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sum(best.values()), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"mixed": "bf16x3+f64", "d": "f64", "s": "f32"}[args.mode],
+            "data": f"synthetic ({args.layout}, seeded)",
+            "config": {"workload": "one solve, stage by stage", "N": args.N, "maxlev": args.maxlev, "mode": args.mode,
+                       "layout": args.layout},
+            "stages_ms": best, "near_pairs": near_pairs(leaf_counts(x, args.maxlev))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def reference_sample_xq(x, q, n, lev):
     """Seconds of one reference CPU solve of the given particles (n, depth lev)."""
     from oracle.oracle import Reference
@@ -658,8 +804,10 @@ def main():
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
     ap.add_argument("--workload", default="uniform-4m",
                     choices=["uniform-4m", "uniform-4m-variants", "uniform-32k", "gradient-1m", "batch-256",
-                             "clustered-16m"],
+                             "clustered-16m", "near-field", "stages"],
                     help="uniform-4m: the headline line; the others measure further configurations")
+    ap.add_argument("--layout", default="uniform", choices=["uniform", "clustered"],
+                    help="near-field / stages workloads: particle layout")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -673,6 +821,10 @@ def main():
         return run_batch_256(args)
     if args.workload == "clustered-16m":
         return run_clustered_16m(args)
+    if args.workload == "near-field":
+        return run_near_field(args)
+    if args.workload == "stages":
+        return run_stages(args)
 
     import torch
     import torch.distributed as dist
@@ -775,8 +927,18 @@ def main():
     sol.set_timing(False)
     m2l_ms, lead_ms = sol.time_m2l(lev, reps=3)
     I_leaf = interactions_per_level(lev)
+    I_all = sum(interactions_per_level(l) for l in range(2, lev + 1))
     r = n ** 3 // 2
     hbm, bf16, bf16_sus, peak_src = measured_peaks()
+    clk_now = clk.summary()
+    sm_mhz = clk_now["sm_mhz"] or MAX_SM_MHZ
+    # M2L flop counts: 2 r^2 per (target, source) pair, and the reference's own r (2r - 1)
+    # (m2l_aux.c:967-979), for the leaf launch and for all levels of the step
+    m2l_counts = {"pairs_leaf_level": I_leaf, "pairs_all_levels": I_all,
+                  "leaf_launch_gflops_2r2": 2.0 * r * r * I_leaf / (m2l_ms / 1e3) / 1e9,
+                  "leaf_launch_gflops_reference_count": r * (2 * r - 1) * I_leaf / (m2l_ms / 1e3) / 1e9,
+                  "stage_gflops_2r2": 2.0 * r * r * I_all / (stages["m2l"] / 1e3) / 1e9,
+                  "stage_gflops_reference_count": r * (2 * r - 1) * I_all / (stages["m2l"] / 1e3) / 1e9}
     if args.mode == "mixed":
         # MMA work the leaf launch executes: every target of the level against all 189 offsets
         # (zero-filled out-of-grid sources included), per 32-component chunk hi*hi over the 256
@@ -785,28 +947,44 @@ def main():
         split_chunks, split_rows, chunks = 2, 64, r // 32  # TC_SPLIT_CHUNKS, TC_SPLIT_ROWS
         macs_per_pair = 32 * (split_chunks * (256 + 2 * split_rows) + (chunks - split_chunks) * 256)
         exec_flop = 2.0 * macs_per_pair * 189 * 8 ** lev
-        tc_flop = 2.0 * r * (r - sol.lead) * I_leaf           # algorithmic flops of the tensor-core part
         achieved = exec_flop / (m2l_ms / 1e3) / 1e12
-        # the launch is timed back to back inside a long power-capped step: sustained peak
-        roof = {"kernel": "m2l_tc2 (split-bf16 tcgen05 M2L with the FP64 leading block, leaf level)",
-                "bound": "tensor",
-                "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s", "frac": achieved / bf16_sus,
-                "peak_source": f"{peak_src} bf16 dense sustained",
+        # the launch is timed alone (bbfmm_b200_time_m2l, 3 launches back to back): burst peak
+        roof = {"kernel": "m2l_tc2_kernel (split-bf16 tcgen05 M2L with the FP64 leading block, leaf level, "
+                          "timed alone in the form the solve launches it)",
+                "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                "peak_source": f"{peak_src} bf16 dense burst (the launch is timed alone)",
                 "achieved_note": "executed BF16 MMA flops (adaptive split-BF16 product map) / launch time; "
                                  "the same launch also runs the FP64 leading block (i < 32, j < 16) on DMMA",
+                "clock_normalised": {"sm_mhz_median_of_step": sm_mhz,
+                                     "launch_ms_at_max_clock": m2l_ms * sm_mhz / MAX_SM_MHZ,
+                                     "frac_at_max_clock": achieved * MAX_SM_MHZ / sm_mhz / bf16},
+                "algorithmic_tflops": 2.0 * r * r * I_leaf / (m2l_ms / 1e3) / 1e12,
+                "algorithmic_frac": 2.0 * r * r * I_leaf / (m2l_ms / 1e3) / 1e12 / bf16,
                 "fp64_lead_flop": 2.0 * 32 * 16 * I_leaf,
-                "algorithmic_tflops": tc_flop / (m2l_ms / 1e3) / 1e12,
-                "traffic": TC_DRAM_BYTES_PER_CELL * 8 ** lev,
-                "traffic_note": "ncu dram bytes of the level-5 launch scaled by cells",
+                "traffic": TC_DRAM_BYTES_PER_CELL * 8 ** lev if TC_DRAM_BYTES_PER_CELL else None,
+                "traffic_note": "ncu DRAM bytes of the level-6 launch (split rows written) scaled by cells",
                 "flop_per_launch": exec_flop, "launch_ms": m2l_ms}
     else:
         flop = 2.0 * r * r * I_leaf
         achieved = flop / (m2l_ms / 1e3) / 1e12
-        peak = 40.0 if args.mode == "d" else 80.0
-        roof = {"kernel": "m2l_simt (leaf level)", "bound": "fp64" if args.mode == "d" else "fp32",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": "nominal B200 FP64/FP32 vector rate (no measured figure)", "traffic": None,
-                "flop_per_launch": flop, "launch_ms": m2l_ms}
+        fp64 = args.mode == "d" and r == 256
+        peak = DMMA_TFLOPS if fp64 else FP32_TFLOPS
+        roof = {"kernel": "m2l_dmma_kernel (leaf level)" if fp64 else "m2l_simt_kernel (leaf level)",
+                "bound": "tensor" if fp64 else "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "peak_source": "FP64 tensor (DMMA) rate, 128 flops/clock/SM at 1965 MHz" if fp64 else
+                               "FP32 FMA rate, 128 lanes/SM at 1965 MHz",
+                "traffic": None, "flop_per_launch": flop, "launch_ms": m2l_ms}
+    # near field and passes: pairs exact from the tree, bytes of the passes
+    counts = leaf_counts(x, lev)
+    pairs = near_pairs(counts)
+    p2p = {"pairs": pairs, "ms": stages["p2p"], "gpairs_per_s": pairs / (stages["p2p"] / 1e3) / 1e9,
+           "roof_gpairs_per_s": P2P_ROOF_PAIRS / 1e9, "frac": pairs / (stages["p2p"] / 1e3) / P2P_ROOF_PAIRS,
+           "roof_note": "min(FP32 issue / 7 ops per pair, MUFU rsqrt 16/clk/SM) at 1965 MHz; the mixed kernel also "
+                        "does 6 FP64 operations per pair (separation and its square)"}
+    pb = pass_bytes(n, lev, N, int((counts > 0).sum()), args.mode == "mixed")
+    passes = {k: {"bytes": b, "ms": stages[k], "gb_per_s": b / (stages[k] / 1e3) / 1e9,
+                  "frac_hbm": b / (stages[k] / 1e3) / 1e9 / hbm} for k, b in pb.items()}
 
     # plain FP64 GPU form of the same FMM (the speed-up denominator)
     plain = None
@@ -882,6 +1060,9 @@ def main():
             "plain_fp64": plain,
             "tolerance_rank": tolr,
             "stages_ms": stages,
+            "m2l_flops": m2l_counts,
+            "p2p": p2p,
+            "passes_hbm": passes,
             "setup_ms": {"host_tree": t_setup_host * 1e3, "device_tree": t_setup_dev * 1e3,
                          "note": "octree + upload of the particles, outside the metric (bitwise the same tree)"},
             "e2e": {"value": world / t_e2e, "unit": "solve/s", "h2d_bytes_per_step": N * esz,
@@ -889,7 +1070,7 @@ def main():
             "gpu_launches": launches * args.steps,
             "roofline": roof,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clk_now,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -151,9 +151,10 @@ BBFMM_B200_API int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *s, int level, v
  * its full FP64 output), r values per cell in the reference's Morton cell order. */
 BBFMM_B200_API int bbfmm_b200_copy_m2l(bbfmm_b200_solver *s, int level, void *host_out);
 
-/* Re-run the M2L of one level `reps` times (inputs of the last solve) between CUDA events
- * on the solver's stream: ms[0] = mean time of the main M2L kernel per launch, ms[1] =
- * mean time of the FP64 leading-component kernel (MIXED only, else 0). */
+/* Re-run the M2L of one level `reps` times (inputs of the last solve), each launch as the
+ * solve makes it, between CUDA events on the solver's stream: ms[0] = mean time of the main
+ * M2L kernel per launch, ms[1] = mean time of a separate FP64 leading-component kernel
+ * (MIXED where the tensor-core kernel does not compute that block itself, else 0). */
 BBFMM_B200_API int bbfmm_b200_time_m2l(bbfmm_b200_solver *s, int level, int reps, float *ms);
 
 /* FP64 direct sum on the device (DirectCalc3D, bbfmm.c:471-504): out[t] =
@@ -248,10 +249,11 @@ BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
 /* Kernel of the solver (the reference's compile-time kernels, bbfmm.c:109-144, 798-849):
  * BBFMM_B200_KERNEL_LAPLACIAN (1/r, the default), BBFMM_B200_KERNEL_LAPLACIAN_FORCE (x / r^3,
  * x the first component of source - target, homogeneity 2) or BBFMM_B200_KERNEL_ONEOVERR4
- * (1/r^4, homogeneity 4). The last two run in modes D and S (BBFMM_B200_ERR_UNSUPPORTED in
- * MIXED mode), and the operators given at create must be that kernel's, e.g. the reference's
- * laplacianforce{K,U}{n}.bin or oneoverr4{K,U}{n}.bin. It sets the near-field pair value and
- * the per-level scale (1/L_l)^homogeneity after the M2L. Field solves are for 1/r. */
+ * (1/r^4, homogeneity 4), in every mode; the operators given at create must be that kernel's,
+ * e.g. the reference's laplacianforce{K,U}{n}.bin or oneoverr4{K,U}{n}.bin. It sets the
+ * near-field pair value (MIXED: the separation in FP64, dx r^-3 or r^-4 in FP32 with the
+ * compensated sum) and the per-level scale (1/L_l)^homogeneity after the M2L. Field solves
+ * are for 1/r. */
 #define BBFMM_B200_KERNEL_LAPLACIAN 0
 #define BBFMM_B200_KERNEL_LAPLACIAN_FORCE 1
 #define BBFMM_B200_KERNEL_ONEOVERR4 2

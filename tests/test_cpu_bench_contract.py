@@ -35,3 +35,28 @@ def test_reference_arm_other_ranks_exit_silently():
     p = _run({"RANK": "1", "WORLD_SIZE": "2"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert not [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_near_pair_count_and_interaction_count_are_exact():
+    """The bench's exact counts: near-field pairs from the library's leaf sort equal a brute
+    force over the leaves and their neighbours; the M2L pairs of a full level equal the
+    interaction lists of the oracle's tree."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    from oracle.oracle import Oracle, levsta
+    rng = np.random.default_rng(3)
+    x = rng.random((3000, 3)) - 0.5
+    lev = 3
+    g = bench.leaf_counts(x, lev)
+    assert g.sum() == 3000
+    m = 2 ** lev
+    want = 0
+    for i in np.ndindex(m, m, m):
+        lo = [max(0, a - 1) for a in i]
+        hi = [min(m, a + 2) for a in i]
+        want += g[i] * g[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]].sum()
+    assert bench.near_pairs(g) == want
+    tree = Oracle("d").build_tree(x, 4)
+    for l in (2, 3, 4):
+        assert bench.interactions_per_level(l) == int(tree.iinter[levsta(l):levsta(l + 1)].sum()), l

@@ -9,7 +9,7 @@ two-box tiles per sibling class.
   (bbfmm_b200_copy_m2l) on 384 cells -- the domain's corners, cells on the faces of the
   8 x 8 x 4 tile boxes of every sibling class, random cells -- against the oracle's M2L of the
   same cells from the solver's own multipoles of that level (interaction lists enumerated from
-  the grid, Oracle.m2l_sample). FP64: 1e-12; mixed: 1e-5 relative L2 over the sampled rows
+  the grid, Oracle.m2l_sample). FP64: 1e-12; mixed: 1e-6 relative L2 over the sampled rows
   (split-BF16 products with FP32 accumulation outside the FP64 leading block).
 * Mixed, n = 8, depth 6 (N = 524,288): the whole solve against the FP64 solve < 3e-7, its
   error against the FP64 direct sum on 2,048 targets within 1.2x of the FP64 solve's, and the
@@ -71,7 +71,7 @@ def _sample_cells(lev, seed):
     return grid_to_morton(g[:, 0], g[:, 1], g[:, 2], lev)
 
 
-@pytest.mark.parametrize("mode,tol", [("d", 1e-12), ("mixed", 1e-5)])
+@pytest.mark.parametrize("mode,tol", [("d", 1e-12), ("mixed", 1e-6)])
 @pytest.mark.parametrize("lev,N", [(6, 524_288), (7, 2_097_152)])
 def test_m2l_level_matches_oracle_on_sampled_cells(oracle_d, mode, tol, lev, N):
     import torch
