@@ -51,6 +51,8 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_stage_times.argtypes = [vp, C.POINTER(C.c_float), i]
         L.bbfmm_b200_copy_multipoles.argtypes = [vp, i, vp]
         L.bbfmm_b200_copy_m2l.argtypes = [vp, i, vp]
+        L.bbfmm_b200_set_target_region.argtypes = [vp, i, vp]
+        L.bbfmm_b200_set_first_m2l_level.argtypes = [vp, i]
         L.bbfmm_b200_time_m2l.argtypes = [vp, i, i, C.POINTER(C.c_float)]
         L.bbfmm_b200_direct.argtypes = [i, vp, vp, i, vp, vp, vp]
         L.bbfmm_b200_direct_field.argtypes = [i, vp, vp, i, vp, vp, vp, vp]

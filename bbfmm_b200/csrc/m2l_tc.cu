@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(192, 1)
                    const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                    double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
                    int split_chunks, int ncols, const double *__restrict__ Mlead, const double *__restrict__ Erow,
-                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows) {
+                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows, const int *__restrict__ tile_list) {
   constexpr int STAGE_BYTES = STAGE2_BYTES;
   constexpr int DNZ = 16;  // components the fused down projection takes in FP64
   constexpr int split_rows = TC_SPLIT_ROWS;
@@ -357,7 +357,8 @@ __global__ void __launch_bounds__(192, 1)
   const int tiles_per_class = nbx * nby * nbz;
   // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
   // of neighbouring boxes, which read one source region that stays in L2
-  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;  // a list: only those tiles
+  const int set_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
   const int c = set_ * 8 + loc_ % 8;
   const int tb = loc_ / 8;
   const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX2_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
@@ -1151,7 +1152,7 @@ bool tc_fuses_lead(const void *opsv, int nprod, int rank) {
 
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets, int nprod, int rank, const double *Mlead,
-                  const double *Erow, void *Lsplit) {
+                  const double *Erow, void *Lsplit, const int *tile_list, int ntiles) {
   const TcOps *ops = (const TcOps *)opsv;
   if (nprod != 0 && nprod != 1 && nprod != 3)
     return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 0 (adaptive), 1 or 3");
@@ -1209,9 +1210,11 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     const int tiles2 = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX2_Y) * (P / tc::BOX_Z);
     const bool fuse = Mlead && Erow && tc_fuses_lead(ops, nprod, rank) && kfirst == 0 && ilead == 32;
     if (Lsplit && !fuse) return bbfmm_set_error(BBFMM_ERR_ARG, "split M2L output needs the fused leading block");
-    tc::m2l_tc2_kernel<<<tiles2, 192, tc::SMEM2_BYTES, s>>>(
+    if (tile_list && (ntiles < 0 || ntiles > tiles2)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
+    if (tile_list && ntiles == 0) return BBFMM_OK;
+    tc::m2l_tc2_kernel<<<tile_list ? ntiles : tiles2, 192, tc::SMEM2_BYTES, s>>>(
         mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst, ilead, split_chunks, rank, fuse ? Mlead : nullptr,
-        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P);
+        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P, tile_list);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
   }
   static bool attr = false;
@@ -1220,6 +1223,7 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc smem attribute", __FILE__, __LINE__);
     attr = true;
   }
+  if (tile_list) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tile lists are for the two-box tensor-core M2L");
   const int tiles = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
   tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst,
                                                        ilead, split_chunks, split_rows, rank);

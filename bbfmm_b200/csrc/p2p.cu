@@ -82,15 +82,22 @@ __device__ __forceinline__ typename NearTypes<MODE>::S stage_src(const typename 
 }
 
 // Per-target accumulator. v: sum of q_j K (FIELD: q_j / r), c: Neumaier compensation of v
-// (mixed), g*: sum of q_j (x_j - x_i) / r^3 (FIELD). H: homogeneity of the kernel.
+// (mixed), g*: sum of q_j (x_j - x_i) / r^3 (FIELD; FP64 in the mixed mode, where the FP32
+// factor q_j / r^3 times the FP64 separation costs one conversion per pair instead of three).
+// H: homogeneity of the kernel.
 template <int MODE, int H, bool FIELD>
 struct NearAcc {
   using T = NearTypes<MODE>;
   using C = typename T::C;
   using A = typename T::A;
+  using G = std::conditional_t<MODE == MODE_MIXED, double, A>;
   using Src = typename T::S;
-  A v, c, gx, gy, gz;
-  __device__ __forceinline__ void zero() { v = c = gx = gy = gz = (A)0; }
+  A v, c;
+  G gx, gy, gz;
+  __device__ __forceinline__ void zero() {
+    v = c = (A)0;
+    gx = gy = gz = (G)0;
+  }
   // The pair's contribution to v (0 for coincident points); FIELD: the gradient terms are
   // added here.
   __device__ __forceinline__ A term(C fx, C fy, C fz, const Src &g) {
@@ -107,10 +114,10 @@ struct NearAcc {
       else if constexpr (H == 2) t = __fmul_rn(g.q, (float)ex * (rinv * rinv * rinv));
       else t = __fmul_rn(g.q, rinv);
       if constexpr (FIELD) {
-        const float t3 = t * rinv * rinv;
-        gx += t3 * (float)ex;
-        gy += t3 * (float)ey;
-        gz += t3 * (float)ez;
+        const double t3 = (double)(t * rinv * rinv);
+        gx = fma(t3, ex, gx);
+        gy = fma(t3, ey, gy);
+        gz = fma(t3, ez, gz);
       }
       return t;
     } else {
@@ -187,12 +194,24 @@ static int *near_work_flag(void *scratch) { return (int *)((char *)scratch + 8);
 // Items of block b (leaves [64 b, 64 b + 64)): 0 when empty, 1 (sparse) when it holds at
 // most 2 x threads particles, else one per `threads` particles of each of its leaves. With
 // `items`, writes them at items[base ...], skipping indices >= cap.
-__device__ int64_t block_items(const int *__restrict__ ls, int64_t b, int N, int threads, int2 *items = nullptr,
+// mask (optional): target mask over the cells of a level R <= maxlev (stacked numbering); a
+// leaf m is active when mask[m >> mask_shift] is set, mask_shift = 3 (maxlev - R). Only active
+// leaves' targets are computed: dense chunks of inactive leaves are not emitted, sparse blocks
+// only when one of their leaves is active (the kernel skips the inactive ones' targets).
+__device__ __forceinline__ bool leaf_active(const unsigned char *mask, int shift, int64_t m) {
+  return !mask || mask[m >> shift];
+}
+
+__device__ int64_t block_items(const int *__restrict__ ls, int64_t b, int N, int threads,
+                               const unsigned char *__restrict__ mask, int mask_shift, int2 *items = nullptr,
                                int64_t base = 0, int64_t cap = 0) {
   const int64_t m0 = b * 64;
   const int first = clamp_n(ls[m0], N), last = max(first, clamp_n(ls[m0 + 64], N));
   if (last == first) return 0;
   if (last - first <= 2 * threads) {
+    bool any = !mask;
+    for (int k = 0; k < 64 && !any; ++k) any = leaf_active(mask, mask_shift, m0 + k);
+    if (!any) return 0;
     if (items && base < cap) items[base] = make_int2((int)b, 0);
     return 1;
   }
@@ -200,7 +219,7 @@ __device__ int64_t block_items(const int *__restrict__ ls, int64_t b, int N, int
   int prev = first;
   for (int k = 1; k <= 64; ++k) {
     const int v = max(prev, min(clamp_n(ls[m0 + k], N), last));
-    const int ch = (v - prev + threads - 1) / threads;
+    const int ch = leaf_active(mask, mask_shift, m0 + k - 1) ? (v - prev + threads - 1) / threads : 0;
     if (items)
       for (int j = 0; j < ch && base + n + j < cap; ++j) items[base + n + j] = make_int2(-(int)(m0 + k - 1) - 1, j);
     n += ch;
@@ -242,10 +261,11 @@ __device__ int64_t cta_exclusive_scan(int64_t x, int64_t *s_warp, int64_t *total
 // Pass 1: items per tile of P2P_SCAN_THREADS blocks, and the leaf-range checks (offsets in
 // [0, N], non-decreasing, leaf_start[0] = 0, leaf_start[nleaf] = N), swept coalesced.
 __global__ void __launch_bounds__(P2P_SCAN_THREADS) near_count_kernel(int64_t nblocks, const int *__restrict__ ls,
-                                                                      int N, int threads, int64_t *tiles, int *flag) {
+                                                                      int N, int threads, int64_t *tiles, int *flag,
+                                                                      const unsigned char *mask, int mask_shift) {
   __shared__ int64_t s_warp[33];
   const int64_t b = (int64_t)blockIdx.x * P2P_SCAN_THREADS + threadIdx.x;
-  const int64_t x = b < nblocks ? block_items(ls, b, N, threads) : 0;
+  const int64_t x = b < nblocks ? block_items(ls, b, N, threads, mask, mask_shift) : 0;
   int64_t total = 0;
   cta_exclusive_scan(x, s_warp, &total);
   if (threadIdx.x == 0) tiles[blockIdx.x] = total;
@@ -280,20 +300,23 @@ __global__ void __launch_bounds__(1024) near_scan_tiles_kernel(int64_t ntiles, i
 // Pass 3: every block writes its items at its offset (indices below cap only).
 __global__ void __launch_bounds__(P2P_SCAN_THREADS) near_emit_kernel(int64_t nblocks, const int *__restrict__ ls,
                                                                      int N, int threads, const int64_t *tiles,
-                                                                     int2 *items, int64_t cap) {
+                                                                     int2 *items, int64_t cap,
+                                                                     const unsigned char *mask, int mask_shift) {
   __shared__ int64_t s_warp[33];
   const int64_t b = (int64_t)blockIdx.x * P2P_SCAN_THREADS + threadIdx.x;
-  const int64_t x = b < nblocks ? block_items(ls, b, N, threads) : 0;
+  const int64_t x = b < nblocks ? block_items(ls, b, N, threads, mask, mask_shift) : 0;
   int64_t total = 0;
   const int64_t ex = cta_exclusive_scan(x, s_warp, &total);
-  if (x > 0) block_items(ls, b, N, threads, items, tiles[blockIdx.x] + ex, cap);
+  if (x > 0) block_items(ls, b, N, threads, mask, mask_shift, items, tiles[blockIdx.x] + ex, cap);
 }
 
 // Builds the work list for `threads` threads per CTA into `scratch` (near_work_bytes). With
 // nitems_host, synchronises `s` and returns the item count (at most N; a larger count sets
 // *flag_host) and the leaf-range flag.
 int near_work_build(int N, const int *leaf_start, int maxlev, int nsets, int threads, void *scratch, cudaStream_t s,
-                    int *nitems_host, int *flag_host) {
+                    int *nitems_host, int *flag_host, const unsigned char *mask, int mask_level) {
+  const int mask_shift = mask ? 3 * (maxlev - mask_level) : 0;
+  if (mask && (mask_level < 0 || mask_level > maxlev)) return bbfmm_set_error(BBFMM_ERR_ARG, "mask level out of range");
   if (maxlev < BBFMM_MINLEV) return bbfmm_set_error(BBFMM_ERR_ARG, "near field: maxlev >= 2");
   if (threads != 64 && threads != 128 && threads != 256)
     return bbfmm_set_error(BBFMM_ERR_ARG, "near field: 64, 128 or 256 threads per block");
@@ -303,10 +326,10 @@ int near_work_build(int N, const int *leaf_start, int maxlev, int nsets, int thr
   const int64_t nblocks = near_blocks(maxlev, nsets), ntiles = near_tiles(maxlev, nsets);
   BBFMM_CUDA_OK(cudaMemsetAsync(scratch, 0, 16, s));
   near_count_kernel<<<(unsigned)ntiles, P2P_SCAN_THREADS, 0, s>>>(nblocks, leaf_start, N, threads, tiles,
-                                                                  near_work_flag(scratch));
+                                                                  near_work_flag(scratch), mask, mask_shift);
   near_scan_tiles_kernel<<<1, 1024, 0, s>>>(ntiles, tiles, count);
   near_emit_kernel<<<(unsigned)ntiles, P2P_SCAN_THREADS, 0, s>>>(nblocks, leaf_start, N, threads, tiles, items,
-                                                                 (int64_t)N);
+                                                                 (int64_t)N, mask, mask_shift);
   BBFMM_CUDA_OK(cudaGetLastError());
   if (nitems_host || flag_host) {
     int64_t h[2] = {0, 0};
@@ -326,7 +349,8 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
                                                    const int *__restrict__ leaf_start, int maxlev,
                                                    const int2 *__restrict__ items, int nitems,
                                                    typename NearTypes<MODE>::R *__restrict__ pot,
-                                                   typename NearTypes<MODE>::R *__restrict__ fld, int *flag) {
+                                                   typename NearTypes<MODE>::R *__restrict__ fld, int *flag,
+                                                   const unsigned char *__restrict__ mask, int mask_shift) {
   using NT = NearTypes<MODE>;
   using P4 = typename NT::P4;
   using C = typename NT::C;
@@ -336,7 +360,7 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
   static_assert(sizeof(Acc) * 256 <= sizeof(Src) * P2P_TILE, "group partials fit the tile buffer");
   __shared__ __align__(16) unsigned char s_buf[sizeof(Src) * P2P_TILE];
   __shared__ int s_start[P2P_REGION], s_off[P2P_REGION + 1];
-  __shared__ unsigned char s_tleaf[512];
+  __shared__ unsigned char s_tleaf[512], s_act[P2P_REGION];
   Src *s_src = reinterpret_cast<Src *>(s_buf);
   const int nt = blockDim.x, tid = threadIdx.x;
   const int ncpd = 1 << maxlev;
@@ -377,13 +401,16 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
       const int rx = rho / (RR * RR), ry = (rho / RR) % RR, rz = rho % RR;
       const int gx = ox + rx, gy = oy + ry, gz = oz + rz;
       int s0 = 0, cnt = 0;
+      bool act = false;
       if (gx >= 0 && gx < ncpd && gy >= 0 && gy < ncpd && gz >= 0 && gz < ncpd) {
         const int64_t B = setbase + grid_to_morton(gx, gy, gz, maxlev);
         s0 = clamp_n(leaf_start[B], N);
         cnt = max(0, clamp_n(leaf_start[B + 1], N) - s0);
+        act = leaf_active(mask, mask_shift, B);
       }
       s_start[rho] = s0;
       s_off[rho] = cnt;
+      s_act[rho] = act;
     }
     __syncthreads();
     // exclusive scan of the counts (one warp; <= 7 entries per lane)
@@ -415,7 +442,7 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
     if (!dense) {
       for (int rho = tid; rho < nreg; rho += nt) {
         const int rx = rho / 36, ry = (rho / 6) % 6, rz = rho % 6;
-        if (rx < 1 || rx > 4 || ry < 1 || ry > 4 || rz < 1 || rz > 4) continue;
+        if (rx < 1 || rx > 4 || ry < 1 || ry > 4 || rz < 1 || rz > 4 || !s_act[rho]) continue;
         const int a = max(s_start[rho], t0), e = min(s_start[rho] + s_off[rho + 1] - s_off[rho], t1);
         for (int p = a; p < e; ++p) s_tleaf[p - t0] = (unsigned char)rho;
       }
@@ -537,14 +564,18 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
 
 template <int MODE, int H, bool FIELD>
 static void near_launch(int N, const void *pos4, const int *leaf_start, int maxlev, const int2 *items, int nitems,
-                        int threads, void *pot, void *fld, int *flag, cudaStream_t s) {
+                        int threads, void *pot, void *fld, int *flag, const unsigned char *mask, int mask_shift,
+                        cudaStream_t s) {
   using NT = NearTypes<MODE>;
   near_kernel<MODE, H, FIELD><<<nitems, threads, 0, s>>>(N, (const typename NT::P4 *)pos4, leaf_start, maxlev, items,
-                                                         nitems, (typename NT::R *)pot, (typename NT::R *)fld, flag);
+                                                         nitems, (typename NT::R *)pot, (typename NT::R *)fld, flag,
+                                                         mask, mask_shift);
 }
 
 int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_start, int maxlev,
-                const void *work, int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s) {
+                const void *work, int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s,
+                const unsigned char *mask, int mask_level) {
+  const int mask_shift = mask ? 3 * (maxlev - mask_level) : 0;
   if (N <= 0 || nitems <= 0) return BBFMM_OK;
   if (threads != 64 && threads != 128 && threads != 256)
     return bbfmm_set_error(BBFMM_ERR_ARG, "near field: 64, 128 or 256 threads per block");
@@ -554,10 +585,10 @@ int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_
   const int2 *items = near_work_items(work, maxlev, nsets);
   int *flag = near_work_flag(const_cast<void *>(work));
 #define NEAR_CASE(M)                                                                                     \
-  if (fld) near_launch<M, 1, true>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, fld, flag, s); \
-  else if (homogen == 1) near_launch<M, 1, false>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, nullptr, flag, s); \
-  else if (homogen == 2) near_launch<M, 2, false>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, nullptr, flag, s); \
-  else near_launch<M, 4, false>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, nullptr, flag, s);
+  if (fld) near_launch<M, 1, true>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, fld, flag, mask, mask_shift, s); \
+  else if (homogen == 1) near_launch<M, 1, false>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, nullptr, flag, mask, mask_shift, s); \
+  else if (homogen == 2) near_launch<M, 2, false>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, nullptr, flag, mask, mask_shift, s); \
+  else near_launch<M, 4, false>(N, pos4, leaf_start, maxlev, items, nitems, threads, pot, nullptr, flag, mask, mask_shift, s);
   if (mode == MODE_D) { NEAR_CASE(MODE_D) }
   else if (mode == MODE_S) { NEAR_CASE(MODE_S) }
   else if (mode == MODE_MIXED) { NEAR_CASE(MODE_MIXED) }

@@ -474,7 +474,7 @@ int Solver<T>::leaf_down(bool field) {
     if (slabbed()) {
       TRY(proj_down(maxlev, c, a, Fl));
       mark(ST_PROJ_DOWN);
-      if (maxlev > BBFMM_MINLEV) {
+      if (maxlev > m2l_first) {
         TRY(launch_l2l<T>(n, F[(maxlev - 1) & 1], Fl, maxlev - 1, tb, stream, nsets, a / 8, c / 8));
         mark(ST_L2L);
       }
@@ -491,7 +491,7 @@ int Solver<T>::interaction(int lo, int hi) {
   const Tables tb = tables();
   for (int l = lo; l <= hi; ++l) {
     TRY(m2l_post(l));
-    if (l > BBFMM_MINLEV && !(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
+    if (l > m2l_first && !(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
       TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream, nsets));
       mark(ST_L2L);
     }
@@ -511,11 +511,15 @@ int Solver<T>::m2l_post(int l) {
       // split-bf16 tensor-core kernel adds everything else into the same FP64 output; the
       // two-box kernel computes the block itself in its otherwise idle epilogue warps
       if (lead > 0 && tc_fuses_lead(tcops, tc_products, rk())) {
+        // a target region: only the tiles above active cells run, the rest of the output is zero
+        const bool masked = region_tiles[l] != nullptr;
         // whole level with mixed projections: the kernel also writes the split rows that the
         // down projection reads (and the FP64 output only where that pass reads it)
-        presplit = proj_tc() && cells(l) <= Lsplit_rows && !(l == maxlev && slabbed());
+        presplit = !masked && proj_tc() && cells(l) <= Lsplit_rows && !(l == maxlev && slabbed());
+        if (masked) BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * (size_t)cells(l) * r, stream));
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
-                          tc_products, rk(), (const double *)Ml, (const double *)Ert, presplit ? Lsplit : nullptr));
+                          tc_products, rk(), (const double *)Ml, (const double *)Ert, presplit ? Lsplit : nullptr,
+                          region_tiles[l], region_ntiles[l]));
         mark(ST_M2L, 1);
       } else if (lead > 0) {
         TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
@@ -565,7 +569,7 @@ int Solver<T>::solve(const void *q_dev, void *phi_dev, int io_double) {
     mark(-1, 0);
   }
   TRY(upward(q_dev, io_double));
-  TRY(interaction(BBFMM_MINLEV, maxlev));
+  TRY(interaction(m2l_first, maxlev));
   TRY(downward_finish(phi_dev, io_double, true));
   return BBFMM_OK;
 }
@@ -615,8 +619,60 @@ int Solver<T>::near(T *pot, T *fld) {
   // ~1e-7 relative rounding of FP32 pair terms; its M2L and projections stay split-BF16.
   const int near_mode = mode == MODE_MIXED && homogen == 4 ? (int)MODE_D : mode;
   TRY(launch_near(near_mode, homogen, N, pos4, leaf_start, maxlev, near_work, nsets, near_items, near_threads, pot,
-                  fld, stream));
+                  fld, stream, region_mask, region_level));
   mark(ST_P2P);
+  return BBFMM_OK;
+}
+
+// Target region: active cells of `level` (8^level bytes, Morton order, host); level < 0 clears.
+template <typename T>
+int Solver<T>::set_target_region(int level, const unsigned char *active_host) {
+  for (int l = 0; l <= 10; ++l) {
+    if (region_tiles[l]) cudaFree(region_tiles[l]);
+    region_tiles[l] = nullptr;
+    region_ntiles[l] = 0;
+  }
+  if (region_mask) cudaFree(region_mask);
+  region_mask = nullptr;
+  region_host.clear();
+  region_level = -1;
+  if (level >= 0) {
+    if (nsets != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "target regions are for single-set solvers");
+    if (level < BBFMM_MINLEV || level > maxlev || !active_host)
+      return bbfmm_set_error(BBFMM_ERR_ARG, "target region: level in [2, maxlev] and a mask of 8^level bytes");
+    region_host.assign(active_host, active_host + pow8i(level));
+    TRY(dalloc(&region_mask, (size_t)pow8i(level)));
+    BBFMM_CUDA_OK(cudaMemcpy(region_mask, region_host.data(), region_host.size(), cudaMemcpyHostToDevice));
+    region_level = level;
+    TRY(build_region_tiles());
+  }
+  return pos4 ? build_near_work() : BBFMM_OK;
+}
+
+// Active two-box tiles of every tensor-core level above the region level: a tile (8 x 8 x 4
+// parent cells of one sibling class) is active when one of its cells descends from an active
+// region cell. Ids as the tensor-core M2L numbers its full grid: (box, then class fastest).
+template <typename T>
+int Solver<T>::build_region_tiles() {
+  for (int l = region_level + 1; l <= maxlev; ++l) {
+    if (l < TC_MIN_LEVEL) continue;
+    const int P = 1 << (l - 1), nbx = P / 8, nby = P / 8, nbz = P / 4, sh = l - 1 - region_level;
+    std::vector<int> ids;
+    for (int tb = 0; tb < nbx * nby * nbz; ++tb) {
+      const int bx0 = (tb % nbx) * 8, by0 = ((tb / nbx) % nby) * 8, bz0 = (tb / (nbx * nby)) * 4;
+      bool act = false;
+      for (int az = bz0 >> sh; az <= (bz0 + 3) >> sh && !act; ++az)
+        for (int ay = by0 >> sh; ay <= (by0 + 7) >> sh && !act; ++ay)
+          for (int ax = bx0 >> sh; ax <= (bx0 + 7) >> sh && !act; ++ax)
+            act = region_host[(size_t)grid_to_morton(ax, ay, az, region_level)] != 0;
+      if (act)
+        for (int c = 0; c < 8; ++c) ids.push_back(tb * 8 + c);
+    }
+    region_ntiles[l] = (int)ids.size();
+    TRY(dalloc(&region_tiles[l], ids.size() > 0 ? ids.size() : 1));
+    if (!ids.empty())
+      BBFMM_CUDA_OK(cudaMemcpy(region_tiles[l], ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+  }
   return BBFMM_OK;
 }
 
@@ -626,7 +682,8 @@ template <typename T>
 int Solver<T>::build_near_work() {
   if (!near_work) TRY(dalloc((unsigned char **)&near_work, near_work_bytes(N, maxlev, nsets)));
   int flag = 0;
-  TRY(near_work_build(N, leaf_start, maxlev, nsets, tune.p2p_threads, near_work, stream, &near_items, &flag));
+  TRY(near_work_build(N, leaf_start, maxlev, nsets, tune.p2p_threads, near_work, stream, &near_items, &flag,
+                      region_mask, region_level));
   if (flag) return bbfmm_set_error(BBFMM_ERR_ARG, "leaf offsets must rise from 0 to N without decreasing");
   near_threads = tune.p2p_threads;
   return BBFMM_OK;
@@ -642,7 +699,7 @@ int Solver<T>::solve_fields(const void *q_dev, void *pot_dev, void *fld_dev) {
   if (!flds) TRY(dalloc(&flds, 3 * (size_t)(N > 0 ? N : 1)));
   kernel_launches = 0;
   TRY(upward(q_dev, sizeof(T) == 8));
-  TRY(interaction(BBFMM_MINLEV, maxlev));
+  TRY(interaction(m2l_first, maxlev));
   const Tables tb = tables();
   TRY(leaf_down(true));
   TRY(near(phis, flds));
@@ -809,6 +866,9 @@ int Solver<T>::copy_m2l_morton(int level, T *host_out) {
 
 template <typename T>
 void Solver<T>::release() {
+  for (int l = 0; l <= 10; ++l)
+    if (region_tiles[l]) cudaFree(region_tiles[l]);
+  if (region_mask) cudaFree(region_mask);
   void *ptrs[] = {offs, perm, leaf_start, near_work, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
                   phis, flds, Ssplit, Lsplit, io_q, io_phi};
   for (void *p : ptrs)
@@ -968,6 +1028,20 @@ int bbfmm_b200_copy_multipoles(bbfmm_b200_solver *h, int level, void *host_out) 
   if (!h || !host_out) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   if (h->f) return h->f->copy_multipoles_morton(level, (float *)host_out);
   return h->d->copy_multipoles_morton(level, (double *)host_out);
+}
+
+int bbfmm_b200_set_target_region(bbfmm_b200_solver *h, int level, const unsigned char *active) {
+  if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
+  return h->f ? h->f->set_target_region(level, active) : h->d->set_target_region(level, active);
+}
+
+int bbfmm_b200_set_first_m2l_level(bbfmm_b200_solver *h, int level) {
+  if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
+  const int maxlev = h->f ? h->f->maxlev : h->d->maxlev;
+  if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "first M2L level in [2, maxlev]");
+  if (h->f) h->f->m2l_first = level;
+  else h->d->m2l_first = level;
+  return BBFMM_OK;
 }
 
 int bbfmm_b200_copy_m2l(bbfmm_b200_solver *h, int level, void *host_out) {

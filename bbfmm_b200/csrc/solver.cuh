@@ -43,10 +43,13 @@ template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *d
 // on pot then). nitems_host / flag_host: synchronise and return the item count and whether
 // the offsets were malformed.
 size_t near_work_bytes(int N, int maxlev, int nsets);
+// mask (optional, device): the near field computes only the targets of leaves whose ancestor at
+// mask_level (<= maxlev) has its mask byte set (stacked cell numbering); the others are not written.
 int near_work_build(int N, const int *leaf_start, int maxlev, int nsets, int threads, void *scratch, cudaStream_t s,
-                    int *nitems_host, int *flag_host);
+                    int *nitems_host, int *flag_host, const unsigned char *mask = nullptr, int mask_level = 0);
 int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_start, int maxlev, const void *work,
-                int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s);
+                int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s,
+                const unsigned char *mask = nullptr, int mask_level = 0);
 int near_status(int clear);
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
@@ -85,9 +88,12 @@ size_t tc_split_bytes(int r, int64_t ncell);
 // 32 x 64.
 constexpr int TC_SPLIT_CHUNKS = 2, TC_SPLIT_ROWS = 64;
 // rank: the effective rank (outputs i and components j below it; 0 = r).
+// tile_list (ntiles entries): run only these two-box tiles (ids as the full grid numbers them:
+// set, then box, then sibling class fastest); the outputs of the other cells are not written.
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0,
-                  const double *Mlead = nullptr, const double *Erow = nullptr, void *Lsplit = nullptr);
+                  const double *Mlead = nullptr, const double *Erow = nullptr, void *Lsplit = nullptr,
+                  const int *tile_list = nullptr, int ntiles = 0);
 bool tc_fuses_lead(const void *ops, int nprod, int rank);
 int tc_status(int clear);
 int tc_wait_probe(unsigned limit, int code);
@@ -155,6 +161,19 @@ struct Solver {
   int *perm = nullptr, *leaf_start = nullptr;
   void *near_work = nullptr;  // near-field work list (near_work_build) for near_threads
   int near_items = 0, near_threads = 0;
+  // Target region (bbfmm_b200_set_target_region, one set): results are wanted only at the
+  // particles inside the active cells of region_level. The near field skips the other targets,
+  // and the tensor-core M2L of every level above region_level runs only on the two-box tiles
+  // that hold descendants of active cells (the rest of that level's output is zero).
+  int region_level = -1;                       // < 0: every particle
+  unsigned char *region_mask = nullptr;        // device, 8^region_level bytes
+  std::vector<unsigned char> region_host;
+  int *region_tiles[11] = {};                  // per level: active two-box tile ids (device)
+  int region_ntiles[11] = {};
+  // First level whose M2L runs (bbfmm_b200_set_first_m2l_level): the local expansions start
+  // there (no L2L from the level above), so the solve gathers, for every target, only the
+  // sources inside the neighbourhood of its ancestor one level up.
+  int m2l_first = BBFMM_MINLEV;
   T *pos4 = nullptr;
   // expansions
   T *S[2] = {nullptr, nullptr};
@@ -195,6 +214,8 @@ struct Solver {
   int alloc_partials();                          // Lpart for the current tuning
   int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
   int build_near_work();                         // the work list for tune.p2p_threads
+  int set_target_region(int level, const unsigned char *active_host);  // level < 0 clears
+  int build_region_tiles();                      // region_tiles from region_host (after particles/alloc)
   bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
   int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false);  // S rows -> Mall (cpg)
   int proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit = false);    // Lbuf -> F rows (Morton, assign)

@@ -185,6 +185,22 @@ class Solver:
         3 (split BF16 for every term) or 1 (plain BF16) products per M2L term."""
         _lib.check(_lib.lib().bbfmm_b200_set_tc_products(self.h, int(nprod)))
 
+    def set_target_region(self, level: int, active=None):
+        """Results wanted only at the particles inside the active cells of `level` (a bool or
+        uint8 array of 8^level cells in Morton order; level < 0 clears): the near field skips
+        the other targets and the tensor-core M2L above `level` runs only above active cells."""
+        if level < 0:
+            _lib.check(_lib.lib().bbfmm_b200_set_target_region(self.h, -1, None))
+            return
+        a = np.ascontiguousarray(np.asarray(active).astype(np.uint8).reshape(-1))
+        _check_count("active", a.size, 8 ** level)
+        _lib.check(_lib.lib().bbfmm_b200_set_target_region(self.h, int(level), _ptr(a)))
+
+    def set_first_m2l_level(self, level: int):
+        """The local expansions start at `level`: the solve gathers, for every target, only the
+        sources in the 3 x 3 x 3 neighbourhood of its ancestor at level - 1."""
+        _lib.check(_lib.lib().bbfmm_b200_set_first_m2l_level(self.h, int(level)))
+
     def set_leaf_slab(self, cells: int):
         """Leaf cells per slab of the leaf level (multiple of 64; 0 = automatic)."""
         _lib.check(_lib.lib().bbfmm_b200_set_leaf_slab(self.h, int(cells)))
@@ -234,6 +250,117 @@ class Solver:
         out = np.empty(8 ** level * self.r, dtype=self.np_dtype)
         _lib.check(_lib.lib().bbfmm_b200_copy_m2l(self.h, level, _ptr(out)))
         return out.reshape(8 ** level, self.r)
+
+
+def morton_to_grid(m, level: int):
+    """Grid coordinates of Morton cell indices (the reference's bit order,
+    anotherFMMDistribute.c:239-253)."""
+    m = np.asarray(m, np.int64)
+    ix, iy, iz = (np.zeros_like(m) for _ in range(3))
+    for b in range(level):
+        t = (m >> (3 * b)) & 7
+        ix |= ((t >> 2) & 1) << b
+        iy |= ((t >> 1) & 1) << b
+        iz |= (t & 1) << b
+    return ix, iy, iz
+
+
+def leaf_of_particles(xyz, L: float, level: int):
+    """Morton leaf of every particle at `level` (the library's own leaf assignment), and the
+    particle count of every leaf."""
+    x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+    N = x.shape[0]
+    perm = np.zeros(N, np.int32)
+    ls = np.zeros(8 ** level + 1, np.int32)
+    _lib.check(_lib.lib().bbfmm_b200_sort_particles(N, 0, _ptr(x), float(L), level,
+                                                    perm.ctypes.data_as(C.POINTER(C.c_int)),
+                                                    ls.ctypes.data_as(C.POINTER(C.c_int))))
+    counts = np.diff(ls)
+    leaf = np.empty(N, np.int64)
+    leaf[perm] = np.repeat(np.arange(8 ** level, dtype=np.int64), counts)
+    return leaf, counts
+
+
+class AdaptiveSolver:
+    """Two-level adaptive refinement over uniform solvers (no counterpart in the reference,
+    whose octrees are uniform, anotherBuildFMMHierachy.c:44-55).
+
+    A coarse solver of depth `coarse_depth` takes every particle; its leaves holding more than
+    `cap` particles are heavy. For a target in a heavy leaf A, the near field -- the direct sum
+    over A's 3 x 3 x 3 neighbourhood N(A) -- is computed instead by a refined solver of depth
+    `fine_depth` over the particles of the heavy leaves' neighbourhoods, whose local expansions
+    start at level coarse_depth + 1: its interaction lists at the levels below and its leaf-level
+    near field together cover exactly N(A), so it returns that near field, FMM-approximated at
+    the finer depth. So
+
+        phi = coarse (far field of everyone, near field of the light leaves)
+            + refined (near field of the heavy leaves' particles)
+
+    The coarse solver's near field skips the heavy leaves and the refined solver's skips the
+    rest (target regions), and the refined tensor-core M2L runs only on the tiles above heavy
+    leaves, so its cost follows the heavy volume rather than the whole grid. Positions and
+    charges are in the caller's order throughout."""
+
+    def __init__(self, n: int, coarse_depth: int, fine_depth: int, L: float = 1.0, mode: str = "mixed",
+                 cap: int = 256, device: int = 0, **kw):
+        if fine_depth <= coarse_depth:
+            raise ValueError("fine_depth must exceed coarse_depth")
+        self.n, self.Dc, self.Df, self.L, self.mode, self.cap, self.device = (
+            n, coarse_depth, fine_depth, float(L), mode, int(cap), device)
+        self.kw = kw
+        self.coarse = Solver(n, coarse_depth, L, mode=mode, device=device, **kw)
+        self.fine = None
+
+    def close(self):
+        for s in (self.coarse, self.fine):
+            if s is not None:
+                s.close()
+
+    def set_particles(self, xyz):
+        torch = self.coarse.torch
+        x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+        self.N = x.shape[0]
+        self.coarse.set_particles(x)
+        leaf, counts = leaf_of_particles(x, self.L, self.Dc)
+        heavy = counts > self.cap
+        self.heavy_leaves = int(heavy.sum())
+        if self.fine is not None:
+            self.fine.close()
+            self.fine = None
+        if not heavy.any():
+            self.coarse.set_target_region(-1)
+            return
+        self.coarse.set_target_region(self.Dc, ~heavy)
+        # particles of the heavy leaves' 3 x 3 x 3 neighbourhoods
+        m = 2 ** self.Dc
+        gx, gy, gz = morton_to_grid(np.arange(8 ** self.Dc), self.Dc)
+        g = np.zeros((m + 2, m + 2, m + 2), bool)
+        g[gx + 1, gy + 1, gz + 1] = heavy
+        d = np.zeros_like(g)
+        for a in (-1, 0, 1):
+            for b in (-1, 0, 1):
+                for c in (-1, 0, 1):
+                    d |= np.roll(np.roll(np.roll(g, a, 0), b, 1), c, 2)
+        near_region = d[gx + 1, gy + 1, gz + 1]  # Morton order
+        sel = np.nonzero(near_region[leaf])[0]
+        keep = heavy[leaf[sel]]
+        self.fine = Solver(self.n, self.Df, self.L, mode=self.mode, device=self.device, **self.kw)
+        self.fine.set_particles(x[sel])
+        self.fine.set_first_m2l_level(self.Dc + 1)
+        self.fine.set_target_region(self.Dc, heavy)
+        dev = f"cuda:{self.device}"
+        self.sel = torch.as_tensor(sel, device=dev)
+        self.keep_local = torch.as_tensor(np.nonzero(keep)[0], device=dev)
+        self.keep_global = torch.as_tensor(sel[keep], device=dev)
+        self.fine_particles = int(sel.size)
+
+    def solve(self, q, out=None):
+        """q: CUDA tensor (N,) -> q_i * phi_i (CUDA tensor) on the caller's stream."""
+        phi = self.coarse.solve(q, out=out)
+        if self.fine is not None:
+            pf = self.fine.solve(q.index_select(0, self.sel))
+            phi.index_add_(0, self.keep_global, pf.index_select(0, self.keep_local))
+        return phi
 
 
 def batch_depth(N: int, per_leaf: float = 32.0) -> int:

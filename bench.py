@@ -543,6 +543,56 @@ def run_clustered_16m(args):
     return 0
 
 
+def run_clustered_16m_adaptive(args):
+    """The N = 16,777,216 clustered input (configuration 3) through the two-level adaptive
+    solver (coarse depth 6 for the uniform half, depth-8 refinement of the leaves holding more
+    than 256 particles) beside the uniform mixed solve of depth 8, both against the FP64 direct
+    sum on the same 8,192 targets."""
+    import torch
+    from bbfmm_b200 import AdaptiveSolver, Solver
+    from bbfmm_b200.fmm import direct
+    N = 16_777_216
+    x, q = clustered_16m_inputs()
+    targets = np.random.default_rng(4321).choice(N, 8192, replace=False).astype(np.int32)
+    ref = direct(torch.as_tensor(x, device="cuda"), torch.as_tensor(q, device="cuda"),
+                 torch.as_tensor(targets, device="cuda")).cpu().numpy()
+    qd = torch.as_tensor(q, device="cuda")
+    res = {}
+    for name in ("adaptive", "uniform"):
+        t0 = time.perf_counter()
+        if name == "adaptive":
+            s = AdaptiveSolver(8, 6, 8, mode="mixed", cap=256)
+        else:
+            s = Solver(8, 8, 1.0, mode="mixed")
+        s.set_particles(x)
+        t_setup = time.perf_counter() - t0
+        out = s.solve(qd)
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            t = _device_time(lambda: s.solve(qd, out=out), args.steps)
+        phi = out.double().cpu().numpy()[targets]
+        r = {"s_per_solve": t, "setup_s": t_setup, "clocks": clk.summary(),
+             "err_rel_l2": float(np.linalg.norm(phi - ref) / np.linalg.norm(ref))}
+        if name == "adaptive":
+            r.update({"heavy_leaves_depth6": s.heavy_leaves, "refined_particles": s.fine_particles})
+        res[name] = r
+        s.close()
+        del s, out
+        torch.cuda.empty_cache()
+    head = res["adaptive"]
+    line = {"metric": "FMM solves/s at N=16,777,216 clustered, n=8: two-level adaptive (depth 6 + 8) vs uniform depth 8",
+            "value": 1.0 / head["s_per_solve"], "unit": "solve/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": head["s_per_solve"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3+f64",
+            "data": "synthetic (seeded; 50% uniform, 50% in 16 Gaussians sigma 0.03; q ~ N(0,1))",
+            "config": {"workload": "bbFMM Laplace 1/r, N=16,777,216 clustered, n=8, adaptive depth 6 + 8", "N": N,
+                       "n": 8, "n_targets": 8192, "cap": 256},
+            "variants": res, "speedup_vs_uniform": res["uniform"]["s_per_solve"] / head["s_per_solve"],
+            "err_ratio_vs_uniform": head["err_rel_l2"] / res["uniform"]["err_rel_l2"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def batch_sets(seed=5, nsets=256):
     """256 independent sets: N log-uniform in [4096, 262144], half uniform in the unit cube and
     half from 4 Gaussian clusters (sigma 0.04, centres U[0.1, 0.9]^3, clipped), n = 4 or 8 at
@@ -804,7 +854,7 @@ def main():
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
     ap.add_argument("--workload", default="uniform-4m",
                     choices=["uniform-4m", "uniform-4m-variants", "uniform-32k", "gradient-1m", "batch-256",
-                             "clustered-16m", "near-field", "stages"],
+                             "clustered-16m", "clustered-16m-adaptive", "near-field", "stages"],
                     help="uniform-4m: the headline line; the others measure further configurations")
     ap.add_argument("--layout", default="uniform", choices=["uniform", "clustered"],
                     help="near-field / stages workloads: particle layout")
@@ -821,6 +871,8 @@ def main():
         return run_batch_256(args)
     if args.workload == "clustered-16m":
         return run_clustered_16m(args)
+    if args.workload == "clustered-16m-adaptive":
+        return run_clustered_16m_adaptive(args)
     if args.workload == "near-field":
         return run_near_field(args)
     if args.workload == "stages":

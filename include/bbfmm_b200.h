@@ -259,6 +259,20 @@ BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
 #define BBFMM_B200_KERNEL_ONEOVERR4 2
 BBFMM_B200_API int bbfmm_b200_set_kernel(bbfmm_b200_solver *s, int kernel);
 
+/* Adaptive refinement support (no counterpart in the reference, whose trees are uniform,
+ * anotherBuildFMMHierachy.c:44-55). A target region marks the cells of one level whose
+ * particles' results are wanted: active[m] != 0 for the Morton cells m of `level` (8^level
+ * bytes, host; level < 0 clears). The solve then computes the near field only for particles
+ * in active cells (others keep what the far field gives them), and the tensor-core M2L of every
+ * level above `level` (MIXED, two-box kernel) runs only on the tiles holding descendants of
+ * active cells. The first M2L level (default 2) starts the local expansions at that level:
+ * with first = l + 1 the solve gathers, for every target, only the sources inside the
+ * 3 x 3 x 3 neighbourhood of its level-l ancestor -- exactly the near field of a level-l
+ * leaf, computed by a deeper FMM. bbfmm_b200.AdaptiveSolver composes a coarse and a refined
+ * solver this way. Single-set solvers only. */
+BBFMM_B200_API int bbfmm_b200_set_target_region(bbfmm_b200_solver *s, int level, const unsigned char *active);
+BBFMM_B200_API int bbfmm_b200_set_first_m2l_level(bbfmm_b200_solver *s, int level);
+
 /* MIXED mode: products per term of the tensor-core M2L. 0 (default, adaptive): the three
  * split-BF16 products hi*hi + hi*lo + lo*hi for the contraction components j < 64 and the
  * outputs i < 64 of every operator, hi*hi alone for the rest, whose terms are small enough

@@ -1,0 +1,104 @@
+"""Two-level adaptive refinement (-m gpu): bbfmm_b200_set_first_m2l_level,
+bbfmm_b200_set_target_region and AdaptiveSolver. The reference has uniform trees only, so the
+oracle here is the FP64 direct sum.
+
+* Partition: a solve whose local expansions start at level l + 1 returns, for every target,
+  the sum over the sources in the 3 x 3 x 3 neighbourhood of its level-l ancestor -- checked
+  against that restricted direct sum (FP64 solve, n = 8: relative L2 < 1e-6, the FMM's own
+  approximation at these separations), with a target region that drops the near field of the
+  inactive cells' targets.
+* Composition: on a clustered set (four tight Gaussian clusters over a uniform background), the
+  adaptive solve against the FP64 direct sum on 2,048 targets, half of them in heavy leaves:
+  FP64 and mixed within 1.2x the error of the uniform FP64 solve at the fine depth; with no heavy
+  leaf it is exactly the coarse solve.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _clustered(N, seed):
+    rng = np.random.default_rng(seed)
+    nb = N // 4
+    c = rng.uniform(-0.3, 0.3, (4, 3))
+    xc = c[rng.integers(0, 4, N - nb)] + 0.02 * rng.standard_normal((N - nb, 3))
+    x = np.concatenate([rng.random((nb, 3)) - 0.5, np.clip(xc, -0.5, np.nextafter(0.5, 0))])
+    return x, rng.uniform(-1.0, 1.0, N)
+
+
+def test_first_m2l_level_gives_the_ancestor_neighbourhood():
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.fmm import leaf_of_particles, morton_to_grid
+    rng = np.random.default_rng(3)
+    N, lev, l = 30000, 4, 2
+    x = rng.random((N, 3)) - 0.5
+    q = rng.uniform(-1, 1, N)
+    s = Solver(8, lev, 1.0, mode="d")
+    s.set_particles(x)
+    s.set_first_m2l_level(l + 1)
+    # targets only in the level-l cells with an even Morton index
+    active = (np.arange(8 ** l) % 2 == 0)
+    s.set_target_region(l, active)
+    got = s.solve(torch.as_tensor(q, device="cuda")).cpu().numpy()
+    s.close()
+    anc, _ = leaf_of_particles(x, 1.0, l)
+    g = np.stack(morton_to_grid(anc, l), 1)
+    t = np.random.default_rng(4).choice(N, 600, replace=False)
+    want = np.empty(t.size)
+    for k, i in enumerate(t):
+        near = np.all(np.abs(g - g[i]) <= 1, axis=1)
+        near[i] = False
+        r = np.linalg.norm(x[near] - x[i], axis=1)
+        want[k] = q[i] * np.sum(q[near] / r)
+    act = active[anc[t]]  # targets outside the region get no near field and are not checked
+    assert rel_l2(got[t[act]], want[act]) < 1e-6, rel_l2(got[t[act]], want[act])
+    assert np.all(np.isfinite(got))
+
+
+@pytest.mark.parametrize("mode", ["d", "mixed"])
+def test_adaptive_solver_against_direct(mode):
+    import torch
+    from bbfmm_b200 import AdaptiveSolver, Solver
+    from bbfmm_b200.fmm import direct, leaf_of_particles
+    N = 400_000
+    x, q = _clustered(N, 7)
+    qd = torch.as_tensor(q, device="cuda")
+    a = AdaptiveSolver(8, 4, 6, mode=mode, cap=256)
+    a.set_particles(x)
+    assert a.heavy_leaves > 0 and a.fine is not None
+    got = a.solve(qd).double().cpu().numpy()
+    u = Solver(8, 6, 1.0, mode="d")
+    u.set_particles(x)
+    uni = u.solve(qd).cpu().numpy()
+    u.close()
+    leaf, counts = leaf_of_particles(x, 1.0, 4)
+    heavy = counts[leaf] > 256
+    rng = np.random.default_rng(8)
+    t = np.concatenate([rng.choice(np.nonzero(heavy)[0], 1024, replace=False),
+                        rng.choice(np.nonzero(~heavy)[0], 1024, replace=False)]).astype(np.int32)
+    ref = direct(torch.as_tensor(x, device="cuda"), qd, torch.as_tensor(t, device="cuda")).cpu().numpy()
+    e_a, e_u = rel_l2(got[t], ref), rel_l2(uni[t], ref)
+    print(f"adaptive ({mode}) {e_a:.3e}, uniform FP64 depth 6 {e_u:.3e}, heavy leaves {a.heavy_leaves}, "
+          f"refined particles {a.fine_particles}")
+    assert e_a <= 1.2 * e_u, (e_a, e_u)
+    a.close()
+
+
+def test_adaptive_without_heavy_leaves_is_the_coarse_solve():
+    import torch
+    from bbfmm_b200 import AdaptiveSolver, Solver
+    rng = np.random.default_rng(9)
+    x = rng.random((50000, 3)) - 0.5
+    q = torch.as_tensor(rng.uniform(-1, 1, 50000), device="cuda")
+    a = AdaptiveSolver(8, 4, 6, mode="mixed", cap=10_000)
+    a.set_particles(x)
+    assert a.fine is None
+    s = Solver(8, 4, 1.0, mode="mixed")
+    s.set_particles(x)
+    assert torch.equal(a.solve(q), s.solve(q))
+    a.close()
+    s.close()
