@@ -82,22 +82,15 @@ __device__ __forceinline__ typename NearTypes<MODE>::S stage_src(const typename 
 }
 
 // Per-target accumulator. v: sum of q_j K (FIELD: q_j / r), c: Neumaier compensation of v
-// (mixed), g*: sum of q_j (x_j - x_i) / r^3 (FIELD; FP64 in the mixed mode, where the FP32
-// factor q_j / r^3 times the FP64 separation costs one conversion per pair instead of three).
-// H: homogeneity of the kernel.
+// (mixed), g*: sum of q_j (x_j - x_i) / r^3 (FIELD). H: homogeneity of the kernel.
 template <int MODE, int H, bool FIELD>
 struct NearAcc {
   using T = NearTypes<MODE>;
   using C = typename T::C;
   using A = typename T::A;
-  using G = std::conditional_t<MODE == MODE_MIXED, double, A>;
   using Src = typename T::S;
-  A v, c;
-  G gx, gy, gz;
-  __device__ __forceinline__ void zero() {
-    v = c = (A)0;
-    gx = gy = gz = (G)0;
-  }
+  A v, c, gx, gy, gz;
+  __device__ __forceinline__ void zero() { v = c = gx = gy = gz = (A)0; }
   // The pair's contribution to v (0 for coincident points); FIELD: the gradient terms are
   // added here.
   __device__ __forceinline__ A term(C fx, C fy, C fz, const Src &g) {
@@ -114,10 +107,10 @@ struct NearAcc {
       else if constexpr (H == 2) t = __fmul_rn(g.q, (float)ex * (rinv * rinv * rinv));
       else t = __fmul_rn(g.q, rinv);
       if constexpr (FIELD) {
-        const double t3 = (double)(t * rinv * rinv);
-        gx = fma(t3, ex, gx);
-        gy = fma(t3, ey, gy);
-        gz = fma(t3, ez, gz);
+        const float t3 = t * rinv * rinv;
+        gx += t3 * (float)ex;
+        gy += t3 * (float)ey;
+        gz += t3 * (float)ez;
       }
       return t;
     } else {
