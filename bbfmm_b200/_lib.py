@@ -65,6 +65,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_batch_create.argtypes = [C.POINTER(Config), i, ip, ip, ip, vp, vp, vp, vp, vp, i, C.POINTER(vp)]
         L.bbfmm_b200_batch_solve.argtypes = [vp, vp, vp, i]
         L.bbfmm_b200_batch_autotune.argtypes = [vp, vp]
+        L.bbfmm_b200_batch_set_target_regions.argtypes = [vp, i, vp, i]
         L.bbfmm_b200_batch_groups.argtypes = [vp]
         L.bbfmm_b200_batch_graph_nodes.argtypes = [vp]
         L.bbfmm_b200_batch_graph_nodes.restype = C.c_longlong

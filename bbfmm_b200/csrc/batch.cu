@@ -199,6 +199,38 @@ struct Batch {
     return BBFMM_OK;
   }
 
+  // Target regions of every set at level depth_s - levels_up: active holds, set after set,
+  // the 8^(depth_s - levels_up) mask bytes of each set (null clears); with first_m2l the local
+  // expansions of each group start one level below its region level.
+  int set_target_regions(int levels_up, const unsigned char *active, int first_m2l) {
+    drop_graph();
+    std::vector<int64_t> off(nsets + 1, 0);
+    std::vector<int> depth(nsets, 0);
+    for (auto &g : groups)
+      for (int s : g.sets) depth[s] = g.maxlev;
+    for (int s = 0; s < nsets; ++s) {
+      const int R = depth[s] - levels_up;
+      if (active && (R < BBFMM_MINLEV || levels_up < 0))
+        return bbfmm_set_error(BBFMM_ERR_ARG, "region level below 2 for a set of the batch");
+      off[s + 1] = off[s] + (active ? pow8i(R) : 0);
+    }
+    for (auto &g : groups) {
+      Solver<T> &sv = *g.solver;
+      const int R = g.maxlev - levels_up;
+      if (!active) {
+        TRY_(sv.set_target_region(-1, nullptr));
+        TRY_(sv.set_m2l_first(BBFMM_MINLEV));
+        continue;
+      }
+      std::vector<unsigned char> m;
+      m.reserve(g.sets.size() * pow8i(R));
+      for (int s : g.sets) m.insert(m.end(), active + off[s], active + off[s + 1]);
+      TRY_(sv.set_target_region(R, m.data()));
+      TRY_(sv.set_m2l_first(first_m2l ? R + 1 : BBFMM_MINLEV));
+    }
+    return BBFMM_OK;
+  }
+
   int autotune(const void *q) {
     drop_graph();
     for (auto &g : groups) TRY_(g.solver->autotune(q, sizeof(T) == 8));
@@ -248,6 +280,13 @@ int bbfmm_b200_batch_solve(bbfmm_b200_batch *b, const void *q_dev, void *phi_dev
 int bbfmm_b200_batch_autotune(bbfmm_b200_batch *b, const void *q_dev) {
   if (!b || !q_dev) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   return b->d ? b->d->autotune(q_dev) : b->f->autotune(q_dev);
+}
+
+int bbfmm_b200_batch_set_target_regions(bbfmm_b200_batch *b, int levels_up, const unsigned char *active,
+                                        int first_m2l) {
+  if (!b) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  return b->d ? b->d->set_target_regions(levels_up, active, first_m2l)
+              : b->f->set_target_regions(levels_up, active, first_m2l);
 }
 
 int bbfmm_b200_batch_groups(const bbfmm_b200_batch *b) {

@@ -64,6 +64,19 @@ __host__ __device__ inline int64_t grid_to_cpg(int ix, int iy, int iz, int l) {
   return ((c * P + (iz >> 1)) * P + (iy >> 1)) * P + (ix >> 1);
 }
 
+// Cell (stacked Morton row) of local row t of a pass: rows[t] when the pass runs over a row
+// list (a local solve), else the slab's first row row0 + t.
+__host__ __device__ inline int64_t pass_cell(const int64_t *rows, int64_t row0, int64_t t) {
+  return rows ? rows[t] : row0 + t;
+}
+
+// Class-major row of stacked Morton row m of level l: set base + in-set cpg index.
+__host__ __device__ inline int64_t morton_to_cpg_row(int64_t m, int l) {
+  int ix, iy, iz;
+  morton_to_grid(m, l, ix, iy, iz);  // the set index above bit 3 l is ignored
+  return (m & ~(pow8i(l) - 1)) + grid_to_cpg(ix, iy, iz, l);
+}
+
 // Centre of a cell exactly as the reference accumulates it from the root
 // (anotherFMMDistribute.c:191-255, 336-344): c_l = c_{l-1} +/- celeng[l]/2, with
 // celeng[l] = L * 0.5^l obtained by repeated halving.

@@ -42,7 +42,8 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restrict__ M,
                                                           const double *__restrict__ Ecol,
                                                           double *__restrict__ Lout, int level, int j0, int j1,
-                                                          int ni, const int4 *__restrict__ offs) {
+                                                          int ni, const int4 *__restrict__ offs,
+                                                          const int *__restrict__ tile_list, int nsets) {
   // blockIdx.y selects one of gridDim.y groups of the 189 offsets; with several groups each
   // writes its partial sums to its own slice of Lout (level cells x R apart)
   extern __shared__ __align__(16) double smem[];
@@ -52,7 +53,8 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   const int tiles_per_class = nbox * nbox * nbox;
   // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
   // of neighbouring boxes, which read one source region that stays in L2
-  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;  // a list: only those tiles
+  const int set_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
   const int c = set_ * 8 + loc_ % 8;
   const int tb = loc_ / 8;
   const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   const int og = blockIdx.y, ng = gridDim.y;
   const int o0 = (189 * og) / ng, o1 = (189 * (og + 1)) / ng;
   const int niter = (o1 - o0) * nchunk;
-  Lout += (int64_t)og * (gridDim.x / tiles_per_class) * P3 * R;  // all classes of all sets
+  Lout += (int64_t)og * 8 * nsets * P3 * R;  // all classes of all sets
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
 
   auto issue = [&](int it, int buf) {
@@ -313,7 +315,8 @@ int64_t dmma_part_elems(int level, int nsets, int groups, int r) {
 // (0: dmma_default_groups) whose partials go to `part` (part_elems doubles) and are then
 // summed in a fixed order; with too little scratch the groups are reduced to fit.
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
-                    const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets, int ngroups) {
+                    const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets, int ngroups,
+                    const int *tile_list, int ntiles) {
   if (r != dm::R) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "FP64 tensor M2L is built for r = 256");
   if (j0 < 0 || j1 > r || j0 >= j1 || ni < 2 || ni > r || ni % 2)
     return bbfmm_set_error(BBFMM_ERR_ARG, "bad contraction / output range");
@@ -321,6 +324,10 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
   const int bw = P < 4 ? P : 4;
   const int nbox = P / bw;
   const int grid = 8 * nsets * nbox * nbox * nbox;
+  if (tile_list && (j0 != 0 || j1 != r || ni != r))
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tile lists are for the full FP64 M2L");
+  if (tile_list && (ntiles < 0 || ntiles > grid)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
+  if (tile_list && ntiles == 0) return BBFMM_OK;
   if (j0 == 0 && j1 <= 64 && (ni == 32 || ni == 64)) {  // the FP64 leading block
     static bool lattr = false;
     if (!lattr) {
@@ -350,17 +357,19 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
   int ng = ngroups > 0 ? ngroups : dmma_default_groups(level, nsets);
   if (ng > DMMA_PARTS) ng = DMMA_PARTS;
   const int64_t count = 8 * (int64_t)nsets * P * P * P * r;
-  if (!part) ng = 1;
+  if (!part || tile_list) ng = 1;
   else if ((int64_t)ng * count > part_elems) ng = (int)(part_elems / count);
   if (ng > 1) {
     // few target tiles: spread the offsets over ng CTAs per tile, then sum the partials
-    dm::m2l_dmma_kernel<<<dim3(grid, ng), 256, dm::SMEM_BYTES, s>>>(M, Ecol, part, level, j0, j1, ni, offs);
+    dm::m2l_dmma_kernel<<<dim3(grid, ng), 256, dm::SMEM_BYTES, s>>>(M, Ecol, part, level, j0, j1, ni, offs, nullptr,
+                                                                   nsets);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma", __FILE__, __LINE__);
     dm::sum_parts_kernel<<<(int)((count + 255) / 256), 256, 0, s>>>(count, ng, part, Lout);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma parts", __FILE__, __LINE__);
   }
-  dm::m2l_dmma_kernel<<<grid, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs);
+  dm::m2l_dmma_kernel<<<tile_list ? ntiles : grid, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs,
+                                                                             tile_list, nsets);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma", __FILE__, __LINE__);
 }
 

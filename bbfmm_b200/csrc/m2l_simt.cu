@@ -13,6 +13,7 @@
 // staging the shifted source box and the operator chunk in shared memory, and keeps a
 // register-blocked accumulator. With [j0, j1) = [0, r) this is the plain FP64 (or FP32)
 // M2L; with [0, 16) it is the FP64 leading-component part of the mixed-precision M2L.
+// A tile list (ids as the full grid numbers its tiles) runs only those tiles.
 //
 // Operators: Ert[k][i][j] = E_k(i, j) (row-major), i.e. the transpose of the
 // reference's column-major K file blocks.
@@ -30,7 +31,8 @@ struct OffsetTable {
 template <typename T, int R, int TM, int TN>
 __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T *__restrict__ M, const T *__restrict__ Ert,
                                                        T *__restrict__ Lout, int level, int j0, int j1,
-                                                       const int4 *__restrict__ offs, int accumulate) {
+                                                       const int4 *__restrict__ offs, int accumulate,
+                                                       const int *__restrict__ tile_list, int nsets) {
   constexpr int BK = 16;
   constexpr int NT = 64;  // targets per tile (4x4x4 box)
   constexpr int THREADS = (NT / TM) * (R / TN);
@@ -43,7 +45,8 @@ __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T 
   const int tiles_per_class = nbox * nbox * nbox;
   // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
   // of neighbouring boxes, which read one source region that stays in L2
-  const int set_ = (int)(blockIdx.x / (8 * tiles_per_class)), loc_ = (int)(blockIdx.x % (8 * tiles_per_class));
+  const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;
+  const int set_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
   const int c = set_ * 8 + loc_ % 8;
   const int tb = loc_ / 8;
   const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
@@ -61,7 +64,7 @@ __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T 
   // writes its partial sums to its own slice of Lout (all classes of all sets apart)
   const int grp = blockIdx.y, ngrp = gridDim.y;
   const int o0 = (189 * grp) / ngrp, o1 = (189 * (grp + 1)) / ngrp;
-  Lout += (int64_t)grp * (gridDim.x / tiles_per_class) * P3 * R;
+  Lout += (int64_t)grp * 8 * nsets * P3 * R;  // all classes of all sets
   for (int o = o0; o < o1; ++o) {
     const int4 ov = offs[(c & 7) * 189 + o];
     const int k = ov.x;
@@ -136,24 +139,31 @@ __global__ void simt_sum_parts_kernel(int64_t count, int ng, const T *__restrict
 
 // ngroups > 1 splits the 189 offsets over that many CTAs per target tile; their partials go
 // to `part` (part_elems elements) and are summed in a fixed order (groups are reduced to
-// fit the scratch; accumulate then does not apply).
+// fit the scratch; accumulate then does not apply). With a tile list of ntiles ids only those
+// tiles run, in one group, and the rest of Lout is left as it is.
 template <typename T>
 int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs,
-                    int accumulate, cudaStream_t s, int nsets, int ngroups, T *part, int64_t part_elems) {
-  const int tiles = nsets * m2l_simt_tiles(level);  // the class index runs over all sets' 8 classes
+                    int accumulate, cudaStream_t s, int nsets, int ngroups, T *part, int64_t part_elems,
+                    const int *tile_list, int ntiles) {
+  const int all = nsets * m2l_simt_tiles(level);  // the class index runs over all sets' 8 classes
+  if (tile_list && (ntiles < 0 || ntiles > all)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
+  if (tile_list && ntiles == 0) return BBFMM_OK;
+  const int tiles = tile_list ? ntiles : all;
   const int64_t P = (int64_t)1 << (level - 1);
   const int64_t count = 8 * nsets * P * P * P * r;
   int ng = ngroups > 0 ? ngroups : 1;
   if (ng > 21) ng = 21;
-  if (!part) ng = 1;
+  if (!part || tile_list) ng = 1;
   else if ((int64_t)ng * count > part_elems) ng = (int)(part_elems / count);
   if (ng < 1) ng = 1;
   T *dst = ng > 1 ? part : Lout;
   const dim3 grid(tiles, ng);
   if (r == 256) {
-    m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
+    m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate,
+                                                       tile_list, nsets);
   } else if (r == 32) {
-    m2l_simt_kernel<T, 32, 4, 4><<<grid, 128, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate);
+    m2l_simt_kernel<T, 32, 4, 4><<<grid, 128, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate,
+                                                     tile_list, nsets);
   } else {
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L rank must be 32 or 256 (n = 4 or 8)");
   }
@@ -166,9 +176,9 @@ int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0,
 }
 
 template int launch_m2l_simt<double>(int, const double *, const double *, double *, int, int, int, const int4 *, int,
-                                     cudaStream_t, int, int, double *, int64_t);
+                                     cudaStream_t, int, int, double *, int64_t, const int *, int);
 template int launch_m2l_simt<float>(int, const float *, const float *, float *, int, int, int, const int4 *, int,
-                                    cudaStream_t, int, int, float *, int64_t);
+                                    cudaStream_t, int, int, float *, int64_t, const int *, int);
 
 // Host table of the 189 offsets of each sibling class, as (k, vx, vy, vz).
 void build_offset_table(int *out /* 8*189*4 */) {

@@ -312,6 +312,11 @@ __global__ void __launch_bounds__(192, 1)
 // targets) as two M = 128 halves, each with its own 128 x 256 FP32 accumulator in TMEM (all
 // 512 columns), so every operator chunk loaded into shared memory serves 256 targets and the
 // operator traffic from L2 is halved. The lo halves of B cover the first TC_SPLIT_ROWS rows.
+// At levels 3 and 2, whose class grids are only 4 x 4 x 4 and 2 x 2 x 2, the 256 targets are
+// that whole grid in 4 or 32 consecutive stacked sets (one box load of 4 KB or 512 B per set
+// and operand half; slots past the last set load the last set again and write nothing), so a
+// batch of small trees runs its upper levels on the tensor cores as well. Rows: x fastest,
+// then y, z, set.
 // Stage: A_hi 16 KB | A_lo 16 KB | B_hi 16 KB | B_lo TC_SPLIT_ROWS x 32 BF16 (4 KB).
 // With Mlead and Erow given (leading block i < 32, j < 16), the four epilogue warps, idle
 // while the tensor cores run the ~1 ms mainloop of a CTA, compute that block in FP64 for the
@@ -327,7 +332,6 @@ __global__ void __launch_bounds__(192, 1)
 constexpr int A2_BYTES = 2 * A_BYTES, BLO2_BYTES = TC_SPLIT_ROWS * BK * 2;
 constexpr int STAGE2_BYTES = 2 * A2_BYTES + B_BYTES + BLO2_BYTES;
 constexpr int SMEM2_BYTES = STAGES * STAGE2_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-constexpr int BOX2_Y = 8;
 static_assert(SMEM2_BYTES <= 232448, "two-box stages exceed the shared memory of a CTA");
 
 __global__ void __launch_bounds__(192, 1)
@@ -335,7 +339,8 @@ __global__ void __launch_bounds__(192, 1)
                    const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                    double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
                    int split_chunks, int ncols, const double *__restrict__ Mlead, const double *__restrict__ Erow,
-                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows, const int *__restrict__ tile_list) {
+                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows, const int *__restrict__ tile_list,
+                   int nsets) {
   constexpr int STAGE_BYTES = STAGE2_BYTES;
   constexpr int DNZ = 16;  // components the fused down projection takes in FP64
   constexpr int split_rows = TC_SPLIT_ROWS;
@@ -353,16 +358,17 @@ __global__ void __launch_bounds__(192, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int P = 1 << (level - 1);
-  const int nbx = P / BOX_X, nby = P / BOX2_Y, nbz = P / BOX_Z;
+  const Tc2Box g = tc2_box(level);
+  const int nbx = P >> g.lx, nby = P >> g.ly, nbz = P >> g.lz;
   const int tiles_per_class = nbx * nby * nbz;
-  // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
-  // of neighbouring boxes, which read one source region that stays in L2
+  // sibling class fastest (the set group above it): the CTAs resident at one time are the 8
+  // classes of neighbouring boxes, which read one source region that stays in L2
   const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;  // a list: only those tiles
-  const int set_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
-  const int c = set_ * 8 + loc_ % 8;
-  const int tb = loc_ / 8;
-  const int bx0 = (tb % nbx) * BOX_X, by0 = ((tb / nbx) % nby) * BOX2_Y, bz0 = (tb / (nbx * nby)) * BOX_Z;
-  const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
+  const int sg_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
+  const int cls = loc_ % 8, tb = loc_ / 8;
+  const int set0 = sg_ << (8 - g.lb());  // first set of the tile
+  const int bx0 = (tb % nbx) << g.lx, by0 = ((tb / nbx) % nby) << g.ly, bz0 = (tb / (nbx * nby)) << g.lz;
+  const int cbx = (cls >> 2) & 1, cby = (cls >> 1) & 1, cbz = cls & 1;
   const int nchunk = ncols / BK;  // K-chunks per offset: the effective rank / 32 (8 for r = 256)
   const int chunk0 = kfirst / KS;  // whole chunks skipped
   const int kstep0 = kfirst % KS;  // K-steps skipped in the first used chunk
@@ -396,7 +402,7 @@ __global__ void __launch_bounds__(192, 1)
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
       if (!mbar_wait(empty_bar(s), ph ^ 1u, 1)) break;
       const int o = it / used_chunks, kc = chunk0 + it % used_chunks;
-      const int4 ov = offs[(c & 7) * 189 + o];
+      const int4 ov = offs[cls * 189 + o];
       const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
       const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
       const int sc = (scx << 2) | (scy << 1) | scz;
@@ -407,12 +413,15 @@ __global__ void __launch_bounds__(192, 1)
       const bool three = kc < split_chunks;
       const uint32_t bhi_bytes = (uint32_t)ncols * BK * 2;  // the B box holds the first ncols rows i
       mbar_expect_tx(full_bar(s), three ? 2 * A2_BYTES + bhi_bytes + BLO2_BYTES : A2_BYTES + bhi_bytes);
-      tma_load_5d(st, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
-      tma_load_3d(st + 2 * A2_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
-      if (three) {
-        tma_load_5d(st + A2_BYTES, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, (c & ~7) + sc);
-        tma_load_3d(st + 2 * A2_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
+      // one box per set of the tile (sets past the last one load the last set: the same bytes)
+      const uint32_t box_bytes = (uint32_t)BK * 2u << g.lb();
+      for (int k = 0; k < (1 << (8 - g.lb())); ++k) {
+        const int sidx = (set0 + k < nsets ? set0 + k : nsets - 1) * 8 + sc;
+        tma_load_5d(st + k * box_bytes, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, sidx);
+        if (three) tma_load_5d(st + A2_BYTES + k * box_bytes, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, sidx);
       }
+      tma_load_3d(st + 2 * A2_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
+      if (three) tma_load_3d(st + 2 * A2_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
@@ -448,30 +457,37 @@ __global__ void __launch_bounds__(192, 1)
     // ---------------- epilogue: TMEM -> registers -> Lacc
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;
+    const int64_t P3 = (int64_t)P * P * P;
     if (Mlead) {
       // FP64 leading block of rows h * 128 + q * 32 + [0, 32): fragment m holds the 8 rows
-      // 8m .. 8m + 7 of that range (x = 0..7 at one y, z of the box)
-      const int64_t P3 = (int64_t)P * P * P;
+      // 8m .. 8m + 7 of that range, this lane's A row being 8m + (lane >> 2)
       const int u = lane & 3, tr = lane >> 2;
       for (int h = 0; h < 2; ++h) {
         double acc[4][4][2];
+        int ax[4], ay[4], az[4], aset[4];  // grid position and set of this lane's A rows
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
+        for (int m = 0; m < 4; ++m) {
 #pragma unroll
           for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
+          g.pos(h * 128 + q * 32 + 8 * m + tr, ax[m], ay[m], az[m], aset[m]);
+          ax[m] += bx0;
+          ay[m] += by0;
+          az[m] += bz0;
+          aset[m] += set0;
+        }
         for (int o = 0; o < 189; ++o) {
-          const int4 ov = offs[(c & 7) * 189 + o];
+          const int4 ov = offs[cls * 189 + o];
           const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
           const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
           const int sc = (scx << 2) | (scy << 1) | scz;
-          const int px = bx0 + tr + (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
-          const double *Mc = Mlead + (int64_t)((c & ~7) + sc) * P3 * BN + 4 * u;
+          const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;
           double2 a[4][2], b[4][2];
 #pragma unroll
           for (int m = 0; m < 4; ++m) {
-            const int r0 = h * 128 + q * 32 + 8 * m;
-            const int py = by0 + ((r0 >> 3) & 7) + shy, pz = bz0 + (r0 >> 6) + shz;
-            if ((unsigned)px < (unsigned)P && (unsigned)py < (unsigned)P && (unsigned)pz < (unsigned)P) {
+            const int px = ax[m] + shx, py = ay[m] + shy, pz = az[m] + shz;
+            if ((unsigned)px < (unsigned)P && (unsigned)py < (unsigned)P && (unsigned)pz < (unsigned)P &&
+                aset[m] < nsets) {
+              const double *Mc = Mlead + (int64_t)(aset[m] * 8 + sc) * P3 * BN + 4 * u;
               const double2 *src = reinterpret_cast<const double2 *>(Mc + (((int64_t)pz * P + py) * P + px) * BN);
               a[m][0] = src[0];
               a[m][1] = src[1];
@@ -496,12 +512,11 @@ __global__ void __launch_bounds__(192, 1)
                 dmma_f64(acc[m][f][0], acc[m][f][1], av, (ks & 1) ? b[f][ks >> 1].y : b[f][ks >> 1].x);
             }
         }
-        // D fragment: row tr of fragment m, columns 8f + 2u + {0, 1}
+        // D fragment: row tr of fragment m (the A row of this lane), columns 8f + 2u + {0, 1}
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-          const int rr = h * 128 + q * 32 + 8 * m + tr;
-          const int64_t cell =
-              (int64_t)c * P3 + ((int64_t)(bz0 + (rr >> 6)) * P + (by0 + ((rr >> 3) & 7))) * P + (bx0 + tr);
+          if (aset[m] >= nsets) continue;
+          const int64_t cell = (int64_t)(aset[m] * 8 + cls) * P3 + ((int64_t)az[m] * P + ay[m]) * P + ax[m];
           double *dst = Lacc + cell * BN;
 #pragma unroll
           for (int f = 0; f < 4; ++f)
@@ -514,18 +529,20 @@ __global__ void __launch_bounds__(192, 1)
     const bool ok = mbar_wait(acc_bar, 0, 3);
     tc_fence_after();
     for (int h = 0; h < 2 && ok; ++h) {
-      const int rr = h * 128 + row;  // row of the 8x8x4 box: x fastest, then y, then z
-      const int tx = rr % BOX_X, ty = (rr / BOX_X) % BOX2_Y, tz = rr / (BOX_X * BOX2_Y);
-      const int64_t P3 = (int64_t)P * P * P;
-      const int64_t cell = (int64_t)c * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
+      int tx, ty, tz, ts;
+      g.pos(h * 128 + row, tx, ty, tz, ts);
+      const int set = set0 + ts;
+      const bool valid = set < nsets;  // rows of sets past the last: read from TMEM, not written
+      const int64_t cell = (int64_t)(set * 8 + cls) * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
       double *dst = Lacc + cell * BN;
       int64_t mrow = 0;  // Morton row of the cell: set base + Morton index of its grid position
       if (Lsplit)
-        mrow = (int64_t)(c >> 3) * 8 * P3 +
+        mrow = (int64_t)set * 8 * P3 +
                grid_to_morton(2 * (bx0 + tx) + cbx, 2 * (by0 + ty) + cby, 2 * (bz0 + tz) + cbz, level);
       for (int col = 0; col < ncols; col += 32) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 256 + col), v);
+        if (!valid) continue;
         const bool add = col < ilead;  // ilead is a multiple of 32
         const bool fp = !Lsplit || col < 32;
         __align__(16) __nv_bfloat16 sh[32], sl[32];
@@ -650,7 +667,8 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
                       const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                       const double *__restrict__ Lfp, int ldl, const double *__restrict__ Dlead,
                       double *__restrict__ F, int ldf, int64_t rows, int level, int64_t row0, int kc0, int kc1,
-                      const double *__restrict__ cs, double scale, int64_t ntiles, int col_skip) {
+                      const double *__restrict__ cs, double scale, int64_t ntiles, int col_skip,
+                      const int64_t *__restrict__ rowlist) {
   constexpr int ncb = UP ? 1 : 2;  // 256-column blocks: r = 256 outputs up, n3 = 512 down
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -758,22 +776,14 @@ __global__ void __launch_bounds__(PD_THREADS, 1)
       const int col0 = (int)(tile % ncb) * BN;
       // output row of row 16h + (lane & 15) of the quarter (up: read back by shuffles)
       int64_t orow = tq + 16 * h + (lane & 15);
-      if (UP) {
-        const int64_t g = row0 + orow;
-        int ix, iy, iz;
-        morton_to_grid(g, level, ix, iy, iz);
-        orow = (g & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
-      }
+      if (UP && orow < rows) orow = morton_to_cpg_row(pass_cell(rowlist, row0, orow), level);
       // A fragments: rows tq + 16h + 8m + tr, components 4u .. 4u + 3 (FP64 L in cpg order)
       double2 a[2][2];
 #pragma unroll
       for (int m = 0; m < 2; ++m) {
         const int64_t t = tq + 16 * h + 8 * m + tr;
         if (!UP && t < rows) {
-          const int64_t g = row0 + t;
-          int ix, iy, iz;
-          morton_to_grid(g, level, ix, iy, iz);
-          const int64_t crow = (g & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
+          const int64_t crow = morton_to_cpg_row(pass_cell(rowlist, row0, t), level);
           const double2 *src = reinterpret_cast<const double2 *>(Lfp + crow * ldl + 4 * u);
           a[m][0] = src[0];
           a[m][1] = src[1];
@@ -863,18 +873,12 @@ __global__ void lead_transpose_kernel(int K, int N, int lead, const double *__re
 // loads, one 16-byte store per plane. K is a multiple of 256.
 __global__ void split_rows_kernel(int64_t rows, int K, const double *__restrict__ src, int gather, int level,
                                   int64_t row0, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
-                                  int zlead) {
+                                  int zlead, const int64_t *__restrict__ rowlist) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t t = warp; t < rows; t += nwarps) {
-    int64_t sr = t;
-    if (gather) {
-      const int64_t m = row0 + t;
-      int ix, iy, iz;
-      morton_to_grid(m, level, ix, iy, iz);
-      sr = (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);
-    }
+    const int64_t sr = gather ? morton_to_cpg_row(pass_cell(rowlist, row0, t), level) : t;
     const double4 *in = reinterpret_cast<const double4 *>(src + sr * K);
     uint4 *oh = reinterpret_cast<uint4 *>(hi + t * K), *ol = reinterpret_cast<uint4 *>(lo + t * K);
     for (int c = lane; c < K / 8; c += 32) {
@@ -1067,7 +1071,7 @@ void tc_free_projections(void *v) {
 // (sum_{j < 16} L[cpg(row0 + t)][j] Bdn[j][l] in FP64 + sum_{16 <= j < rank} L'[t][j] Bdn[j][l]
 // from the split rows L' = Asplit, whose components j < 16 are zero), F rows n3 apart, assigned.
 int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int64_t rows, double *F, int level,
-                     int64_t row0, const double *cs, double scale, cudaStream_t s, int rank) {
+                     int64_t row0, const double *cs, double scale, cudaStream_t s, int rank, const int64_t *rowlist) {
   const TcProj *p = (const TcProj *)pv;
   if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
   if (rows <= 0) return BBFMM_OK;
@@ -1089,7 +1093,7 @@ int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int6
   const int grid = (int)(ntiles < 148 ? ntiles : 148);
   tc::proj_fused_kernel<false><<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(
       ahi, alo, p->dn_hi, p->dn_lo, Lfp, p->r, p->dn_lead, F, p->n3, rows, level, row0, 0,
-      (rank > 0 ? rank : p->r) / tc::BK, cs, scale, ntiles, 0);
+      (rank > 0 ? rank : p->r) / tc::BK, cs, scale, ntiles, 0, rowlist);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_down", __FILE__, __LINE__);
 }
 
@@ -1097,7 +1101,7 @@ int launch_proj_down(const void *pv, const void *Asplit, const double *Lfp, int6
 // Bup[l][j] from the split S rows (Asplit, rows x n3), assigned for every j; the split operator
 // is zero for j < lead, whose FP64 values proj_narrow_kernel writes afterwards.
 int launch_proj_up(const void *pv, const void *Asplit, int64_t rows, double *M, int level, int64_t row0,
-                   cudaStream_t s) {
+                   cudaStream_t s, const int64_t *rowlist) {
   const TcProj *p = (const TcProj *)pv;
   if (!p) return bbfmm_set_error(BBFMM_ERR_STATE, "tensor-core projections not prepared");
   if (rows <= 0) return BBFMM_OK;
@@ -1118,17 +1122,18 @@ int launch_proj_up(const void *pv, const void *Asplit, int64_t rows, double *M, 
   const int grid = (int)(ntiles < 148 ? ntiles : 148);
   tc::proj_fused_kernel<true><<<grid, tc::PD_THREADS, tc::PD_SMEM, s>>>(
       ahi, alo, p->up_hi, p->up_lo, nullptr, 0, nullptr, M, p->r, rows, level, row0, 0, p->n3 / tc::BK, nullptr, 1.0,
-      ntiles, 0);
+      ntiles, 0, rowlist);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_up", __FILE__, __LINE__);
 }
 
 // [hi | lo] split of rows x K FP64 values; gather != 0 reads row t from the cpg row of Morton
 // cell row0 + t of `level`.
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
-                  cudaStream_t s, int zlead) {
+                  cudaStream_t s, int zlead, const int64_t *rowlist) {
   if (K % 256) return bbfmm_set_error(BBFMM_ERR_ARG, "split rows: K must be a multiple of 256");
   __nv_bfloat16 *hi = (__nv_bfloat16 *)dst;
-  tc::split_rows_kernel<<<148 * 16, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K, zlead);
+  tc::split_rows_kernel<<<148 * 16, 256, 0, s>>>(rows, K, src, gather, level, row0, hi, hi + rows * K, zlead,
+                                                 rowlist);
   return bbfmm_set_cuda_error(cudaGetLastError(), "split", __FILE__, __LINE__);
 }
 
@@ -1166,7 +1171,12 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   if (split_rows > rank) split_rows = rank;
   if (!ops || r != 256) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tensor-core M2L needs r = 256 operators");
   const int P = 1 << (level - 1);
-  if (P < tc::BOX_X) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs level >= 4");
+  // the adaptive map runs two 128-target halves of a 256-target box per CTA (m2l_tc2_kernel)
+  const bool two = nprod == 0 && split_rows == TC_SPLIT_ROWS;
+  if (level < (two ? TC2_MIN_LEVEL : TC_MIN_LEVEL))
+    return bbfmm_set_error(BBFMM_ERR_ARG, two ? "tensor-core M2L needs level >= 2" : "tensor-core M2L needs level >= 4");
+  if (nsets < 1) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs a set");
+  const Tc2Box g2 = tc2_box(level);
   const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Msplit + (size_t)cell_offset * r;
   const __nv_bfloat16 *lo = (const __nv_bfloat16 *)Msplit + (size_t)(ncell_total + cell_offset) * r;
   CUtensorMap mapAhi, mapAlo;
@@ -1174,9 +1184,8 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   const cuuint64_t dims[5] = {(cuuint64_t)r, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)8 * nsets};
   const cuuint64_t strides[4] = {(cuuint64_t)r * 2, (cuuint64_t)r * 2 * P, (cuuint64_t)r * 2 * P * P,
                                  (cuuint64_t)r * 2 * P * P * P};
-  // the adaptive map runs two 128-target halves of an 8x8x4 box per CTA (m2l_tc2_kernel)
-  const bool two = nprod == 0 && split_rows == TC_SPLIT_ROWS;
-  const cuuint32_t box[5] = {tc::BK, tc::BOX_X, (cuuint32_t)(two ? tc::BOX2_Y : tc::BOX_Y), tc::BOX_Z, 1};
+  const cuuint32_t box[5] = {tc::BK, two ? 1u << g2.lx : (cuuint32_t)tc::BOX_X,
+                             two ? 1u << g2.ly : (cuuint32_t)tc::BOX_Y, two ? 1u << g2.lz : (cuuint32_t)tc::BOX_Z, 1};
   int rc = make_map(&mapAhi, (void *)hi, 5, dims, strides, box);
   if (rc == BBFMM_OK) rc = make_map(&mapAlo, (void *)lo, 5, dims, strides, box);
   if (rc != BBFMM_OK) return rc;
@@ -1207,14 +1216,14 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
       if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc2 smem attribute", __FILE__, __LINE__);
       attr2 = true;
     }
-    const int tiles2 = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX2_Y) * (P / tc::BOX_Z);
+    const int64_t tiles2 = tc2_tiles(level, nsets);
     const bool fuse = Mlead && Erow && tc_fuses_lead(ops, nprod, rank) && kfirst == 0 && ilead == 32;
     if (Lsplit && !fuse) return bbfmm_set_error(BBFMM_ERR_ARG, "split M2L output needs the fused leading block");
     if (tile_list && (ntiles < 0 || ntiles > tiles2)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
     if (tile_list && ntiles == 0) return BBFMM_OK;
-    tc::m2l_tc2_kernel<<<tile_list ? ntiles : tiles2, 192, tc::SMEM2_BYTES, s>>>(
+    tc::m2l_tc2_kernel<<<(unsigned)(tile_list ? (int64_t)ntiles : tiles2), 192, tc::SMEM2_BYTES, s>>>(
         mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst, ilead, split_chunks, rank, fuse ? Mlead : nullptr,
-        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P, tile_list);
+        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P, tile_list, nsets);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
   }
   static bool attr = false;

@@ -56,7 +56,8 @@ template <> __device__ __forceinline__ const float *tab_cw<float>(const Tables &
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   int maxlev, T L, Tables tabs, T *__restrict__ S, int64_t m0,
-                                                  int64_t count, __nv_bfloat16 *__restrict__ Ssplit) {
+                                                  int64_t count, __nv_bfloat16 *__restrict__ Ssplit,
+                                                  const int64_t *__restrict__ rows) {
   constexpr int N3 = NN * NN * NN;
   constexpr int PER = (N3 + 31) / 32;
   __shared__ T s_tkz[NN * NN];
@@ -71,7 +72,7 @@ __global__ void __launch_bounds__(128) p2m_kernel(const T *__restrict__ pos4, co
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t mm = warp; mm < count; mm += nwarps) {
-    const int64_t m = m0 + mm;  // leaf; S holds leaves m0 .. m0 + count - 1
+    const int64_t m = pass_cell(rows, m0, mm);  // leaf; S holds the pass's leaves in order
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);  // the set index above bit 3 maxlev is ignored
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
@@ -281,24 +282,25 @@ template <int NN> __device__ __forceinline__ int f_l2(int k, int lane) {
 // one is evaluated. body(leaf m, local index mm, p0, p1, F registers) does the arithmetic.
 template <typename T, int NN, typename Body>
 __device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start, const T *__restrict__ F, int64_t m0,
-                                             int64_t count, Body body) {
+                                             int64_t count, const int64_t *__restrict__ rows, Body body) {
   constexpr int PER = NN * NN * NN / 32;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   T fc[PER], fn[PER];
   int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-  if (warp < count) { a0 = leaf_start[m0 + warp]; a1 = leaf_start[m0 + warp + 1]; }
-  if (warp + nwarps < count) { b0 = leaf_start[m0 + warp + nwarps]; b1 = leaf_start[m0 + warp + nwarps + 1]; }
+  auto leaf = [&](int64_t mm) { return pass_cell(rows, m0, mm); };
+  if (warp < count) { a0 = leaf_start[leaf(warp)]; a1 = leaf_start[leaf(warp) + 1]; }
+  if (warp + nwarps < count) { b0 = leaf_start[leaf(warp + nwarps)]; b1 = leaf_start[leaf(warp + nwarps) + 1]; }
 #pragma unroll
   for (int k = 0; k < PER; ++k) fc[k] = a1 > a0 ? F[warp * (NN * NN * NN) + lane + 32 * k] : (T)0;
   for (int64_t mm = warp; mm < count; mm += nwarps) {
     int c0 = 0, c1 = 0;
-    if (mm + 2 * nwarps < count) { c0 = leaf_start[m0 + mm + 2 * nwarps]; c1 = leaf_start[m0 + mm + 2 * nwarps + 1]; }
+    if (mm + 2 * nwarps < count) { c0 = leaf_start[leaf(mm + 2 * nwarps)]; c1 = leaf_start[leaf(mm + 2 * nwarps) + 1]; }
     const bool nxt = mm + nwarps < count && b1 > b0;
 #pragma unroll
     for (int k = 0; k < PER; ++k) fn[k] = nxt ? F[(mm + nwarps) * (NN * NN * NN) + lane + 32 * k] : (T)0;
-    if (a1 > a0) body(m0 + mm, a0, a1, fc);
+    if (a1 > a0) body(leaf(mm), a0, a1, fc);
 #pragma unroll
     for (int k = 0; k < PER; ++k) fc[k] = fn[k];
     a0 = b0; a1 = b1; b0 = c0; b1 = c1;
@@ -315,7 +317,8 @@ template <> struct Vec4<float> { using type = float4; };
 template <typename T, int NN>
 __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   int maxlev, T L, Tables tabs, const T *__restrict__ F,
-                                                  T *__restrict__ phi, int64_t m0, int64_t count) {
+                                                  T *__restrict__ phi, int64_t m0, int64_t count,
+                                                  const int64_t *__restrict__ rows) {
   constexpr int PER = NN * NN * NN / 32;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
@@ -328,7 +331,7 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
   const T pre3 = prefac * prefac * prefac;
   using V4 = typename Vec4<T>::type;
   const V4 *p4 = reinterpret_cast<const V4 *>(pos4);
-  l2p_pipeline<T, NN>(leaf_start, F, m0, count, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
+  l2p_pipeline<T, NN>(leaf_start, F, m0, count, rows, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
@@ -370,21 +373,17 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
 // Register-blocked SIMT GEMM: CTA tile 128 x BN, K-chunks of 16, 256 threads.
 // Local row m of a slab starting at cell row0: its cpg index when `which` is the mapped
 // side, else m itself.
-__device__ __forceinline__ int64_t map_row(int64_t m, int64_t row0, int level, int which, int mode) {
-  if (mode == which) {
-    m += row0;
-    int ix, iy, iz;
-    morton_to_grid(m, level, ix, iy, iz);
-    return (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);  // set base + in-set index
-  }
-  return m;
+__device__ __forceinline__ int64_t map_row(int64_t m, int64_t row0, const int64_t *rows, int level, int which,
+                                           int mode) {
+  return mode == which ? morton_to_cpg_row(pass_cell(rows, row0, m), level) : m;
 }
 
 template <typename T, int BN>
 __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N, const T *__restrict__ A,
                                                         const float *__restrict__ A2, const T *__restrict__ B,
                                                         const T *__restrict__ cs, T scale, T *__restrict__ C,
-                                                        int level, int mapmode, int64_t row0, int ldc, int lda) {
+                                                        int level, int mapmode, int64_t row0, int ldc, int lda,
+                                                        const int64_t *__restrict__ rows) {
   constexpr int BM = 128, BK = 16, TN = BN / 16;
   __shared__ T sa[BK][BM + 1];
   __shared__ T sb[BK][BN];
@@ -403,7 +402,7 @@ __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N,
       const int64_t m = m0 + r;
       T v = 0;
       if (m < M && k0 + c < K) {
-        const int64_t ar = map_row(m, row0, level, MAP_IN_CPG, mapmode);
+        const int64_t ar = map_row(m, row0, rows, level, MAP_IN_CPG, mapmode);
         v = A[ar * lda + k0 + c];
         if (A2) v += (T)A2[ar * lda + k0 + c];
       }
@@ -432,7 +431,7 @@ __global__ void __launch_bounds__(256) proj_gemm_kernel(int64_t M, int K, int N,
   for (int i = 0; i < 8; ++i) {
     const int64_t m = m0 + ty * 8 + i;
     if (m >= M) continue;
-    const int64_t cr = map_row(m, row0, level, MAP_OUT_CPG, mapmode);
+    const int64_t cr = map_row(m, row0, rows, level, MAP_OUT_CPG, mapmode);
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
       const int n = n0 + tx + 16 * j;
@@ -503,13 +502,13 @@ static int resident_grid(int threads) {
 
 template <typename T>
 int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s,
-               int nsets, int64_t first, int64_t count, void *Ssplit) {
+               int nsets, int64_t first, int64_t count, void *Ssplit, const int64_t *rows) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
   const int grid = grid_for(count, 4, 148 * 64);
   __nv_bfloat16 *sp = (__nv_bfloat16 *)Ssplit;
-  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count, sp);
-  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count, sp);
+  if (n == 4) p2m_kernel<T, 4><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count, sp, rows);
+  else if (n == 8) p2m_kernel<T, 8><<<grid, 128, 0, s>>>(pos4, leaf_start, maxlev, L, t, S, first, count, sp, rows);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "p2m", __FILE__, __LINE__);
 }
@@ -554,31 +553,33 @@ int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream
 
 template <typename T>
 int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi,
-               cudaStream_t s, int nsets, int64_t first, int64_t count) {
+               cudaStream_t s, int nsets, int64_t first, int64_t count, const int64_t *rows) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
   if (n == 4)
     l2p_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 4>>(128)), 128, 0, s>>>(
-        pos4, leaf_start, maxlev, L, t, F, phi, first, count);
+        pos4, leaf_start, maxlev, L, t, F, phi, first, count, rows);
   else if (n == 8)
     l2p_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 8>>(128)), 128, 0, s>>>(
-        pos4, leaf_start, maxlev, L, t, F, phi, first, count);
+        pos4, leaf_start, maxlev, L, t, F, phi, first, count, rows);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p", __FILE__, __LINE__);
 }
 
 template <typename T>
 int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C,
-                int level, int mapmode, cudaStream_t s, int64_t row0, int ldc, int lda) {
+                int level, int mapmode, cudaStream_t s, int64_t row0, int ldc, int lda, const int64_t *rows) {
   if (M <= 0) return BBFMM_OK;
   if (ldc <= 0) ldc = N;
   if (lda <= 0) lda = K;
   if (N >= 64) {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 63) / 64));
-    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc, lda);
+    proj_gemm_kernel<T, 64><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc, lda,
+                                                 rows);
   } else {
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + 31) / 32));
-    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc, lda);
+    proj_gemm_kernel<T, 32><<<grid, 256, 0, s>>>(M, K, N, A, A2, B, cs, scale, C, level, mapmode, row0, ldc, lda,
+                                                 rows);
   }
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj", __FILE__, __LINE__);
 }
@@ -605,13 +606,13 @@ int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaS
 
 #define INST(T)                                                                                           \
   template int launch_p2m<T>(int, const T *, const int *, int, T, const Tables &, T *, cudaStream_t, int,   \
-                             int64_t, int64_t, void *);                                                    \
+                             int64_t, int64_t, void *, const int64_t *);                                   \
   template int launch_m2m<T>(int, const T *, T *, int, const Tables &, cudaStream_t, int, int64_t, int64_t); \
   template int launch_l2l<T>(int, const T *, T *, int, const Tables &, cudaStream_t, int, int64_t, int64_t); \
   template int launch_l2p<T>(int, const T *, const int *, int, T, const Tables &, const T *, T *,          \
-                             cudaStream_t, int, int64_t, int64_t);                                         \
+                             cudaStream_t, int, int64_t, int64_t, const int64_t *);                        \
   template int launch_proj<T>(int64_t, int, int, const T *, const float *, const T *, const T *, T, T *,   \
-                              int, int, cudaStream_t, int64_t, int, int);                                  \
+                              int, int, cudaStream_t, int64_t, int, int, const int64_t *);                 \
   template int launch_morton_cpg<T>(int, int, const T *, T *, int, cudaStream_t);
 INST(float)
 INST(double)
@@ -655,7 +656,7 @@ template <typename T, int NN>
 __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                         int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                         T *__restrict__ pot, T *__restrict__ fld, int64_t m0,
-                                                        int64_t count) {
+                                                        int64_t count, const int64_t *__restrict__ rows) {
   constexpr int PER = NN * NN * NN / 32;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
@@ -668,7 +669,7 @@ __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ po
   const T pre3 = prefac * prefac * prefac;
   using V4 = typename Vec4<T>::type;
   const V4 *p4 = reinterpret_cast<const V4 *>(pos4);
-  l2p_pipeline<T, NN>(leaf_start, F, m0, count, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
+  l2p_pipeline<T, NN>(leaf_start, F, m0, count, rows, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
@@ -757,15 +758,15 @@ __global__ void scatter_field_kernel(int N, const int *__restrict__ perm, const 
 
 template <typename T>
 int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F,
-                     T *pot, T *fld, cudaStream_t s, int nsets, int64_t first, int64_t count) {
+                     T *pot, T *fld, cudaStream_t s, int nsets, int64_t first, int64_t count, const int64_t *rows) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
   if (n == 4)
     l2p_field_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 4>>(128)), 128, 0, s>>>(
-        pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
+        pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count, rows);
   else if (n == 8)
     l2p_field_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 8>>(128)), 128, 0, s>>>(
-        pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count);
+        pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count, rows);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p_field", __FILE__, __LINE__);
 }
@@ -779,9 +780,9 @@ int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO 
 }
 
 template int launch_l2p_field<double>(int, const double *, const int *, int, double, const Tables &, const double *,
-                                      double *, double *, cudaStream_t, int, int64_t, int64_t);
+                                      double *, double *, cudaStream_t, int, int64_t, int64_t, const int64_t *);
 template int launch_l2p_field<float>(int, const float *, const int *, int, float, const Tables &, const float *,
-                                     float *, float *, cudaStream_t, int, int64_t, int64_t);
+                                     float *, float *, cudaStream_t, int, int64_t, int64_t, const int64_t *);
 template int launch_scatter_field<double, double>(int, const int *, const double *, const double *, double *,
                                                   double *, cudaStream_t);
 template int launch_scatter_field<float, float>(int, const int *, const float *, const float *, float *, float *,

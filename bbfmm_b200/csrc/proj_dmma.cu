@@ -30,20 +30,17 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-// Local row m of a slab starting at cell row0: its cpg index (to_cpg) or m itself.
-__device__ __forceinline__ int64_t remap(int64_t m, int64_t row0, int level, bool to_cpg) {
-  if (!to_cpg) return m;
-  m += row0;
-  int ix, iy, iz;
-  morton_to_grid(m, level, ix, iy, iz);
-  return (m & ~(pow8i(level) - 1)) + grid_to_cpg(ix, iy, iz, level);  // set base + in-set index
+// Local row m of a pass (the slab from cell row0, or the row list `rows`): the cpg row of its
+// cell (to_cpg) or m itself.
+__device__ __forceinline__ int64_t remap(int64_t m, int64_t row0, const int64_t *rows, int level, bool to_cpg) {
+  return to_cpg ? morton_to_cpg_row(pass_cell(rows, row0, m), level) : m;
 }
 
 __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int N, const double *__restrict__ A,
                                                            const double *__restrict__ B,
                                                            const double *__restrict__ cs, double scale,
                                                            double *__restrict__ C, int level, int mapmode,
-                                                           int64_t row0, int lda) {
+                                                           int64_t row0, int lda, const int64_t *__restrict__ rows) {
   extern __shared__ __align__(16) double smem[];
   __shared__ int64_t arow[BM];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -54,7 +51,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
   const int nk = K / BK;
   if (tid < BM) {
     const int64_t m = m0 + tid;
-    arow[tid] = m < M ? remap(m, row0, level, mapmode == MAP_IN_CPG) : -1;
+    arow[tid] = m < M ? remap(m, row0, rows, level, mapmode == MAP_IN_CPG) : -1;
   }
   __syncthreads();
 
@@ -111,7 +108,7 @@ __global__ void __launch_bounds__(256, 1) proj_dmma_kernel(int64_t M, int K, int
   for (int mf = 0; mf < 4; ++mf) {
     const int64_t m = m0 + wm * 32 + mf * 8 + (lane >> 2);
     if (m >= M) continue;
-    double *dst = C + remap(m, row0, level, mapmode == MAP_OUT_CPG) * N;
+    double *dst = C + remap(m, row0, rows, level, mapmode == MAP_OUT_CPG) * N;
 #pragma unroll
     for (int nf = 0; nf < 8; ++nf) {
       const int n = n0 + wn * 64 + nf * 8 + 2 * (lane & 3);
@@ -132,7 +129,8 @@ constexpr int SMEM_BYTES = 2 * STAGE * 8;
 
 __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, const double *__restrict__ A,
                                                           const double *__restrict__ B, double *__restrict__ C,
-                                                          int ldc, int level, int mapmode, int64_t row0) {
+                                                          int ldc, int level, int mapmode, int64_t row0,
+                                                          const int64_t *__restrict__ rows) {
   extern __shared__ __align__(16) double smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, r8 = lane >> 2, c4 = lane & 3;
   const int64_t m0 = (int64_t)blockIdx.x * nw::BM;
@@ -145,7 +143,7 @@ __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, cons
     for (int e = tid; e < nw::BM * (nw::BK / 2); e += 256) {  // 128 rows x 8 pairs
       const int row = e / (nw::BK / 2), k2 = (e % (nw::BK / 2)) * 2;
       const int64_t m = m0 + row;
-      const int64_t ar = m < M ? remap(m, row0, level, mapmode == MAP_IN_CPG) : -1;
+      const int64_t ar = m < M ? remap(m, row0, rows, level, mapmode == MAP_IN_CPG) : -1;
       cp_async16(sa + (uint32_t)(row * nw::AST + k2) * 8u, ar >= 0 ? A + ar * K + k0 + k2 : A, ar >= 0);
     }
     for (int e = tid; e < nw::BK * (nw::BN / 2); e += 256) {  // 16 rows x 8 pairs
@@ -191,7 +189,7 @@ __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, cons
   for (int mf = 0; mf < 2; ++mf) {
     const int64_t m = m0 + warp * 16 + mf * 8 + r8;
     if (m >= M) continue;
-    double *dst = C + remap(m, row0, level, mapmode == MAP_OUT_CPG) * ldc;
+    double *dst = C + remap(m, row0, rows, level, mapmode == MAP_OUT_CPG) * ldc;
 #pragma unroll
     for (int nf = 0; nf < NF; ++nf)
       *reinterpret_cast<double2 *>(dst + nf * 8 + 2 * c4) = make_double2(acc[mf][nf][0], acc[mf][nf][1]);
@@ -201,7 +199,7 @@ __global__ void __launch_bounds__(256) proj_narrow_kernel(int64_t M, int K, cons
 }  // namespace pj
 
 int launch_proj_narrow(int64_t M, int K, const double *A, const double *B, double *C, int ldc, int level,
-                       int mapmode, cudaStream_t s, int64_t row0) {
+                       int mapmode, cudaStream_t s, int64_t row0, const int64_t *rows) {
   if (K % pj::nw::BK) return bbfmm_set_error(BBFMM_ERR_ARG, "narrow projection: K must be a multiple of 16");
   if (M <= 0) return BBFMM_OK;
   static bool attr = false;  // 47 KB of dynamic shared memory
@@ -212,14 +210,15 @@ int launch_proj_narrow(int64_t M, int K, const double *A, const double *B, doubl
     attr = true;
   }
   pj::proj_narrow_kernel<<<(unsigned)((M + pj::nw::BM - 1) / pj::nw::BM), 256, pj::nw::SMEM_BYTES, s>>>(
-      M, K, A, B, C, ldc, level, mapmode, row0);
+      M, K, A, B, C, ldc, level, mapmode, row0, rows);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_narrow", __FILE__, __LINE__);
 }
 
 // Returns BBFMM_ERR_UNSUPPORTED (without recording an error) when the shape does not fit
 // the tile (K % 16, N % 256); the caller then uses the CUDA-core GEMM.
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
-                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0, int lda) {
+                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0, int lda,
+                     const int64_t *rows) {
   if (K % pj::BK || N % pj::BN) return BBFMM_ERR_UNSUPPORTED;
   if (M <= 0) return BBFMM_OK;
   static bool attr = false;
@@ -231,7 +230,7 @@ int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, 
   }
   dim3 grid((unsigned)((M + pj::BM - 1) / pj::BM), (unsigned)(N / pj::BN));
   pj::proj_dmma_kernel<<<grid, 256, pj::SMEM_BYTES, s>>>(M, K, N, A, B, cs, scale, C, level, mapmode, row0,
-                                                          lda > 0 ? lda : K);
+                                                          lda > 0 ? lda : K, rows);
   return bbfmm_set_cuda_error(cudaGetLastError(), "proj_dmma", __FILE__, __LINE__);
 }
 

@@ -196,7 +196,7 @@ int Solver<T>::alloc_partials() {
   int64_t need = 0;
   {  // every full M2L (FP64 DMMA or SIMT) may split its offsets
     for (int l = BBFMM_MINLEV; l <= maxlev; ++l) {
-      const bool tc = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
+      const bool tc = tc_m2l(l);
       if (tc) continue;
       const int g = tune.m2l_groups[l] > 0 ? tune.m2l_groups[l] : dmma_default_groups(l, nsets);
       const int64_t e = dmma_part_elems(l, nsets, g, r);
@@ -240,6 +240,8 @@ int Solver<T>::alloc_work() {
   }
   if (Mall) cudaFree(Mall);
   TRY(dalloc(&Mall, (size_t)tot));
+  // zeros where no pass writes (the cells outside a local solve's source region)
+  BBFMM_CUDA_OK(cudaMemset(Mall, 0, sizeof(T) * (size_t)tot));
   if (Lbuf) cudaFree(Lbuf);
   TRY(dalloc(&Lbuf, (size_t)nl * r));
   TRY(alloc_partials());
@@ -375,28 +377,33 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
     else TRY((launch_gather<T, float>(N, perm, nullptr, (const float *)q_dev, pos4, stream)));
     mark(ST_GATHER);
   }
-  // leaf level, slab by slab: P2M, up projection, M2M into the parents
+  // leaf level, slab by slab (a local solve: its source runs): P2M, up projection, M2M into
+  // the parents; the multipoles of the levels below m2l_first are not needed in a local solve
+  // (a local solve: its source cells in compact order, and no level below m2l_first)
+  const int lowest = local_solve ? m2l_first : BBFMM_MINLEV;
+  auto count = [&](int l) { return local_solve ? n_src[l] : cells(l); };
   T *Sl = S[maxlev & 1];
-  const int64_t nl = cells(maxlev), sl = leaf_slab();
+  const int64_t *lr = local_solve ? src_list[maxlev] : nullptr;
+  const int64_t nl = count(maxlev), sl = leaf_slab();
   for (int64_t a = 0; a < nl; a += sl) {
     const int64_t c = nl - a < sl ? nl - a : sl;
     // mixed mode: P2M also writes the BF16 split of S that the tensor-core up projection reads
     void *sp = proj_tc() && c <= Ssplit_rows ? Ssplit : nullptr;
-    TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream, nsets, a, c, sp));
+    TRY(launch_p2m<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Sl, stream, nsets, a, c, sp, lr ? lr + a : nullptr));
     mark(ST_P2M);
-    TRY(proj_up(c, Sl, maxlev, a, sp != nullptr));
+    TRY(proj_up(c, Sl, maxlev, a, sp != nullptr, lr ? lr + a : nullptr));
     mark(ST_PROJ_UP);
-    if (maxlev - 1 >= BBFMM_MINLEV) {
+    if (maxlev - 1 >= lowest) {
       TRY(launch_m2m<T>(n, Sl, S[(maxlev - 1) & 1], maxlev - 1, tb, stream, nsets, a / 8, c / 8));
       mark(ST_M2M);
     }
   }
-  for (int l = maxlev - 1; l >= BBFMM_MINLEV; --l) {
+  for (int l = maxlev - 1; l >= lowest; --l) {
     if (l < maxlev - 1) {
-      TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream, nsets));
+      TRY(launch_m2m<T>(n, S[(l + 1) & 1], S[l & 1], l, tb, stream, nsets, 0, count(l)));
       mark(ST_M2M);
     }
-    TRY(proj_up(cells(l), S[l & 1], l, 0));
+    TRY(proj_up(count(l), S[l & 1], l, 0, false, local_solve ? src_list[l] : nullptr));
     mark(ST_PROJ_UP);
   }
   if (mode == MODE_MIXED && tcops) {
@@ -408,58 +415,60 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
 
 // FP64 with r = 256 runs on the FP64 tensor path (DMMA); FP32 and r = 32 on CUDA cores.
 template <typename T>
-int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni) {
+int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni, const int *tile_list, int ntiles) {
   if (sizeof(T) == 8 && r == 256)
     return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
-                           (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level]);
+                           (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level], tile_list, ntiles);
   // the SIMT kernel writes all r outputs; in the rank mode (ni = rk()) the outputs i >= rank
   // of the zero-padded operators come out as zeros, so only other partial ranges are refused
   if (ni != r && ni != rk())
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
   const int g = tune.m2l_groups[level] > 0 ? tune.m2l_groups[level] : dmma_default_groups(level, nsets);
-  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets, g, Lpart, Lpart_elems);
+  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets, g, Lpart, Lpart_elems,
+                            tile_list, ntiles);
 }
 
 template <typename T>
 int Solver<T>::proj(int64_t Mrows, int K, int Ncols, const T *A, const T *B, const T *cs, T scale, T *C, int level,
-                    int mapmode, int64_t row0, int lda) {
+                    int mapmode, int64_t row0, int lda, const int64_t *rowlist) {
   if (sizeof(T) == 8) {
     int rc = launch_proj_dmma(Mrows, K, Ncols, (const double *)A, (const double *)B, (const double *)cs,
-                              (double)scale, (double *)C, level, mapmode, stream, row0, lda);
+                              (double)scale, (double *)C, level, mapmode, stream, row0, lda, rowlist);
     if (rc != BBFMM_ERR_UNSUPPORTED) return rc;
   }
-  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream, row0, 0, lda);
+  return launch_proj<T>(Mrows, K, Ncols, A, nullptr, B, cs, scale, C, level, mapmode, stream, row0, 0, lda, rowlist);
 }
 
 // Up projection of `rows` S rows (Morton cells row0 .. of `level`) into the level's M (cpg).
 // Mixed mode: components j < PROJ_LEAD in FP64, the rest as split-BF16 tensor-core products.
 template <typename T>
-int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit) {
+int Solver<T>::proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit,
+                       const int64_t *rowlist) {
   T *Mdst = Mall + Moff[level];
   if (!proj_tc() || rows > Ssplit_rows)
-    return proj(rows, n3, r, S_rows, Bup, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, row0);
+    return proj(rows, n3, r, S_rows, Bup, nullptr, (T)1, Mdst, level, MAP_OUT_CPG, row0, 0, rowlist);
   // the tensor cores write all r columns (zero for j < PROJ_LEAD: those operator rows are
   // zero in the split copy), then the FP64 pass overwrites the leading columns
   if (!presplit) TRY(tc_split_rows(rows, n3, (const double *)S_rows, 0, level, row0, Ssplit, stream));
-  TRY(launch_proj_up(tcproj, Ssplit, rows, (double *)Mdst, level, row0, stream));
+  TRY(launch_proj_up(tcproj, Ssplit, rows, (double *)Mdst, level, row0, stream, rowlist));
   return launch_proj_narrow(rows, n3, (const double *)S_rows, (const double *)Bup_lead, (double *)Mdst, r, level,
-                            MAP_OUT_CPG, stream, row0);
+                            MAP_OUT_CPG, stream, row0, rowlist);
 }
 
 // Down projection of the level's M2L output (Lbuf, cpg) into `rows` F rows (Morton cells
 // row0 .., assign). Mixed mode: one pass, the contraction over j < 16 in FP64 and the rest on
 // the tensor cores from L rows gathered into Morton order as split BF16.
 template <typename T>
-int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit) {
+int Solver<T>::proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit, const int64_t *rowlist) {
   // (1/L_l)^homogen in T, as the reference's POW(iL, homogen) (anotherFMMInteraction.c:7545-7549)
   const T iL = (T)1 / cell_length<T>(level, (T)L);
   const T scale = homogen == 1 ? iL : (T)std::pow(iL, (T)homogen);
   if (!proj_tc() || rows > Lsplit_rows)  // contraction over the effective rank (j < rk())
-    return proj(rows, rk(), n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0, r);
+    return proj(rows, rk(), n3, Lbuf, Bdn, kw, scale, F_rows, level, MAP_IN_CPG, row0, r, rowlist);
   // components j < 16 in FP64 and the rest as split-BF16 tensor-core products, one pass
-  if (!presplit) TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream, 16));
+  if (!presplit) TRY(tc_split_rows(rows, r, (const double *)Lbuf, 1, level, row0, Lsplit, stream, 16, rowlist));
   return launch_proj_down(tcproj, Lsplit, (const double *)Lbuf, rows, (double *)F_rows, level, row0,
-                          (const double *)kw, (double)scale, stream, rk());
+                          (const double *)kw, (double)scale, stream, rk(), rowlist);
 }
 
 // Leaf level after the M2L: per slab, the down projection of the M2L output (assign), L2L
@@ -468,19 +477,27 @@ template <typename T>
 int Solver<T>::leaf_down(bool field) {
   const Tables tb = tables();
   T *Fl = F[maxlev & 1];
-  const int64_t nl = cells(maxlev), sl = leaf_slab();
+  if (local_solve) {  // targets outside the region's leaf runs get zero
+    BBFMM_CUDA_OK(cudaMemsetAsync(phis, 0, sizeof(T) * (size_t)(N > 0 ? N : 1), stream));
+    if (field) BBFMM_CUDA_OK(cudaMemsetAsync(flds, 0, sizeof(T) * 3 * (size_t)(N > 0 ? N : 1), stream));
+  }
+  // slabs of the leaf level, or of a local solve's target leaves in compact order
+  const int64_t *lr = local_solve ? tgt_list[maxlev] : nullptr;
+  const int64_t nl = local_solve ? n_tgt[maxlev] : cells(maxlev), sl = leaf_slab();
   for (int64_t a = 0; a < nl; a += sl) {
     const int64_t c = nl - a < sl ? nl - a : sl;
-    if (slabbed()) {
-      TRY(proj_down(maxlev, c, a, Fl));
+    const int64_t *rl = lr ? lr + a : nullptr;
+    if (chunked()) {
+      TRY(proj_down(maxlev, c, a, Fl, false, rl));
       mark(ST_PROJ_DOWN);
       if (maxlev > m2l_first) {
         TRY(launch_l2l<T>(n, F[(maxlev - 1) & 1], Fl, maxlev - 1, tb, stream, nsets, a / 8, c / 8));
         mark(ST_L2L);
       }
     }
-    if (field) TRY(launch_l2p_field<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Fl, phis, flds, stream, nsets, a, c));
-    else TRY(launch_l2p<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Fl, phis, stream, nsets, a, c));
+    if (field)
+      TRY(launch_l2p_field<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Fl, phis, flds, stream, nsets, a, c, rl));
+    else TRY(launch_l2p<T>(n, pos4, leaf_start, maxlev, (T)L, tb, Fl, phis, stream, nsets, a, c, rl));
     mark(ST_L2P);
   }
   return BBFMM_OK;
@@ -491,8 +508,9 @@ int Solver<T>::interaction(int lo, int hi) {
   const Tables tb = tables();
   for (int l = lo; l <= hi; ++l) {
     TRY(m2l_post(l));
-    if (l > m2l_first && !(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
-      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream, nsets));
+    if (l > m2l_first && !(l == maxlev && chunked())) {  // chunked leaf level: in leaf_down
+      TRY(launch_l2l<T>(n, F[(l - 1) & 1], F[l & 1], l - 1, tb, stream, nsets, 0,
+                        local_solve ? n_tgt[l - 1] : cells(l - 1)));
       mark(ST_L2L);
     }
   }
@@ -505,7 +523,7 @@ int Solver<T>::m2l_post(int l) {
   {
     const T *Ml = Mall + Moff[l];
     bool presplit = false;  // the M2L kernel wrote the split rows of the down projection
-    const bool split = mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL && tune.m2l_kind[l] == 0;
+    const bool split = tc_m2l(l);
     if (split) {
       // FP64 leading block (i < lead_rows, j < lead) on the FP64 tensor path, then the
       // split-bf16 tensor-core kernel adds everything else into the same FP64 output; the
@@ -515,7 +533,7 @@ int Solver<T>::m2l_post(int l) {
         const bool masked = region_tiles[l] != nullptr;
         // whole level with mixed projections: the kernel also writes the split rows that the
         // down projection reads (and the FP64 output only where that pass reads it)
-        presplit = !masked && proj_tc() && cells(l) <= Lsplit_rows && !(l == maxlev && slabbed());
+        presplit = !masked && proj_tc() && cells(l) <= Lsplit_rows && !(l == maxlev && chunked());
         if (masked) BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * (size_t)cells(l) * r, stream));
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
                           tc_products, rk(), (const double *)Ml, (const double *)Ert, presplit ? Lsplit : nullptr,
@@ -531,14 +549,20 @@ int Solver<T>::m2l_post(int l) {
                           tc_products, rk()));
         mark(ST_M2L, 1);
       }
+    } else if (region_tiles4[l]) {
+      // a target region: only the tiles above active cells run (one offset group), the rest
+      // of the output is zero
+      BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * (size_t)cells(l) * r, stream));
+      TRY(m2l_fp(Ml, l, 0, rk(), rk(), region_tiles4[l], region_ntiles4[l]));
+      mark(ST_M2L, 1);
     } else {
       TRY(m2l_fp(Ml, l, 0, rk(), rk()));
       int g = tune.m2l_groups[l] > 0 ? tune.m2l_groups[l] : dmma_default_groups(l, nsets);
       if ((int64_t)g * cells(l) * r > Lpart_elems) g = 1;
       mark(ST_M2L, g > 1 ? 2 : 1);  // groups add the partial sum
     }
-    if (!(l == maxlev && slabbed())) {  // slabbed leaf level: in leaf_down
-      TRY(proj_down(l, cells(l), 0, F[l & 1], presplit));
+    if (!(l == maxlev && chunked())) {  // chunked leaf level: in leaf_down
+      TRY(proj_down(l, local_solve ? n_tgt[l] : cells(l), 0, F[l & 1], presplit, local_solve ? tgt_list[l] : nullptr));
       mark(ST_PROJ_DOWN);
     }
   }
@@ -583,11 +607,12 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   BBFMM_CUDA_OK(cudaEventCreate(&a));
   BBFMM_CUDA_OK(cudaEventCreate(&b));
   const T *Ml = Mall + Moff[level];
-  const bool split = mode == MODE_MIXED && tcops && level >= TC_MIN_LEVEL && tune.m2l_kind[level] == 0;
+  const bool split = tc_m2l(level);
   const bool fused = split && lead > 0 && tc_fuses_lead(tcops, tc_products, rk());
   // the launch as the solve makes it: a whole level with the mixed projections also writes
   // the split rows of the down projection (m2l_post)
-  const bool presplit = fused && proj_tc() && cells(level) <= Lsplit_rows && !(level == maxlev && slabbed());
+  const bool presplit = fused && proj_tc() && cells(level) <= Lsplit_rows && !(level == maxlev && chunked()) &&
+                        !region_tiles[level];
   int rc = BBFMM_OK;
   float tot[2] = {0.f, 0.f};
   for (int part = 0; part < (split ? 2 : 1) && rc == BBFMM_OK; ++part) {
@@ -629,49 +654,138 @@ template <typename T>
 int Solver<T>::set_target_region(int level, const unsigned char *active_host) {
   for (int l = 0; l <= 10; ++l) {
     if (region_tiles[l]) cudaFree(region_tiles[l]);
-    region_tiles[l] = nullptr;
-    region_ntiles[l] = 0;
+    if (region_tiles4[l]) cudaFree(region_tiles4[l]);
+    region_tiles[l] = region_tiles4[l] = nullptr;
+    region_ntiles[l] = region_ntiles4[l] = 0;
   }
   if (region_mask) cudaFree(region_mask);
   region_mask = nullptr;
   region_host.clear();
   region_level = -1;
   if (level >= 0) {
-    if (nsets != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "target regions are for single-set solvers");
     if (level < BBFMM_MINLEV || level > maxlev || !active_host)
-      return bbfmm_set_error(BBFMM_ERR_ARG, "target region: level in [2, maxlev] and a mask of 8^level bytes");
-    region_host.assign(active_host, active_host + pow8i(level));
-    TRY(dalloc(&region_mask, (size_t)pow8i(level)));
+      return bbfmm_set_error(BBFMM_ERR_ARG, "target region: level in [2, maxlev] and a mask of nsets 8^level bytes");
+    region_host.assign(active_host, active_host + cells(level));
+    TRY(dalloc(&region_mask, (size_t)cells(level)));
     BBFMM_CUDA_OK(cudaMemcpy(region_mask, region_host.data(), region_host.size(), cudaMemcpyHostToDevice));
     region_level = level;
     TRY(build_region_tiles());
   }
+  TRY(build_local());
   return pos4 ? build_near_work() : BBFMM_OK;
 }
 
-// Active two-box tiles of every tensor-core level above the region level: a tile (8 x 8 x 4
-// parent cells of one sibling class) is active when one of its cells descends from an active
-// region cell. Ids as the tensor-core M2L numbers its full grid: (box, then class fastest).
+template <typename T>
+int Solver<T>::set_m2l_first(int level) {
+  if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "first M2L level in [2, maxlev]");
+  m2l_first = level;
+  return build_local();
+}
+
+template <typename T>
+void Solver<T>::free_local() {
+  for (int l = 0; l <= 10; ++l) {
+    if (src_list[l]) cudaFree(src_list[l]);
+    if (tgt_list[l]) cudaFree(tgt_list[l]);
+    src_list[l] = tgt_list[l] = nullptr;
+    n_src[l] = n_tgt[l] = 0;
+  }
+}
+
+// Runs of the region cells (tgt) and of those with their neighbours (src) at region_level,
+// then their cells at every level from m2l_first down to the leaves as device row lists.
+template <typename T>
+int Solver<T>::build_local() {
+  free_local();
+  src_runs.clear();
+  tgt_runs.clear();
+  local_solve = region_level >= BBFMM_MINLEV && m2l_first > region_level;
+  if (!local_solve) return BBFMM_OK;
+  const int R = region_level, m = 1 << R;
+  const int64_t per = pow8i(R);
+  std::vector<unsigned char> near((size_t)per);
+  auto append = [](std::vector<std::pair<int64_t, int64_t>> &runs, int64_t row) {
+    if (!runs.empty() && runs.back().first + runs.back().second == row) ++runs.back().second;
+    else runs.push_back({row, 1});
+  };
+  for (int set = 0; set < nsets; ++set) {
+    const unsigned char *act = region_host.data() + (size_t)set * per;
+    std::fill(near.begin(), near.end(), (unsigned char)0);
+    for (int64_t i = 0; i < per; ++i) {
+      if (!act[i]) continue;
+      int x, y, z;
+      morton_to_grid(i, R, x, y, z);
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int u = x + dx, v = y + dy, w = z + dz;
+            if (u >= 0 && u < m && v >= 0 && v < m && w >= 0 && w < m) near[(size_t)grid_to_morton(u, v, w, R)] = 1;
+          }
+    }
+    for (int64_t i = 0; i < per; ++i) {
+      if (near[(size_t)i]) append(src_runs, set * per + i);
+      if (act[i]) append(tgt_runs, set * per + i);
+    }
+  }
+  auto upload = [&](const std::vector<std::pair<int64_t, int64_t>> &runs, int l, int64_t **dst, int64_t *count) -> int {
+    const int sh = 3 * (l - R);
+    std::vector<int64_t> rows;
+    for (const auto &ru : runs)
+      for (int64_t c = ru.first << sh; c < (ru.first + ru.second) << sh; ++c) rows.push_back(c);
+    *count = (int64_t)rows.size();
+    TRY(dalloc(dst, rows.size() > 0 ? rows.size() : 1));
+    if (!rows.empty()) BBFMM_CUDA_OK(cudaMemcpy(*dst, rows.data(), sizeof(int64_t) * rows.size(), cudaMemcpyHostToDevice));
+    return BBFMM_OK;
+  };
+  for (int l = m2l_first; l <= maxlev; ++l) {
+    TRY(upload(src_runs, l, &src_list[l], &n_src[l]));
+    TRY(upload(tgt_runs, l, &tgt_list[l], &n_tgt[l]));
+  }
+  return BBFMM_OK;
+}
+
+// Active tiles of every level above the region level, for the two M2L tilings: the two-box
+// tensor-core kernel's (a box of parent cells of one sibling class in one or more consecutive
+// sets, Tc2Box) and the 4 x 4 x 4 boxes of one class and set of the FP64 / FP32 kernels. A
+// tile is active when one of its cells descends from an active region cell. Ids as the
+// kernels number their full grids: (set group, box, then class fastest).
 template <typename T>
 int Solver<T>::build_region_tiles() {
-  for (int l = region_level + 1; l <= maxlev; ++l) {
-    if (l < TC_MIN_LEVEL) continue;
-    const int P = 1 << (l - 1), nbx = P / 8, nby = P / 8, nbz = P / 4, sh = l - 1 - region_level;
-    std::vector<int> ids;
-    for (int tb = 0; tb < nbx * nby * nbz; ++tb) {
-      const int bx0 = (tb % nbx) * 8, by0 = ((tb / nbx) % nby) * 8, bz0 = (tb / (nbx * nby)) * 4;
-      bool act = false;
-      for (int az = bz0 >> sh; az <= (bz0 + 3) >> sh && !act; ++az)
-        for (int ay = by0 >> sh; ay <= (by0 + 7) >> sh && !act; ++ay)
-          for (int ax = bx0 >> sh; ax <= (bx0 + 7) >> sh && !act; ++ax)
-            act = region_host[(size_t)grid_to_morton(ax, ay, az, region_level)] != 0;
-      if (act)
-        for (int c = 0; c < 8; ++c) ids.push_back(tb * 8 + c);
+  auto active_tiles = [&](int l, int lx, int ly, int lz, int spt, std::vector<int> &ids) {
+    const int P = 1 << (l - 1), nbx = P >> lx, nby = P >> ly, nbz = P >> lz, sh = l - 1 - region_level;
+    const int tpc = nbx * nby * nbz, ex = 1 << lx, ey = 1 << ly, ez = 1 << lz;
+    for (int sg = 0; sg * spt < nsets; ++sg) {
+      for (int tb = 0; tb < tpc; ++tb) {
+        const int bx0 = (tb % nbx) * ex, by0 = ((tb / nbx) % nby) * ey, bz0 = (tb / (nbx * nby)) * ez;
+        bool act = false;
+        for (int set = sg * spt; set < nsets && set < (sg + 1) * spt && !act; ++set) {
+          const unsigned char *mask = region_host.data() + (size_t)set * pow8i(region_level);
+          for (int az = bz0 >> sh; az <= (bz0 + ez - 1) >> sh && !act; ++az)
+            for (int ay = by0 >> sh; ay <= (by0 + ey - 1) >> sh && !act; ++ay)
+              for (int ax = bx0 >> sh; ax <= (bx0 + ex - 1) >> sh && !act; ++ax)
+                act = mask[(size_t)grid_to_morton(ax, ay, az, region_level)] != 0;
+        }
+        if (act)
+          for (int c = 0; c < 8; ++c) ids.push_back((sg * tpc + tb) * 8 + c);
+      }
     }
-    region_ntiles[l] = (int)ids.size();
-    TRY(dalloc(&region_tiles[l], ids.size() > 0 ? ids.size() : 1));
-    if (!ids.empty())
-      BBFMM_CUDA_OK(cudaMemcpy(region_tiles[l], ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+  };
+  auto upload = [&](const std::vector<int> &ids, int **dst, int *count) -> int {
+    *count = (int)ids.size();
+    TRY(dalloc(dst, ids.size() > 0 ? ids.size() : 1));
+    if (!ids.empty()) BBFMM_CUDA_OK(cudaMemcpy(*dst, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+    return BBFMM_OK;
+  };
+  for (int l = region_level + 1; l <= maxlev; ++l) {
+    std::vector<int> ids, ids4;
+    if (l >= TC2_MIN_LEVEL) {
+      const Tc2Box g = tc2_box(l);
+      active_tiles(l, g.lx, g.ly, g.lz, 1 << (8 - g.lb()), ids);
+      TRY(upload(ids, &region_tiles[l], &region_ntiles[l]));
+    }
+    const int lb4 = l - 1 < 2 ? l - 1 : 2;  // boxes of min(P, 4) cells per axis
+    active_tiles(l, lb4, lb4, lb4, 1, ids4);
+    TRY(upload(ids4, &region_tiles4[l], &region_ntiles4[l]));
   }
   return BBFMM_OK;
 }
@@ -744,7 +858,7 @@ int Solver<T>::autotune(const void *q_dev, int io_double) {
     }
     // candidates: (kind, offset groups); only the mixed mode has the tensor-core kind
     std::vector<std::pair<int, int>> cand;
-    if (mode == MODE_MIXED && tcops && l >= TC_MIN_LEVEL) cand.push_back({0, 0});
+    if (tc_level(l)) cand.push_back({0, 0});
     // the DMMA and the SIMT M2L both split their offsets over groups
     for (int g : {1, 3, 7, 21})
       if (dmma_part_elems(l, nsets, g, r) * (int64_t)sizeof(T) <= ((int64_t)1 << 30)) cand.push_back({1, g});
@@ -843,7 +957,7 @@ int Solver<T>::copy_m2l_morton(int level, T *host_out) {
   if (nsets != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L copies are per single-set solver");
   if (!pos4 || !Lbuf) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
   const T *Ml = Mall + Moff[level];
-  const bool split = mode == MODE_MIXED && tcops && level >= TC_MIN_LEVEL && tune.m2l_kind[level] == 0;
+  const bool split = tc_m2l(level);
   if (split) {
     const bool fused = lead > 0 && tc_fuses_lead(tcops, tc_products, rk());
     if (lead > 0 && !fused) TRY(m2l_fp(Ml, level, 0, lead, lead_rows));
@@ -866,8 +980,11 @@ int Solver<T>::copy_m2l_morton(int level, T *host_out) {
 
 template <typename T>
 void Solver<T>::release() {
-  for (int l = 0; l <= 10; ++l)
+  for (int l = 0; l <= 10; ++l) {
     if (region_tiles[l]) cudaFree(region_tiles[l]);
+    if (region_tiles4[l]) cudaFree(region_tiles4[l]);
+  }
+  free_local();
   if (region_mask) cudaFree(region_mask);
   void *ptrs[] = {offs, perm, leaf_start, near_work, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
                   phis, flds, Ssplit, Lsplit, io_q, io_phi};
@@ -1039,9 +1156,7 @@ int bbfmm_b200_set_first_m2l_level(bbfmm_b200_solver *h, int level) {
   if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
   const int maxlev = h->f ? h->f->maxlev : h->d->maxlev;
   if (level < BBFMM_MINLEV || level > maxlev) return bbfmm_set_error(BBFMM_ERR_ARG, "first M2L level in [2, maxlev]");
-  if (h->f) h->f->m2l_first = level;
-  else h->d->m2l_first = level;
-  return BBFMM_OK;
+  return h->f ? h->f->set_m2l_first(level) : h->d->set_m2l_first(level);
 }
 
 int bbfmm_b200_copy_m2l(bbfmm_b200_solver *h, int level, void *host_out) {

@@ -27,12 +27,12 @@ enum Stage {
 // level can be processed in slabs; count < 0 means every cell from `first` on.
 template <typename T>
 int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf_start, cudaStream_t s);
-template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, void *Ssplit = nullptr);
+template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, void *Ssplit = nullptr, const int64_t *rows = nullptr);
 template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
-template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *phi, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, const int64_t *rows = nullptr);
 // rows are a slab of the level starting at cell row0 (the cpg side is indexed by level cell)
-template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int ldc = 0, int lda = 0);
+template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int ldc = 0, int lda = 0, const int64_t *rows = nullptr);
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
@@ -51,21 +51,22 @@ int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_
                 int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s,
                 const unsigned char *mask = nullptr, int mask_level = 0);
 int near_status(int clear);
-template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
+template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, const int64_t *rows = nullptr);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
-template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0);
+template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0, const int *tile_list = nullptr, int ntiles = 0);
 void build_offset_table(int *out);
 constexpr int DMMA_PARTS = 21;  // most offset groups of the FP64 M2L (189 = 9 x 21)
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
                     const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets = 1,
-                    int ngroups = 0);
+                    int ngroups = 0, const int *tile_list = nullptr, int ntiles = 0);
 int dmma_default_groups(int level, int nsets);
 int64_t dmma_part_elems(int level, int nsets, int groups, int r);
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
-                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int lda = 0);
+                     double *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int lda = 0,
+                     const int64_t *rows = nullptr);
 // C[out(m)][0:32] = sum_k A[m][k] B[k][0:32] on the FP64 tensor path (B: K x 32 contiguous).
 int launch_proj_narrow(int64_t M, int K, const double *A, const double *B, double *C, int ldc, int level,
-                       int mapmode, cudaStream_t s, int64_t row0);
+                       int mapmode, cudaStream_t s, int64_t row0, const int64_t *rows = nullptr);
 int launch_direct_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *out, cudaStream_t s);
 int launch_direct_field_fp64(int N, const double *xyz, const double *q, int nt, const int *targets, double *pot,
                              double *fld, cudaStream_t s);
@@ -95,6 +96,8 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
                   const double *Mlead = nullptr, const double *Erow = nullptr, void *Lsplit = nullptr,
                   const int *tile_list = nullptr, int ntiles = 0);
 bool tc_fuses_lead(const void *ops, int nprod, int rank);
+// Whether launch_m2l_tc runs the two-box kernel (the adaptive product map at full split rows).
+inline bool tc_two_box(int nprod, int rank) { return nprod == 0 && (rank <= 0 || rank >= TC_SPLIT_ROWS); }
 int tc_status(int clear);
 int tc_wait_probe(unsigned limit, int code);
 // Tensor-core projections (m2l_tc.cu): the components j >= lead of the up projection and the
@@ -102,11 +105,40 @@ int tc_wait_probe(unsigned limit, int code);
 int tc_prepare_projections(int n3, int r, const double *Bup, const double *Bdn, int lead, void **out, cudaStream_t s);
 void tc_free_projections(void *p);
 int launch_proj_down(const void *p, const void *Asplit, const double *Lfp, int64_t rows, double *F, int level,
-                     int64_t row0, const double *cs, double scale, cudaStream_t s, int rank = 0);
-int launch_proj_up(const void *p, const void *Asplit, int64_t rows, double *M, int level, int64_t row0, cudaStream_t s);
+                     int64_t row0, const double *cs, double scale, cudaStream_t s, int rank = 0,
+                     const int64_t *rowlist = nullptr);
+int launch_proj_up(const void *p, const void *Asplit, int64_t rows, double *M, int level, int64_t row0, cudaStream_t s,
+                   const int64_t *rowlist = nullptr);
+// rowlist (optional): the pass's Morton rows, row t being rowlist[t] instead of row0 + t
 int tc_split_rows(int64_t rows, int K, const double *src, int gather, int level, int64_t row0, void *dst,
-                  cudaStream_t s, int zlead = 0);
-constexpr int TC_MIN_LEVEL = 4;  // the tensor-core M2L tiles need a parent grid of >= 8 per axis
+                  cudaStream_t s, int zlead = 0, const int64_t *rowlist = nullptr);
+constexpr int TC_MIN_LEVEL = 4;   // the one-box tensor-core M2L needs a parent grid of >= 8 per axis
+constexpr int TC2_MIN_LEVEL = 2;  // the two-box kernel tiles every level (stacked sets below 4)
+
+// Target box of the two-box tensor-core M2L at one level: 2^lx x 2^ly x 2^lz parent cells of
+// one sibling class grid in each of 2^(8 - lb()) consecutive stacked sets, 256 target rows in
+// all, x fastest, then y, z, set. Level >= 4: an 8 x 8 x 4 box of one set; level 3: the whole
+// 4 x 4 x 4 grid of four sets; level 2: the whole 2 x 2 x 2 grid of 32 sets.
+struct Tc2Box {
+  int lx, ly, lz;
+  __host__ __device__ int lb() const { return lx + ly + lz; }
+  __host__ __device__ void pos(int row, int &x, int &y, int &z, int &set) const {
+    x = row & ((1 << lx) - 1);
+    y = (row >> lx) & ((1 << ly) - 1);
+    z = (row >> (lx + ly)) & ((1 << lz) - 1);
+    set = row >> lb();
+  }
+};
+__host__ __device__ inline Tc2Box tc2_box(int level) {
+  const int p = level - 1;  // log2 of the class grid's cells per axis
+  return Tc2Box{p < 3 ? p : 3, p < 3 ? p : 3, p < 2 ? p : 2};
+}
+// Tiles of the two-box kernel over a whole level: 8 classes x set groups x boxes per class grid.
+inline int64_t tc2_tiles(int level, int nsets) {
+  const Tc2Box g = tc2_box(level);
+  const int P = 1 << (level - 1), spt = 1 << (8 - g.lb());
+  return 8 * (int64_t)((nsets + spt - 1) / spt) * (P >> g.lx) * (P >> g.ly) * (P >> g.lz);
+}
 
 // Launch choices of one solver, per level (index = level): what the autotuner sets.
 struct Tuning {
@@ -161,19 +193,34 @@ struct Solver {
   int *perm = nullptr, *leaf_start = nullptr;
   void *near_work = nullptr;  // near-field work list (near_work_build) for near_threads
   int near_items = 0, near_threads = 0;
-  // Target region (bbfmm_b200_set_target_region, one set): results are wanted only at the
+  // Target region (bbfmm_b200_set_target_region): results are wanted only at the
   // particles inside the active cells of region_level. The near field skips the other targets,
   // and the tensor-core M2L of every level above region_level runs only on the two-box tiles
   // that hold descendants of active cells (the rest of that level's output is zero).
   int region_level = -1;                       // < 0: every particle
-  unsigned char *region_mask = nullptr;        // device, 8^region_level bytes
+  unsigned char *region_mask = nullptr;        // device, nsets 8^region_level bytes (stacked numbering)
   std::vector<unsigned char> region_host;
   int *region_tiles[11] = {};                  // per level: active two-box tile ids (device)
   int region_ntiles[11] = {};
+  int *region_tiles4[11] = {};                 // per level: active 4 x 4 x 4 tiles of the FP64 / FP32 M2L
+  int region_ntiles4[11] = {};
   // First level whose M2L runs (bbfmm_b200_set_first_m2l_level): the local expansions start
   // there (no L2L from the level above), so the solve gathers, for every target, only the
   // sources inside the neighbourhood of its ancestor one level up.
   int m2l_first = BBFMM_MINLEV;
+  // Local solve (a target region and m2l_first > region_level): every source that a target of
+  // the region gathers lies in an active cell of region_level or in one of its neighbours, so
+  // the passes at the levels >= m2l_first run only over those cells' descendants -- the upward
+  // ones over src_runs (active cells and their neighbours), the downward ones over tgt_runs
+  // (active cells) -- and the levels below m2l_first are skipped. Runs: Morton rows [a, a + c)
+  // of region_level over the stacked sets, neighbouring rows merged. Targets outside the
+  // region get zero.
+  bool local_solve = false;
+  std::vector<std::pair<int64_t, int64_t>> src_runs, tgt_runs;
+  // the runs' cells at each level >= m2l_first, in order (device lists): the passes of a local
+  // solve keep S and F rows in this compact order, the children of compact row p at 8p .. 8p + 7
+  int64_t *src_list[11] = {}, *tgt_list[11] = {};
+  int64_t n_src[11] = {}, n_tgt[11] = {};
   T *pos4 = nullptr;
   // expansions
   T *S[2] = {nullptr, nullptr};
@@ -215,10 +262,25 @@ struct Solver {
   int near(T *pot, T *fld);                      // P2P (add) into sorted pot (and field)
   int build_near_work();                         // the work list for tune.p2p_threads
   int set_target_region(int level, const unsigned char *active_host);  // level < 0 clears
+  int set_m2l_first(int level);                                        // m2l_first, then the runs
+  int build_local();                                                   // runs and row lists
+  void free_local();
+  bool chunked() const { return slabbed() || local_solve; }  // leaf passes run per leaf chunk
   int build_region_tiles();                      // region_tiles from region_host (after particles/alloc)
   bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
-  int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false);  // S rows -> Mall (cpg)
-  int proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit = false);    // Lbuf -> F rows (Morton, assign)
+  // level l has a tensor-core M2L under the current product map and rank (mixed mode), and
+  // the solve runs it there (the level's tuning keeps the default kind)
+  bool tc_level(int l) const {
+    return mode == MODE_MIXED && tcops &&
+           (l >= TC_MIN_LEVEL || (l >= TC2_MIN_LEVEL && tc_two_box(tc_products, rk())));
+  }
+  bool tc_m2l(int l) const { return tc_level(l) && tune.m2l_kind[l] == 0; }
+  // S rows -> Mall (cpg); F rows <- Lbuf (Morton, assign). Row t is cell row0 + t, or
+  // rowlist[t] when a row list is given.
+  int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false,
+              const int64_t *rowlist = nullptr);
+  int proj_down(int level, int64_t rows, int64_t row0, T *F_rows, bool presplit = false,
+                const int64_t *rowlist = nullptr);
   // Times the launch choices of every level's M2L and of the near field on this solver's
   // own tree (after an upward pass with q_dev) and keeps the fastest; results are cached per
   // (mode, n, level, target tiles) and (mode, particles, leaves) for later solvers.
@@ -234,9 +296,10 @@ struct Solver {
   int copy_m2l_morton(int level, T *host_out);         // level's M2L output, recomputed, Morton order
   void mark(int stage, int launches = 1);
   int time_m2l(int level, int reps, float *ms);
-  int m2l_fp(const T *Ml, int level, int j0, int j1, int ni);  // FP64 (DMMA) / FP32 (SIMT) M2L part
+  int m2l_fp(const T *Ml, int level, int j0, int j1, int ni,  // FP64 (DMMA) / FP32 (SIMT) M2L part
+             const int *tile_list = nullptr, int ntiles = 0);
   int proj(int64_t M, int K, int N, const T *A, const T *B, const T *cs, T scale, T *C, int level, int mapmode,
-           int64_t row0 = 0, int lda = 0);
+           int64_t row0 = 0, int lda = 0, const int64_t *rowlist = nullptr);
   void release();
 };
 

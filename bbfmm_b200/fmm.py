@@ -265,20 +265,42 @@ def morton_to_grid(m, level: int):
     return ix, iy, iz
 
 
-def leaf_of_particles(xyz, L: float, level: int):
-    """Morton leaf of every particle at `level` (the library's own leaf assignment), and the
-    particle count of every leaf."""
-    x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+def leaf_of_particles(xyz, L: float, level: int, fp32: bool = False):
+    """Morton leaf of every particle at `level` (the library's own leaf assignment, from FP32
+    positions as an FP32 solver has them when fp32), and the particle count of every leaf."""
+    x = np.ascontiguousarray(np.asarray(xyz, np.float32 if fp32 else np.float64).reshape(-1, 3))
     N = x.shape[0]
     perm = np.zeros(N, np.int32)
     ls = np.zeros(8 ** level + 1, np.int32)
-    _lib.check(_lib.lib().bbfmm_b200_sort_particles(N, 0, _ptr(x), float(L), level,
+    _lib.check(_lib.lib().bbfmm_b200_sort_particles(N, int(fp32), _ptr(x), float(L), level,
                                                     perm.ctypes.data_as(C.POINTER(C.c_int)),
                                                     ls.ctypes.data_as(C.POINTER(C.c_int))))
     counts = np.diff(ls)
     leaf = np.empty(N, np.int64)
     leaf[perm] = np.repeat(np.arange(8 ** level, dtype=np.int64), counts)
     return leaf, counts
+
+
+def refinement_plan(xyz, L: float, depth: int, cap: int):
+    """Heavy leaves of a set at `depth` (more than cap particles; a Morton-order mask of 8^depth
+    cells), the particles inside their 3 x 3 x 3 neighbourhoods (`sel`, indices into xyz) and,
+    among those, the ones in heavy leaves (`keep`, a mask over sel)."""
+    leaf, counts = leaf_of_particles(xyz, L, depth)
+    heavy = counts > cap
+    if not heavy.any():
+        return heavy, np.zeros(0, np.int64), np.zeros(0, bool)
+    m = 2 ** depth
+    gx, gy, gz = morton_to_grid(np.arange(8 ** depth), depth)
+    g = np.zeros((m + 2, m + 2, m + 2), bool)
+    g[gx + 1, gy + 1, gz + 1] = heavy
+    d = np.zeros_like(g)
+    for a in (-1, 0, 1):
+        for b in (-1, 0, 1):
+            for c in (-1, 0, 1):
+                d |= np.roll(np.roll(np.roll(g, a, 0), b, 1), c, 2)
+    near_region = d[gx + 1, gy + 1, gz + 1]  # Morton order
+    sel = np.nonzero(near_region[leaf])[0]
+    return heavy, sel, heavy[leaf[sel]]
 
 
 class AdaptiveSolver:
@@ -321,8 +343,7 @@ class AdaptiveSolver:
         x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
         self.N = x.shape[0]
         self.coarse.set_particles(x)
-        leaf, counts = leaf_of_particles(x, self.L, self.Dc)
-        heavy = counts > self.cap
+        heavy, sel, keep = refinement_plan(x, self.L, self.Dc, self.cap)
         self.heavy_leaves = int(heavy.sum())
         if self.fine is not None:
             self.fine.close()
@@ -331,19 +352,6 @@ class AdaptiveSolver:
             self.coarse.set_target_region(-1)
             return
         self.coarse.set_target_region(self.Dc, ~heavy)
-        # particles of the heavy leaves' 3 x 3 x 3 neighbourhoods
-        m = 2 ** self.Dc
-        gx, gy, gz = morton_to_grid(np.arange(8 ** self.Dc), self.Dc)
-        g = np.zeros((m + 2, m + 2, m + 2), bool)
-        g[gx + 1, gy + 1, gz + 1] = heavy
-        d = np.zeros_like(g)
-        for a in (-1, 0, 1):
-            for b in (-1, 0, 1):
-                for c in (-1, 0, 1):
-                    d |= np.roll(np.roll(np.roll(g, a, 0), b, 1), c, 2)
-        near_region = d[gx + 1, gy + 1, gz + 1]  # Morton order
-        sel = np.nonzero(near_region[leaf])[0]
-        keep = heavy[leaf[sel]]
         self.fine = Solver(self.n, self.Df, self.L, mode=self.mode, device=self.device, **self.kw)
         self.fine.set_particles(x[sel])
         self.fine.set_first_m2l_level(self.Dc + 1)
@@ -367,6 +375,82 @@ def batch_depth(N: int, per_leaf: float = 32.0) -> int:
     """Leaf depth for about `per_leaf` particles per leaf: round(log8(N / per_leaf)), >= 2."""
     return max(2, int(round(math.log(max(N, 1) / per_leaf, 8)))) if N > 0 else 2
 
+
+
+class AdaptiveBatch:
+    """Two-level adaptive refinement of a batch (AdaptiveSolver for many sets): a coarse Batch of
+    the sets as given, whose near field skips the heavy leaves (more than `cap` particles), and a
+    refined Batch of each set with heavy leaves -- the particles of their neighbourhoods, at the
+    set's depth + `refine`, local expansions starting one level below the coarse leaves -- whose
+    results are added at the heavy leaves' particles. Charges and results as for Batch."""
+
+    def __init__(self, sets, mode: str = "mixed", cap: int = 256, refine: int = 2, L: float = 1.0, **kw):
+        import torch
+        self.torch = torch
+        self.coarse = Batch(sets, mode=mode, L=L, **kw)
+        self.offsets = self.coarse.offsets
+        self.N = self.coarse.N
+        light, refined, heavy_masks, sel_all, keep_local, keep_global = [], [], [], [], [], []
+        rbase = 0
+        self.heavy_leaves = 0
+        for s, (x, n, lev) in enumerate(sets):
+            x = np.asarray(x, np.float64).reshape(-1, 3)
+            heavy, sel, keep = refinement_plan(x, L, lev, cap)
+            light.append(~heavy)
+            if heavy.any() and lev + refine <= 10:
+                self.heavy_leaves += int(heavy.sum())
+                refined.append((x[sel], n, lev + refine))
+                heavy_masks.append(heavy)
+                sel_all.append(self.offsets[s] + sel)
+                keep_global.append(self.offsets[s] + sel[keep])
+                keep_local.append(rbase + np.nonzero(keep)[0])
+                rbase += sel.size
+            else:
+                light[-1] = np.ones_like(heavy)
+        self.coarse.set_target_regions(0, np.concatenate(light))
+        self.refined = None
+        self.refined_particles = rbase
+        if refined:
+            self.refined = Batch(refined, mode=mode, L=L, **kw)
+            self.refined.set_target_regions(refine, np.concatenate(heavy_masks), first_m2l=True)
+            dev = f"cuda:{self.coarse.device}"
+            self.sel = torch.as_tensor(np.concatenate(sel_all), device=dev)
+            self.keep_local = torch.as_tensor(np.concatenate(keep_local), device=dev)
+            self.keep_global = torch.as_tensor(np.concatenate(keep_global), device=dev)
+            # fixed buffers for the refined batch, whose captured graph is tied to its pointers
+            self.q_ref = torch.empty(rbase, dtype=self.coarse.dtype, device=dev)
+            self.phi_ref = torch.empty_like(self.q_ref)
+
+    def close(self):
+        for b in (self.coarse, self.refined):
+            if b is not None:
+                b.close()
+
+    def autotune(self, q):
+        self.coarse.autotune(q)
+        if self.refined is not None:
+            torch = self.torch
+            torch.index_select(q.to(self.q_ref.dtype), 0, self.sel, out=self.q_ref)
+            self.refined.autotune(self.q_ref)
+
+    def solve(self, q, out=None, graph: bool = True):
+        """As Batch.solve. The coarse and the refined batch run at the same time on their own
+        streams (both read charges gathered before either starts); the refined results are
+        added on the caller's stream once both are done."""
+        torch = self.torch
+        if self.refined is None:
+            return self.coarse.solve(q, out=out, graph=graph)
+        _check_count("q", q.numel(), self.N)
+        q = q.to(device=f"cuda:{self.coarse.device}", dtype=self.coarse.dtype).contiguous()
+        if out is None:
+            out = torch.empty_like(q)
+        torch.index_select(q, 0, self.sel, out=self.q_ref)
+        done = [self.coarse._submit(q, out, graph), self.refined._submit(self.q_ref, self.phi_ref, graph)]
+        caller = torch.cuda.current_stream(q.device)
+        for d in done:
+            caller.wait_event(d)
+        out.index_add_(0, self.keep_global, self.phi_ref.index_select(0, self.keep_local))
+        return out
 
 def set_cost(N: int, n: int, maxlev: int) -> float:
     """Model of one set's device work: M2L flops 2 r^2 x (about 189 8^l pairs per level) plus
@@ -407,6 +491,7 @@ class Batch:
         counts = np.array([len(x) for x, _, _ in sets], dtype=np.int32)
         ns = np.array([n for _, n, _ in sets], dtype=np.int32)
         levs = np.array([lv for _, _, lv in sets], dtype=np.int32)
+        self.depths = levs.tolist()
         self.offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         self.N = int(self.offsets[-1])
         xyz = np.ascontiguousarray(np.concatenate([np.asarray(x, np_dtype).reshape(-1, 3) for x, _, _ in sets])
@@ -442,6 +527,17 @@ class Batch:
     def stream(self):
         return _lib.lib().bbfmm_b200_batch_stream(self.h)
 
+    def set_target_regions(self, levels_up: int, active=None, first_m2l: bool = False):
+        """Target regions of every set at level depth_s - levels_up: `active` concatenates, in
+        set order, each set's mask over the 8^(depth_s - levels_up) cells of that level (None
+        clears); first_m2l also starts each set's local expansions one level below it."""
+        if active is None:
+            _lib.check(_lib.lib().bbfmm_b200_batch_set_target_regions(self.h, 0, None, 0))
+            return
+        a = np.ascontiguousarray(np.asarray(active).astype(np.uint8).reshape(-1))
+        _check_count("active", a.size, int(sum(8 ** (lv - levels_up) for lv in self.depths)))
+        _lib.check(_lib.lib().bbfmm_b200_batch_set_target_regions(self.h, int(levels_up), _ptr(a), int(first_m2l)))
+
     def _order(self, q):
         torch = self.torch
         caller = torch.cuda.current_stream(q.device)
@@ -451,6 +547,18 @@ class Batch:
         mine.wait_event(ev)
         return caller, mine
 
+    def _submit(self, q, out, graph: bool):
+        """Launches the solve of q (on this device, this dtype, contiguous) into out on the
+        batch's stream after the work already queued on the caller's stream; returns the event
+        that marks its end, which the caller's stream does not wait for."""
+        _check_out(out, q)
+        _, mine = self._order(q)
+        _lib.check(_lib.lib().bbfmm_b200_batch_solve(self.h, C.c_void_p(q.data_ptr()), C.c_void_p(out.data_ptr()),
+                                                      int(graph)))
+        done = self.torch.cuda.Event()
+        done.record(mine)
+        return done
+
     def solve(self, q, out=None, graph: bool = True):
         """q: CUDA tensor (N_total,) -> q_i * phi_i of every set (same layout)."""
         torch = self.torch
@@ -458,13 +566,8 @@ class Batch:
         q = q.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
         if out is None:
             out = torch.empty_like(q)
-        _check_out(out, q)
-        caller, mine = self._order(q)
-        _lib.check(_lib.lib().bbfmm_b200_batch_solve(self.h, C.c_void_p(q.data_ptr()), C.c_void_p(out.data_ptr()),
-                                                      int(graph)))
-        done = torch.cuda.Event()
-        done.record(mine)
-        caller.wait_event(done)
+        done = self._submit(q, out, graph)
+        torch.cuda.current_stream(q.device).wait_event(done)
         return out
 
     def set_tc_products(self, nprod: int):

@@ -613,13 +613,14 @@ def batch_sets(seed=5, nsets=256):
     return sets, q
 
 
-def run_batch_256(args):
+def run_batch_256(args, adaptive=False):
     """256 uneven sets in one batch (stacked per (n, depth), one launch per pass per group,
     the groups as parallel branches of one CUDA graph), after the autotuner; per-set error
-    against the FP64 direct sum on 512 sampled targets per set."""
+    against the FP64 direct sum on 512 sampled targets per set. adaptive: the same sets through
+    AdaptiveBatch (leaves of more than 256 particles refined by two levels in a second batch)."""
     import torch
     import torch.distributed as dist
-    from bbfmm_b200 import Batch, set_cost, shard_sets
+    from bbfmm_b200 import AdaptiveBatch, Batch, set_cost, shard_sets
     from bbfmm_b200.fmm import direct
     mode = args.mode
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -637,15 +638,20 @@ def run_batch_256(args):
     sets = [all_sets[i] for i in mine]
     q = np.concatenate([all_q[offs_all[i]:offs_all[i + 1]] for i in mine]) if mine else np.zeros(0)
     t0 = time.perf_counter()
-    b = Batch(sets, mode=mode, device=local)
+    b = AdaptiveBatch(sets, mode=mode, cap=256, device=local) if adaptive else Batch(sets, mode=mode, device=local)
     t_setup = time.perf_counter() - t0
     dt = torch.float32 if mode == "s" else torch.float64
     qd = torch.as_tensor(q, dtype=dt, device="cuda")
     out = torch.empty_like(qd)
     t0 = time.perf_counter()
-    groups = b.autotune(qd)
+    if adaptive:
+        b.autotune(qd)
+        groups = b.coarse.groups() + (b.refined.groups() if b.refined is not None else [])
+    else:
+        groups = b.autotune(qd)
     t_tune = time.perf_counter() - t0
-    stream = torch.cuda.ExternalStream(b.stream)
+    # the adaptive batch's solve spans two batch streams and the caller's: time on the caller's
+    stream = None if adaptive else torch.cuda.ExternalStream(b.stream)
     for _ in range(args.warmup):
         b.solve(qd, out=out, graph=True)
     def barrier():
@@ -664,7 +670,12 @@ def run_batch_256(args):
         t_graph = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=True), args.steps, stream))
     barrier()
     t_eager = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=False), args.steps, stream))
-    group_ms = [b.group_stage_times(qd, g) for g in range(len(groups))]
+    if adaptive:  # the coarse groups, then the refined ones on the charges the last solve gathered
+        group_ms = [b.coarse.group_stage_times(qd, g) for g in range(len(b.coarse.groups()))]
+        if b.refined is not None:
+            group_ms += [b.refined.group_stage_times(b.q_ref, g) for g in range(len(b.refined.groups()))]
+    else:
+        group_ms = [b.group_stage_times(qd, g) for g in range(len(groups))]
     phi = out.double().cpu().numpy()
     # per-set error on 512 sampled targets
     rng = np.random.default_rng(77)
@@ -712,7 +723,8 @@ def run_batch_256(args):
             cpu = {"value": (n_ref / t_ref) / Ntot, "unit": "batch/s", "cores": cores, "kind": kind,
                    "sample": f"the reference CPU code on {len(kinds)} of the sets ({n_ref} particles, {t_ref:.2f} s), "
                              f"scaled to the batch's {Ntot} particles"}
-    line = {"metric": "batched solves of 256 uneven sets (N log-uniform 4,096..262,144, n in {4,8})",
+    line = {"metric": "batched solves of 256 uneven sets (N log-uniform 4,096..262,144, n in {4,8})"
+                      + (", two-level adaptive" if adaptive else ""),
             "value": 1.0 / t_graph, "unit": "batch/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_graph * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": {"mixed": "bf16x3+f64", "d": "f64", "s": "f32"}[mode],
@@ -721,7 +733,10 @@ def run_batch_256(args):
                        "particles": Ntot, "mode": mode, "parallelism": f"sets sharded over {world} GPU(s)",
                        "groups": [{k: g[k] for k in ("n", "maxlev", "sets", "particles", "p2p_threads",
                                                       "m2l_kind", "m2l_groups")} for g in groups]},
-            "particles_per_s": Ntot / t_graph, "eager_ms": t_eager * 1e3, "graph_nodes": b.graph_nodes,
+            "particles_per_s": Ntot / t_graph, "eager_ms": t_eager * 1e3,
+            "graph_nodes": None if adaptive else b.graph_nodes,
+            "adaptive": {"heavy_leaves": b.heavy_leaves, "refined_particles": b.refined_particles,
+                         "cap": 256, "refine_levels": 2} if adaptive else None,
             "group_stage_ms": group_ms,
             "setup_s": t_setup, "autotune_s": t_tune,
             "err_vs_fp64_direct": {"median": float(np.median(errs)), "max": float(errs.max()),
@@ -854,7 +869,8 @@ def main():
     ap.add_argument("--maxlev", type=int, default=MAXLEV)
     ap.add_argument("--workload", default="uniform-4m",
                     choices=["uniform-4m", "uniform-4m-variants", "uniform-32k", "gradient-1m", "batch-256",
-                             "clustered-16m", "clustered-16m-adaptive", "near-field", "stages"],
+                             "clustered-16m", "clustered-16m-adaptive", "batch-256-adaptive", "near-field",
+                             "stages"],
                     help="uniform-4m: the headline line; the others measure further configurations")
     ap.add_argument("--layout", default="uniform", choices=["uniform", "clustered"],
                     help="near-field / stages workloads: particle layout")
@@ -871,6 +887,8 @@ def main():
         return run_batch_256(args)
     if args.workload == "clustered-16m":
         return run_clustered_16m(args)
+    if args.workload == "batch-256-adaptive":
+        return run_batch_256(args, adaptive=True)
     if args.workload == "clustered-16m-adaptive":
         return run_clustered_16m_adaptive(args)
     if args.workload == "near-field":

@@ -263,13 +263,15 @@ BBFMM_B200_API int bbfmm_b200_set_kernel(bbfmm_b200_solver *s, int kernel);
  * anotherBuildFMMHierachy.c:44-55). A target region marks the cells of one level whose
  * particles' results are wanted: active[m] != 0 for the Morton cells m of `level` (8^level
  * bytes, host; level < 0 clears). The solve then computes the near field only for particles
- * in active cells (others keep what the far field gives them), and the tensor-core M2L of every
- * level above `level` (MIXED, two-box kernel) runs only on the tiles holding descendants of
- * active cells. The first M2L level (default 2) starts the local expansions at that level:
- * with first = l + 1 the solve gathers, for every target, only the sources inside the
- * 3 x 3 x 3 neighbourhood of its level-l ancestor -- exactly the near field of a level-l
- * leaf, computed by a deeper FMM. bbfmm_b200.AdaptiveSolver composes a coarse and a refined
- * solver this way. Single-set solvers only. */
+ * in active cells (others keep what the far field gives them), and the M2L of every level
+ * above `level` runs only on the tiles holding descendants of active cells. The first M2L
+ * level (default 2) starts the local expansions at that level: with first = l + 1 the solve
+ * gathers, for every target, only the sources inside the 3 x 3 x 3 neighbourhood of its
+ * level-l ancestor -- exactly the near field of a level-l leaf, computed by a deeper FMM.
+ * With both (first > region level: a local solve) every pass runs only below the active cells
+ * (downward) and below them and their neighbours (upward), the levels above the first M2L
+ * level are skipped, and particles outside the region get 0. bbfmm_b200.AdaptiveSolver
+ * composes a coarse and a refined solver this way. Single-set solvers only. */
 BBFMM_B200_API int bbfmm_b200_set_target_region(bbfmm_b200_solver *s, int level, const unsigned char *active);
 BBFMM_B200_API int bbfmm_b200_set_first_m2l_level(bbfmm_b200_solver *s, int level);
 
@@ -314,6 +316,13 @@ BBFMM_B200_API int bbfmm_b200_batch_create(const bbfmm_b200_config *cfg, int nse
 BBFMM_B200_API int bbfmm_b200_batch_solve(bbfmm_b200_batch *b, const void *q_dev, void *phi_dev, int use_graph);
 /* bbfmm_b200_autotune for every group (drops the captured graph). */
 BBFMM_B200_API int bbfmm_b200_batch_autotune(bbfmm_b200_batch *b, const void *q_dev);
+/* Target regions of a batch (bbfmm_b200_set_target_region for every set): active holds, set
+ * after set in set order, the mask bytes of the cells of level depth_s - levels_up of set s
+ * (8^(depth_s - levels_up) each; NULL clears); first_m2l != 0 also starts each set's local
+ * expansions one level below its region level (bbfmm_b200_set_first_m2l_level). Drops the
+ * captured graph. bbfmm_b200.AdaptiveBatch refines the heavy leaves of a batch with it. */
+BBFMM_B200_API int bbfmm_b200_batch_set_target_regions(bbfmm_b200_batch *b, int levels_up,
+                                                       const unsigned char *active, int first_m2l);
 BBFMM_B200_API int bbfmm_b200_batch_groups(const bbfmm_b200_batch *b);
 /* Nodes of the captured graph (0 before the first graph solve). */
 BBFMM_B200_API long long bbfmm_b200_batch_graph_nodes(const bbfmm_b200_batch *b);

@@ -2,6 +2,8 @@
 bbfmm_b200_set_target_region and AdaptiveSolver. The reference has uniform trees only, so the
 oracle here is the FP64 direct sum.
 
+* Local solves: with a target region below the first M2L level the passes run only over the
+  region's cells and their neighbours; the region's results equal the unrestricted solve's.
 * Partition: a solve whose local expansions start at level l + 1 returns, for every target,
   the sum over the sources in the 3 x 3 x 3 neighbourhood of its level-l ancestor -- checked
   against that restricted direct sum (FP64 solve, n = 8: relative L2 < 1e-6, the FMM's own
@@ -11,6 +13,9 @@ oracle here is the FP64 direct sum.
   adaptive solve against the FP64 direct sum on 2,048 targets, half of them in heavy leaves:
   FP64 and mixed within 1.2x the error of the uniform FP64 solve at the fine depth; with no heavy
   leaf it is exactly the coarse solve.
+* Batches (AdaptiveBatch): every set equal to its own AdaptiveSolver (FP64, 1e-12), graph replay
+  bitwise equal to eager launches, mixed within 1.2x the error of the uniform solve at the fine
+  depth per set (the larger of its FP64 and its mixed error).
 """
 import numpy as np
 import pytest
@@ -59,6 +64,40 @@ def test_first_m2l_level_gives_the_ancestor_neighbourhood():
     assert np.all(np.isfinite(got))
 
 
+@pytest.mark.parametrize("mode,n,slab", [("d", 8, 0), ("mixed", 8, 0), ("s", 4, 0), ("mixed", 8, 512),
+                                         ("d", 4, 64)])
+def test_local_solve_equals_the_unrestricted_solve(mode, n, slab):
+    """A local solve (first M2L level above the region level) runs its passes only below the
+    active cells and their neighbours, in compact row order, and skips the levels above: its
+    results on the region's targets equal those of the same solve without the region (FP64 and
+    mixed 1e-12, FP32 1e-5), and the other targets get 0. slab > 0 also cuts the compact leaf
+    rows into slabs of that many cells."""
+    import torch
+    from bbfmm_b200 import Solver
+    from bbfmm_b200.fmm import leaf_of_particles
+    x, q = _clustered(60000, 11)
+    qd = torch.as_tensor(q, device="cuda")
+    lev, R = 5, 3
+    rng = np.random.default_rng(12)
+    active = rng.random(8 ** R) < 0.1
+    out = []
+    for region in (False, True):
+        s = Solver(n, lev, 1.0, mode=mode)
+        if slab:
+            s.set_leaf_slab(slab)
+        s.set_particles(x)
+        s.set_first_m2l_level(R + 1)
+        if region:
+            s.set_target_region(R, active)
+        out.append(s.solve(qd).double().cpu().numpy())
+        s.close()
+    anc, _ = leaf_of_particles(x, 1.0, R, fp32=(mode == "s"))  # the solver's own cells
+    act = active[anc]
+    tol = 1e-5 if mode == "s" else 1e-12
+    assert act.any() and rel_l2(out[1][act], out[0][act]) < tol, rel_l2(out[1][act], out[0][act])
+    assert np.all(out[1][~act] == 0.0)
+
+
 @pytest.mark.parametrize("mode", ["d", "mixed"])
 def test_adaptive_solver_against_direct(mode):
     import torch
@@ -102,3 +141,70 @@ def test_adaptive_without_heavy_leaves_is_the_coarse_solve():
     assert torch.equal(a.solve(q), s.solve(q))
     a.close()
     s.close()
+
+
+def _batch_sets(seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for N, n, lev, clustered in [(60000, 8, 3, True), (50000, 8, 3, False), (80000, 4, 3, True),
+                                 (30000, 8, 2, True), (40000, 8, 3, True)]:
+        if clustered:
+            x, _ = _clustered(N, int(rng.integers(1 << 30)))
+        else:
+            x = rng.random((N, 3)) - 0.5
+        out.append((x, n, lev))
+    q = rng.uniform(-1, 1, sum(len(x) for x, _, _ in out))
+    return out, q
+
+
+def test_adaptive_batch_matches_adaptive_solvers():
+    """Every set of an adaptive batch (heavy leaves refined by two levels in a second, stacked
+    batch) gets the result of an AdaptiveSolver of its own (FP64: 1e-12; the batch stacks sets,
+    which changes no arithmetic but the autotuned offset split); graph replay equals eager
+    launches bitwise."""
+    import torch
+    from bbfmm_b200 import AdaptiveBatch, AdaptiveSolver
+    sets, q = _batch_sets(21)
+    qd = torch.as_tensor(q, device="cuda")
+    b = AdaptiveBatch(sets, mode="d", cap=256)
+    assert b.refined is not None and b.heavy_leaves > 0
+    eager = b.solve(qd, graph=False).cpu().numpy()
+    g1 = b.solve(qd, graph=True).cpu().numpy()
+    g2 = b.solve(qd, graph=True).cpu().numpy()
+    assert np.array_equal(eager, g1) and np.array_equal(g1, g2)
+    for k, (x, n, lev) in enumerate(sets):
+        a0, a1 = b.offsets[k], b.offsets[k + 1]
+        s = AdaptiveSolver(n, lev, lev + 2, mode="d", cap=256)
+        s.set_particles(x)
+        want = s.solve(qd[a0:a1]).cpu().numpy()
+        s.close()
+        assert rel_l2(eager[a0:a1], want) < 1e-12, (k, rel_l2(eager[a0:a1], want))
+    b.close()
+
+
+def test_adaptive_batch_mixed_against_direct():
+    import torch
+    from bbfmm_b200 import AdaptiveBatch, Solver
+    from bbfmm_b200.fmm import direct
+    sets, q = _batch_sets(22)
+    qd = torch.as_tensor(q, device="cuda")
+    b = AdaptiveBatch(sets, mode="mixed", cap=256)
+    got = b.solve(qd).cpu().numpy()
+    rng = np.random.default_rng(23)
+    for k, (x, n, lev) in enumerate(sets):
+        a0, a1 = b.offsets[k], b.offsets[k + 1]
+        uni = {}
+        for m in ("d", "mixed"):
+            u = Solver(n, lev + 2, 1.0, mode=m)
+            u.set_particles(x)
+            uni[m] = u.solve(qd[a0:a1]).cpu().numpy()
+            u.close()
+        t = rng.choice(a1 - a0, 512, replace=False).astype(np.int32)
+        ref = direct(torch.as_tensor(x, device="cuda"), qd[a0:a1], torch.as_tensor(t, device="cuda")).cpu().numpy()
+        e_a, e_u, e_m = rel_l2(got[a0:a1][t], ref), rel_l2(uni["d"][t], ref), rel_l2(uni["mixed"][t], ref)
+        print(f"set {k} (n={n}, depth {lev}): adaptive mixed {e_a:.3e}, uniform depth {lev + 2}: "
+              f"FP64 {e_u:.3e}, mixed {e_m:.3e}")
+        # the FMM's own error, or the mixed mode's rounding where that is larger (a set with few
+        # particles per leaf, whose FP64 error falls below what FP32 near-field sums resolve)
+        assert e_a <= 1.2 * max(e_u, e_m), (k, e_a, e_u, e_m)
+    b.close()

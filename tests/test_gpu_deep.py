@@ -11,6 +11,9 @@ two-box tiles per sibling class.
   same cells from the solver's own multipoles of that level (interaction lists enumerated from
   the grid, Oracle.m2l_sample). FP64: 1e-12; mixed: 1e-6 relative L2 over the sampled rows
   (split-BF16 products with FP32 accumulation outside the FP64 leading block).
+* Levels 2 and 3 (mixed): every cell of a single set's level-2 and level-3 M2L against the
+  oracle, where the tensor-core kernel tiles 32 or 4 stacked sets' class grids at once, and a
+  batch with partial set groups against single solvers.
 * Mixed, n = 8, depth 6 (N = 524,288): the whole solve against the FP64 solve < 3e-7, its
   error against the FP64 direct sum on 2,048 targets within 1.2x of the FP64 solve's, and the
   tolerance-rank form (SVD cut 1e-8 -> rank 160) mixed vs FP64 at the same rank < 3e-7.
@@ -92,6 +95,48 @@ def test_m2l_level_matches_oracle_on_sampled_cells(oracle_d, mode, tol, lev, N):
     row = np.linalg.norm(got[cells] - want, axis=1) / np.linalg.norm(want, axis=1)
     assert row.max() < 50 * tol, (row.max(), cells[row.argmax()])
     s.close()
+
+
+def test_m2l_levels_2_3_stacked_set_tiles(oracle_d):
+    """Levels 2 and 3 on the tensor cores, whose 2 x 2 x 2 and 4 x 4 x 4 class grids the two-box
+    kernel tiles 32 and 4 stacked sets at a time. One set (the other slots of each tile load it
+    again and are not written): every cell of both levels against the oracle's M2L of the
+    solver's own multipoles, mixed tolerance 1e-6. A batch of depth-2, depth-3 and depth-4 sets
+    (a full and a partial group of four at level 3) gives each set the result of its own mixed
+    solver."""
+    import torch
+    from bbfmm_b200 import Batch, Solver
+    from bbfmm_b200 import operators as ops
+    _, _, E = ops.load_operators(8, single=False)
+    x, q = uniform_inputs(40_000, seed=33)
+    s = _solver("mixed", 3, x)
+    s.solve(torch.as_tensor(q, device="cuda"))
+    torch.cuda.synchronize()
+    for lev in (2, 3):
+        cells = np.arange(8 ** lev)
+        want = oracle_d.m2l_sample(lev, 256, E, s.multipoles(lev), cells)
+        got = s.m2l_output(lev)
+        err = rel_l2(got, want)
+        row = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+        print(f"level {lev} mixed: M2L relL2 {err:.3e}, worst row {row.max():.3e}")
+        assert err < 1e-6 and row.max() < 5e-5, (lev, err, row.max())
+    s.close()
+    rng = np.random.default_rng(34)
+    sets = [(rng.random((int(rng.integers(5000, 30000)), 3)) - 0.5, 8, 3) for _ in range(6)]
+    sets += [(rng.random((40000, 3)) - 0.5, 8, 4), (rng.random((3000, 3)) - 0.5, 8, 2),
+             (rng.random((2500, 3)) - 0.5, 8, 2)]
+    qs = rng.uniform(-1, 1, sum(len(a) for a, _, _ in sets))
+    qd = torch.as_tensor(qs, device="cuda")
+    b = Batch(sets, mode="mixed")
+    got = b.solve(qd).cpu().numpy()
+    for k, (xs, n, lev) in enumerate(sets):
+        a0, a1 = b.offsets[k], b.offsets[k + 1]
+        one = Solver(n, lev, 1.0, mode="mixed")
+        one.set_particles(xs)
+        want = one.solve(qd[a0:a1]).cpu().numpy()
+        one.close()
+        assert rel_l2(got[a0:a1], want) < 1e-12, (k, rel_l2(got[a0:a1], want))
+    b.close()
 
 
 def test_mixed_depth6_against_fp64_and_direct():
