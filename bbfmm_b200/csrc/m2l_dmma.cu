@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
                                                           const double *__restrict__ Ecol,
                                                           double *__restrict__ Lout, int level, int j0, int j1,
                                                           int ni, const int4 *__restrict__ offs,
-                                                          const int *__restrict__ tile_list, int nsets) {
+                                                          const int4 *__restrict__ boxes, int nboxes, int nsets) {
   // blockIdx.y selects one of gridDim.y groups of the 189 offsets; with several groups each
   // writes its partial sums to its own slice of Lout (level cells x R apart)
   extern __shared__ __align__(16) double smem[];
@@ -53,15 +53,42 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
   const int tiles_per_class = nbox * nbox * nbox;
   // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
   // of neighbouring boxes, which read one source region that stays in L2
-  const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;  // a list: only those tiles
-  const int set_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
-  const int c = set_ * 8 + loc_ % 8;
+  // a box list (a target region): 8 listed 2 x 2 x 2 blocks of parent cells of one class per tile
+  const bool listed = boxes != nullptr;
+  const int tpc = listed ? 1 : tiles_per_class;
+  const int set_ = (int)(blockIdx.x / (8 * tpc)), loc_ = (int)(blockIdx.x % (8 * tpc));
+  const int c = (listed ? 0 : set_ * 8) + loc_ % 8;  // class (and set base when not listed)
   const int tb = loc_ / 8;
   const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int nt = bw * bw * bw;
+  const int nt = listed ? NT : bw * bw * bw;
   const int64_t P3 = (int64_t)P * P * P;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  __shared__ int4 s_box[8];  // listed: (set, or -1 - set past the list; x0, y0, z0) of the 8 slots
+  if (listed && tid < 8) {
+    const int bi = set_ * 8 + tid;
+    int4 b = boxes[bi < nboxes ? bi : nboxes - 1];
+    if (bi >= nboxes) b.x = -1 - b.x;
+    s_box[tid] = b;
+  }
+  __syncthreads();
+  // target t of the tile: set base (8 set), class-grid position, whether it is written
+  auto cell = [&](int t, int &sb, int &px, int &py, int &pz, bool &ok) {
+    if (listed) {
+      const int4 b = s_box[t >> 3];
+      ok = b.x >= 0;
+      sb = 8 * (ok ? b.x : -1 - b.x);
+      px = b.y + (t & 1);
+      py = b.z + ((t >> 1) & 1);
+      pz = b.w + ((t >> 2) & 1);
+    } else {
+      ok = t < nt;
+      sb = c & ~7;
+      px = bxo + (t % bw);
+      py = byo + ((t / bw) % bw);
+      pz = bzo + (t / (bw * bw));
+    }
+  };
   const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warp grid
   const bool active = wn * 64 < ni;         // this warp has outputs to compute
   const int nb = ni < R ? ((ni + 63) / 64) * 64 : R;  // B columns staged
@@ -84,9 +111,14 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
     // A: 64 targets x 16 j, 8-byte copies, zero outside the grid / j range
     for (int e = tid; e < NT * BK; e += 256) {
       const int t = e / BK, jj = e % BK;
-      const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
+      int sb, px, py, pz;
+      bool wr;
+      cell(t, sb, px, py, pz, wr);
+      px += shx;
+      py += shy;
+      pz += shz;
       const bool ok = t < nt && jc + jj < j1 && px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P;
-      const double *src = ok ? M + ((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + jj : M;
+      const double *src = ok ? M + ((int64_t)(sb + sc) * P3 + ((int64_t)pz * P + py) * P + px) * R + jc + jj : M;
       cp_async8(sa + (uint32_t)(jj * AST + t) * 8u, src, ok);
     }
     // B: 16 rows j of E_k (the first nb outputs i), 16-byte copies
@@ -139,9 +171,11 @@ __global__ void __launch_bounds__(256, 1) m2l_dmma_kernel(const double *__restri
 #pragma unroll
   for (int mf = 0; mf < 4; ++mf) {
     const int t = wm * 32 + mf * 8 + (lane >> 2);
-    if (t >= nt) continue;
-    const int px = bxo + (t % bw), py = byo + ((t / bw) % bw), pz = bzo + (t / (bw * bw));
-    double *dst = Lout + ((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px) * R;
+    int sb, px, py, pz;
+    bool wr;
+    cell(t, sb, px, py, pz, wr);
+    if (!wr) continue;
+    double *dst = Lout + ((int64_t)(sb + (c & 7)) * P3 + ((int64_t)pz * P + py) * P + px) * R;
 #pragma unroll
     for (int nf = 0; nf < 8; ++nf) {
       const int i = wn * 64 + nf * 8 + 2 * (lane & 3);
@@ -316,7 +350,7 @@ int64_t dmma_part_elems(int level, int nsets, int groups, int r) {
 // summed in a fixed order; with too little scratch the groups are reduced to fit.
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
                     const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets, int ngroups,
-                    const int *tile_list, int ntiles) {
+                    const int4 *boxes, int nboxes) {
   if (r != dm::R) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "FP64 tensor M2L is built for r = 256");
   if (j0 < 0 || j1 > r || j0 >= j1 || ni < 2 || ni > r || ni % 2)
     return bbfmm_set_error(BBFMM_ERR_ARG, "bad contraction / output range");
@@ -324,10 +358,11 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
   const int bw = P < 4 ? P : 4;
   const int nbox = P / bw;
   const int grid = 8 * nsets * nbox * nbox * nbox;
-  if (tile_list && (j0 != 0 || j1 != r || ni != r))
-    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tile lists are for the full FP64 M2L");
-  if (tile_list && (ntiles < 0 || ntiles > grid)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
-  if (tile_list && ntiles == 0) return BBFMM_OK;
+  if (boxes && (j0 != 0 || j1 != r || ni != r))
+    return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "box lists are for the full FP64 M2L");
+  if (boxes && (nboxes < 0 || nboxes > (int64_t)nsets * P * P * P / 8 || P < 2))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "box list longer than the level");
+  if (boxes && nboxes == 0) return BBFMM_OK;
   if (j0 == 0 && j1 <= 64 && (ni == 32 || ni == 64)) {  // the FP64 leading block
     static bool lattr = false;
     if (!lattr) {
@@ -357,19 +392,19 @@ int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, in
   int ng = ngroups > 0 ? ngroups : dmma_default_groups(level, nsets);
   if (ng > DMMA_PARTS) ng = DMMA_PARTS;
   const int64_t count = 8 * (int64_t)nsets * P * P * P * r;
-  if (!part || tile_list) ng = 1;
+  if (!part || boxes) ng = 1;
   else if ((int64_t)ng * count > part_elems) ng = (int)(part_elems / count);
   if (ng > 1) {
     // few target tiles: spread the offsets over ng CTAs per tile, then sum the partials
-    dm::m2l_dmma_kernel<<<dim3(grid, ng), 256, dm::SMEM_BYTES, s>>>(M, Ecol, part, level, j0, j1, ni, offs, nullptr,
+    dm::m2l_dmma_kernel<<<dim3(grid, ng), 256, dm::SMEM_BYTES, s>>>(M, Ecol, part, level, j0, j1, ni, offs, nullptr, 0,
                                                                    nsets);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_dmma", __FILE__, __LINE__);
     dm::sum_parts_kernel<<<(int)((count + 255) / 256), 256, 0, s>>>(count, ng, part, Lout);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma parts", __FILE__, __LINE__);
   }
-  dm::m2l_dmma_kernel<<<tile_list ? ntiles : grid, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1, ni, offs,
-                                                                             tile_list, nsets);
+  dm::m2l_dmma_kernel<<<boxes ? 8 * ((nboxes + 7) / 8) : grid, 256, dm::SMEM_BYTES, s>>>(M, Ecol, Lout, level, j0, j1,
+                                                                                        ni, offs, boxes, nboxes, nsets);
   return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_dmma", __FILE__, __LINE__);
 }
 

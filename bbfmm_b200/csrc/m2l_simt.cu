@@ -13,7 +13,9 @@
 // staging the shifted source box and the operator chunk in shared memory, and keeps a
 // register-blocked accumulator. With [j0, j1) = [0, r) this is the plain FP64 (or FP32)
 // M2L; with [0, 16) it is the FP64 leading-component part of the mixed-precision M2L.
-// A tile list (ids as the full grid numbers its tiles) runs only those tiles.
+// With a box list (a target region) a tile is instead 8 listed 2 x 2 x 2 blocks of parent
+// cells of one class, each of its own set and origin (slots past the list's end are not
+// written).
 //
 // Operators: Ert[k][i][j] = E_k(i, j) (row-major), i.e. the transpose of the
 // reference's column-major K file blocks.
@@ -32,7 +34,7 @@ template <typename T, int R, int TM, int TN>
 __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T *__restrict__ M, const T *__restrict__ Ert,
                                                        T *__restrict__ Lout, int level, int j0, int j1,
                                                        const int4 *__restrict__ offs, int accumulate,
-                                                       const int *__restrict__ tile_list, int nsets) {
+                                                       const int4 *__restrict__ boxes, int nboxes, int nsets) {
   constexpr int BK = 16;
   constexpr int NT = 64;  // targets per tile (4x4x4 box)
   constexpr int THREADS = (NT / TM) * (R / TN);
@@ -45,14 +47,40 @@ __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T 
   const int tiles_per_class = nbox * nbox * nbox;
   // sibling class fastest (the set above it): the CTAs resident at one time are the 8 classes
   // of neighbouring boxes, which read one source region that stays in L2
-  const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;
-  const int set_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
-  const int c = set_ * 8 + loc_ % 8;
+  const bool listed = boxes != nullptr;
+  const int tpc = listed ? 1 : tiles_per_class;
+  const int set_ = (int)(blockIdx.x / (8 * tpc)), loc_ = (int)(blockIdx.x % (8 * tpc));
+  const int c = (listed ? 0 : set_ * 8) + loc_ % 8;  // class (and set base when not listed)
   const int tb = loc_ / 8;
   const int bxo = (tb % nbox) * bw, byo = ((tb / nbox) % nbox) * bw, bzo = (tb / (nbox * nbox)) * bw;
   const int cbx = (c >> 2) & 1, cby = (c >> 1) & 1, cbz = c & 1;
-  const int nt = bw * bw * bw;
+  const int nt = listed ? NT : bw * bw * bw;
   const int tid = threadIdx.x;
+  __shared__ int4 s_box[8];  // listed: (set, or -1 - set past the list; x0, y0, z0) of the 8 slots
+  if (listed && tid < 8) {
+    const int bi = set_ * 8 + tid;
+    int4 b = boxes[bi < nboxes ? bi : nboxes - 1];
+    if (bi >= nboxes) b.x = -1 - b.x;
+    s_box[tid] = b;
+  }
+  __syncthreads();
+  // target t of the tile: set base (8 set), class-grid position, whether it is written
+  auto cell = [&](int t, int &sb, int &px, int &py, int &pz, bool &ok) {
+    if (listed) {
+      const int4 b = s_box[t >> 3];
+      ok = b.x >= 0;
+      sb = 8 * (ok ? b.x : -1 - b.x);
+      px = b.y + (t & 1);
+      py = b.z + ((t >> 1) & 1);
+      pz = b.w + ((t >> 2) & 1);
+    } else {
+      ok = t < nt;
+      sb = c & ~7;
+      px = bxo + (t % bw);
+      py = byo + ((t / bw) % bw);
+      pz = bzo + (t / (bw * bw));
+    }
+  };
   const int tg = tid % TGX, og = tid / TGX;
   T acc[TM][TN];
 #pragma unroll
@@ -78,10 +106,15 @@ __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T 
       for (int e = tid; e < NT * BK; e += THREADS) {
         const int t = e / BK, jj = e % BK;
         T v = 0;
+        int sb, px, py, pz;
+        bool ok;
+        cell(t, sb, px, py, pz, ok);
         if (t < nt && jc + jj < j1) {
-          const int px = bxo + (t % bw) + shx, py = byo + ((t / bw) % bw) + shy, pz = bzo + (t / (bw * bw)) + shz;
+          px += shx;
+          py += shy;
+          pz += shz;
           if (px >= 0 && px < P && py >= 0 && py < P && pz >= 0 && pz < P)
-            v = M[(((int64_t)((c & ~7) + sc) * P3 + ((int64_t)pz * P + py) * P + px)) * R + jc + jj];
+            v = M[(((int64_t)(sb + sc) * P3 + ((int64_t)pz * P + py) * P + px)) * R + jc + jj];
         }
         sa[jj][t] = v;
       }
@@ -108,9 +141,11 @@ __global__ void __launch_bounds__((64 / TM) * (R / TN)) m2l_simt_kernel(const T 
 #pragma unroll
   for (int x = 0; x < TM; ++x) {
     const int t = tg + TGX * x;
-    if (t >= nt) continue;
-    const int px = bxo + (t % bw), py = byo + ((t / bw) % bw), pz = bzo + (t / (bw * bw));
-    T *dst = Lout + (((int64_t)c * P3 + ((int64_t)pz * P + py) * P + px)) * R;
+    int sb, px, py, pz;
+    bool ok;
+    cell(t, sb, px, py, pz, ok);
+    if (!ok) continue;
+    T *dst = Lout + (((int64_t)(sb + (c & 7)) * P3 + ((int64_t)pz * P + py) * P + px)) * R;
 #pragma unroll
     for (int y = 0; y < TN; ++y) {
       const int i = og + (R / TN) * y;
@@ -139,31 +174,33 @@ __global__ void simt_sum_parts_kernel(int64_t count, int ng, const T *__restrict
 
 // ngroups > 1 splits the 189 offsets over that many CTAs per target tile; their partials go
 // to `part` (part_elems elements) and are summed in a fixed order (groups are reduced to
-// fit the scratch; accumulate then does not apply). With a tile list of ntiles ids only those
-// tiles run, in one group, and the rest of Lout is left as it is.
+// fit the scratch; accumulate then does not apply). With a list of nboxes 2 x 2 x 2 blocks of
+// parent cells (set, x0, y0, z0) only their targets are computed, in one group, and the rest
+// of Lout is left as it is.
 template <typename T>
 int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs,
                     int accumulate, cudaStream_t s, int nsets, int ngroups, T *part, int64_t part_elems,
-                    const int *tile_list, int ntiles) {
-  const int all = nsets * m2l_simt_tiles(level);  // the class index runs over all sets' 8 classes
-  if (tile_list && (ntiles < 0 || ntiles > all)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
-  if (tile_list && ntiles == 0) return BBFMM_OK;
-  const int tiles = tile_list ? ntiles : all;
+                    const int4 *boxes, int nboxes) {
   const int64_t P = (int64_t)1 << (level - 1);
+  if (boxes && (nboxes < 0 || nboxes > nsets * P * P * P / 8 || P < 2))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "box list longer than the level");
+  if (boxes && nboxes == 0) return BBFMM_OK;
+  // the class index runs over all sets' 8 classes; a box list: 8 classes x groups of 8 blocks
+  const int tiles = boxes ? 8 * ((nboxes + 7) / 8) : nsets * m2l_simt_tiles(level);
   const int64_t count = 8 * nsets * P * P * P * r;
   int ng = ngroups > 0 ? ngroups : 1;
   if (ng > 21) ng = 21;
-  if (!part || tile_list) ng = 1;
+  if (!part || boxes) ng = 1;
   else if ((int64_t)ng * count > part_elems) ng = (int)(part_elems / count);
   if (ng < 1) ng = 1;
   T *dst = ng > 1 ? part : Lout;
   const dim3 grid(tiles, ng);
   if (r == 256) {
     m2l_simt_kernel<T, 256, 8, 8><<<grid, 256, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate,
-                                                       tile_list, nsets);
+                                                       boxes, nboxes, nsets);
   } else if (r == 32) {
     m2l_simt_kernel<T, 32, 4, 4><<<grid, 128, 0, s>>>(M, Ert, dst, level, j0, j1, offs, ng > 1 ? 0 : accumulate,
-                                                     tile_list, nsets);
+                                                     boxes, nboxes, nsets);
   } else {
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "M2L rank must be 32 or 256 (n = 4 or 8)");
   }
@@ -176,9 +213,9 @@ int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0,
 }
 
 template int launch_m2l_simt<double>(int, const double *, const double *, double *, int, int, int, const int4 *, int,
-                                     cudaStream_t, int, int, double *, int64_t, const int *, int);
+                                     cudaStream_t, int, int, double *, int64_t, const int4 *, int);
 template int launch_m2l_simt<float>(int, const float *, const float *, float *, int, int, int, const int4 *, int,
-                                    cudaStream_t, int, int, float *, int64_t, const int *, int);
+                                    cudaStream_t, int, int, float *, int64_t, const int4 *, int);
 
 // Host table of the 189 offsets of each sibling class, as (k, vx, vy, vz).
 void build_offset_table(int *out /* 8*189*4 */) {

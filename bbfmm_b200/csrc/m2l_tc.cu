@@ -316,7 +316,11 @@ __global__ void __launch_bounds__(192, 1)
 // that whole grid in 4 or 32 consecutive stacked sets (one box load of 4 KB or 512 B per set
 // and operand half; slots past the last set load the last set again and write nothing), so a
 // batch of small trees runs its upper levels on the tensor cores as well. Rows: x fastest,
-// then y, z, set.
+// then y, z, set. With a box list (a target region) a tile is instead 256 / (bx by bz) listed
+// bx x by x bz blocks of parent cells (2 x 2 x 2 or 4 x 4 x 2: lgeom), each of its own set and
+// origin (one box load per block and operand half; slots past the list's end load its last
+// block and write nothing), so the tiles follow the region. The box of slot k is loaded by
+// lane k of the producer warp, so the small boxes of a stage go out together.
 // Stage: A_hi 16 KB | A_lo 16 KB | B_hi 16 KB | B_lo TC_SPLIT_ROWS x 32 BF16 (4 KB).
 // With Mlead and Erow given (leading block i < 32, j < 16), the four epilogue warps, idle
 // while the tensor cores run the ~1 ms mainloop of a CTA, compute that block in FP64 for the
@@ -339,8 +343,8 @@ __global__ void __launch_bounds__(192, 1)
                    const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                    double *__restrict__ Lacc, int level, const int4 *__restrict__ offs, int kfirst, int ilead,
                    int split_chunks, int ncols, const double *__restrict__ Mlead, const double *__restrict__ Erow,
-                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows, const int *__restrict__ tile_list,
-                   int nsets) {
+                   __nv_bfloat16 *__restrict__ Lsplit, int64_t nrows, const int4 *__restrict__ boxes,
+                   int nboxes, int lgeom, int nsets) {
   constexpr int STAGE_BYTES = STAGE2_BYTES;
   constexpr int DNZ = 16;  // components the fused down projection takes in FP64
   constexpr int split_rows = TC_SPLIT_ROWS;
@@ -358,17 +362,53 @@ __global__ void __launch_bounds__(192, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int P = 1 << (level - 1);
-  const Tc2Box g = tc2_box(level);
+  const bool listed = boxes != nullptr;
+  const Tc2Box g = listed ? Tc2Box{lgeom & 15, (lgeom >> 4) & 15, (lgeom >> 8) & 15} : tc2_box(level);
   const int nbx = P >> g.lx, nby = P >> g.ly, nbz = P >> g.lz;
-  const int tiles_per_class = nbx * nby * nbz;
-  // sibling class fastest (the set group above it): the CTAs resident at one time are the 8
-  // classes of neighbouring boxes, which read one source region that stays in L2
-  const int bid_ = tile_list ? tile_list[blockIdx.x] : (int)blockIdx.x;  // a list: only those tiles
+  const int tiles_per_class = listed ? 1 : nbx * nby * nbz;
+  // sibling class fastest (the set group or list group above it): the CTAs resident at one
+  // time are the 8 classes of neighbouring boxes, which read one source region that stays in L2
+  const int bid_ = (int)blockIdx.x;
   const int sg_ = bid_ / (8 * tiles_per_class), loc_ = bid_ % (8 * tiles_per_class);
   const int cls = loc_ % 8, tb = loc_ / 8;
-  const int set0 = sg_ << (8 - g.lb());  // first set of the tile
+  const int set0 = sg_ << (8 - g.lb());  // first set (or list entry) of the tile
   const int bx0 = (tb % nbx) << g.lx, by0 = ((tb / nbx) % nby) << g.ly, bz0 = (tb / (nbx * nby)) << g.lz;
   const int cbx = (cls >> 2) & 1, cby = (cls >> 1) & 1, cbz = cls & 1;
+  // slot k of the tile (rows k 2^lb ..): its set, the origin of its box in the class grid, and
+  // whether its rows are written (a slot past the last set or list entry loads a valid box)
+  __shared__ int4 s_box[32];  // listed: (set, or -1 - set for a slot past the list; x0, y0, z0)
+  if (listed && threadIdx.x < (1 << (8 - g.lb()))) {
+    const int bi = set0 + threadIdx.x;
+    int4 b = boxes[bi < nboxes ? bi : nboxes - 1];
+    if (bi >= nboxes) b.x = -1 - b.x;
+    s_box[threadIdx.x] = b;
+  }
+  auto slot = [&](int k, int &set, int &x0, int &y0, int &z0, bool &ok) {
+    if (listed) {
+      const int4 b = s_box[k];
+      ok = b.x >= 0;
+      set = ok ? b.x : -1 - b.x;
+      x0 = b.y;
+      y0 = b.z;
+      z0 = b.w;
+    } else {
+      set = set0 + k;
+      ok = set < nsets;
+      if (!ok) set = nsets - 1;
+      x0 = bx0;
+      y0 = by0;
+      z0 = bz0;
+    }
+  };
+  // row of the tile -> its cell's set and class-grid position
+  auto row_cell = [&](int row, int &set, int &x, int &y, int &z, bool &ok) {
+    int k, x0, y0, z0;
+    g.pos(row, x, y, z, k);
+    slot(k, set, x0, y0, z0, ok);
+    x += x0;
+    y += y0;
+    z += z0;
+  };
   const int nchunk = ncols / BK;  // K-chunks per offset: the effective rank / 32 (8 for r = 256)
   const int chunk0 = kfirst / KS;  // whole chunks skipped
   const int kstep0 = kfirst % KS;  // K-steps skipped in the first used chunk
@@ -395,33 +435,46 @@ __global__ void __launch_bounds__(192, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0 && lane == 0) {
-    // ---------------- TMA producer
+  if (warp == 0) {
+    // ---------------- TMA producer: lane 0 takes the stage and loads the operator; the box of
+    // slot k of the tile is loaded by lane k
+    const int nslot = 1 << (8 - g.lb());
+    int set_k = 0, x0_k = 0, y0_k = 0, z0_k = 0;  // this lane's slot
+    if (lane < nslot) {
+      bool ok;
+      slot(lane, set_k, x0_k, y0_k, z0_k, ok);
+    }
+    const uint32_t box_bytes = (uint32_t)BK * 2u << g.lb();
     for (int it = 0; it < niter; ++it) {
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
-      if (!mbar_wait(empty_bar(s), ph ^ 1u, 1)) break;
+      const bool got = lane == 0 ? mbar_wait(empty_bar(s), ph ^ 1u, 1) : true;
+      if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) break;
       const int o = it / used_chunks, kc = chunk0 + it % used_chunks;
       const int4 ov = offs[cls * 189 + o];
       const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
       const int scx = gx & 1, scy = gy & 1, scz = gz & 1;
       const int sc = (scx << 2) | (scy << 1) | scz;
-      const int sx = bx0 + (gx - scx) / 2, sy = by0 + (gy - scy) / 2, sz = bz0 + (gz - scz) / 2;
+      const int shx = (gx - scx) / 2, shy = (gy - scy) / 2, shz = (gz - scz) / 2;  // parent-grid step
       const uint32_t st = base + s * STAGE_BYTES;
       // chunks kc < split_chunks take three products and need the lo halves (of B only its
       // first split_rows rows, the box of mapBlo); the others take hi x hi alone
       const bool three = kc < split_chunks;
       const uint32_t bhi_bytes = (uint32_t)ncols * BK * 2;  // the B box holds the first ncols rows i
-      mbar_expect_tx(full_bar(s), three ? 2 * A2_BYTES + bhi_bytes + BLO2_BYTES : A2_BYTES + bhi_bytes);
-      // one box per set of the tile (sets past the last one load the last set: the same bytes)
-      const uint32_t box_bytes = (uint32_t)BK * 2u << g.lb();
-      for (int k = 0; k < (1 << (8 - g.lb())); ++k) {
-        const int sidx = (set0 + k < nsets ? set0 + k : nsets - 1) * 8 + sc;
-        tma_load_5d(st + k * box_bytes, &mapAhi, full_bar(s), kc * BK, sx, sy, sz, sidx);
-        if (three) tma_load_5d(st + A2_BYTES + k * box_bytes, &mapAlo, full_bar(s), kc * BK, sx, sy, sz, sidx);
+      if (lane == 0) {
+        mbar_expect_tx(full_bar(s), three ? 2 * A2_BYTES + bhi_bytes + BLO2_BYTES : A2_BYTES + bhi_bytes);
+        tma_load_3d(st + 2 * A2_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
+        if (three) tma_load_3d(st + 2 * A2_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
       }
-      tma_load_3d(st + 2 * A2_BYTES, &mapBhi, full_bar(s), kc * BK, 0, ov.x);
-      if (three) tma_load_3d(st + 2 * A2_BYTES + B_BYTES, &mapBlo, full_bar(s), kc * BK, 0, ov.x);
+      __syncwarp();
+      // a slot past the last set or list entry loads a valid box: the same bytes
+      if (lane < nslot) {
+        const int sidx = set_k * 8 + sc;
+        tma_load_5d(st + lane * box_bytes, &mapAhi, full_bar(s), kc * BK, x0_k + shx, y0_k + shy, z0_k + shz, sidx);
+        if (three)
+          tma_load_5d(st + A2_BYTES + lane * box_bytes, &mapAlo, full_bar(s), kc * BK, x0_k + shx, y0_k + shy,
+                      z0_k + shz, sidx);
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
@@ -465,16 +518,14 @@ __global__ void __launch_bounds__(192, 1)
       for (int h = 0; h < 2; ++h) {
         double acc[4][4][2];
         int ax[4], ay[4], az[4], aset[4];  // grid position and set of this lane's A rows
+        bool aok[4];                       // whether those rows are written
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
 #pragma unroll
           for (int f = 0; f < 4; ++f) acc[m][f][0] = acc[m][f][1] = 0.0;
-          g.pos(h * 128 + q * 32 + 8 * m + tr, ax[m], ay[m], az[m], aset[m]);
-          ax[m] += bx0;
-          ay[m] += by0;
-          az[m] += bz0;
-          aset[m] += set0;
+          row_cell(h * 128 + q * 32 + 8 * m + tr, aset[m], ax[m], ay[m], az[m], aok[m]);
         }
+        __syncwarp();
         for (int o = 0; o < 189; ++o) {
           const int4 ov = offs[cls * 189 + o];
           const int gx = cbx + ov.y, gy = cby + ov.z, gz = cbz + ov.w;
@@ -485,8 +536,7 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
           for (int m = 0; m < 4; ++m) {
             const int px = ax[m] + shx, py = ay[m] + shy, pz = az[m] + shz;
-            if ((unsigned)px < (unsigned)P && (unsigned)py < (unsigned)P && (unsigned)pz < (unsigned)P &&
-                aset[m] < nsets) {
+            if ((unsigned)px < (unsigned)P && (unsigned)py < (unsigned)P && (unsigned)pz < (unsigned)P) {
               const double *Mc = Mlead + (int64_t)(aset[m] * 8 + sc) * P3 * BN + 4 * u;
               const double2 *src = reinterpret_cast<const double2 *>(Mc + (((int64_t)pz * P + py) * P + px) * BN);
               a[m][0] = src[0];
@@ -515,13 +565,15 @@ __global__ void __launch_bounds__(192, 1)
         // D fragment: row tr of fragment m (the A row of this lane), columns 8f + 2u + {0, 1}
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-          if (aset[m] >= nsets) continue;
-          const int64_t cell = (int64_t)(aset[m] * 8 + cls) * P3 + ((int64_t)az[m] * P + ay[m]) * P + ax[m];
-          double *dst = Lacc + cell * BN;
+          if (aok[m]) {
+            const int64_t cell = (int64_t)(aset[m] * 8 + cls) * P3 + ((int64_t)az[m] * P + ay[m]) * P + ax[m];
+            double *dst = Lacc + cell * BN;
 #pragma unroll
-          for (int f = 0; f < 4; ++f)
-            *reinterpret_cast<double2 *>(dst + 8 * f + 2 * u) = make_double2(acc[m][f][0], acc[m][f][1]);
+            for (int f = 0; f < 4; ++f)
+              *reinterpret_cast<double2 *>(dst + 8 * f + 2 * u) = make_double2(acc[m][f][0], acc[m][f][1]);
+          }
         }
+        __syncwarp();
       }
       __threadfence_block();
       __syncwarp();  // the rows written here are read back below by other lanes of this warp
@@ -529,18 +581,16 @@ __global__ void __launch_bounds__(192, 1)
     const bool ok = mbar_wait(acc_bar, 0, 3);
     tc_fence_after();
     for (int h = 0; h < 2 && ok; ++h) {
-      int tx, ty, tz, ts;
-      g.pos(h * 128 + row, tx, ty, tz, ts);
-      const int set = set0 + ts;
-      const bool valid = set < nsets;  // rows of sets past the last: read from TMEM, not written
-      const int64_t cell = (int64_t)(set * 8 + cls) * P3 + ((int64_t)(bz0 + tz) * P + (by0 + ty)) * P + (bx0 + tx);
+      int tx, ty, tz, set;
+      bool valid;  // rows of slots past the last set or list entry: read from TMEM, not written
+      row_cell(h * 128 + row, set, tx, ty, tz, valid);
+      const int64_t cell = (int64_t)(set * 8 + cls) * P3 + ((int64_t)tz * P + ty) * P + tx;
       double *dst = Lacc + cell * BN;
       int64_t mrow = 0;  // Morton row of the cell: set base + Morton index of its grid position
-      if (Lsplit)
-        mrow = (int64_t)set * 8 * P3 +
-               grid_to_morton(2 * (bx0 + tx) + cbx, 2 * (by0 + ty) + cby, 2 * (bz0 + tz) + cbz, level);
+      if (Lsplit) mrow = (int64_t)set * 8 * P3 + grid_to_morton(2 * tx + cbx, 2 * ty + cby, 2 * tz + cbz, level);
       for (int col = 0; col < ncols; col += 32) {
         float v[32];
+        __syncwarp();
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 256 + col), v);
         if (!valid) continue;
         const bool add = col < ilead;  // ilead is a multiple of 32
@@ -1157,7 +1207,7 @@ bool tc_fuses_lead(const void *opsv, int nprod, int rank) {
 
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *opsv, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets, int nprod, int rank, const double *Mlead,
-                  const double *Erow, void *Lsplit, const int *tile_list, int ntiles) {
+                  const double *Erow, void *Lsplit, const int4 *boxes, int nboxes, int lgeom) {
   const TcOps *ops = (const TcOps *)opsv;
   if (nprod != 0 && nprod != 1 && nprod != 3)
     return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core products must be 0 (adaptive), 1 or 3");
@@ -1176,7 +1226,9 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
   if (level < (two ? TC2_MIN_LEVEL : TC_MIN_LEVEL))
     return bbfmm_set_error(BBFMM_ERR_ARG, two ? "tensor-core M2L needs level >= 2" : "tensor-core M2L needs level >= 4");
   if (nsets < 1) return bbfmm_set_error(BBFMM_ERR_ARG, "tensor-core M2L needs a set");
-  const Tc2Box g2 = tc2_box(level);
+  const Tc2Box g2 = boxes ? Tc2Box{lgeom & 15, (lgeom >> 4) & 15, (lgeom >> 8) & 15} : tc2_box(level);
+  if (boxes && (g2.lb() < 3 || g2.lb() > 8 || (1 << g2.lx) > P || (1 << g2.ly) > P || (1 << g2.lz) > P))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "box-list geometry: 8 to 256 rows inside the class grid");
   const __nv_bfloat16 *hi = (const __nv_bfloat16 *)Msplit + (size_t)cell_offset * r;
   const __nv_bfloat16 *lo = (const __nv_bfloat16 *)Msplit + (size_t)(ncell_total + cell_offset) * r;
   CUtensorMap mapAhi, mapAlo;
@@ -1216,14 +1268,16 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
       if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc2 smem attribute", __FILE__, __LINE__);
       attr2 = true;
     }
-    const int64_t tiles2 = tc2_tiles(level, nsets);
     const bool fuse = Mlead && Erow && tc_fuses_lead(ops, nprod, rank) && kfirst == 0 && ilead == 32;
     if (Lsplit && !fuse) return bbfmm_set_error(BBFMM_ERR_ARG, "split M2L output needs the fused leading block");
-    if (tile_list && (ntiles < 0 || ntiles > tiles2)) return bbfmm_set_error(BBFMM_ERR_ARG, "tile list longer than the level");
-    if (tile_list && ntiles == 0) return BBFMM_OK;
-    tc::m2l_tc2_kernel<<<(unsigned)(tile_list ? (int64_t)ntiles : tiles2), 192, tc::SMEM2_BYTES, s>>>(
+    const int spl = 1 << (8 - g2.lb());  // listed blocks per tile
+    if (boxes && (nboxes < 0 || nboxes > (int64_t)nsets * (P >> g2.lx) * (P >> g2.ly) * (P >> g2.lz)))
+      return bbfmm_set_error(BBFMM_ERR_ARG, "box list longer than the level");
+    if (boxes && nboxes == 0) return BBFMM_OK;
+    const int64_t tiles2 = boxes ? 8 * (int64_t)((nboxes + spl - 1) / spl) : tc2_tiles(level, nsets);
+    tc::m2l_tc2_kernel<<<(unsigned)tiles2, 192, tc::SMEM2_BYTES, s>>>(
         mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst, ilead, split_chunks, rank, fuse ? Mlead : nullptr,
-        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P, tile_list, nsets);
+        fuse ? Erow : nullptr, (__nv_bfloat16 *)Lsplit, 8 * (int64_t)nsets * P * P * P, boxes, nboxes, lgeom, nsets);
     return bbfmm_set_cuda_error(cudaGetLastError(), "m2l_tc2", __FILE__, __LINE__);
   }
   static bool attr = false;
@@ -1232,7 +1286,7 @@ int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_o
     if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "m2l_tc smem attribute", __FILE__, __LINE__);
     attr = true;
   }
-  if (tile_list) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "tile lists are for the two-box tensor-core M2L");
+  if (boxes) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "box lists are for the two-box tensor-core M2L");
   const int tiles = 8 * nsets * (P / tc::BOX_X) * (P / tc::BOX_Y) * (P / tc::BOX_Z);
   tc::m2l_tc_kernel<<<tiles, 192, tc::SMEM_BYTES, s>>>(mapAhi, mapAlo, mapBhi, mapBlo, Lacc, level, offs, kfirst,
                                                        ilead, split_chunks, split_rows, rank);

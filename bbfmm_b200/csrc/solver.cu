@@ -5,6 +5,7 @@
 //   gather q -> P2M (maxlev) -> [U-projection, M2M] up to level 2      (upward)
 //   per level 2..maxlev: M2L -> post projection (assign) -> L2L from the parent level
 //   L2P (assign) -> P2P (add) -> scatter phi to the caller's particle order
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -415,17 +416,17 @@ int Solver<T>::upward(const void *q_dev, int q_is_double) {
 
 // FP64 with r = 256 runs on the FP64 tensor path (DMMA); FP32 and r = 32 on CUDA cores.
 template <typename T>
-int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni, const int *tile_list, int ntiles) {
+int Solver<T>::m2l_fp(const T *Ml, int level, int j0, int j1, int ni, const int4 *boxes, int nboxes) {
   if (sizeof(T) == 8 && r == 256)
     return launch_m2l_dmma(r, (const double *)Ml, (const double *)Ecol, (double *)Lbuf, level, j0, j1, ni, offs,
-                           (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level], tile_list, ntiles);
+                           (double *)Lpart, Lpart_elems, stream, nsets, tune.m2l_groups[level], boxes, nboxes);
   // the SIMT kernel writes all r outputs; in the rank mode (ni = rk()) the outputs i >= rank
   // of the zero-padded operators come out as zeros, so only other partial ranges are refused
   if (ni != r && ni != rk())
     return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "partial output range needs the FP64 r = 256 path");
   const int g = tune.m2l_groups[level] > 0 ? tune.m2l_groups[level] : dmma_default_groups(level, nsets);
-  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets, g, Lpart, Lpart_elems,
-                            tile_list, ntiles);
+  return launch_m2l_simt<T>(r, Ml, Ert, Lbuf, level, j0, j1, offs, 0, stream, nsets, g, Lpart, Lpart_elems, boxes,
+                            nboxes);
 }
 
 template <typename T>
@@ -530,14 +531,14 @@ int Solver<T>::m2l_post(int l) {
       // two-box kernel computes the block itself in its otherwise idle epilogue warps
       if (lead > 0 && tc_fuses_lead(tcops, tc_products, rk())) {
         // a target region: only the tiles above active cells run, the rest of the output is zero
-        const bool masked = region_tiles[l] != nullptr;
+        const bool masked = region_tcboxes[l] != nullptr;
         // whole level with mixed projections: the kernel also writes the split rows that the
         // down projection reads (and the FP64 output only where that pass reads it)
         presplit = !masked && proj_tc() && cells(l) <= Lsplit_rows && !(l == maxlev && chunked());
         if (masked) BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * (size_t)cells(l) * r, stream));
         TRY(launch_m2l_tc(r, Msplit, Mcells(), Moff[l] / r, tcops, (double *)Lbuf, l, offs, stream, nsets,
                           tc_products, rk(), (const double *)Ml, (const double *)Ert, presplit ? Lsplit : nullptr,
-                          region_tiles[l], region_ntiles[l]));
+                          region_tcboxes[l], region_ntcboxes[l], region_tcgeom[l]));
         mark(ST_M2L, 1);
       } else if (lead > 0) {
         TRY(m2l_fp(Ml, l, 0, lead, lead_rows));
@@ -549,11 +550,11 @@ int Solver<T>::m2l_post(int l) {
                           tc_products, rk()));
         mark(ST_M2L, 1);
       }
-    } else if (region_tiles4[l]) {
-      // a target region: only the tiles above active cells run (one offset group), the rest
+    } else if (region_boxes[l]) {
+      // a target region: only the blocks above active cells run (one offset group), the rest
       // of the output is zero
       BBFMM_CUDA_OK(cudaMemsetAsync(Lbuf, 0, sizeof(T) * (size_t)cells(l) * r, stream));
-      TRY(m2l_fp(Ml, l, 0, rk(), rk(), region_tiles4[l], region_ntiles4[l]));
+      TRY(m2l_fp(Ml, l, 0, rk(), rk(), region_boxes[l], region_nboxes[l]));
       mark(ST_M2L, 1);
     } else {
       TRY(m2l_fp(Ml, l, 0, rk(), rk()));
@@ -612,7 +613,7 @@ int Solver<T>::time_m2l(int level, int reps, float *ms) {
   // the launch as the solve makes it: a whole level with the mixed projections also writes
   // the split rows of the down projection (m2l_post)
   const bool presplit = fused && proj_tc() && cells(level) <= Lsplit_rows && !(level == maxlev && chunked()) &&
-                        !region_tiles[level];
+                        !region_tcboxes[level];
   int rc = BBFMM_OK;
   float tot[2] = {0.f, 0.f};
   for (int part = 0; part < (split ? 2 : 1) && rc == BBFMM_OK; ++part) {
@@ -653,10 +654,10 @@ int Solver<T>::near(T *pot, T *fld) {
 template <typename T>
 int Solver<T>::set_target_region(int level, const unsigned char *active_host) {
   for (int l = 0; l <= 10; ++l) {
-    if (region_tiles[l]) cudaFree(region_tiles[l]);
-    if (region_tiles4[l]) cudaFree(region_tiles4[l]);
-    region_tiles[l] = region_tiles4[l] = nullptr;
-    region_ntiles[l] = region_ntiles4[l] = 0;
+    if (region_boxes[l]) cudaFree(region_boxes[l]);
+    if (region_tcboxes[l]) cudaFree(region_tcboxes[l]);
+    region_boxes[l] = region_tcboxes[l] = nullptr;
+    region_nboxes[l] = region_ntcboxes[l] = 0;
   }
   if (region_mask) cudaFree(region_mask);
   region_mask = nullptr;
@@ -744,48 +745,62 @@ int Solver<T>::build_local() {
   return BBFMM_OK;
 }
 
-// Active tiles of every level above the region level, for the two M2L tilings: the two-box
-// tensor-core kernel's (a box of parent cells of one sibling class in one or more consecutive
-// sets, Tc2Box) and the 4 x 4 x 4 boxes of one class and set of the FP64 / FP32 kernels. A
-// tile is active when one of its cells descends from an active region cell. Ids as the
-// kernels number their full grids: (set group, box, then class fastest).
+// Active blocks of parent cells of every level above the region level, the tiles of the M2L
+// kernels under a target region: a block is active when one of its cells descends from an
+// active region cell. The FP64 / FP32 kernels take 2 x 2 x 2 blocks, 8 per tile. The
+// tensor-core kernel takes 2 x 2 x 2 blocks (32 per tile) or 4 x 4 x 2 blocks (8 per tile),
+// whichever costs less by a model of its tiles: a tile's tensor-core mainloop against the TMA
+// requests of its box loads (two per block and stage), of which about 22 fit in the mainloop's
+// time (measured: 32 blocks of 2 x 2 x 2 per tile run 3x slower than one 8 x 8 x 4 box).
+// Morton order of the blocks within each set.
 template <typename T>
 int Solver<T>::build_region_tiles() {
-  auto active_tiles = [&](int l, int lx, int ly, int lz, int spt, std::vector<int> &ids) {
-    const int P = 1 << (l - 1), nbx = P >> lx, nby = P >> ly, nbz = P >> lz, sh = l - 1 - region_level;
-    const int tpc = nbx * nby * nbz, ex = 1 << lx, ey = 1 << ly, ez = 1 << lz;
-    for (int sg = 0; sg * spt < nsets; ++sg) {
-      for (int tb = 0; tb < tpc; ++tb) {
-        const int bx0 = (tb % nbx) * ex, by0 = ((tb / nbx) % nby) * ey, bz0 = (tb / (nbx * nby)) * ez;
-        bool act = false;
-        for (int set = sg * spt; set < nsets && set < (sg + 1) * spt && !act; ++set) {
-          const unsigned char *mask = region_host.data() + (size_t)set * pow8i(region_level);
-          for (int az = bz0 >> sh; az <= (bz0 + ez - 1) >> sh && !act; ++az)
-            for (int ay = by0 >> sh; ay <= (by0 + ey - 1) >> sh && !act; ++ay)
-              for (int ax = bx0 >> sh; ax <= (bx0 + ex - 1) >> sh && !act; ++ax)
-                act = mask[(size_t)grid_to_morton(ax, ay, az, region_level)] != 0;
-        }
-        if (act)
-          for (int c = 0; c < 8; ++c) ids.push_back((sg * tpc + tb) * 8 + c);
-      }
+  auto blocks = [&](int l, int lx, int ly, int lz, std::vector<int4> &bl) {
+    const int lp = l - 1, sh = lp - region_level;
+    const int nx = (1 << lp) >> lx, ny = (1 << lp) >> ly, nz = (1 << lp) >> lz;
+    for (int set = 0; set < nsets; ++set) {
+      const unsigned char *mask = region_host.data() + (size_t)set * pow8i(region_level);
+      // blocks in Morton order of their corner cell
+      std::vector<std::pair<int64_t, int4>> v;
+      for (int bz = 0; bz < nz; ++bz)
+        for (int by = 0; by < ny; ++by)
+          for (int bx = 0; bx < nx; ++bx) {
+            bool act = false;
+            for (int z = bz << lz; z < (bz + 1) << lz && !act; ++z)
+              for (int y = by << ly; y < (by + 1) << ly && !act; ++y)
+                for (int x = bx << lx; x < (bx + 1) << lx && !act; ++x)
+                  act = mask[(size_t)grid_to_morton(x >> sh, y >> sh, z >> sh, region_level)] != 0;
+            if (act) v.push_back({grid_to_morton(bx << lx, by << ly, bz << lz, lp), make_int4(set, bx << lx, by << ly, bz << lz)});
+          }
+      std::sort(v.begin(), v.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+      for (const auto &e : v) bl.push_back(e.second);
     }
   };
-  auto upload = [&](const std::vector<int> &ids, int **dst, int *count) -> int {
-    *count = (int)ids.size();
-    TRY(dalloc(dst, ids.size() > 0 ? ids.size() : 1));
-    if (!ids.empty()) BBFMM_CUDA_OK(cudaMemcpy(*dst, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+  auto upload = [&](const std::vector<int4> &bl, int4 **dst, int *count) -> int {
+    *count = (int)bl.size();
+    TRY(dalloc(dst, bl.size() > 0 ? bl.size() : 1));
+    if (!bl.empty()) BBFMM_CUDA_OK(cudaMemcpy(*dst, bl.data(), sizeof(int4) * bl.size(), cudaMemcpyHostToDevice));
     return BBFMM_OK;
   };
   for (int l = region_level + 1; l <= maxlev; ++l) {
-    std::vector<int> ids, ids4;
-    if (l >= TC2_MIN_LEVEL) {
-      const Tc2Box g = tc2_box(l);
-      active_tiles(l, g.lx, g.ly, g.lz, 1 << (8 - g.lb()), ids);
-      TRY(upload(ids, &region_tiles[l], &region_ntiles[l]));
+    std::vector<int4> b2, b4;
+    blocks(l, 1, 1, 1, b2);
+    TRY(upload(b2, &region_boxes[l], &region_nboxes[l]));
+    int geom = 0x111;
+    const std::vector<int4> *tc = &b2;
+    if ((1 << (l - 1)) >= 4) {  // 4 x 4 x 2 blocks need a class grid of 4 per axis
+      blocks(l, 2, 2, 1, b4);
+      auto cost = [](size_t nb, int per) {
+        const double tiles = (double)((nb + per - 1) / per);
+        return tiles * std::max(1.0, (2.0 * per + 2.0) / 22.0);
+      };
+      if (cost(b4.size(), 8) < cost(b2.size(), 32)) {
+        geom = 0x122;
+        tc = &b4;
+      }
     }
-    const int lb4 = l - 1 < 2 ? l - 1 : 2;  // boxes of min(P, 4) cells per axis
-    active_tiles(l, lb4, lb4, lb4, 1, ids4);
-    TRY(upload(ids4, &region_tiles4[l], &region_ntiles4[l]));
+    region_tcgeom[l] = geom;
+    TRY(upload(*tc, &region_tcboxes[l], &region_ntcboxes[l]));
   }
   return BBFMM_OK;
 }
@@ -981,8 +996,8 @@ int Solver<T>::copy_m2l_morton(int level, T *host_out) {
 template <typename T>
 void Solver<T>::release() {
   for (int l = 0; l <= 10; ++l) {
-    if (region_tiles[l]) cudaFree(region_tiles[l]);
-    if (region_tiles4[l]) cudaFree(region_tiles4[l]);
+    if (region_boxes[l]) cudaFree(region_boxes[l]);
+    if (region_tcboxes[l]) cudaFree(region_tcboxes[l]);
   }
   free_local();
   if (region_mask) cudaFree(region_mask);

@@ -53,12 +53,12 @@ int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_
 int near_status(int clear);
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, const int64_t *rows = nullptr);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
-template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0, const int *tile_list = nullptr, int ntiles = 0);
+template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0, const int4 *boxes = nullptr, int nboxes = 0);
 void build_offset_table(int *out);
 constexpr int DMMA_PARTS = 21;  // most offset groups of the FP64 M2L (189 = 9 x 21)
 int launch_m2l_dmma(int r, const double *M, const double *Ecol, double *Lout, int level, int j0, int j1, int ni,
                     const int4 *offs, double *part, int64_t part_elems, cudaStream_t s, int nsets = 1,
-                    int ngroups = 0, const int *tile_list = nullptr, int ntiles = 0);
+                    int ngroups = 0, const int4 *boxes = nullptr, int nboxes = 0);
 int dmma_default_groups(int level, int nsets);
 int64_t dmma_part_elems(int level, int nsets, int groups, int r);
 int launch_proj_dmma(int64_t M, int K, int N, const double *A, const double *B, const double *cs, double scale,
@@ -89,12 +89,14 @@ size_t tc_split_bytes(int r, int64_t ncell);
 // 32 x 64.
 constexpr int TC_SPLIT_CHUNKS = 2, TC_SPLIT_ROWS = 64;
 // rank: the effective rank (outputs i and components j below it; 0 = r).
-// tile_list (ntiles entries): run only these two-box tiles (ids as the full grid numbers them:
-// set, then box, then sibling class fastest); the outputs of the other cells are not written.
+// boxes (nboxes entries of set, x0, y0, z0): run only the targets of these blocks of parent
+// cells, of 2^lx x 2^ly x 2^lz cells (lgeom = lx | ly << 4 | lz << 8, 8 to 256 cells, origins
+// multiples of the extents), 256 / cells per tile; the outputs of the other cells are not
+// written.
 int launch_m2l_tc(int r, const void *Msplit, int64_t ncell_total, int64_t cell_offset, const void *ops, double *Lacc,
                   int level, const int4 *offs, cudaStream_t s, int nsets = 1, int nprod = 3, int rank = 0,
                   const double *Mlead = nullptr, const double *Erow = nullptr, void *Lsplit = nullptr,
-                  const int *tile_list = nullptr, int ntiles = 0);
+                  const int4 *boxes = nullptr, int nboxes = 0, int lgeom = 0x111);
 bool tc_fuses_lead(const void *ops, int nprod, int rank);
 // Whether launch_m2l_tc runs the two-box kernel (the adaptive product map at full split rows).
 inline bool tc_two_box(int nprod, int rank) { return nprod == 0 && (rank <= 0 || rank >= TC_SPLIT_ROWS); }
@@ -200,10 +202,10 @@ struct Solver {
   int region_level = -1;                       // < 0: every particle
   unsigned char *region_mask = nullptr;        // device, nsets 8^region_level bytes (stacked numbering)
   std::vector<unsigned char> region_host;
-  int *region_tiles[11] = {};                  // per level: active two-box tile ids (device)
-  int region_ntiles[11] = {};
-  int *region_tiles4[11] = {};                 // per level: active 4 x 4 x 4 tiles of the FP64 / FP32 M2L
-  int region_ntiles4[11] = {};
+  int4 *region_boxes[11] = {};                 // per level: active 2 x 2 x 2 parent blocks (set, x0, y0, z0)
+  int region_nboxes[11] = {};
+  int4 *region_tcboxes[11] = {};               // per level: the tensor-core M2L's active blocks,
+  int region_ntcboxes[11] = {}, region_tcgeom[11] = {};  // of geometry region_tcgeom (lgeom)
   // First level whose M2L runs (bbfmm_b200_set_first_m2l_level): the local expansions start
   // there (no L2L from the level above), so the solve gathers, for every target, only the
   // sources inside the neighbourhood of its ancestor one level up.
@@ -266,7 +268,7 @@ struct Solver {
   int build_local();                                                   // runs and row lists
   void free_local();
   bool chunked() const { return slabbed() || local_solve; }  // leaf passes run per leaf chunk
-  int build_region_tiles();                      // region_tiles from region_host (after particles/alloc)
+  int build_region_tiles();                      // region_boxes from region_host
   bool proj_tc() const { return mode == MODE_MIXED && mixed_proj && tcproj != nullptr; }
   // level l has a tensor-core M2L under the current product map and rank (mixed mode), and
   // the solve runs it there (the level's tuning keeps the default kind)
@@ -297,7 +299,7 @@ struct Solver {
   void mark(int stage, int launches = 1);
   int time_m2l(int level, int reps, float *ms);
   int m2l_fp(const T *Ml, int level, int j0, int j1, int ni,  // FP64 (DMMA) / FP32 (SIMT) M2L part
-             const int *tile_list = nullptr, int ntiles = 0);
+             const int4 *boxes = nullptr, int nboxes = 0);
   int proj(int64_t M, int K, int N, const T *A, const T *B, const T *cs, T scale, T *C, int level, int mapmode,
            int64_t row0 = 0, int lda = 0, const int64_t *rowlist = nullptr);
   void release();
