@@ -38,6 +38,22 @@ __device__ __forceinline__ T sn_lane(const T *__restrict__ tkz, int lane, T x, T
   return c * d1 - d2 + (T)0.5 * tkz[m * NN];
 }
 
+// S(x_m, c) for axis idx / NN (c = x, y, z) and node m = idx % NN, idx < 3 NN: the value
+// lane idx of sn_lane returns.
+template <typename T, int NN>
+__device__ __forceinline__ T sn_value(const T *__restrict__ tkz, int idx, T x, T y, T z) {
+  const int a = idx / NN, m = idx % NN;
+  const T c = a == 0 ? x : (a == 1 ? y : z);
+  T d1 = 0, d2 = 0;
+#pragma unroll
+  for (int j = NN - 1; j > 0; --j) {
+    const T d0 = 2 * c * d1 - d2 + tkz[m * NN + j];
+    d2 = d1;
+    d1 = d0;
+  }
+  return c * d1 - d2 + (T)0.5 * tkz[m * NN];
+}
+
 template <typename T>
 __device__ __forceinline__ T wshfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 
@@ -276,35 +292,155 @@ template <int NN> __device__ __forceinline__ int f_l2(int k, int lane) {
   return NN == 8 ? 4 * (k & 1) + (lane >> 3) : (lane >> 2) & 3;
 }
 
-// Warp-per-leaf pipeline shared by the L2P kernels: the leaf offsets are loaded two leaves
-// ahead and the next leaf's F (coalesced, n^3 / 32 values per lane; skipped for empty
-// leaves) one leaf ahead, so the HBM loads of the next leaf are in flight while the current
-// one is evaluated. body(leaf m, local index mm, p0, p1, F registers) does the arithmetic.
-template <typename T, int NN, typename Body>
-__device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start, const T *__restrict__ F, int64_t m0,
-                                             int64_t count, const int64_t *__restrict__ rows, Body body) {
-  constexpr int PER = NN * NN * NN / 32;
-  const int lane = threadIdx.x & 31;
+// Status word of the passes' bounded waits (0 = every wait completed).
+__device__ int g_pass_status = 0;
+constexpr uint32_t PASS_WAIT_LIMIT = 1u << 26;
+constexpr int PASS_WAIT_CODE = 31;  // an L2P leaf copy did not arrive
+
+constexpr int L2P_DEPTH = 3;   // leaf slots per warp (51 KB per CTA at n = 8 in FP64: 4 CTAs per SM)
+constexpr int L2P_WARPS = 4;   // warps per CTA (128 threads)
+constexpr int L2P_PCAP = 8;    // particle positions a slot carries (the leaf's first ones)
+// one slot: the leaf's n^3 values, then up to L2P_PCAP positions (x, y, z, q)
+template <typename T, int NN>
+constexpr int l2p_slot_elems() { return NN * NN * NN + 4 * L2P_PCAP; }
+template <typename T, int NN>
+constexpr int l2p_smem_bytes() { return L2P_WARPS * L2P_DEPTH * l2p_slot_elems<T, NN>() * (int)sizeof(T); }
+
+__device__ __forceinline__ uint32_t pass_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Warp-per-leaf pipeline shared by the L2P kernels: each warp keeps a ring of L2P_DEPTH leaf
+// slots in shared memory, filled by bulk copies that complete on the slot's mbarrier -- the
+// leaf's n^3 values (one contiguous row of F) and the positions of its first L2P_PCAP
+// particles (contiguous in the sorted order) -- so L2P_DEPTH - 1 leaves, positions included,
+// are on their way from HBM while one is evaluated, without holding them in registers. The warp's leaves are
+// taken in chunks of 32 whose cells and offsets its lanes load together one chunk ahead, so
+// no leaf waits for its own offset loads. Empty leaves take no copy (the slot's barrier is
+// arrived at without bytes). The lane reads of a leaf are coalesced (lane + 32 k),
+// conflict-free: with LANES = 32 lane j holds values j + 32 k, with LANES = 16 both half-warps
+// hold values (j mod 16) + 16 k. body(leaf m, p0, p1, F registers, positions of particles
+// p0 .. p0 + L2P_PCAP - 1 in shared memory) does the arithmetic. A wait that gives up records
+// PASS_WAIT_CODE in g_pass_status and ends the warp's work.
+template <typename T, int NN, int LANES, typename Body>
+__device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start, const T *__restrict__ F,
+                                             const T *__restrict__ pos4, int64_t m0, int64_t count,
+                                             const int64_t *__restrict__ rows, T *ring_all, uint64_t *bars_all,
+                                             int2 *offs_all, Body body) {
+  constexpr int N3 = NN * NN * NN, PER = N3 / LANES, D = L2P_DEPTH, SLOT = l2p_slot_elems<T, NN>();
+  static_assert(D < 32, "the slots run at most one offset chunk ahead");
+  constexpr uint32_t BYTES = N3 * sizeof(T);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  T fc[PER], fn[PER];
-  int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-  auto leaf = [&](int64_t mm) { return pass_cell(rows, m0, mm); };
-  if (warp < count) { a0 = leaf_start[leaf(warp)]; a1 = leaf_start[leaf(warp) + 1]; }
-  if (warp + nwarps < count) { b0 = leaf_start[leaf(warp + nwarps)]; b1 = leaf_start[leaf(warp + nwarps) + 1]; }
-#pragma unroll
-  for (int k = 0; k < PER; ++k) fc[k] = a1 > a0 ? F[warp * (NN * NN * NN) + lane + 32 * k] : (T)0;
-  for (int64_t mm = warp; mm < count; mm += nwarps) {
-    int c0 = 0, c1 = 0;
-    if (mm + 2 * nwarps < count) { c0 = leaf_start[leaf(mm + 2 * nwarps)]; c1 = leaf_start[leaf(mm + 2 * nwarps) + 1]; }
-    const bool nxt = mm + nwarps < count && b1 > b0;
-#pragma unroll
-    for (int k = 0; k < PER; ++k) fn[k] = nxt ? F[(mm + nwarps) * (NN * NN * NN) + lane + 32 * k] : (T)0;
-    if (a1 > a0) body(leaf(mm), a0, a1, fc);
-#pragma unroll
-    for (int k = 0; k < PER; ++k) fc[k] = fn[k];
-    a0 = b0; a1 = b1; b0 = c0; b1 = c1;
+  // leaves of this warp: index i is local row warp + i nwarps
+  const int64_t nmine = warp < count ? (count - warp + nwarps - 1) / nwarps : 0;
+  T *ring = ring_all + (size_t)wib * D * SLOT;
+  uint64_t *bars = bars_all + wib * D;
+  int2 *offs = offs_all + wib * D;
+  if (lane == 0) {
+    for (int d = 0; d < D; ++d)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(pass_smem_u32(bars + d)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  __syncwarp();
+  // chunk c of 32 leaves: lane j holds leaf 32 c + j's cell and offsets
+  auto load_chunk = [&](int64_t c, int64_t &m, int &p0, int &p1) {
+    const int64_t i = 32 * c + lane;
+    m = 0;
+    p0 = p1 = 0;
+    if (i < nmine) {
+      m = pass_cell(rows, m0, warp + i * nwarps);
+      p0 = leaf_start[m];
+      p1 = leaf_start[m + 1];
+    }
+  };
+  int64_t cm, nm;  // cells of the current chunk and the next one
+  int c0, c1, n0, n1;
+  load_chunk(0, cm, c0, c1);
+  load_chunk(1, nm, n0, n1);
+  // lane 0: slot (i % D) <- leaf i, whose offsets are (p0, p1)
+  auto issue = [&](int64_t i, int p0, int p1) {
+    const int d = (int)(i % D);
+    offs[d] = make_int2(p0, p1);
+    const uint32_t bar = pass_smem_u32(bars + d);
+    const int np = p1 - p0 < L2P_PCAP ? p1 - p0 : L2P_PCAP;
+    const uint32_t pbytes = np > 0 ? (uint32_t)np * 4u * (uint32_t)sizeof(T) : 0u;
+    const uint32_t tx = p1 > p0 ? BYTES + pbytes : 0u;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tx) : "memory");
+    if (tx) {
+      T *slot = ring + (size_t)d * SLOT;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the slot's earlier lane reads
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              pass_smem_u32(slot)),
+          "l"(F + (warp + i * nwarps) * N3), "r"(BYTES), "r"(bar)
+          : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              pass_smem_u32(slot + N3)),
+          "l"(pos4 + 4 * (int64_t)p0), "r"(pbytes), "r"(bar)
+          : "memory");
+    }
+  };
+  // offsets of leaf j (in the current chunk of leaf i or the next one), from its lane
+  auto offsets_of = [&](int64_t j, int64_t i, int &p0, int &p1) {
+    const bool here = (j >> 5) == (i >> 5);
+    const int a0 = __shfl_sync(0xffffffffu, c0, (int)(j & 31)), a1 = __shfl_sync(0xffffffffu, c1, (int)(j & 31));
+    const int b0 = __shfl_sync(0xffffffffu, n0, (int)(j & 31)), b1 = __shfl_sync(0xffffffffu, n1, (int)(j & 31));
+    p0 = here ? a0 : b0;
+    p1 = here ? a1 : b1;
+  };
+  int64_t nxt = 0;  // next leaf to issue
+  for (; nxt < D && nxt < nmine; ++nxt) {
+    int p0, p1;
+    offsets_of(nxt, 0, p0, p1);
+    if (lane == 0) issue(nxt, p0, p1);
+  }
+  auto wait_slot = [&](int64_t i) -> bool {  // bounded wait for leaf i's slot
+    const uint32_t bar = pass_smem_u32(bars + (int)(i % D));
+    const uint32_t par = (uint32_t)(i / D) & 1u;
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < PASS_WAIT_LIMIT && !done; ++it)
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(bar), "r"(par)
+          : "memory");
+    return done != 0;
+  };
+  int64_t i = 0;
+  for (; i < nmine; ++i) {
+    if (i > 0 && (i & 31) == 0) {  // next chunk: shift, and fetch the one after it
+      cm = nm;
+      c0 = n0;
+      c1 = n1;
+      load_chunk((i >> 5) + 1, nm, n0, n1);
+    }
+    if (!wait_slot(i)) {
+      if (lane == 0) atomicCAS(&g_pass_status, 0, PASS_WAIT_CODE);
+      break;
+    }
+    const int d = (int)(i % D);
+    const int2 po = offs[d];
+    const int64_t m = __shfl_sync(0xffffffffu, cm, (int)(i & 31));
+    if (po.y > po.x) {
+      T fr[PER];
+#pragma unroll
+      for (int k = 0; k < PER; ++k) fr[k] = ring[(size_t)d * SLOT + (lane & (LANES - 1)) + LANES * k];
+      body(m, po.x, po.y, fr, ring + (size_t)d * SLOT + N3);
+    }
+    __syncwarp();  // every lane has used the slot's values
+    if (nxt < nmine) {
+      int p0, p1;
+      offsets_of(nxt, i, p0, p1);
+      if (lane == 0) issue(nxt, p0, p1);
+      ++nxt;
+    }
+  }
+  // a warp that gave up still lets the copies it issued land (each wait bounded) before its
+  // shared memory can be reused
+  for (int64_t j = i + 1; j < nxt; ++j) wait_slot(j);
 }
 
 template <typename T> struct Vec4;
@@ -319,7 +455,6 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
                                                   int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                   T *__restrict__ phi, int64_t m0, int64_t count,
                                                   const int64_t *__restrict__ rows) {
-  constexpr int PER = NN * NN * NN / 32;
   __shared__ T s_tkz[NN * NN];
   const T *tkz = tab_tkz<T>(tabs);
   for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
@@ -331,37 +466,47 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
   const T pre3 = prefac * prefac * prefac;
   using V4 = typename Vec4<T>::type;
   const V4 *p4 = reinterpret_cast<const V4 *>(pos4);
-  l2p_pipeline<T, NN>(leaf_start, F, m0, count, rows, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
+  extern __shared__ __align__(128) unsigned char l2p_ring[];  // l2p_smem_bytes<T, NN>()
+  __shared__ __align__(8) uint64_t l2p_bars[L2P_WARPS * L2P_DEPTH];
+  __shared__ int2 l2p_offs[L2P_WARPS * L2P_DEPTH];
+  // two particles at a time, one per half-warp: lanes s = lane mod 16 of half h hold the
+  // leaf's values s + 16 k, evaluate the half's particle's 3 n S values (two per lane at
+  // most) into shared memory, read the ones their values need, and reduce over the half
+  __shared__ T s_S[L2P_WARPS][2][3 * NN];
+  const int h = lane >> 4, s = lane & 15;
+  T *sS = s_S[threadIdx.x >> 5][h];
+  l2p_pipeline<T, NN, 16>(leaf_start, F, pos4, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars, l2p_offs,
+                          [&](int64_t m, int p0, int p1, const T(&fr)[NN * NN * NN / 16], const T *spos) {
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
             cz = cell_center_1d<T>(iz, maxlev, L);
-    for (int pb = p0; pb < p1; pb += 32) {
-      const int np = min(32, p1 - pb);
-      V4 mine = {};
-      if (lane < np) mine = p4[pb + lane];
-      T res = 0;
-      for (int k = 0; k < np; ++k) {
-        const T x = ihalf * (wshfl(mine.x, k) - cx), y = ihalf * (wshfl(mine.y, k) - cy),
-                z = ihalf * (wshfl(mine.z, k) - cz);
-        const T val = sn_lane<T, NN>(s_tkz, lane, x, y, z);
-        // sum over the lane's F values of F Sx[l1] Sy[l2], then times Sz[l3]
-        T part = 0;
-        if constexpr (NN == 8) {
-          const T sya = wshfl(val, NN + (lane >> 3)), syb = wshfl(val, NN + 4 + (lane >> 3));
+    for (int pb = p0; pb < p1; pb += 2) {
+      const int p = pb + h;
+      const bool has = p < p1;
+      // the slot holds the first L2P_PCAP positions; later ones come from global memory
+      const V4 me = !has ? V4{} : (p - p0 < L2P_PCAP ? reinterpret_cast<const V4 *>(spos)[p - p0] : p4[p]);
+      const T x = ihalf * (me.x - cx), y = ihalf * (me.y - cy), z = ihalf * (me.z - cz);
+      for (int idx = s; idx < 3 * NN; idx += 16) sS[idx] = sn_value<T, NN>(s_tkz, idx, x, y, z);
+      __syncwarp();
+      T part = 0;
+      if constexpr (NN == 8) {  // value s + 16 k: l1 = k / 4, l2 = s / 8 + 2 (k mod 4), l3 = s mod 8
+        T sy[4];
 #pragma unroll
-          for (int a = 0; a < NN; ++a) part += wshfl(val, a) * (fr[2 * a] * sya + fr[2 * a + 1] * syb);
-        } else {
-          const T sy = wshfl(val, NN + f_l2<NN>(0, lane));
+        for (int b = 0; b < 4; ++b) sy[b] = sS[NN + (s >> 3) + 2 * b];
 #pragma unroll
-          for (int kk = 0; kk < PER; ++kk) part += fr[kk] * wshfl(val, f_l1<NN>(kk, lane)) * sy;
-        }
-        part *= wshfl(val, 2 * NN + (lane & (NN - 1)));
+        for (int a = 0; a < NN; ++a)
+          part += sS[a] * (fr[4 * a] * sy[0] + fr[4 * a + 1] * sy[1] + fr[4 * a + 2] * sy[2] + fr[4 * a + 3] * sy[3]);
+      } else {  // n = 4, value s + 16 k: l1 = k, l2 = s / 4, l3 = s mod 4
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-        if (lane == k) res = mine.w * pre3 * part;
+        for (int k = 0; k < NN; ++k) part += fr[k] * sS[k];
+        part *= sS[NN + (s >> 2)];
       }
-      if (lane < np) phi[pb + lane] = res;
+      part *= sS[2 * NN + (s & (NN - 1))];
+#pragma unroll
+      for (int off = 8; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+      if (s == 0 && has) phi[p] = me.w * pre3 * part;
+      __syncwarp();  // sS is rewritten for the next pair
     }
   });
 }
@@ -488,16 +633,29 @@ static int grid_for(int64_t work, int per_block, int cap) {
 // One wave of `kernel` at `threads` per CTA: SMs x resident CTAs per SM (looked up once per
 // kernel), so that grid-stride pipelines run for the whole launch.
 template <auto Kernel>
-static int resident_grid(int threads) {
+static int resident_grid(int threads, int smem = 0) {
   static int blocks = 0;  // one cache per kernel
   if (!blocks) {
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, Kernel, threads, 0);
+    // dynamic plus static shared memory above 48 KB needs the opt-in
+    if (smem > 0) cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, Kernel, threads, smem);
     blocks = sms * (per > 0 ? per : 1);
   }
   return blocks;
+}
+
+// Reads (and with clear, resets) the passes' status word: PASS_WAIT_CODE when an L2P wait gave up.
+int pass_status(int clear) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_pass_status, sizeof(int)) != cudaSuccess) return -1;
+  if (clear && v) {
+    int z = 0;
+    cudaMemcpyToSymbol(g_pass_status, &z, sizeof(int));
+  }
+  return v;
 }
 
 template <typename T>
@@ -556,11 +714,12 @@ int launch_l2p(int n, const T *pos4, const int *leaf_start, int maxlev, T L, con
                cudaStream_t s, int nsets, int64_t first, int64_t count, const int64_t *rows) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
+  constexpr int sm4 = l2p_smem_bytes<T, 4>(), sm8 = l2p_smem_bytes<T, 8>();
   if (n == 4)
-    l2p_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 4>>(128)), 128, 0, s>>>(
+    l2p_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 4>>(128, sm4)), 128, sm4, s>>>(
         pos4, leaf_start, maxlev, L, t, F, phi, first, count, rows);
   else if (n == 8)
-    l2p_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 8>>(128)), 128, 0, s>>>(
+    l2p_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_kernel<T, 8>>(128, sm8)), 128, sm8, s>>>(
         pos4, leaf_start, maxlev, L, t, F, phi, first, count, rows);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p", __FILE__, __LINE__);
@@ -669,7 +828,11 @@ __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ po
   const T pre3 = prefac * prefac * prefac;
   using V4 = typename Vec4<T>::type;
   const V4 *p4 = reinterpret_cast<const V4 *>(pos4);
-  l2p_pipeline<T, NN>(leaf_start, F, m0, count, rows, [&](int64_t m, int p0, int p1, const T(&fr)[PER]) {
+  extern __shared__ __align__(128) unsigned char l2p_ring[];  // l2p_smem_bytes<T, NN>()
+  __shared__ __align__(8) uint64_t l2p_bars[L2P_WARPS * L2P_DEPTH];
+  __shared__ int2 l2p_offs[L2P_WARPS * L2P_DEPTH];
+  l2p_pipeline<T, NN, 32>(leaf_start, F, pos4, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars, l2p_offs,
+                          [&](int64_t m, int p0, int p1, const T(&fr)[PER], const T *spos) {
     int ix, iy, iz;
     morton_to_grid(m, maxlev, ix, iy, iz);
     const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
@@ -677,7 +840,7 @@ __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ po
     for (int pb = p0; pb < p1; pb += 32) {
       const int np = min(32, p1 - pb);
       V4 mine = {};
-      if (lane < np) mine = p4[pb + lane];
+      if (lane < np) mine = pb + lane - p0 < L2P_PCAP ? reinterpret_cast<const V4 *>(spos)[pb + lane - p0] : p4[pb + lane];
       T rv = 0, rx = 0, ry = 0, rz = 0;
       for (int k = 0; k < np; ++k) {
         const T x = ihalf * (wshfl(mine.x, k) - cx), y = ihalf * (wshfl(mine.y, k) - cy),
@@ -761,11 +924,12 @@ int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T 
                      T *pot, T *fld, cudaStream_t s, int nsets, int64_t first, int64_t count, const int64_t *rows) {
   if (count < 0) count = nsets * pow8i(maxlev) - first;
   if (count <= 0) return BBFMM_OK;
+  constexpr int sm4 = l2p_smem_bytes<T, 4>(), sm8 = l2p_smem_bytes<T, 8>();
   if (n == 4)
-    l2p_field_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 4>>(128)), 128, 0, s>>>(
+    l2p_field_kernel<T, 4><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 4>>(128, sm4)), 128, sm4, s>>>(
         pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count, rows);
   else if (n == 8)
-    l2p_field_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 8>>(128)), 128, 0, s>>>(
+    l2p_field_kernel<T, 8><<<grid_for(count, 4, resident_grid<l2p_field_kernel<T, 8>>(128, sm8)), 128, sm8, s>>>(
         pos4, leaf_start, maxlev, L, t, F, pot, fld, first, count, rows);
   else return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "order n must be 4 or 8");
   return bbfmm_set_cuda_error(cudaGetLastError(), "l2p_field", __FILE__, __LINE__);

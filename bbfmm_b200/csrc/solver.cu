@@ -1186,8 +1186,8 @@ int bbfmm_b200_time_m2l(bbfmm_b200_solver *h, int level, int reps, float *ms) {
 }
 
 int bbfmm_b200_device_status(int clear) {
-  const int a = bbfmm::tc_status(clear), b = bbfmm::near_status(clear);
-  return a != 0 ? a : b;
+  const int a = bbfmm::tc_status(clear), b = bbfmm::near_status(clear), c = bbfmm::pass_status(clear);
+  return a != 0 ? a : (b != 0 ? b : c);
 }
 
 int bbfmm_b200_wait_selftest(unsigned limit) {

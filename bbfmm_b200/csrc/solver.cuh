@@ -51,6 +51,7 @@ int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_
                 int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s,
                 const unsigned char *mask = nullptr, int mask_level = 0);
 int near_status(int clear);
+int pass_status(int clear);  // the passes' bounded waits (L2P leaf copies)
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, const int64_t *rows = nullptr);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
 template <typename T> int launch_m2l_simt(int r, const T *M, const T *Ert, T *Lout, int level, int j0, int j1, const int4 *offs, int accumulate, cudaStream_t s, int nsets = 1, int ngroups = 1, T *part = nullptr, int64_t part_elems = 0, const int4 *boxes = nullptr, int nboxes = 0);

@@ -171,10 +171,11 @@ BBFMM_B200_API int bbfmm_b200_direct_field(int N, const double *xyz_dev, const d
                                            const int *targets_dev, double *pot_dev, double *field_dev,
                                            void *stream);
 
-/* Status word of the device kernels: 0 when every bounded wait of every tensor-core launch so
- * far completed and every near-field launch found well-formed leaf offsets, else the code of
- * the first failure: the code of a wait that gave up (the launch then skipped its remaining
- * work and returned), or BBFMM_B200_LEAF_RANGE_CODE when a near-field call was given leaf
+/* Status word of the device kernels: 0 when every bounded wait of every tensor-core launch and
+ * of every L2P launch (its leaf copies) so far completed and every near-field launch found
+ * well-formed leaf offsets, else the code of the first failure: the code of a wait that gave
+ * up (the launch then skipped its remaining work and returned; 31 for an L2P leaf copy), or
+ * BBFMM_B200_LEAF_RANGE_CODE when a near-field call was given leaf
  * offsets that are out of [0, N] or decrease (the kernels clamp every offset, so nothing was
  * read or written outside the caller's arrays). Synchronises the device; clear != 0 resets
  * the word. */
