@@ -39,19 +39,20 @@ __device__ __forceinline__ T sn_lane(const T *__restrict__ tkz, int lane, T x, T
 }
 
 // S(x_m, c) for axis idx / NN (c = x, y, z) and node m = idx % NN, idx < 3 NN: the value
-// lane idx of sn_lane returns.
+// lane idx of sn_lane returns, from the transposed table tkzT[j n + m] = T_j(x_m) (lanes of
+// consecutive nodes read consecutive words).
 template <typename T, int NN>
-__device__ __forceinline__ T sn_value(const T *__restrict__ tkz, int idx, T x, T y, T z) {
+__device__ __forceinline__ T sn_value(const T *__restrict__ tkzT, int idx, T x, T y, T z) {
   const int a = idx / NN, m = idx % NN;
   const T c = a == 0 ? x : (a == 1 ? y : z);
   T d1 = 0, d2 = 0;
 #pragma unroll
   for (int j = NN - 1; j > 0; --j) {
-    const T d0 = 2 * c * d1 - d2 + tkz[m * NN + j];
+    const T d0 = 2 * c * d1 - d2 + tkzT[j * NN + m];
     d2 = d1;
     d1 = d0;
   }
-  return c * d1 - d2 + (T)0.5 * tkz[m * NN];
+  return c * d1 - d2 + (T)0.5 * tkzT[m];
 }
 
 template <typename T>
@@ -312,20 +313,19 @@ __device__ __forceinline__ uint32_t pass_smem_u32(const void *p) { return (uint3
 // slots in shared memory, filled by bulk copies that complete on the slot's mbarrier -- the
 // leaf's n^3 values (one contiguous row of F) and the positions of its first L2P_PCAP
 // particles (contiguous in the sorted order) -- so L2P_DEPTH - 1 leaves, positions included,
-// are on their way from HBM while one is evaluated, without holding them in registers. The warp's leaves are
-// taken in chunks of 32 whose cells and offsets its lanes load together one chunk ahead, so
-// no leaf waits for its own offset loads. Empty leaves take no copy (the slot's barrier is
-// arrived at without bytes). The lane reads of a leaf are coalesced (lane + 32 k),
-// conflict-free: with LANES = 32 lane j holds values j + 32 k, with LANES = 16 both half-warps
-// hold values (j mod 16) + 16 k. body(leaf m, p0, p1, F registers, positions of particles
-// p0 .. p0 + L2P_PCAP - 1 in shared memory) does the arithmetic. A wait that gives up records
+// are on their way from HBM while one is evaluated, without holding them in registers. The
+// warp's leaves are taken in chunks of 32 whose cells and offsets its lanes load together one
+// chunk ahead (and whose centres they compute, one leaf per lane), so no leaf waits for its own
+// offset loads. Empty leaves take no copy (the slot's barrier is arrived at without bytes).
+// body(p0, p1, the slot -- the leaf's n^3 values, then the positions of particles
+// p0 .. p0 + L2P_PCAP - 1 --, leaf centre) does the arithmetic. A wait that gives up records
 // PASS_WAIT_CODE in g_pass_status and ends the warp's work.
-template <typename T, int NN, int LANES, typename Body>
+template <typename T, int NN, typename Body>
 __device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start, const T *__restrict__ F,
-                                             const T *__restrict__ pos4, int64_t m0, int64_t count,
+                                             const T *__restrict__ pos4, int maxlev, T L, int64_t m0, int64_t count,
                                              const int64_t *__restrict__ rows, T *ring_all, uint64_t *bars_all,
                                              int2 *offs_all, Body body) {
-  constexpr int N3 = NN * NN * NN, PER = N3 / LANES, D = L2P_DEPTH, SLOT = l2p_slot_elems<T, NN>();
+  constexpr int N3 = NN * NN * NN, D = L2P_DEPTH, SLOT = l2p_slot_elems<T, NN>();
   static_assert(D < 32, "the slots run at most one offset chunk ahead");
   constexpr uint32_t BYTES = N3 * sizeof(T);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -342,7 +342,8 @@ __device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start,
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
-  // chunk c of 32 leaves: lane j holds leaf 32 c + j's cell and offsets
+  // chunk c of 32 leaves: lane j holds leaf 32 c + j's cell and offsets (loaded one chunk
+  // ahead) and, for the current chunk, its centre
   auto load_chunk = [&](int64_t c, int64_t &m, int &p0, int &p1) {
     const int64_t i = 32 * c + lane;
     m = 0;
@@ -353,10 +354,19 @@ __device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start,
       p1 = leaf_start[m + 1];
     }
   };
+  T ccx, ccy, ccz;  // centre of this lane's leaf of the current chunk
+  auto centre = [&](int64_t m) {
+    int ix, iy, iz;
+    morton_to_grid(m, maxlev, ix, iy, iz);
+    ccx = cell_center_1d<T>(ix, maxlev, L);
+    ccy = cell_center_1d<T>(iy, maxlev, L);
+    ccz = cell_center_1d<T>(iz, maxlev, L);
+  };
   int64_t cm, nm;  // cells of the current chunk and the next one
   int c0, c1, n0, n1;
   load_chunk(0, cm, c0, c1);
   load_chunk(1, nm, n0, n1);
+  centre(cm);
   // lane 0: slot (i % D) <- leaf i, whose offsets are (p0, p1)
   auto issue = [&](int64_t i, int p0, int p1) {
     const int d = (int)(i % D);
@@ -416,6 +426,7 @@ __device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start,
       c0 = n0;
       c1 = n1;
       load_chunk((i >> 5) + 1, nm, n0, n1);
+      centre(cm);
     }
     if (!wait_slot(i)) {
       if (lane == 0) atomicCAS(&g_pass_status, 0, PASS_WAIT_CODE);
@@ -423,12 +434,10 @@ __device__ __forceinline__ void l2p_pipeline(const int *__restrict__ leaf_start,
     }
     const int d = (int)(i % D);
     const int2 po = offs[d];
-    const int64_t m = __shfl_sync(0xffffffffu, cm, (int)(i & 31));
     if (po.y > po.x) {
-      T fr[PER];
-#pragma unroll
-      for (int k = 0; k < PER; ++k) fr[k] = ring[(size_t)d * SLOT + (lane & (LANES - 1)) + LANES * k];
-      body(m, po.x, po.y, fr, ring + (size_t)d * SLOT + N3);
+      const int src = (int)(i & 31);
+      const T cx = wshfl(ccx, src), cy = wshfl(ccy, src), cz = wshfl(ccz, src);
+      body(po.x, po.y, ring + (size_t)d * SLOT, cx, cy, cz);
     }
     __syncwarp();  // every lane has used the slot's values
     if (nxt < nmine) {
@@ -447,17 +456,16 @@ template <typename T> struct Vec4;
 template <> struct Vec4<double> { using type = double4; };
 template <> struct Vec4<float> { using type = float4; };
 
-// One warp per leaf; phi_sorted[p] = q_p (2/n)^3 sum_l F[l] Sx Sy Sz (assign). A leaf's
-// particles are loaded by its lanes at once and broadcast one by one; the S values of a
-// particle come from sn_lane (one Clenshaw evaluation per lane) by shuffles.
+// One warp per leaf; phi_sorted[p] = q_p (2/n)^3 sum_l F[l] Sx Sy Sz (assign), the leaf's
+// values and first positions taken from its ring slot (l2p_pipeline), two particles per pass.
 template <typename T, int NN>
-__global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
+__global__ void __launch_bounds__(128, 4) l2p_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                   int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                   T *__restrict__ phi, int64_t m0, int64_t count,
                                                   const int64_t *__restrict__ rows) {
-  __shared__ T s_tkz[NN * NN];
+  __shared__ T s_tkzT[NN * NN];  // transposed: s_tkzT[j n + m] = T_j(x_m)
   const T *tkz = tab_tkz<T>(tabs);
-  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
+  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkzT[(i % NN) * NN + i / NN] = tkz[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const T len = cell_length<T>(maxlev, L);
@@ -475,19 +483,17 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
   __shared__ T s_S[L2P_WARPS][2][3 * NN];
   const int h = lane >> 4, s = lane & 15;
   T *sS = s_S[threadIdx.x >> 5][h];
-  l2p_pipeline<T, NN, 16>(leaf_start, F, pos4, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars, l2p_offs,
-                          [&](int64_t m, int p0, int p1, const T(&fr)[NN * NN * NN / 16], const T *spos) {
-    int ix, iy, iz;
-    morton_to_grid(m, maxlev, ix, iy, iz);
-    const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
-            cz = cell_center_1d<T>(iz, maxlev, L);
+  l2p_pipeline<T, NN>(leaf_start, F, pos4, maxlev, L, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars,
+                      l2p_offs, [&](int p0, int p1, const T *slot, T cx, T cy, T cz) {
+    const T *spos = slot + NN * NN * NN;
+    const T *sF = slot + s;  // this lane's values s + 16 k are sF[16 k]
     for (int pb = p0; pb < p1; pb += 2) {
       const int p = pb + h;
       const bool has = p < p1;
       // the slot holds the first L2P_PCAP positions; later ones come from global memory
       const V4 me = !has ? V4{} : (p - p0 < L2P_PCAP ? reinterpret_cast<const V4 *>(spos)[p - p0] : p4[p]);
       const T x = ihalf * (me.x - cx), y = ihalf * (me.y - cy), z = ihalf * (me.z - cz);
-      for (int idx = s; idx < 3 * NN; idx += 16) sS[idx] = sn_value<T, NN>(s_tkz, idx, x, y, z);
+      for (int idx = s; idx < 3 * NN; idx += 16) sS[idx] = sn_value<T, NN>(s_tkzT, idx, x, y, z);
       __syncwarp();
       T part = 0;
       if constexpr (NN == 8) {  // value s + 16 k: l1 = k / 4, l2 = s / 8 + 2 (k mod 4), l3 = s mod 8
@@ -496,10 +502,11 @@ __global__ void __launch_bounds__(128) l2p_kernel(const T *__restrict__ pos4, co
         for (int b = 0; b < 4; ++b) sy[b] = sS[NN + (s >> 3) + 2 * b];
 #pragma unroll
         for (int a = 0; a < NN; ++a)
-          part += sS[a] * (fr[4 * a] * sy[0] + fr[4 * a + 1] * sy[1] + fr[4 * a + 2] * sy[2] + fr[4 * a + 3] * sy[3]);
+          part += sS[a] * (sF[64 * a] * sy[0] + sF[64 * a + 16] * sy[1] + sF[64 * a + 32] * sy[2] +
+                           sF[64 * a + 48] * sy[3]);
       } else {  // n = 4, value s + 16 k: l1 = k, l2 = s / 4, l3 = s mod 4
 #pragma unroll
-        for (int k = 0; k < NN; ++k) part += fr[k] * sS[k];
+        for (int k = 0; k < NN; ++k) part += sF[16 * k] * sS[k];
         part *= sS[NN + (s >> 2)];
       }
       part *= sS[2 * NN + (s & (NN - 1))];
@@ -812,7 +819,7 @@ __device__ __forceinline__ void sn_lane_d(const T *__restrict__ tkz, int lane, T
 // fld[3p + a] = d pot / d x_a, with the chain factor 2 / leaf length of the leaf map; the
 // same load pipeline as l2p_kernel.
 template <typename T, int NN>
-__global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
+__global__ void __launch_bounds__(128, 4) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                         int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                         T *__restrict__ pot, T *__restrict__ fld, int64_t m0,
                                                         int64_t count, const int64_t *__restrict__ rows) {
@@ -831,12 +838,12 @@ __global__ void __launch_bounds__(128) l2p_field_kernel(const T *__restrict__ po
   extern __shared__ __align__(128) unsigned char l2p_ring[];  // l2p_smem_bytes<T, NN>()
   __shared__ __align__(8) uint64_t l2p_bars[L2P_WARPS * L2P_DEPTH];
   __shared__ int2 l2p_offs[L2P_WARPS * L2P_DEPTH];
-  l2p_pipeline<T, NN, 32>(leaf_start, F, pos4, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars, l2p_offs,
-                          [&](int64_t m, int p0, int p1, const T(&fr)[PER], const T *spos) {
-    int ix, iy, iz;
-    morton_to_grid(m, maxlev, ix, iy, iz);
-    const T cx = cell_center_1d<T>(ix, maxlev, L), cy = cell_center_1d<T>(iy, maxlev, L),
-            cz = cell_center_1d<T>(iz, maxlev, L);
+  l2p_pipeline<T, NN>(leaf_start, F, pos4, maxlev, L, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars,
+                      l2p_offs, [&](int p0, int p1, const T *slot, T cx, T cy, T cz) {
+    const T *spos = slot + NN * NN * NN;
+    T fr[PER];  // lane's values lane + 32 k
+#pragma unroll
+    for (int k = 0; k < PER; ++k) fr[k] = slot[lane + 32 * k];
     for (int pb = p0; pb < p1; pb += 32) {
       const int np = min(32, p1 - pb);
       V4 mine = {};
