@@ -47,6 +47,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_solve.argtypes = [vp, vp, vp]
         L.bbfmm_b200_solve_host.argtypes = [vp, vp, vp]
         L.bbfmm_b200_solve_fields.argtypes = [vp, vp, vp, vp]
+        L.bbfmm_b200_solve_fields2.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.bbfmm_b200_set_timing.argtypes = [vp, i]
         L.bbfmm_b200_stage_times.argtypes = [vp, C.POINTER(C.c_float), i]
         L.bbfmm_b200_copy_multipoles.argtypes = [vp, i, vp]

@@ -14,7 +14,8 @@ Two ways to get pot(q) and field(q) to the backward (``save``):
                field (4 values per particle); the backward is ONE more solve, with charges
                g o q.
   "recompute"  the forward runs the plain solve and keeps nothing but q; the backward
-               solves twice (charges q and g o q).
+               solves for both charge vectors q and g o q in one call (solve_fields2:
+               two far fields, one near-field pass over the pairs for both).
 
 Neither keeps per-level expansions between the passes (each solve rebuilds them on the
 device in its own work buffers), so the saved state is O(N) either way.
@@ -45,14 +46,18 @@ class _FMMPhi(torch.autograd.Function):
         q, pot, fld = ctx.saved_tensors
         solver = ctx.solver
         if ctx.recompute:
-            pot, fld = solver.solve_fields(q, want_field=ctx.need_field)
-        g = g.to(pot.dtype).contiguous()
-        q = q.to(pot.dtype)
-        pot2, fld2 = solver.solve_fields(g * q, want_field=ctx.need_field)
-        dq = g * pot + pot2 if ctx.needs_input_grad[0] else None
+            qs = q.to(solver.dtype)
+            g = g.to(solver.dtype).contiguous()
+            pot, fld, pot2, fld2 = solver.solve_fields2(qs, g * qs, want_field=ctx.need_field)
+            q = qs
+        else:
+            g = g.to(pot.dtype).contiguous()
+            q = q.to(pot.dtype)
+            pot2, fld2 = solver.solve_fields(g * q, want_field=ctx.need_field)
+        dq = torch.addcmul(pot2, g, pot) if ctx.needs_input_grad[0] else None
         dx = None
         if ctx.needs_input_grad[1] and ctx.need_field:
-            dx = q[:, None] * (g[:, None] * fld + fld2)
+            dx = torch.addcmul(fld2, fld, g[:, None]).mul_(q[:, None])
         return dq, dx, None, None, None
 
 

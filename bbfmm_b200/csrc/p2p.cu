@@ -154,6 +154,71 @@ struct NearAcc {
       for (int k = 0; k < 4; ++k) accum(term(fx, fy, fz, g[k]));
     }
   }
+  // Two charge vectors (FIELD, 1/r): the pair's geometry once; this accumulator takes the
+  // staged charge and o the source's second charge q2, each with the arithmetic of term/add.
+  __device__ __forceinline__ void add2(NearAcc &o, C fx, C fy, C fz, const Src &g, A q2) {
+    static_assert(FIELD && H == 1, "two charge vectors: potentials and fields of 1/r");
+    const C ex = g.x - fx, ey = g.y - fy, ez = g.z - fz;
+    if constexpr (MODE == MODE_MIXED) {
+      const double rr = fma(ex, ex, fma(ey, ey, ez * ez));
+      const float rrf = (float)rr;
+      const float rinv = rrf > 0.f ? rsqrt_nr(rrf) : 0.f;
+      const float t = __fmul_rn(g.q, rinv), u = __fmul_rn(q2, rinv);
+      const float t3 = t * rinv * rinv, u3 = u * rinv * rinv;
+      gx += t3 * (float)ex;
+      gy += t3 * (float)ey;
+      gz += t3 * (float)ez;
+      o.gx += u3 * (float)ex;
+      o.gy += u3 * (float)ey;
+      o.gz += u3 * (float)ez;
+      accum(t);
+      o.accum(u);
+    } else {
+      const C rr = ex * ex + ey * ey + ez * ez;
+      if (rr == (C)0) return;  // both terms 0, as add adds
+      const C rinv = (C)1 / sqrt(rr);
+      const C qr = g.w * rinv, qr3 = qr * rinv * rinv;
+      const C ur = q2 * rinv, ur3 = ur * rinv * rinv;
+      gx += qr3 * ex;
+      gy += qr3 * ey;
+      gz += qr3 * ez;
+      o.gx += ur3 * ex;
+      o.gy += ur3 * ey;
+      o.gz += ur3 * ez;
+      accum(qr);
+      o.accum(ur);
+    }
+  }
+  // add4 for two charge vectors: the same grouping of the four terms in each sum.
+  __device__ __forceinline__ void add2x4(NearAcc &o, C fx, C fy, C fz, const Src *g, const A *q2) {
+    if constexpr (MODE == MODE_MIXED) {
+      NearAcc a = *this, b = o;  // the gradients accumulate term by term; the potentials in fours
+      float t[4], u[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const C ex = g[k].x - fx, ey = g[k].y - fy, ez = g[k].z - fz;
+        const double rr = fma(ex, ex, fma(ey, ey, ez * ez));
+        const float rrf = (float)rr;
+        const float rinv = rrf > 0.f ? rsqrt_nr(rrf) : 0.f;
+        t[k] = __fmul_rn(g[k].q, rinv);
+        u[k] = __fmul_rn(q2[k], rinv);
+        const float t3 = t[k] * rinv * rinv, u3 = u[k] * rinv * rinv;
+        a.gx += t3 * (float)ex;
+        a.gy += t3 * (float)ey;
+        a.gz += t3 * (float)ez;
+        b.gx += u3 * (float)ex;
+        b.gy += u3 * (float)ey;
+        b.gz += u3 * (float)ez;
+      }
+      a.accum((t[0] + t[1]) + (t[2] + t[3]));
+      b.accum((u[0] + u[1]) + (u[2] + u[3]));
+      *this = a;
+      o = b;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) add2(o, fx, fy, fz, g[k], q2[k]);
+    }
+  }
   // potential part in the output precision
   __device__ __forceinline__ typename T::R pot() const {
     if constexpr (MODE == MODE_MIXED) return (double)v + (double)c;
@@ -337,21 +402,28 @@ int near_work_build(int N, const int *leaf_start, int maxlev, int nsets, int thr
 }
 
 // ------------------------------------------------------------------ the near-field kernel
-template <int MODE, int H, bool FIELD>
+// RHS2: a second charge vector q2 (sorted order) whose potentials and fields go to pot2 and
+// fld2, from the same pair evaluations.
+template <int MODE, int H, bool FIELD, bool RHS2 = false>
 __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTypes<MODE>::P4 *__restrict__ pos4,
                                                    const int *__restrict__ leaf_start, int maxlev,
                                                    const int2 *__restrict__ items, int nitems,
                                                    typename NearTypes<MODE>::R *__restrict__ pot,
                                                    typename NearTypes<MODE>::R *__restrict__ fld, int *flag,
-                                                   const unsigned char *__restrict__ mask, int mask_shift) {
+                                                   const unsigned char *__restrict__ mask, int mask_shift,
+                                                   const typename NearTypes<MODE>::R *__restrict__ q2 = nullptr,
+                                                   typename NearTypes<MODE>::R *__restrict__ pot2 = nullptr,
+                                                   typename NearTypes<MODE>::R *__restrict__ fld2 = nullptr) {
   using NT = NearTypes<MODE>;
   using P4 = typename NT::P4;
   using C = typename NT::C;
   using R = typename NT::R;
   using Src = typename NT::S;
   using Acc = NearAcc<MODE, H, FIELD>;
+  using A = typename NT::A;
   static_assert(sizeof(Acc) * 256 <= sizeof(Src) * P2P_TILE, "group partials fit the tile buffer");
   __shared__ __align__(16) unsigned char s_buf[sizeof(Src) * P2P_TILE];
+  __shared__ A s_q2[RHS2 ? P2P_TILE : 1];  // the staged sources' second charges
   __shared__ int s_start[P2P_REGION], s_off[P2P_REGION + 1];
   __shared__ unsigned char s_tleaf[512], s_act[P2P_REGION];
   Src *s_src = reinterpret_cast<Src *>(s_buf);
@@ -446,12 +518,13 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
     const int g = dense && ntg > 0 ? nt / ntg : 1;
     const int slot = dense && ntg > 0 ? tid % ntg : tid, grp = dense && ntg > 0 ? tid / ntg : 0;
     const bool active = dense ? (ntg > 0 && grp < g) : true;
-    Acc acc[2];
+    Acc acc[2], acc2[2];
     C fx[2], fy[2], fz[2];
     int trho[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       acc[k].zero();
+      acc2[k].zero();
       fx[k] = fy[k] = fz[k] = (C)0;
       trho[k] = 255;
       const int i = t0 + slot + k * nt;
@@ -472,7 +545,9 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
           if (s_off[mid] <= v) lo = mid;
           else hi = mid;
         }
-        s_src[k] = stage_src<MODE>(pos4[s_start[lo] + (v - s_off[lo])]);
+        const int src = s_start[lo] + (v - s_off[lo]);
+        s_src[k] = stage_src<MODE>(pos4[src]);
+        if constexpr (RHS2) s_q2[k] = (A)q2[src];
       }
       __syncthreads();
       if (dense) {
@@ -480,8 +555,13 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
           // group grp takes the contiguous slice [j0, j1) of the tile
           const int j0 = (int)((int64_t)tn * grp / g), j1 = (int)((int64_t)tn * (grp + 1) / g);
           int j = j0;
-          for (; j + 4 <= j1; j += 4) acc[0].add4(fx[0], fy[0], fz[0], s_src + j);
-          for (; j < j1; ++j) acc[0].add(fx[0], fy[0], fz[0], s_src[j]);
+          if constexpr (RHS2) {
+            for (; j + 4 <= j1; j += 4) acc[0].add2x4(acc2[0], fx[0], fy[0], fz[0], s_src + j, s_q2 + j);
+            for (; j < j1; ++j) acc[0].add2(acc2[0], fx[0], fy[0], fz[0], s_src[j], s_q2[j]);
+          } else {
+            for (; j + 4 <= j1; j += 4) acc[0].add4(fx[0], fy[0], fz[0], s_src + j);
+            for (; j < j1; ++j) acc[0].add(fx[0], fy[0], fz[0], s_src[j]);
+          }
         }
       } else {
 #pragma unroll
@@ -503,7 +583,8 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
               run(u, j, e);
               continue;
             }
-            acc[k].add(fx[k], fy[k], fz[k], s_src[j]);
+            if constexpr (RHS2) acc[k].add2(acc2[k], fx[k], fy[k], fz[k], s_src[j], s_q2[j]);
+            else acc[k].add(fx[k], fy[k], fz[k], s_src[j]);
             ++j;
           }
         }
@@ -513,30 +594,35 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
     if (dense) {
       if (ntg <= 0) continue;
       Acc *red = reinterpret_cast<Acc *>(s_buf);
-      __syncthreads();  // the last tile is consumed
-      if (active) red[tid] = acc[0];
-      __syncthreads();
-      if (tid < ntg) {
-        R p = (R)0, qx = (R)0, qy = (R)0, qz = (R)0;
-        for (int k = 0; k < g; ++k) {
-          const Acc &a = red[tid + k * ntg];
-          p += a.pot();
+      // the groups' partial sums of one charge vector, added in a fixed order
+      auto flush = [&](const Acc &mine, R *po, R *fl) {
+        __syncthreads();  // the last tile (or the previous flush) is consumed
+        if (active) red[tid] = mine;
+        __syncthreads();
+        if (tid < ntg) {
+          R p = (R)0, qx = (R)0, qy = (R)0, qz = (R)0;
+          for (int k = 0; k < g; ++k) {
+            const Acc &a = red[tid + k * ntg];
+            p += a.pot();
+            if constexpr (FIELD) {
+              qx += (R)a.gx;
+              qy += (R)a.gy;
+              qz += (R)a.gz;
+            }
+          }
+          const int i = t0 + tid;
           if constexpr (FIELD) {
-            qx += (R)a.gx;
-            qy += (R)a.gy;
-            qz += (R)a.gz;
+            po[i] += p;
+            fl[3 * (int64_t)i] += qx;
+            fl[3 * (int64_t)i + 1] += qy;
+            fl[3 * (int64_t)i + 2] += qz;
+          } else {
+            po[i] += (R)pos4[i].w * p;
           }
         }
-        const int i = t0 + tid;
-        if constexpr (FIELD) {
-          pot[i] += p;
-          fld[3 * (int64_t)i] += qx;
-          fld[3 * (int64_t)i + 1] += qy;
-          fld[3 * (int64_t)i + 2] += qz;
-        } else {
-          pot[i] += (R)pos4[i].w * p;
-        }
-      }
+      };
+      flush(acc[0], pot, fld);
+      if constexpr (RHS2) flush(acc2[0], pot2, fld2);
     } else {
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
@@ -547,6 +633,12 @@ __global__ void __launch_bounds__(256) near_kernel(int N, const typename NearTyp
           fld[3 * (int64_t)i] += (R)acc[k].gx;
           fld[3 * (int64_t)i + 1] += (R)acc[k].gy;
           fld[3 * (int64_t)i + 2] += (R)acc[k].gz;
+          if constexpr (RHS2) {
+            pot2[i] += acc2[k].pot();
+            fld2[3 * (int64_t)i] += (R)acc2[k].gx;
+            fld2[3 * (int64_t)i + 1] += (R)acc2[k].gy;
+            fld2[3 * (int64_t)i + 2] += (R)acc2[k].gz;
+          }
         } else {
           pot[i] += (R)pos4[i].w * acc[k].pot();
         }
@@ -588,6 +680,35 @@ int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_
   else return bbfmm_set_error(BBFMM_ERR_ARG, "near field: unknown precision mode");
 #undef NEAR_CASE
   return bbfmm_set_cuda_error(cudaGetLastError(), "near field", __FILE__, __LINE__);
+}
+
+// Potentials and fields of 1/r for two charge vectors in one pass over the pairs: the charges
+// in pos4's fourth component into (pot, fld), the sorted charges q2 into (pot2, fld2), each
+// added and each with the arithmetic of a launch_near call of its own.
+int launch_near2(int mode, int N, const void *pos4, const int *leaf_start, int maxlev, const void *work, int nsets,
+                 int nitems, int threads, const void *q2, void *pot, void *fld, void *pot2, void *fld2, cudaStream_t s,
+                 const unsigned char *mask, int mask_level) {
+  const int mask_shift = mask ? 3 * (maxlev - mask_level) : 0;
+  if (N <= 0 || nitems <= 0) return BBFMM_OK;
+  if (threads != 64 && threads != 128 && threads != 256)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "near field: 64, 128 or 256 threads per block");
+  if (!q2 || !pot || !fld || !pot2 || !fld2) return bbfmm_set_error(BBFMM_ERR_ARG, "near field: null pointer");
+  const int2 *items = near_work_items(work, maxlev, nsets);
+  int *flag = near_work_flag(const_cast<void *>(work));
+#define NEAR2_CASE(M)                                                                                       \
+  {                                                                                                          \
+    using NT = NearTypes<M>;                                                                                 \
+    using R = typename NT::R;                                                                                \
+    near_kernel<M, 1, true, true><<<nitems, threads, 0, s>>>(                                                \
+        N, (const typename NT::P4 *)pos4, leaf_start, maxlev, items, nitems, (R *)pot, (R *)fld, flag, mask, \
+        mask_shift, (const R *)q2, (R *)pot2, (R *)fld2);                                                    \
+  }
+  if (mode == MODE_D) NEAR2_CASE(MODE_D)
+  else if (mode == MODE_S) NEAR2_CASE(MODE_S)
+  else if (mode == MODE_MIXED) NEAR2_CASE(MODE_MIXED)
+  else return bbfmm_set_error(BBFMM_ERR_ARG, "near field: unknown precision mode");
+#undef NEAR2_CASE
+  return bbfmm_set_cuda_error(cudaGetLastError(), "near field (two charge vectors)", __FILE__, __LINE__);
 }
 
 // Reads and clears this file's status word (0, or LEAF_RANGE_CODE after malformed offsets).

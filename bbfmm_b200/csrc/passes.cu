@@ -284,15 +284,6 @@ __global__ void __launch_bounds__(256) l2l_kernel(const T *__restrict__ Fp, T *_
 }
 
 // ----------------------------------------------------------------------------- L2P
-// Lane share of a leaf's F (n^3 values, l = (l1 n + l2) n + l3) when a warp loads it
-// coalesced, lane + 32 k for k < n^3 / 32: l3 = lane % n for every k (32 % n == 0); for n = 8,
-// l1 = k / 2 and l2 = 4 (k % 2) + lane / 8; for n = 4, l1 = 2 k + lane / 16 and
-// l2 = (lane / 4) % 4.
-template <int NN> __device__ __forceinline__ int f_l1(int k, int lane) { return NN == 8 ? k >> 1 : 2 * k + (lane >> 4); }
-template <int NN> __device__ __forceinline__ int f_l2(int k, int lane) {
-  return NN == 8 ? 4 * (k & 1) + (lane >> 3) : (lane >> 2) & 3;
-}
-
 // Status word of the passes' bounded waits (0 = every wait completed).
 __device__ int g_pass_status = 0;
 constexpr uint32_t PASS_WAIT_LIMIT = 1u << 26;
@@ -782,6 +773,37 @@ int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaS
   template int launch_morton_cpg<T>(int, int, const T *, T *, int, cudaStream_t);
 INST(float)
 INST(double)
+// y[i] += x[i].
+template <typename T>
+__global__ void add_kernel(int64_t n, const T *__restrict__ x, T *__restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+template <typename T>
+int launch_add(int64_t n, const T *x, T *y, cudaStream_t s) {
+  if (n <= 0) return BBFMM_OK;
+  add_kernel<T><<<grid_for(n, 256, 148 * 32), 256, 0, s>>>(n, x, y);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "add", __FILE__, __LINE__);
+}
+template int launch_add<double>(int64_t, const double *, double *, cudaStream_t);
+template int launch_add<float>(int64_t, const float *, float *, cudaStream_t);
+
+// q[i] = the charge of sorted particle i (pos4's fourth component).
+template <typename T>
+__global__ void charges_of_kernel(int N, const T *__restrict__ pos4, T *__restrict__ q) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) q[i] = pos4[4 * (int64_t)i + 3];
+}
+
+template <typename T>
+int launch_charges_of(int N, const T *pos4, T *q, cudaStream_t s) {
+  if (N <= 0) return BBFMM_OK;
+  charges_of_kernel<T><<<grid_for(N, 256, 148 * 32), 256, 0, s>>>(N, pos4, q);
+  return bbfmm_set_cuda_error(cudaGetLastError(), "charges", __FILE__, __LINE__);
+}
+template int launch_charges_of<double>(int, const double *, double *, cudaStream_t);
+template int launch_charges_of<float>(int, const float *, float *, cudaStream_t);
+
 template int launch_gather<double, double>(int, const int *, const double *, const double *, double *, cudaStream_t);
 template int launch_gather<float, double>(int, const int *, const double *, const double *, float *, cudaStream_t);
 template int launch_gather<float, float>(int, const int *, const float *, const float *, float *, cudaStream_t);
@@ -796,37 +818,35 @@ template int launch_scatter<double, float>(int, const int *, const double *, flo
 // ------------------------------------------------------------ L2P with gradient
 namespace bbfmm {
 
-// sn_lane and dS/dc: the Clenshaw recurrence differentiated term by term (e_j = d'_j).
+// S and dS/dc of sn_value for idx < 3 NN, from the transposed table tkzT[j n + m] = T_j(x_m):
+// the Clenshaw recurrence differentiated term by term (e_j = d'_j).
 template <typename T, int NN>
-__device__ __forceinline__ void sn_lane_d(const T *__restrict__ tkz, int lane, T x, T y, T z, T &sv, T &dv) {
-  sv = dv = (T)0;
-  if (lane >= 3 * NN) return;
-  const int a = lane / NN, m = lane % NN;
+__device__ __forceinline__ void sn_value_d(const T *__restrict__ tkzT, int idx, T x, T y, T z, T &sv, T &dv) {
+  const int a = idx / NN, m = idx % NN;
   const T c = a == 0 ? x : (a == 1 ? y : z);
   T d1 = 0, d2 = 0, e1 = 0, e2 = 0;
 #pragma unroll
   for (int j = NN - 1; j > 0; --j) {
-    const T d0 = 2 * c * d1 - d2 + tkz[m * NN + j];
+    const T d0 = 2 * c * d1 - d2 + tkzT[j * NN + m];
     const T e0 = 2 * d1 + 2 * c * e1 - e2;
     d2 = d1; d1 = d0;
     e2 = e1; e1 = e0;
   }
-  sv = c * d1 - d2 + (T)0.5 * tkz[m * NN];
+  sv = c * d1 - d2 + (T)0.5 * tkzT[m];
   dv = d1 + c * e1 - e2;
 }
 
 // One warp per leaf: pot[p] = (2/n)^3 sum_l F[l] Sx Sy Sz (no target factor) and
 // fld[3p + a] = d pot / d x_a, with the chain factor 2 / leaf length of the leaf map; the
-// same load pipeline as l2p_kernel.
+// same pipeline and particle pairs as l2p_kernel, each half-warp also evaluating dS.
 template <typename T, int NN>
 __global__ void __launch_bounds__(128, 4) l2p_field_kernel(const T *__restrict__ pos4, const int *__restrict__ leaf_start,
                                                         int maxlev, T L, Tables tabs, const T *__restrict__ F,
                                                         T *__restrict__ pot, T *__restrict__ fld, int64_t m0,
                                                         int64_t count, const int64_t *__restrict__ rows) {
-  constexpr int PER = NN * NN * NN / 32;
-  __shared__ T s_tkz[NN * NN];
+  __shared__ T s_tkzT[NN * NN];  // transposed: s_tkzT[j n + m] = T_j(x_m)
   const T *tkz = tab_tkz<T>(tabs);
-  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkz[i] = tkz[i];
+  for (int i = threadIdx.x; i < NN * NN; i += blockDim.x) s_tkzT[(i % NN) * NN + i / NN] = tkz[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const T len = cell_length<T>(maxlev, L);
@@ -838,75 +858,72 @@ __global__ void __launch_bounds__(128, 4) l2p_field_kernel(const T *__restrict__
   extern __shared__ __align__(128) unsigned char l2p_ring[];  // l2p_smem_bytes<T, NN>()
   __shared__ __align__(8) uint64_t l2p_bars[L2P_WARPS * L2P_DEPTH];
   __shared__ int2 l2p_offs[L2P_WARPS * L2P_DEPTH];
+  // S and dS of the half-warp's particle (3 n each)
+  __shared__ T s_S[L2P_WARPS][2][3 * NN], s_D[L2P_WARPS][2][3 * NN];
+  const int h = lane >> 4, s = lane & 15;
+  T *sS = s_S[threadIdx.x >> 5][h], *sD = s_D[threadIdx.x >> 5][h];
   l2p_pipeline<T, NN>(leaf_start, F, pos4, maxlev, L, m0, count, rows, reinterpret_cast<T *>(l2p_ring), l2p_bars,
                       l2p_offs, [&](int p0, int p1, const T *slot, T cx, T cy, T cz) {
     const T *spos = slot + NN * NN * NN;
-    T fr[PER];  // lane's values lane + 32 k
+    const T *sF = slot + s;  // this lane's values s + 16 k are sF[16 k]
+    for (int pb = p0; pb < p1; pb += 2) {
+      const int p = pb + h;
+      const bool has = p < p1;
+      const V4 me = !has ? V4{} : (p - p0 < L2P_PCAP ? reinterpret_cast<const V4 *>(spos)[p - p0] : p4[p]);
+      const T x = ihalf * (me.x - cx), y = ihalf * (me.y - cy), z = ihalf * (me.z - cz);
+      for (int idx = s; idx < 3 * NN; idx += 16) sn_value_d<T, NN>(s_tkzT, idx, x, y, z, sS[idx], sD[idx]);
+      __syncwarp();
+      // per l1 row a: A = sum F Sy[l2], B = sum F dSy[l2]; then v = sum Sx A, gx = sum dSx A,
+      // gy = sum Sx B (times Sz, or dSz for gz, below)
+      T v = 0, gx = 0, gy = 0;
+      if constexpr (NN == 8) {  // value s + 16 k: l1 = k / 4, l2 = s / 8 + 2 (k mod 4), l3 = s mod 8
+        T sy[4], dy[4];
 #pragma unroll
-    for (int k = 0; k < PER; ++k) fr[k] = slot[lane + 32 * k];
-    for (int pb = p0; pb < p1; pb += 32) {
-      const int np = min(32, p1 - pb);
-      V4 mine = {};
-      if (lane < np) mine = pb + lane - p0 < L2P_PCAP ? reinterpret_cast<const V4 *>(spos)[pb + lane - p0] : p4[pb + lane];
-      T rv = 0, rx = 0, ry = 0, rz = 0;
-      for (int k = 0; k < np; ++k) {
-        const T x = ihalf * (wshfl(mine.x, k) - cx), y = ihalf * (wshfl(mine.y, k) - cy),
-                z = ihalf * (wshfl(mine.z, k) - cz);
-        T vs, vd;
-        sn_lane_d<T, NN>(s_tkz, lane, x, y, z, vs, vd);
-        // per l1 row: A = sum F Sy[l2], B = sum F dSy[l2]; then v = sum Sx A, gx = sum dSx A,
-        // gy = sum Sx B (times Sz or dSz below)
-        T v = 0, gx = 0, gy = 0;
-        if constexpr (NN == 8) {
-          const int ba = NN + (lane >> 3), bb = NN + 4 + (lane >> 3);
-          const T sya = wshfl(vs, ba), syb = wshfl(vs, bb), dya = wshfl(vd, ba), dyb = wshfl(vd, bb);
-#pragma unroll
-          for (int a = 0; a < NN; ++a) {
-            const T A = fr[2 * a] * sya + fr[2 * a + 1] * syb, B = fr[2 * a] * dya + fr[2 * a + 1] * dyb;
-            const T sx = wshfl(vs, a), dx = wshfl(vd, a);
-            v += sx * A;
-            gx += dx * A;
-            gy += sx * B;
-          }
-        } else {
-          const int b = NN + f_l2<NN>(0, lane);
-          const T sy = wshfl(vs, b), dy = wshfl(vd, b);
-#pragma unroll
-          for (int kk = 0; kk < PER; ++kk) {
-            const int a = f_l1<NN>(kk, lane);
-            const T sx = wshfl(vs, a), dx = wshfl(vd, a);
-            v += fr[kk] * sx * sy;
-            gx += fr[kk] * dx * sy;
-            gy += fr[kk] * sx * dy;
-          }
+        for (int b = 0; b < 4; ++b) {
+          sy[b] = sS[NN + (s >> 3) + 2 * b];
+          dy[b] = sD[NN + (s >> 3) + 2 * b];
         }
-        const int c = 2 * NN + (lane & (NN - 1));
-        const T sz = wshfl(vs, c), dz = wshfl(vd, c);
-        T gz = v * dz;
-        v *= sz;
-        gx *= sz;
-        gy *= sz;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          v += __shfl_xor_sync(0xffffffffu, v, off);
-          gx += __shfl_xor_sync(0xffffffffu, gx, off);
-          gy += __shfl_xor_sync(0xffffffffu, gy, off);
-          gz += __shfl_xor_sync(0xffffffffu, gz, off);
+        for (int a = 0; a < NN; ++a) {
+          const T f0 = sF[64 * a], f1 = sF[64 * a + 16], f2 = sF[64 * a + 32], f3 = sF[64 * a + 48];
+          const T A = f0 * sy[0] + f1 * sy[1] + f2 * sy[2] + f3 * sy[3];
+          const T B = f0 * dy[0] + f1 * dy[1] + f2 * dy[2] + f3 * dy[3];
+          v += sS[a] * A;
+          gx += sD[a] * A;
+          gy += sS[a] * B;
         }
-        if (lane == k) {
-          rv = pre3 * v;
-          rx = pre3 * ihalf * gx;
-          ry = pre3 * ihalf * gy;
-          rz = pre3 * ihalf * gz;
+      } else {  // n = 4, value s + 16 k: l1 = k, l2 = s / 4, l3 = s mod 4
+        T A = 0, Bx = 0;
+#pragma unroll
+        for (int k = 0; k < NN; ++k) {
+          A += sF[16 * k] * sS[k];
+          Bx += sF[16 * k] * sD[k];
         }
+        const T sy = sS[NN + (s >> 2)], dy = sD[NN + (s >> 2)];
+        v = A * sy;
+        gx = Bx * sy;
+        gy = A * dy;
       }
-      if (lane < np) {
-        const int64_t p = pb + lane;
-        pot[p] = rv;
-        fld[3 * p] = rx;
-        fld[3 * p + 1] = ry;
-        fld[3 * p + 2] = rz;
+      const int c = 2 * NN + (s & (NN - 1));
+      const T sz = sS[c], dz = sD[c];
+      T gz = v * dz;
+      v *= sz;
+      gx *= sz;
+      gy *= sz;
+#pragma unroll
+      for (int off = 8; off > 0; off >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+        gx += __shfl_xor_sync(0xffffffffu, gx, off);
+        gy += __shfl_xor_sync(0xffffffffu, gy, off);
+        gz += __shfl_xor_sync(0xffffffffu, gz, off);
       }
+      if (s == 0 && has) {
+        pot[p] = pre3 * v;
+        fld[3 * (int64_t)p] = pre3 * ihalf * gx;
+        fld[3 * (int64_t)p + 1] = pre3 * ihalf * gy;
+        fld[3 * (int64_t)p + 2] = pre3 * ihalf * gz;
+      }
+      __syncwarp();  // sS, sD are rewritten for the next pair
     }
   });
 }

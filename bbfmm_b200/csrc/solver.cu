@@ -293,6 +293,9 @@ int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const
   near_work = nullptr;
   near_items = near_threads = 0;
   if (flds) cudaFree(flds);  // sized 3 N: reallocated by the next solve_fields
+  for (T *p : {phis2, flds2, qs2, phisn, fldsn})
+    if (p) cudaFree(p);
+  phis2 = flds2 = qs2 = phisn = fldsn = nullptr;
   if (io_q) cudaFree(io_q);  // sized N: reallocated by the next host-buffer solve
   if (io_phi) cudaFree(io_phi);
   io_q = io_phi = nullptr;
@@ -332,6 +335,9 @@ int Solver<T>::set_particles_device(int N_, const T *xyz_d) {
   near_work = nullptr;
   near_items = near_threads = 0;
   if (flds) cudaFree(flds);
+  for (T *p : {phis2, flds2, qs2, phisn, fldsn})
+    if (p) cudaFree(p);
+  phis2 = flds2 = qs2 = phisn = fldsn = nullptr;
   if (io_q) cudaFree(io_q);
   if (io_phi) cudaFree(io_phi);
   io_q = io_phi = nullptr;
@@ -827,12 +833,87 @@ int Solver<T>::solve_fields(const void *q_dev, void *pot_dev, void *fld_dev) {
   if (!Ert) return bbfmm_set_error(BBFMM_ERR_STATE, "operators not set");
   if (!flds) TRY(dalloc(&flds, 3 * (size_t)(N > 0 ? N : 1)));
   kernel_launches = 0;
+  if (timing) {  // stage times of this call alone, as solve keeps them
+    for (int i = 0; i < ST_COUNT; ++i) stage_ms[i] = 0.f;
+    if (!ev[ST_COUNT]) cudaEventCreate(&ev[ST_COUNT]);
+    mark(-1, 0);
+  }
   TRY(upward(q_dev, sizeof(T) == 8));
   TRY(interaction(m2l_first, maxlev));
   const Tables tb = tables();
   TRY(leaf_down(true));
   TRY(near(phis, flds));
   TRY((launch_scatter_field<T, T>(N, perm, phis, flds, (T *)pot_dev, (T *)fld_dev, stream)));
+  mark(ST_SCATTER);
+  return BBFMM_OK;
+}
+
+// Both far fields one after the other (each through the passes of solve_fields) and one
+// near-field pass with both charge vectors: each pair's separation, distance and powers are
+// computed once for both (the backward of a recomputing gradient needs pot and field for the
+// charges q and g o q). The near-field pass needs only the sorted positions and charges, so it
+// runs on a second stream while the second far field runs (in its own output buffers, added
+// afterwards; with stage timing on, after it on the solver's stream). Results equal those of
+// two solve_fields calls.
+template <typename T>
+int Solver<T>::solve_fields2(const void *q1_dev, const void *q2_dev, void *pot1_dev, void *fld1_dev, void *pot2_dev,
+                             void *fld2_dev) {
+  if (!pos4) return bbfmm_set_error(BBFMM_ERR_STATE, "particles not set");
+  if (homogen != 1) return bbfmm_set_error(BBFMM_ERR_UNSUPPORTED, "fields are computed for the 1/r kernel");
+  if (!Ert) return bbfmm_set_error(BBFMM_ERR_STATE, "operators not set");
+  const size_t n1 = N > 0 ? N : 1;
+  for (auto pr : {std::make_pair(&flds, 3 * n1), std::make_pair(&phis2, n1), std::make_pair(&flds2, 3 * n1),
+                  std::make_pair(&qs2, n1), std::make_pair(&phisn, n1), std::make_pair(&fldsn, 3 * n1)})
+    if (!*pr.first) TRY(dalloc(pr.first, pr.second));
+  if (!side) BBFMM_CUDA_OK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  for (cudaEvent_t &e : side_ev)
+    if (!e) BBFMM_CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  kernel_launches = 0;
+  if (timing) {
+    for (int i = 0; i < ST_COUNT; ++i) stage_ms[i] = 0.f;
+    if (!ev[ST_COUNT]) cudaEventCreate(&ev[ST_COUNT]);
+    mark(-1, 0);
+  }
+  // far field of q1 into (phis2, flds2), and q1 in sorted order kept for the near field
+  std::swap(phis, phis2);
+  std::swap(flds, flds2);
+  int rc = upward(q1_dev, sizeof(T) == 8);
+  if (rc == BBFMM_OK) rc = interaction(m2l_first, maxlev);
+  if (rc == BBFMM_OK) rc = leaf_down(true);
+  std::swap(phis, phis2);
+  std::swap(flds, flds2);
+  TRY(rc);
+  TRY(launch_charges_of<T>(N, pos4, qs2, stream));
+  // q2 into pos4, then the near field (pos4's charges q2 into (phisn, fldsn), q1 added to the
+  // far field in (phis2, flds2)) beside the far field of q2 into (phis, flds)
+  if (sizeof(T) == 8) TRY((launch_gather<T, double>(N, perm, nullptr, (const double *)q2_dev, pos4, stream)));
+  else TRY((launch_gather<T, float>(N, perm, nullptr, (const float *)q2_dev, pos4, stream)));
+  mark(ST_GATHER);
+  if (near_threads != tune.p2p_threads) TRY(build_near_work());
+  cudaStream_t ns = timing ? stream : side;
+  auto near_pass = [&]() -> int {
+    BBFMM_CUDA_OK(cudaMemsetAsync(phisn, 0, sizeof(T) * n1, ns));
+    BBFMM_CUDA_OK(cudaMemsetAsync(fldsn, 0, sizeof(T) * 3 * n1, ns));
+    return launch_near2(mode, N, pos4, leaf_start, maxlev, near_work, nsets, near_items, near_threads, qs2, phisn,
+                        fldsn, phis2, flds2, ns, region_mask, region_level);
+  };
+  if (!timing) {
+    BBFMM_CUDA_OK(cudaEventRecord(side_ev[0], stream));
+    BBFMM_CUDA_OK(cudaStreamWaitEvent(side, side_ev[0], 0));
+    TRY(near_pass());
+    BBFMM_CUDA_OK(cudaEventRecord(side_ev[1], side));
+  }
+  TRY(upward(nullptr, sizeof(T) == 8));  // pos4 already holds q2
+  TRY(interaction(m2l_first, maxlev));
+  TRY(leaf_down(true));
+  if (timing) TRY(near_pass());
+  else BBFMM_CUDA_OK(cudaStreamWaitEvent(stream, side_ev[1], 0));
+  mark(ST_P2P);
+  // the second vector's potential and field: far + near, one addition per value as near() makes it
+  TRY(launch_add<T>(N, phisn, phis, stream));
+  TRY(launch_add<T>(3 * (int64_t)N, fldsn, flds, stream));
+  TRY((launch_scatter_field<T, T>(N, perm, phis2, flds2, (T *)pot1_dev, (T *)fld1_dev, stream)));
+  TRY((launch_scatter_field<T, T>(N, perm, phis, flds, (T *)pot2_dev, (T *)fld2_dev, stream)));
   mark(ST_SCATTER);
   return BBFMM_OK;
 }
@@ -1002,7 +1083,7 @@ void Solver<T>::release() {
   free_local();
   if (region_mask) cudaFree(region_mask);
   void *ptrs[] = {offs, perm, leaf_start, near_work, pos4, S[0], S[1], F[0], F[1], Mall, Lbuf, Lpart, Msplit,
-                  phis, flds, Ssplit, Lsplit, io_q, io_phi};
+                  phis, flds, Ssplit, Lsplit, io_q, io_phi, phis2, flds2, qs2, phisn, fldsn};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (own_ops) {
@@ -1013,6 +1094,9 @@ void Solver<T>::release() {
     if (tcproj) tc_free_projections(tcproj);
   }
   if (ev[ST_COUNT]) cudaEventDestroy(ev[ST_COUNT]);
+  for (cudaEvent_t e : side_ev)
+    if (e) cudaEventDestroy(e);
+  if (side) cudaStreamDestroy(side);
   if (own_stream && stream) cudaStreamDestroy(stream);
   *this = Solver<T>();
 }
@@ -1112,6 +1196,14 @@ int bbfmm_b200_solve_fields(bbfmm_b200_solver *h, const void *q_dev, void *pot_d
   if (!h || !q_dev || (!pot_dev && !field_dev)) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   if (h->f) return h->f->solve_fields(q_dev, pot_dev, field_dev);
   return h->d->solve_fields(q_dev, pot_dev, field_dev);
+}
+
+int bbfmm_b200_solve_fields2(bbfmm_b200_solver *h, const void *q1_dev, const void *q2_dev, void *pot1_dev,
+                             void *field1_dev, void *pot2_dev, void *field2_dev) {
+  if (!h || !q1_dev || !q2_dev || (!pot1_dev && !field1_dev) || (!pot2_dev && !field2_dev))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  if (h->f) return h->f->solve_fields2(q1_dev, q2_dev, pot1_dev, field1_dev, pot2_dev, field2_dev);
+  return h->d->solve_fields2(q1_dev, q2_dev, pot1_dev, field1_dev, pot2_dev, field2_dev);
 }
 
 int bbfmm_b200_solve_host(bbfmm_b200_solver *h, const void *q_host, void *phi_host) {

@@ -34,6 +34,8 @@ template <typename T> int launch_l2p(int n, const T *pos4, const int *leaf_start
 // rows are a slab of the level starting at cell row0 (the cpg side is indexed by level cell)
 template <typename T> int launch_proj(int64_t M, int K, int N, const T *A, const float *A2, const T *B, const T *cs, T scale, T *C, int level, int mapmode, cudaStream_t s, int64_t row0 = 0, int ldc = 0, int lda = 0, const int64_t *rows = nullptr);
 template <typename T, typename TI> int launch_gather(int N, const int *perm, const TI *xyz, const TI *q, T *pos4, cudaStream_t s);
+template <typename T> int launch_charges_of(int N, const T *pos4, T *q, cudaStream_t s);  // sorted charges
+template <typename T> int launch_add(int64_t n, const T *x, T *y, cudaStream_t s);        // y += x
 template <typename T, typename TO> int launch_scatter(int N, const int *perm, const T *phis, TO *phi, cudaStream_t s);
 template <typename T> int launch_morton_cpg(int level, int r, const T *src, T *dst, int inverse, cudaStream_t s);
 // Near field (p2p.cu): a work list built on the device from the leaf offsets (near_work_build,
@@ -51,6 +53,9 @@ int launch_near(int mode, int homogen, int N, const void *pos4, const int *leaf_
                 int nsets, int nitems, int threads, void *pot, void *fld, cudaStream_t s,
                 const unsigned char *mask = nullptr, int mask_level = 0);
 int near_status(int clear);
+int launch_near2(int mode, int N, const void *pos4, const int *leaf_start, int maxlev, const void *work, int nsets,
+                 int nitems, int threads, const void *q2, void *pot, void *fld, void *pot2, void *fld2, cudaStream_t s,
+                 const unsigned char *mask = nullptr, int mask_level = 0);
 int pass_status(int clear);  // the passes' bounded waits (L2P leaf copies)
 template <typename T> int launch_l2p_field(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, const T *F, T *pot, T *fld, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, const int64_t *rows = nullptr);
 template <typename T, typename TO> int launch_scatter_field(int N, const int *perm, const T *pot, const T *fld, TO *pot_out, TO *fld_out, cudaStream_t s);
@@ -236,6 +241,10 @@ struct Solver {
   void *Msplit = nullptr;
   T *phis = nullptr;
   T *flds = nullptr;  // 3 N, sorted field of the last solve_fields
+  T *phis2 = nullptr, *flds2 = nullptr, *qs2 = nullptr;  // solve_fields2: second potential, field, charges
+  T *phisn = nullptr, *fldsn = nullptr;  // solve_fields2: near field of the second vector
+  cudaStream_t side = nullptr;           // solve_fields2: the near field beside the far field
+  cudaEvent_t side_ev[2] = {};
   void *io_q = nullptr, *io_phi = nullptr;  // device staging of the host-buffer solve (N each)
   // timing
   bool timing = false;
@@ -295,6 +304,9 @@ struct Solver {
   int downward_finish(void *phi_dev, int phi_is_double, bool near);  // L2P, P2P, scatter
   int solve(const void *q_dev, void *phi_dev, int io_double);
   int solve_fields(const void *q_dev, void *pot_dev, void *fld_dev);  // potential and its gradient
+  // solve_fields for two charge vectors, the near-field pairs evaluated once for both
+  int solve_fields2(const void *q1_dev, const void *q2_dev, void *pot1_dev, void *fld1_dev, void *pot2_dev,
+                    void *fld2_dev);
   int copy_multipoles_morton(int level, T *host_out);  // level's M in reference (Morton) order
   int copy_m2l_morton(int level, T *host_out);         // level's M2L output, recomputed, Morton order
   void mark(int stage, int launches = 1);

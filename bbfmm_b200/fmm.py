@@ -169,6 +169,30 @@ class Solver:
         caller.wait_event(done)
         return pot, fld
 
+    def solve_fields2(self, q1, q2, want_field=True):
+        """solve_fields for two charge vectors in one call (bbfmm_b200_solve_fields2: the
+        near-field pairs evaluated once for both) -> (pot1, field1, pot2, field2)."""
+        torch = self.torch
+        _check_count("q1", q1.numel(), self.N)
+        _check_count("q2", q2.numel(), self.N)
+        q1 = q1.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        q2 = q2.to(device=f"cuda:{self.device}", dtype=self.dtype).contiguous()
+        pot1, pot2 = torch.empty_like(q1), torch.empty_like(q2)
+        mk = lambda: torch.empty((q1.numel(), 3), dtype=self.dtype, device=q1.device) if want_field else None
+        fld1, fld2 = mk(), mk()
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        caller = torch.cuda.current_stream(q1.device)
+        mine = torch.cuda.ExternalStream(self.stream, device=q1.device)
+        ready = torch.cuda.Event()
+        ready.record(caller)
+        mine.wait_event(ready)
+        _lib.check(_lib.lib().bbfmm_b200_solve_fields2(self.h, ptr(q1), ptr(q2), ptr(pot1), ptr(fld1), ptr(pot2),
+                                                        ptr(fld2)))
+        done = torch.cuda.Event()
+        done.record(mine)
+        caller.wait_event(done)
+        return pot1, fld1, pot2, fld2
+
     def solve_host(self, q, out=None):
         """Host charges -> host q_i * phi_i (copies in, solves, copies out, synchronises).
         out: an optional host array of the same size (pinned memory makes the copy direct)."""

@@ -129,6 +129,13 @@ BBFMM_B200_API int bbfmm_b200_solve(bbfmm_b200_solver *s, const void *q_dev, voi
  * derivative code; the gradient of the Chebyshev interpolant (S_n of bbfmm.c:1682-1690) is
  * new. Runs on the solver's stream without synchronising. */
 BBFMM_B200_API int bbfmm_b200_solve_fields(bbfmm_b200_solver *s, const void *q_dev, void *pot_dev, void *field_dev);
+/* bbfmm_b200_solve_fields for two charge vectors q1 and q2 (device, N each) in one call, the
+ * same results as two calls: the two far fields run one after the other and one near-field pass
+ * evaluates each pair once for both (no counterpart in the reference, which has no derivative
+ * code; it serves the backward of bbfmm_b200.autograd.fmm_phi with save="recompute"). Either
+ * output of each pair may be NULL, not both. */
+BBFMM_B200_API int bbfmm_b200_solve_fields2(bbfmm_b200_solver *s, const void *q1_dev, const void *q2_dev,
+                                            void *pot1_dev, void *field1_dev, void *pot2_dev, void *field2_dev);
 
 /* The same with host buffers: copies q in, solves, copies phi out and synchronises. The
  * device staging (2 N values) is allocated on the first call and kept until the particles

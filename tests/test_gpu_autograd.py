@@ -94,10 +94,10 @@ def test_gradients_match_direct_sum(oracle_d, mode, save):
     s.close()
 
 
-@pytest.mark.parametrize("save,n_fields,n_plain", [("fields", 2, 0), ("recompute", 2, 1)])
-def test_solves_per_forward_backward(save, n_fields, n_plain):
+@pytest.mark.parametrize("save,n_fields,n_plain,n_pair", [("fields", 2, 0, 0), ("recompute", 0, 1, 1)])
+def test_solves_per_forward_backward(save, n_fields, n_plain, n_pair):
     """fields: forward + backward = two solves of fields (the backward is one solve);
-    recompute: one plain solve forward, two solves of fields backward."""
+    recompute: one plain solve forward, one solve of fields for both charge vectors backward."""
     import torch
     from bbfmm_b200 import Solver
     from bbfmm_b200.autograd import fmm_phi
@@ -108,18 +108,40 @@ def test_solves_per_forward_backward(save, n_fields, n_plain):
     qt = torch.as_tensor(q, device="cuda").requires_grad_(True)
     xt = torch.as_tensor(x, device="cuda").requires_grad_(True)
     wt = torch.as_tensor(w, device="cuda")
-    calls = {"fields": 0, "plain": 0}
-    of, op = s.solve_fields, s.solve
+    calls = {"fields": 0, "plain": 0, "pair": 0}
+    of, op, o2 = s.solve_fields, s.solve, s.solve_fields2
 
     def count(kind, f):
         def g(*a, **k):
             calls[kind] += 1
             return f(*a, **k)
         return g
-    s.solve_fields, s.solve = count("fields", of), count("plain", op)
+    s.solve_fields, s.solve, s.solve_fields2 = count("fields", of), count("plain", op), count("pair", o2)
     (wt * fmm_phi(s, qt, xt, save=save)).sum().backward()
-    assert calls == {"fields": n_fields, "plain": n_plain}
+    assert calls == {"fields": n_fields, "plain": n_plain, "pair": n_pair}
     assert qt.grad is not None and xt.grad is not None
+    s.close()
+
+
+@pytest.mark.parametrize("mode", ["d", "s", "mixed"])
+def test_fields_for_two_charge_vectors_equal_two_solves(mode):
+    """bbfmm_b200_solve_fields2 gives, bitwise, what two bbfmm_b200_solve_fields calls give: the
+    same far-field passes per charge vector and, in its single near-field pass, each pair's
+    terms for both vectors with the arithmetic and summation order of one vector's pass
+    (clustered input: sparse and dense near-field items)."""
+    import torch
+    from bbfmm_b200 import Solver
+    x, q, w = _clustered(150000, 6)
+    s = Solver(8, 4, 1.0, mode=mode)
+    s.set_particles(x)
+    q1 = torch.as_tensor(q, device="cuda")
+    q2 = torch.as_tensor(w * q, device="cuda")
+    a = s.solve_fields(q1) + s.solve_fields(q2)
+    b = s.solve_fields2(q1, q2)
+    for u, v in zip(a, b):
+        assert torch.equal(u, v)
+    p1, _, p2, _ = s.solve_fields2(q1, q2, want_field=False)
+    assert torch.equal(p1, a[0]) and torch.equal(p2, a[2])
     s.close()
 
 
