@@ -954,7 +954,7 @@ int Solver<T>::autotune(const void *q_dev, int io_double) {
     }
     // candidates: (kind, offset groups); only the mixed mode has the tensor-core kind
     std::vector<std::pair<int, int>> cand;
-    if (tc_level(l)) cand.push_back({0, 0});
+    if (tc_default(l)) cand.push_back({0, 0});
     // the DMMA and the SIMT M2L both split their offsets over groups
     for (int g : {1, 3, 7, 21})
       if (dmma_part_elems(l, nsets, g, r) * (int64_t)sizeof(T) <= ((int64_t)1 << 30)) cand.push_back({1, g});
@@ -1352,8 +1352,8 @@ int bbfmm_b200_set_tuning(bbfmm_b200_solver *h, const int *info) {
   const int th = info[0];
   if (th != 64 && th != 128 && th != 256) return bbfmm_set_error(BBFMM_ERR_ARG, "P2P threads: 64, 128 or 256");
   for (int l = 0; l <= 10; ++l)
-    if ((info[1 + l] != 0 && info[1 + l] != 1) || info[12 + l] < 0 || info[12 + l] > bbfmm::DMMA_PARTS)
-      return bbfmm_set_error(BBFMM_ERR_ARG, "M2L kind must be 0 or 1 and groups in [0, 21]");
+    if (info[1 + l] < 0 || info[1 + l] > 2 || info[12 + l] < 0 || info[12 + l] > bbfmm::DMMA_PARTS)
+      return bbfmm_set_error(BBFMM_ERR_ARG, "M2L kind must be 0, 1 or 2 and groups in [0, 21]");
   auto apply = [&](auto &sv) -> int {
     sv.tune.p2p_threads = th;
     for (int l = 0; l <= 10; ++l) {

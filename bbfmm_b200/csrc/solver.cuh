@@ -150,7 +150,9 @@ inline int64_t tc2_tiles(int level, int nsets) {
 
 // Launch choices of one solver, per level (index = level): what the autotuner sets.
 struct Tuning {
-  int m2l_kind[11] = {};    // 0: default (tensor-core split M2L where the mode has it), 1: FP64/SIMT M2L
+  // 0: default (the tensor-core split M2L where the mode has it, from level 4, and at levels
+  // 2-3 for stacked sets), 1: FP64/SIMT M2L, 2: the tensor-core M2L wherever it tiles the level
+  int m2l_kind[11] = {};
   int m2l_groups[11] = {};  // offset groups of the FP64 DMMA M2L (0: dmma_default_groups)
   int p2p_threads = 128;    // threads per block of the near-field kernel
 };
@@ -286,7 +288,15 @@ struct Solver {
     return mode == MODE_MIXED && tcops &&
            (l >= TC_MIN_LEVEL || (l >= TC2_MIN_LEVEL && tc_two_box(tc_products, rk())));
   }
-  bool tc_m2l(int l) const { return tc_level(l) && tune.m2l_kind[l] == 0; }
+  // The default keeps a single set's levels 2-3 in FP64: they are a few tiles either way, and
+  // their split-BF16 M2L raised the 4M uniform solve's error ratio against the FP64 direct sum
+  // from 1.05 to 1.10; stacked sets take the tensor cores there (the FP64 M2L of a batch's
+  // levels 2-3 took tens of ms).
+  bool tc_default(int l) const { return tc_level(l) && (l >= TC_MIN_LEVEL || nsets > 1); }
+  bool tc_m2l(int l) const {
+    const int k = tune.m2l_kind[l];
+    return k == 2 ? tc_level(l) : (k == 0 && tc_default(l));
+  }
   // S rows -> Mall (cpg); F rows <- Lbuf (Morton, assign). Row t is cell row0 + t, or
   // rowlist[t] when a row list is given.
   int proj_up(int64_t rows, const T *S_rows, int level, int64_t row0, bool presplit = false,

@@ -298,7 +298,9 @@ BBFMM_B200_API int bbfmm_b200_set_tc_products(bbfmm_b200_solver *s, int nprod);
  * of similar shape reuse them without timing. Synchronises the device. */
 BBFMM_B200_API int bbfmm_b200_autotune(bbfmm_b200_solver *s, const void *q_dev);
 /* Current choices: info[0] = P2P threads per block, info[1 + l] = M2L kind of level l
- * (0 default, 1 FP64/SIMT), info[12 + l] = offset groups of level l (0 = default); 23 ints. */
+ * (0 default: mixed mode on the tensor cores from level 4, and at levels 2-3 in batches;
+ * 1 FP64/SIMT; 2 the tensor cores wherever they tile the level), info[12 + l] = offset groups
+ * of level l (0 = default); 23 ints. */
 BBFMM_B200_API int bbfmm_b200_tuning(const bbfmm_b200_solver *s, int *info);
 /* Sets the choices (same 23 ints; for replaying a tuning or for tests). */
 BBFMM_B200_API int bbfmm_b200_set_tuning(bbfmm_b200_solver *s, const int *info);

@@ -97,10 +97,19 @@ def test_m2l_level_matches_oracle_on_sampled_cells(oracle_d, mode, tol, lev, N):
     s.close()
 
 
+def force_tc(solver, levels):
+    """M2L kind 2 (the tensor cores wherever they tile the level) at the given levels."""
+    t = solver.tuning()
+    for lev in levels:
+        t["m2l_kind"][lev] = 2
+    solver.set_tuning(t)
+
+
 def test_m2l_levels_2_3_stacked_set_tiles(oracle_d):
     """Levels 2 and 3 on the tensor cores, whose 2 x 2 x 2 and 4 x 4 x 4 class grids the two-box
-    kernel tiles 32 and 4 stacked sets at a time. One set (the other slots of each tile load it
-    again and are not written): every cell of both levels against the oracle's M2L of the
+    kernel tiles 32 and 4 stacked sets at a time. One set with those levels put on the tensor
+    cores (kind 2; by default a single set keeps them in FP64; the other slots of each tile load
+    it again and are not written): every cell of both levels against the oracle's M2L of the
     solver's own multipoles, mixed tolerance 1e-6. A batch of depth-2, depth-3 and depth-4 sets
     (a full and a partial group of four at level 3) gives each set the result of its own mixed
     solver."""
@@ -110,6 +119,7 @@ def test_m2l_levels_2_3_stacked_set_tiles(oracle_d):
     _, _, E = ops.load_operators(8, single=False)
     x, q = uniform_inputs(40_000, seed=33)
     s = _solver("mixed", 3, x)
+    force_tc(s, (2, 3))  # a single set keeps levels 2-3 in FP64 by default
     s.solve(torch.as_tensor(q, device="cuda"))
     torch.cuda.synchronize()
     for lev in (2, 3):
@@ -129,10 +139,13 @@ def test_m2l_levels_2_3_stacked_set_tiles(oracle_d):
     qd = torch.as_tensor(qs, device="cuda")
     b = Batch(sets, mode="mixed")
     got = b.solve(qd).cpu().numpy()
+    stacked = {lev: sum(1 for _, _, lv in sets if lv == lev) > 1 for _, _, lev in sets}
     for k, (xs, n, lev) in enumerate(sets):
         a0, a1 = b.offsets[k], b.offsets[k + 1]
         one = Solver(n, lev, 1.0, mode="mixed")
         one.set_particles(xs)
+        if stacked[lev]:  # the batch runs this group's levels 2-3 on the tensor cores
+            force_tc(one, (2, 3))
         want = one.solve(qd[a0:a1]).cpu().numpy()
         one.close()
         assert rel_l2(got[a0:a1], want) < 1e-12, (k, rel_l2(got[a0:a1], want))
