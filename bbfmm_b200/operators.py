@@ -227,6 +227,26 @@ def write_operator_files(dirpath: str, n: int, Ucol: np.ndarray, Ecol: np.ndarra
     _write_atomic(os.path.join(dirpath, kname), E.tobytes())
 
 
+def _parse_text(tokens, single: bool):
+    """Decimal tokens -> FP64, or FP32 correctly rounded from the decimal as strtof gives it.
+    Going through FP64 rounds twice, which differs from one rounding only where the FP64 value
+    lies exactly halfway between two FP32 values; those tokens are parsed again by strtof."""
+    d = np.array(tokens, dtype=np.float64)
+    if not single:
+        return d
+    f = d.astype(np.float32)
+    bits = d.view(np.int64)
+    tie = (bits & ((1 << 29) - 1)) == (1 << 28)  # low 29 of the 52 mantissa bits: a float32 midpoint
+    if tie.any():
+        import ctypes
+        libc = ctypes.CDLL(None)
+        libc.strtof.restype = ctypes.c_float
+        libc.strtof.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+        for i in np.nonzero(tie)[0]:
+            f[i] = libc.strtof(tokens[i].encode(), None)
+    return f
+
+
 def read_operator_files(dirpath: str, n: int, single: bool, kernel: str = "laplacian", ascii: bool = False):
     """Read ``[s]<kernel>{K,U}{n}.bin`` (bbfmm.c:216-254), or with ``ascii`` the ``.out`` text
     form of the reference's ENABLE_ASCII_IO builds. Returns (r, Ucol, Ecol)."""
@@ -235,10 +255,10 @@ def read_operator_files(dirpath: str, n: int, single: bool, kernel: str = "lapla
     if ascii:
         u = open(os.path.join(dirpath, uname)).read().split()
         r = int(u[0])
-        # text to FP64, then to the file's precision, as fscanf "%f" / "%lf" read it
-        Ucol = np.array(u[1:1 + n ** 3 * r], dtype=np.float64).astype(dt)
+        # as fscanf "%f" / "%lf" read the text: correctly rounded to the file's precision
+        Ucol = _parse_text(u[1:1 + n ** 3 * r], single)
         e = open(os.path.join(dirpath, kname)).read().split()
-        Ecol = np.array(e[:NUM_OFFSETS * r * r], dtype=np.float64).astype(dt)
+        Ecol = _parse_text(e[:NUM_OFFSETS * r * r], single)
         if Ucol.size != n ** 3 * r or Ecol.size != NUM_OFFSETS * r * r:
             raise ValueError("operator text files are shorter than their cutoff implies")
         return r, Ucol, Ecol

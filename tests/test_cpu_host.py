@@ -156,3 +156,22 @@ def test_operator_text_files(tmp_path):
     ops.write_operator_files(str(tmp_path), 4, U2, E2, True, ascii=True)
     _, Us, _ = ops.read_operator_files(str(tmp_path), 4, True, ascii=True)
     assert Us.dtype == np.float32 and np.array_equal(Us, U2.astype(np.float32))
+
+
+def test_ascii_single_operator_text_rounds_once():
+    """The FP32 reader of the reference's ENABLE_ASCII_IO operator text rounds each decimal once,
+    as strtof does (fscanf "%f"), also where FP64 would land exactly between two FP32 values."""
+    import ctypes
+    from bbfmm_b200.operators import _parse_text
+    libc = ctypes.CDLL(None)
+    libc.strtof.restype = ctypes.c_float
+    libc.strtof.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    a = np.float32(1.0)
+    mid = (float(a) + float(np.nextafter(a, np.float32(2)))) / 2
+    tokens = [repr(mid) + "0000000001", "0.1", "-3.25e-7", repr(mid)]
+    assert float(tokens[0]) == mid  # FP64 alone loses the digits above the midpoint
+    want = np.array([libc.strtof(t.encode(), None) for t in tokens], dtype=np.float32)
+    got = _parse_text(tokens, True)
+    assert got.dtype == np.float32 and np.array_equal(got, want)
+    assert got[0] != np.float32(float(tokens[0]))  # the double rounding it avoids
+    assert np.array_equal(_parse_text(tokens, False), np.array([float(t) for t in tokens]))
