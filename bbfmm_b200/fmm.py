@@ -451,17 +451,38 @@ class AdaptiveBatch:
                 b.close()
 
     def autotune(self, q):
+        """Both batches' launch choices, then the submission (replayed graphs or launches) that
+        runs the two batches faster side by side: their graphs each run every group as a
+        parallel branch, which can crowd the two batches' kernels onto the SMs together."""
         self.coarse.autotune(q)
+        torch = self.torch
         if self.refined is not None:
-            torch = self.torch
             torch.index_select(q.to(self.q_ref.dtype), 0, self.sel, out=self.q_ref)
             self.refined.autotune(self.q_ref)
+        out = torch.empty_like(q.to(self.coarse.dtype))
+        ms = {}
+        for graph in (True, False):
+            for _ in range(2):
+                self.solve(q, out=out, graph=graph)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(3):
+                self.solve(q, out=out, graph=graph)
+            b.record()
+            b.synchronize()
+            ms[graph] = a.elapsed_time(b)
+        self.graph = ms[True] <= ms[False]
 
-    def solve(self, q, out=None, graph: bool = True):
-        """As Batch.solve. The coarse and the refined batch run at the same time on their own
-        streams (both read charges gathered before either starts); the refined results are
-        added on the caller's stream once both are done."""
+    graph = True  # submission of solve(graph=None): replayed graphs (set by autotune)
+
+    def solve(self, q, out=None, graph: bool | None = None):
+        """As Batch.solve (graph None: the submission autotune chose). The coarse and the
+        refined batch run at the same time on their own streams (both read charges gathered
+        before either starts); the refined results are added on the caller's stream once both
+        are done."""
         torch = self.torch
+        if graph is None:
+            graph = self.graph
         if self.refined is None:
             return self.coarse.solve(q, out=out, graph=graph)
         _check_count("q", q.numel(), self.N)

@@ -666,10 +666,13 @@ def run_batch_256(args, adaptive=False):
         return float(t.item())
 
     barrier()
+    # the adaptive batch: the submission its autotune chose (graphs or launches)
+    sub = b.graph if adaptive else True
     with ClockSampler(local) as clk:
-        t_graph = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=True), args.steps, stream))
+        t_graph = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=sub), args.steps, stream))
     barrier()
     t_eager = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=False), args.steps, stream))
+    t_replay = max_over_ranks(_device_time(lambda: b.solve(qd, out=out, graph=True), args.steps, stream))
     if adaptive:  # the coarse groups, then the refined ones on the charges the last solve gathered
         group_ms = [b.coarse.group_stage_times(qd, g) for g in range(len(b.coarse.groups()))]
         if b.refined is not None:
@@ -701,7 +704,7 @@ def run_batch_256(args, adaptive=False):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         qd.copy_(qh, non_blocking=True)
-        b.solve(qd, out=out, graph=True)
+        b.solve(qd, out=out, graph=sub)
         ph.copy_(out, non_blocking=True)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
@@ -733,7 +736,8 @@ def run_batch_256(args, adaptive=False):
                        "particles": Ntot, "mode": mode, "parallelism": f"sets sharded over {world} GPU(s)",
                        "groups": [{k: g[k] for k in ("n", "maxlev", "sets", "particles", "p2p_threads",
                                                       "m2l_kind", "m2l_groups")} for g in groups]},
-            "particles_per_s": Ntot / t_graph, "eager_ms": t_eager * 1e3,
+            "particles_per_s": Ntot / t_graph, "eager_ms": t_eager * 1e3, "graph_ms": t_replay * 1e3,
+            "submission": "graph" if sub else "launches",
             "graph_nodes": None if adaptive else b.graph_nodes,
             "adaptive": {"heavy_leaves": b.heavy_leaves, "refined_particles": b.refined_particles,
                          "cap": 256, "refine_levels": 2} if adaptive else None,
