@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_batch_solve.argtypes = [vp, vp, vp, i]
         L.bbfmm_b200_batch_autotune.argtypes = [vp, vp]
         L.bbfmm_b200_batch_set_target_regions.argtypes = [vp, i, vp, i]
+        L.bbfmm_b200_batch_set_kernel.argtypes = [vp, i]
         L.bbfmm_b200_batch_groups.argtypes = [vp]
         L.bbfmm_b200_batch_graph_nodes.argtypes = [vp]
         L.bbfmm_b200_batch_graph_nodes.restype = C.c_longlong

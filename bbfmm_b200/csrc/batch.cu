@@ -231,6 +231,13 @@ struct Batch {
     return BBFMM_OK;
   }
 
+  // Degree of homogeneity of the kernel of every group (Solver::homogen).
+  int set_kernel(int hg) {
+    drop_graph();
+    for (auto &g : groups) g.solver->homogen = hg;
+    return BBFMM_OK;
+  }
+
   int autotune(const void *q) {
     drop_graph();
     for (auto &g : groups) TRY_(g.solver->autotune(q, sizeof(T) == 8));
@@ -287,6 +294,13 @@ int bbfmm_b200_batch_set_target_regions(bbfmm_b200_batch *b, int levels_up, cons
   if (!b) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   return b->d ? b->d->set_target_regions(levels_up, active, first_m2l)
               : b->f->set_target_regions(levels_up, active, first_m2l);
+}
+
+int bbfmm_b200_batch_set_kernel(bbfmm_b200_batch *b, int kernel) {
+  if (!b) return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
+  const int hg = bbfmm::kernel_homogen(kernel);
+  if (!hg) return bbfmm_set_error(BBFMM_ERR_ARG, "unknown kernel");
+  return b->d ? b->d->set_kernel(hg) : b->f->set_kernel(hg);
 }
 
 int bbfmm_b200_batch_groups(const bbfmm_b200_batch *b) {

@@ -1315,10 +1315,8 @@ int bbfmm_b200_set_leaf_slab(bbfmm_b200_solver *h, long long cells) {
 
 int bbfmm_b200_set_kernel(bbfmm_b200_solver *h, int kernel) {
   if (!h) return bbfmm_set_error(BBFMM_ERR_ARG, "null handle");
-  if (kernel != BBFMM_B200_KERNEL_LAPLACIAN && kernel != BBFMM_B200_KERNEL_LAPLACIAN_FORCE &&
-      kernel != BBFMM_B200_KERNEL_ONEOVERR4)
-    return bbfmm_set_error(BBFMM_ERR_ARG, "unknown kernel");
-  const int hg = kernel == BBFMM_B200_KERNEL_ONEOVERR4 ? 4 : (kernel == BBFMM_B200_KERNEL_LAPLACIAN_FORCE ? 2 : 1);
+  const int hg = bbfmm::kernel_homogen(kernel);
+  if (!hg) return bbfmm_set_error(BBFMM_ERR_ARG, "unknown kernel");
   if (h->f) h->f->homogen = hg;
   else h->d->homogen = hg;
   return BBFMM_OK;

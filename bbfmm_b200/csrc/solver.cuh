@@ -6,6 +6,7 @@
 
 #include <vector>
 
+#include "../../include/bbfmm_b200.h"
 #include "common.cuh"
 
 struct __nv_bfloat16;
@@ -148,6 +149,14 @@ inline int64_t tc2_tiles(int level, int nsets) {
   return 8 * (int64_t)((nsets + spt - 1) / spt) * (P >> g.lx) * (P >> g.ly) * (P >> g.lz);
 }
 
+// Degree of homogeneity of a BBFMM_B200_KERNEL_* value (bbfmm.c:109-144), 0 for an unknown one.
+inline int kernel_homogen(int kernel) {
+  return kernel == BBFMM_B200_KERNEL_LAPLACIAN         ? 1
+         : kernel == BBFMM_B200_KERNEL_LAPLACIAN_FORCE ? 2
+         : kernel == BBFMM_B200_KERNEL_ONEOVERR4       ? 4
+                                                       : 0;
+}
+
 // Launch choices of one solver, per level (index = level): what the autotuner sets.
 struct Tuning {
   // 0: default (the tensor-core split M2L where the mode has it, from level 4, and at levels
@@ -162,7 +171,7 @@ struct Solver {
   int n = 0, r = 0, n3 = 0, maxlev = 0, mode = MODE_D, lead = 16, lead_rows = 32, device = 0;
   int nsets = 1;  // particle sets of this depth stacked in every launch (set k = cells [k 8^l, (k+1) 8^l))
   // kernel: degree of homogeneity, 1 (1/r, LAPLACIAN), 2 (x/r^3, LAPLACIANFORCE) or 4 (1/r^4,
-  // ONEOVERR4); 2 and 4 in modes D and S: the near-field pair value and the per-level scale
+  // ONEOVERR4), in every mode: the near-field pair value and the per-level scale
   // (1/L_l)^homogen after the M2L
   int homogen = 1;
   // Effective rank (0 = r): the operators hold a rank-rank_eff truncation zero-padded to r,

@@ -524,10 +524,10 @@ class Batch:
 
     sets: a list of (xyz, n, maxlev) with xyz an (N_s, 3) host array inside [-L/2, L/2]^3.
     Charges and results are CUDA tensors holding the sets back to back in list order
-    (``offsets[s]:offsets[s + 1]``)."""
+    (``offsets[s]:offsets[s + 1]``). kernel: as for Solver, one for every set."""
 
     def __init__(self, sets, mode: str = "mixed", L: float = 1.0, lead: int = 16, lead_rows: int = 32,
-                 device: int = 0):
+                 device: int = 0, kernel: str = "laplacian"):
         import torch
         self.torch = torch
         self.mode, self.L, self.device = mode, float(L), device
@@ -541,9 +541,12 @@ class Batch:
         self.N = int(self.offsets[-1])
         xyz = np.ascontiguousarray(np.concatenate([np.asarray(x, np_dtype).reshape(-1, 3) for x, _, _ in sets])
                                    if len(sets) else np.zeros((0, 3), np_dtype))
+        if kernel not in ops.KERNELS:
+            raise ValueError(f"unknown kernel {kernel!r} ({', '.join(ops.KERNELS)})")
+        self.kernel = kernel
         ops_ = {}
         for n in sorted(set(ns.tolist())):
-            _, U, E = ops.load_operators(n, single=(mode == "s"))
+            _, U, E = ops.load_operators(n, single=(mode == "s"), kernel=kernel)
             ops_[n] = (np.ascontiguousarray(U), np.ascontiguousarray(E))
         fp32 = int(mode == "s")
         p = lambda n, k: _ptr(ops_[n][k]) if n in ops_ else None
@@ -555,6 +558,8 @@ class Batch:
                                                        levs.ctypes.data_as(ip), counts.ctypes.data_as(ip), _ptr(xyz),
                                                        p(4, 0), p(4, 1), p(8, 0), p(8, 1), fp32, C.byref(h)))
         self.h = h
+        if kernel != "laplacian":
+            _lib.check(_lib.lib().bbfmm_b200_batch_set_kernel(h, ops.KERNELS[kernel][1]))
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -259,9 +259,9 @@ BBFMM_B200_API int bbfmm_b200_set_rank(bbfmm_b200_solver *s, int rank);
  * x the first component of source - target, homogeneity 2) or BBFMM_B200_KERNEL_ONEOVERR4
  * (1/r^4, homogeneity 4), in every mode; the operators given at create must be that kernel's,
  * e.g. the reference's laplacianforce{K,U}{n}.bin or oneoverr4{K,U}{n}.bin. It sets the
- * near-field pair value (MIXED: the separation in FP64, dx r^-3 or r^-4 in FP32 with the
- * compensated sum) and the per-level scale (1/L_l)^homogeneity after the M2L. Field solves
- * are for 1/r. */
+ * near-field pair value (MIXED: x / r^3 with the separation in FP64 and dx r^-3 in FP32 with
+ * the compensated sum; 1/r^4 in FP64, its potentials being near-field dominated) and the
+ * per-level scale (1/L_l)^homogeneity after the M2L. Field solves are for 1/r. */
 #define BBFMM_B200_KERNEL_LAPLACIAN 0
 #define BBFMM_B200_KERNEL_LAPLACIAN_FORCE 1
 #define BBFMM_B200_KERNEL_ONEOVERR4 2
@@ -333,6 +333,9 @@ BBFMM_B200_API int bbfmm_b200_batch_autotune(bbfmm_b200_batch *b, const void *q_
  * captured graph. bbfmm_b200.AdaptiveBatch refines the heavy leaves of a batch with it. */
 BBFMM_B200_API int bbfmm_b200_batch_set_target_regions(bbfmm_b200_batch *b, int levels_up,
                                                        const unsigned char *active, int first_m2l);
+/* Kernel of every set of the batch (as bbfmm_b200_set_kernel; the operators given at create
+ * must be that kernel's). Drops the captured graph. */
+BBFMM_B200_API int bbfmm_b200_batch_set_kernel(bbfmm_b200_batch *b, int kernel);
 BBFMM_B200_API int bbfmm_b200_batch_groups(const bbfmm_b200_batch *b);
 /* Nodes of the captured graph (0 before the first graph solve). */
 BBFMM_B200_API long long bbfmm_b200_batch_graph_nodes(const bbfmm_b200_batch *b);

@@ -102,6 +102,7 @@ def test_handle_setters_reject_null_handles_and_bad_values():
     L = _lib.lib()  # argument types as declared by bbfmm_b200._lib
     for k in (0, 1, 2):  # LAPLACIAN, LAPLACIAN_FORCE, ONEOVERR4
         assert L.bbfmm_b200_set_kernel(None, k) == 1
+        assert L.bbfmm_b200_batch_set_kernel(None, k) == 1
     assert L.bbfmm_b200_set_rank(None, 64) == 1
     assert L.bbfmm_b200_set_tc_products(None, 0) == 1
     assert L.bbfmm_b200_set_leaf_slab(None, 64) == 1

@@ -33,7 +33,7 @@ SPEC = [(5000, 8, 3, "u"), (12000, 4, 3, "c"), (0, 8, 3, "u"), (7000, 8, 3, "c")
         (3000, 4, 2, "u"), (20000, 4, 3, "u"), (9000, 8, 4, "c")]
 
 
-def _single(sets, q, offsets, mode):
+def _single(sets, q, offsets, mode, kernel="laplacian"):
     import torch
     from bbfmm_b200 import Solver
     out = np.zeros(q.size)
@@ -41,7 +41,7 @@ def _single(sets, q, offsets, mode):
         a, b = offsets[k], offsets[k + 1]
         if b == a:
             continue
-        s = Solver(n, lev, 1.0, mode=mode)
+        s = Solver(n, lev, 1.0, mode=mode, kernel=kernel)
         s.set_particles(x)
         out[a:b] = s.solve(torch.as_tensor(q[a:b], device="cuda")).double().cpu().numpy()
         s.close()
@@ -117,6 +117,32 @@ def test_mixed_batch_error_vs_direct():
         ref = direct(torch.as_tensor(x, device="cuda"), qd[a:e], torch.as_tensor(t, device="cuda")).cpu().numpy()
         err = {m: rel_l2(res[m][a:e][t], ref) for m in res}
         assert err["mixed"] <= 1.2 * err["d"] + 1e-9, (k, err)
+
+
+@pytest.mark.parametrize("kernel", ["oneoverr4", "laplacianforce"])
+def test_batch_other_kernels(kernel):
+    """The 1/r^4 and x / r^3 kernels in a batch (bbfmm_b200_batch_set_kernel): FP64 sets equal
+    single-set FP64 solvers of that kernel (relative L2 1e-13, as for 1/r), graph replay equals
+    eager launch bitwise, and the mixed batch is within 1e-5 relative L2 of the FP64 batch per
+    set (the mixed single-solver bound of these kernels)."""
+    import torch
+    from bbfmm_b200 import Batch
+    sets, q = _sets(6, SPEC[:6])
+    qd = torch.as_tensor(q, device="cuda")
+    b = Batch(sets, mode="d", kernel=kernel)
+    eager = b.solve(qd, graph=False).cpu().numpy()
+    got = b.solve(qd, graph=True).cpu().numpy()
+    assert np.array_equal(eager, got)
+    b.close()
+    want = _single(sets, q, b.offsets, "d", kernel)
+    bm = Batch(sets, mode="mixed", kernel=kernel)
+    mixed = bm.solve(qd).cpu().numpy()
+    bm.close()
+    for k in range(len(sets)):
+        a, e = b.offsets[k], b.offsets[k + 1]
+        if e > a:
+            assert rel_l2(got[a:e], want[a:e]) < 1e-13, k
+            assert rel_l2(mixed[a:e], got[a:e]) < 1e-5, (k, rel_l2(mixed[a:e], got[a:e]))
 
 
 def test_mixed_mode_order4_single_solver(oracle_d):
