@@ -43,7 +43,7 @@ SMS, MAX_SM_MHZ = 148, 1965.0
 DMMA_TFLOPS = SMS * 128 * MAX_SM_MHZ * 1e6 / 1e12
 # FP32 SIMT peak (an FMA as two flops per lane, 128 lanes per SM)
 FP32_TFLOPS = SMS * 256 * MAX_SM_MHZ * 1e6 / 1e12
-# Near-field roof of the survey: min(FP32 issue / 7 FP32 operations per pair, reciprocal
+# Near-field roof: min(FP32 issue / 7 FP32 operations per pair, reciprocal
 # square roots at 16 per clock per SM), in pairs/s at the maximum SM clock
 P2P_ROOF_PAIRS = min(SMS * 128 * MAX_SM_MHZ * 1e6 / 7, SMS * 16 * MAX_SM_MHZ * 1e6)
 

@@ -1,4 +1,4 @@
-"""bench.py's reference arm on the CPU: the JSON line the driver parses (keys, types, the
+"""bench.py's reference arm on the CPU: the JSON line a benchmark harness parses (keys, types, the
 reference-arm fields) and the silent exit of ranks other than 0 under a multi-rank launch."""
 import json
 import os
