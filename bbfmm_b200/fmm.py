@@ -305,11 +305,13 @@ def leaf_of_particles(xyz, L: float, level: int, fp32: bool = False):
     return leaf, counts
 
 
-def refinement_plan(xyz, L: float, depth: int, cap: int):
+def refinement_plan(xyz, L: float, depth: int, cap: int, fp32: bool = False):
     """Heavy leaves of a set at `depth` (more than cap particles; a Morton-order mask of 8^depth
     cells), the particles inside their 3 x 3 x 3 neighbourhoods (`sel`, indices into xyz) and,
-    among those, the ones in heavy leaves (`keep`, a mask over sel)."""
-    leaf, counts = leaf_of_particles(xyz, L, depth)
+    among those, the ones in heavy leaves (`keep`, a mask over sel). Leaves are assigned as the
+    solvers assign them: from FP32 positions when fp32 (an FP32 solver's own view; a particle
+    within FP32 rounding of a leaf face can sit in another leaf than its FP64 position says)."""
+    leaf, counts = leaf_of_particles(xyz, L, depth, fp32=fp32)
     heavy = counts > cap
     if not heavy.any():
         return heavy, np.zeros(0, np.int64), np.zeros(0, bool)
@@ -367,7 +369,7 @@ class AdaptiveSolver:
         x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
         self.N = x.shape[0]
         self.coarse.set_particles(x)
-        heavy, sel, keep = refinement_plan(x, self.L, self.Dc, self.cap)
+        heavy, sel, keep = refinement_plan(x, self.L, self.Dc, self.cap, fp32=self.mode == "s")
         self.heavy_leaves = int(heavy.sum())
         if self.fine is not None:
             self.fine.close()
@@ -419,7 +421,7 @@ class AdaptiveBatch:
         self.heavy_leaves = 0
         for s, (x, n, lev) in enumerate(sets):
             x = np.asarray(x, np.float64).reshape(-1, 3)
-            heavy, sel, keep = refinement_plan(x, L, lev, cap)
+            heavy, sel, keep = refinement_plan(x, L, lev, cap, fp32=mode == "s")
             light.append(~heavy)
             if heavy.any() and lev + refine <= 10:
                 self.heavy_leaves += int(heavy.sum())

@@ -175,3 +175,45 @@ def test_ascii_single_operator_text_rounds_once():
     assert got.dtype == np.float32 and np.array_equal(got, want)
     assert got[0] != np.float32(float(tokens[0]))  # the double rounding it avoids
     assert np.array_equal(_parse_text(tokens, False), np.array([float(t) for t in tokens]))
+
+
+def _plan_brute(xyz, L, depth, cap, dtype):
+    """Refinement plan by direct enumeration: each particle's leaf grid cell from truncated
+    (x + L/2) / leaf length in `dtype` (the leaf sort's arithmetic), heavy leaves by count, and
+    a particle selected when a heavy leaf lies within one cell of its own along every axis."""
+    x = np.asarray(xyz, dtype)
+    m = 2 ** depth
+    inv = dtype(1) / (dtype(L) * dtype(0.5) ** depth)
+    g = np.minimum(((x + dtype(L) / dtype(2)) * inv).astype(np.int64), m - 1)
+    key = (g[:, 0] * m + g[:, 1]) * m + g[:, 2]
+    cnt = np.bincount(key, minlength=m ** 3)
+    hv = np.nonzero(cnt > cap)[0]
+    hg = np.stack([hv // (m * m), (hv // m) % m, hv % m], 1)
+    near = (np.abs(g[:, None, :] - hg[None, :, :]).max(2) <= 1).any(1)
+    return cnt > cap, key, near
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_refinement_plan_equals_enumeration(fp32):
+    """fmm.refinement_plan (heavy leaves, their neighbourhoods' particles, the heavy ones among
+    them) against a direct enumeration in the leaf sort's own precision, on clustered points
+    that include particles within FP32 rounding of leaf faces."""
+    from bbfmm_b200.fmm import morton_to_grid, refinement_plan
+    rng = np.random.default_rng(3)
+    L, depth, cap = 1.0, 3, 40
+    x = np.clip(rng.uniform(0.2, 0.8, (3, 3))[rng.integers(0, 3, 4000)] + 0.03 * rng.standard_normal((4000, 3)),
+                0.0, np.nextafter(1.0, 0.0)) - 0.5
+    # particles just below a leaf face in FP64 that round onto it in FP32
+    face = -0.5 + np.arange(1, 8) / 8.0
+    x[:7, 0] = face - 1e-12
+    x[7:14, 1] = face - 1e-12
+    heavy, sel, keep = refinement_plan(x, L, depth, cap, fp32=fp32)
+    h_b, key, near = _plan_brute(x, L, depth, cap, np.float32 if fp32 else np.float64)
+    gx, gy, gz = morton_to_grid(np.arange(8 ** depth), depth)
+    m = 2 ** depth
+    assert np.array_equal(heavy, h_b[(gx * m + gy) * m + gz])
+    assert heavy.any() and not heavy.all()
+    assert np.array_equal(sel, np.nonzero(near)[0])
+    assert np.array_equal(keep, h_b[key[sel]])
+    if fp32:  # the face particles change leaf between the two precisions
+        assert not np.array_equal(_plan_brute(x, L, depth, cap, np.float64)[1], key)
