@@ -64,6 +64,8 @@ def lib() -> C.CDLL:
         L.bbfmm_b200_tuning.argtypes = [vp, ip]
         L.bbfmm_b200_set_tuning.argtypes = [vp, ip]
         L.bbfmm_b200_batch_create.argtypes = [C.POINTER(Config), i, ip, ip, ip, vp, vp, vp, vp, vp, i, C.POINTER(vp)]
+        L.bbfmm_b200_batch_create_device.argtypes = [C.POINTER(Config), i, ip, ip, ip, vp, vp, vp, vp, vp, i,
+                                                     C.POINTER(vp)]
         L.bbfmm_b200_batch_solve.argtypes = [vp, vp, vp, i]
         L.bbfmm_b200_batch_autotune.argtypes = [vp, vp]
         L.bbfmm_b200_batch_set_target_regions.argtypes = [vp, i, vp, i]

@@ -11,7 +11,9 @@
 //
 // Particles: the caller's arrays hold all sets back to back (set s at offset
 // sum_{t<s} counts[t]); every group's permutation indexes those arrays directly, so q is
-// read and phi written in place, each group touching only its own sets' entries.
+// read and phi written in place, each group touching only its own sets' entries. The trees
+// are sorted on the host (positions in host memory) or on the device (positions in device
+// memory: one stable radix sort per group over (set slot, leaf) keys), with the same result.
 #include <algorithm>
 #include <cstdio>
 #include <map>
@@ -90,7 +92,7 @@ struct Batch {
 
   int create(int mode_, double L_, int device_, int lead, int lead_rows, int nsets_, const int *n_of,
              const int *maxlev_of, const int *counts, const T *xyz, const void *const *U_by_n,
-             const void *const *E_by_n, int ops_fp32) {
+             const void *const *E_by_n, int ops_fp32, bool xyz_on_device = false) {
     mode = mode_;
     L = L_;
     device = device_;
@@ -140,6 +142,16 @@ struct Batch {
         owner[g.n] = &sv;
       } else {
         TRY_(sv.share_operators(*it->second));
+      }
+      if (xyz_on_device) {  // the group's trees in one device sort
+        std::vector<int> offs(g.sets.size()), cnts(g.sets.size());
+        for (size_t j = 0; j < g.sets.size(); ++j) {
+          offs[j] = (int)off[g.sets[j]];
+          cnts[j] = counts[g.sets[j]];
+        }
+        TRY_(sv.set_particles_sets_device((int)g.sets.size(), offs.data(), cnts.data(), (int)ntotal, xyz));
+        BBFMM_CUDA_OK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+        continue;
       }
       // per set: leaf sort on the host, then one permutation / leaf table over the group
       const int64_t nl = pow8i(g.maxlev);
@@ -255,9 +267,9 @@ struct bbfmm_b200_batch {
 
 extern "C" {
 
-int bbfmm_b200_batch_create(const bbfmm_b200_config *cfg, int nsets, const int *n, const int *maxlev,
-                            const int *counts, const void *xyz, const void *U4, const void *E4, const void *U8,
-                            const void *E8, int operators_fp32, bbfmm_b200_batch **out) {
+static int batch_create(const bbfmm_b200_config *cfg, int nsets, const int *n, const int *maxlev, const int *counts,
+                        const void *xyz, const void *U4, const void *E4, const void *U8, const void *E8,
+                        int operators_fp32, bool xyz_on_device, bbfmm_b200_batch **out) {
   if (!cfg || !out || !n || !maxlev || !counts || (nsets > 0 && !xyz))
     return bbfmm_set_error(BBFMM_ERR_ARG, "null argument");
   *out = nullptr;
@@ -267,15 +279,27 @@ int bbfmm_b200_batch_create(const bbfmm_b200_config *cfg, int nsets, const int *
   if (cfg->mode == BBFMM_B200_MODE_S) {
     b->f.reset(new bbfmm::Batch<float>());
     rc = b->f->create(cfg->mode, cfg->L, cfg->device, cfg->lead, cfg->lead_rows, nsets, n, maxlev, counts,
-                      (const float *)xyz, U, E, operators_fp32);
+                      (const float *)xyz, U, E, operators_fp32, xyz_on_device);
   } else {
     b->d.reset(new bbfmm::Batch<double>());
     rc = b->d->create(cfg->mode, cfg->L, cfg->device, cfg->lead, cfg->lead_rows, nsets, n, maxlev, counts,
-                      (const double *)xyz, U, E, operators_fp32);
+                      (const double *)xyz, U, E, operators_fp32, xyz_on_device);
   }
   if (rc != BBFMM_OK) return rc;
   *out = b.release();
   return BBFMM_OK;
+}
+
+int bbfmm_b200_batch_create(const bbfmm_b200_config *cfg, int nsets, const int *n, const int *maxlev,
+                            const int *counts, const void *xyz, const void *U4, const void *E4, const void *U8,
+                            const void *E8, int operators_fp32, bbfmm_b200_batch **out) {
+  return batch_create(cfg, nsets, n, maxlev, counts, xyz, U4, E4, U8, E8, operators_fp32, false, out);
+}
+
+int bbfmm_b200_batch_create_device(const bbfmm_b200_config *cfg, int nsets, const int *n, const int *maxlev,
+                                   const int *counts, const void *xyz_dev, const void *U4, const void *E4,
+                                   const void *U8, const void *E8, int operators_fp32, bbfmm_b200_batch **out) {
+  return batch_create(cfg, nsets, n, maxlev, counts, xyz_dev, U4, E4, U8, E8, operators_fp32, true, out);
 }
 
 int bbfmm_b200_batch_solve(bbfmm_b200_batch *b, const void *q_dev, void *phi_dev, int use_graph) {

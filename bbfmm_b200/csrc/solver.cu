@@ -328,7 +328,26 @@ int Solver<T>::set_particles_global(int nsets_, int N_, const int *perm_h, const
 template <typename T>
 int Solver<T>::set_particles_device(int N_, const T *xyz_d) {
   if (N_ < 0 || (N_ > 0 && !xyz_d)) return bbfmm_set_error(BBFMM_ERR_ARG, "bad particle arguments");
-  nsets = 1;
+  const int off = 0;
+  return set_particles_sets_device(1, &off, &N_, N_, xyz_d);
+}
+
+// The same state as set_particles_global, with the stacked sets' octrees built on the device
+// (build_tree_device_sets: per set the host sort's perm and leaf_start, bit for bit).
+template <typename T>
+int Solver<T>::set_particles_sets_device(int nsets_, const int *off_h, const int *count_h, int Nxyz, const T *xyz_d) {
+  if (nsets_ < 1 || nsets_ * pow8i(maxlev) > (int64_t)1 << 30)
+    return bbfmm_set_error(BBFMM_ERR_ARG, "number of stacked sets out of range");
+  int64_t total = 0;
+  for (int j = 0; j < nsets_; ++j) {
+    if (count_h[j] < 0 || off_h[j] < 0 || (int64_t)off_h[j] + count_h[j] > Nxyz)
+      return bbfmm_set_error(BBFMM_ERR_ARG, "set range outside the positions array");
+    total += count_h[j];
+  }
+  if (total > 0x7fffffff) return bbfmm_set_error(BBFMM_ERR_ARG, "more than 2^31 - 1 particles");
+  if (total > 0 && !xyz_d) return bbfmm_set_error(BBFMM_ERR_ARG, "bad particle arguments");
+  const int N_ = (int)total;
+  nsets = nsets_;
   const int64_t nl = cells(maxlev);
   if (perm) { cudaFree(perm); cudaFree(leaf_start); cudaFree(pos4); cudaFree(phis); }
   if (near_work) cudaFree(near_work);
@@ -347,7 +366,7 @@ int Solver<T>::set_particles_device(int N_, const T *xyz_d) {
   TRY(dalloc(&leaf_start, nl + 1));
   TRY(dalloc(&pos4, 4 * (size_t)(N > 0 ? N : 1)));
   TRY(dalloc(&phis, N > 0 ? N : 1));
-  TRY(build_tree_device<T>(N, xyz_d, (T)L, maxlev, perm, leaf_start, stream));
+  TRY(build_tree_device_sets<T>(nsets, off_h, count_h, xyz_d, (T)L, maxlev, perm, leaf_start, stream));
   TRY(build_near_work());
   if (N > 0) TRY((launch_gather<T, T>(N, perm, xyz_d, nullptr, pos4, stream)));
   TRY(alloc_work());

@@ -28,6 +28,11 @@ enum Stage {
 // level can be processed in slabs; count < 0 means every cell from `first` on.
 template <typename T>
 int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf_start, cudaStream_t s);
+// The same for nseg stacked sets, set j the particles xyz[off[j] .. off[j] + count[j]) (off and
+// count on the host, every range inside the positions array): perm holds indices into xyz.
+template <typename T>
+int build_tree_device_sets(int nseg, const int *off, const int *count, const T *xyz, T L, int maxlev, int *perm,
+                           int *leaf_start, cudaStream_t s);
 template <typename T> int launch_p2m(int n, const T *pos4, const int *leaf_start, int maxlev, T L, const Tables &t, T *S, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1, void *Ssplit = nullptr, const int64_t *rows = nullptr);
 template <typename T> int launch_m2m(int n, const T *Sc, T *Sp, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
 template <typename T> int launch_l2l(int n, const T *Fp, T *Fc, int level, const Tables &t, cudaStream_t s, int nsets = 1, int64_t first = 0, int64_t count = -1);
@@ -274,6 +279,10 @@ struct Solver {
   int set_operators(const T *U, const T *E);                              // host, reference layout
   // positions already on the device ([N][3], this solver's precision): the tree is built there
   int set_particles_device(int N_, const T *xyz_dev);
+  // nsets_ stacked sets whose positions are on the device: set j is the particles
+  // xyz_dev[off_host[j] .. off_host[j] + count_host[j]) of an array of Nxyz (the tree of every set
+  // built there, one sort for all; perm indexes that array, as for set_particles_global)
+  int set_particles_sets_device(int nsets_, const int *off_host, const int *count_host, int Nxyz, const T *xyz_dev);
   int set_particles_sorted(int N_, const int *perm_host, const int *leaf_start_host, const T *xyz_host);
   // N_ particles of nsets_ stacked sets: perm_host[k] indexes the caller's arrays of Nxyz
   // particles (positions xyz_host, and later q and phi); leaf_start_host has nsets_ 8^maxlev + 1

@@ -13,7 +13,14 @@
 //    ranks from a block-wide scan of the per-thread digit counts. Each pass keeps the
 //    relative order of equal digits, so the result is the stable order by key.
 //  * leaf_start[m] = the first sorted position whose key is >= m (a binary search per leaf).
+//
+// Several particle sets stacked for one solver (a batch group: set slot j owns the leaves
+// [j 8^maxlev, (j+1) 8^maxlev)) are one sort: slot j's particles are the range [off_j, off_j +
+// count_j) of the positions array, their keys j 8^maxlev + leaf and their indices global, so
+// the stable order is each set's own stable leaf order, set after set -- what per-set host
+// sorts concatenated give.
 #include <utility>
+#include <vector>
 
 #include "common.cuh"
 
@@ -31,16 +38,26 @@ template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
 template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
 template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
 
+// Sort item i belongs to slot j with base[j] <= i < base[j + 1] (base[0] = 0, base[nseg] = N;
+// empty slots repeat a base) and is particle g = off[j] + i - base[j] of xyz.
 template <typename T>
-__global__ void tree_keys_kernel(int N, const T *__restrict__ xyz, T L0half, T iLm, int maxlev, int *__restrict__ key,
+__global__ void tree_keys_kernel(int N, int nseg, const int *__restrict__ base, const int *__restrict__ off,
+                                 const T *__restrict__ xyz, T L0half, T iLm, int maxlev, int *__restrict__ key,
                                  int *__restrict__ idx) {
   const int ncpd = 1 << maxlev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const T x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
+    int lo = 0, hi = nseg;  // base[lo] <= i < base[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (base[mid] <= i) lo = mid;
+      else hi = mid;
+    }
+    const int g = off[lo] + (i - base[lo]);
+    const T x = xyz[3 * (int64_t)g], y = xyz[3 * (int64_t)g + 1], z = xyz[3 * (int64_t)g + 2];
     if (!(x >= -L0half && x <= L0half && y >= -L0half && y <= L0half && z >= -L0half && z <= L0half)) {
       g_tree_status = 1;
       key[i] = 0;
-      idx[i] = i;
+      idx[i] = g;
       continue;
     }
     int ix = (int)mul_rn<T>(add_rn<T>(x, L0half), iLm);
@@ -49,8 +66,8 @@ __global__ void tree_keys_kernel(int N, const T *__restrict__ xyz, T L0half, T i
     if (ix > ncpd - 1) ix = ncpd - 1;
     if (iy > ncpd - 1) iy = ncpd - 1;
     if (iz > ncpd - 1) iz = ncpd - 1;
-    key[i] = (int)grid_to_morton(ix, iy, iz, maxlev);
-    idx[i] = i;
+    key[i] = (int)(((int64_t)lo << (3 * maxlev)) + grid_to_morton(ix, iy, iz, maxlev));
+    idx[i] = g;
   }
 }
 
@@ -210,13 +227,27 @@ static int scan_exclusive(int64_t n, int *data, int *sums, cudaStream_t s) {
   return bbfmm_set_cuda_error(cudaGetLastError(), "tree scan", __FILE__, __LINE__);
 }
 
-// perm (N) and leaf_start (8^maxlev + 1) on the device for N particles at xyz (device, [N][3]).
-// Scratch: 4 N + 16 ceil(N / 4096) + ceil(that / 4096) + 1 ints, allocated here.
+// perm (N = sum of counts) and leaf_start (nseg 8^maxlev + 1) on the device for the stacked
+// sets whose particles are xyz[off[j] .. off[j] + count[j]) (device, [..][3]; off and count on
+// the host). Scratch: 4 N + 16 ceil(N / 4096) + ceil(that / 4096) + 1 + 2 nseg + 1 ints,
+// allocated here.
 template <typename T>
-int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf_start, cudaStream_t s) {
-  if (N < 0 || maxlev < BBFMM_MINLEV || maxlev > 10)
-    return bbfmm_set_error(BBFMM_ERR_ARG, "need N >= 0 and 2 <= maxlev <= 10");
-  const int64_t nleaf = pow8i(maxlev);
+int build_tree_device_sets(int nseg, const int *off_h, const int *count_h, const T *xyz, T L, int maxlev, int *perm,
+                           int *leaf_start, cudaStream_t s) {
+  if (nseg < 1 || maxlev < BBFMM_MINLEV || maxlev > 10 || nseg * pow8i(maxlev) > ((int64_t)1 << 30))
+    return bbfmm_set_error(BBFMM_ERR_ARG, "need 1 <= sets, 2 <= maxlev <= 10 and sets x 8^maxlev <= 2^30");
+  std::vector<int> seg(2 * (size_t)nseg + 1);  // base[0..nseg], then off[0..nseg)
+  int64_t total = 0;
+  for (int j = 0; j < nseg; ++j) {
+    if (count_h[j] < 0 || off_h[j] < 0) return bbfmm_set_error(BBFMM_ERR_ARG, "negative set offset or size");
+    seg[j] = (int)total;
+    seg[nseg + 1 + j] = off_h[j];
+    total += count_h[j];
+    if (total > 0x7fffffff) return bbfmm_set_error(BBFMM_ERR_ARG, "more than 2^31 - 1 particles");
+  }
+  seg[nseg] = (int)total;
+  const int N = (int)total;
+  const int64_t nleaf = nseg * pow8i(maxlev);
   if (N == 0) {
     BBFMM_CUDA_OK(cudaMemsetAsync(leaf_start, 0, sizeof(int) * (nleaf + 1), s));
     return bbfmm_set_cuda_error(cudaStreamSynchronize(s), "tree build", __FILE__, __LINE__);
@@ -228,20 +259,22 @@ int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf
   const int64_t nh = (int64_t)tr::DIGITS * nb;
   const int64_t nsum = (nh + tr::TILE - 1) / tr::TILE + 1;
   int *buf = nullptr;
-  const size_t words = 4 * (size_t)N + nh + nsum + 1;
+  const size_t words = 4 * (size_t)N + nh + nsum + 1 + seg.size();
   cudaError_t e = cudaMalloc(&buf, words * sizeof(int));
   if (e != cudaSuccess) return bbfmm_set_cuda_error(e, "tree build scratch", __FILE__, __LINE__);
   int *k0 = buf, *i0 = buf + N, *k1 = buf + 2 * (size_t)N, *i1 = buf + 3 * (size_t)N;
-  int *hist = buf + 4 * (size_t)N, *sums = hist + nh;
+  int *hist = buf + 4 * (size_t)N, *sums = hist + nh, *seg_d = sums + nsum + 1;
   int rc = BBFMM_OK;
   const int zero = 0;
-  e = cudaMemcpyToSymbolAsync(tr::g_tree_status, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+  e = cudaMemcpyAsync(seg_d, seg.data(), sizeof(int) * seg.size(), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(tr::g_tree_status, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     const int g = (int)((N + 255) / 256 < 148 * 32 ? (N + 255) / 256 : 148 * 32);
-    tr::tree_keys_kernel<T><<<g, 256, 0, s>>>(N, xyz, L0half, iLm, maxlev, k0, i0);
+    tr::tree_keys_kernel<T><<<g, 256, 0, s>>>(N, nseg, seg_d, seg_d + nseg + 1, xyz, L0half, iLm, maxlev, k0, i0);
     e = cudaGetLastError();
   }
-  const int bits = 3 * maxlev;
+  int bits = 3 * maxlev;  // keys < nseg 8^maxlev
+  while (((int64_t)1 << bits) < nleaf) ++bits;
   for (int shift = 0; e == cudaSuccess && rc == BBFMM_OK && shift < bits; shift += 4) {
     tr::radix_hist_kernel<<<nb, tr::THREADS, 0, s>>>(N, k0, shift, hist);
     rc = scan_exclusive(nh, hist, sums, s);
@@ -268,7 +301,19 @@ int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf
   return BBFMM_OK;
 }
 
+// One set: perm (N) and leaf_start (8^maxlev + 1) for the N particles at xyz.
+template <typename T>
+int build_tree_device(int N, const T *xyz, T L, int maxlev, int *perm, int *leaf_start, cudaStream_t s) {
+  if (N < 0) return bbfmm_set_error(BBFMM_ERR_ARG, "need N >= 0");
+  const int off = 0;
+  return build_tree_device_sets<T>(1, &off, &N, xyz, L, maxlev, perm, leaf_start, s);
+}
+
 template int build_tree_device<double>(int, const double *, double, int, int *, int *, cudaStream_t);
 template int build_tree_device<float>(int, const float *, float, int, int *, int *, cudaStream_t);
+template int build_tree_device_sets<double>(int, const int *, const int *, const double *, double, int, int *, int *,
+                                            cudaStream_t);
+template int build_tree_device_sets<float>(int, const int *, const int *, const float *, float, int, int *, int *,
+                                           cudaStream_t);
 
 }  // namespace bbfmm

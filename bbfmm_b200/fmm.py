@@ -524,7 +524,9 @@ def shard_sets(costs, world: int):
 class Batch:
     """Many independent particle sets solved together (bbfmm_b200_batch_*).
 
-    sets: a list of (xyz, n, maxlev) with xyz an (N_s, 3) host array inside [-L/2, L/2]^3.
+    sets: a list of (xyz, n, maxlev) with xyz an (N_s, 3) array inside [-L/2, L/2]^3: host
+    arrays (the trees are sorted on the host) or, all of them, CUDA tensors (the trees are built
+    on the GPU, bbfmm_b200_batch_create_device; the same particle order and leaf ranges).
     Charges and results are CUDA tensors holding the sets back to back in list order
     (``offsets[s]:offsets[s + 1]``). kernel: as for Solver, one for every set."""
 
@@ -535,14 +537,20 @@ class Batch:
         self.mode, self.L, self.device = mode, float(L), device
         self.dtype = torch.float32 if mode == "s" else torch.float64
         np_dtype = np.float32 if mode == "s" else np.float64
-        counts = np.array([len(x) for x, _, _ in sets], dtype=np.int32)
+        on_device = len(sets) > 0 and all(isinstance(x, torch.Tensor) and x.is_cuda for x, _, _ in sets)
+        counts = np.array([(x.numel() if on_device else np.asarray(x).size) // 3 for x, _, _ in sets], dtype=np.int32)
         ns = np.array([n for _, n, _ in sets], dtype=np.int32)
         levs = np.array([lv for _, _, lv in sets], dtype=np.int32)
         self.depths = levs.tolist()
         self.offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         self.N = int(self.offsets[-1])
-        xyz = np.ascontiguousarray(np.concatenate([np.asarray(x, np_dtype).reshape(-1, 3) for x, _, _ in sets])
-                                   if len(sets) else np.zeros((0, 3), np_dtype))
+        if on_device:
+            xyz = torch.cat([x.to(device=f"cuda:{device}", dtype=self.dtype).reshape(-1, 3) for x, _, _ in sets])
+            xyz = xyz.contiguous()
+            torch.cuda.synchronize(xyz.device)  # the batch's streams read xyz
+        else:
+            xyz = np.ascontiguousarray(np.concatenate([np.asarray(x, np_dtype).reshape(-1, 3) for x, _, _ in sets])
+                                       if len(sets) else np.zeros((0, 3), np_dtype))
         if kernel not in ops.KERNELS:
             raise ValueError(f"unknown kernel {kernel!r} ({', '.join(ops.KERNELS)})")
         self.kernel = kernel
@@ -556,9 +564,10 @@ class Batch:
                           lead_rows=lead_rows if mode == "mixed" else 0, device=device, stream=None)
         h = C.c_void_p()
         ip = C.POINTER(C.c_int)
-        _lib.check(_lib.lib().bbfmm_b200_batch_create(C.byref(cfg), len(sets), ns.ctypes.data_as(ip),
-                                                       levs.ctypes.data_as(ip), counts.ctypes.data_as(ip), _ptr(xyz),
-                                                       p(4, 0), p(4, 1), p(8, 0), p(8, 1), fp32, C.byref(h)))
+        create = _lib.lib().bbfmm_b200_batch_create_device if on_device else _lib.lib().bbfmm_b200_batch_create
+        _lib.check(create(C.byref(cfg), len(sets), ns.ctypes.data_as(ip), levs.ctypes.data_as(ip),
+                          counts.ctypes.data_as(ip), _ptr(xyz),
+                          p(4, 0), p(4, 1), p(8, 0), p(8, 1), fp32, C.byref(h)))
         self.h = h
         if kernel != "laplacian":
             _lib.check(_lib.lib().bbfmm_b200_batch_set_kernel(h, ops.KERNELS[kernel][1]))

@@ -321,6 +321,15 @@ BBFMM_B200_API int bbfmm_b200_batch_create(const bbfmm_b200_config *cfg, int nse
                                            const int *counts, const void *xyz, const void *U4, const void *E4,
                                            const void *U8, const void *E8, int operators_fp32,
                                            bbfmm_b200_batch **out);
+/* The same with the positions in device memory on cfg->device (xyz_dev, the sets back to back,
+ * in the batch's precision: FP32 for BBFMM_B200_MODE_S, else FP64): every group's octrees are
+ * built there by one stable radix sort over (set, Morton leaf) keys -- per set the particle order
+ * and leaf ranges of the host sort, bit for bit, so every solve is the same. Particles outside
+ * [-L/2, L/2]^3 are rejected with BBFMM_B200_ERR_ARG. Synchronises the device. */
+BBFMM_B200_API int bbfmm_b200_batch_create_device(const bbfmm_b200_config *cfg, int nsets, const int *n,
+                                                  const int *maxlev, const int *counts, const void *xyz_dev,
+                                                  const void *U4, const void *E4, const void *U8, const void *E8,
+                                                  int operators_fp32, bbfmm_b200_batch **out);
 /* One solve of every set (phi as in bbfmm_b200_solve), on the batch stream, without
  * synchronising; use_graph != 0 replays the captured graph. */
 BBFMM_B200_API int bbfmm_b200_batch_solve(bbfmm_b200_batch *b, const void *q_dev, void *phi_dev, int use_graph);
