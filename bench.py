@@ -708,6 +708,15 @@ def run_batch_256(args, adaptive=False):
         ph.copy_(out, non_blocking=True)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    t_setup_dev = None
+    if not adaptive:  # the same batch from positions already on the device (trees sorted there)
+        dsets = [(torch.as_tensor(x, dtype=dt, device="cuda"), n, lev) for x, n, lev in sets]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bd = Batch(dsets, mode=mode, device=local)
+        t_setup_dev = time.perf_counter() - t0
+        bd.close()
+        del dsets
     cpu = None
     if not args.no_cpu_baseline and rank == 0:
         # the reference CPU code on 4 of the sets (one per (n, depth) seen first), scaled by particles
@@ -742,7 +751,7 @@ def run_batch_256(args, adaptive=False):
             "adaptive": {"heavy_leaves": b.heavy_leaves, "refined_particles": b.refined_particles,
                          "cap": 256, "refine_levels": 2} if adaptive else None,
             "group_stage_ms": group_ms,
-            "setup_s": t_setup, "autotune_s": t_tune,
+            "setup_s": t_setup, "setup_device_trees_s": t_setup_dev, "autotune_s": t_tune,
             "err_vs_fp64_direct": {"median": float(np.median(errs)), "max": float(errs.max()),
                                    "max_n4": float(errs[ns == 4].max()), "max_n8": float(errs[ns == 8].max()),
                                    "targets_per_set": 512},
