@@ -310,7 +310,10 @@ def refinement_plan(xyz, L: float, depth: int, cap: int, fp32: bool = False):
     cells), the particles inside their 3 x 3 x 3 neighbourhoods (`sel`, indices into xyz) and,
     among those, the ones in heavy leaves (`keep`, a mask over sel). Leaves are assigned as the
     solvers assign them: from FP32 positions when fp32 (an FP32 solver's own view; a particle
-    within FP32 rounding of a leaf face can sit in another leaf than its FP64 position says)."""
+    within FP32 rounding of a leaf face can sit in another leaf than its FP64 position says).
+    xyz a torch tensor: the same plan computed on its device, returned as tensors there."""
+    if type(xyz).__module__.startswith("torch"):
+        return _refinement_plan_tensor(xyz, L, depth, cap, fp32)
     leaf, counts = leaf_of_particles(xyz, L, depth, fp32=fp32)
     heavy = counts > cap
     if not heavy.any():
@@ -327,6 +330,32 @@ def refinement_plan(xyz, L: float, depth: int, cap: int, fp32: bool = False):
     near_region = d[gx + 1, gy + 1, gz + 1]  # Morton order
     sel = np.nonzero(near_region[leaf])[0]
     return heavy, sel, heavy[leaf[sel]]
+
+
+def _refinement_plan_tensor(xyz, L: float, depth: int, cap: int, fp32: bool):
+    """refinement_plan on the tensor's device: the leaf sort's arithmetic ((x + L/2) times the
+    reciprocal leaf length, each operation rounded in the solver's precision, truncated and
+    clamped to the last leaf; anotherFMMDistribute.c:258-298), counts by bincount and the
+    3 x 3 x 3 neighbourhoods of the heavy leaves by a max filter."""
+    import torch
+    npdt, dt = (np.float32, torch.float32) if fp32 else (np.float64, torch.float64)
+    x = xyz.to(dt).reshape(-1, 3)
+    cel = npdt(L)
+    for _ in range(depth):
+        cel = npdt(cel * npdt(0.5))
+    half, inv = float(npdt(npdt(L) / npdt(2))), float(npdt(npdt(1) / cel))  # exact in dt
+    m = 2 ** depth
+    g = ((x + half) * inv).to(torch.int64).clamp_(max=m - 1)
+    key = (g[:, 0] * m + g[:, 1]) * m + g[:, 2]
+    heavy_g = torch.bincount(key, minlength=m ** 3) > cap
+    gx, gy, gz = morton_to_grid(np.arange(8 ** depth), depth)
+    heavy = heavy_g[torch.as_tensor((gx * m + gy) * m + gz, device=x.device)]  # Morton order
+    if not bool(heavy_g.any()):
+        return heavy, torch.zeros(0, dtype=torch.int64, device=x.device), torch.zeros(0, dtype=torch.bool,
+                                                                                      device=x.device)
+    near_g = torch.nn.functional.max_pool3d(heavy_g.view(1, 1, m, m, m).float(), 3, stride=1, padding=1).view(-1) > 0
+    sel = torch.nonzero(near_g[key]).squeeze(1)
+    return heavy, sel, heavy_g[key[sel]]
 
 
 class AdaptiveSolver:
@@ -365,11 +394,19 @@ class AdaptiveSolver:
                 s.close()
 
     def set_particles(self, xyz):
+        """Positions as for Solver.set_particles: a host array, or a CUDA tensor (the trees and
+        the refinement plan are then built on the GPU)."""
         torch = self.coarse.torch
-        x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+        on_device = isinstance(xyz, torch.Tensor) and xyz.is_cuda
+        if on_device:
+            x = xyz.to(f"cuda:{self.device}").reshape(-1, 3)
+        else:
+            x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
         self.N = x.shape[0]
         self.coarse.set_particles(x)
         heavy, sel, keep = refinement_plan(x, self.L, self.Dc, self.cap, fp32=self.mode == "s")
+        if on_device:
+            heavy = heavy.cpu().numpy()
         self.heavy_leaves = int(heavy.sum())
         if self.fine is not None:
             self.fine.close()
@@ -384,9 +421,9 @@ class AdaptiveSolver:
         self.fine.set_target_region(self.Dc, heavy)
         dev = f"cuda:{self.device}"
         self.sel = torch.as_tensor(sel, device=dev)
-        self.keep_local = torch.as_tensor(np.nonzero(keep)[0], device=dev)
+        self.keep_local = torch.nonzero(keep).squeeze(1) if on_device else torch.as_tensor(np.nonzero(keep)[0], device=dev)
         self.keep_global = torch.as_tensor(sel[keep], device=dev)
-        self.fine_particles = int(sel.size)
+        self.fine_particles = int(sel.shape[0])
 
     def solve(self, q, out=None):
         """q: CUDA tensor (N,) -> q_i * phi_i (CUDA tensor) on the caller's stream."""
@@ -408,7 +445,8 @@ class AdaptiveBatch:
     the sets as given, whose near field skips the heavy leaves (more than `cap` particles), and a
     refined Batch of each set with heavy leaves -- the particles of their neighbourhoods, at the
     set's depth + `refine`, local expansions starting one level below the coarse leaves -- whose
-    results are added at the heavy leaves' particles. Charges and results as for Batch."""
+    results are added at the heavy leaves' particles. Charges and results as for Batch; positions
+    host arrays, or all CUDA tensors (the trees and the refinement plans built on the GPU)."""
 
     def __init__(self, sets, mode: str = "mixed", cap: int = 256, refine: int = 2, L: float = 1.0, **kw):
         import torch
@@ -416,21 +454,27 @@ class AdaptiveBatch:
         self.coarse = Batch(sets, mode=mode, L=L, **kw)
         self.offsets = self.coarse.offsets
         self.N = self.coarse.N
+        on_device = len(sets) > 0 and all(isinstance(x, torch.Tensor) and x.is_cuda for x, _, _ in sets)
+        nonzero = (lambda k: torch.nonzero(k).squeeze(1)) if on_device else (lambda k: np.nonzero(k)[0])
+        cat = torch.cat if on_device else np.concatenate
         light, refined, heavy_masks, sel_all, keep_local, keep_global = [], [], [], [], [], []
         rbase = 0
         self.heavy_leaves = 0
         for s, (x, n, lev) in enumerate(sets):
-            x = np.asarray(x, np.float64).reshape(-1, 3)
+            x = x.reshape(-1, 3) if on_device else np.asarray(x, np.float64).reshape(-1, 3)
             heavy, sel, keep = refinement_plan(x, L, lev, cap, fp32=mode == "s")
+            if on_device:
+                heavy = heavy.cpu().numpy()
             light.append(~heavy)
+            off = int(self.offsets[s])
             if heavy.any() and lev + refine <= 10:
                 self.heavy_leaves += int(heavy.sum())
                 refined.append((x[sel], n, lev + refine))
                 heavy_masks.append(heavy)
-                sel_all.append(self.offsets[s] + sel)
-                keep_global.append(self.offsets[s] + sel[keep])
-                keep_local.append(rbase + np.nonzero(keep)[0])
-                rbase += sel.size
+                sel_all.append(off + sel)
+                keep_global.append(off + sel[keep])
+                keep_local.append(rbase + nonzero(keep))
+                rbase += int(sel.shape[0])
             else:
                 light[-1] = np.ones_like(heavy)
         self.coarse.set_target_regions(0, np.concatenate(light))
@@ -440,9 +484,9 @@ class AdaptiveBatch:
             self.refined = Batch(refined, mode=mode, L=L, **kw)
             self.refined.set_target_regions(refine, np.concatenate(heavy_masks), first_m2l=True)
             dev = f"cuda:{self.coarse.device}"
-            self.sel = torch.as_tensor(np.concatenate(sel_all), device=dev)
-            self.keep_local = torch.as_tensor(np.concatenate(keep_local), device=dev)
-            self.keep_global = torch.as_tensor(np.concatenate(keep_global), device=dev)
+            self.sel = torch.as_tensor(cat(sel_all), device=dev)
+            self.keep_local = torch.as_tensor(cat(keep_local), device=dev)
+            self.keep_global = torch.as_tensor(cat(keep_global), device=dev)
             # fixed buffers for the refined batch, whose captured graph is tied to its pointers
             self.q_ref = torch.empty(rbase, dtype=self.coarse.dtype, device=dev)
             self.phi_ref = torch.empty_like(self.q_ref)

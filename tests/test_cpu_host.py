@@ -217,3 +217,29 @@ def test_refinement_plan_equals_enumeration(fp32):
     assert np.array_equal(keep, h_b[key[sel]])
     if fp32:  # the face particles change leaf between the two precisions
         assert not np.array_equal(_plan_brute(x, L, depth, cap, np.float64)[1], key)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+@pytest.mark.parametrize("L,depth", [(1.0, 3), (1.3, 4)])
+def test_refinement_plan_on_tensors_equals_host_plan(fp32, L, depth):
+    """The tensor form of the refinement plan (used for positions already on the GPU; run here on
+    CPU tensors) gives the host plan bit for bit: heavy leaves, selected particles and the kept
+    ones, with particles on and within rounding of leaf faces, and an L whose leaf length is not
+    a power of two."""
+    import torch
+    from bbfmm_b200.fmm import refinement_plan
+    rng = np.random.default_rng(5)
+    N = 6000
+    x = np.clip(rng.uniform(0.2, 0.8, (3, 3))[rng.integers(0, 3, N)] + 0.03 * rng.standard_normal((N, 3)),
+                0.0, np.nextafter(1.0, 0.0)) * L - L / 2
+    k = np.arange(1, 2 ** depth)
+    face = -L / 2 + k * (L / 2 ** depth)
+    x[:k.size, 0] = face
+    x[k.size:2 * k.size, 1] = np.nextafter(face, -1.0)
+    x[2 * k.size:2 * k.size + 2] = [[-L / 2] * 3, [L / 2] * 3]
+    cap = 30
+    want = refinement_plan(x, L, depth, cap, fp32=fp32)
+    got = refinement_plan(torch.as_tensor(x), L, depth, cap, fp32=fp32)
+    assert want[0].any() and want[1].size > 0
+    for w, g in zip(want, got):
+        assert np.array_equal(w, g.numpy())

@@ -208,3 +208,33 @@ def test_adaptive_batch_mixed_against_direct():
         # particles per leaf, whose FP64 error falls below what FP32 near-field sums resolve)
         assert e_a <= 1.2 * max(e_u, e_m), (k, e_a, e_u, e_m)
     b.close()
+
+
+@pytest.mark.parametrize("mode", ["d", "mixed"])
+def test_adaptive_from_device_positions_equals_host_positions(mode):
+    """AdaptiveBatch and AdaptiveSolver from positions already on the GPU -- trees and refinement
+    plans built there (the plan's leaf assignment in the solver's own arithmetic) -- give the
+    results of the host-built ones bit for bit."""
+    import torch
+    from bbfmm_b200 import AdaptiveBatch, AdaptiveSolver
+    sets, q = _batch_sets(24)
+    qd = torch.as_tensor(q, device="cuda")
+    out = []
+    for on_device in (False, True):
+        ss = [(torch.as_tensor(x, device="cuda") if on_device else x, n, lev) for x, n, lev in sets]
+        b = AdaptiveBatch(ss, mode=mode, cap=256)
+        assert b.refined is not None and b.heavy_leaves > 0
+        out.append(b.solve(qd, graph=False).cpu().numpy())
+        b.close()
+    assert np.isfinite(out[0]).all()
+    assert np.array_equal(out[0], out[1])
+    x, q1 = _clustered(100000, 7)
+    q1d = torch.as_tensor(q1, device="cuda")
+    res = []
+    for on_device in (False, True):
+        a = AdaptiveSolver(8, 3, 5, mode=mode, cap=256)
+        a.set_particles(torch.as_tensor(x, device="cuda") if on_device else x)
+        assert a.fine is not None
+        res.append(a.solve(q1d).cpu().numpy())
+        a.close()
+    assert np.array_equal(res[0], res[1])
