@@ -243,3 +243,17 @@ def test_refinement_plan_on_tensors_equals_host_plan(fp32, L, depth):
     assert want[0].any() and want[1].size > 0
     for w, g in zip(want, got):
         assert np.array_equal(w, g.numpy())
+
+
+def test_refinement_plan_of_an_empty_set_and_unknown_batch_kernel():
+    """Host logic that runs before any device work: an empty set has no heavy leaves in either
+    form of the plan, and a batch with an unknown kernel name is refused with ValueError."""
+    import torch
+    from bbfmm_b200 import Batch
+    from bbfmm_b200.fmm import refinement_plan
+    for x in (np.zeros((0, 3)), torch.zeros((0, 3), dtype=torch.float64)):
+        heavy, sel, keep = refinement_plan(x, 1.0, 2, 4)
+        assert len(heavy) == 64 and not np.asarray(heavy).any()
+        assert len(sel) == 0 and len(keep) == 0
+    with pytest.raises(ValueError):
+        Batch([(np.zeros((1, 3)), 4, 2)], kernel="oneoverr3")
