@@ -105,8 +105,12 @@ def test_m2l_drv_and_near_field_symbols(oracle_d):
     want = oracle_d.m2l(t, 32, E, P)
     L = np.zeros_like(want)
     dp = C.POINTER(C.c_double)
-    shim.m2l_drv.argtypes = [C.c_int, dp, dp, dp, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 7 + [C.c_int]
-    args = [32, L.ctypes.data_as(dp), E.ctypes.data_as(dp), P.ctypes.data_as(dp), 2, lev, 1.0] + [None] * 7
+    vp, i = C.c_void_p, C.c_int
+    # r, L, K, M, minlev, maxlev, L0, center, ineigh, pitch_neighbors, neighbors, iinter,
+    # pitch_interaction, interaction, scheme (m2l_drv.cu:14-19); the lists are implied, not read
+    shim.m2l_drv.argtypes = [i, dp, dp, dp, i, i, C.c_double, vp, vp, i, vp, vp, i, vp, i]
+    args = [32, L.ctypes.data_as(dp), E.ctypes.data_as(dp), P.ctypes.data_as(dp), 2, lev, 1.0,
+            None, None, 0, None, None, 0, None]
     assert shim.m2l_drv(*args, 3) == 0
     lo = 9 * 32
     assert rel_l2(L[lo:], want[lo:]) < 1e-12
