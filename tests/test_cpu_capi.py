@@ -22,6 +22,47 @@ def test_library_exports_every_declared_symbol():
         getattr(L, n)
 
 
+def _c_kind(decl):
+    """Kind of one C parameter or return type of include/bbfmm_b200.h."""
+    import re
+    d = decl.strip()
+    if d in ("", "void"):
+        return None
+    if "*" in d:
+        return "ptr"
+    for pat, k in ((r"long long", "i64"), (r"\bdouble\b", "f64"), (r"\bfloat\b", "f32"), (r"\bunsigned\b", "u32"),
+                   (r"\bint\b", "i32")):
+        if re.search(pat, d):
+            return k
+    return "?" + d
+
+
+def _py_kind(t):
+    if t is None:
+        return None
+    if t in (C.c_void_p, C.c_char_p) or (isinstance(t, type) and issubclass(t, C._Pointer)):
+        return "ptr"
+    return {C.c_int: "i32", C.c_double: "f64", C.c_float: "f32", C.c_uint: "u32", C.c_longlong: "i64"}.get(t, "?")
+
+
+def test_ctypes_declarations_match_the_header():
+    """Every function of include/bbfmm_b200.h has ctypes argument and result types in _lib.py of
+    the same kinds (int, unsigned, long long, float, double, pointer) in the same order."""
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(_lib.HERE), "include", "bbfmm_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    decls = re.findall(r"BBFMM_B200_API\s+([\w\s\*]+?)\s*\b(bbfmm_b200_\w+)\s*\(([^)]*)\)\s*;", src)
+    assert len(decls) >= 40
+    L = _lib.lib()
+    for ret, name, params in decls:
+        f = getattr(L, name)
+        want = [k for k in (_c_kind(p) for p in params.split(",")) if k is not None]
+        got = [_py_kind(t) for t in (f.argtypes or [])]
+        assert got == want, (name, got, want)
+        assert _py_kind(f.restype) == _c_kind(ret), (name, f.restype, ret)
+
+
 @pytest.mark.parametrize("shim", ["libbbfmm_b200_ref_d.so", "libbbfmm_b200_ref_s.so"])
 def test_reference_name_shims_export_the_reference_symbols(shim):
     import os
